@@ -1,0 +1,71 @@
+"""Seeded synthetic inputs for the Cartesian Darcy workloads.
+
+The reference project publishes no dataset for these problems, so every input
+is generated here deterministically from a seed:
+
+* ``lognormal_permeability``: log-kappa is a stationary Gaussian field with
+  exponential covariance ``sigma^2 exp(-|r|/ell)`` sampled on the fine-cell
+  centres of a regular grid by circulant embedding on a doubled periodic grid
+  (NumPy PCG64 generator, float64 FFTs).  Negative embedding eigenvalues, if
+  any, are clipped to zero and reported.
+* ``sine_source``: ``f = 2 pi^2 sin(pi x) sin(pi y)``, the manufactured source
+  whose exact pressure is ``sin(pi x) sin(pi y)`` with homogeneous Dirichlet data.
+
+Arrays follow the reference's pixel-field layout: ``values[ix, iy]`` with the
+first axis along x (``materials/cartesian.py:14-72`` of PyMHM).
+"""
+
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+
+DEFAULT_SEED = 20261203
+
+
+def lognormal_permeability(cells_x: int, cells_y: int | None = None, *, sigma: float = 2.0,
+                           ell: float = 0.05, seed: int = DEFAULT_SEED,
+                           extent: tuple[float, float] = (1.0, 1.0)) -> np.ndarray:
+    """Return ``exp(G)`` on a ``(cells_x, cells_y)`` grid of fine-cell centres.
+
+    ``G`` has zero mean and covariance ``sigma^2 exp(-|x-y|/ell)``.  The
+    embedding grid is ``2 cells`` per axis with the same spacing as the field.
+    """
+    cells_y = cells_x if cells_y is None else cells_y
+    hx, hy = extent[0] / cells_x, extent[1] / cells_y
+    mx, my = 2 * cells_x, 2 * cells_y
+    kx = np.arange(mx)
+    ky = np.arange(my)
+    dx = np.minimum(kx, mx - kx) * hx
+    dy = np.minimum(ky, my - ky) * hy
+    r = np.sqrt(dx[:, None] ** 2 + dy[None, :] ** 2)
+    cov = sigma ** 2 * np.exp(-r / ell)
+    eig = np.fft.fft2(cov).real
+    eig = np.maximum(eig, 0.0)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    z = rng.standard_normal((mx, my)) + 1j * rng.standard_normal((mx, my))
+    field = np.fft.fft2(np.sqrt(eig / (mx * my)) * z).real[:cells_x, :cells_y]
+    return np.exp(field)
+
+
+def sine_source(points: np.ndarray) -> np.ndarray:
+    """Manufactured source ``2 pi^2 sin(pi x) sin(pi y)``."""
+    return 2 * np.pi ** 2 * np.sin(np.pi * points[:, 0]) * np.sin(np.pi * points[:, 1])
+
+
+def sine_pressure(points: np.ndarray) -> np.ndarray:
+    return np.sin(np.pi * points[:, 0]) * np.sin(np.pi * points[:, 1])
+
+
+def digest(array: np.ndarray) -> str:
+    """SHA-256 of an array's C-order bytes (records seeded inputs and outputs)."""
+    a = np.ascontiguousarray(array)
+    return hashlib.sha256(a.tobytes()).hexdigest()
+
+
+# Workload descriptions used by bench.py and the parity tests.
+POISSON_8x8 = dict(name="poisson-q1-8x8-r4-p1", macro=8, local=4, face_degree=1,
+                   permeability="one", source="sine")
+DARCY_64x64 = dict(name="darcy-q1-64x64-r16-p2-lognormal", macro=64, local=16, face_degree=2,
+                   permeability="lognormal", source="one", sigma=2.0, ell=0.05, seed=DEFAULT_SEED)

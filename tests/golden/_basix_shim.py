@@ -1,0 +1,84 @@
+"""Clean-room stand-in for the two Basix tabulations the Cartesian Q1 path uses.
+
+Fixture generation only: this module is imported by ``make_golden.py`` in a
+development checkout, never by the library, the oracle or the GPU tests.
+
+PyMHM 1.3.2 reaches Basix (``fenics-basix`` 0.11.0 pinned in the project's
+``pixi.lock``) only through ``pymhm.fem.reference``.  The Cartesian Qk path
+calls two of its functions:
+
+* ``simplex_lagrange_tabulation("interval", k, bary, nodes=..., nderiv)``
+  (``src/pymhm/fem/reference.py:497-540``) from ``_cardinal_values``
+  (``src/pymhm/fem/scalar/quadrilateral.py:58-68``) and continuous faces;
+* ``legendre_values`` / ``legendre_tabulation``
+  (``src/pymhm/fem/reference.py:596-625``) from ``FaceSpace.evaluate``
+  (``src/pymhm/fem/traces/interval.py:54-89``).
+
+Both are restated here from their published mathematics: the nodal Lagrange
+basis on the declared node order (unique polynomial interpolant, obtained by a
+Legendre-Vandermonde solve) with exact Kronecker rows at literal nodes, as the
+reference wrapper enforces (``reference.py:484-488``); and the conventional
+Legendre polynomials ``L_j(1)=1`` by the three-term recurrence.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+from numpy.polynomial import legendre as npleg
+
+
+def _interval_lagrange(degree, points, nodes, nderiv):
+    x = np.asarray(points, dtype=float)
+    c = np.asarray(nodes, dtype=float)
+    # Vandermonde in shifted Legendre polynomials on [0, 1]: V[i, j] = P_j(2 c_i - 1)
+    vand = npleg.legvander(2 * c - 1, degree)
+    coef = np.linalg.solve(vand, np.eye(degree + 1))  # column j: coefficients of phi_j
+    vals = npleg.legvander(2 * x - 1, degree) @ coef
+    ders = np.zeros_like(vals)
+    if nderiv:
+        for j in range(degree + 1):
+            d = npleg.legder(coef[:, j]) * 2.0
+            ders[:, j] = npleg.legval(2 * x - 1, d) if len(d) else 0.0
+    rows, cols = np.nonzero(x[:, None] == c[None, :])
+    vals[rows] = 0.0
+    vals[rows, cols] = 1.0
+    return vals, ders
+
+
+def simplex_lagrange_tabulation(cell, degree, bary, *, nodes, nderiv=2):
+    if cell != "interval":
+        raise NotImplementedError("the fixture shim covers interval tabulation only")
+    bary = np.asarray(bary, dtype=float)
+    nodes = np.asarray(nodes, dtype=float)
+    vals, ders = _interval_lagrange(int(degree), bary[:, 1], nodes[:, 1], nderiv)
+    gradient = ders[:, :, None] if nderiv else np.empty((*vals.shape, 0))
+    hessian = np.empty((*vals.shape, 0, 0))
+    return vals, gradient, hessian
+
+
+def legendre_tabulation(points, degree, nderiv=0):
+    x = np.asarray(points, dtype=float)
+    out = np.zeros((nderiv + 1, *x.shape, degree + 1))
+    for j in range(degree + 1):
+        e = np.zeros(degree + 1)
+        e[j] = 1.0
+        out[0, ..., j] = npleg.legval(x, e)
+        for d in range(1, nderiv + 1):
+            e = npleg.legder(e)
+            out[d, ..., j] = npleg.legval(x, e) if len(e) else 0.0
+    return out
+
+
+def legendre_values(points, degree):
+    return legendre_tabulation(points, degree)[0]
+
+
+def install():
+    """Patch the reference modules in place (idempotent)."""
+    import pymhm.fem.reference as ref
+    import pymhm.fem.scalar.quadrilateral as quad
+
+    ref.simplex_lagrange_tabulation = simplex_lagrange_tabulation
+    ref.legendre_tabulation = legendre_tabulation
+    ref.legendre_values = legendre_values
+    quad.simplex_lagrange_tabulation = simplex_lagrange_tabulation
