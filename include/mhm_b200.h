@@ -1,0 +1,210 @@
+/*
+ * mhm_b200.h - C ABI of the B200 Primal-MHM hot path (libmhm_b200.so).
+ *
+ * Plain pointers and sizes only.  Every pointer argument is a device pointer
+ * unless its comment says "host"; every call is asynchronous on `stream`
+ * (a cudaStream_t passed as void*, NULL = legacy default stream) and returns
+ * an MHM_* status for argument/launch errors.  Per-cell numerical outcomes
+ * are reported in caller-owned status arrays after the stream completes.
+ * The library never allocates device memory: scratch space is passed in by
+ * the caller and sized with the matching *_workspace_bytes query.
+ *
+ * Reference interfaces (PyMHM 1.3.2, paths relative to src/pymhm/):
+ *   mhm_q1_condense        replaces _assemble_quad (_legacy/models/darcy/
+ *                          cartesian.py:69-83) + condense_local
+ *                          (core/condensation.py:21-122) + local_global_
+ *                          contribution (core/contributions.py:14-74) for all
+ *                          macrocells of a Cartesian Q1 problem at once.
+ *   mhm_skeleton_scatter   replaces assemble_hybrid_contributions
+ *                          (core/contributions.py:77-195) and the Numba
+ *                          leaves core/_assembly.py:10-42.
+ *   mhm_skeleton_solve     replaces solve_hybrid_system's global solve
+ *                          (core/system.py:355-528 -> linalg/linear.py:798)
+ *                          for Dirichlet/weak-boundary systems without gauges.
+ *   mhm_q1_reconstruct     replaces reconstruct_response (core/reconstruction.py:
+ *                          130-141) and the flux samples of
+ *                          QuadrilateralDarcySolution.evaluate
+ *                          (postprocessing/solutions.py:278-324).
+ *   mhm_batched_factor /   replace BatchedFactorization.__init__/solve
+ *   mhm_batched_solve      (execution/cuda.py:165-288): equilibrated dense LU
+ *                          with FP64 residual refinement.
+ */
+#ifndef MHM_B200_H
+#define MHM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Call status (return value of every entry point). */
+#define MHM_OK 0
+#define MHM_ERR_ARGUMENT 1     /* invalid sizes, modes or null pointers        */
+#define MHM_ERR_LAUNCH 2       /* a CUDA launch or attribute call failed        */
+#define MHM_ERR_UNSUPPORTED 3  /* problem too large for the on-chip layout      */
+
+/* Per-cell / per-matrix numerical status (written to status arrays). */
+#define MHM_CELL_OK 0
+#define MHM_CELL_KERNEL 1          /* declared constant kernel is not a nullspace  */
+#define MHM_CELL_SINGULAR_PIVOT 2  /* zero or negative pivot                       */
+#define MHM_CELL_RANK_DEFICIENT 3  /* pivot below eps * n * max pivot              */
+#define MHM_CELL_RESIDUAL 4        /* refinement did not reach the tolerance       */
+#define MHM_CELL_NONFINITE 5       /* non-finite input or result                   */
+#define MHM_CELL_ZERO_ROW 6        /* equilibration met a zero row                  */
+#define MHM_CELL_ZERO_COLUMN 7     /* equilibration met a zero column               */
+
+/* Global solve status (mhm_skeleton_solve `info` array, entry 0). */
+#define MHM_SOLVE_OK 0
+#define MHM_SOLVE_NOT_CONVERGED 1
+#define MHM_SOLVE_BREAKDOWN 2      /* non-positive curvature in projected CG        */
+#define MHM_SOLVE_BARRIER_TIMEOUT 3 /* a grid barrier exceeded its spin limit        */
+#define MHM_SOLVE_NONFINITE 4
+
+/* Arithmetic of the local factorisations. */
+#define MHM_PRECISION_FP64 0   /* factor + sweeps in binary64                    */
+#define MHM_PRECISION_MIXED 1  /* factor + sweeps in binary32, FP64 refinement   */
+
+/* ------------------------------------------------------------------------ */
+/* Cartesian Q1 macrocells: assembly + constrained condensation + Schur block */
+/* ------------------------------------------------------------------------ */
+typedef struct mhm_q1_problem {
+    int32_t macro_nx, macro_ny;   /* macro grid; cell = iy * macro_nx + ix       */
+    int32_t rx, ry;               /* fine subdivisions per macrocell              */
+    double hx, hy;                /* fine cell widths                             */
+    double x0, y0;                /* lower-left corner of the domain              */
+    int32_t tf_h, tf_v;           /* trace DOFs on horizontal / vertical faces    */
+    /* coupling_table[kind][orient][k][j]: kind 0 = horizontal side (rx+1 nodes),
+     * kind 1 = vertical side (ry+1 nodes); orient 0 = face parameter increases
+     * with the coordinate, 1 = decreases; k = node along the side in increasing
+     * coordinate order; j < tf (kind).  Physical face length is included, the
+     * cell's orientation sign is not.  Shape [2][2][kmax][jmax],
+     * kmax = max(rx,ry)+1, jmax = max(tf_h,tf_v).                              */
+    const double* coupling_table;
+    const int8_t* side_sign;      /* (cells, 4): +-1, sides bottom,right,top,left */
+    const int8_t* side_orient;    /* (cells, 4): 0/1 as in coupling_table          */
+    int32_t kappa_mode;           /* 0 constant, 1 isotropic per fine cell,
+                                     2 (kxx,kxy,kyy) per fine cell                */
+    const double* kappa;          /* global fine grid, [gx][gy][comp] (x-major)    */
+    double kappa_const[3];        /* kxx, kxy, kyy for kappa_mode 0                */
+    int32_t source_mode;          /* 0 constant, 1 per fine cell,
+                                     2 per Gauss point of the fine cell            */
+    const double* source;         /* [gx][gy] or [gx][gy][q] (q = qy*order + qx)   */
+    double source_const;
+    int32_t quad_order;           /* Gauss points per axis for source_mode 2      */
+} mhm_q1_problem;
+
+/* Width of the per-cell right-hand side block: 1 source + trace + 1 retained. */
+int32_t mhm_q1_rhs_width(const mhm_q1_problem* p /* host */);
+
+/* Shared-memory bytes one cell needs (0 if the size is unsupported). */
+int64_t mhm_q1_condense_smem_bytes(const mhm_q1_problem* p /* host */, int32_t precision);
+
+/*
+ * Assemble, constrain, factor and solve every macrocell, then form its oriented
+ * Schur block and reduced load.
+ *   solution (cells, w, n+1): augmented responses, column-major per cell:
+ *            column 0 = R f, columns 1..t = R B, column w-1 = R (A 1)
+ *            (row n = constraint multiplier).
+ *   blocks   (cells, t+1, t+1), loads (cells, t+1): local_global_contribution.
+ *   corrected (cells): 1 when the assembled A 1 is not exactly zero.
+ *   cell_status (cells): MHM_CELL_*; cell_iters (cells): refinement sweeps.
+ * tol is the per-column relative residual of the augmented system
+ * (||b - K x||_2 <= tol ||b||_2); max_refine bounds the correction sweeps.
+ */
+int mhm_q1_condense(const mhm_q1_problem* p /* host */, int32_t precision, int32_t max_refine,
+                    double tol, double* solution, double* blocks, double* loads,
+                    uint8_t* corrected, int32_t* cell_status, int32_t* cell_iters, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Ordered skeleton reduction                                                 */
+/* ------------------------------------------------------------------------ */
+/*
+ * vals[s] = sum_{e in slot_ptr[s]..slot_ptr[s+1]} blocks_flat[contrib[e]] in
+ * ascending cell order (precomputed by the host from the DOF maps); likewise
+ * rhs[g] = sum loads_flat[load_contrib[.]] - boundary[g] (g < trace_size) and
+ * load_scale[g] = sum |loads| + |boundary[g]|.  Deterministic, no atomics.
+ */
+int mhm_skeleton_scatter(int64_t nnz, const int64_t* slot_ptr, const int64_t* contrib,
+                         const double* blocks, double* vals, int64_t size, int64_t trace_size,
+                         const int64_t* load_ptr, const int64_t* load_contrib, const double* loads,
+                         const double* boundary, double* rhs, double* load_scale, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Global skeleton solve: projected PCG with an outer FP64 defect correction  */
+/* ------------------------------------------------------------------------ */
+typedef struct mhm_skeleton_system {
+    int64_t size;                 /* N = trace_size + cells                        */
+    int64_t trace_size;           /* T                                             */
+    const int64_t* indptr;        /* CSR of the full matrix K (N+1)                */
+    const int32_t* indices;       /* column indices, sorted per row                */
+    const double* values;
+    const int64_t* trace_end;     /* (T): first CSR slot of row r with col >= T    */
+    int32_t faces;                /* number of skeleton faces                      */
+    int32_t face_size;            /* DOFs per face (uniform skeleton)              */
+    int32_t cells;
+    int32_t cell_width;           /* t: trace DOFs per cell                        */
+    const int64_t* cell_dofs;     /* (cells, t)                                    */
+    const double* cell_g0;        /* (cells, t): geometric constraint column        */
+    const int32_t* dof_cells;     /* (T, 2): cells sharing the DOF (-1 = none)      */
+    const int32_t* dof_slot;      /* (T, 2): position of the DOF in each cell      */
+    int32_t nx, ny;               /* macro grid of the coarse Poisson operator     */
+    const double* qx;             /* (nx, nx) orthonormal sine transform           */
+    const double* qy;             /* (ny, ny)                                      */
+    const double* coarse_eig;     /* (ny, nx) eigenvalues of G0^T G0               */
+} mhm_skeleton_system;
+
+int64_t mhm_skeleton_workspace_bytes(const mhm_skeleton_system* s /* host */, int32_t grid);
+
+/*
+ * Solve K x = rhs.  x (N) is output.  info (device int32[4]): status, total
+ * inner iterations, outer corrections, barrier error flag.  stats (device
+ * double[4]): final relative residual ||rhs - K x|| / ||rhs||, the physical
+ * certificate ||K x - rhs|| / max(||rhs||, ||load_scale||, || |K||x| ||),
+ * first inner relative residual, unused.  grid = number of persistent CTAs
+ * (0 = one per SM); workspace sized by mhm_skeleton_workspace_bytes.
+ */
+int mhm_skeleton_solve(const mhm_skeleton_system* s /* host */, const double* rhs,
+                       const double* load_scale, double* x, double rtol, double inner_rtol,
+                       int32_t max_inner, int32_t max_outer, int32_t grid, void* workspace,
+                       int64_t workspace_bytes, int32_t* info, double* stats, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Reconstruction u_K = R f - (R B) lambda_K + E c_K and flux -K grad u       */
+/* ------------------------------------------------------------------------ */
+int mhm_q1_reconstruct(const mhm_q1_problem* p /* host */, const double* solution,
+                       const int64_t* cell_dofs, int64_t trace_size, const double* x,
+                       double* fields, double* flux, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Batched dense equilibrated LU (BatchedFactorization contract)              */
+/* ------------------------------------------------------------------------ */
+/*
+ * factors (count, n, n) receives the row/column-equilibrated LU of matrices
+ * (count, n, n), row-major; pivots (count, n); row_scale/col_scale (count, n)
+ * hold 1/max; status (count) receives MHM_CELL_*.
+ */
+int mhm_batched_factor(int64_t count, int32_t n, const double* matrices, double* factors,
+                       int32_t* pivots, double* row_scale, double* col_scale, int32_t* status,
+                       void* stream);
+
+/*
+ * Solve matrices @ x = rhs for rhs (count, n, nrhs) row-major using the factors,
+ * with up to max_refine FP64 residual corrections; each column must satisfy
+ * ||A x - b|| <= max(atol, rtol ||b||) with the reference's max-scaling, else
+ * status = MHM_CELL_RESIDUAL.  x (count, n, nrhs); work (count, n, nrhs).
+ */
+int mhm_batched_solve(int64_t count, int32_t n, int32_t nrhs, const double* matrices,
+                      const double* factors, const int32_t* pivots, const double* row_scale,
+                      const double* col_scale, const double* rhs, double* x, double* work,
+                      double rtol, double atol, int32_t max_refine, int32_t* status,
+                      void* stream);
+
+/* Library version string (host). */
+const char* mhm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MHM_B200_H */

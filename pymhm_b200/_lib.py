@@ -1,0 +1,134 @@
+"""ctypes binding of ``libmhm_b200.so`` (the C ABI declared in ``include/mhm_b200.h``).
+
+The shared library is the only compute path: there is no CPU fallback.  If
+it is missing or no CUDA device is visible, ``lib()`` raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+LIBRARY = Path(__file__).resolve().parent / "libmhm_b200.so"
+
+MHM_OK, MHM_ERR_ARGUMENT, MHM_ERR_LAUNCH, MHM_ERR_UNSUPPORTED = 0, 1, 2, 3
+CELL_OK, CELL_KERNEL, CELL_SINGULAR_PIVOT, CELL_RANK_DEFICIENT = 0, 1, 2, 3
+CELL_RESIDUAL, CELL_NONFINITE, CELL_ZERO_ROW, CELL_ZERO_COLUMN = 4, 5, 6, 7
+SOLVE_OK, SOLVE_NOT_CONVERGED, SOLVE_BREAKDOWN, SOLVE_BARRIER_TIMEOUT, SOLVE_NONFINITE = 0, 1, 2, 3, 4
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+
+CALL_ERRORS = {
+    MHM_ERR_ARGUMENT: "invalid arguments",
+    MHM_ERR_LAUNCH: "CUDA launch failed",
+    MHM_ERR_UNSUPPORTED: "problem size is outside the supported on-chip layout",
+}
+
+# Per-cell status -> the reference's error wording (linalg/linear.py, execution/cuda.py,
+# core/contracts.py) so callers can match the same messages.
+CELL_MESSAGES = {
+    CELL_KERNEL: "declared kernel is not a left and right nullspace",
+    CELL_SINGULAR_PIVOT: "batched LU failed: a local matrix has a singular pivot",
+    CELL_RANK_DEFICIENT: "batched local matrix is numerically rank deficient",
+    CELL_RESIDUAL: "batched residual criterion failed",
+    CELL_NONFINITE: "batched solver returned nonfinite coefficients",
+    CELL_ZERO_ROW: "batched matrix contains a zero row",
+    CELL_ZERO_COLUMN: "batched matrix contains a zero column",
+}
+
+SOLVE_MESSAGES = {
+    SOLVE_NOT_CONVERGED: "skeleton CG failed to converge",
+    SOLVE_BREAKDOWN: "skeleton CG breakdown: non-positive curvature",
+    SOLVE_BARRIER_TIMEOUT: "skeleton CG grid barrier timed out",
+    SOLVE_NONFINITE: "skeleton CG produced nonfinite values",
+}
+
+
+class Q1Problem(C.Structure):
+    _fields_ = [
+        ("macro_nx", C.c_int32), ("macro_ny", C.c_int32), ("rx", C.c_int32), ("ry", C.c_int32),
+        ("hx", C.c_double), ("hy", C.c_double), ("x0", C.c_double), ("y0", C.c_double),
+        ("tf_h", C.c_int32), ("tf_v", C.c_int32),
+        ("coupling_table", C.c_void_p), ("side_sign", C.c_void_p), ("side_orient", C.c_void_p),
+        ("kappa_mode", C.c_int32), ("kappa", C.c_void_p), ("kappa_const", C.c_double * 3),
+        ("source_mode", C.c_int32), ("source", C.c_void_p), ("source_const", C.c_double),
+        ("quad_order", C.c_int32),
+    ]
+
+
+class SkeletonSystem(C.Structure):
+    _fields_ = [
+        ("size", C.c_int64), ("trace_size", C.c_int64),
+        ("indptr", C.c_void_p), ("indices", C.c_void_p), ("values", C.c_void_p),
+        ("trace_end", C.c_void_p),
+        ("faces", C.c_int32), ("face_size", C.c_int32), ("cells", C.c_int32), ("cell_width", C.c_int32),
+        ("cell_dofs", C.c_void_p), ("cell_g0", C.c_void_p), ("dof_cells", C.c_void_p),
+        ("dof_slot", C.c_void_p), ("nx", C.c_int32), ("ny", C.c_int32),
+        ("qx", C.c_void_p), ("qy", C.c_void_p), ("coarse_eig", C.c_void_p),
+    ]
+
+
+P = C.c_void_p
+_SIGNATURES = {
+    "mhm_q1_rhs_width": (C.c_int32, [C.POINTER(Q1Problem)]),
+    "mhm_q1_condense_smem_bytes": (C.c_int64, [C.POINTER(Q1Problem), C.c_int32]),
+    "mhm_q1_condense": (C.c_int, [C.POINTER(Q1Problem), C.c_int32, C.c_int32, C.c_double, P, P, P, P, P, P, P]),
+    "mhm_skeleton_scatter": (C.c_int, [C.c_int64, P, P, P, P, C.c_int64, C.c_int64, P, P, P, P, P, P, P]),
+    "mhm_skeleton_workspace_bytes": (C.c_int64, [C.POINTER(SkeletonSystem), C.c_int32]),
+    "mhm_skeleton_solve": (C.c_int, [C.POINTER(SkeletonSystem), P, P, P, C.c_double, C.c_double, C.c_int32,
+                                     C.c_int32, C.c_int32, P, C.c_int64, P, P, P]),
+    "mhm_q1_reconstruct": (C.c_int, [C.POINTER(Q1Problem), P, P, C.c_int64, P, P, P, P]),
+    "mhm_batched_factor": (C.c_int, [C.c_int64, C.c_int32, P, P, P, P, P, P, P]),
+    "mhm_batched_solve": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, P, P, P, P, P, P, P, C.c_double,
+                                    C.c_double, C.c_int32, P, P]),
+    "mhm_version": (C.c_char_p, []),
+}
+
+_LOCK = threading.Lock()
+_LIB: C.CDLL | None = None
+
+
+def load() -> C.CDLL:
+    """Load the library and bind every declared symbol (no GPU needed)."""
+    global _LIB
+    with _LOCK:
+        if _LIB is None:
+            if not LIBRARY.exists():
+                raise RuntimeError(f"{LIBRARY.name} is not built; run `python -m pymhm_b200.build`")
+            lib = C.CDLL(str(LIBRARY))
+            for name, (res, args) in _SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _LIB = lib
+    return _LIB
+
+
+def lib() -> C.CDLL:
+    """The library, after checking that a CUDA device is usable."""
+    import torch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("pymhm_b200 requires a CUDA device (no CPU fallback)")
+    return load()
+
+
+def check(rc: int, what: str) -> None:
+    if rc != MHM_OK:
+        raise RuntimeError(f"{what}: {CALL_ERRORS.get(rc, rc)}")
+
+
+def ptr(t) -> int:
+    """Device pointer of a torch tensor (None -> NULL)."""
+    return 0 if t is None else int(t.data_ptr())
+
+
+def stream_handle(stream) -> int:
+    import torch
+
+    s = torch.cuda.current_stream() if stream is None else stream
+    return int(s.cuda_stream)
+
+
+def declared_symbols() -> list[str]:
+    return list(_SIGNATURES)

@@ -1,0 +1,436 @@
+"""Cartesian Q1 Primal-MHM Darcy solve on one B200: the host side of the hot path.
+
+``solve_darcy_quadrilateral`` mirrors PyMHM's driver of the same name
+(``src/pymhm/_legacy/models/darcy/cartesian.py:86-168``) for degree-one local
+spaces and weak Dirichlet data; ``CartesianQ1Plan`` is the reusable,
+device-resident form used for repeated solves and serving.
+
+Per solve, four kernels run back to back on one stream:
+
+1. ``mhm_q1_condense``   one CTA per macrocell: Q1 assembly from the fine-cell
+   coefficients, pinned band LDL^T of the Neumann operator, FP64-refined
+   augmented responses ``[R f | R B | R A1]``, Schur block and reduced load;
+2. ``mhm_skeleton_scatter``  deterministic ordered reduction into the
+   precomputed skeleton CSR (no atomics);
+3. ``mhm_skeleton_solve``  persistent projected PCG with an outer FP64
+   defect correction on the assembled skeleton matrix;
+4. ``mhm_q1_reconstruct``  fields ``u_K = R f - (R B) lambda_K + E c_K`` and
+   fine-cell-centre fluxes ``-K grad u``.
+"""
+
+from __future__ import annotations
+
+import numbers
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+from numpy.polynomial.legendre import leggauss
+
+from . import _lib
+from .errors import LinearSolveError
+from .topology import (
+    CartesianMacroMesh,
+    FaceSpace,
+    SkeletonSpace,
+    boundary_data,
+    coarse_eigenvalues,
+    coupling_tables,
+    dof_cell_maps,
+    geometric_constraint,
+    mesh_arrays,
+    side_orientation,
+    sine_transform,
+    skeleton_pattern,
+)
+
+PRECISIONS = {"fp64": _lib.PRECISION_FP64, "mixed": _lib.PRECISION_MIXED}
+
+
+def _refinement(value) -> tuple[int, int]:
+    if isinstance(value, tuple):
+        if len(value) != 2:
+            raise ValueError("local_refinement requires two integers")
+        rx, ry = (int(v) for v in value)
+    else:
+        rx = ry = int(value)
+    if rx < 1 or ry < 1:
+        raise ValueError("local_refinement must be positive")
+    return rx, ry
+
+
+def _is_number(value) -> bool:
+    if isinstance(value, (bool, np.bool_)):
+        return False
+    if isinstance(value, numbers.Real):
+        return True
+    return isinstance(value, np.ndarray) and value.ndim == 0 and value.dtype.kind in "iuf"
+
+
+def fine_grid(mesh: CartesianMacroMesh, rx: int, ry: int):
+    """Fine spacing, counts and the lower-left corner of the global fine grid."""
+    hx, hy = mesh.spacing
+    return hx / rx, hy / ry, mesh.nx * rx, mesh.ny * ry, mesh.bounds[0], mesh.bounds[2]
+
+
+def _quad_points(mesh, rx, ry, order):
+    fhx, fhy, nxf, nyf, x0, y0 = fine_grid(mesh, rx, ry)
+    g, _ = leggauss(order)
+    g = (g + 1) / 2
+    gx = x0 + (np.arange(nxf)[:, None] + g[None, :]) * fhx  # (nxf, q)
+    gy = y0 + (np.arange(nyf)[:, None] + g[None, :]) * fhy
+    # [gx][gy][qy][qx]
+    px = np.broadcast_to(gx[:, None, None, :], (nxf, nyf, order, order))
+    py = np.broadcast_to(gy[None, :, :, None], (nxf, nyf, order, order))
+    return np.stack((px, py), axis=-1).reshape(-1, 2)
+
+
+def _fine_centres(mesh, rx, ry):
+    fhx, fhy, nxf, nyf, x0, y0 = fine_grid(mesh, rx, ry)
+    cx = x0 + (np.arange(nxf) + 0.5) * fhx
+    cy = y0 + (np.arange(nyf) + 0.5) * fhy
+    return np.stack(np.meshgrid(cx, cy, indexing="ij"), axis=-1).reshape(-1, 2)
+
+
+def _tensor_components(values: np.ndarray) -> tuple[int, np.ndarray]:
+    """(mode, array) for scalar (mode 1) or 2x2 SPD tensor (mode 2) fine-cell values."""
+    values = np.asarray(values, dtype=float)
+    if values.ndim == 2:
+        if not np.all(np.isfinite(values)) or np.any(values <= 0):
+            raise ValueError("diffusion tensor must be finite, symmetric and positive definite")
+        return 1, np.ascontiguousarray(values)
+    if values.ndim == 4 and values.shape[2:] == (2, 2):
+        if not np.allclose(values, values.swapaxes(2, 3), rtol=1e-12, atol=1e-14):
+            raise ValueError("diffusion tensor must be finite, symmetric and positive definite")
+        comp = np.stack((values[..., 0, 0], values[..., 0, 1], values[..., 1, 1]), axis=-1)
+        det = comp[..., 0] * comp[..., 2] - comp[..., 1] ** 2
+        if not np.all(np.isfinite(comp)) or np.any(comp[..., 0] <= 0) or np.any(det <= 0):
+            raise ValueError("diffusion tensor must be finite, symmetric and positive definite")
+        return 2, np.ascontiguousarray(comp)
+    raise ValueError("fine-cell permeability must have shape (nx, ny) or (nx, ny, 2, 2)")
+
+
+def permeability_input(permeability, mesh: CartesianMacroMesh, rx: int, ry: int, order: int):
+    """Map a permeability description to (mode, fine-grid array | None, constant triple).
+
+    Accepted: a positive scalar or constant 2x2 tensor; a grid-aligned pixel field
+    with ``values``, ``spacing`` and ``origin`` (``materials/cartesian.py``), whose
+    lines coincide with fine-grid lines; an array of fine-cell values; or a
+    callable that is constant on every fine cell at the Gauss points.  Material
+    lines crossing fine cells need the reference's cut quadrature
+    (``quadrilateral.py:136-188``), which this path does not implement.
+    """
+    _, _, nxf, nyf, _, _ = fine_grid(mesh, rx, ry)
+    if _is_number(permeability):
+        k = float(permeability)
+        if not (np.isfinite(k) and k > 0):
+            raise ValueError("diffusion tensor must be finite, symmetric and positive definite")
+        return 0, None, (k, 0.0, k)
+    arr = None if callable(permeability) or hasattr(permeability, "spacing") else np.asarray(permeability)
+    if arr is not None and arr.shape == (2, 2):
+        mode, comp = _tensor_components(arr.reshape(1, 1, 2, 2))
+        return 0, None, tuple(float(v) for v in comp.reshape(3))
+    if arr is not None:
+        if arr.shape[:2] != (nxf, nyf):
+            raise ValueError(f"fine-cell permeability must have leading shape ({nxf}, {nyf})")
+        mode, comp = _tensor_components(arr)
+        return mode, comp, (0.0, 0.0, 0.0)
+    if hasattr(permeability, "spacing") and hasattr(permeability, "values"):
+        fhx, fhy, _, _, x0, y0 = fine_grid(mesh, rx, ry)
+        spacing = np.asarray(permeability.spacing, dtype=float)
+        origin = np.zeros(2) if getattr(permeability, "origin", None) is None else np.asarray(permeability.origin, float)
+        ratio = spacing / np.array([fhx, fhy])
+        offset = (np.array([x0, y0]) - origin) / np.array([fhx, fhy])
+        if (spacing.shape != (2,) or np.any(np.abs(ratio - np.rint(ratio)) > 1e-9 * np.maximum(1, ratio))
+                or np.any(np.abs(offset - np.rint(offset)) > 1e-9 * np.maximum(1, np.abs(offset)))
+                or np.any(np.rint(ratio) < 1)):
+            raise NotImplementedError(
+                "material lines must coincide with fine-grid lines (cut-cell quadrature is not on this path)")
+        centres = _fine_centres(mesh, rx, ry)
+        idx = np.floor((centres - origin) / spacing).astype(np.int64)
+        vals = np.asarray(permeability.values, dtype=float)
+        shape = np.array(vals.shape[:2])
+        if np.any(idx < 0) or np.any(idx >= shape):
+            raise ValueError("a fine rectangle lies outside the Cartesian material field")
+        sampled = vals[idx[:, 0], idx[:, 1]]
+        sampled = sampled.reshape(nxf, nyf, *vals.shape[2:])
+        mode, comp = _tensor_components(sampled)
+        return mode, comp, (0.0, 0.0, 0.0)
+    if callable(permeability):
+        pts = _quad_points(mesh, rx, ry, order)
+        raw = np.asarray(permeability(pts), dtype=float)
+        q = order * order
+        if raw.shape == (len(pts),):
+            per = raw.reshape(nxf, nyf, q)
+            if np.any(per != per[..., :1]):
+                raise NotImplementedError("permeability must be constant on each fine cell")
+            mode, comp = _tensor_components(per[..., 0])
+            return mode, comp, (0.0, 0.0, 0.0)
+        if raw.shape == (len(pts), 2, 2):
+            per = raw.reshape(nxf, nyf, q, 2, 2)
+            if np.any(per != per[:, :, :1]):
+                raise NotImplementedError("permeability must be constant on each fine cell")
+            mode, comp = _tensor_components(per[:, :, 0])
+            return mode, comp, (0.0, 0.0, 0.0)
+        raise ValueError("permeability callable must return scalars or 2x2 tensors per point")
+    raise TypeError("unsupported permeability description")
+
+
+def source_input(source, mesh: CartesianMacroMesh, rx: int, ry: int, order: int):
+    """(mode, array | None, constant) for a scalar, fine-cell array or pointwise callable."""
+    _, _, nxf, nyf, _, _ = fine_grid(mesh, rx, ry)
+    if _is_number(source):
+        return 0, None, float(source)
+    if callable(source):
+        pts = _quad_points(mesh, rx, ry, order)
+        vals = np.broadcast_to(np.asarray(source(pts), dtype=float), (len(pts),))
+        if not np.all(np.isfinite(vals)):
+            raise ValueError("scalar coefficient must be finite")
+        return 2, np.ascontiguousarray(vals.reshape(nxf, nyf, order * order)), 0.0
+    arr = np.asarray(source, dtype=float)
+    if arr.shape != (nxf, nyf):
+        raise ValueError(f"fine-cell source must have shape ({nxf}, {nyf})")
+    return 1, np.ascontiguousarray(arr), 0.0
+
+
+@dataclass
+class Q1Solution:
+    """Host copy of one solve (``HybridSolution`` + ``QuadrilateralDarcySolution`` fields)."""
+
+    trace: np.ndarray
+    coarse: np.ndarray
+    fields: np.ndarray
+    flux: np.ndarray
+    residual: float
+    raw_residual: float
+    corrected: np.ndarray
+    local_iterations: np.ndarray
+    global_iterations: int
+    outer_corrections: int
+    seconds: float = 0.0
+    extra: dict = field(default_factory=dict)
+
+
+class CartesianQ1Plan:
+    """Device-resident plan: topology, tables, pattern and buffers for one problem shape.
+
+    The plan owns every device buffer the four kernels use, so repeated solves
+    (new coefficients or sources on the same mesh) allocate nothing.
+    """
+
+    def __init__(self, mesh, skeleton=None, local_refinement=4, *, dirichlet=0.0, quadrature_order=4,
+                 degree=1, precision="fp64", device=None, max_refine=None, local_tol=1e-12,
+                 global_rtol=1e-13, inner_rtol=1e-12, max_inner=5000, max_outer=6, grid=0):
+        import torch
+
+        if int(degree) != 1:
+            raise NotImplementedError("the GPU path implements degree-one (Q1) local spaces")
+        if precision not in PRECISIONS:
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.torch = torch
+        self.mesh = mesh_arrays(mesh)
+        self.skeleton = SkeletonSpace(self.mesh) if skeleton is None else SkeletonSpace.of(skeleton, self.mesh)
+        self.rx, self.ry = _refinement(local_refinement)
+        self.order = max(int(quadrature_order), 2)
+        self.precision = precision
+        self.device = torch.device("cuda" if device is None else device)
+        self.max_refine = int(max_refine or (10 if precision == "fp64" else 30))
+        self.local_tol = float(local_tol)
+        self.global_rtol, self.inner_rtol = float(global_rtol), float(inner_rtol)
+        self.max_inner, self.max_outer, self.grid = int(max_inner), int(max_outer), int(grid)
+        self.lib = _lib.lib()
+        m, sk = self.mesh, self.skeleton
+        space_h, space_v = sk.uniform_by_orientation()
+        fs = space_h.size
+        if space_v.size != fs:
+            raise NotImplementedError("the GPU skeleton solver requires equal face sizes")
+        self.cells = len(m.cells)
+        self.n = (self.rx + 1) * (self.ry + 1)
+        self.t = 2 * (space_h.size + space_v.size)
+        self.w = self.t + 2
+        self.T = sk.size
+        self.N = self.T + self.cells
+        self.nfine = self.rx * self.ry
+        # ---- host tables --------------------------------------------------------------
+        hx, hy = m.spacing
+        self.table_h = coupling_tables(space_h, space_v, self.rx, self.ry, hx, hy)
+        self.cell_dofs_h = sk.cell_dof_array
+        self.pattern = skeleton_pattern(self.cell_dofs_h, self.T)
+        dof_cells, dof_slot = dof_cell_maps(self.cell_dofs_h, self.T)
+        g0 = geometric_constraint(m, space_h, space_v)
+        self.boundary_h = boundary_data(sk, dirichlet, self.order)
+        # ---- device constants ---------------------------------------------------------
+        dev = self.device
+        f64 = dict(dtype=torch.float64, device=dev)
+
+        def up(a, dtype):
+            return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype).to(dev)
+
+        self.d_table = up(self.table_h, torch.float64)
+        self.d_sign = up(m.signs.astype(np.int8), torch.int8)
+        self.d_orient = up(side_orientation(m), torch.int8)
+        self.d_cell_dofs = up(self.cell_dofs_h, torch.int64)
+        p = self.pattern
+        self.d_indptr = up(p.indptr, torch.int64)
+        self.d_indices = up(p.indices, torch.int32)
+        self.d_slot_ptr = up(p.slot_ptr, torch.int64)
+        self.d_contrib = up(p.contrib, torch.int64)
+        self.d_load_ptr = up(p.load_ptr, torch.int64)
+        self.d_load_contrib = up(p.load_contrib, torch.int64)
+        self.d_trace_end = up(p.trace_end, torch.int64)
+        self.d_boundary = up(self.boundary_h, torch.float64)
+        self.d_g0 = up(g0, torch.float64)
+        self.d_dof_cells = up(dof_cells, torch.int32)
+        self.d_dof_slot = up(dof_slot, torch.int32)
+        self.d_qx = up(sine_transform(m.nx), torch.float64)
+        self.d_qy = up(sine_transform(m.ny), torch.float64)
+        self.d_eig = up(coarse_eigenvalues(m, space_h, space_v), torch.float64)
+        # ---- device buffers -----------------------------------------------------------
+        M, n, w, t1 = self.cells, self.n, self.w, self.t + 1
+        self.solution = torch.empty((M, w, n + 1), **f64)
+        self.blocks = torch.empty((M, t1, t1), **f64)
+        self.loads = torch.empty((M, t1), **f64)
+        self.corrected = torch.empty(M, dtype=torch.uint8, device=dev)
+        self.cell_status = torch.empty(M, dtype=torch.int32, device=dev)
+        self.cell_iters = torch.empty(M, dtype=torch.int32, device=dev)
+        self.values = torch.empty(len(p.indices), **f64)
+        self.rhs = torch.empty(self.N, **f64)
+        self.load_scale = torch.empty(self.N, **f64)
+        self.x = torch.empty(self.N, **f64)
+        self.info = torch.zeros(4, dtype=torch.int32, device=dev)
+        self.stats = torch.zeros(4, **f64)
+        self.fields = torch.empty((M, n), **f64)
+        self.flux = torch.empty((M, self.nfine, 2), **f64)
+        self.kappa = None
+        self.source = None
+        # structures
+        fhx, fhy, self.nxf, self.nyf, x0, y0 = fine_grid(m, self.rx, self.ry)
+        self.q1 = _lib.Q1Problem()
+        q = self.q1
+        q.macro_nx, q.macro_ny, q.rx, q.ry = m.nx, m.ny, self.rx, self.ry
+        q.hx, q.hy, q.x0, q.y0 = fhx, fhy, x0, y0
+        q.tf_h, q.tf_v = space_h.size, space_v.size
+        q.coupling_table = _lib.ptr(self.d_table)
+        q.side_sign = _lib.ptr(self.d_sign)
+        q.side_orient = _lib.ptr(self.d_orient)
+        q.quad_order = self.order
+        if self.lib.mhm_q1_condense_smem_bytes(q, PRECISIONS[precision]) <= 0:
+            raise NotImplementedError("local refinement too large for the on-chip factor layout")
+        self.sys = _lib.SkeletonSystem()
+        s = self.sys
+        s.size, s.trace_size = self.N, self.T
+        s.indptr, s.indices, s.values = _lib.ptr(self.d_indptr), _lib.ptr(self.d_indices), _lib.ptr(self.values)
+        s.trace_end = _lib.ptr(self.d_trace_end)
+        s.faces, s.face_size, s.cells, s.cell_width = len(m.faces), fs, M, self.t
+        s.cell_dofs, s.cell_g0 = _lib.ptr(self.d_cell_dofs), _lib.ptr(self.d_g0)
+        s.dof_cells, s.dof_slot = _lib.ptr(self.d_dof_cells), _lib.ptr(self.d_dof_slot)
+        s.nx, s.ny = m.nx, m.ny
+        s.qx, s.qy, s.coarse_eig = _lib.ptr(self.d_qx), _lib.ptr(self.d_qy), _lib.ptr(self.d_eig)
+        nbytes = self.lib.mhm_skeleton_workspace_bytes(s, self.grid)
+        if nbytes <= 0:
+            raise RuntimeError("could not size the skeleton solver workspace")
+        self.workspace = torch.empty(int(nbytes), dtype=torch.uint8, device=dev)
+
+    # ------------------------------------------------------------------------------------
+    def set_coefficients(self, permeability=1.0, source=0.0, *, non_blocking=False):
+        """Upload (or keep constant) coefficient data for the next ``launch``."""
+        torch = self.torch
+        kmode, karr, kconst = permeability_input(permeability, self.mesh, self.rx, self.ry, self.order)
+        smode, sarr, sconst = source_input(source, self.mesh, self.rx, self.ry, self.order)
+        self.kappa = None if karr is None else torch.as_tensor(karr).to(self.device, non_blocking=non_blocking)
+        self.source = None if sarr is None else torch.as_tensor(sarr).to(self.device, non_blocking=non_blocking)
+        self.set_device_coefficients(kmode, self.kappa, kconst, smode, self.source, sconst)
+
+    def set_device_coefficients(self, kmode, kappa, kconst, smode, source, sconst):
+        """Point the plan at device-resident coefficient tensors (no copies)."""
+        q = self.q1
+        q.kappa_mode, q.kappa = kmode, _lib.ptr(kappa)
+        q.kappa_const[0], q.kappa_const[1], q.kappa_const[2] = kconst
+        q.source_mode, q.source, q.source_const = smode, _lib.ptr(source), float(sconst)
+        self._keep = (kappa, source)
+
+    def launch(self, stream=None, *, reconstruct=True):
+        """Enqueue the four kernels on ``stream`` (no host synchronisation)."""
+        L, s = self.lib, _lib.stream_handle(stream)
+        P = _lib.ptr
+        _lib.check(L.mhm_q1_condense(self.q1, PRECISIONS[self.precision], self.max_refine, self.local_tol,
+                                     P(self.solution), P(self.blocks), P(self.loads), P(self.corrected),
+                                     P(self.cell_status), P(self.cell_iters), s), "mhm_q1_condense")
+        pat = self.pattern
+        _lib.check(L.mhm_skeleton_scatter(len(pat.indices), P(self.d_slot_ptr), P(self.d_contrib),
+                                          P(self.blocks), P(self.values), self.N, self.T,
+                                          P(self.d_load_ptr), P(self.d_load_contrib), P(self.loads),
+                                          P(self.d_boundary), P(self.rhs), P(self.load_scale), s),
+                   "mhm_skeleton_scatter")
+        _lib.check(L.mhm_skeleton_solve(self.sys, P(self.rhs), P(self.load_scale), P(self.x), self.global_rtol,
+                                        self.inner_rtol, self.max_inner, self.max_outer, self.grid,
+                                        P(self.workspace), self.workspace.numel(), P(self.info), P(self.stats), s),
+                   "mhm_skeleton_solve")
+        if reconstruct:
+            _lib.check(L.mhm_q1_reconstruct(self.q1, P(self.solution), P(self.d_cell_dofs), self.T, P(self.x),
+                                            P(self.fields), P(self.flux), s), "mhm_q1_reconstruct")
+
+    def check(self):
+        """Synchronise and raise the reference's error for any failed cell or solve."""
+        torch = self.torch
+        status = self.cell_status.cpu().numpy()
+        bad = np.flatnonzero(status)
+        if len(bad):
+            code = int(status[bad[0]])
+            msg = _lib.CELL_MESSAGES.get(code, f"status {code}")
+            if code == _lib.CELL_KERNEL:
+                raise ValueError(msg)
+            raise LinearSolveError(f"{msg} (macrocell {int(bad[0])}, {len(bad)} cells)")
+        info = self.info.cpu().numpy()
+        if info[0] != _lib.SOLVE_OK:
+            raise LinearSolveError(_lib.SOLVE_MESSAGES.get(int(info[0]), f"status {info[0]}"))
+        stats = self.stats.cpu().numpy()
+        if not stats[1] <= 1e-8:
+            raise ValueError("incompatible data: gauge changed physical equations")
+        del torch
+        return info, stats
+
+    def result(self, seconds=0.0) -> Q1Solution:
+        info, stats = self.check()
+        x = self.x.cpu().numpy()
+        return Q1Solution(
+            trace=x[: self.T].copy(), coarse=x[self.T:].copy(), fields=self.fields.cpu().numpy(),
+            flux=self.flux.cpu().numpy(), residual=float(stats[1]), raw_residual=float(stats[0]),
+            corrected=self.corrected.cpu().numpy().astype(bool), local_iterations=self.cell_iters.cpu().numpy(),
+            global_iterations=int(info[1]), outer_corrections=int(info[2]), seconds=seconds)
+
+    def solve(self, permeability=1.0, source=0.0, stream=None) -> Q1Solution:
+        t0 = time.perf_counter()
+        self.set_coefficients(permeability, source)
+        self.launch(stream)
+        sol = self.result()
+        sol.seconds = time.perf_counter() - t0
+        return sol
+
+    def matrix(self):
+        """Host CSR copy of the assembled skeleton matrix (structural pattern)."""
+        from scipy import sparse
+
+        p = self.pattern
+        return sparse.csr_matrix((self.values.cpu().numpy(), p.indices.astype(np.int64), p.indptr),
+                                 shape=(self.N, self.N))
+
+
+def solve_darcy_quadrilateral(mesh, *, permeability=1.0, source=0.0, dirichlet=0.0, neumann=None,
+                              skeleton=None, local_refinement=4, degree=1, quadrature_order=4,
+                              mean_pressure=0.0, solver="gpu", local_solver="gpu", backend="serial",
+                              workers=None, precision="fp64") -> Q1Solution:
+    """GPU counterpart of ``solve_darcy_quadrilateral`` (``cartesian.py:86-168``).
+
+    Weak Dirichlet data on every boundary face; pure-Neumann gauges and Neumann
+    faces are rejected with ``NotImplementedError`` (not on this path).  The
+    ``solver``, ``local_solver``, ``backend`` and ``workers`` arguments are
+    accepted for signature compatibility: the whole solve runs on the GPU.
+    """
+    if neumann:
+        raise NotImplementedError("Neumann faces are not on the GPU path")
+    del mean_pressure, solver, local_solver, backend, workers
+    order = max(int(quadrature_order), int(degree) + 1)
+    plan = CartesianQ1Plan(mesh, skeleton, local_refinement, dirichlet=dirichlet, quadrature_order=order,
+                           degree=degree, precision=precision)
+    return plan.solve(permeability, source)
