@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Primal-MHM solves/s on B200: one JSON line per run.
+
+Workload: 64x64 Cartesian macrocells x 16x16 local Q1 (289 local DOFs),
+discontinuous P2 traces per macro edge (12 trace + 1 source right-hand sides
+per cell), log-normal permeability (Gaussian log-field, exponential covariance,
+sigma = 2, correlation length 0.05, PCG64 seed 20261203) on the 1024x1024 fine
+cells, f = 1, homogeneous Dirichlet data.  Synthetic, seeded inputs.
+
+A step is one complete MHM solve: local assembly + condensation, ordered
+skeleton reduction, global skeleton solve, reconstruction of fields and
+fluxes.  ``value`` is solves/s with the permeability already resident in HBM
+(mixed precision: binary32 local factors + FP64 refinement; the FP64-factor
+path is reported beside it); ``e2e`` times the public API with the
+permeability copied from pinned host memory and fields, fluxes and skeleton
+unknowns copied back every step.  L2 is flushed (256 MiB write) between timed
+steps, outside the timed region.
+
+``--impl reference`` times the CPU restatement of the reference path (the
+oracle) on the host cores instead: each step runs the local stage on a
+bounded sample of macrocells in a spawn process pool and scales to the full
+4096-cell solve.
+
+Multi-GPU: replicas only (one independent solve per rank, no collective in
+the data path); torch.distributed is used for barriers and the max-over-ranks
+timing.
+"""
+
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MACRO, LOCAL, FACE_DEGREE = 64, 16, 2
+SIGMA, ELL, SEED = 2.0, 0.05, 20261203
+METRIC = "MHM solves/s (64x64 Q1 Darcy, lognormal kappa), mixed vs FP64 GPU"
+CPU_SAMPLE_CELLS = 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="small run for ncu (no baselines, no e2e)")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (median SM clock, throttle reasons)."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.seek(0)
+        rows = [r for r in csv.reader(io.StringIO(self.file.read())) if len(r) >= 9]
+        os.unlink(self.file.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def workload_kappa():
+    from pymhm_b200.workloads import lognormal_permeability
+
+    return lognormal_permeability(MACRO * LOCAL, MACRO * LOCAL, sigma=SIGMA, ell=ELL, seed=SEED)
+
+
+def cpu_rate(kappa, cells, workers):
+    from oracle.q1_mhm import local_stage_rate
+
+    rng = np.random.default_rng(0)
+    sample = np.sort(rng.choice(MACRO * MACRO, size=cells, replace=False))
+    rate, seconds = local_stage_rate(MACRO, LOCAL, FACE_DEGREE, kappa, 1.0, sample, workers)
+    return rate, seconds
+
+
+def cpu_baseline_entry(kappa, cells=CPU_SAMPLE_CELLS):
+    workers = os.cpu_count() or 1
+    rate, seconds = cpu_rate(kappa, cells, workers)
+    return {
+        "value": rate / (MACRO * MACRO), "unit": "solves/s", "cores": workers, "kind": "port",
+        "sample": (f"oracle local stage (Q1 assembly + equilibrated SuperLU condensation + Schur block) on "
+                   f"{cells} of {MACRO * MACRO} macrocells in {workers} spawn processes, {seconds:.1f} s wall; "
+                   f"scaled to 4096 cells; global SuperLU solve (about 1% of the reference's time at this size) "
+                   f"not included"),
+    }
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    kappa = workload_kappa()
+    workers = os.cpu_count() or 1
+    import multiprocessing as mp
+
+    from oracle.q1_mhm import _sample_cells, _sample_init
+
+    pool = mp.get_context("spawn").Pool(workers, initializer=_sample_init,
+                                        initargs=(MACRO, LOCAL, FACE_DEGREE, kappa, 1.0))
+    from oracle.q1_mhm import local_stage_rate
+
+    rng = np.random.default_rng(1)
+    cells_per_step = max(workers * 8, 64)
+    pool.map(_sample_cells, [[c] for c in range(workers)])
+    for _ in range(args.warmup):
+        local_stage_rate(MACRO, LOCAL, FACE_DEGREE, kappa, 1.0, rng.choice(MACRO * MACRO, cells_per_step, False),
+                         workers, pool)
+    times = []
+    for _ in range(args.steps):
+        rate, _ = local_stage_rate(MACRO, LOCAL, FACE_DEGREE, kappa, 1.0,
+                                   rng.choice(MACRO * MACRO, cells_per_step, False), workers, pool)
+        times.append(MACRO * MACRO / rate)
+    pool.close()
+    pool.join()
+    ms = 1000.0 * float(np.mean(times))
+    value = 1000.0 / ms
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lognormal kappa)",
+        "config": workload_config(args), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers, "kind": "port",
+                         "sample": f"oracle local stage on {cells_per_step} random macrocells per step, "
+                                   f"{workers} spawn processes, scaled to 4096 cells (global solve excluded)"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args):
+    return {"workload": f"darcy-q1-{MACRO}x{MACRO}-r{LOCAL}-p{FACE_DEGREE}-lognormal-s{SIGMA:g}-l{ELL:g}",
+            "macrocells": MACRO * MACRO, "local_dofs": (LOCAL + 1) ** 2, "rhs_per_cell": 4 * (FACE_DEGREE + 1) + 1,
+            "skeleton_unknowns": None, "fine_cells": (MACRO * LOCAL) ** 2, "seed": SEED,
+            "parallelism": f"replicas x{args.gpus}", "l2": "flushed between timed steps (256 MiB write)"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, local = dist_env()
+    kappa = workload_kappa()
+    # CPU baseline first (spawned pool before any CUDA context exists)
+    cpu = None
+    if rank == 0 and world >= 1 and args.gpus == 1 and not args.no_cpu_baseline and not args.profile:
+        cpu = cpu_baseline_entry(kappa)
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as td
+
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = td
+    from pymhm_b200.darcy import CartesianQ1Plan
+    from pymhm_b200.topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
+
+    mesh = CartesianMacroMesh(MACRO)
+    sk = SkeletonSpace(mesh, (FaceSpace.uniform(FACE_DEGREE),) * len(mesh.faces))
+    plans = {p: CartesianQ1Plan(mesh, sk, LOCAL, precision=p) for p in ("mixed", "fp64")}
+    dev = torch.device("cuda", local)
+    kappa_host = torch.from_numpy(np.ascontiguousarray(kappa)).pin_memory()
+    kappa_dev = kappa_host.to(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    results = {}
+    for prec, plan in plans.items():
+        plan.set_device_coefficients(1, kappa_dev, (0.0, 0.0, 0.0), 0, None, 1.0)
+        for _ in range(args.warmup):
+            plan.launch(stream)
+        torch.cuda.synchronize()
+        plan.check()
+        steps, kern = [], []
+        clocks = Clocks(local) if prec == "mixed" else None
+        barrier()
+        for _ in range(args.steps):
+            flush.zero_()
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+            plan.launch(stream, events=ev)
+            torch.cuda.synchronize()
+            steps.append(ev[0].elapsed_time(ev[4]))
+            kern.append([ev[k].elapsed_time(ev[k + 1]) for k in range(4)])
+        barrier()
+        clk = clocks.stop() if clocks else None
+        info, stats = plan.check()
+        results[prec] = dict(steps=np.array(steps), kern=np.array(kern), info=info, stats=stats, clocks=clk)
+
+    # end to end through the public API: H2D kappa, solve, D2H fields/flux/x/status
+    plan = plans["mixed"]
+    n_out = plan.fields.numel() + plan.flux.numel() + plan.x.numel()
+    host_fields = torch.empty(plan.fields.shape, dtype=torch.float64).pin_memory()
+    host_flux = torch.empty(plan.flux.shape, dtype=torch.float64).pin_memory()
+    host_x = torch.empty(plan.x.shape, dtype=torch.float64).pin_memory()
+    host_status = torch.empty(plan.cell_status.shape, dtype=torch.int32).pin_memory()
+    host_info = torch.empty(4, dtype=torch.int32).pin_memory()
+    e2e_ms = []
+    kdev = torch.empty_like(kappa_dev)
+    plan.set_device_coefficients(1, kdev, (0.0, 0.0, 0.0), 0, None, 1.0)
+    for it in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        kdev.copy_(kappa_host, non_blocking=True)
+        plan.launch(stream)
+        host_fields.copy_(plan.fields, non_blocking=True)
+        host_flux.copy_(plan.flux, non_blocking=True)
+        host_x.copy_(plan.x, non_blocking=True)
+        host_status.copy_(plan.cell_status, non_blocking=True)
+        host_info.copy_(plan.info, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        if it >= args.warmup:
+            e2e_ms.append(e0.elapsed_time(e1))
+        if int(host_status.numpy().max()) != 0 or int(host_info[0]) != 0:
+            raise RuntimeError("end-to-end solve reported a failure")
+    h2d = kappa_host.numel() * 8
+    d2h = n_out * 8 + host_status.numel() * 4 + 16
+
+    # accuracy against the reference's FP64 solution (golden fixture of the same workload)
+    acc = {}
+    gpath = os.path.join(ROOT, "tests", "golden", "darcy_64x64_r16_p2_lognormal.npz")
+    if os.path.exists(gpath):
+        g = np.load(gpath)
+        x = host_x.numpy()
+        T = plan.T
+        rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        acc = {"lambda": rel(x[:T], g["trace"]), "coarse": rel(x[T:], g["coarse"]),
+               "u_norm": abs(float(np.linalg.norm(host_fields.numpy())) / float(g["fields_norm"]) - 1),
+               "flux_norm": abs(float(np.linalg.norm(host_flux.numpy())) / float(g["flux_norm"]) - 1)}
+        keep = list(g["keep_cells"])
+        acc["u_cells"] = rel(host_fields.numpy()[keep], g["fields_cells"])
+        acc["flux_cells"] = rel(host_flux.numpy()[keep], g["flux_cells"])
+
+    def agg(v):
+        return max_over_ranks(v, dist, dev)
+
+    mixed, fp64 = results["mixed"], results["fp64"]
+    ms = agg(float(mixed["steps"].mean()))
+    ms64 = agg(float(fp64["steps"].mean()))
+    ms_e2e = agg(float(np.mean(e2e_ms)))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    kern = mixed["kern"].mean(axis=0)
+    names = ["q1_condense", "skeleton_scatter", "skeleton_pcg", "q1_reconstruct"]
+    top = int(np.argmax(kern))
+    roof = roofline(plan, names[top], kern[top], int(mixed["info"][1]), int(mixed["info"][2]))
+    from pymhm_b200 import darcy as _d  # noqa: F401
+
+    line = {
+        "metric": METRIC, "value": world * 1000.0 / ms, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (seeded lognormal kappa, f=1)", "config": workload_config(args),
+        "latency_ms": {"p50": float(np.percentile(mixed["steps"], 50)), "p99": float(np.percentile(mixed["steps"], 99))},
+        "fp64": {"value": world * 1000.0 / ms64, "ms_per_step": ms64,
+                 "p50": float(np.percentile(fp64["steps"], 50)), "p99": float(np.percentile(fp64["steps"], 99)),
+                 "kernels_ms": dict(zip(names, map(float, fp64["kern"].mean(axis=0)))),
+                 "global_iterations": int(fp64["info"][1])},
+        "mixed_over_fp64": ms64 / ms,
+        "kernels_ms": dict(zip(names, map(float, kern))),
+        "global_iterations": int(mixed["info"][1]), "outer_corrections": int(mixed["info"][2]),
+        "residual": float(mixed["stats"][0]), "certificate": float(mixed["stats"][1]),
+        "error_vs_reference": acc,
+        "e2e": {"value": world * 1000.0 / ms_e2e, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e},
+        "gpu_launches": 4 * args.steps,
+        "roofline": roof, "cpu_baseline": cpu, "clocks": mixed["clocks"],
+    }
+    line["config"]["skeleton_unknowns"] = plan.N
+    print(json.dumps(line), flush=True)
+
+
+def max_over_ranks(value, dist, device):
+    """Max of a per-rank scalar (the job's time is its slowest replica)."""
+    if dist is None:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def roofline(plan, kernel, ms, inner_iters, outer):
+    """Algorithmic bytes of the dominant kernel per launch over its measured time."""
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, source = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            peak, source = float(json.load(f)["hbm_gbs"]), "measured"
+    p = plan.pattern
+    nnz = len(p.indices)
+    nnz_s = int((p.trace_end - p.indptr[:plan.T]).sum())
+    M, n, w, T = plan.cells, plan.n, plan.w, plan.T
+    if kernel == "skeleton_pcg":
+        # per inner iteration: S values+indices once, ~14 trace vectors, 4 coarse passes over the
+        # (nx x nx) sine transforms and the cell maps; per outer correction one full K SpMV
+        per_iter = nnz_s * 12 + 14 * T * 8 + 4 * (2 * plan.mesh.nx * plan.mesh.nx * 8 + M * 8) + 2 * M * plan.t * 16
+        bytes_ = inner_iters * per_iter + (outer + 2) * (nnz * 12 + 2 * plan.N * 8)
+    elif kernel == "q1_condense":
+        bytes_ = plan.nxf * plan.nyf * 8 + M * w * (n + 1) * 8 + M * (plan.t + 1) * (plan.t + 2) * 8
+    elif kernel == "q1_reconstruct":
+        bytes_ = M * w * (n + 1) * 8 + plan.nxf * plan.nyf * 8 + M * n * 8 + M * plan.nfine * 16
+    else:
+        bytes_ = nnz * 24 + plan.N * 24
+    achieved = bytes_ / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None, "algorithmic_bytes": int(bytes_),
+            "peak_source": source + " (MEASURED_PEAKS.json hbm_gbs)" if source == "measured" else source}
+
+
+if __name__ == "__main__":
+    main()

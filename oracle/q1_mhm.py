@@ -705,3 +705,50 @@ def solve_darcy_q1(mesh, skeleton, refinement, permeability=1.0, source=0.0, dir
     corrected = np.array([r.coarse_vectors is not None for r in responses])
     return Q1Solution(trace, coarse, fields, flux, residual, matrix, rhs, corrected,
                       responses if keep_responses else [])
+
+
+# --------------------------------------------------------------------------------------
+# Timed CPU baseline: the local stage of the oracle over a sample of macrocells
+# --------------------------------------------------------------------------------------
+_SAMPLE_STATE = {}
+
+
+def _sample_init(macro, local, face_degree, kappa, source):
+    mesh = cartesian_mesh(macro)
+    sk = Skeleton(mesh, (FaceSpace.uniform(face_degree),) * len(mesh.faces))
+    nf = macro * local
+    perm = PixelField(kappa, (1.0 / nf, 1.0 / nf)) if kappa is not None else 1.0
+    _SAMPLE_STATE.update(mesh=mesh, sk=sk, local=local, perm=perm, source=source)
+
+
+def _sample_cells(cells):
+    st = _SAMPLE_STATE
+    for cell in cells:
+        _, problem = local_problem(st["mesh"], st["sk"], int(cell), (st["local"], st["local"]), st["perm"],
+                                   st["source"])
+        contribution(condense(problem), st["sk"].size + int(cell))
+    return len(cells)
+
+
+def local_stage_rate(macro, local, face_degree, kappa, source, cells, workers, pool=None):
+    """Macrocells per second of the oracle's assembly + condensation + contribution.
+
+    ``cells`` is the sampled list of macrocell ids, split over ``workers``
+    spawn processes (each owns its own copy of the mesh and coefficients).
+    """
+    import multiprocessing as mp
+    import time
+
+    chunks = [c for c in np.array_split(np.asarray(cells), workers) if len(c)]
+    own = pool is None
+    if own:
+        pool = mp.get_context("spawn").Pool(workers, initializer=_sample_init,
+                                            initargs=(macro, local, face_degree, kappa, source))
+        pool.map(_sample_cells, [c[:1] for c in chunks])  # warm imports and caches
+    t0 = time.perf_counter()
+    done = sum(pool.map(_sample_cells, chunks))
+    dt = time.perf_counter() - t0
+    if own:
+        pool.close()
+        pool.join()
+    return done / dt, dt

@@ -337,8 +337,8 @@ class CartesianQ1Plan:
         torch = self.torch
         kmode, karr, kconst = permeability_input(permeability, self.mesh, self.rx, self.ry, self.order)
         smode, sarr, sconst = source_input(source, self.mesh, self.rx, self.ry, self.order)
-        self.kappa = None if karr is None else torch.as_tensor(karr).to(self.device, non_blocking=non_blocking)
-        self.source = None if sarr is None else torch.as_tensor(sarr).to(self.device, non_blocking=non_blocking)
+        self.kappa = None if karr is None else torch.as_tensor(np.array(karr)).to(self.device, non_blocking=non_blocking)
+        self.source = None if sarr is None else torch.as_tensor(np.array(sarr)).to(self.device, non_blocking=non_blocking)
         self.set_device_coefficients(kmode, self.kappa, kconst, smode, self.source, sconst)
 
     def set_device_coefficients(self, kmode, kappa, kconst, smode, source, sconst):
@@ -349,26 +349,42 @@ class CartesianQ1Plan:
         q.source_mode, q.source, q.source_const = smode, _lib.ptr(source), float(sconst)
         self._keep = (kappa, source)
 
-    def launch(self, stream=None, *, reconstruct=True):
-        """Enqueue the four kernels on ``stream`` (no host synchronisation)."""
+    def launch(self, stream=None, *, reconstruct=True, events=None):
+        """Enqueue the four kernels on ``stream`` (no host synchronisation).
+
+        ``events``, if given, is a list of at least five ``torch.cuda.Event``s
+        recorded before, between and after the kernels (per-kernel timing).
+        """
         L, s = self.lib, _lib.stream_handle(stream)
         P = _lib.ptr
+        torch = self.torch
+        cur = torch.cuda.current_stream() if stream is None else stream
+
+        def mark(k):
+            if events is not None:
+                events[k].record(cur)
+
+        mark(0)
         _lib.check(L.mhm_q1_condense(self.q1, PRECISIONS[self.precision], self.max_refine, self.local_tol,
                                      P(self.solution), P(self.blocks), P(self.loads), P(self.corrected),
                                      P(self.cell_status), P(self.cell_iters), s), "mhm_q1_condense")
+        mark(1)
         pat = self.pattern
         _lib.check(L.mhm_skeleton_scatter(len(pat.indices), P(self.d_slot_ptr), P(self.d_contrib),
                                           P(self.blocks), P(self.values), self.N, self.T,
                                           P(self.d_load_ptr), P(self.d_load_contrib), P(self.loads),
                                           P(self.d_boundary), P(self.rhs), P(self.load_scale), s),
                    "mhm_skeleton_scatter")
+        mark(2)
         _lib.check(L.mhm_skeleton_solve(self.sys, P(self.rhs), P(self.load_scale), P(self.x), self.global_rtol,
                                         self.inner_rtol, self.max_inner, self.max_outer, self.grid,
                                         P(self.workspace), self.workspace.numel(), P(self.info), P(self.stats), s),
                    "mhm_skeleton_solve")
+        mark(3)
         if reconstruct:
             _lib.check(L.mhm_q1_reconstruct(self.q1, P(self.solution), P(self.d_cell_dofs), self.T, P(self.x),
                                             P(self.fields), P(self.flux), s), "mhm_q1_reconstruct")
+        mark(4)
 
     def check(self):
         """Synchronise and raise the reference's error for any failed cell or solve."""

@@ -1,0 +1,146 @@
+"""GPU global skeleton solver behind the reference's ``LinearFactorization`` contract.
+
+``SkeletonFactorization`` follows ``LinearFactorization`` (``src/pymhm/linalg/
+linear.py:240-331``) the way ``SaddleBlockSolver.as_factorization`` does
+(``linalg/block.py:211-217``): ``matches``, ``solve``, ``close``, ``rtol``.  It is
+passed as ``HybridSystem.solve(factorization=...)`` (``core/system.py:448-457``)
+for a Cartesian macro mesh with a uniform scalar skeleton and no fixed DOFs or
+gauge rows.  The solve is ``mhm_skeleton_solve`` (projected PCG with FP64 outer
+correction); every result is checked against the columnwise residual criterion
+of ``_checked`` (``linear.py:132-152``).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+from scipy import sparse
+
+from . import _lib
+from .errors import LinearSolveError
+from .topology import (
+    SkeletonSpace,
+    coarse_eigenvalues,
+    dof_cell_maps,
+    geometric_constraint,
+    mesh_arrays,
+    sine_transform,
+    skeleton_pattern,
+)
+
+
+def _canonical(matrix) -> sparse.csr_matrix:
+    op = sparse.csr_matrix(matrix, dtype=float, copy=True)
+    op.sum_duplicates()
+    op.sort_indices()
+    return op
+
+
+class SkeletonFactorization:
+    """Prepared GPU solver for one assembled skeleton matrix."""
+
+    solver = "mhm_b200"
+
+    def __init__(self, matrix, mesh, skeleton=None, *, rtol: float = 1e-10, inner_rtol: float = 1e-12,
+                 max_inner: int = 5000, max_outer: int = 8):
+        import torch
+
+        self.torch = torch
+        self.lib = _lib.lib()
+        self.mesh = mesh_arrays(mesh)
+        self.skeleton = SkeletonSpace(self.mesh) if skeleton is None else SkeletonSpace.of(skeleton, self.mesh)
+        space_h, space_v = self.skeleton.uniform_by_orientation()
+        if space_h.size != space_v.size:
+            raise NotImplementedError("the GPU skeleton solver requires equal face sizes")
+        self._matrix = _canonical(matrix)
+        self.rtol = float(rtol)
+        cell_dofs = self.skeleton.cell_dof_array
+        T = self.skeleton.size
+        M = len(self.mesh.cells)
+        N = T + M
+        if self._matrix.shape != (N, N):
+            raise ValueError("matrix does not match the skeleton layout")
+        pat = skeleton_pattern(cell_dofs, T)
+        rows = np.repeat(np.arange(N), np.diff(pat.indptr))
+        cols = pat.indices.astype(np.int64)
+        values = np.asarray(self._matrix[rows, cols]).ravel()
+        if not np.isclose(np.abs(values).sum(), np.abs(self._matrix.data).sum(), rtol=1e-14, atol=0):
+            raise ValueError("matrix has entries outside the skeleton pattern")
+        dev = torch.device("cuda")
+
+        def up(a, dtype):
+            return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=dev)
+
+        dof_cells, dof_slot = dof_cell_maps(cell_dofs, T)
+        self._keep = dict(
+            indptr=up(pat.indptr, torch.int64), indices=up(pat.indices, torch.int32),
+            values=up(values, torch.float64), trace_end=up(pat.trace_end, torch.int64),
+            cell_dofs=up(cell_dofs, torch.int64), g0=up(geometric_constraint(self.mesh, space_h, space_v), torch.float64),
+            dof_cells=up(dof_cells, torch.int32), dof_slot=up(dof_slot, torch.int32),
+            qx=up(sine_transform(self.mesh.nx), torch.float64), qy=up(sine_transform(self.mesh.ny), torch.float64),
+            eig=up(coarse_eigenvalues(self.mesh, space_h, space_v), torch.float64))
+        k = self._keep
+        s = self.sys = _lib.SkeletonSystem()
+        s.size, s.trace_size = N, T
+        s.indptr, s.indices, s.values = _lib.ptr(k["indptr"]), _lib.ptr(k["indices"]), _lib.ptr(k["values"])
+        s.trace_end = _lib.ptr(k["trace_end"])
+        s.faces, s.face_size, s.cells, s.cell_width = len(self.mesh.faces), space_h.size, M, cell_dofs.shape[1]
+        s.cell_dofs, s.cell_g0 = _lib.ptr(k["cell_dofs"]), _lib.ptr(k["g0"])
+        s.dof_cells, s.dof_slot = _lib.ptr(k["dof_cells"]), _lib.ptr(k["dof_slot"])
+        s.nx, s.ny = self.mesh.nx, self.mesh.ny
+        s.qx, s.qy, s.coarse_eig = _lib.ptr(k["qx"]), _lib.ptr(k["qy"]), _lib.ptr(k["eig"])
+        nbytes = self.lib.mhm_skeleton_workspace_bytes(s, 0)
+        self.workspace = torch.empty(int(nbytes), dtype=torch.uint8, device=dev)
+        self.info = torch.zeros(4, dtype=torch.int32, device=dev)
+        self.stats = torch.zeros(4, dtype=torch.float64, device=dev)
+        self.inner_rtol, self.max_inner, self.max_outer = inner_rtol, max_inner, max_outer
+        self._open = True
+        self.N = N
+
+    def matches(self, matrix) -> bool:
+        other = _canonical(matrix)
+        return bool(self._matrix.shape == other.shape and (self._matrix != other).nnz == 0)
+
+    def _solve_one(self, b: np.ndarray) -> np.ndarray:
+        torch = self.torch
+        rhs = torch.as_tensor(np.ascontiguousarray(b, dtype=np.float64), device="cuda")
+        x = torch.empty_like(rhs)
+        P = _lib.ptr
+        _lib.check(self.lib.mhm_skeleton_solve(self.sys, P(rhs), 0, P(x), 1e-13,
+                                               self.inner_rtol, self.max_inner, self.max_outer, 0,
+                                               P(self.workspace), self.workspace.numel(), P(self.info),
+                                               P(self.stats), _lib.stream_handle(None)), "mhm_skeleton_solve")
+        info = self.info.cpu().numpy()
+        if info[0] not in (_lib.SOLVE_OK, _lib.SOLVE_NOT_CONVERGED):
+            raise LinearSolveError(_lib.SOLVE_MESSAGES.get(int(info[0]), f"status {info[0]}"))
+        return x.cpu().numpy()
+
+    def solve(self, rhs, *, refinement_precision: str = "double", refinement_steps: int = 2) -> np.ndarray:
+        if not self._open:
+            raise RuntimeError("factorization is closed")
+        if refinement_precision != "double":
+            raise ValueError("the GPU skeleton solver refines in double precision")
+        del refinement_steps
+        forcing = np.asarray(rhs, dtype=float)
+        if forcing.ndim not in (1, 2) or forcing.shape[0] != self.N or not np.all(np.isfinite(forcing)):
+            raise ValueError("rhs must have shape (n,) or (n, nrhs) matching matrix")
+        cols = forcing[:, None] if forcing.ndim == 1 else forcing
+        out = np.column_stack([self._solve_one(cols[:, j]) for j in range(cols.shape[1])])
+        # columnwise acceptance as in linalg/linear.py:132-152
+        diff = self._matrix @ out - cols
+        scale = np.max(np.abs(cols), axis=0)
+        scale = np.where(scale > 0, scale, 1.0)
+        res = np.linalg.norm(diff / scale, axis=0)
+        thr = self.rtol * np.linalg.norm(cols / scale, axis=0)
+        if np.any(res > thr):
+            raise LinearSolveError(f"residual criterion failed: scaled ||Ax-b||={res}, allowed={thr}")
+        return out[:, 0] if forcing.ndim == 1 else out
+
+    def close(self) -> None:
+        self._open = False
+        self._keep = {}
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

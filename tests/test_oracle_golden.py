@@ -1,0 +1,100 @@
+"""The oracle against fixtures written by the reference itself (tests/golden/make_golden.py)."""
+
+import numpy as np
+import pytest
+from scipy import sparse
+
+from oracle import q1_mhm as o
+from tests._cases import CASES, load, rel
+
+
+def oracle_case(name):
+    g = load(name)
+    margs, (deg, sub), ref, perm, src, dr = CASES[name]
+    mesh = o.cartesian_mesh(*margs)
+    sk = o.Skeleton(mesh, (o.FaceSpace.uniform(deg, sub),) * len(mesh.faces))
+    p = perm(g)
+    if hasattr(p, "values"):
+        p = o.PixelField(p.values, p.spacing, p.origin)
+    return g, mesh, sk, ref, p, src, dr
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_oracle_matches_reference(name):
+    g, mesh, sk, ref, perm, src, dr = oracle_case(name)
+    assert np.array_equal(mesh.cell_faces, g["cell_faces"])
+    assert np.array_equal(mesh.signs, g["signs"])
+    assert np.array_equal(mesh.faces, g["faces"])
+    assert np.array_equal(sk.offsets, g["offsets"])
+    sol = o.solve_darcy_q1(mesh, sk, ref, perm, src, dr, keep_responses=True)
+    # bit-exact sparsity after the reference's eliminate_zeros
+    assert np.array_equal(sol.matrix.indptr, g["indptr"])
+    assert np.array_equal(sol.matrix.indices, g["indices"])
+    # values: identical arithmetic except the breakpoint-split trace integrals (1e-16 level)
+    tol = 0.0 if name != "affine_3x2_rect_r4x5_p1s2" else 1e-13
+    assert np.max(np.abs(sol.matrix.data - g["data"])) <= tol * np.max(np.abs(g["data"]))
+    for key, val in (("trace", sol.trace), ("coarse", sol.coarse), ("fields", sol.fields), ("flux", sol.flux),
+                     ("rhs", sol.rhs)):
+        assert rel(val, g[key]) <= max(tol, 0.0) * 100, key
+    assert np.array_equal(sol.corrected, g["corrected"])
+    for c in g["keep_cells"]:
+        r = sol.responses[c]
+        idx, block, ld = o.contribution(r, sk.size + c)
+        assert rel(r.lifts, g[f"cell{c}_lifts"]) <= tol * 100
+        assert rel(block, g[f"cell{c}_block"]) <= tol * 100
+        assert rel(ld, g[f"cell{c}_load"]) <= max(tol * 100, 1e-12)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_structural_pattern_covers_reference(name):
+    """Reference nonzeros = structural pattern minus entries that sum to exactly zero."""
+    from pymhm_b200.topology import skeleton_pattern
+
+    g, mesh, sk, ref, perm, src, dr = oracle_case(name)
+    cell_dofs = np.array([sk.cell_dofs(c) for c in range(len(mesh.cells))])
+    pat = skeleton_pattern(cell_dofs, sk.size)
+    N = pat.size
+    struct = sparse.csr_matrix((np.ones(len(pat.indices)), pat.indices, pat.indptr), shape=(N, N))
+    ref_m = sparse.csc_matrix((g["data"], g["indices"], g["indptr"]), shape=(N, N)).tocsr()
+    ref_m.sort_indices()
+    ones = ref_m.copy()
+    ones.data[:] = 1.0
+    assert (ones - ones.multiply(struct)).nnz == 0  # reference pattern inside the structural one
+    # the oracle's own pre-elimination assembly is zero exactly on the difference
+    contribs = []
+    for c in range(len(mesh.cells)):
+        _, prob = o.local_problem(mesh, sk, c, ref, perm, src)
+        contribs.append(o.contribution(o.condense(prob), sk.size + c))
+    rows = np.concatenate([np.repeat(i, len(i)) for i, _, _ in contribs])
+    cols = np.concatenate([np.tile(i, len(i)) for i, _, _ in contribs])
+    vals = np.concatenate([b.ravel() for _, b, _ in contribs])
+    full = sparse.coo_matrix((vals, (rows, cols)), shape=(N, N)).tocsr()
+    full.sum_duplicates()
+    missing = struct - ones.multiply(struct)
+    r, cc = missing.nonzero()
+    if len(r):
+        assert np.all(np.asarray(full[r, cc]).ravel() == 0.0)
+    assert len(pat.indices) - len(g["indices"]) == len(r)
+
+
+def test_full_size_topology_digests():
+    from pymhm_b200.workloads import digest
+
+    g = load("darcy_64x64_r16_p2_lognormal")
+    mesh = o.cartesian_mesh(64)
+    sk = o.Skeleton(mesh, (o.FaceSpace.uniform(2),) * len(mesh.faces))
+    cell_dofs = np.array([sk.cell_dofs(c) for c in range(len(mesh.cells))])
+    assert digest(mesh.cell_faces) == str(g["cell_faces_sha256"])
+    assert digest(mesh.signs) == str(g["signs_sha256"])
+    assert digest(mesh.faces) == str(g["faces_sha256"])
+    assert digest(cell_dofs) == str(g["cell_dofs_sha256"])
+
+
+def test_oracle_condensation_matches_monolithic_solve():
+    """The reference's algebraic check (tests/test_hybrid.py:28-42) on a Q1 cell."""
+    g = load("poisson_8x8_r4_p1")
+    aug, rhs = g["cell0_aug"], g["cell0_rhs"]
+    x = np.linalg.solve(aug, rhs)
+    n = len(g["cell0_source"])
+    assert np.allclose(x[:n, 0], g["cell0_source"], atol=1e-13)
+    assert np.allclose(x[:n, 1:1 + g["cell0_lifts"].shape[1]], g["cell0_lifts"], atol=1e-13)
