@@ -169,6 +169,27 @@ int mhm_skeleton_solve(const mhm_skeleton_system* s /* host */, const double* rh
                        int32_t max_inner, int32_t max_outer, int32_t grid, void* workspace,
                        int64_t workspace_bytes, int32_t* info, double* stats, void* stream);
 
+/*
+ * Allocation-free form of mhm_skeleton_solve, for callers that cannot allocate
+ * device memory (a C/Fortran/FFI host code without its own CUDA allocator, or a
+ * serving process that reserves all device memory up front and must not call
+ * cudaMalloc/cudaFree, which also synchronise the device).  It has no
+ * counterpart in the reference, which solves the global system on the host.
+ * The scratch is a fixed 4 MiB file-scope device array that every GPU loading
+ * the library holds until exit; systems whose mhm_skeleton_workspace_bytes
+ * exceeds 4 MiB are rejected with MHM_ERR_UNSUPPORTED (64x64 macrocells with
+ * three DOFs per face need about 2.6 MiB).  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU (other streams, other host threads) race
+ * and must be serialised by the caller.  Arguments and results are those of
+ * mhm_skeleton_solve.
+ */
+int mhm_skeleton_solve_static(const mhm_skeleton_system* s /* host */, const double* rhs,
+                              const double* load_scale, double* x, double rtol, double inner_rtol,
+                              int32_t max_inner, int32_t max_outer, int32_t grid, int32_t* info,
+                              double* stats, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Reconstruction u_K = R f - (R B) lambda_K + E c_K and flux -K grad u       */
 /* ------------------------------------------------------------------------ */

@@ -77,6 +77,8 @@ _SIGNATURES = {
     "mhm_skeleton_workspace_bytes": (C.c_int64, [C.POINTER(SkeletonSystem), C.c_int32]),
     "mhm_skeleton_solve": (C.c_int, [C.POINTER(SkeletonSystem), P, P, P, C.c_double, C.c_double, C.c_int32,
                                      C.c_int32, C.c_int32, P, C.c_int64, P, P, P]),
+    "mhm_skeleton_solve_static": (C.c_int, [C.POINTER(SkeletonSystem), P, P, P, C.c_double, C.c_double,
+                                            C.c_int32, C.c_int32, C.c_int32, P, P, P]),
     "mhm_q1_reconstruct": (C.c_int, [C.POINTER(Q1Problem), P, P, C.c_int64, P, P, P, P]),
     "mhm_batched_factor": (C.c_int, [C.c_int64, C.c_int32, P, P, P, P, P, P, P]),
     "mhm_batched_solve": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, P, P, P, P, P, P, P, C.c_double,
