@@ -149,9 +149,9 @@ typedef struct mhm_skeleton_system {
     const int32_t* dof_cells;     /* (T, 2): cells sharing the DOF (-1 = none)      */
     const int32_t* dof_slot;      /* (T, 2): position of the DOF in each cell      */
     int32_t nx, ny;               /* macro grid of the coarse Poisson operator     */
-    const double* qx;             /* (nx, nx) orthonormal sine transform           */
-    const double* qy;             /* (ny, ny)                                      */
-    const double* coarse_eig;     /* (ny, nx) eigenvalues of G0^T G0               */
+    const double* qx;             /* (nx, nx) orthonormal sine transform along x   */
+    /* G0^T G0 = coarse_ay (T_y (x) I) + coarse_ax (I (x) T_x), T = tridiag(-1,2,-1) */
+    double coarse_ax, coarse_ay;
 } mhm_skeleton_system;
 
 int64_t mhm_skeleton_workspace_bytes(const mhm_skeleton_system* s /* host */, int32_t grid);
@@ -161,8 +161,11 @@ int64_t mhm_skeleton_workspace_bytes(const mhm_skeleton_system* s /* host */, in
  * inner iterations, outer corrections, barrier error flag.  stats (device
  * double[4]): final relative residual ||rhs - K x|| / ||rhs||, the physical
  * certificate ||K x - rhs|| / max(||rhs||, ||load_scale||, || |K||x| ||),
- * first inner relative residual, unused.  grid = number of persistent CTAs
- * (0 = one per SM); workspace sized by mhm_skeleton_workspace_bytes.
+ * first inner relative residual, unused.  The solve runs as one persistent
+ * cooperative kernel with one CTA per macro row (ny CTAs, all co-resident;
+ * MHM_ERR_UNSUPPORTED when they do not fit or a row's tables exceed shared
+ * memory); `grid` is accepted for ABI stability and ignored.  workspace is
+ * sized by mhm_skeleton_workspace_bytes.
  */
 int mhm_skeleton_solve(const mhm_skeleton_system* s /* host */, const double* rhs,
                        const double* load_scale, double* x, double rtol, double inner_rtol,

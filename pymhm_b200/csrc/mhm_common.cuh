@@ -85,6 +85,6 @@ __device__ __forceinline__ double block_min(double v, double* scratch) {
   return r;
 }
 
-inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
 }  // namespace mhm

@@ -34,7 +34,7 @@ from .topology import (
     FaceSpace,
     SkeletonSpace,
     boundary_data,
-    coarse_eigenvalues,
+    coarse_coefficients,
     coupling_tables,
     dof_cell_maps,
     geometric_constraint,
@@ -283,8 +283,7 @@ class CartesianQ1Plan:
         self.d_dof_cells = up(dof_cells, torch.int32)
         self.d_dof_slot = up(dof_slot, torch.int32)
         self.d_qx = up(sine_transform(m.nx), torch.float64)
-        self.d_qy = up(sine_transform(m.ny), torch.float64)
-        self.d_eig = up(coarse_eigenvalues(m, space_h, space_v), torch.float64)
+        self.coarse_ab = coarse_coefficients(m, space_h, space_v)
         # ---- device buffers -----------------------------------------------------------
         M, n, w, t1 = self.cells, self.n, self.w, self.t + 1
         self.solution = torch.empty((M, w, n + 1), **f64)
@@ -325,7 +324,8 @@ class CartesianQ1Plan:
         s.cell_dofs, s.cell_g0 = _lib.ptr(self.d_cell_dofs), _lib.ptr(self.d_g0)
         s.dof_cells, s.dof_slot = _lib.ptr(self.d_dof_cells), _lib.ptr(self.d_dof_slot)
         s.nx, s.ny = m.nx, m.ny
-        s.qx, s.qy, s.coarse_eig = _lib.ptr(self.d_qx), _lib.ptr(self.d_qy), _lib.ptr(self.d_eig)
+        s.qx = _lib.ptr(self.d_qx)
+        s.coarse_ax, s.coarse_ay = self.coarse_ab
         nbytes = self.lib.mhm_skeleton_workspace_bytes(s, self.grid)
         if nbytes <= 0:
             raise RuntimeError("could not size the skeleton solver workspace")

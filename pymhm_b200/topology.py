@@ -454,12 +454,21 @@ def sine_transform(n: int) -> np.ndarray:
     return np.sqrt(2.0 / (n + 1)) * np.sin(np.pi * np.outer(k, k) / (n + 1))
 
 
-def coarse_eigenvalues(mesh: CartesianMacroMesh, space_h: FaceSpace, space_v: FaceSpace) -> np.ndarray:
-    """Eigenvalues (ny, nx) of G0^T G0 in the sine basis."""
+def coarse_coefficients(mesh: CartesianMacroMesh, space_h: FaceSpace, space_v: FaceSpace) -> tuple[float, float]:
+    """(ax, ay) with G0^T G0 = ay (T_y (x) I) + ax (I (x) T_x), T = tridiag(-1, 2, -1).
+
+    A vertical face couples x-neighbours with weight hy^2 |int psi|^2 summed over its
+    basis, a horizontal face couples y-neighbours with hx^2 |int psi|^2.
+    """
     mh2 = float(np.sum(space_h.moments() ** 2))
     mv2 = float(np.sum(space_v.moments() ** 2))
     hx, hy = mesh.spacing
-    ax, ay = hy * hy * mv2, hx * hx * mh2
+    return hy * hy * mv2, hx * hx * mh2
+
+
+def coarse_eigenvalues(mesh: CartesianMacroMesh, space_h: FaceSpace, space_v: FaceSpace) -> np.ndarray:
+    """Eigenvalues (ny, nx) of G0^T G0 in the sine basis."""
+    ax, ay = coarse_coefficients(mesh, space_h, space_v)
     lx = 2 - 2 * np.cos(np.pi * np.arange(1, mesh.nx + 1) / (mesh.nx + 1))
     ly = 2 - 2 * np.cos(np.pi * np.arange(1, mesh.ny + 1) / (mesh.ny + 1))
     return ay * ly[:, None] + ax * lx[None, :]

@@ -40,12 +40,12 @@ def test_struct_layout_matches_header(tmp_path):
         "int main(void){printf(\"%zu %zu %zu %zu %zu %zu\\n\", sizeof(mhm_q1_problem),"
         " offsetof(mhm_q1_problem, kappa_const), offsetof(mhm_q1_problem, quad_order),"
         " sizeof(mhm_skeleton_system), offsetof(mhm_skeleton_system, nx),"
-        " offsetof(mhm_skeleton_system, coarse_eig)); return 0;}\n")
+        " offsetof(mhm_skeleton_system, coarse_ay)); return 0;}\n")
     exe = tmp_path / "layout"
     subprocess.run(["gcc", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [ctypes.sizeof(_lib.Q1Problem), _lib.Q1Problem.kappa_const.offset, _lib.Q1Problem.quad_order.offset,
-            ctypes.sizeof(_lib.SkeletonSystem), _lib.SkeletonSystem.nx.offset, _lib.SkeletonSystem.coarse_eig.offset]
+            ctypes.sizeof(_lib.SkeletonSystem), _lib.SkeletonSystem.nx.offset, _lib.SkeletonSystem.coarse_ay.offset]
     assert got == want
 
 
