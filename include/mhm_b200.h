@@ -149,9 +149,16 @@ typedef struct mhm_skeleton_system {
     const int32_t* dof_cells;     /* (T, 2): cells sharing the DOF (-1 = none)      */
     const int32_t* dof_slot;      /* (T, 2): position of the DOF in each cell      */
     int32_t nx, ny;               /* macro grid of the coarse Poisson operator     */
-    const double* qx;             /* (nx, nx) orthonormal sine transform along x   */
     /* G0^T G0 = coarse_ay (T_y (x) I) + coarse_ax (I (x) T_x), T = tridiag(-1,2,-1) */
     double coarse_ax, coarse_ay;
+    /* Optional (NULL allowed): the cells' own trace blocks, (cells, block_ld,
+     * block_ld) row-major, top-left cell_width x cell_width used; S must equal
+     * their sum scattered through cell_dofs (mhm_q1_condense's `blocks` with
+     * block_ld = cell_width + 1).  With them the solve uses the cell-Dirichlet
+     * preconditioner; without them it splits S from the CSR matrix and uses
+     * additive Schwarz over the cells' 12 x 12 principal submatrices.          */
+    const double* cell_blocks;
+    int32_t block_ld;
 } mhm_skeleton_system;
 
 int64_t mhm_skeleton_workspace_bytes(const mhm_skeleton_system* s /* host */, int32_t grid);

@@ -64,7 +64,8 @@ class SkeletonSystem(C.Structure):
         ("faces", C.c_int32), ("face_size", C.c_int32), ("cells", C.c_int32), ("cell_width", C.c_int32),
         ("cell_dofs", C.c_void_p), ("cell_g0", C.c_void_p), ("dof_cells", C.c_void_p),
         ("dof_slot", C.c_void_p), ("nx", C.c_int32), ("ny", C.c_int32),
-        ("qx", C.c_void_p), ("coarse_ax", C.c_double), ("coarse_ay", C.c_double),
+        ("coarse_ax", C.c_double), ("coarse_ay", C.c_double),
+        ("cell_blocks", C.c_void_p), ("block_ld", C.c_int32),
     ]
 
 

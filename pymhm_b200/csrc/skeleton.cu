@@ -8,25 +8,45 @@
 // The global unknown is (lambda, c): skeleton traces and one retained constant per
 // macrocell.  Its operator is the symmetric saddle K = [[S, -G], [-G^T, -C]] with
 // C at rounding level.  The solver here is an outer FP64 defect correction on K
-// whose inner solve is a FETI-style projected CG on
+// (residuals from the assembled CSR matrix) whose inner solve is a FETI-style
+// projected CG on
 //     K0 = [[S, -G0], [-G0^T, 0]],
 // G0 the exact geometric net-flux operator of the Cartesian macro grid.
 // G0^T G0 = ay (T_y (x) I) + ax (I (x) T_x) is a scaled 2-D Dirichlet Laplacian
 // on the macro cells; it is inverted exactly by an orthonormal sine transform
 // along x, the inverse of one tridiagonal Toeplitz matrix along y per sine mode
 // (closed form through Chebyshev polynomials of the second kind), and the
-// inverse transform.  The preconditioner is block Jacobi over skeleton faces.
-// K - K0 is at rounding level, so two or three outer corrections reach FP64
-// accuracy.
+// inverse transform.  K - K0 is at rounding level, so two or three outer
+// corrections reach FP64 accuracy.
+//
+// Cell form.  S = sum_c R_c^T S_c R_c over macrocells c (S_c the t x t trace
+// block each cell contributes), so S u is applied as per-cell products S_c u_c
+// whose face partials are summed per DOF (first cell + second cell, a fixed
+// order).  With the cells' own blocks available the preconditioner is the
+// cell-Dirichlet one, M^-1 = sum_c R_c^T D_c S_c^-1 D_c R_c with stiffness
+// weights D_c,a = S_c,aa / sum_{c' containing the DOF} S_c',a'a'.  From an
+// assembled matrix alone, S is split exactly into cell parts (entries of a face
+// shared by two cells halved) and the preconditioner is additive Schwarz over
+// the cells' principal 12 x 12 submatrices.
+//
+// The inner CG uses the single-reduction recurrence of Chronopoulos and Gear
+// (J. Comput. Appl. Math. 25 (1989) 153-168): with u = P M^-1 r and w = S u,
+//   gamma = (r, u), delta = (u, w), beta = gamma / gamma_prev,
+//   alpha = gamma / (delta - beta gamma / alpha_prev),
+//   p = u + beta p, P S p = P w + beta P S p_prev, r -= alpha P S p,
+// P = I - G0 (G0^T G0)^-1 G0^T.  Every kReproject iterations r and P S p are
+// projected again, which removes the drift of the recurrences out of range(P).
 //
 // Everything runs in one persistent cooperative kernel with one CTA per macro
-// row: CTA r owns the faces first met by the cells of row r (a contiguous DOF
-// range in the reference's numbering), the row's coarse unknowns and the row's
-// sine transform.  An inner iteration needs four grid barriers.  Each phase
-// stages what it reads from other CTAs into shared memory with batched loads
-// and computes from there.  The barrier is a monotonic arrival counter with a
-// bounded spin: on timeout every CTA sets the error flag and returns
-// (MHM_SOLVE_BARRIER_TIMEOUT).
+// row.  CTA r owns the DOFs first met by the cells of row r (a contiguous range
+// in the reference's numbering) and keeps the iteration vectors on the DOFs of
+// its own cells (owned DOFs plus the bottom faces).  Each CTA turns its cells'
+// partials into coarse data for its own row and for the two neighbouring rows
+// (G0^T of a partial reaches the neighbour through the shared face), so an inner
+// iteration needs two grid barriers and every cross-CTA value it reads arrives
+// in one batch of loads after a barrier.  The barrier is a monotonic arrival
+// counter with a bounded spin: on timeout every CTA sets the error flag and
+// returns (MHM_SOLVE_BARRIER_TIMEOUT).
 #include <cmath>
 
 #include "mhm_common.cuh"
@@ -35,6 +55,8 @@ namespace mhm {
 namespace {
 
 constexpr int kSolveThreads = 512;
+constexpr int kWarps = kSolveThreads / 32;
+constexpr int kReproject = 16;
 constexpr long long kSpinLimit = 1ll << 26;
 
 struct Sys {
@@ -49,17 +71,25 @@ struct Sys {
   const int32_t* dof_cells;
   const int32_t* dof_slot;
   int nx, ny;
-  const double* qx;
   double ax, ay;
+  const double* blocks;
+  int ld;
+};
+
+// Coarse data of one quantity: U[row][k] = self[row] + below[row] + above[row],
+// `below` written by the CTA of row-1, `above` by the CTA of row+1 (null: absent).
+struct Coarse {
+  double *self, *below, *above;
 };
 
 struct Work {
-  double *lam, *rho, *rhoP, *z, *zt, *p, *q, *tmp;  // T each
-  double* rfull;                                    // N
-  double *U, *U2;                                   // M each ([iy][k]), two buffers
-  double* cheb;                                     // nx * (ny + 1) Chebyshev tables
-  double* part;                                     // grid * 4
-  unsigned* bar;                                    // arrival counter
+  double *Zf, *Zs, *Vf, *Vs;  // T each: per-DOF partials of the first / second cell
+  Coarse Uz, Uw;              // M each part
+  double *Ux1, *Ux2;          // M each: coarse data of DOF vectors
+  double* rfull;              // N: outer residual
+  double* cheb;               // nx * (ny + 1) Chebyshev tables
+  double* part;               // grid * 4 partial sums
+  unsigned* bar;              // arrival counter
   int* err;
 };
 
@@ -112,23 +142,64 @@ __device__ bool grid_sync(const Work& w, unsigned& epoch) {
   return bad == 0;
 }
 
-// Sum of the per-CTA partials `slot` (fixed order, identical in every CTA).
-__device__ double grid_total(const Work& w, int slot, double* sh) {
+// Sums of the per-CTA partials in slots [slot, slot + n) (fixed order, identical
+// in every CTA); the loads of all slots are issued together.
+template <int NS>
+__device__ void grid_totals(const Work& w, int slot, double (&out)[NS], double* sh) {
   if (threadIdx.x < 32) {
-    double v = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) v += __ldcg(w.part + i * 4 + slot);
-    v = warp_sum(v);
-    if (threadIdx.x == 0) sh[0] = v;
+    double v[NS][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = threadIdx.x + 32 * q;
+#pragma unroll
+      for (int n = 0; n < NS; ++n) v[n][q] = i < (int)gridDim.x ? __ldcg(w.part + i * 4 + slot + n) : 0.0;
+    }
+    for (int i0 = threadIdx.x + 128; i0 < (int)gridDim.x; i0 += 32)
+#pragma unroll
+      for (int n = 0; n < NS; ++n) v[n][0] += __ldcg(w.part + i0 * 4 + slot + n);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      const double a = warp_sum((v[n][0] + v[n][1]) + (v[n][2] + v[n][3]));
+      if (threadIdx.x == 0) sh[n] = a;
+    }
   }
   __syncthreads();
-  const double r = sh[0];
+#pragma unroll
+  for (int n = 0; n < NS; ++n) out[n] = sh[n];
   __syncthreads();
-  return r;
+}
+
+__device__ double grid_total(const Work& w, int slot, double* sh) {
+  double o[1];
+  grid_totals<1>(w, slot, o, sh);
+  return o[0];
 }
 
 __device__ void put_partial(const Work& w, int slot, double v, double* red) {
   v = block_sum(v, red);
   if (threadIdx.x == 0) w.part[blockIdx.x * 4 + slot] = v;
+}
+
+// Two partials in one block reduction (red >= 64 doubles).
+__device__ void put_partial2(const Work& w, int slot, double a, double b, double* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  a = warp_sum(a);
+  b = warp_sum(b);
+  __syncthreads();
+  if (lane == 0) {
+    red[wid] = a;
+    red[32 + wid] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sa = 0.0, sb = 0.0;
+    for (int i = 0; i < nw; ++i) {
+      sa += red[i];
+      sb += red[32 + i];
+    }
+    w.part[blockIdx.x * 4 + slot] = sa;
+    w.part[blockIdx.x * 4 + slot + 1] = sb;
+  }
 }
 
 __device__ __forceinline__ double krow(const Sys& s, int64_t i, const double* v) {
@@ -137,91 +208,56 @@ __device__ __forceinline__ double krow(const Sys& s, int64_t i, const double* v)
   return acc;
 }
 
-// Per-CTA state.  CTA r owns macro row r: DOFs [d0, d1) (the faces first met by
-// the row's cells), the row's coarse unknowns and sine mode r.  The "G range"
-// [gs, d1) covers row r-1's and row r's DOFs: every DOF whose G0 coefficients,
-// face inverse or preconditioned residual the CTA needs; all of their cells lie
-// in rows r-1..r+1.  The window [w0, w1) covers rows r-1..r+1 (SpMV columns).
+// S[i][j] of the assembled CSR (0 when the entry is not stored).
+__device__ double csr_entry(const Sys& s, int64_t i, int64_t j) {
+  int64_t lo = s.indptr[i], hi = s.indptr[i + 1];
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) / 2;
+    const int64_t c = s.indices[mid];
+    if (c == j) return s.values[mid];
+    if (c < j) lo = mid + 1; else hi = mid;
+  }
+  return 0.0;
+}
+
+// Per-CTA state.  CTA r owns macro row r and the DOFs [d0, d1) first met in it.
+// Local DOFs ("G"): l < nown are the owned DOFs d0 + l; l >= nown (rows r > 0)
+// are the bottom faces of the row's cells, nown + cx * fs + j.  These are all
+// the DOFs of the row's cells; their cells lie in rows r-1 .. r+1, whose coarse
+// values are kept in yrow slots 0..2 (slot = row - r + 1).
 struct Row {
-  int r, c0;
-  int64_t d0, d1, gs, w0, w1;
-  double* qx;    // nx*nx
-  double* yrow;  // 3*nx: Y of rows r-1, r, r+1
-  double* col;   // max(nx, ny) scratch
-  double* win;   // staged vector (window or G range)
-  double* ga;    // G range: G0 coefficient of the first / second cell
-  double* gb;
-  int16_t* ya;   // yrow index of the first / second cell (second: -1 = none)
-  int16_t* yb;
-  double* minv;  // face inverses of the G range
-  int16_t* cl;   // own cells: G-range index of each cell DOF (nx*t)
-  double* cg;    // own cells: G0 coefficient of each cell DOF
-  double* cheb;  // Chebyshev tables U_m(theta_k), m = 0..ny, of every sine mode
-  double* wrow;  // W rows r-1..r+1 (sine space along x)
-  double* cinv;  // 1 / (ay U_ny(theta_k)) per mode
-  double* ust;   // staged U, transposed [k][iy] with row pitch ny+1
+  int r, c0, nown, ng;
+  int64_t d0, d1;
+  double* sine;  // 2 (nx + 1): sqrt(2/(nx+1)) sin(pi m / (nx+1))
+  double* yrow;  // 3 nx
+  double* col;   // 8 nx: self, bottom, right, top, left sums; then self, up, down columns
+  double* wrow;  // 3 nx
+  double* cinv;  // nx
+  double* cheb;  // nx (ny + 1)
+  double *vr, *vps, *vp, *vlam, *vu, *vt;  // G vectors: r, P S p, p, lambda, u, staging
+  double* cpart;  // nx t: per-cell partials
+  double* Sb;     // nx np: packed symmetric S_c
+  double* Pb;     // nx np: packed symmetric preconditioner block
+  double *ga, *gb;  // G: G0 coefficient of the first / second cell
+  int16_t *ya, *yb; // G: yrow index of the first / second cell (second: -1 = none)
+  int32_t* gdof;    // G: global DOF
+  int16_t* cl;      // nx t: local DOF of each cell slot
+  double* gself;    // nx t: g0 of the cell on its slot
+  double* gnb;      // nx t: g0 of the other cell on the same DOF (0: none)
+  uint8_t* role;    // nx t: bit 0 = the cell is the DOF's second cell, bit 1 = the DOF has two cells
+  uint8_t* pidx;    // t t: packed symmetric index
+  double* scratch;  // kWarps t t (aliases the G vectors during setup)
 };
 
-__device__ __forceinline__ double g0y(const Row& R, int64_t l) {
+__device__ __forceinline__ double g0y(const Row& R, int l) {
   double v = R.ga[l] * R.yrow[R.ya[l]];
   const int b = R.yb[l];
   if (b >= 0) v = fma(R.gb[l], R.yrow[b], v);
   return v;
 }
 
-// dst[k] = src[k] (k < n) through L2; each thread issues eight loads before it stores
-// any of them, so a staging pass costs one round trip instead of one per element.
-__device__ __forceinline__ void copy_l2(double* dst, const double* src, int64_t n) {
-  for (int64_t base = threadIdx.x; base < n; base += 8 * (int64_t)blockDim.x) {
-    double v[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int64_t k = base + (int64_t)u * blockDim.x;
-      v[u] = k < n ? __ldcg(src + k) : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int64_t k = base + (int64_t)u * blockDim.x;
-      if (k < n) dst[k] = v[u];
-    }
-  }
-}
-
-// Stage v over the SpMV window [w0, w1) or over the G range [gs, d1) into R.win.
-__device__ void stage(const Row& R, const double* v) {
-  __syncthreads();
-  copy_l2(R.win, v + R.w0, R.w1 - R.w0);
-  __syncthreads();
-}
-
-__device__ void stage_g(const Row& R, const double* v) {
-  __syncthreads();
-  copy_l2(R.win, v + R.gs, R.d1 - R.gs);
-  __syncthreads();
-}
-
-// (S v)_i with v staged in R.win over the window; matrix entries are fetched
-// sixteen at a time, all loads of a chunk in flight together.
-__device__ __forceinline__ double srow_win(const Sys& s, const Row& R, int64_t i) {
-  const int64_t e1 = s.trace_end[i];
-  double acc = 0.0;
-  for (int64_t e = s.indptr[i]; e < e1; e += 16) {
-    double v[16];
-    int c[16];
-#pragma unroll
-    for (int u = 0; u < 16; ++u) {
-      const bool ok = e + u < e1;
-      v[u] = ok ? s.values[e + u] : 0.0;
-      c[u] = ok ? s.indices[e + u] : (int)R.w0;
-    }
-#pragma unroll
-    for (int u = 0; u < 16; ++u) acc = fma(v[u], R.win[c[u] - R.w0], acc);
-  }
-  return acc;
-}
-
-// Dot products by 8-lane groups: out o = sum over lanes of partial(o, lane).  Every
-// lane of the block runs the same number of rounds, so the shuffles never diverge.
+// Sums over 8-lane groups: out o = sum over lanes of partial(o, lane); every lane
+// of the block runs the same number of rounds, so the shuffles never diverge.
 template <typename F, typename G>
 __device__ __forceinline__ void group8(int nout, F partial, G store) {
   const int lane8 = threadIdx.x & 7, grp = threadIdx.x >> 3, ngrp = blockDim.x >> 3;
@@ -235,150 +271,287 @@ __device__ __forceinline__ void group8(int nout, F partial, G store) {
   }
 }
 
-// U[r][:] = v_row Qx  (v_row in R.col, nx values; Qx symmetric).  U is one of two
-// buffers: a phase that reads one may write the other before the next barrier.
-__device__ void coarse_rowfwd(const Sys& s, double* U, const Row& R) {
-  __syncthreads();
-  group8(
-      s.nx,
-      [&](int k, int l) {
-        double acc = 0.0;
-#pragma unroll 8
-        for (int ix = l; ix < s.nx; ix += 8) acc = fma(R.col[ix], R.qx[k * s.nx + ix], acc);
-        return acc;
-      },
-      [&](int k, double v) { U[(size_t)R.r * s.nx + k] = v; });
+// Orthonormal sine transform Q[k][i] = sine[(k+1)(i+1) mod 2(n+1)] (symmetric):
+// sum_{k = l, l+8, ...} a[k] Q[k][i].
+__device__ __forceinline__ double sine_dot(const double* a, const double* sine, int n, int i, int l) {
+  const int period = 2 * (n + 1);
+  int m = ((l + 1) * (i + 1)) % period;
+  const int step = (8 * (i + 1)) % period;
+  double acc = 0.0;
+  for (int k = l; k < n; k += 8) {
+    acc = fma(a[k], sine[m], acc);
+    m += step;
+    if (m >= period) m -= period;
+  }
+  return acc;
 }
 
-// After every row's U is written: W rows r-1+j (j in [j0, j1)) = T_k^-1 U[:, k]
-// restricted to those rows, then Y rows = W rows Qx.  Inverse entry (i, j) of mode k
-// (i <= j): U_i U_{ny-1-j} / (ay U_ny), U the Chebyshev table of the mode.
-__device__ void coarse_rows(const Sys& s, const double* U, const Row& R, int j0, int j1) {
+// Row transform of nrow column vectors (R.col + src[j] * nx) into dst[j] + r' * nx,
+// r' = R.r + shift[j] (null dst: skipped).
+__device__ void coarse_rowfwd(const Sys& s, const Row& R, int nrow, const int* src, double* const* dst,
+                              const int* shift) {
   __syncthreads();
+  const int nx = s.nx;
+  group8(
+      nrow * nx,
+      [&](int o, int l) {
+        const int j = o / nx, k = o - j * nx;
+        return dst[j] ? sine_dot(R.col + src[j] * nx, R.sine, nx, k, l) : 0.0;
+      },
+      [&](int o, double v) {
+        const int j = o / nx, k = o - j * nx;
+        if (dst[j]) dst[j][(size_t)(R.r + shift[j]) * nx + k] = v;
+      });
+}
+
+__device__ void coarse_rowfwd1(const Sys& s, const Row& R, double* dst) {
+  const int src[1] = {0};
+  double* const d[1] = {dst};
+  const int sh[1] = {0};
+  coarse_rowfwd(s, R, 1, src, d, sh);
+}
+
+// After every row's coarse data is written: coarse solution rows [lo, hi) (clipped
+// to the grid, within r-1 .. r+1) into yrow; other slots zero.  Per sine mode k,
+// W[ir][k] = sum_iy Tinv_k[ir][iy] U[iy][k] with Tinv_k[i][j] = U_i U_{ny-1-j} /
+// (ay U_ny) for i <= j (U the mode's Chebyshev table; symmetric), then Y rows =
+// W rows Q.
+__device__ void coarse_rows(const Sys& s, const Coarse& U, const Row& R, int lo, int hi) {
   const int ny = s.ny, nx = s.nx;
-  for (int base = threadIdx.x; base < nx * ny; base += 8 * blockDim.x) {
-    double v[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int idx = base + u * blockDim.x;
-      v[u] = idx < nx * ny ? __ldcg(U + idx) : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int idx = base + u * blockDim.x;
-      if (idx < nx * ny) {
-        const int iy = idx / nx, k = idx - iy * nx;
-        R.ust[k * (ny + 1) + iy] = v[u];
-      }
-    }
-  }
+  if (lo < 0) lo = 0;
+  if (hi > ny) hi = ny;
+  const int r0 = R.r - 1;
   __syncthreads();
   {
     const int lane8 = threadIdx.x & 7, grp = threadIdx.x >> 3, ngrp = blockDim.x >> 3;
     for (int base = 0; base < nx; base += ngrp) {
       const int k = base + grp;
-      double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+      double a[3] = {0.0, 0.0, 0.0};
       if (k < nx) {
         const double* u = R.cheb + (size_t)k * (ny + 1);
-        const double* uc = R.ust + (size_t)k * (ny + 1);
-        const int r0 = R.r - 1;
-#pragma unroll 4
-        for (int iy = lane8; iy < ny; iy += 8) {
-          const double v = uc[iy];
-          const double ulo = u[iy], uhi = u[ny - 1 - iy];
-          // row ir = r0 + j, column iy: U_min U_{ny-1-max}
-          if (r0 >= 0) a0 = fma((r0 < iy ? u[r0] * uhi : ulo * u[ny - 1 - r0]), v, a0);
-          if (r0 + 1 < ny) a1 = fma((r0 + 1 < iy ? u[r0 + 1] * uhi : ulo * u[ny - 2 - r0]), v, a1);
-          if (r0 + 2 < ny) a2 = fma((r0 + 2 < iy ? u[r0 + 2] * uhi : ulo * u[ny - 3 - r0]), v, a2);
+        double uir[3], unir[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const int ir = r0 + j;
+          const bool on = ir >= lo && ir < hi;
+          uir[j] = on ? u[ir] : 0.0;
+          unir[j] = on ? u[ny - 1 - ir] : 0.0;
+        }
+        for (int iy0 = lane8; iy0 < ny; iy0 += 64) {
+          double v0[8], v1[8], v2[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int iy = iy0 + 8 * q;
+            const size_t at = (size_t)iy * nx + k;
+            v0[q] = iy < ny ? __ldcg(U.self + at) : 0.0;
+            v1[q] = (iy < ny && iy > 0 && U.below) ? __ldcg(U.below + at) : 0.0;
+            v2[q] = (iy < ny - 1 && U.above) ? __ldcg(U.above + at) : 0.0;
+          }
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int iy = iy0 + 8 * q;
+            if (iy < ny) {
+              const double v = (v0[q] + v1[q]) + v2[q];
+              const double ulo = u[iy], uhi = u[ny - 1 - iy];
+#pragma unroll
+              for (int j = 0; j < 3; ++j) a[j] = fma((r0 + j < iy ? uir[j] * uhi : ulo * unir[j]), v, a[j]);
+            }
+          }
         }
       }
-      for (int o = 4; o > 0; o >>= 1) {
-        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        a[j] += __shfl_xor_sync(0xffffffffu, a[j], 4);
+        a[j] += __shfl_xor_sync(0xffffffffu, a[j], 2);
+        a[j] += __shfl_xor_sync(0xffffffffu, a[j], 1);
       }
       if (k < nx && lane8 == 0) {
         const double c = R.cinv[k];
-        R.wrow[k] = (j0 <= 0 && j1 > 0) ? a0 * c : 0.0;
-        R.wrow[nx + k] = (j0 <= 1 && j1 > 1) ? a1 * c : 0.0;
-        R.wrow[2 * nx + k] = (j0 <= 2 && j1 > 2) ? a2 * c : 0.0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) R.wrow[j * nx + k] = a[j] * c;
       }
     }
   }
   __syncthreads();
-  group8(
-      3 * nx,
-      [&](int o, int l) {
-        const int j = o / nx, ix = o - j * nx;
-        double acc = 0.0;
-#pragma unroll 8
-        for (int k = l; k < nx; k += 8) acc = fma(R.wrow[j * nx + k], R.qx[ix * nx + k], acc);
-        return acc;
-      },
-      [&](int o, double v) { R.yrow[o] = v; });
+  const int j0 = lo - r0 > 0 ? lo - r0 : 0, j1 = hi - r0 < 3 ? hi - r0 : 3;
+  for (int idx = threadIdx.x; idx < 3 * nx; idx += blockDim.x) {
+    const int j = idx / nx;
+    if (j < j0 || j >= j1) R.yrow[idx] = 0.0;
+  }
+  if (j1 > j0) {
+    group8(
+        (j1 - j0) * nx,
+        [&](int o, int l) {
+          const int j = j0 + o / nx, ix = o % nx;
+          return sine_dot(R.wrow + j * nx, R.sine, nx, ix, l);
+        },
+        [&](int o, double v) { R.yrow[j0 * nx + o] = v; });
+  }
   __syncthreads();
 }
 
-// R.col[cx] = sum_a g0[c,a] v[cl] over the row's cells (v over the G range, shared memory).
-__device__ void row_g0t(const Sys& s, const Row& R, const double* v) {
-  __syncthreads();
-  group8(
-      s.nx,
-      [&](int cx, int l) {
-        double acc = 0.0;
-        for (int a = l; a < s.t; a += 8) acc = fma(R.cg[cx * s.t + a], v[R.cl[cx * s.t + a]], acc);
-        return acc;
-      },
-      [&](int cx, double v2) { R.col[cx] = v2; });
+__device__ void coarse_rows1(const Sys& s, const double* U, const Row& R, int lo, int hi) {
+  const Coarse c{const_cast<double*>(U), nullptr, nullptr};
+  coarse_rows(s, c, R, lo, hi);
 }
 
-// Projected residual rho = rhoP - G0 Y and zt = Minv rho on the face whose first DOF is
-// at G-range position l0; rhoP is staged over the G range in shared memory.
-template <int FS>
-__device__ __forceinline__ void face_precondition(const Row& R, int l0, const double* rhoP_win,
-                                                  double (&rho_out)[FS], double (&z_out)[FS]) {
-#pragma unroll
-  for (int r = 0; r < FS; ++r) rho_out[r] = rhoP_win[l0 + r] - g0y(R, l0 + r);
-  const double* m = R.minv + (l0 / FS) * FS * FS;
-#pragma unroll
-  for (int r = 0; r < FS; ++r) {
+// Per-cell products cpart[cx][a] = sum_b B_c[a][b] v[cl[cx][b]] (B packed symmetric);
+// returns this thread's sum of v[cl] * cpart (for (u, S u)).
+__device__ double cell_matvec(const Sys& s, const Row& R, const double* B, const double* v) {
+  __syncthreads();
+  const int t = s.t, np = t * (t + 1) / 2;
+  double dot = 0.0;
+  for (int idx = threadIdx.x; idx < s.nx * t; idx += blockDim.x) {
+    const int cx = idx / t, a = idx - cx * t;
+    const double* blk = B + (size_t)cx * np;
+    const int16_t* c = R.cl + cx * t;
+    const uint8_t* pi = R.pidx + a * t;
     double acc = 0.0;
-#pragma unroll
-    for (int c = 0; c < FS; ++c) acc = fma(m[r * FS + c], rho_out[c], acc);
-    z_out[r] = acc;
+    for (int b = 0; b < t; ++b) acc = fma(blk[pi[b]], v[c[b]], acc);
+    R.cpart[idx] = acc;
+    dot = fma(v[c[a]], acc, dot);
+  }
+  return dot;
+}
+
+// Partials of the row's cells to the per-DOF exchange arrays (first / second cell).
+__device__ void write_exchange(const Row& R, int nslot, double* Xf, double* Xs) {
+  for (int idx = threadIdx.x; idx < nslot; idx += blockDim.x) {
+    const int64_t i = R.gdof[R.cl[idx]];
+    ((R.role[idx] & 1) ? Xs : Xf)[i] = R.cpart[idx];
   }
 }
 
-__host__ __device__ size_t smem_layout(const mhm_skeleton_system* s, size_t* off) {
-  // bounds: a row owns at most (3 nx + 1) faces (row 0), later rows 2 nx + 1
-  const int fs = s->face_size;
-  const size_t own0 = (size_t)(3 * s->nx + 1) * fs, own = (size_t)(2 * s->nx + 1) * fs;
-  const size_t own_max = own0 > own ? own0 : own;
-  const size_t g = own_max + own;              // rows r-1 and r
-  const size_t wmax = own_max + 2 * own_max;   // rows r-1..r+1
-  const size_t m = s->nx > s->ny ? s->nx : s->ny;
-  const size_t win = wmax > 3 * (size_t)s->nx ? wmax : 3 * (size_t)s->nx;
+// out[l] = Xf + Xs over the G DOFs (four loads of each array in flight per thread).
+__device__ void read_exchange(const Row& R, const double* Xf, const double* Xs, double* out) {
+  for (int base = threadIdx.x; base < R.ng; base += 4 * blockDim.x) {
+    double a[4], b[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int l = base + q * blockDim.x;
+      const int64_t i = l < R.ng ? R.gdof[l] : 0;
+      a[q] = l < R.ng ? __ldcg(Xf + i) : 0.0;
+      b[q] = l < R.ng ? __ldcg(Xs + i) : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int l = base + q * blockDim.x;
+      if (l < R.ng) out[l] = a[q] + b[q];
+    }
+  }
+}
+
+// Coarse data of sum_c cpart_c (minus G0^T of the G vector `minus`, if given) for
+// this row and, through the shared faces, for rows r+1 and r-1.
+__device__ void partial_coarse(const Sys& s, const Row& R, const Coarse& U, const double* minus) {
+  const int nx = s.nx, t = s.t, fs = s.fs;
+  __syncthreads();
+  // col[0..5nx): per cell the self sum and the sums across bottom, right, top, left
+  for (int idx = threadIdx.x; idx < 5 * nx; idx += blockDim.x) {
+    const int kind = idx / nx, cx = idx - kind * nx;
+    const double* p = R.cpart + cx * t;
+    double acc = 0.0;
+    if (kind == 0) {
+      const double* g = R.gself + cx * t;
+      for (int a = 0; a < t; ++a) acc = fma(g[a], p[a], acc);
+      if (minus) {
+        double m = 0.0;
+        for (int a = 0; a < t; ++a) m = fma(g[a], minus[R.cl[cx * t + a]], m);
+        acc -= m;
+      }
+    } else {
+      const int a0 = (kind - 1) * fs;
+      const double* g = R.gnb + cx * t;
+      for (int j = 0; j < fs; ++j) acc = fma(g[a0 + j], p[a0 + j], acc);
+    }
+    R.col[idx] = acc;
+  }
+  __syncthreads();
+  for (int cx = threadIdx.x; cx < nx; cx += blockDim.x) {
+    const double from_left = cx > 0 ? R.col[2 * nx + cx - 1] : 0.0;       // right side of cx-1
+    const double from_right = cx + 1 < nx ? R.col[4 * nx + cx + 1] : 0.0;  // left side of cx+1
+    R.col[5 * nx + cx] = (R.col[cx] + from_left) + from_right;
+    R.col[6 * nx + cx] = R.col[3 * nx + cx];  // to row r+1 (top)
+    R.col[7 * nx + cx] = R.col[nx + cx];      // to row r-1 (bottom)
+  }
+  const int src[3] = {5, 6, 7};
+  double* const dst[3] = {U.self, R.r + 1 < s.ny ? U.below : nullptr, R.r > 0 ? U.above : nullptr};
+  const int shift[3] = {0, 1, -1};
+  coarse_rowfwd(s, R, 3, src, dst, shift);
+}
+
+// col[j nx + cx] = sum_a g0[c][a] v_j[cl] over the row's cells, for up to two vectors.
+__device__ void dof_coarse(const Sys& s, const Row& R, const double* v0, const double* v1) {
+  __syncthreads();
+  const int nx = s.nx, t = s.t, n = v1 ? 2 : 1;
+  for (int idx = threadIdx.x; idx < n * nx; idx += blockDim.x) {
+    const int j = idx / nx, cx = idx - j * nx;
+    const double* v = j ? v1 : v0;
+    double acc = 0.0;
+    for (int a = 0; a < t; ++a) acc = fma(R.gself[cx * t + a], v[R.cl[cx * t + a]], acc);
+    R.col[idx] = acc;
+  }
+}
+
+// In-place Gauss-Jordan inverse of the t x t matrix a (symmetric positive definite,
+// no pivoting) by one warp.
+__device__ void warp_invert(double* a, int t) {
+  const int lane = threadIdx.x & 31;
+  for (int k = 0; k < t; ++k) {
+    __syncwarp();
+    const double d = 1.0 / a[k * t + k];
+    __syncwarp();
+    for (int j = lane; j < t; j += 32)
+      if (j != k) a[k * t + j] *= d;
+    __syncwarp();
+    for (int e = lane; e < t * t; e += 32) {
+      const int i = e / t, j = e - i * t;
+      if (i != k && j != k) a[e] = fma(-a[i * t + k], a[k * t + j], a[e]);
+    }
+    __syncwarp();
+    for (int i = lane; i < t; i += 32)
+      if (i != k) a[i * t + k] = -a[i * t + k] * d;
+    __syncwarp();
+    if (lane == 0) a[k * t + k] = d;
+  }
+  __syncwarp();
+}
+
+constexpr int kSmemArrays = 23;
+
+__host__ __device__ size_t smem_layout(int nx, int ny, int fs, int t, size_t* off) {
+  // a row owns at most 3 nx + 1 faces (row 0); later rows own 2 nx + 1 and add the
+  // nx bottom faces of their cells
+  const size_t g = (size_t)(3 * nx + 1) * fs;
+  const size_t np = (size_t)t * (t + 1) / 2;
+  const size_t vec = 6 * g > (size_t)kWarps * t * t ? 6 * g : (size_t)kWarps * t * t;
   size_t o = 0;
-  auto take = [&](int k, size_t bytes) {
-    off[k] = o;
+  int k = 0;
+  auto take = [&](size_t bytes) {
+    off[k++] = o;
     o = align16(o + bytes);
   };
-  take(0, (size_t)s->nx * s->nx * 8);           // qx
-  take(1, 3 * (size_t)s->nx * 8);               // yrow
-  take(2, m * 8);                               // col
-  take(3, win * 8);                             // win
-  take(4, g * 8);                               // ga
-  take(5, g * 8);                               // gb
-  take(6, g * 2);                               // ya
-  take(7, g * 2);                               // yb
-  take(8, (g / fs + 1) * fs * fs * 8);          // minv
-  take(9, (size_t)s->nx * s->cell_width * 2);   // cl
-  take(10, (size_t)s->nx * s->cell_width * 8);  // cg
-  take(11, (size_t)s->nx * (s->ny + 1) * 8);    // cheb
-  take(12, 3 * (size_t)s->nx * 8);              // wrow
-  take(13, (size_t)s->nx * 8);                  // cinv
-  take(14, (size_t)s->nx * (s->ny + 1) * 8);    // ust (transposed, padded)
-  off[15] = o;
+  take(2 * ((size_t)nx + 1) * 8);   // 0 sine
+  take(3 * (size_t)nx * 8);         // 1 yrow
+  take(8 * (size_t)nx * 8);         // 2 col
+  take(3 * (size_t)nx * 8);         // 3 wrow
+  take((size_t)nx * 8);             // 4 cinv
+  take((size_t)nx * (ny + 1) * 8);  // 5 cheb
+  take(vec * 8);                    // 6 G vectors (6 g) / setup scratch
+  take((size_t)nx * t * 8);         // 7 cpart
+  take((size_t)nx * np * 8);        // 8 Sb
+  take((size_t)nx * np * 8);        // 9 Pb
+  take(g * 8);                      // 10 ga
+  take(g * 8);                      // 11 gb
+  take(g * 2);                      // 12 ya
+  take(g * 2);                      // 13 yb
+  take(g * 4);                      // 14 gdof
+  take((size_t)nx * t * 2);         // 15 cl
+  take((size_t)nx * t * 8);         // 16 gself
+  take((size_t)nx * t * 8);         // 17 gnb
+  take((size_t)nx * t);             // 18 role
+  take((size_t)t * t);              // 19 pidx
+  off[k] = o;
   return o;
 }
 
@@ -386,12 +559,13 @@ template <int FS>
 __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Params P) {
   const Sys& s = P.s;
   const Work& w = P.w;
-  __shared__ double red[32];
-  __shared__ double sh[2];
-  __shared__ size_t off[16];
+  __shared__ double red[64];
+  __shared__ double sh[4];
+  __shared__ size_t off[kSmemArrays + 1];
   extern __shared__ __align__(16) unsigned char dyn[];
-  constexpr int fs = FS;
   const int tid = threadIdx.x, nth = blockDim.x;
+  const int nx = s.nx, ny = s.ny, t = s.t;
+  const int np = t * (t + 1) / 2;
   unsigned epoch = 0;
   int status = MHM_SOLVE_OK;
   int total_inner = 0, outer = 0;
@@ -401,29 +575,35 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
   do {                 \
     if (!grid_sync(w, epoch)) { status = MHM_SOLVE_BARRIER_TIMEOUT; goto done; } \
   } while (0)
-  if (tid == 0) {
-    mhm_skeleton_system tmp{};
-    tmp.nx = s.nx; tmp.ny = s.ny; tmp.face_size = s.fs; tmp.cell_width = s.t;
-    smem_layout(&tmp, off);
-  }
+  if (tid == 0) smem_layout(nx, ny, FS, t, off);
   __syncthreads();
   R.r = blockIdx.x;
-  R.c0 = R.r * s.nx;
-  R.qx = reinterpret_cast<double*>(dyn + off[0]);
+  R.c0 = R.r * nx;
+  R.sine = reinterpret_cast<double*>(dyn + off[0]);
   R.yrow = reinterpret_cast<double*>(dyn + off[1]);
   R.col = reinterpret_cast<double*>(dyn + off[2]);
-  R.win = reinterpret_cast<double*>(dyn + off[3]);
-  R.ga = reinterpret_cast<double*>(dyn + off[4]);
-  R.gb = reinterpret_cast<double*>(dyn + off[5]);
-  R.ya = reinterpret_cast<int16_t*>(dyn + off[6]);
-  R.yb = reinterpret_cast<int16_t*>(dyn + off[7]);
-  R.minv = reinterpret_cast<double*>(dyn + off[8]);
-  R.cl = reinterpret_cast<int16_t*>(dyn + off[9]);
-  R.cg = reinterpret_cast<double*>(dyn + off[10]);
-  R.cheb = reinterpret_cast<double*>(dyn + off[11]);
-  R.wrow = reinterpret_cast<double*>(dyn + off[12]);
-  R.cinv = reinterpret_cast<double*>(dyn + off[13]);
-  R.ust = reinterpret_cast<double*>(dyn + off[14]);
+  R.wrow = reinterpret_cast<double*>(dyn + off[3]);
+  R.cinv = reinterpret_cast<double*>(dyn + off[4]);
+  R.cheb = reinterpret_cast<double*>(dyn + off[5]);
+  {
+    double* v = reinterpret_cast<double*>(dyn + off[6]);
+    const int g = (3 * nx + 1) * FS;
+    R.vr = v; R.vps = v + g; R.vp = v + 2 * g; R.vlam = v + 3 * g; R.vu = v + 4 * g; R.vt = v + 5 * g;
+    R.scratch = v;
+  }
+  R.cpart = reinterpret_cast<double*>(dyn + off[7]);
+  R.Sb = reinterpret_cast<double*>(dyn + off[8]);
+  R.Pb = reinterpret_cast<double*>(dyn + off[9]);
+  R.ga = reinterpret_cast<double*>(dyn + off[10]);
+  R.gb = reinterpret_cast<double*>(dyn + off[11]);
+  R.ya = reinterpret_cast<int16_t*>(dyn + off[12]);
+  R.yb = reinterpret_cast<int16_t*>(dyn + off[13]);
+  R.gdof = reinterpret_cast<int32_t*>(dyn + off[14]);
+  R.cl = reinterpret_cast<int16_t*>(dyn + off[15]);
+  R.gself = reinterpret_cast<double*>(dyn + off[16]);
+  R.gnb = reinterpret_cast<double*>(dyn + off[17]);
+  R.role = reinterpret_cast<uint8_t*>(dyn + off[18]);
+  R.pidx = reinterpret_cast<uint8_t*>(dyn + off[19]);
   {
     // DOFs are numbered by their first cell: binary search the row boundaries
     auto lower = [&](int cell) {
@@ -435,81 +615,135 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       return lo;
     };
     R.d0 = lower(R.c0);
-    R.d1 = lower(R.c0 + s.nx);
-    R.gs = R.r > 0 ? lower(R.c0 - s.nx) : R.d0;
-    R.w0 = R.gs;
-    R.w1 = R.r + 1 < s.ny ? lower(R.c0 + 2 * s.nx) : R.d1;
+    R.d1 = lower(R.c0 + nx);
+    R.nown = (int)(R.d1 - R.d0);
+    R.ng = R.nown + (R.r > 0 ? nx * FS : 0);
   }
-  for (int idx = tid; idx < s.nx * s.nx; idx += nth) R.qx[idx] = s.qx[idx];
-  // G-range coefficients: (G0 Y)_i = ga Y(first cell) + gb Y(second cell)
-  for (int64_t l = tid; l < R.d1 - R.gs; l += nth) {
-    const int64_t i = R.gs + l;
+  for (int m = tid; m < 2 * (nx + 1); m += nth)
+    R.sine[m] = sqrt(2.0 / (nx + 1)) * sinpi((double)m / (double)(nx + 1));
+  for (int e = tid; e < t * t; e += nth) {
+    const int a = e / t, b = e - a * t;
+    const int i = a < b ? a : b, j = a < b ? b : a;
+    R.pidx[e] = (uint8_t)(i * t - i * (i - 1) / 2 + (j - i));
+  }
+  // G DOFs
+  for (int l = tid; l < R.ng; l += nth) {
+    int64_t i;
+    if (l < R.nown) {
+      i = R.d0 + l;
+    } else {
+      const int q = l - R.nown, cx = q / FS, j = q - cx * FS;
+      i = s.cell_dofs[(size_t)(R.c0 + cx) * t + j];  // bottom side: slots 0 .. fs-1
+    }
+    R.gdof[l] = (int32_t)i;
     for (int k = 0; k < 2; ++k) {
       const int c = s.dof_cells[2 * i + k];
       double g = 0.0;
       int y = -1;
       if (c >= 0) {
-        g = s.g0[(size_t)c * s.t + s.dof_slot[2 * i + k]];
-        const int cy = c / s.nx;
-        y = (cy - R.r + 1) * s.nx + (c - cy * s.nx);
+        g = s.g0[(size_t)c * t + s.dof_slot[2 * i + k]];
+        const int cy = c / nx;
+        y = (cy - R.r + 1) * nx + (c - cy * nx);
       }
       if (k == 0) { R.ga[l] = g; R.ya[l] = (int16_t)(y < 0 ? 0 : y); }
       else { R.gb[l] = g; R.yb[l] = (int16_t)y; }
     }
   }
-  // own cells: G-range position and G0 coefficient of each cell DOF
-  for (int idx = tid; idx < s.nx * s.t; idx += nth) {
-    const int cx = idx / s.t, a = idx - cx * s.t;
+  // the row's cells: local DOF, role and G0 coefficients of each slot
+  for (int idx = tid; idx < nx * t; idx += nth) {
+    const int cx = idx / t, a = idx - cx * t;
     const int c = R.c0 + cx;
-    R.cl[idx] = (int16_t)(s.cell_dofs[(size_t)c * s.t + a] - R.gs);
-    R.cg[idx] = s.g0[(size_t)c * s.t + a];
+    const int64_t i = s.cell_dofs[(size_t)c * t + a];
+    R.cl[idx] = (int16_t)(i >= R.d0 && i < R.d1 ? i - R.d0 : R.nown + cx * FS + a);
+    const int first = s.dof_cells[2 * i];
+    const bool second = first != c;
+    R.role[idx] = (uint8_t)((second ? 1 : 0) | (s.dof_cells[2 * i + 1] >= 0 ? 2 : 0));
+    R.gself[idx] = s.g0[(size_t)c * t + a];
+    const int other = second ? first : s.dof_cells[2 * i + 1];
+    const int oslot = second ? s.dof_slot[2 * i] : s.dof_slot[2 * i + 1];
+    R.gnb[idx] = other >= 0 ? s.g0[(size_t)other * t + oslot] : 0.0;
+  }
+  // DOFs met by one cell only: their second-cell partials stay zero
+  for (int64_t i = R.d0 + tid; i < R.d1; i += nth)
+    if (s.dof_cells[2 * i + 1] < 0) {
+      w.Zs[i] = 0.0;
+      w.Vs[i] = 0.0;
+    }
+  __syncthreads();
+  // packed symmetric S_c (operator) of the row's cells
+  for (int idx = tid; idx < nx * t * t; idx += nth) {
+    const int cx = idx / (t * t), e = idx - cx * t * t, a = e / t, b = e - a * t;
+    if (a > b) continue;
+    const int c = R.c0 + cx;
+    double v;
+    if (s.blocks) {
+      const double* B = s.blocks + (size_t)c * s.ld * s.ld;
+      v = 0.5 * (B[a * s.ld + b] + B[b * s.ld + a]);
+    } else {
+      const int64_t ia = s.cell_dofs[(size_t)c * t + a], ib = s.cell_dofs[(size_t)c * t + b];
+      v = 0.5 * (csr_entry(s, ia, ib) + csr_entry(s, ib, ia));
+      // an entry between two DOFs of a face shared with another cell is split evenly
+      if (a / FS == b / FS && (R.role[cx * t + a] & 2)) v *= 0.5;
+    }
+    R.Sb[(size_t)cx * np + R.pidx[e]] = v;
+  }
+  __syncthreads();
+  // preconditioner blocks: D B^-1 D, B = S_c (cell blocks) or the assembled principal
+  // submatrix (D = 1); one warp inverts one cell's block in the setup scratch
+  {
+    const int warp = tid >> 5, lane = tid & 31;
+    double* a = R.scratch + (size_t)warp * t * t;
+    for (int cx = warp; cx < nx; cx += kWarps) {
+      const int c = R.c0 + cx;
+      for (int e = lane; e < t * t; e += 32) {
+        const int i = e / t, j = e - i * t;
+        double v;
+        if (s.blocks) {
+          v = R.Sb[(size_t)cx * np + R.pidx[e]];
+        } else {
+          const int64_t ia = s.cell_dofs[(size_t)c * t + i], ib = s.cell_dofs[(size_t)c * t + j];
+          v = 0.5 * (csr_entry(s, ia, ib) + csr_entry(s, ib, ia));
+        }
+        a[e] = v;
+      }
+      warp_invert(a, t);
+      for (int e = lane; e < t * t; e += 32) {
+        const int i = e / t, j = e - i * t;
+        if (i > j) continue;
+        double di = 1.0, dj = 1.0;
+        if (s.blocks) {
+          auto weight = [&](int slot) {
+            const int64_t dof = s.cell_dofs[(size_t)c * t + slot];
+            const int c1 = s.dof_cells[2 * dof], c2 = s.dof_cells[2 * dof + 1];
+            const double d1 = s.blocks[(size_t)c1 * s.ld * s.ld + (size_t)s.dof_slot[2 * dof] * (s.ld + 1)];
+            const double d2 =
+                c2 >= 0 ? s.blocks[(size_t)c2 * s.ld * s.ld + (size_t)s.dof_slot[2 * dof + 1] * (s.ld + 1)] : 0.0;
+            return s.blocks[(size_t)c * s.ld * s.ld + (size_t)slot * (s.ld + 1)] / (d1 + d2);
+          };
+          di = weight(i);
+          dj = weight(j);
+        }
+        R.Pb[(size_t)cx * np + R.pidx[e]] = di * (0.5 * (a[i * t + j] + a[j * t + i])) * dj;
+      }
+      __syncwarp();
+    }
   }
   // Chebyshev table of mode k: T_k = ay tridiag(-1, 2 theta_k, -1), theta_k =
-  // 1 + ax lam_k / (2 ay); U_m(theta_k), m = 0..ny.  Row CTA k owns mode k.
+  // 1 + ax lam_k / (2 ay); U_m(theta_k), m = 0..ny.
   if (tid == 0) {
-    for (int k = blockIdx.x; k < s.nx; k += gridDim.x) {
-      double* u = w.cheb + (size_t)k * (s.ny + 1);
-      const double lam = 2.0 - 2.0 * cos(M_PI * (k + 1) / (s.nx + 1));
+    for (int k = blockIdx.x; k < nx; k += gridDim.x) {
+      double* u = w.cheb + (size_t)k * (ny + 1);
+      const double lam = 2.0 - 2.0 * cospi((double)(k + 1) / (double)(nx + 1));
       const double two_theta = 2.0 + s.ax * lam / s.ay;
       double um1 = 0.0, u0 = 1.0;
       u[0] = 1.0;
-      for (int m = 1; m <= s.ny; ++m) {
+      for (int m = 1; m <= ny; ++m) {
         const double un = two_theta * u0 - um1;
         u[m] = un;
         um1 = u0;
         u0 = un;
       }
     }
-  }
-  // face-block Jacobi inverses of the G range (Gauss-Jordan, partial pivoting)
-  for (int64_t fl = tid; fl < (R.d1 - R.gs) / fs; fl += nth) {
-    const int64_t f = R.gs / fs + fl;
-    double a[FS][2 * FS];
-    for (int r = 0; r < fs; ++r) {
-      const int64_t row = f * fs + r;
-      for (int c = 0; c < 2 * fs; ++c) a[r][c] = (c - fs == r) ? 1.0 : 0.0;
-      for (int64_t e = s.indptr[row]; e < s.trace_end[row]; ++e) {
-        const int64_t cidx = s.indices[e];
-        if (cidx >= f * fs && cidx < (f + 1) * fs) a[r][cidx - f * fs] = s.values[e];
-      }
-    }
-    for (int k = 0; k < fs; ++k) {
-      int piv = k;
-      for (int r = k + 1; r < fs; ++r)
-        if (fabs(a[r][k]) > fabs(a[piv][k])) piv = r;
-      if (piv != k)
-        for (int c = 0; c < 2 * fs; ++c) { const double tmp = a[k][c]; a[k][c] = a[piv][c]; a[piv][c] = tmp; }
-      const double d = a[k][k];
-      const double inv = (d != 0.0) ? 1.0 / d : 0.0;
-      for (int c = 0; c < 2 * fs; ++c) a[k][c] *= inv;
-      for (int r = 0; r < fs; ++r) {
-        if (r == k) continue;
-        const double m = a[r][k];
-        for (int c = 0; c < 2 * fs; ++c) a[r][c] = fma(-m, a[k][c], a[r][c]);
-      }
-    }
-    for (int r = 0; r < fs; ++r)
-      for (int c = 0; c < fs; ++c) R.minv[fl * fs * fs + r * fs + c] = a[r][fs + c];
   }
   // x = 0, r_full = rhs on owned rows; ||rhs||
   {
@@ -520,7 +754,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       w.rfull[i] = v;
       b2 += v * v;
     }
-    for (int cx = tid; cx < s.nx; cx += nth) {
+    for (int cx = tid; cx < nx; cx += nth) {
       const int64_t i = s.T + R.c0 + cx;
       P.x[i] = 0.0;
       const double v = P.rhs[i];
@@ -531,9 +765,9 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
   }
   SYNC_OR_EXIT();
   // every mode's Chebyshev table (complete now) into shared memory
-  copy_l2(R.cheb, w.cheb, (int64_t)s.nx * (s.ny + 1));
+  for (int e = tid; e < nx * (ny + 1); e += nth) R.cheb[e] = __ldcg(w.cheb + e);
   __syncthreads();
-  for (int k = tid; k < s.nx; k += nth) R.cinv[k] = 1.0 / (s.ay * R.cheb[(size_t)k * (s.ny + 1) + s.ny]);
+  for (int k = tid; k < nx; k += nth) R.cinv[k] = 1.0 / (s.ay * R.cheb[(size_t)k * (ny + 1) + ny]);
   __syncthreads();
   bnorm = sqrt(grid_total(w, 0, sh));
   if (bnorm == 0.0) goto finish;
@@ -545,7 +779,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
         w.rfull[i] = v;
         r2 += v * v;
       }
-      for (int cx = tid; cx < s.nx; cx += nth) {
+      for (int cx = tid; cx < nx; cx += nth) {
         const int64_t i = s.T + R.c0 + cx;
         const double v = P.rhs[i] - krow(s, i, P.x);
         w.rfull[i] = v;
@@ -560,179 +794,123 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
     }
     {
       const double itol = (outer == 0) ? P.inner_rtol : fmax(P.inner_rtol, 1e-4);
-      // lambda0 = -G0 C^-1 r2
-      for (int cx = tid; cx < s.nx; cx += nth) R.col[cx] = w.rfull[s.T + R.c0 + cx];
-      coarse_rowfwd(s, w.U, R);
+      // coarse data of r2
+      for (int cx = tid; cx < nx; cx += nth) R.col[cx] = w.rfull[s.T + R.c0 + cx];
+      coarse_rowfwd1(s, R, w.Ux1);
       SYNC_OR_EXIT();
-      coarse_rows(s, w.U, R, 1, 3);
-      for (int64_t i = R.d0 + tid; i < R.d1; i += nth) w.lam[i] = -g0y(R, i - R.gs);
+      // lambda0 = -G0 (G0^T G0)^-1 r2 on G; cell partials of S lambda0; r1 on G
+      coarse_rows1(s, w.Ux1, R, R.r - 1, R.r + 2);
+      for (int l = tid; l < R.ng; l += nth) R.vlam[l] = -g0y(R, l);
+      for (int l = tid; l < R.ng; l += nth) R.vt[l] = __ldcg(w.rfull + R.gdof[l]);
+      cell_matvec(s, R, R.Sb, R.vlam);
+      __syncthreads();
+      write_exchange(R, nx * t, w.Vf, w.Vs);
       SYNC_OR_EXIT();
-      // rhoP = r1 - S lam
-      stage(R, w.lam);
-      for (int64_t i = R.d0 + tid; i < R.d1; i += nth) w.rhoP[i] = w.rfull[i] - srow_win(s, R, i);
+      // rhoP = r1 - S lambda0 on G; its coarse data
+      read_exchange(R, w.Vf, w.Vs, R.vu);
+      __syncthreads();
+      for (int l = tid; l < R.ng; l += nth) R.vr[l] = R.vt[l] - R.vu[l];
+      dof_coarse(s, R, R.vr, nullptr);
+      coarse_rowfwd1(s, R, w.Ux1);
       SYNC_OR_EXIT();
-      stage_g(R, w.rhoP);
-      row_g0t(s, R, R.win);
-      coarse_rowfwd(s, w.U, R);
-      SYNC_OR_EXIT();
-      coarse_rows(s, w.U, R, 0, 3);
-      stage_g(R, w.rhoP);
-      double r2 = 0.0;
-      for (int64_t f = R.d0 / fs + tid; f < R.d1 / fs; f += nth) {
-        double rl[FS], zl[FS];
-        face_precondition<FS>(R, (int)(f * fs - R.gs), R.win, rl, zl);
-        for (int r = 0; r < fs; ++r) {
-          w.rho[f * fs + r] = rl[r];
-          w.zt[f * fs + r] = zl[r];
-          r2 += rl[r] * rl[r];
-        }
-      }
-      put_partial(w, 1, r2, red);
-      SYNC_OR_EXIT();  // zt of neighbouring rows is needed below
-      const double r0 = sqrt(grid_total(w, 1, sh));
-      stage_g(R, w.zt);
-      row_g0t(s, R, R.win);
-      coarse_rowfwd(s, w.U, R);
-      SYNC_OR_EXIT();
-      coarse_rows(s, w.U, R, 1, 3);
+      // r0 = P rhoP; preconditioned partials and their coarse data; |r0|^2
+      coarse_rows1(s, w.Ux1, R, R.r - 1, R.r + 2);
+      for (int l = tid; l < R.ng; l += nth) R.vr[l] -= g0y(R, l);
       {
-        double rz = 0.0;
-        for (int64_t i = R.d0 + tid; i < R.d1; i += nth) {
-          const double zi = w.zt[i] - g0y(R, i - R.gs);
-          w.z[i] = zi;
-          w.p[i] = zi;
-          rz += w.rho[i] * zi;
-        }
-        put_partial(w, 2, rz, red);
+        double r2 = 0.0;
+        for (int l = tid; l < R.nown; l += nth) r2 = fma(R.vr[l], R.vr[l], r2);
+        cell_matvec(s, R, R.Pb, R.vr);
+        __syncthreads();
+        write_exchange(R, nx * t, w.Zf, w.Zs);
+        partial_coarse(s, R, w.Uz, nullptr);
+        put_partial(w, 0, r2, red);
       }
       SYNC_OR_EXIT();
-      double rz = grid_total(w, 2, sh);
-      {
-        stage(R, w.p);
-        double pq = 0.0;
-        for (int64_t i = R.d0 + tid; i < R.d1; i += nth) {
-          const double qi = srow_win(s, R, i);
-          w.q[i] = qi;
-          pq += R.win[i - R.w0] * qi;
-        }
-        put_partial(w, 3, pq, red);
-      }
-      SYNC_OR_EXIT();
+      double r0 = 0.0, gam_prev = 1.0, alpha_prev = 1.0;
       int k = 0;
-      if (r0 > 0.0) {
-        for (k = 0; k < P.max_inner; ++k) {
-          // A: step along p; coarse data of the updated residual
-          const double pq = grid_total(w, 3, sh);
-          if (!(pq > 0.0)) { status = MHM_SOLVE_BREAKDOWN; break; }
-          const double alpha = rz / pq;
-          for (int64_t i = R.d0 + tid; i < R.d1; i += nth) {
-            w.lam[i] = fma(alpha, w.p[i], w.lam[i]);
-            w.rhoP[i] = fma(-alpha, w.q[i], w.rho[i]);
-          }
-          __syncthreads();
-          {
-            const int64_t ng = R.d1 - R.gs;
-            for (int64_t base = tid; base < ng; base += 4 * (int64_t)nth) {
-              double qv[4], rv[4];
-#pragma unroll
-              for (int u = 0; u < 4; ++u) {
-                const int64_t k2 = base + (int64_t)u * nth;
-                qv[u] = k2 < ng ? __ldcg(w.q + R.gs + k2) : 0.0;
-                rv[u] = k2 < ng ? __ldcg(w.rho + R.gs + k2) : 0.0;
-              }
-#pragma unroll
-              for (int u = 0; u < 4; ++u) {
-                const int64_t k2 = base + (int64_t)u * nth;
-                if (k2 < ng) R.win[k2] = fma(-alpha, qv[u], rv[u]);
-              }
-            }
-          }
-          row_g0t(s, R, R.win);
-          coarse_rowfwd(s, w.U, R);
-          SYNC_OR_EXIT();
-          // B: W and Y rows of the projection; project and precondition the owned faces;
-          //    coarse data of G0^T Minv rho
-          coarse_rows(s, w.U, R, 0, 3);
-          stage_g(R, w.rhoP);
-          double r2b = 0.0;
-          for (int64_t f = R.d0 / fs + tid; f < R.d1 / fs; f += nth) {
-            double rl[FS], zl[FS];
-            face_precondition<FS>(R, (int)(f * fs - R.gs), R.win, rl, zl);
-            for (int r = 0; r < fs; ++r) {
-              w.rho[f * fs + r] = rl[r];
-              w.zt[f * fs + r] = zl[r];
-              r2b += rl[r] * rl[r];
-            }
-          }
-          // four threads per cell, one per side, reduced over 4-lane groups
-          for (int base = 0; base < 4 * s.nx; base += nth) {
-            const int idx = base + tid;
-            const int cx = idx >> 2, side = idx & 3;
-            double acc = 0.0;
-            if (cx < s.nx) {
-              const int a = side * fs;
-              double rl[FS], zl[FS];
-              face_precondition<FS>(R, R.cl[cx * s.t + a], R.win, rl, zl);
-#pragma unroll
-              for (int r = 0; r < FS; ++r) acc = fma(R.cg[cx * s.t + a + r], zl[r], acc);
-            }
-            acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-            acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-            if (cx < s.nx && side == 0) R.col[cx] = acc;
-          }
-          coarse_rowfwd(s, w.U2, R);
-          put_partial(w, 1, r2b, red);
-          SYNC_OR_EXIT();
-          // C: convergence test; projected preconditioned residual
-          {
-            const double rn = sqrt(grid_total(w, 1, sh));
-            if (!isfinite(rn)) { status = MHM_SOLVE_NONFINITE; break; }
-            if (rn <= itol * r0) { ++k; break; }
-          }
-          coarse_rows(s, w.U2, R, 1, 3);
-          {
-            double rzn = 0.0;
-            for (int64_t i = R.d0 + tid; i < R.d1; i += nth) {
-              const double zi = w.zt[i] - g0y(R, i - R.gs);
-              w.z[i] = zi;
-              rzn += w.rho[i] * zi;
-            }
-            put_partial(w, 2, rzn, red);
-          }
-          SYNC_OR_EXIT();
-          // D: new direction, q = S p by recurrence
-          {
-            const double rzn = grid_total(w, 2, sh);
-            const double beta = rzn / rz;
-            rz = rzn;
-            stage(R, w.z);
-            double pq2 = 0.0;
-            for (int64_t i = R.d0 + tid; i < R.d1; i += nth) {
-              const double pi = fma(beta, w.p[i], R.win[i - R.w0]);
-              const double qi = fma(beta, w.q[i], srow_win(s, R, i));
-              w.p[i] = pi;
-              w.q[i] = qi;
-              pq2 += pi * qi;
-            }
-            put_partial(w, 3, pq2, red);
-          }
-          SYNC_OR_EXIT();
+      for (;; ++k) {
+        // (1) u = P M^-1 r and w = S u (cell partials) on G; gamma, delta
+        const double rn = sqrt(grid_total(w, 0, sh));
+        if (!isfinite(rn)) { status = MHM_SOLVE_NONFINITE; break; }
+        if (k == 0) {
+          r0 = rn;
+          if (r0 == 0.0) break;
+        } else if (rn <= itol * r0) {
+          break;
         }
-        if (k >= P.max_inner && status == MHM_SOLVE_OK) status = MHM_SOLVE_NOT_CONVERGED;
+        if (k >= P.max_inner) { status = MHM_SOLVE_NOT_CONVERGED; break; }
+        read_exchange(R, w.Zf, w.Zs, R.vt);
+        coarse_rows(s, w.Uz, R, R.r - 1, R.r + 2);
+        for (int l = tid; l < R.ng; l += nth) R.vu[l] = R.vt[l] - g0y(R, l);
+        double gam = 0.0;
+        for (int l = tid; l < R.nown; l += nth) gam = fma(R.vr[l], R.vu[l], gam);
+        {
+          const double del = cell_matvec(s, R, R.Sb, R.vu);
+          __syncthreads();
+          write_exchange(R, nx * t, w.Vf, w.Vs);
+          partial_coarse(s, R, w.Uw, nullptr);
+          put_partial2(w, 1, gam, del, red);
+        }
+        SYNC_OR_EXIT();
+        // (2) step: P S p by recurrence, r -= alpha P S p; preconditioned partials
+        {
+          double gd[2];
+          grid_totals<2>(w, 1, gd, sh);
+          const double g = gd[0], d = gd[1];
+          const double beta = k > 0 ? g / gam_prev : 0.0;
+          const double pq = k > 0 ? d - beta * g / alpha_prev : d;
+          if (!(pq > 0.0) || !isfinite(g)) { status = MHM_SOLVE_BREAKDOWN; break; }
+          const double alpha = g / pq;
+          read_exchange(R, w.Vf, w.Vs, R.vt);
+          coarse_rows(s, w.Uw, R, R.r - 1, R.r + 2);
+          for (int l = tid; l < R.ng; l += nth) {
+            const double pw = R.vt[l] - g0y(R, l);
+            const double ps = k > 0 ? fma(beta, R.vps[l], pw) : pw;
+            R.vps[l] = ps;
+            R.vr[l] = fma(-alpha, ps, R.vr[l]);
+            const double p = k > 0 ? fma(beta, R.vp[l], R.vu[l]) : R.vu[l];
+            R.vp[l] = p;
+            R.vlam[l] = fma(alpha, p, R.vlam[l]);
+          }
+          gam_prev = g;
+          alpha_prev = alpha;
+        }
+        if ((k + 1) % kReproject == 0) {
+          // project r and P S p again
+          dof_coarse(s, R, R.vr, R.vps);
+          {
+            const int src[2] = {0, 1};
+            double* const dst[2] = {w.Ux1, w.Ux2};
+            const int shift[2] = {0, 0};
+            coarse_rowfwd(s, R, 2, src, dst, shift);
+          }
+          SYNC_OR_EXIT();
+          coarse_rows1(s, w.Ux1, R, R.r - 1, R.r + 2);
+          for (int l = tid; l < R.ng; l += nth) R.vr[l] -= g0y(R, l);
+          coarse_rows1(s, w.Ux2, R, R.r - 1, R.r + 2);
+          for (int l = tid; l < R.ng; l += nth) R.vps[l] -= g0y(R, l);
+        }
+        {
+          double r2 = 0.0;
+          for (int l = tid; l < R.nown; l += nth) r2 = fma(R.vr[l], R.vr[l], r2);
+          cell_matvec(s, R, R.Pb, R.vr);
+          __syncthreads();
+          write_exchange(R, nx * t, w.Zf, w.Zs);
+          partial_coarse(s, R, w.Uz, nullptr);
+          put_partial(w, 0, r2, red);
+        }
+        SYNC_OR_EXIT();
       }
       total_inner += k;
       if (status != MHM_SOLVE_OK) goto finish;
-      // c = C^-1 G0^T (S lam - r1)
-      stage(R, w.lam);
-      for (int64_t i = R.d0 + tid; i < R.d1; i += nth) w.tmp[i] = srow_win(s, R, i) - w.rfull[i];
+      // c = (G0^T G0)^-1 G0^T (S lambda - r1): cell partials of S lambda, minus r1
+      for (int l = tid; l < R.ng; l += nth) R.vt[l] = __ldcg(w.rfull + R.gdof[l]);
+      cell_matvec(s, R, R.Sb, R.vlam);
+      partial_coarse(s, R, w.Uw, R.vt);
       SYNC_OR_EXIT();
-      stage_g(R, w.tmp);
-      row_g0t(s, R, R.win);
-      coarse_rowfwd(s, w.U, R);
-      SYNC_OR_EXIT();
-      coarse_rows(s, w.U, R, 1, 2);
-      for (int64_t i = R.d0 + tid; i < R.d1; i += nth) P.x[i] += w.lam[i];
-      for (int cx = tid; cx < s.nx; cx += nth) P.x[s.T + R.c0 + cx] += R.yrow[s.nx + cx];
+      coarse_rows(s, w.Uw, R, R.r, R.r + 1);
+      for (int l = tid; l < R.nown; l += nth) P.x[R.d0 + l] += R.vlam[l];
+      for (int cx = tid; cx < nx; cx += nth) P.x[s.T + R.c0 + cx] += R.yrow[nx + cx];
       SYNC_OR_EXIT();
     }
   }
@@ -742,7 +920,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       const double v = P.rhs[i] - krow(s, i, P.x);
       r2 += v * v;
     }
-    for (int cx = tid; cx < s.nx; cx += nth) {
+    for (int cx = tid; cx < nx; cx += nth) {
       const int64_t i = s.T + R.c0 + cx;
       const double v = P.rhs[i] - krow(s, i, P.x);
       r2 += v * v;
@@ -772,14 +950,14 @@ finish:
       l2 += ls * ls;
     };
     for (int64_t i = R.d0 + tid; i < R.d1; i += nth) row(i);
-    for (int cx = tid; cx < s.nx; cx += nth) row(s.T + R.c0 + cx);
+    for (int cx = tid; cx < nx; cx += nth) row(s.T + R.c0 + cx);
     put_partial(w, 0, d2, red);
     put_partial(w, 1, a2, red);
     put_partial(w, 2, l2, red);
     if (!grid_sync(w, epoch)) { status = MHM_SOLVE_BARRIER_TIMEOUT; goto done; }
-    const double dn = sqrt(grid_total(w, 0, sh));
-    const double an = sqrt(grid_total(w, 1, sh));
-    const double ln = sqrt(grid_total(w, 2, sh));
+    double tot[3];
+    grid_totals<3>(w, 0, tot, sh);
+    const double dn = sqrt(tot[0]), an = sqrt(tot[1]), ln = sqrt(tot[2]);
     const double scale = fmax(fmax(bnorm, ln), fmax(an, 2.2250738585072014e-308));
     if (blockIdx.x == 0 && tid == 0) {
       P.stats[0] = (bnorm > 0.0) ? dn / bnorm : 0.0;
@@ -825,7 +1003,7 @@ __global__ void scatter_kernel(int64_t nnz, const int64_t* slot_ptr, const int64
 }
 
 struct Layout {
-  size_t lam, rho, rhoP, z, zt, p, q, tmp, rfull, U, U2, cheb, part, bar, err, total;
+  size_t Zf, Zs, Vf, Vs, U[8], rfull, cheb, part, bar, err, total;
 };
 
 Layout layout(const mhm_skeleton_system* s, int grid) {
@@ -837,10 +1015,12 @@ Layout layout(const mhm_skeleton_system* s, int grid) {
     return at;
   };
   const size_t T = (size_t)s->trace_size, N = (size_t)s->size, M = (size_t)s->cells;
-  L.lam = take(T * 8); L.rho = take(T * 8); L.rhoP = take(T * 8); L.z = take(T * 8);
-  L.zt = take(T * 8); L.p = take(T * 8); L.q = take(T * 8); L.tmp = take(T * 8);
+  L.Zf = take(T * 8);
+  L.Zs = take(T * 8);
+  L.Vf = take(T * 8);
+  L.Vs = take(T * 8);
+  for (int k = 0; k < 8; ++k) L.U[k] = take(M * 8);
   L.rfull = take(N * 8);
-  L.U = take(M * 8); L.U2 = take(M * 8);
   L.cheb = take((size_t)s->nx * (s->ny + 1) * 8);
   L.part = take((size_t)grid * 4 * 8);
   L.bar = take(2 * sizeof(unsigned));
@@ -850,8 +1030,8 @@ Layout layout(const mhm_skeleton_system* s, int grid) {
 }
 
 size_t dyn_smem(const mhm_skeleton_system* s) {
-  size_t off[16];
-  return smem_layout(s, off);
+  size_t off[kSmemArrays + 1];
+  return smem_layout(s->nx, s->ny, s->face_size, s->cell_width, off);
 }
 
 const void* kernel_for(int fs) {
@@ -865,10 +1045,12 @@ const void* kernel_for(int fs) {
 }
 
 // One CTA per macro row; all rows must be co-resident for the cooperative launch.
+// Local DOF indices are int16 and the DOF ids int32.
 int resolve_grid(const mhm_skeleton_system* s) {
   int dev = 0, sms = 0, per_sm = 0;
   const void* kern = kernel_for(s->face_size);
   if (!kern) return 0;
+  if ((int64_t)(3 * (int64_t)s->nx + 1) * s->face_size > 32767 || s->trace_size > INT32_MAX) return 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return -1;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
   const size_t smem = dyn_smem(s);
@@ -886,10 +1068,10 @@ int resolve_grid(const mhm_skeleton_system* s) {
 bool valid(const mhm_skeleton_system* s) {
   return s && s->size == s->trace_size + s->cells && s->face_size >= 1 && s->face_size <= 4 &&
          (int64_t)s->faces * s->face_size == s->trace_size && s->cell_width == 4 * s->face_size &&
-         s->nx >= 1 && s->ny >= 1 && (int64_t)s->nx * s->ny == s->cells && s->qx && s->indptr &&
+         s->nx >= 1 && s->ny >= 1 && (int64_t)s->nx * s->ny == s->cells && s->indptr &&
          s->indices && s->values && s->trace_end && s->cell_dofs && s->cell_g0 && s->dof_cells &&
          s->dof_slot && std::isfinite(s->coarse_ax) && std::isfinite(s->coarse_ay) &&
-         s->coarse_ax > 0 && s->coarse_ay > 0;
+         s->coarse_ax > 0 && s->coarse_ay > 0 && (!s->cell_blocks || s->block_ld >= s->cell_width);
 }
 
 // The Chebyshev values U_m(theta) grow like rho^m, rho = theta + sqrt(theta^2 - 1);
@@ -950,14 +1132,21 @@ extern "C" int mhm_skeleton_solve(const mhm_skeleton_system* s, const double* rh
   Params P{};
   P.s = Sys{s->size, s->trace_size, s->indptr, s->indices, s->values, s->trace_end, s->faces,
             s->face_size, s->cells, s->cell_width, s->cell_dofs, s->cell_g0, s->dof_cells,
-            s->dof_slot, s->nx, s->ny, s->qx, s->coarse_ax, s->coarse_ay};
-  P.w.lam = (double*)(base + L.lam); P.w.rho = (double*)(base + L.rho);
-  P.w.rhoP = (double*)(base + L.rhoP); P.w.z = (double*)(base + L.z);
-  P.w.zt = (double*)(base + L.zt); P.w.p = (double*)(base + L.p); P.w.q = (double*)(base + L.q);
-  P.w.tmp = (double*)(base + L.tmp); P.w.rfull = (double*)(base + L.rfull);
-  P.w.U = (double*)(base + L.U); P.w.U2 = (double*)(base + L.U2);
-  P.w.cheb = (double*)(base + L.cheb); P.w.part = (double*)(base + L.part);
-  P.w.bar = (unsigned*)(base + L.bar); P.w.err = (int*)(base + L.err);
+            s->dof_slot, s->nx, s->ny, s->coarse_ax, s->coarse_ay, s->cell_blocks, s->block_ld};
+  auto at = [&](size_t o) { return reinterpret_cast<double*>(base + o); };
+  P.w.Zf = at(L.Zf);
+  P.w.Zs = at(L.Zs);
+  P.w.Vf = at(L.Vf);
+  P.w.Vs = at(L.Vs);
+  P.w.Uz = Coarse{at(L.U[0]), at(L.U[1]), at(L.U[2])};
+  P.w.Uw = Coarse{at(L.U[3]), at(L.U[4]), at(L.U[5])};
+  P.w.Ux1 = at(L.U[6]);
+  P.w.Ux2 = at(L.U[7]);
+  P.w.rfull = at(L.rfull);
+  P.w.cheb = at(L.cheb);
+  P.w.part = at(L.part);
+  P.w.bar = reinterpret_cast<unsigned*>(base + L.bar);
+  P.w.err = reinterpret_cast<int*>(base + L.err);
   P.rhs = rhs; P.load_scale = load_scale; P.x = x; P.rtol = rtol; P.inner_rtol = inner_rtol;
   P.max_inner = max_inner; P.max_outer = max_outer; P.info = info; P.stats = stats;
   cudaStream_t st = static_cast<cudaStream_t>(stream);

@@ -40,7 +40,6 @@ from .topology import (
     geometric_constraint,
     mesh_arrays,
     side_orientation,
-    sine_transform,
     skeleton_pattern,
 )
 
@@ -282,7 +281,6 @@ class CartesianQ1Plan:
         self.d_g0 = up(g0, torch.float64)
         self.d_dof_cells = up(dof_cells, torch.int32)
         self.d_dof_slot = up(dof_slot, torch.int32)
-        self.d_qx = up(sine_transform(m.nx), torch.float64)
         self.coarse_ab = coarse_coefficients(m, space_h, space_v)
         # ---- device buffers -----------------------------------------------------------
         M, n, w, t1 = self.cells, self.n, self.w, self.t + 1
@@ -324,8 +322,8 @@ class CartesianQ1Plan:
         s.cell_dofs, s.cell_g0 = _lib.ptr(self.d_cell_dofs), _lib.ptr(self.d_g0)
         s.dof_cells, s.dof_slot = _lib.ptr(self.d_dof_cells), _lib.ptr(self.d_dof_slot)
         s.nx, s.ny = m.nx, m.ny
-        s.qx = _lib.ptr(self.d_qx)
         s.coarse_ax, s.coarse_ay = self.coarse_ab
+        s.cell_blocks, s.block_ld = _lib.ptr(self.blocks), self.t + 1
         nbytes = self.lib.mhm_skeleton_workspace_bytes(s, self.grid)
         if nbytes <= 0:
             raise RuntimeError("could not size the skeleton solver workspace")

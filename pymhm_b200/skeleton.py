@@ -23,7 +23,6 @@ from .topology import (
     dof_cell_maps,
     geometric_constraint,
     mesh_arrays,
-    sine_transform,
     skeleton_pattern,
 )
 
@@ -75,8 +74,7 @@ class SkeletonFactorization:
             indptr=up(pat.indptr, torch.int64), indices=up(pat.indices, torch.int32),
             values=up(values, torch.float64), trace_end=up(pat.trace_end, torch.int64),
             cell_dofs=up(cell_dofs, torch.int64), g0=up(geometric_constraint(self.mesh, space_h, space_v), torch.float64),
-            dof_cells=up(dof_cells, torch.int32), dof_slot=up(dof_slot, torch.int32),
-            qx=up(sine_transform(self.mesh.nx), torch.float64))
+            dof_cells=up(dof_cells, torch.int32), dof_slot=up(dof_slot, torch.int32))
         k = self._keep
         s = self.sys = _lib.SkeletonSystem()
         s.size, s.trace_size = N, T
@@ -86,7 +84,6 @@ class SkeletonFactorization:
         s.cell_dofs, s.cell_g0 = _lib.ptr(k["cell_dofs"]), _lib.ptr(k["g0"])
         s.dof_cells, s.dof_slot = _lib.ptr(k["dof_cells"]), _lib.ptr(k["dof_slot"])
         s.nx, s.ny = self.mesh.nx, self.mesh.ny
-        s.qx = _lib.ptr(k["qx"])
         s.coarse_ax, s.coarse_ay = coarse_coefficients(self.mesh, space_h, space_v)
         nbytes = self.lib.mhm_skeleton_workspace_bytes(s, 0)
         self.workspace = torch.empty(int(nbytes), dtype=torch.uint8, device=dev)

@@ -57,7 +57,7 @@ def test_static_scratch_rejects_oversized_systems():
     from pymhm_b200.darcy import CartesianQ1Plan
     from pymhm_b200.topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
 
-    mesh = CartesianMacroMesh(96)
+    mesh = CartesianMacroMesh(128)
     sk = SkeletonSpace(mesh, (FaceSpace.uniform(2),) * len(mesh.faces))
     plan = CartesianQ1Plan(mesh, sk, 2, precision="fp64")
     lib = _lib.load()
