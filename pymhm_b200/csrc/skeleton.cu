@@ -14,8 +14,8 @@
 // G0 the exact geometric net-flux operator of the Cartesian macro grid.
 // G0^T G0 = ay (T_y (x) I) + ax (I (x) T_x) is a scaled 2-D Dirichlet Laplacian
 // on the macro cells; it is inverted exactly by an orthonormal sine transform
-// along x, the inverse of one tridiagonal Toeplitz matrix along y per sine mode
-// (closed form through Chebyshev polynomials of the second kind), and the
+// along x (Q), the inverse of one tridiagonal Toeplitz matrix along y per sine
+// mode (closed form through Chebyshev polynomials of the second kind), and the
 // inverse transform.  K - K0 is at rounding level, so two or three outer
 // corrections reach FP64 accuracy.
 //
@@ -27,7 +27,7 @@
 // weights D_c,a = S_c,aa / sum_{c' containing the DOF} S_c',a'a'.  From an
 // assembled matrix alone, S is split exactly into cell parts (entries of a face
 // shared by two cells halved) and the preconditioner is additive Schwarz over
-// the cells' principal 12 x 12 submatrices.
+// the cells' principal t x t submatrices.
 //
 // The inner CG uses the single-reduction recurrence of Chronopoulos and Gear
 // (J. Comput. Appl. Math. 25 (1989) 153-168): with u = P M^-1 r and w = S u,
@@ -40,13 +40,14 @@
 // Everything runs in one persistent cooperative kernel with one CTA per macro
 // row.  CTA r owns the DOFs first met by the cells of row r (a contiguous range
 // in the reference's numbering) and keeps the iteration vectors on the DOFs of
-// its own cells (owned DOFs plus the bottom faces).  Each CTA turns its cells'
-// partials into coarse data for its own row and for the two neighbouring rows
-// (G0^T of a partial reaches the neighbour through the shared face), so an inner
-// iteration needs two grid barriers and every cross-CTA value it reads arrives
-// in one batch of loads after a barrier.  The barrier is a monotonic arrival
-// counter with a bounded spin: on timeout every CTA sets the error flag and
-// returns (MHM_SOLVE_BARRIER_TIMEOUT).
+// its own cells (owned DOFs plus the bottom faces).  A coarse solve takes two
+// steps between grid barriers: row owners transform their rows along x (their
+// cells' partials also reach the two neighbouring rows through the shared
+// faces); then CTA k solves sine mode k along y for all rows; the row owners
+// read back the three rows they need.  Every cross-CTA value a step reads
+// arrives in one batch of loads after a barrier.  The barrier is a monotonic
+// arrival counter with a bounded spin: on timeout every CTA sets the error flag
+// and returns (MHM_SOLVE_BARRIER_TIMEOUT).
 #include <cmath>
 
 #include "mhm_common.cuh"
@@ -76,20 +77,21 @@ struct Sys {
   int ld;
 };
 
-// Coarse data of one quantity: U[row][k] = self[row] + below[row] + above[row],
-// `below` written by the CTA of row-1, `above` by the CTA of row+1 (null: absent).
+// Row-transformed coarse data of one quantity, layout [mode][row]:
+// U = self + below + above, `below` written by the CTA of row-1 and `above` by
+// the CTA of row+1 (null: absent).
 struct Coarse {
   double *self, *below, *above;
 };
 
 struct Work {
-  double *Zf, *Zs, *Vf, *Vs;  // T each: per-DOF partials of the first / second cell
-  Coarse Uz, Uw;              // M each part
-  double *Ux1, *Ux2;          // M each: coarse data of DOF vectors
-  double* rfull;              // N: outer residual
-  double* cheb;               // nx * (ny + 1) Chebyshev tables
-  double* part;               // grid * 4 partial sums
-  unsigned* bar;              // arrival counter
+  double *Zf, *Zs, *Vf, *Vs;       // T each: per-DOF partials of the first / second cell
+  Coarse Uz, Uw;                   // M each part
+  double *Ux1, *Ux2;               // M each: coarse data of DOF vectors
+  double *Wz, *Ww, *Wx1, *Wx2;     // M each, [row][mode]: solved coarse data
+  double* rfull;                   // N: outer residual
+  double* part;                    // grid * 4 partial sums
+  unsigned* bar;                   // arrival counter
   int* err;
 };
 
@@ -142,7 +144,7 @@ __device__ bool grid_sync(const Work& w, unsigned& epoch) {
   return bad == 0;
 }
 
-// Sums of the per-CTA partials in slots [slot, slot + n) (fixed order, identical
+// Sums of the per-CTA partials in slots [slot, slot + NS) (fixed order, identical
 // in every CTA); the loads of all slots are issued together.
 template <int NS>
 __device__ void grid_totals(const Work& w, int slot, double (&out)[NS], double* sh) {
@@ -220,20 +222,26 @@ __device__ double csr_entry(const Sys& s, int64_t i, int64_t j) {
   return 0.0;
 }
 
+// Row stride of the shared-memory sine transform: = 8 (mod 16) doubles, so the
+// two half-warps of a transform step read disjoint banks.
+__host__ __device__ inline int q_stride(int nx) { return nx + ((8 - nx % 16) + 16) % 16; }
+
 // Per-CTA state.  CTA r owns macro row r and the DOFs [d0, d1) first met in it.
 // Local DOFs ("G"): l < nown are the owned DOFs d0 + l; l >= nown (rows r > 0)
 // are the bottom faces of the row's cells, nown + cx * fs + j.  These are all
 // the DOFs of the row's cells; their cells lie in rows r-1 .. r+1, whose coarse
-// values are kept in yrow slots 0..2 (slot = row - r + 1).
+// values are kept in yrow slots 0..2 (slot = row - r + 1).  The CTA also solves
+// sine modes blockIdx.x + j * gridDim.x (Chebyshev tables in mcheb).
 struct Row {
-  int r, c0, nown, ng;
+  int r, c0, nown, ng, qs, nmode;
   int64_t d0, d1;
-  double* sine;  // 2 (nx + 1): sqrt(2/(nx+1)) sin(pi m / (nx+1))
-  double* yrow;  // 3 nx
-  double* col;   // 8 nx: self, bottom, right, top, left sums; then self, up, down columns
-  double* wrow;  // 3 nx
-  double* cinv;  // nx
-  double* cheb;  // nx (ny + 1)
+  double* Q;      // nx x qs: Q[k][i] = sqrt(2/(nx+1)) sin(pi (k+1)(i+1) / (nx+1))
+  double* yrow;   // 3 nx
+  double* col;    // 8 nx: self, bottom, right, top, left sums; then self, up, down columns
+  double* wrow;   // 3 nx
+  double* mcheb;  // nmode (ny + 1): U_m(theta_k)
+  double* mcinv;  // nmode: 1 / (ay U_ny(theta_k))
+  double* ucol;   // ny
   double *vr, *vps, *vp, *vlam, *vu, *vt;  // G vectors: r, P S p, p, lambda, u, staging
   double* cpart;  // nx t: per-cell partials
   double* Sb;     // nx np: packed symmetric S_c
@@ -245,7 +253,6 @@ struct Row {
   double* gself;    // nx t: g0 of the cell on its slot
   double* gnb;      // nx t: g0 of the other cell on the same DOF (0: none)
   uint8_t* role;    // nx t: bit 0 = the cell is the DOF's second cell, bit 1 = the DOF has two cells
-  uint8_t* pidx;    // t t: packed symmetric index
   double* scratch;  // kWarps t t (aliases the G vectors during setup)
 };
 
@@ -256,52 +263,52 @@ __device__ __forceinline__ double g0y(const Row& R, int l) {
   return v;
 }
 
-// Sums over 8-lane groups: out o = sum over lanes of partial(o, lane); every lane
-// of the block runs the same number of rounds, so the shuffles never diverge.
-template <typename F, typename G>
-__device__ __forceinline__ void group8(int nout, F partial, G store) {
-  const int lane8 = threadIdx.x & 7, grp = threadIdx.x >> 3, ngrp = blockDim.x >> 3;
-  for (int base = 0; base < nout; base += ngrp) {
-    const int o = base + grp;
-    double v = (o < nout) ? partial(o, lane8) : 0.0;
-    v += __shfl_xor_sync(0xffffffffu, v, 4);
-    v += __shfl_xor_sync(0xffffffffu, v, 2);
-    v += __shfl_xor_sync(0xffffffffu, v, 1);
-    if (o < nout && lane8 == 0) store(o, v);
+// Packed index of (i, j) in a symmetric T x T block stored by upper rows.
+template <int T>
+__device__ __forceinline__ int packed(int a, int b) {
+  const int i = a < b ? a : b, j = a < b ? b : a;
+  return i * T - (i * (i - 1)) / 2 + (j - i);
+}
+
+// out(j, i, v): v = sum_k in[j][k] Q[k][i] for j < nin (in[j] in shared memory),
+// i < nx.  Warp w takes columns 8w .. 8w+7 (repeating every 128); lane bits 3-4
+// split k four ways, reduced by shuffles.
+template <typename F>
+__device__ void sine_apply(const Row& R, int nx, int nin, const double* const* in, F out) {
+  const int lane = threadIdx.x & 31, q = lane >> 3;
+  for (int base = (threadIdx.x >> 5) * 8; base < nx; base += kWarps * 8) {
+    const int i = base + (lane & 7);
+    double acc[3] = {0.0, 0.0, 0.0};
+    if (i < nx) {
+      const double* qc = R.Q + i;
+#pragma unroll 4
+      for (int k = q; k < nx; k += 4) {
+        const double qv = qc[k * R.qs];
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          if (j < nin) acc[j] = fma(in[j][k], qv, acc[j]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], 8);
+      acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], 16);
+    }
+    if (i < nx && q == 0)
+      for (int j = 0; j < nin; ++j) out(j, i, acc[j]);
   }
 }
 
-// Orthonormal sine transform Q[k][i] = sine[(k+1)(i+1) mod 2(n+1)] (symmetric):
-// sum_{k = l, l+8, ...} a[k] Q[k][i].
-__device__ __forceinline__ double sine_dot(const double* a, const double* sine, int n, int i, int l) {
-  const int period = 2 * (n + 1);
-  int m = ((l + 1) * (i + 1)) % period;
-  const int step = (8 * (i + 1)) % period;
-  double acc = 0.0;
-  for (int k = l; k < n; k += 8) {
-    acc = fma(a[k], sine[m], acc);
-    m += step;
-    if (m >= period) m -= period;
-  }
-  return acc;
-}
-
-// Row transform of nrow column vectors (R.col + src[j] * nx) into dst[j] + r' * nx,
-// r' = R.r + shift[j] (null dst: skipped).
-__device__ void coarse_rowfwd(const Sys& s, const Row& R, int nrow, const int* src, double* const* dst,
+// Row transform of nin column vectors R.col + src[j] nx into dst[j] at row
+// R.r + shift[j] (layout [mode][row]; null dst: skipped).
+__device__ void coarse_rowfwd(const Sys& s, const Row& R, int nin, const int* src, double* const* dst,
                               const int* shift) {
   __syncthreads();
-  const int nx = s.nx;
-  group8(
-      nrow * nx,
-      [&](int o, int l) {
-        const int j = o / nx, k = o - j * nx;
-        return dst[j] ? sine_dot(R.col + src[j] * nx, R.sine, nx, k, l) : 0.0;
-      },
-      [&](int o, double v) {
-        const int j = o / nx, k = o - j * nx;
-        if (dst[j]) dst[j][(size_t)(R.r + shift[j]) * nx + k] = v;
-      });
+  const double* in[3] = {R.col + src[0] * s.nx, R.col + src[nin > 1 ? 1 : 0] * s.nx,
+                         R.col + src[nin > 2 ? 2 : 0] * s.nx};
+  sine_apply(R, s.nx, nin, in, [&](int j, int k, double v) {
+    if (dst[j]) dst[j][(size_t)k * s.ny + R.r + shift[j]] = v;
+  });
 }
 
 __device__ void coarse_rowfwd1(const Sys& s, const Row& R, double* dst) {
@@ -311,103 +318,79 @@ __device__ void coarse_rowfwd1(const Sys& s, const Row& R, double* dst) {
   coarse_rowfwd(s, R, 1, src, d, sh);
 }
 
-// After every row's coarse data is written: coarse solution rows [lo, hi) (clipped
-// to the grid, within r-1 .. r+1) into yrow; other slots zero.  Per sine mode k,
-// W[ir][k] = sum_iy Tinv_k[ir][iy] U[iy][k] with Tinv_k[i][j] = U_i U_{ny-1-j} /
-// (ay U_ny) for i <= j (U the mode's Chebyshev table; symmetric), then Y rows =
-// W rows Q.
-__device__ void coarse_rows(const Sys& s, const Coarse& U, const Row& R, int lo, int hi) {
+// After every row's coarse data is written: for each sine mode k this CTA owns,
+// W[ir][k] = sum_iy Tinv_k[ir][iy] U[k][iy] for every row ir, with
+// Tinv_k[i][j] = U_i U_{ny-1-j} / (ay U_ny) for i <= j (U the mode's Chebyshev
+// values; symmetric).
+__device__ void mode_solve(const Sys& s, const Row& R, const Coarse& U, double* W) {
   const int ny = s.ny, nx = s.nx;
-  if (lo < 0) lo = 0;
-  if (hi > ny) hi = ny;
-  const int r0 = R.r - 1;
-  __syncthreads();
-  {
+  for (int j = 0; j < R.nmode; ++j) {
+    const int k = blockIdx.x + j * gridDim.x;
+    __syncthreads();
+    for (int iy = threadIdx.x; iy < ny; iy += blockDim.x) {
+      const size_t at = (size_t)k * ny + iy;
+      const double v0 = __ldcg(U.self + at);
+      const double v1 = (iy > 0 && U.below) ? __ldcg(U.below + at) : 0.0;
+      const double v2 = (iy < ny - 1 && U.above) ? __ldcg(U.above + at) : 0.0;
+      R.ucol[iy] = (v0 + v1) + v2;
+    }
+    __syncthreads();
+    const double* u = R.mcheb + (size_t)j * (ny + 1);
+    const double c = R.mcinv[j];
     const int lane8 = threadIdx.x & 7, grp = threadIdx.x >> 3, ngrp = blockDim.x >> 3;
-    for (int base = 0; base < nx; base += ngrp) {
-      const int k = base + grp;
-      double a[3] = {0.0, 0.0, 0.0};
-      if (k < nx) {
-        const double* u = R.cheb + (size_t)k * (ny + 1);
-        double uir[3], unir[3];
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          const int ir = r0 + j;
-          const bool on = ir >= lo && ir < hi;
-          uir[j] = on ? u[ir] : 0.0;
-          unir[j] = on ? u[ny - 1 - ir] : 0.0;
-        }
-        for (int iy0 = lane8; iy0 < ny; iy0 += 64) {
-          double v0[8], v1[8], v2[8];
-#pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int iy = iy0 + 8 * q;
-            const size_t at = (size_t)iy * nx + k;
-            v0[q] = iy < ny ? __ldcg(U.self + at) : 0.0;
-            v1[q] = (iy < ny && iy > 0 && U.below) ? __ldcg(U.below + at) : 0.0;
-            v2[q] = (iy < ny - 1 && U.above) ? __ldcg(U.above + at) : 0.0;
-          }
-#pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int iy = iy0 + 8 * q;
-            if (iy < ny) {
-              const double v = (v0[q] + v1[q]) + v2[q];
-              const double ulo = u[iy], uhi = u[ny - 1 - iy];
-#pragma unroll
-              for (int j = 0; j < 3; ++j) a[j] = fma((r0 + j < iy ? uir[j] * uhi : ulo * unir[j]), v, a[j]);
-            }
-          }
-        }
+    for (int base = 0; base < ny; base += ngrp) {
+      const int ir = base + grp;
+      double acc = 0.0;
+      if (ir < ny) {
+        const double uir = u[ir], unir = u[ny - 1 - ir];
+        for (int iy = lane8; iy < ny; iy += 8)
+          acc = fma((ir < iy ? uir * u[ny - 1 - iy] : u[iy] * unir), R.ucol[iy], acc);
       }
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        a[j] += __shfl_xor_sync(0xffffffffu, a[j], 4);
-        a[j] += __shfl_xor_sync(0xffffffffu, a[j], 2);
-        a[j] += __shfl_xor_sync(0xffffffffu, a[j], 1);
-      }
-      if (k < nx && lane8 == 0) {
-        const double c = R.cinv[k];
-#pragma unroll
-        for (int j = 0; j < 3; ++j) R.wrow[j * nx + k] = a[j] * c;
-      }
+      acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+      acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+      acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+      if (ir < ny && lane8 == 0) W[(size_t)ir * nx + k] = acc * c;
     }
   }
-  __syncthreads();
-  const int j0 = lo - r0 > 0 ? lo - r0 : 0, j1 = hi - r0 < 3 ? hi - r0 : 3;
-  for (int idx = threadIdx.x; idx < 3 * nx; idx += blockDim.x) {
-    const int j = idx / nx;
-    if (j < j0 || j >= j1) R.yrow[idx] = 0.0;
-  }
-  if (j1 > j0) {
-    group8(
-        (j1 - j0) * nx,
-        [&](int o, int l) {
-          const int j = j0 + o / nx, ix = o % nx;
-          return sine_dot(R.wrow + j * nx, R.sine, nx, ix, l);
-        },
-        [&](int o, double v) { R.yrow[j0 * nx + o] = v; });
-  }
-  __syncthreads();
 }
 
-__device__ void coarse_rows1(const Sys& s, const double* U, const Row& R, int lo, int hi) {
-  const Coarse c{const_cast<double*>(U), nullptr, nullptr};
-  coarse_rows(s, c, R, lo, hi);
+// Coarse solution rows [lo, hi) (clipped to the grid, within r-1 .. r+1) from W
+// into yrow; other slots zero.  Y row = W row Q.
+__device__ void coarse_rows(const Sys& s, const Row& R, const double* W, int lo, int hi) {
+  const int ny = s.ny, nx = s.nx, r0 = R.r - 1;
+  if (lo < 0) lo = 0;
+  if (hi > ny) hi = ny;
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < 3 * nx; idx += blockDim.x) {
+    const int ir = r0 + idx / nx;
+    R.wrow[idx] = (ir >= lo && ir < hi) ? __ldcg(W + (size_t)ir * nx + idx % nx) : 0.0;
+  }
+  __syncthreads();
+  const double* in[3] = {R.wrow, R.wrow + nx, R.wrow + 2 * nx};
+  sine_apply(R, nx, 3, in, [&](int j, int i, double v) { R.yrow[j * nx + i] = v; });
+  __syncthreads();
 }
 
 // Per-cell products cpart[cx][a] = sum_b B_c[a][b] v[cl[cx][b]] (B packed symmetric);
 // returns this thread's sum of v[cl] * cpart (for (u, S u)).
+template <int T>
 __device__ double cell_matvec(const Sys& s, const Row& R, const double* B, const double* v) {
   __syncthreads();
-  const int t = s.t, np = t * (t + 1) / 2;
+  constexpr int np = T * (T + 1) / 2;
   double dot = 0.0;
-  for (int idx = threadIdx.x; idx < s.nx * t; idx += blockDim.x) {
-    const int cx = idx / t, a = idx - cx * t;
+  for (int idx = threadIdx.x; idx < s.nx * T; idx += blockDim.x) {
+    const int cx = idx / T, a = idx - cx * T;
     const double* blk = B + (size_t)cx * np;
-    const int16_t* c = R.cl + cx * t;
-    const uint8_t* pi = R.pidx + a * t;
+    const int16_t* c = R.cl + cx * T;
+    double bv[T], xv[T];
+#pragma unroll
+    for (int b = 0; b < T; ++b) {
+      bv[b] = blk[packed<T>(a, b)];
+      xv[b] = v[c[b]];
+    }
     double acc = 0.0;
-    for (int b = 0; b < t; ++b) acc = fma(blk[pi[b]], v[c[b]], acc);
+#pragma unroll
+    for (int b = 0; b < T; ++b) acc = fma(bv[b], xv[b], acc);
     R.cpart[idx] = acc;
     dot = fma(v[c[a]], acc, dot);
   }
@@ -441,8 +424,8 @@ __device__ void read_exchange(const Row& R, const double* Xf, const double* Xs, 
   }
 }
 
-// Coarse data of sum_c cpart_c (minus G0^T of the G vector `minus`, if given) for
-// this row and, through the shared faces, for rows r+1 and r-1.
+// Row-transformed coarse data of sum_c cpart_c (minus G0^T of the G vector
+// `minus`, if given) for this row and, through the shared faces, rows r+1, r-1.
 __device__ void partial_coarse(const Sys& s, const Row& R, const Coarse& U, const double* minus) {
   const int nx = s.nx, t = s.t, fs = s.fs;
   __syncthreads();
@@ -519,44 +502,47 @@ __device__ void warp_invert(double* a, int t) {
 
 constexpr int kSmemArrays = 23;
 
-__host__ __device__ size_t smem_layout(int nx, int ny, int fs, int t, size_t* off) {
+__host__ __device__ size_t smem_layout(int nx, int ny, int fs, int t, int grid, size_t* off) {
   // a row owns at most 3 nx + 1 faces (row 0); later rows own 2 nx + 1 and add the
   // nx bottom faces of their cells
   const size_t g = (size_t)(3 * nx + 1) * fs;
   const size_t np = (size_t)t * (t + 1) / 2;
   const size_t vec = 6 * g > (size_t)kWarps * t * t ? 6 * g : (size_t)kWarps * t * t;
+  const size_t nmode = grid > 0 ? (size_t)((nx + grid - 1) / grid) : 1;
   size_t o = 0;
   int k = 0;
   auto take = [&](size_t bytes) {
     off[k++] = o;
     o = align16(o + bytes);
   };
-  take(2 * ((size_t)nx + 1) * 8);   // 0 sine
-  take(3 * (size_t)nx * 8);         // 1 yrow
-  take(8 * (size_t)nx * 8);         // 2 col
-  take(3 * (size_t)nx * 8);         // 3 wrow
-  take((size_t)nx * 8);             // 4 cinv
-  take((size_t)nx * (ny + 1) * 8);  // 5 cheb
-  take(vec * 8);                    // 6 G vectors (6 g) / setup scratch
-  take((size_t)nx * t * 8);         // 7 cpart
-  take((size_t)nx * np * 8);        // 8 Sb
-  take((size_t)nx * np * 8);        // 9 Pb
-  take(g * 8);                      // 10 ga
-  take(g * 8);                      // 11 gb
-  take(g * 2);                      // 12 ya
-  take(g * 2);                      // 13 yb
-  take(g * 4);                      // 14 gdof
-  take((size_t)nx * t * 2);         // 15 cl
-  take((size_t)nx * t * 8);         // 16 gself
-  take((size_t)nx * t * 8);         // 17 gnb
-  take((size_t)nx * t);             // 18 role
-  take((size_t)t * t);              // 19 pidx
+  take((size_t)nx * q_stride(nx) * 8);   // 0 Q
+  take(3 * (size_t)nx * 8);              // 1 yrow
+  take(8 * (size_t)nx * 8);              // 2 col
+  take(3 * (size_t)nx * 8);              // 3 wrow
+  take(nmode * (ny + 1) * 8);            // 4 mcheb
+  take(nmode * 8);                       // 5 mcinv
+  take((size_t)ny * 8);                  // 6 ucol
+  take(vec * 8);                         // 7 G vectors (6 g) / setup scratch
+  take((size_t)nx * t * 8);              // 8 cpart
+  take((size_t)nx * np * 8);             // 9 Sb
+  take((size_t)nx * np * 8);             // 10 Pb
+  take(g * 8);                           // 11 ga
+  take(g * 8);                           // 12 gb
+  take(g * 2);                           // 13 ya
+  take(g * 2);                           // 14 yb
+  take(g * 4);                           // 15 gdof
+  take((size_t)nx * t * 2);              // 16 cl
+  take((size_t)nx * t * 8);              // 17 gself
+  take((size_t)nx * t * 8);              // 18 gnb
+  take((size_t)nx * t);                  // 19 role
   off[k] = o;
   return o;
 }
 
 template <int FS>
 __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Params P) {
+  constexpr int T = 4 * FS;
+  constexpr int np = T * (T + 1) / 2;
   const Sys& s = P.s;
   const Work& w = P.w;
   __shared__ double red[64];
@@ -564,8 +550,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
   __shared__ size_t off[kSmemArrays + 1];
   extern __shared__ __align__(16) unsigned char dyn[];
   const int tid = threadIdx.x, nth = blockDim.x;
-  const int nx = s.nx, ny = s.ny, t = s.t;
-  const int np = t * (t + 1) / 2;
+  const int nx = s.nx, ny = s.ny;
   unsigned epoch = 0;
   int status = MHM_SOLVE_OK;
   int total_inner = 0, outer = 0;
@@ -575,35 +560,38 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
   do {                 \
     if (!grid_sync(w, epoch)) { status = MHM_SOLVE_BARRIER_TIMEOUT; goto done; } \
   } while (0)
-  if (tid == 0) smem_layout(nx, ny, FS, t, off);
+  if (tid == 0) smem_layout(nx, ny, FS, T, gridDim.x, off);
   __syncthreads();
   R.r = blockIdx.x;
   R.c0 = R.r * nx;
-  R.sine = reinterpret_cast<double*>(dyn + off[0]);
+  R.qs = q_stride(nx);
+  R.nmode = (nx - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  if (R.nmode < 0) R.nmode = 0;
+  R.Q = reinterpret_cast<double*>(dyn + off[0]);
   R.yrow = reinterpret_cast<double*>(dyn + off[1]);
   R.col = reinterpret_cast<double*>(dyn + off[2]);
   R.wrow = reinterpret_cast<double*>(dyn + off[3]);
-  R.cinv = reinterpret_cast<double*>(dyn + off[4]);
-  R.cheb = reinterpret_cast<double*>(dyn + off[5]);
+  R.mcheb = reinterpret_cast<double*>(dyn + off[4]);
+  R.mcinv = reinterpret_cast<double*>(dyn + off[5]);
+  R.ucol = reinterpret_cast<double*>(dyn + off[6]);
   {
-    double* v = reinterpret_cast<double*>(dyn + off[6]);
+    double* v = reinterpret_cast<double*>(dyn + off[7]);
     const int g = (3 * nx + 1) * FS;
     R.vr = v; R.vps = v + g; R.vp = v + 2 * g; R.vlam = v + 3 * g; R.vu = v + 4 * g; R.vt = v + 5 * g;
     R.scratch = v;
   }
-  R.cpart = reinterpret_cast<double*>(dyn + off[7]);
-  R.Sb = reinterpret_cast<double*>(dyn + off[8]);
-  R.Pb = reinterpret_cast<double*>(dyn + off[9]);
-  R.ga = reinterpret_cast<double*>(dyn + off[10]);
-  R.gb = reinterpret_cast<double*>(dyn + off[11]);
-  R.ya = reinterpret_cast<int16_t*>(dyn + off[12]);
-  R.yb = reinterpret_cast<int16_t*>(dyn + off[13]);
-  R.gdof = reinterpret_cast<int32_t*>(dyn + off[14]);
-  R.cl = reinterpret_cast<int16_t*>(dyn + off[15]);
-  R.gself = reinterpret_cast<double*>(dyn + off[16]);
-  R.gnb = reinterpret_cast<double*>(dyn + off[17]);
-  R.role = reinterpret_cast<uint8_t*>(dyn + off[18]);
-  R.pidx = reinterpret_cast<uint8_t*>(dyn + off[19]);
+  R.cpart = reinterpret_cast<double*>(dyn + off[8]);
+  R.Sb = reinterpret_cast<double*>(dyn + off[9]);
+  R.Pb = reinterpret_cast<double*>(dyn + off[10]);
+  R.ga = reinterpret_cast<double*>(dyn + off[11]);
+  R.gb = reinterpret_cast<double*>(dyn + off[12]);
+  R.ya = reinterpret_cast<int16_t*>(dyn + off[13]);
+  R.yb = reinterpret_cast<int16_t*>(dyn + off[14]);
+  R.gdof = reinterpret_cast<int32_t*>(dyn + off[15]);
+  R.cl = reinterpret_cast<int16_t*>(dyn + off[16]);
+  R.gself = reinterpret_cast<double*>(dyn + off[17]);
+  R.gnb = reinterpret_cast<double*>(dyn + off[18]);
+  R.role = reinterpret_cast<uint8_t*>(dyn + off[19]);
   {
     // DOFs are numbered by their first cell: binary search the row boundaries
     auto lower = [&](int cell) {
@@ -619,12 +607,27 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
     R.nown = (int)(R.d1 - R.d0);
     R.ng = R.nown + (R.r > 0 ? nx * FS : 0);
   }
-  for (int m = tid; m < 2 * (nx + 1); m += nth)
-    R.sine[m] = sqrt(2.0 / (nx + 1)) * sinpi((double)m / (double)(nx + 1));
-  for (int e = tid; e < t * t; e += nth) {
-    const int a = e / t, b = e - a * t;
-    const int i = a < b ? a : b, j = a < b ? b : a;
-    R.pidx[e] = (uint8_t)(i * t - i * (i - 1) / 2 + (j - i));
+  for (int e = tid; e < nx * nx; e += nth) {
+    const int k = e / nx, i = e - k * nx;
+    const int m = ((k + 1) * (i + 1)) % (2 * (nx + 1));
+    R.Q[k * R.qs + i] = sqrt(2.0 / (nx + 1)) * sinpi((double)m / (double)(nx + 1));
+  }
+  // Chebyshev values of this CTA's sine modes: T_k = ay tridiag(-1, 2 theta_k, -1),
+  // theta_k = 1 + ax lam_k / (2 ay); U_m(theta_k), m = 0..ny
+  for (int j = tid; j < R.nmode; j += nth) {
+    const int k = blockIdx.x + j * gridDim.x;
+    double* u = R.mcheb + (size_t)j * (ny + 1);
+    const double lam = 2.0 - 2.0 * cospi((double)(k + 1) / (double)(nx + 1));
+    const double two_theta = 2.0 + s.ax * lam / s.ay;
+    double um1 = 0.0, u0 = 1.0;
+    u[0] = 1.0;
+    for (int m = 1; m <= ny; ++m) {
+      const double un = two_theta * u0 - um1;
+      u[m] = un;
+      um1 = u0;
+      u0 = un;
+    }
+    R.mcinv[j] = 1.0 / (s.ay * u[ny]);
   }
   // G DOFs
   for (int l = tid; l < R.ng; l += nth) {
@@ -633,7 +636,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       i = R.d0 + l;
     } else {
       const int q = l - R.nown, cx = q / FS, j = q - cx * FS;
-      i = s.cell_dofs[(size_t)(R.c0 + cx) * t + j];  // bottom side: slots 0 .. fs-1
+      i = s.cell_dofs[(size_t)(R.c0 + cx) * T + j];  // bottom side: slots 0 .. fs-1
     }
     R.gdof[l] = (int32_t)i;
     for (int k = 0; k < 2; ++k) {
@@ -641,7 +644,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       double g = 0.0;
       int y = -1;
       if (c >= 0) {
-        g = s.g0[(size_t)c * t + s.dof_slot[2 * i + k]];
+        g = s.g0[(size_t)c * T + s.dof_slot[2 * i + k]];
         const int cy = c / nx;
         y = (cy - R.r + 1) * nx + (c - cy * nx);
       }
@@ -650,18 +653,18 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
     }
   }
   // the row's cells: local DOF, role and G0 coefficients of each slot
-  for (int idx = tid; idx < nx * t; idx += nth) {
-    const int cx = idx / t, a = idx - cx * t;
+  for (int idx = tid; idx < nx * T; idx += nth) {
+    const int cx = idx / T, a = idx - cx * T;
     const int c = R.c0 + cx;
-    const int64_t i = s.cell_dofs[(size_t)c * t + a];
+    const int64_t i = s.cell_dofs[(size_t)c * T + a];
     R.cl[idx] = (int16_t)(i >= R.d0 && i < R.d1 ? i - R.d0 : R.nown + cx * FS + a);
     const int first = s.dof_cells[2 * i];
     const bool second = first != c;
     R.role[idx] = (uint8_t)((second ? 1 : 0) | (s.dof_cells[2 * i + 1] >= 0 ? 2 : 0));
-    R.gself[idx] = s.g0[(size_t)c * t + a];
+    R.gself[idx] = s.g0[(size_t)c * T + a];
     const int other = second ? first : s.dof_cells[2 * i + 1];
     const int oslot = second ? s.dof_slot[2 * i] : s.dof_slot[2 * i + 1];
-    R.gnb[idx] = other >= 0 ? s.g0[(size_t)other * t + oslot] : 0.0;
+    R.gnb[idx] = other >= 0 ? s.g0[(size_t)other * T + oslot] : 0.0;
   }
   // DOFs met by one cell only: their second-cell partials stay zero
   for (int64_t i = R.d0 + tid; i < R.d1; i += nth)
@@ -671,8 +674,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
     }
   __syncthreads();
   // packed symmetric S_c (operator) of the row's cells
-  for (int idx = tid; idx < nx * t * t; idx += nth) {
-    const int cx = idx / (t * t), e = idx - cx * t * t, a = e / t, b = e - a * t;
+  for (int idx = tid; idx < nx * T * T; idx += nth) {
+    const int cx = idx / (T * T), e = idx - cx * T * T, a = e / T, b = e - a * T;
     if (a > b) continue;
     const int c = R.c0 + cx;
     double v;
@@ -680,40 +683,40 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       const double* B = s.blocks + (size_t)c * s.ld * s.ld;
       v = 0.5 * (B[a * s.ld + b] + B[b * s.ld + a]);
     } else {
-      const int64_t ia = s.cell_dofs[(size_t)c * t + a], ib = s.cell_dofs[(size_t)c * t + b];
+      const int64_t ia = s.cell_dofs[(size_t)c * T + a], ib = s.cell_dofs[(size_t)c * T + b];
       v = 0.5 * (csr_entry(s, ia, ib) + csr_entry(s, ib, ia));
       // an entry between two DOFs of a face shared with another cell is split evenly
-      if (a / FS == b / FS && (R.role[cx * t + a] & 2)) v *= 0.5;
+      if (a / FS == b / FS && (R.role[cx * T + a] & 2)) v *= 0.5;
     }
-    R.Sb[(size_t)cx * np + R.pidx[e]] = v;
+    R.Sb[(size_t)cx * np + packed<T>(a, b)] = v;
   }
   __syncthreads();
   // preconditioner blocks: D B^-1 D, B = S_c (cell blocks) or the assembled principal
   // submatrix (D = 1); one warp inverts one cell's block in the setup scratch
   {
     const int warp = tid >> 5, lane = tid & 31;
-    double* a = R.scratch + (size_t)warp * t * t;
+    double* a = R.scratch + (size_t)warp * T * T;
     for (int cx = warp; cx < nx; cx += kWarps) {
       const int c = R.c0 + cx;
-      for (int e = lane; e < t * t; e += 32) {
-        const int i = e / t, j = e - i * t;
+      for (int e = lane; e < T * T; e += 32) {
+        const int i = e / T, j = e - i * T;
         double v;
         if (s.blocks) {
-          v = R.Sb[(size_t)cx * np + R.pidx[e]];
+          v = R.Sb[(size_t)cx * np + packed<T>(i, j)];
         } else {
-          const int64_t ia = s.cell_dofs[(size_t)c * t + i], ib = s.cell_dofs[(size_t)c * t + j];
+          const int64_t ia = s.cell_dofs[(size_t)c * T + i], ib = s.cell_dofs[(size_t)c * T + j];
           v = 0.5 * (csr_entry(s, ia, ib) + csr_entry(s, ib, ia));
         }
         a[e] = v;
       }
-      warp_invert(a, t);
-      for (int e = lane; e < t * t; e += 32) {
-        const int i = e / t, j = e - i * t;
+      warp_invert(a, T);
+      for (int e = lane; e < T * T; e += 32) {
+        const int i = e / T, j = e - i * T;
         if (i > j) continue;
         double di = 1.0, dj = 1.0;
         if (s.blocks) {
           auto weight = [&](int slot) {
-            const int64_t dof = s.cell_dofs[(size_t)c * t + slot];
+            const int64_t dof = s.cell_dofs[(size_t)c * T + slot];
             const int c1 = s.dof_cells[2 * dof], c2 = s.dof_cells[2 * dof + 1];
             const double d1 = s.blocks[(size_t)c1 * s.ld * s.ld + (size_t)s.dof_slot[2 * dof] * (s.ld + 1)];
             const double d2 =
@@ -723,26 +726,9 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
           di = weight(i);
           dj = weight(j);
         }
-        R.Pb[(size_t)cx * np + R.pidx[e]] = di * (0.5 * (a[i * t + j] + a[j * t + i])) * dj;
+        R.Pb[(size_t)cx * np + packed<T>(i, j)] = di * (0.5 * (a[i * T + j] + a[j * T + i])) * dj;
       }
       __syncwarp();
-    }
-  }
-  // Chebyshev table of mode k: T_k = ay tridiag(-1, 2 theta_k, -1), theta_k =
-  // 1 + ax lam_k / (2 ay); U_m(theta_k), m = 0..ny.
-  if (tid == 0) {
-    for (int k = blockIdx.x; k < nx; k += gridDim.x) {
-      double* u = w.cheb + (size_t)k * (ny + 1);
-      const double lam = 2.0 - 2.0 * cospi((double)(k + 1) / (double)(nx + 1));
-      const double two_theta = 2.0 + s.ax * lam / s.ay;
-      double um1 = 0.0, u0 = 1.0;
-      u[0] = 1.0;
-      for (int m = 1; m <= ny; ++m) {
-        const double un = two_theta * u0 - um1;
-        u[m] = un;
-        um1 = u0;
-        u0 = un;
-      }
     }
   }
   // x = 0, r_full = rhs on owned rows; ||rhs||
@@ -764,11 +750,6 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
     put_partial(w, 0, b2, red);
   }
   SYNC_OR_EXIT();
-  // every mode's Chebyshev table (complete now) into shared memory
-  for (int e = tid; e < nx * (ny + 1); e += nth) R.cheb[e] = __ldcg(w.cheb + e);
-  __syncthreads();
-  for (int k = tid; k < nx; k += nth) R.cinv[k] = 1.0 / (s.ay * R.cheb[(size_t)k * (ny + 1) + ny]);
-  __syncthreads();
   bnorm = sqrt(grid_total(w, 0, sh));
   if (bnorm == 0.0) goto finish;
   for (outer = 0; outer < P.max_outer; ++outer) {
@@ -794,17 +775,20 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
     }
     {
       const double itol = (outer == 0) ? P.inner_rtol : fmax(P.inner_rtol, 1e-4);
+      const Coarse Cx1{w.Ux1, nullptr, nullptr}, Cx2{w.Ux2, nullptr, nullptr};
       // coarse data of r2
       for (int cx = tid; cx < nx; cx += nth) R.col[cx] = w.rfull[s.T + R.c0 + cx];
       coarse_rowfwd1(s, R, w.Ux1);
       SYNC_OR_EXIT();
+      mode_solve(s, R, Cx1, w.Wx1);
+      SYNC_OR_EXIT();
       // lambda0 = -G0 (G0^T G0)^-1 r2 on G; cell partials of S lambda0; r1 on G
-      coarse_rows1(s, w.Ux1, R, R.r - 1, R.r + 2);
+      coarse_rows(s, R, w.Wx1, R.r - 1, R.r + 2);
       for (int l = tid; l < R.ng; l += nth) R.vlam[l] = -g0y(R, l);
       for (int l = tid; l < R.ng; l += nth) R.vt[l] = __ldcg(w.rfull + R.gdof[l]);
-      cell_matvec(s, R, R.Sb, R.vlam);
+      cell_matvec<T>(s, R, R.Sb, R.vlam);
       __syncthreads();
-      write_exchange(R, nx * t, w.Vf, w.Vs);
+      write_exchange(R, nx * T, w.Vf, w.Vs);
       SYNC_OR_EXIT();
       // rhoP = r1 - S lambda0 on G; its coarse data
       read_exchange(R, w.Vf, w.Vs, R.vu);
@@ -813,18 +797,22 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       dof_coarse(s, R, R.vr, nullptr);
       coarse_rowfwd1(s, R, w.Ux1);
       SYNC_OR_EXIT();
+      mode_solve(s, R, Cx1, w.Wx1);
+      SYNC_OR_EXIT();
       // r0 = P rhoP; preconditioned partials and their coarse data; |r0|^2
-      coarse_rows1(s, w.Ux1, R, R.r - 1, R.r + 2);
+      coarse_rows(s, R, w.Wx1, R.r - 1, R.r + 2);
       for (int l = tid; l < R.ng; l += nth) R.vr[l] -= g0y(R, l);
       {
         double r2 = 0.0;
         for (int l = tid; l < R.nown; l += nth) r2 = fma(R.vr[l], R.vr[l], r2);
-        cell_matvec(s, R, R.Pb, R.vr);
+        cell_matvec<T>(s, R, R.Pb, R.vr);
         __syncthreads();
-        write_exchange(R, nx * t, w.Zf, w.Zs);
+        write_exchange(R, nx * T, w.Zf, w.Zs);
         partial_coarse(s, R, w.Uz, nullptr);
         put_partial(w, 0, r2, red);
       }
+      SYNC_OR_EXIT();
+      mode_solve(s, R, w.Uz, w.Wz);
       SYNC_OR_EXIT();
       double r0 = 0.0, gam_prev = 1.0, alpha_prev = 1.0;
       int k = 0;
@@ -840,17 +828,19 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
         }
         if (k >= P.max_inner) { status = MHM_SOLVE_NOT_CONVERGED; break; }
         read_exchange(R, w.Zf, w.Zs, R.vt);
-        coarse_rows(s, w.Uz, R, R.r - 1, R.r + 2);
+        coarse_rows(s, R, w.Wz, R.r - 1, R.r + 2);
         for (int l = tid; l < R.ng; l += nth) R.vu[l] = R.vt[l] - g0y(R, l);
         double gam = 0.0;
         for (int l = tid; l < R.nown; l += nth) gam = fma(R.vr[l], R.vu[l], gam);
         {
-          const double del = cell_matvec(s, R, R.Sb, R.vu);
+          const double del = cell_matvec<T>(s, R, R.Sb, R.vu);
           __syncthreads();
-          write_exchange(R, nx * t, w.Vf, w.Vs);
+          write_exchange(R, nx * T, w.Vf, w.Vs);
           partial_coarse(s, R, w.Uw, nullptr);
           put_partial2(w, 1, gam, del, red);
         }
+        SYNC_OR_EXIT();
+        mode_solve(s, R, w.Uw, w.Ww);
         SYNC_OR_EXIT();
         // (2) step: P S p by recurrence, r -= alpha P S p; preconditioned partials
         {
@@ -862,7 +852,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
           if (!(pq > 0.0) || !isfinite(g)) { status = MHM_SOLVE_BREAKDOWN; break; }
           const double alpha = g / pq;
           read_exchange(R, w.Vf, w.Vs, R.vt);
-          coarse_rows(s, w.Uw, R, R.r - 1, R.r + 2);
+          coarse_rows(s, R, w.Ww, R.r - 1, R.r + 2);
           for (int l = tid; l < R.ng; l += nth) {
             const double pw = R.vt[l] - g0y(R, l);
             const double ps = k > 0 ? fma(beta, R.vps[l], pw) : pw;
@@ -885,30 +875,37 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
             coarse_rowfwd(s, R, 2, src, dst, shift);
           }
           SYNC_OR_EXIT();
-          coarse_rows1(s, w.Ux1, R, R.r - 1, R.r + 2);
+          mode_solve(s, R, Cx1, w.Wx1);
+          mode_solve(s, R, Cx2, w.Wx2);
+          SYNC_OR_EXIT();
+          coarse_rows(s, R, w.Wx1, R.r - 1, R.r + 2);
           for (int l = tid; l < R.ng; l += nth) R.vr[l] -= g0y(R, l);
-          coarse_rows1(s, w.Ux2, R, R.r - 1, R.r + 2);
+          coarse_rows(s, R, w.Wx2, R.r - 1, R.r + 2);
           for (int l = tid; l < R.ng; l += nth) R.vps[l] -= g0y(R, l);
         }
         {
           double r2 = 0.0;
           for (int l = tid; l < R.nown; l += nth) r2 = fma(R.vr[l], R.vr[l], r2);
-          cell_matvec(s, R, R.Pb, R.vr);
+          cell_matvec<T>(s, R, R.Pb, R.vr);
           __syncthreads();
-          write_exchange(R, nx * t, w.Zf, w.Zs);
+          write_exchange(R, nx * T, w.Zf, w.Zs);
           partial_coarse(s, R, w.Uz, nullptr);
           put_partial(w, 0, r2, red);
         }
+        SYNC_OR_EXIT();
+        mode_solve(s, R, w.Uz, w.Wz);
         SYNC_OR_EXIT();
       }
       total_inner += k;
       if (status != MHM_SOLVE_OK) goto finish;
       // c = (G0^T G0)^-1 G0^T (S lambda - r1): cell partials of S lambda, minus r1
       for (int l = tid; l < R.ng; l += nth) R.vt[l] = __ldcg(w.rfull + R.gdof[l]);
-      cell_matvec(s, R, R.Sb, R.vlam);
+      cell_matvec<T>(s, R, R.Sb, R.vlam);
       partial_coarse(s, R, w.Uw, R.vt);
       SYNC_OR_EXIT();
-      coarse_rows(s, w.Uw, R, R.r, R.r + 1);
+      mode_solve(s, R, w.Uw, w.Ww);
+      SYNC_OR_EXIT();
+      coarse_rows(s, R, w.Ww, R.r, R.r + 1);
       for (int l = tid; l < R.nown; l += nth) P.x[R.d0 + l] += R.vlam[l];
       for (int cx = tid; cx < nx; cx += nth) P.x[s.T + R.c0 + cx] += R.yrow[nx + cx];
       SYNC_OR_EXIT();
@@ -1003,7 +1000,7 @@ __global__ void scatter_kernel(int64_t nnz, const int64_t* slot_ptr, const int64
 }
 
 struct Layout {
-  size_t Zf, Zs, Vf, Vs, U[8], rfull, cheb, part, bar, err, total;
+  size_t Zf, Zs, Vf, Vs, U[12], rfull, part, bar, err, total;
 };
 
 Layout layout(const mhm_skeleton_system* s, int grid) {
@@ -1019,9 +1016,8 @@ Layout layout(const mhm_skeleton_system* s, int grid) {
   L.Zs = take(T * 8);
   L.Vf = take(T * 8);
   L.Vs = take(T * 8);
-  for (int k = 0; k < 8; ++k) L.U[k] = take(M * 8);
+  for (int k = 0; k < 12; ++k) L.U[k] = take(M * 8);
   L.rfull = take(N * 8);
-  L.cheb = take((size_t)s->nx * (s->ny + 1) * 8);
   L.part = take((size_t)grid * 4 * 8);
   L.bar = take(2 * sizeof(unsigned));
   L.err = take(sizeof(int));
@@ -1029,9 +1025,9 @@ Layout layout(const mhm_skeleton_system* s, int grid) {
   return L;
 }
 
-size_t dyn_smem(const mhm_skeleton_system* s) {
+size_t dyn_smem(const mhm_skeleton_system* s, int grid) {
   size_t off[kSmemArrays + 1];
-  return smem_layout(s->nx, s->ny, s->face_size, s->cell_width, off);
+  return smem_layout(s->nx, s->ny, s->face_size, s->cell_width, grid, off);
 }
 
 const void* kernel_for(int fs) {
@@ -1053,7 +1049,7 @@ int resolve_grid(const mhm_skeleton_system* s) {
   if ((int64_t)(3 * (int64_t)s->nx + 1) * s->face_size > 32767 || s->trace_size > INT32_MAX) return 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return -1;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
-  const size_t smem = dyn_smem(s);
+  const size_t smem = dyn_smem(s, s->ny);
   if (smem > 227 * 1024) return 0;
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -1142,8 +1138,11 @@ extern "C" int mhm_skeleton_solve(const mhm_skeleton_system* s, const double* rh
   P.w.Uw = Coarse{at(L.U[3]), at(L.U[4]), at(L.U[5])};
   P.w.Ux1 = at(L.U[6]);
   P.w.Ux2 = at(L.U[7]);
+  P.w.Wz = at(L.U[8]);
+  P.w.Ww = at(L.U[9]);
+  P.w.Wx1 = at(L.U[10]);
+  P.w.Wx2 = at(L.U[11]);
   P.w.rfull = at(L.rfull);
-  P.w.cheb = at(L.cheb);
   P.w.part = at(L.part);
   P.w.bar = reinterpret_cast<unsigned*>(base + L.bar);
   P.w.err = reinterpret_cast<int*>(base + L.err);
@@ -1155,6 +1154,6 @@ extern "C" int mhm_skeleton_solve(const mhm_skeleton_system* s, const double* rh
   if (cudaMemsetAsync(stats, 0, 4 * sizeof(double), st) != cudaSuccess) return MHM_ERR_LAUNCH;
   void* args[] = {&P};
   cudaError_t e = cudaLaunchCooperativeKernel(kernel_for(s->face_size), dim3(g), dim3(kSolveThreads),
-                                              args, dyn_smem(s), st);
+                                              args, dyn_smem(s, g), st);
   return e == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
