@@ -15,8 +15,12 @@
 //
 // B200 design: the augmented saddle [[A, c],[c^T, 0]] is never factored as a
 // saddle.  A is a 9-point Neumann operator whose kernel is the constant; pinning
-// the last node (A + a_pp e_p e_p^T) gives an SPD band matrix of half-bandwidth
-// rx+2 that is factored by an in-place band LDL^T in shared memory.  The exact
+// the last node (A + a_pp e_p e_p^T) and scaling it symmetrically to unit
+// diagonal gives an SPD matrix that is block tridiagonal over the lines of the
+// local grid (nny blocks of nnx x nnx).  It is factored by block LDL^T with the
+// explicit inverse of every Schur-complement block S_y = A_yy - B_y S_{y-1}^-1
+// B_y^T (Gauss-Jordan, one barrier per pivot), so every refinement sweep is
+// 2 nny dense block steps applied to all right-hand sides at once.  The exact
 // augmented inverse is recovered by a rank-one kernel correction and FP64
 // residual refinement against the original augmented operator, so the
 // accepted result is the augmented system's solution to the requested
@@ -34,7 +38,7 @@ constexpr int kThreads = 256;
 constexpr int kMaxQuad = 8;
 
 struct Q1Args {
-  int nx, ny, rx, ry, nnx, nny, n, b, t, w, tfh, tfv, kmax, jmax, npairs;
+  int nx, ny, rx, ry, nnx, nny, n, t, w, tfh, tfv, kmax, jmax;
   int NYf;
   double hx, hy, area;
   const double* table;
@@ -57,7 +61,7 @@ struct Q1Args {
   int32_t* status;
   int32_t* iters;
   // shared-memory carve-up (byte offsets)
-  size_t off_band, off_sten, off_vec, off_work, off_pairs, off_misc, smem;
+  size_t off_sinv, off_gj, off_cpl, off_tmp, off_sten, off_vec, off_work, off_misc, smem;
 };
 
 // Closed form of the Q1 element Gram entry int grad(phi_a) . K grad(phi_c) on an
@@ -151,14 +155,26 @@ __device__ __forceinline__ double stencil_apply(const Q1Args& a, const double* s
   return acc;
 }
 
+// Minimum resident CTAs per SM for the factor precision (register budget).
 template <typename T>
-__global__ void __launch_bounds__(kThreads) q1_condense_kernel(const Q1Args a) {
+struct Occupancy {
+  static constexpr int value = sizeof(T) == 8 ? 2 : 3;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_kernel(const Q1Args a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int cell = blockIdx.x;
   const int tid = threadIdx.x;
-  const int n = a.n, b = a.b, nnx = a.nnx, w = a.w, t = a.t;
-  const int bw = b + 1;
-  T* band = reinterpret_cast<T*>(smem + a.off_band);
+  const int n = a.n, nnx = a.nnx, nny = a.nny, w = a.w, t = a.t;
+  const int nb = nnx * nnx;
+  T* sinv = reinterpret_cast<T*>(smem + a.off_sinv);  // nny blocks of nnx x nnx
+  T* gj0 = reinterpret_cast<T*>(smem + a.off_gj);     // Gauss-Jordan ping-pong
+  T* gj1 = gj0 + nb;
+  T* cdn = reinterpret_cast<T*>(smem + a.off_cpl);    // (n, 3): to (y-1, x-1), (y-1, x), (y-1, x+1)
+  T* dg = cdn + 3 * n;                                // (n): scaled diagonal
+  T* dl = dg + n;                                     // (n): scaled coupling to (y, x-1)
+  T* tmp = reinterpret_cast<T*>(smem + a.off_tmp);    // (nnx, w)
   double* sten = reinterpret_cast<double*>(smem + a.off_sten);
   double* fvec = reinterpret_cast<double*>(smem + a.off_vec);
   double* az = fvec + n;
@@ -167,12 +183,12 @@ __global__ void __launch_bounds__(kThreads) q1_condense_kernel(const Q1Args a) {
   T* work = reinterpret_cast<T*>(smem + a.off_work);
   double* kel = reinterpret_cast<double*>(smem + a.off_work);  // aliases work during assembly
   double* fel = kel + 3 * a.rx * a.ry;
-  uint8_t* pdi = reinterpret_cast<uint8_t*>(smem + a.off_pairs);
-  uint8_t* pdj = pdi + a.npairs;
   double* red = reinterpret_cast<double*>(smem + a.off_misc);
   double* bnorm = red + 32;
   double* rnorm = bnorm + w;
-  int* conv = reinterpret_cast<int*>(rnorm + w);
+  double* cmu = rnorm + w;
+  double* cshift = cmu + w;
+  int* conv = reinterpret_cast<int*>(cshift + w);
   int* flag = conv + w;
 
   const int cx = cell % a.nx, cy = cell / a.nx;
@@ -212,13 +228,6 @@ __global__ void __launch_bounds__(kThreads) q1_condense_kernel(const Q1Args a) {
       fe[0] = fe[1] = fe[2] = fe[3] = a.area * (s * 0.25);
     }
     for (int c = 0; c < 4; ++c) fel[4 * e + c] = fe[c];
-  }
-  // pair table of the band update
-  for (int q = tid; q < a.npairs; q += blockDim.x) {
-    int di = 1, rem = q;
-    while (rem >= di) { rem -= di; ++di; }
-    pdi[q] = (uint8_t)di;
-    pdj[q] = (uint8_t)(rem + 1);
   }
   if (tid < w) { conv[tid] = 0; }
   if (tid == 0) flag[0] = 0;
@@ -294,7 +303,7 @@ __global__ void __launch_bounds__(kThreads) q1_condense_kernel(const Q1Args a) {
     if (iy > 0) dd_add(hi, lo, s[3]);
     if (iy > 0 && ix > 0) dd_add(hi, lo, s[4]);
     if (ix < nnx - 1) dd_add(hi, lo, sten[5 * (i + 1) + 1]);
-    if (iy < a.nny - 1) {
+    if (iy < nny - 1) {
       if (ix > 0) dd_add(hi, lo, sten[5 * (i + nnx - 1) + 2]);
       dd_add(hi, lo, sten[5 * (i + nnx) + 3]);
       if (ix < nnx - 1) dd_add(hi, lo, sten[5 * (i + nnx + 1) + 4]);
@@ -327,71 +336,93 @@ __global__ void __launch_bounds__(kThreads) q1_condense_kernel(const Q1Args a) {
   }
   const double zc = block_sum(zc_part, red);
 
-  // ---- pinned, Jacobi-scaled band matrix ------------------------------------
+  // ---- pinned, Jacobi-scaled operator in line-block form -----------------------
   const int pin = n - 1;
   for (int i = tid; i < n; i += blockDim.x) {
     const double dii = sten[5 * i] * (i == pin ? 2.0 : 1.0);
     dsc[i] = (dii > 0.0) ? rsqrt(dii) : 0.0;
   }
   __syncthreads();
-  for (int idx = tid; idx < n * bw; idx += blockDim.x) band[idx] = T(0);
-  __syncthreads();
   for (int i = tid; i < n; i += blockDim.x) {
     const int ix = i % nnx, iy = i / nnx;
     const double si = dsc[i];
     const double* s = sten + 5 * i;
-    T* row = band + (size_t)i * bw;
-    row[0] = T(s[0] * (i == pin ? 2.0 : 1.0) * si * si);
-    if (ix > 0) row[1] = T(s[1] * si * dsc[i - 1]);
-    if (iy > 0 && ix < nnx - 1) row[nnx - 1] = T(s[2] * si * dsc[i - nnx + 1]);
-    if (iy > 0) row[nnx] = T(s[3] * si * dsc[i - nnx]);
-    if (iy > 0 && ix > 0) row[nnx + 1] = T(s[4] * si * dsc[i - nnx - 1]);
-  }
-  __syncthreads();
-  if (st == MHM_CELL_OK) {
-    for (int i = tid; i < n; i += blockDim.x)
-      if (!(dsc[i] > 0.0)) flag[0] = MHM_CELL_SINGULAR_PIVOT;
+    dg[i] = T(s[0] * (i == pin ? 2.0 : 1.0) * si * si);
+    dl[i] = ix > 0 ? T(s[1] * si * dsc[i - 1]) : T(0);
+    cdn[3 * i + 0] = (iy > 0 && ix > 0) ? T(s[4] * si * dsc[i - nnx - 1]) : T(0);
+    cdn[3 * i + 1] = iy > 0 ? T(s[3] * si * dsc[i - nnx]) : T(0);
+    cdn[3 * i + 2] = (iy > 0 && ix < nnx - 1) ? T(s[2] * si * dsc[i - nnx + 1]) : T(0);
+    if (st == MHM_CELL_OK && !(si > 0.0)) flag[0] = MHM_CELL_SINGULAR_PIVOT;
   }
   __syncthreads();
   if (st == MHM_CELL_OK) st = flag[0];
 
-  // ---- in-place band LDL^T (right-looking); entries keep a_ik = L_ik d_k ------
+  // ---- block LDL^T: S_y^-1 for every line y ------------------------------------
+  // S_y[a][c] = Adiag_y[a][c] - sum_{b,d} B_y[a][b] S_{y-1}^-1[b][d] B_y[c][d], B_y the
+  // (tridiagonal) coupling of line y to line y-1; inverted by Gauss-Jordan without
+  // pivoting (SPD), whose pivots are those of the LDL^T of the whole matrix.
+  double dmin = 1e300, dmax = 0.0;
   if (st == MHM_CELL_OK) {
-    for (int k = 0; k < n; ++k) {
-      const T dk = band[(size_t)k * bw];
-      if (!(dk > T(0))) { st = MHM_CELL_SINGULAR_PIVOT; break; }  // uniform branch
-      const T inv = T(1) / dk;
-      for (int q = tid; q < a.npairs; q += blockDim.x) {
-        const int di = pdi[q], dj = pdj[q];
-        const int i = k + di;
-        if (i >= n) continue;
-        const int j = k + dj;
-        const T aik = band[(size_t)i * bw + di];
-        const T ajk = band[(size_t)j * bw + dj];
-        band[(size_t)i * bw + (di - dj)] -= aik * ajk * inv;
+    for (int y = 0; y < nny && st == MHM_CELL_OK; ++y) {
+      const T* prev = sinv + (size_t)(y - 1) * nb;
+      for (int e = tid; e < nb; e += blockDim.x) {
+        const int r = e / nnx, c = e - r * nnx;
+        const int ir = y * nnx + r, ic = y * nnx + c;
+        T v = T(0);
+        if (r == c) v = dg[ir];
+        else if (c == r - 1) v = dl[ir];
+        else if (r == c - 1) v = dl[ic];
+        if (y > 0) {
+          T acc = T(0);
+#pragma unroll
+          for (int p = 0; p < 3; ++p) {
+            const int b = r - 1 + p;
+            if (b < 0 || b >= nnx) continue;
+            const T brb = cdn[3 * ir + p];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              const int d = c - 1 + q;
+              if (d < 0 || d >= nnx) continue;
+              acc += brb * prev[b * nnx + d] * cdn[3 * ic + q];
+            }
+          }
+          v -= acc;
+        }
+        gj0[e] = v;
       }
       __syncthreads();
+      T* cur = gj0;
+      T* nxt = gj1;
+      for (int k = 0; k < nnx; ++k) {
+        const T d = cur[k * nnx + k];
+        if (!(d > T(0))) { st = MHM_CELL_SINGULAR_PIVOT; break; }  // uniform: every thread reads d
+        dmin = fmin(dmin, (double)d);
+        dmax = fmax(dmax, (double)d);
+        const T inv = T(1) / d;
+        T* dst = (k == nnx - 1) ? sinv + (size_t)y * nb : nxt;
+        for (int e = tid; e < nb; e += blockDim.x) {
+          const int r = e / nnx, c = e - r * nnx;
+          T v;
+          if (r == k) v = (c == k) ? inv : cur[e] * inv;
+          else if (c == k) v = -cur[r * nnx + k] * inv;
+          else v = cur[e] - cur[r * nnx + k] * inv * cur[k * nnx + c];
+          dst[e] = v;
+        }
+        __syncthreads();
+        T* sw = cur; cur = nxt; nxt = sw;
+      }
     }
   }
   if (st == MHM_CELL_OK) {
-    double dmin = 1e300, dmax = 0.0;
-    for (int k = tid; k < n; k += blockDim.x) {
-      const double d = (double)band[(size_t)k * bw];
-      dmin = fmin(dmin, d);
-      dmax = fmax(dmax, d);
-    }
-    dmin = block_min(dmin, red);
-    dmax = block_max(dmax, red);
     const double eps = (sizeof(T) == 8) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
     if (dmin <= eps * n * dmax) st = MHM_CELL_RANK_DEFICIENT;
-    for (int k = tid; k < n; k += blockDim.x) band[(size_t)k * bw] = T(1) / band[(size_t)k * bw];
   }
   __syncthreads();
 
   // ---- right-hand sides, refinement ------------------------------------------
   const int np1 = n + 1;
-  // b norms (warp per column, deterministic)
   const int lane = tid & 31, wid = tid >> 5, nwarps = blockDim.x >> 5;
+  // b norms (warp per column, deterministic)
   for (int col = wid; col < w; col += nwarps) {
     double s2 = 0.0;
     for (int i = lane; i < n; i += 32) {
@@ -408,44 +439,101 @@ __global__ void __launch_bounds__(kThreads) q1_condense_kernel(const Q1Args a) {
   }
   __syncthreads();
   int it = 0;
+  const int nrw = nnx * w;
   if (st == MHM_CELL_OK) {
     for (it = 0; it < a.max_refine; ++it) {
-      // (1) approximate inverse of the augmented operator, one thread per column
-      for (int col = tid; col < w; col += blockDim.x) {
-        if (conv[col]) continue;
-        T* v = work + (size_t)col * np1;
+      // (1) approximate inverse of the augmented operator on every residual column:
+      //     mu = sum(v) / zc; y = D Apin^-1 D (v - c mu); x = y + (v_n - c.y) / zc; x_n = mu
+      for (int col = wid; col < w; col += nwarps) {
+        const T* v = work + (size_t)col * np1;
         double sum = 0.0;
-        for (int i = 0; i < n; ++i) sum += (double)v[i];
-        const double mu = sum / zc;
-        const double rmu = (double)v[n];
-        for (int i = 0; i < n; ++i) {  // forward: z_i = (v_i - sum a_{i,i-d} z_{i-d}) / d_i
-          const T* row = band + (size_t)i * bw;
-          T acc = T(((double)v[i] - ctil[i] * mu) * dsc[i]);
-          const int dm = i < b ? i : b;
-          for (int dd = 1; dd <= dm; ++dd) acc -= row[dd] * v[i - dd];
-          v[i] = acc * row[0];
+        for (int i = lane; i < n; i += 32) sum += (double)v[i];
+        sum = warp_sum(sum);
+        if (lane == 0) cmu[col] = sum / zc;
+      }
+      __syncthreads();
+      for (int idx = tid; idx < w * n; idx += blockDim.x) {
+        const int col = idx / n, i = idx - col * n;
+        T* v = work + (size_t)col * np1 + i;
+        *v = T(((double)*v - ctil[i] * cmu[col]) * dsc[i]);
+      }
+      __syncthreads();
+      // block forward: z_y = S_y^-1 (v_y - B_y z_{y-1})
+      for (int y = 0; y < nny; ++y) {
+        for (int idx = tid; idx < nrw; idx += blockDim.x) {
+          const int col = idx / nnx, r = idx - col * nnx;
+          const int ir = y * nnx + r;
+          const T* v = work + (size_t)col * np1;
+          T acc = v[ir];
+          if (y > 0) {
+#pragma unroll
+            for (int p = 0; p < 3; ++p) {
+              const int b = r - 1 + p;
+              if (b >= 0 && b < nnx) acc -= cdn[3 * ir + p] * v[ir - nnx - r + b];
+            }
+          }
+          tmp[col * nnx + r] = acc;
         }
-        for (int i = n - 1; i >= 0; --i) {  // backward: x_i = z_i - (1/d_i) sum a_{i+d,i} x_{i+d}
-          const int dm = (n - 1 - i) < b ? (n - 1 - i) : b;
+        __syncthreads();
+        const T* S = sinv + (size_t)y * nb;
+        for (int idx = tid; idx < nrw; idx += blockDim.x) {
+          const int col = idx / nnx, r = idx - col * nnx;
+          const T* tc = tmp + col * nnx;
+          const T* sr = S + r * nnx;
+          T acc0 = T(0), acc1 = T(0);
+          int b = 0;
+          for (; b + 1 < nnx; b += 2) {
+            acc0 += sr[b] * tc[b];
+            acc1 += sr[b + 1] * tc[b + 1];
+          }
+          if (b < nnx) acc0 += sr[b] * tc[b];
+          work[(size_t)col * np1 + y * nnx + r] = acc0 + acc1;
+        }
+        __syncthreads();
+      }
+      // block backward: x_y = z_y - S_y^-1 B_{y+1}^T x_{y+1}
+      for (int y = nny - 2; y >= 0; --y) {
+        for (int idx = tid; idx < nrw; idx += blockDim.x) {
+          const int col = idx / nnx, r = idx - col * nnx;
+          const T* v = work + (size_t)col * np1 + (y + 1) * nnx;
+          const int base = 3 * (y + 1) * nnx;
           T acc = T(0);
-          for (int dd = 1; dd <= dm; ++dd) acc += band[(size_t)(i + dd) * bw + dd] * v[i + dd];
-          v[i] -= band[(size_t)i * bw] * acc;
+          // B_{y+1}[q][r] sits in the stencil row of node q = r+1, r, r-1 of line y+1
+          if (r + 1 < nnx) acc += cdn[base + 3 * (r + 1) + 0] * v[r + 1];
+          acc += cdn[base + 3 * r + 1] * v[r];
+          if (r > 0) acc += cdn[base + 3 * (r - 1) + 2] * v[r - 1];
+          tmp[col * nnx + r] = acc;
         }
-        double cy = 0.0;
-        for (int i = 0; i < n; ++i) {
-          const double y = (double)v[i] * dsc[i];
-          v[i] = T(y);
-          cy += ctil[i] * y;
+        __syncthreads();
+        const T* S = sinv + (size_t)y * nb;
+        for (int idx = tid; idx < nrw; idx += blockDim.x) {
+          const int col = idx / nnx, r = idx - col * nnx;
+          const T* tc = tmp + col * nnx;
+          const T* sr = S + r * nnx;
+          T acc0 = T(0), acc1 = T(0);
+          int b = 0;
+          for (; b + 1 < nnx; b += 2) {
+            acc0 += sr[b] * tc[b];
+            acc1 += sr[b + 1] * tc[b + 1];
+          }
+          if (b < nnx) acc0 += sr[b] * tc[b];
+          work[(size_t)col * np1 + y * nnx + r] -= acc0 + acc1;
         }
-        const double shift = (rmu - cy) / zc;
-        for (int i = 0; i < n; ++i) v[i] = T((double)v[i] + shift);
-        v[n] = T(mu);
+        __syncthreads();
+      }
+      // kernel shift per column
+      for (int col = wid; col < w; col += nwarps) {
+        const T* v = work + (size_t)col * np1;
+        double cyv = 0.0;
+        for (int i = lane; i < n; i += 32) cyv = fma(ctil[i], (double)v[i] * dsc[i], cyv);
+        cyv = warp_sum(cyv);
+        if (lane == 0) cshift[col] = ((double)v[n] - cyv) / zc;
       }
       __syncthreads();
       // (2) x += correction (FP64, global)
       for (int idx = tid; idx < w * np1; idx += blockDim.x) {
-        const int col = idx / np1;
-        if (!conv[col]) xg[idx] += (double)work[idx];
+        const int col = idx / np1, i = idx - col * np1;
+        if (!conv[col]) xg[idx] += (i < n) ? (double)work[idx] * dsc[i] + cshift[col] : cmu[col];
       }
       __syncthreads();
       // (3) residual r = b - K x in FP64, warp per column
@@ -634,12 +722,11 @@ int fill_args(const mhm_q1_problem* p, int precision, Q1Args& a) {
   if (!p->coupling_table || !p->side_sign || !p->side_orient) return MHM_ERR_ARGUMENT;
   a = Q1Args{};
   a.nx = p->macro_nx; a.ny = p->macro_ny; a.rx = p->rx; a.ry = p->ry;
-  a.nnx = a.rx + 1; a.nny = a.ry + 1; a.n = a.nnx * a.nny; a.b = a.nnx + 1;
+  a.nnx = a.rx + 1; a.nny = a.ry + 1; a.n = a.nnx * a.nny;
   a.tfh = p->tf_h; a.tfv = p->tf_v; a.t = 2 * (a.tfh + a.tfv); a.w = a.t + 2;
   a.kmax = (a.rx > a.ry ? a.rx : a.ry) + 1;
   a.jmax = a.tfh > a.tfv ? a.tfh : a.tfv;
-  a.npairs = a.b * (a.b + 1) / 2;
-  if (a.b > 255) return MHM_ERR_UNSUPPORTED;
+  if (a.w > 32 * (kThreads / 32)) return MHM_ERR_UNSUPPORTED;
   a.NYf = a.ny * a.ry;
   a.hx = p->hx; a.hy = p->hy; a.area = p->hx * p->hy;
   a.table = p->coupling_table; a.sign = p->side_sign; a.orient = p->side_orient;
@@ -650,15 +737,18 @@ int fill_args(const mhm_q1_problem* p, int precision, Q1Args& a) {
   gauss01(a.qorder, a.gpt, a.gwt);
   const size_t tsz = precision == MHM_PRECISION_FP64 ? 8 : 4;
   size_t off = 0;
-  a.off_band = off; off = align16(off + (size_t)a.n * (a.b + 1) * tsz);
+  const size_t nb = (size_t)a.nnx * a.nnx;
+  a.off_sinv = off; off = align16(off + (size_t)a.nny * nb * tsz);
+  a.off_gj = off; off = align16(off + 2 * nb * tsz);
+  a.off_cpl = off; off = align16(off + (size_t)5 * a.n * tsz);
+  a.off_tmp = off; off = align16(off + (size_t)a.nnx * a.w * tsz);
   a.off_sten = off; off = align16(off + (size_t)5 * a.n * 8);
   a.off_vec = off; off = align16(off + (size_t)4 * a.n * 8);
   a.off_work = off;
   const size_t work = (size_t)a.w * (a.n + 1) * tsz;
   const size_t asm_tmp = (size_t)7 * a.rx * a.ry * 8;
   off = align16(off + (work > asm_tmp ? work : asm_tmp));
-  a.off_pairs = off; off = align16(off + 2 * (size_t)a.npairs);
-  a.off_misc = off; off = align16(off + (32 + 2 * (size_t)a.w) * 8 + ((size_t)a.w + 1) * 4);
+  a.off_misc = off; off = align16(off + (32 + 4 * (size_t)a.w) * 8 + ((size_t)a.w + 1) * 4);
   a.smem = off;
   return MHM_OK;
 }
