@@ -34,7 +34,9 @@
 namespace mhm {
 namespace {
 
-constexpr int kThreads = 256;
+// 7 warps: the 14 right-hand-side columns of P2 traces in two passes, and room for
+// two (FP64) or three (binary32 factor) macrocells per SM.
+constexpr int kThreads = 224;
 constexpr int kMaxQuad = 8;
 
 struct Q1Args {
@@ -61,7 +63,7 @@ struct Q1Args {
   int32_t* status;
   int32_t* iters;
   // shared-memory carve-up (byte offsets)
-  size_t off_sinv, off_gj, off_cpl, off_tmp, off_sten, off_vec, off_work, off_misc, smem;
+  size_t off_sinv, off_gj, off_cpl, off_cb, off_sten, off_vec, off_warp, off_misc, smem;
 };
 
 // Closed form of the Q1 element Gram entry int grad(phi_a) . K grad(phi_c) on an
@@ -113,27 +115,23 @@ __device__ __forceinline__ double coupling(const Q1Args& a, int cell, int s, int
   return a.sign[cell * 4 + s] * v;
 }
 
-// Entry i of right-hand-side column col: [f | B | A 1].
-__device__ __forceinline__ double rhs_entry(const Q1Args& a, int cell, int col, int i,
-                                            const double* fvec, const double* az) {
-  if (i >= a.n) return 0.0;
+// Entry i of right-hand-side column col: [f | B | A 1]; cb[j][k] holds the coupling
+// of trace column j at node k of its side.
+__device__ __forceinline__ double rhs_value(const Q1Args& a, int col, int i, const double* fvec,
+                                            const double* az, const double* cb) {
   if (col == 0) return fvec[i];
   if (col == a.w - 1) return az[i];
-  const Side sd = trace_side(a, col - 1);
+  const int j = col - 1;
+  const Side sd = trace_side(a, j);
   const int ix = i % a.nnx, iy = i / a.nnx;
-  int k = -1;
+  int k;
   switch (sd.s) {
     case 0: k = (iy == 0) ? ix : -1; break;
     case 1: k = (ix == a.nnx - 1) ? iy : -1; break;
     case 2: k = (iy == a.nny - 1) ? ix : -1; break;
     default: k = (ix == 0) ? iy : -1; break;
   }
-  return k < 0 ? 0.0 : coupling(a, cell, sd.s, k, sd.q);
-}
-
-// Lower 9-point stencil slots of node i: 0 diag, 1 (i-1), 2 (i-nnx+1), 3 (i-nnx), 4 (i-nnx-1).
-__device__ __forceinline__ int stencil_offset(const Q1Args& a, int slot) {
-  return slot == 0 ? 0 : slot == 1 ? 1 : slot == 2 ? a.nnx - 1 : slot == 3 ? a.nnx : a.nnx + 1;
+  return k < 0 ? 0.0 : cb[j * a.kmax + k];
 }
 
 // (A x)_i from the lower stencil of i and the lower stencils of its upper neighbours.
@@ -155,47 +153,172 @@ __device__ __forceinline__ double stencil_apply(const Q1Args& a, const double* s
   return acc;
 }
 
+template <typename T>
+__device__ __forceinline__ T shfl(T v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+
+// Block LDL^T of the line-block operator by one warp, lane c holding column c of the
+// current block in registers: S_y = Adiag_y - B_y S_{y-1}^-1 B_y^T, then S_y^-1 by
+// Gauss-Jordan without pivoting (SPD); its pivots are those of the LDL^T of the
+// whole matrix.  S_y^-1 is stored row-major in sinv.
+template <typename T, int NNX>
+__device__ void factor_lines_warp(int nny, const T* dg, const T* dl, const T* cdn, T* sinv, double& dmin,
+                                  double& dmax, int& bad) {
+  const int lane = threadIdx.x & 31;
+  const int c = lane < NNX ? lane : NNX - 1;  // idle lanes mirror the last column
+  T col[NNX];
+  dmin = 1e300;
+  dmax = 0.0;
+  bad = 0;
+  for (int y = 0; y < nny; ++y) {
+    const int base = y * NNX;
+    if (y > 0) {
+      // w[b] = sum_{d = c-1..c+1} S_{y-1}^-1[b][d] B_y[c][d]
+      const T bcm = c > 0 ? cdn[3 * (base + c) + 0] : T(0);
+      const T bc0 = cdn[3 * (base + c) + 1];
+      const T bcp = c < NNX - 1 ? cdn[3 * (base + c) + 2] : T(0);
+      T wv[NNX];
+#pragma unroll
+      for (int b = 0; b < NNX; ++b) {
+        const T lft = __shfl_up_sync(0xffffffffu, col[b], 1);
+        const T rgt = __shfl_down_sync(0xffffffffu, col[b], 1);
+        wv[b] = lft * bcm + col[b] * bc0 + rgt * bcp;
+      }
+#pragma unroll
+      for (int r = 0; r < NNX; ++r) {
+        T v = (r == c) ? dg[base + r] : (c == r - 1) ? dl[base + r] : (r == c - 1) ? dl[base + c] : T(0);
+        T acc = cdn[3 * (base + r) + 1] * wv[r];
+        if (r > 0) acc += cdn[3 * (base + r) + 0] * wv[r - 1];
+        if (r < NNX - 1) acc += cdn[3 * (base + r) + 2] * wv[r + 1];
+        col[r] = v - acc;
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < NNX; ++r)
+        col[r] = (r == c) ? dg[r] : (c == r - 1) ? dl[r] : (r == c - 1) ? dl[c] : T(0);
+    }
+#pragma unroll
+    for (int k = 0; k < NNX; ++k) {
+      const T d = shfl(col[k], k);
+      if (!(d > T(0))) bad = 1;
+      dmin = fmin(dmin, (double)d);
+      dmax = fmax(dmax, (double)d);
+      const T inv = T(1) / d;
+      const T f = col[k] * inv;
+#pragma unroll
+      for (int i = 0; i < NNX; ++i) {
+        const T pk = shfl(col[i], k);
+        if (i == k) col[i] = (c == k) ? inv : f;
+        else col[i] = (c == k) ? -pk * inv : col[i] - pk * f;
+      }
+    }
+    if (lane < NNX) {
+#pragma unroll
+      for (int r = 0; r < NNX; ++r) sinv[(size_t)y * NNX * NNX + r * NNX + c] = col[r];
+    }
+  }
+}
+
+// The same factorization by the whole block in shared memory (any line length):
+// one barrier per Gauss-Jordan pivot, ping-pong buffers gj0 / gj1.
+template <typename T>
+__device__ void factor_lines_block(int nnx, int nny, const T* dg, const T* dl, const T* cdn, T* sinv, T* gj0,
+                                   T* gj1, double& dmin, double& dmax, int& bad) {
+  const int nb = nnx * nnx;
+  dmin = 1e300;
+  dmax = 0.0;
+  bad = 0;
+  for (int y = 0; y < nny && !bad; ++y) {
+    const T* prev = sinv + (size_t)(y - 1) * nb;
+    for (int e = threadIdx.x; e < nb; e += blockDim.x) {
+      const int r = e / nnx, c = e - r * nnx;
+      const int ir = y * nnx + r, ic = y * nnx + c;
+      T v = (r == c) ? dg[ir] : (c == r - 1) ? dl[ir] : (r == c - 1) ? dl[ic] : T(0);
+      if (y > 0) {
+        T acc = T(0);
+        for (int p = 0; p < 3; ++p) {
+          const int b = r - 1 + p;
+          if (b < 0 || b >= nnx) continue;
+          const T brb = cdn[3 * ir + p];
+          for (int q = 0; q < 3; ++q) {
+            const int d = c - 1 + q;
+            if (d < 0 || d >= nnx) continue;
+            acc += brb * prev[b * nnx + d] * cdn[3 * ic + q];
+          }
+        }
+        v -= acc;
+      }
+      gj0[e] = v;
+    }
+    __syncthreads();
+    T* cur = gj0;
+    T* nxt = gj1;
+    for (int k = 0; k < nnx; ++k) {
+      const T d = cur[k * nnx + k];
+      if (!(d > T(0))) { bad = 1; break; }  // uniform: every thread reads d
+      dmin = fmin(dmin, (double)d);
+      dmax = fmax(dmax, (double)d);
+      const T inv = T(1) / d;
+      T* dst = (k == nnx - 1) ? sinv + (size_t)y * nb : nxt;
+      for (int e = threadIdx.x; e < nb; e += blockDim.x) {
+        const int r = e / nnx, c = e - r * nnx;
+        T v;
+        if (r == k) v = (c == k) ? inv : cur[e] * inv;
+        else if (c == k) v = -cur[r * nnx + k] * inv;
+        else v = cur[e] - cur[r * nnx + k] * inv * cur[k * nnx + c];
+        dst[e] = v;
+      }
+      __syncthreads();
+      T* sw = cur; cur = nxt; nxt = sw;
+    }
+  }
+}
+
 // Minimum resident CTAs per SM for the factor precision (register budget).
 template <typename T>
 struct Occupancy {
   static constexpr int value = sizeof(T) == 8 ? 2 : 3;
 };
 
-template <typename T>
+// NNX > 0: the factorization runs in one warp's registers for lines of NNX nodes;
+// NNX = 0: any line length, factorization in shared memory by the whole block.
+template <typename T, int NNX>
 __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_kernel(const Q1Args a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int cell = blockIdx.x;
   const int tid = threadIdx.x;
-  const int n = a.n, nnx = a.nnx, nny = a.nny, w = a.w, t = a.t;
-  const int nb = nnx * nnx;
-  T* sinv = reinterpret_cast<T*>(smem + a.off_sinv);  // nny blocks of nnx x nnx
-  T* gj0 = reinterpret_cast<T*>(smem + a.off_gj);     // Gauss-Jordan ping-pong
+  const int n = a.n, nnx = NNX > 0 ? NNX : a.nnx, nny = a.nny, w = a.w, t = a.t;
+  const int nb = nnx * nnx, np1 = n + 1;
+  const int lane = tid & 31, wid = tid >> 5, nwarps = blockDim.x >> 5;
+  T* sinv = reinterpret_cast<T*>(smem + a.off_sinv);  // nny blocks of nnx x nnx, row-major
+  T* gj0 = reinterpret_cast<T*>(smem + a.off_gj);     // Gauss-Jordan ping-pong (NNX = 0)
   T* gj1 = gj0 + nb;
   T* cdn = reinterpret_cast<T*>(smem + a.off_cpl);    // (n, 3): to (y-1, x-1), (y-1, x), (y-1, x+1)
   T* dg = cdn + 3 * n;                                // (n): scaled diagonal
   T* dl = dg + n;                                     // (n): scaled coupling to (y, x-1)
-  T* tmp = reinterpret_cast<T*>(smem + a.off_tmp);    // (nnx, w)
+  double* cb = reinterpret_cast<double*>(smem + a.off_cb);  // (t, kmax) boundary couplings
+  double* zb = cb + (size_t)t * a.kmax;                     // (t): sum of each column's couplings
   double* sten = reinterpret_cast<double*>(smem + a.off_sten);
   double* fvec = reinterpret_cast<double*>(smem + a.off_vec);
   double* az = fvec + n;
   double* ctil = az + n;
   double* dsc = ctil + n;
-  T* work = reinterpret_cast<T*>(smem + a.off_work);
-  double* kel = reinterpret_cast<double*>(smem + a.off_work);  // aliases work during assembly
+  // per-warp column buffers: x (n+1 doubles) and residual / solve vector (n+1 T)
+  const size_t wstride = align16((size_t)np1 * 8) + align16((size_t)np1 * sizeof(T));
+  double* xw = reinterpret_cast<double*>(smem + a.off_warp + wid * wstride);
+  T* rw = reinterpret_cast<T*>(smem + a.off_warp + wid * wstride + align16((size_t)np1 * 8));
+  double* kel = reinterpret_cast<double*>(smem + a.off_warp);  // aliases the warp buffers
   double* fel = kel + 3 * a.rx * a.ry;
   double* red = reinterpret_cast<double*>(smem + a.off_misc);
-  double* bnorm = red + 32;
-  double* rnorm = bnorm + w;
-  double* cmu = rnorm + w;
-  double* cshift = cmu + w;
-  int* conv = reinterpret_cast<int*>(cshift + w);
-  int* flag = conv + w;
+  double* rnorm = red + 32;
+  int* cstat = reinterpret_cast<int*>(rnorm + w);  // per column: 1 converged, 2 non-finite
+  int* citer = cstat + w;
+  int* flag = citer + w;
 
   const int cx = cell % a.nx, cy = cell / a.nx;
   const int ne = a.rx * a.ry;
-  double* xg = a.sol + (size_t)cell * w * (n + 1);
+  double* xg = a.sol + (size_t)cell * w * np1;
 
-  // ---- element coefficients and element loads --------------------------------
+  // ---- element coefficients and element loads; boundary coupling table ---------
   for (int e = tid; e < ne; e += blockDim.x) {
     const int ex = e % a.rx, ey = e / a.rx;
     const size_t g = (size_t)(cx * a.rx + ex) * a.NYf + (cy * a.ry + ey);
@@ -229,16 +352,26 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
     }
     for (int c = 0; c < 4; ++c) fel[4 * e + c] = fe[c];
   }
-  if (tid < w) { conv[tid] = 0; }
+  for (int idx = tid; idx < t * a.kmax; idx += blockDim.x) {
+    const int j = idx / a.kmax, k = idx - j * a.kmax;
+    const Side sd = trace_side(a, j);
+    cb[idx] = k < side_len(a, sd.s) ? coupling(a, cell, sd.s, k, sd.q) : 0.0;
+  }
   if (tid == 0) flag[0] = 0;
   __syncthreads();
+  for (int j = tid; j < t; j += blockDim.x) {
+    double acc = 0.0;
+    const int len = side_len(a, trace_side(a, j).s);
+    for (int k = 0; k < len; ++k) acc += cb[j * a.kmax + k];
+    zb[j] = acc;
+  }
 
   // ---- node-wise gather of the lower stencil, load and constraint -------------
   const double rxy = a.hy / a.hx, ryx = a.hx / a.hy;
   double amax = 0.0, fro = 0.0, cmax = 0.0;
   for (int i = tid; i < n; i += blockDim.x) {
     const int ix = i % nnx, iy = i / nnx;
-    double s[5] = {0, 0, 0, 0, 0};
+    double sv[5] = {0, 0, 0, 0, 0};
     double f = 0.0;
     int count = 0;
     // candidate elements: E00 (ix-1,iy-1) local 3; E10 (ix,iy-1) local 2;
@@ -247,45 +380,45 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
     if (l && d) {
       const int e = (iy - 1) * a.rx + ix - 1;
       const double* k = kel + 3 * e;
-      s[0] += elem_k(k[0], k[1], k[2], rxy, ryx, 3, 3);
-      s[1] += elem_k(k[0], k[1], k[2], rxy, ryx, 3, 2);
-      s[3] += elem_k(k[0], k[1], k[2], rxy, ryx, 3, 1);
-      s[4] += elem_k(k[0], k[1], k[2], rxy, ryx, 3, 0);
+      sv[0] += elem_k(k[0], k[1], k[2], rxy, ryx, 3, 3);
+      sv[1] += elem_k(k[0], k[1], k[2], rxy, ryx, 3, 2);
+      sv[3] += elem_k(k[0], k[1], k[2], rxy, ryx, 3, 1);
+      sv[4] += elem_k(k[0], k[1], k[2], rxy, ryx, 3, 0);
       f += fel[4 * e + 3];
       ++count;
     }
     if (r && d) {
       const int e = (iy - 1) * a.rx + ix;
       const double* k = kel + 3 * e;
-      s[0] += elem_k(k[0], k[1], k[2], rxy, ryx, 2, 2);
-      s[2] += elem_k(k[0], k[1], k[2], rxy, ryx, 2, 1);
-      s[3] += elem_k(k[0], k[1], k[2], rxy, ryx, 2, 0);
+      sv[0] += elem_k(k[0], k[1], k[2], rxy, ryx, 2, 2);
+      sv[2] += elem_k(k[0], k[1], k[2], rxy, ryx, 2, 1);
+      sv[3] += elem_k(k[0], k[1], k[2], rxy, ryx, 2, 0);
       f += fel[4 * e + 2];
       ++count;
     }
     if (l && u) {
       const int e = iy * a.rx + ix - 1;
       const double* k = kel + 3 * e;
-      s[0] += elem_k(k[0], k[1], k[2], rxy, ryx, 1, 1);
-      s[1] += elem_k(k[0], k[1], k[2], rxy, ryx, 1, 0);
+      sv[0] += elem_k(k[0], k[1], k[2], rxy, ryx, 1, 1);
+      sv[1] += elem_k(k[0], k[1], k[2], rxy, ryx, 1, 0);
       f += fel[4 * e + 1];
       ++count;
     }
     if (r && u) {
       const int e = iy * a.rx + ix;
       const double* k = kel + 3 * e;
-      s[0] += elem_k(k[0], k[1], k[2], rxy, ryx, 0, 0);
+      sv[0] += elem_k(k[0], k[1], k[2], rxy, ryx, 0, 0);
       f += fel[4 * e + 0];
       ++count;
     }
-    for (int q = 0; q < 5; ++q) sten[5 * i + q] = s[q];
+    for (int q = 0; q < 5; ++q) sten[5 * i + q] = sv[q];
     fvec[i] = f;
     ctil[i] = count * (a.area * 0.25);
-    amax = fmax(amax, fabs(s[0]));
-    fro += s[0] * s[0];
+    amax = fmax(amax, fabs(sv[0]));
+    fro += sv[0] * sv[0];
     for (int q = 1; q < 5; ++q) {
-      amax = fmax(amax, fabs(s[q]));
-      fro += 2.0 * s[q] * s[q];
+      amax = fmax(amax, fabs(sv[q]));
+      fro += 2.0 * sv[q] * sv[q];
     }
     cmax = fmax(cmax, ctil[i]);
   }
@@ -295,13 +428,13 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
   int nonzero = 0, nonfinite = 0;
   for (int i = tid; i < n; i += blockDim.x) {
     const int ix = i % nnx, iy = i / nnx;
-    const double* s = sten + 5 * i;
+    const double* sv = sten + 5 * i;
     double hi = 0.0, lo = 0.0;
-    dd_add(hi, lo, s[0]);
-    if (ix > 0) dd_add(hi, lo, s[1]);
-    if (iy > 0 && ix < nnx - 1) dd_add(hi, lo, s[2]);
-    if (iy > 0) dd_add(hi, lo, s[3]);
-    if (iy > 0 && ix > 0) dd_add(hi, lo, s[4]);
+    dd_add(hi, lo, sv[0]);
+    if (ix > 0) dd_add(hi, lo, sv[1]);
+    if (iy > 0 && ix < nnx - 1) dd_add(hi, lo, sv[2]);
+    if (iy > 0) dd_add(hi, lo, sv[3]);
+    if (iy > 0 && ix > 0) dd_add(hi, lo, sv[4]);
     if (ix < nnx - 1) dd_add(hi, lo, sten[5 * (i + 1) + 1]);
     if (iy < nny - 1) {
       if (ix > 0) dd_add(hi, lo, sten[5 * (i + nnx - 1) + 2]);
@@ -346,290 +479,190 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
   for (int i = tid; i < n; i += blockDim.x) {
     const int ix = i % nnx, iy = i / nnx;
     const double si = dsc[i];
-    const double* s = sten + 5 * i;
-    dg[i] = T(s[0] * (i == pin ? 2.0 : 1.0) * si * si);
-    dl[i] = ix > 0 ? T(s[1] * si * dsc[i - 1]) : T(0);
-    cdn[3 * i + 0] = (iy > 0 && ix > 0) ? T(s[4] * si * dsc[i - nnx - 1]) : T(0);
-    cdn[3 * i + 1] = iy > 0 ? T(s[3] * si * dsc[i - nnx]) : T(0);
-    cdn[3 * i + 2] = (iy > 0 && ix < nnx - 1) ? T(s[2] * si * dsc[i - nnx + 1]) : T(0);
+    const double* sv = sten + 5 * i;
+    dg[i] = T(sv[0] * (i == pin ? 2.0 : 1.0) * si * si);
+    dl[i] = ix > 0 ? T(sv[1] * si * dsc[i - 1]) : T(0);
+    cdn[3 * i + 0] = (iy > 0 && ix > 0) ? T(sv[4] * si * dsc[i - nnx - 1]) : T(0);
+    cdn[3 * i + 1] = iy > 0 ? T(sv[3] * si * dsc[i - nnx]) : T(0);
+    cdn[3 * i + 2] = (iy > 0 && ix < nnx - 1) ? T(sv[2] * si * dsc[i - nnx + 1]) : T(0);
     if (st == MHM_CELL_OK && !(si > 0.0)) flag[0] = MHM_CELL_SINGULAR_PIVOT;
   }
   __syncthreads();
   if (st == MHM_CELL_OK) st = flag[0];
 
-  // ---- block LDL^T: S_y^-1 for every line y ------------------------------------
-  // S_y[a][c] = Adiag_y[a][c] - sum_{b,d} B_y[a][b] S_{y-1}^-1[b][d] B_y[c][d], B_y the
-  // (tridiagonal) coupling of line y to line y-1; inverted by Gauss-Jordan without
-  // pivoting (SPD), whose pivots are those of the LDL^T of the whole matrix.
-  double dmin = 1e300, dmax = 0.0;
+  // ---- block LDL^T of the line blocks ------------------------------------------
   if (st == MHM_CELL_OK) {
-    for (int y = 0; y < nny && st == MHM_CELL_OK; ++y) {
-      const T* prev = sinv + (size_t)(y - 1) * nb;
-      for (int e = tid; e < nb; e += blockDim.x) {
-        const int r = e / nnx, c = e - r * nnx;
-        const int ir = y * nnx + r, ic = y * nnx + c;
-        T v = T(0);
-        if (r == c) v = dg[ir];
-        else if (c == r - 1) v = dl[ir];
-        else if (r == c - 1) v = dl[ic];
-        if (y > 0) {
-          T acc = T(0);
-#pragma unroll
-          for (int p = 0; p < 3; ++p) {
-            const int b = r - 1 + p;
-            if (b < 0 || b >= nnx) continue;
-            const T brb = cdn[3 * ir + p];
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-              const int d = c - 1 + q;
-              if (d < 0 || d >= nnx) continue;
-              acc += brb * prev[b * nnx + d] * cdn[3 * ic + q];
-            }
-          }
-          v -= acc;
+    double dmin, dmax;
+    int bad;
+    if constexpr (NNX > 0) {
+      if (wid == 0) {
+        factor_lines_warp<T, NNX>(nny, dg, dl, cdn, sinv, dmin, dmax, bad);
+        if (lane == 0) {
+          const double eps = (sizeof(T) == 8) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
+          flag[0] = bad ? MHM_CELL_SINGULAR_PIVOT : (dmin <= eps * n * dmax ? MHM_CELL_RANK_DEFICIENT : 0);
         }
-        gj0[e] = v;
       }
       __syncthreads();
-      T* cur = gj0;
-      T* nxt = gj1;
-      for (int k = 0; k < nnx; ++k) {
-        const T d = cur[k * nnx + k];
-        if (!(d > T(0))) { st = MHM_CELL_SINGULAR_PIVOT; break; }  // uniform: every thread reads d
-        dmin = fmin(dmin, (double)d);
-        dmax = fmax(dmax, (double)d);
-        const T inv = T(1) / d;
-        T* dst = (k == nnx - 1) ? sinv + (size_t)y * nb : nxt;
-        for (int e = tid; e < nb; e += blockDim.x) {
-          const int r = e / nnx, c = e - r * nnx;
-          T v;
-          if (r == k) v = (c == k) ? inv : cur[e] * inv;
-          else if (c == k) v = -cur[r * nnx + k] * inv;
-          else v = cur[e] - cur[r * nnx + k] * inv * cur[k * nnx + c];
-          dst[e] = v;
-        }
-        __syncthreads();
-        T* sw = cur; cur = nxt; nxt = sw;
-      }
+      st = flag[0];
+    } else {
+      factor_lines_block<T>(nnx, nny, dg, dl, cdn, sinv, gj0, gj1, dmin, dmax, bad);
+      const double eps = (sizeof(T) == 8) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
+      if (bad) st = MHM_CELL_SINGULAR_PIVOT;
+      else if (dmin <= eps * n * dmax) st = MHM_CELL_RANK_DEFICIENT;
+      __syncthreads();
     }
   }
-  if (st == MHM_CELL_OK) {
-    const double eps = (sizeof(T) == 8) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
-    if (dmin <= eps * n * dmax) st = MHM_CELL_RANK_DEFICIENT;
-  }
-  __syncthreads();
 
-  // ---- right-hand sides, refinement ------------------------------------------
-  const int np1 = n + 1;
-  const int lane = tid & 31, wid = tid >> 5, nwarps = blockDim.x >> 5;
-  // b norms (warp per column, deterministic)
+  // ---- refinement, one warp per right-hand-side column ---------------------------
+  // x += y + (r_n - c.y) / zc, x_n += mu with mu = sum(r) / zc and y = D Apin^-1 D
+  // (r - c mu), until ||b - K x|| <= tol ||b|| (columnwise, FP64 residual).
+  double fz = 0.0;
+  for (int i = lane; i < n; i += 32) fz += fvec[i];
+  fz = warp_sum(fz);
+  const int t1 = t + 1;
   for (int col = wid; col < w; col += nwarps) {
     double s2 = 0.0;
     for (int i = lane; i < n; i += 32) {
-      const double v = rhs_entry(a, cell, col, i, fvec, az);
-      s2 += v * v;
+      const double bv = rhs_value(a, col, i, fvec, az, cb);
+      rw[i] = T(bv);
+      xw[i] = 0.0;
+      s2 += bv * bv;
     }
+    if (lane == 0) { rw[n] = T(0); xw[n] = 0.0; }
     s2 = warp_sum(s2);
-    if (lane == 0) { bnorm[col] = sqrt(s2); conv[col] = (s2 == 0.0); }
-  }
-  for (int idx = tid; idx < w * np1; idx += blockDim.x) {
-    const int col = idx / np1, i = idx % np1;
-    xg[idx] = 0.0;
-    work[idx] = T(rhs_entry(a, cell, col, i, fvec, az));
-  }
-  __syncthreads();
-  int it = 0;
-  const int nrw = nnx * w;
-  if (st == MHM_CELL_OK) {
-    for (it = 0; it < a.max_refine; ++it) {
-      // (1) approximate inverse of the augmented operator on every residual column:
-      //     mu = sum(v) / zc; y = D Apin^-1 D (v - c mu); x = y + (v_n - c.y) / zc; x_n = mu
-      for (int col = wid; col < w; col += nwarps) {
-        const T* v = work + (size_t)col * np1;
-        double sum = 0.0;
-        for (int i = lane; i < n; i += 32) sum += (double)v[i];
-        sum = warp_sum(sum);
-        if (lane == 0) cmu[col] = sum / zc;
-      }
-      __syncthreads();
-      for (int idx = tid; idx < w * n; idx += blockDim.x) {
-        const int col = idx / n, i = idx - col * n;
-        T* v = work + (size_t)col * np1 + i;
-        *v = T(((double)*v - ctil[i] * cmu[col]) * dsc[i]);
-      }
-      __syncthreads();
-      // block forward: z_y = S_y^-1 (v_y - B_y z_{y-1})
+    const double bn = sqrt(s2);
+    int done = (s2 == 0.0) ? 1 : 0;
+    double rn = bn;
+    int sweeps = 0;
+    __syncwarp();
+    while (st == MHM_CELL_OK && !done && sweeps < a.max_refine) {
+      double sum = 0.0;
+      for (int i = lane; i < n; i += 32) sum += (double)rw[i];
+      const double mu = warp_sum(sum) / zc;
+      const double rmu = (double)rw[n];
+      // forward: z_y = S_y^-1 (v_y - B_y z_{y-1}), lane = node of the line
+      T zprev = T(0);
       for (int y = 0; y < nny; ++y) {
-        for (int idx = tid; idx < nrw; idx += blockDim.x) {
-          const int col = idx / nnx, r = idx - col * nnx;
-          const int ir = y * nnx + r;
-          const T* v = work + (size_t)col * np1;
-          T acc = v[ir];
-          if (y > 0) {
-#pragma unroll
-            for (int p = 0; p < 3; ++p) {
-              const int b = r - 1 + p;
-              if (b >= 0 && b < nnx) acc -= cdn[3 * ir + p] * v[ir - nnx - r + b];
-            }
+        const int i = y * nnx + lane;
+        T tv = T(0);
+        if (lane < nnx) tv = T(((double)rw[i] - ctil[i] * mu) * dsc[i]);
+        if (y > 0) {
+          const T zl = __shfl_up_sync(0xffffffffu, zprev, 1);
+          const T zr = __shfl_down_sync(0xffffffffu, zprev, 1);
+          if (lane < nnx) {
+            tv -= cdn[3 * i + 1] * zprev;
+            if (lane > 0) tv -= cdn[3 * i + 0] * zl;
+            if (lane < nnx - 1) tv -= cdn[3 * i + 2] * zr;
           }
-          tmp[col * nnx + r] = acc;
         }
-        __syncthreads();
-        const T* S = sinv + (size_t)y * nb;
-        for (int idx = tid; idx < nrw; idx += blockDim.x) {
-          const int col = idx / nnx, r = idx - col * nnx;
-          const T* tc = tmp + col * nnx;
-          const T* sr = S + r * nnx;
-          T acc0 = T(0), acc1 = T(0);
-          int b = 0;
-          for (; b + 1 < nnx; b += 2) {
-            acc0 += sr[b] * tc[b];
-            acc1 += sr[b + 1] * tc[b + 1];
-          }
-          if (b < nnx) acc0 += sr[b] * tc[b];
-          work[(size_t)col * np1 + y * nnx + r] = acc0 + acc1;
+        const T* S = sinv + (size_t)y * nb + (lane < nnx ? lane : 0) * nnx;
+        T acc0 = T(0), acc1 = T(0);
+        int b = 0;
+        for (; b + 1 < nnx; b += 2) {
+          const T t0 = shfl(tv, b), t1v = shfl(tv, b + 1);
+          acc0 += S[b] * t0;
+          acc1 += S[b + 1] * t1v;
         }
-        __syncthreads();
+        if (b < nnx) acc0 += S[b] * shfl(tv, b);
+        zprev = acc0 + acc1;
+        if (lane < nnx) rw[i] = zprev;
       }
-      // block backward: x_y = z_y - S_y^-1 B_{y+1}^T x_{y+1}
+      // backward: x_y = z_y - S_y^-1 B_{y+1}^T x_{y+1}
+      T xnext = zprev;
       for (int y = nny - 2; y >= 0; --y) {
-        for (int idx = tid; idx < nrw; idx += blockDim.x) {
-          const int col = idx / nnx, r = idx - col * nnx;
-          const T* v = work + (size_t)col * np1 + (y + 1) * nnx;
+        const T xl = __shfl_up_sync(0xffffffffu, xnext, 1);
+        const T xr = __shfl_down_sync(0xffffffffu, xnext, 1);
+        T u = T(0);
+        if (lane < nnx) {
           const int base = 3 * (y + 1) * nnx;
-          T acc = T(0);
-          // B_{y+1}[q][r] sits in the stencil row of node q = r+1, r, r-1 of line y+1
-          if (r + 1 < nnx) acc += cdn[base + 3 * (r + 1) + 0] * v[r + 1];
-          acc += cdn[base + 3 * r + 1] * v[r];
-          if (r > 0) acc += cdn[base + 3 * (r - 1) + 2] * v[r - 1];
-          tmp[col * nnx + r] = acc;
+          u = cdn[base + 3 * lane + 1] * xnext;
+          if (lane + 1 < nnx) u += cdn[base + 3 * (lane + 1) + 0] * xr;
+          if (lane > 0) u += cdn[base + 3 * (lane - 1) + 2] * xl;
         }
-        __syncthreads();
-        const T* S = sinv + (size_t)y * nb;
-        for (int idx = tid; idx < nrw; idx += blockDim.x) {
-          const int col = idx / nnx, r = idx - col * nnx;
-          const T* tc = tmp + col * nnx;
-          const T* sr = S + r * nnx;
-          T acc0 = T(0), acc1 = T(0);
-          int b = 0;
-          for (; b + 1 < nnx; b += 2) {
-            acc0 += sr[b] * tc[b];
-            acc1 += sr[b + 1] * tc[b + 1];
-          }
-          if (b < nnx) acc0 += sr[b] * tc[b];
-          work[(size_t)col * np1 + y * nnx + r] -= acc0 + acc1;
+        const T* S = sinv + (size_t)y * nb + (lane < nnx ? lane : 0) * nnx;
+        T acc0 = T(0), acc1 = T(0);
+        int b = 0;
+        for (; b + 1 < nnx; b += 2) {
+          const T u0 = shfl(u, b), u1 = shfl(u, b + 1);
+          acc0 += S[b] * u0;
+          acc1 += S[b + 1] * u1;
         }
-        __syncthreads();
-      }
-      // kernel shift per column
-      for (int col = wid; col < w; col += nwarps) {
-        const T* v = work + (size_t)col * np1;
-        double cyv = 0.0;
-        for (int i = lane; i < n; i += 32) cyv = fma(ctil[i], (double)v[i] * dsc[i], cyv);
-        cyv = warp_sum(cyv);
-        if (lane == 0) cshift[col] = ((double)v[n] - cyv) / zc;
-      }
-      __syncthreads();
-      // (2) x += correction (FP64, global)
-      for (int idx = tid; idx < w * np1; idx += blockDim.x) {
-        const int col = idx / np1, i = idx - col * np1;
-        if (!conv[col]) xg[idx] += (i < n) ? (double)work[idx] * dsc[i] + cshift[col] : cmu[col];
-      }
-      __syncthreads();
-      // (3) residual r = b - K x in FP64, warp per column
-      for (int col = wid; col < w; col += nwarps) {
-        if (conv[col]) continue;
-        const double* x = xg + (size_t)col * np1;
-        T* v = work + (size_t)col * np1;
-        const double xm = x[n];
-        double s2 = 0.0, cr = 0.0;
-        for (int i = lane; i < n; i += 32) {
-          const double r = rhs_entry(a, cell, col, i, fvec, az) - stencil_apply(a, sten, i, x) -
-                           ctil[i] * xm;
-          v[i] = T(r);
-          s2 += r * r;
-          cr = fma(ctil[i], x[i], cr);
+        if (b < nnx) acc0 += S[b] * shfl(u, b);
+        T xv = T(0);
+        if (lane < nnx) {
+          const int i = y * nnx + lane;
+          xv = rw[i] - (acc0 + acc1);
+          rw[i] = xv;
         }
-        s2 = warp_sum(s2);
-        cr = warp_sum(cr);
-        if (lane == 0) {
-          const double rn = -cr;
-          v[n] = T(rn);
-          s2 += rn * rn;
-          rnorm[col] = sqrt(s2);
-        }
+        xnext = xv;
       }
-      __syncthreads();
-      int all = 1;
-      for (int col = 0; col < w; ++col) {
-        if (!conv[col] && !(rnorm[col] <= a.tol * bnorm[col])) all = 0;
+      __syncwarp();
+      // kernel shift and update
+      double cyv = 0.0;
+      for (int i = lane; i < n; i += 32) cyv = fma(ctil[i], (double)rw[i] * dsc[i], cyv);
+      const double shift = (rmu - warp_sum(cyv)) / zc;
+      for (int i = lane; i < n; i += 32) xw[i] += (double)rw[i] * dsc[i] + shift;
+      if (lane == 0) xw[n] += mu;
+      __syncwarp();
+      // FP64 residual of the augmented system
+      double r2 = 0.0, cr = 0.0;
+      const double xm = xw[n];
+      for (int i = lane; i < n; i += 32) {
+        const double rv = rhs_value(a, col, i, fvec, az, cb) - stencil_apply(a, sten, i, xw) - ctil[i] * xm;
+        rw[i] = T(rv);
+        r2 += rv * rv;
+        cr = fma(ctil[i], xw[i], cr);
       }
-      __syncthreads();
-      if (tid < w && !conv[tid] && rnorm[tid] <= a.tol * bnorm[tid]) conv[tid] = 1;
-      __syncthreads();
-      if (all) { ++it; break; }
+      r2 = warp_sum(r2);
+      const double rlast = -warp_sum(cr);
+      if (lane == 0) rw[n] = T(rlast);
+      rn = sqrt(r2 + rlast * rlast);
+      ++sweeps;
+      __syncwarp();
+      if (rn <= a.tol * bn) done = 1;
+      if (!isfinite(rn)) break;
     }
-    int ok = 1;
-    for (int col = 0; col < w; ++col) ok &= conv[col];
-    if (!ok) st = MHM_CELL_RESIDUAL;
-    for (int col = 0; col < w; ++col)
-      if (!isfinite(rnorm[col]) && !conv[col]) st = MHM_CELL_NONFINITE;
+    if (lane == 0) {
+      rnorm[col] = rn;
+      cstat[col] = done ? 1 : (isfinite(rn) ? 0 : 2);
+      citer[col] = sweeps;
+    }
+    // the column to HBM and its entries of the Schur block / load (contributions.py:40-47)
+    for (int i = lane; i < np1; i += 32) xg[(size_t)col * np1 + i] = xw[i];
+    double al = 0.0;
+    for (int i = lane; i < n; i += 32) {
+      const double xv = (col == w - 1) ? 1.0 - xw[i] : xw[i];
+      al = fma(az[i], xv, al);
+    }
+    al = warp_sum(al);
+    if (lane < t) {
+      const Side sd = trace_side(a, lane);
+      const int len = side_len(a, sd.s);
+      double acc = 0.0;
+      for (int k = 0; k < len; ++k) {
+        const double xv = xw[side_node(a, sd.s, k)];
+        acc = fma(cb[lane * a.kmax + k], (col == w - 1) ? 1.0 - xv : xv, acc);
+      }
+      if (col == 0) a.loads[(size_t)cell * t1 + lane] = acc;
+      else if (col == w - 1) a.blocks[(size_t)cell * t1 * t1 + lane * t1 + t] = -acc;
+      else a.blocks[(size_t)cell * t1 * t1 + lane * t1 + (col - 1)] = acc;
+    }
+    if (lane == 0) {
+      if (col == 0) a.loads[(size_t)cell * t1 + t] = al - fz;
+      else if (col == w - 1) a.blocks[(size_t)cell * t1 * t1 + t * t1 + t] = -al;
+      else a.blocks[(size_t)cell * t1 * t1 + t * t1 + (col - 1)] = -(zb[col - 1] - al);
+    }
+    __syncwarp();
   }
   __syncthreads();
-
-  // ---- Schur block and reduced load (contributions.py:40-47) ----------------
-  const int t1 = t + 1;
-  const int nout = t1 * t1 + t1;
-  const double* x0 = xg;                           // R f
-  const double* xr = xg + (size_t)(w - 1) * np1;   // R (A 1)
-  for (int e = wid; e < nout; e += nwarps) {
-    double acc = 0.0;
-    if (e < t1 * t1) {
-      const int r = e / t1, c = e % t1;
-      if (r < t) {
-        const Side sd = trace_side(a, r);
-        const int len = side_len(a, sd.s);
-        for (int k = lane; k < len; k += 32) {
-          const int node = side_node(a, sd.s, k);
-          const double bv = coupling(a, cell, sd.s, k, sd.q);
-          const double v = (c < t) ? xg[(size_t)(1 + c) * np1 + node] : (1.0 - xr[node]);
-          acc = fma(bv, v, acc);
-        }
-        acc = warp_sum(acc);
-        if (c == t) acc = -acc;
-      } else if (c < t) {
-        const Side sd = trace_side(a, c);
-        const int len = side_len(a, sd.s);
-        double zb = 0.0;
-        for (int k = lane; k < len; k += 32) zb += coupling(a, cell, sd.s, k, sd.q);
-        double al = 0.0;
-        for (int i = lane; i < n; i += 32) al = fma(az[i], xg[(size_t)(1 + c) * np1 + i], al);
-        acc = -(warp_sum(zb) - warp_sum(al));
-      } else {
-        for (int i = lane; i < n; i += 32) acc = fma(az[i], 1.0 - xr[i], acc);
-        acc = -warp_sum(acc);
-      }
-      if (lane == 0) a.blocks[(size_t)cell * t1 * t1 + e] = acc;
-    } else {
-      const int r = e - t1 * t1;
-      if (r < t) {
-        const Side sd = trace_side(a, r);
-        const int len = side_len(a, sd.s);
-        for (int k = lane; k < len; k += 32)
-          acc = fma(coupling(a, cell, sd.s, k, sd.q), x0[side_node(a, sd.s, k)], acc);
-        acc = warp_sum(acc);
-      } else {
-        double al = 0.0, fz = 0.0;
-        for (int i = lane; i < n; i += 32) {
-          al = fma(az[i], x0[i], al);
-          fz += fvec[i];
-        }
-        acc = warp_sum(al) - warp_sum(fz);
-      }
-      if (lane == 0) a.loads[(size_t)cell * t1 + r] = acc;
-    }
-  }
   if (tid == 0) {
+    int it = 0, ok = 1, nf = 0;
+    for (int col = 0; col < w; ++col) {
+      it = citer[col] > it ? citer[col] : it;
+      ok &= (cstat[col] == 1);
+      nf |= (cstat[col] == 2);
+    }
+    if (st == MHM_CELL_OK && !ok) st = nf ? MHM_CELL_NONFINITE : MHM_CELL_RESIDUAL;
     a.status[cell] = st;
     a.iters[cell] = it;
     a.corrected[cell] = any_nonzero ? 1 : 0;
@@ -726,7 +759,7 @@ int fill_args(const mhm_q1_problem* p, int precision, Q1Args& a) {
   a.tfh = p->tf_h; a.tfv = p->tf_v; a.t = 2 * (a.tfh + a.tfv); a.w = a.t + 2;
   a.kmax = (a.rx > a.ry ? a.rx : a.ry) + 1;
   a.jmax = a.tfh > a.tfv ? a.tfh : a.tfv;
-  if (a.w > 32 * (kThreads / 32)) return MHM_ERR_UNSUPPORTED;
+  if (a.nnx > 32) return MHM_ERR_UNSUPPORTED;  // one lane per node of a line
   a.NYf = a.ny * a.ry;
   a.hx = p->hx; a.hy = p->hy; a.area = p->hx * p->hy;
   a.table = p->coupling_table; a.sign = p->side_sign; a.orient = p->side_orient;
@@ -737,20 +770,42 @@ int fill_args(const mhm_q1_problem* p, int precision, Q1Args& a) {
   gauss01(a.qorder, a.gpt, a.gwt);
   const size_t tsz = precision == MHM_PRECISION_FP64 ? 8 : 4;
   size_t off = 0;
-  const size_t nb = (size_t)a.nnx * a.nnx;
+  const size_t nb = (size_t)a.nnx * a.nnx, np1 = (size_t)a.n + 1;
   a.off_sinv = off; off = align16(off + (size_t)a.nny * nb * tsz);
-  a.off_gj = off; off = align16(off + 2 * nb * tsz);
+  const bool reg_factor = a.nnx == 5 || a.nnx == 9 || a.nnx == 17;  // see launch_condense
+  a.off_gj = off; off = align16(off + (reg_factor ? 0 : 2 * nb * tsz));
   a.off_cpl = off; off = align16(off + (size_t)5 * a.n * tsz);
-  a.off_tmp = off; off = align16(off + (size_t)a.nnx * a.w * tsz);
+  a.off_cb = off; off = align16(off + ((size_t)a.t * a.kmax + a.t) * 8);
   a.off_sten = off; off = align16(off + (size_t)5 * a.n * 8);
   a.off_vec = off; off = align16(off + (size_t)4 * a.n * 8);
-  a.off_work = off;
-  const size_t work = (size_t)a.w * (a.n + 1) * tsz;
+  a.off_warp = off;
+  const size_t warps = (size_t)(kThreads / 32) * (align16(np1 * 8) + align16(np1 * tsz));
   const size_t asm_tmp = (size_t)7 * a.rx * a.ry * 8;
-  off = align16(off + (work > asm_tmp ? work : asm_tmp));
-  a.off_misc = off; off = align16(off + (32 + 4 * (size_t)a.w) * 8 + ((size_t)a.w + 1) * 4);
+  off = align16(off + (warps > asm_tmp ? warps : asm_tmp));
+  a.off_misc = off; off = align16(off + (32 + (size_t)a.w) * 8 + (2 * (size_t)a.w + 1) * 4);
   a.smem = off;
   return MHM_OK;
+}
+
+template <typename T, int NNX>
+int launch_one(const Q1Args& a, int cells, cudaStream_t s) {
+  if (cudaFuncSetAttribute(q1_condense_kernel<T, NNX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)a.smem) != cudaSuccess)
+    return MHM_ERR_LAUNCH;
+  q1_condense_kernel<T, NNX><<<cells, kThreads, a.smem, s>>>(a);
+  return MHM_OK;
+}
+
+// Register-resident factorization for the common line lengths (4, 8 and 16 fine
+// cells per macrocell side); other lengths use the shared-memory one.
+template <typename T>
+int launch_condense(const Q1Args& a, int cells, cudaStream_t s) {
+  switch (a.nnx) {
+    case 5: return launch_one<T, 5>(a, cells, s);
+    case 9: return launch_one<T, 9>(a, cells, s);
+    case 17: return launch_one<T, 17>(a, cells, s);
+    default: return launch_one<T, 0>(a, cells, s);
+  }
 }
 
 }  // namespace
@@ -787,18 +842,9 @@ extern "C" int mhm_q1_condense(const mhm_q1_problem* p, int32_t precision, int32
   a.status = cell_status; a.iters = cell_iters;
   const int cells = a.nx * a.ny;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  cudaError_t e;
-  if (precision == MHM_PRECISION_FP64) {
-    e = cudaFuncSetAttribute(q1_condense_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)a.smem);
-    if (e != cudaSuccess) return MHM_ERR_LAUNCH;
-    q1_condense_kernel<double><<<cells, kThreads, a.smem, s>>>(a);
-  } else {
-    e = cudaFuncSetAttribute(q1_condense_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)a.smem);
-    if (e != cudaSuccess) return MHM_ERR_LAUNCH;
-    q1_condense_kernel<float><<<cells, kThreads, a.smem, s>>>(a);
-  }
+  const int rc2 = precision == MHM_PRECISION_FP64 ? launch_condense<double>(a, cells, s)
+                                                  : launch_condense<float>(a, cells, s);
+  if (rc2 != MHM_OK) return rc2;
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
 
