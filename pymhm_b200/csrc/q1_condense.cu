@@ -153,69 +153,169 @@ __device__ __forceinline__ double stencil_apply(const Q1Args& a, const double* s
   return acc;
 }
 
-template <typename T>
-__device__ __forceinline__ T shfl(T v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+// Reciprocal of a pivot of the unit-diagonal scaled operator (a value in (0, 2]):
+// the single-precision reciprocal, refined for binary64 by two Newton steps
+// r <- r + r (1 - d r), each doubling the number of correct bits.
+__device__ __forceinline__ float pivot_reciprocal(float d) { return __frcp_rn(d); }
+__device__ __forceinline__ double pivot_reciprocal(double d) {
+  double r = (double)__frcp_rn((float)d);
+  r = fma(r, fma(-d, r, 1.0), r);
+  r = fma(r, fma(-d, r, 1.0), r);
+  return r;
+}
 
-// Block LDL^T of the line-block operator by one warp, lane c holding column c of the
-// current block in registers: S_y = Adiag_y - B_y S_{y-1}^-1 B_y^T, then S_y^-1 by
-// Gauss-Jordan without pivoting (SPD); its pivots are those of the LDL^T of the
-// whole matrix.  S_y^-1 is stored row-major in sinv.
+// Register-resident line blocks: lane c of a warp holds column c of an NNX x NNX
+// block (idle lanes mirror the last column).  Couplings: node (y, a) to line y-1
+// sits in cdn[3 (y nnx + a) + (b - a + 1)] for the node (y-1, b).
 template <typename T, int NNX>
-__device__ void factor_lines_warp(int nny, const T* dg, const T* dl, const T* cdn, T* sinv, double& dmin,
-                                  double& dmax, int& bad) {
+__device__ __forceinline__ void block_diag(T (&col)[NNX], int c, int y, const T* dg, const T* dl) {
+  const int base = y * NNX;
+#pragma unroll
+  for (int r = 0; r < NNX; ++r)
+    col[r] = (r == c) ? dg[base + r] : (c == r - 1) ? dl[base + r] : (r == c - 1) ? dl[base + c] : T(0);
+}
+
+// col -= B_y X B_y^T (X: the block above... i.e. of line y-1, held like col).
+template <typename T, int NNX>
+__device__ __forceinline__ void sub_from_below(T (&col)[NNX], const T (&X)[NNX], int c, int y, const T* cdn) {
+  const int base = y * NNX;
+  const T bcm = c > 0 ? cdn[3 * (base + c) + 0] : T(0);
+  const T bc0 = cdn[3 * (base + c) + 1];
+  const T bcp = c < NNX - 1 ? cdn[3 * (base + c) + 2] : T(0);
+  T wv[NNX];
+#pragma unroll
+  for (int b = 0; b < NNX; ++b) {
+    const T lft = __shfl_up_sync(0xffffffffu, X[b], 1);
+    const T rgt = __shfl_down_sync(0xffffffffu, X[b], 1);
+    wv[b] = lft * bcm + X[b] * bc0 + rgt * bcp;
+  }
+#pragma unroll
+  for (int r = 0; r < NNX; ++r) {
+    T acc = cdn[3 * (base + r) + 1] * wv[r];
+    if (r > 0) acc += cdn[3 * (base + r) + 0] * wv[r - 1];
+    if (r < NNX - 1) acc += cdn[3 * (base + r) + 2] * wv[r + 1];
+    col[r] -= acc;
+  }
+}
+
+// col -= B_{y+1}^T X B_{y+1} (X: the block of line y+1, held like col).
+template <typename T, int NNX>
+__device__ __forceinline__ void sub_from_above(T (&col)[NNX], const T (&X)[NNX], int c, int y, const T* cdn) {
+  const int base = (y + 1) * NNX;
+  // B[p][q]: node (y+1, p) to node (y, q); lane c needs B[c-1][c], B[c][c], B[c+1][c]
+  const T bcm = c > 0 ? cdn[3 * (base + c - 1) + 2] : T(0);
+  const T bc0 = cdn[3 * (base + c) + 1];
+  const T bcp = c < NNX - 1 ? cdn[3 * (base + c + 1) + 0] : T(0);
+  T wv[NNX];
+#pragma unroll
+  for (int p = 0; p < NNX; ++p) {
+    const T lft = __shfl_up_sync(0xffffffffu, X[p], 1);
+    const T rgt = __shfl_down_sync(0xffffffffu, X[p], 1);
+    wv[p] = lft * bcm + X[p] * bc0 + rgt * bcp;
+  }
+#pragma unroll
+  for (int r = 0; r < NNX; ++r) {
+    T acc = cdn[3 * (base + r) + 1] * wv[r];
+    if (r > 0) acc += cdn[3 * (base + r - 1) + 2] * wv[r - 1];
+    if (r < NNX - 1) acc += cdn[3 * (base + r + 1) + 0] * wv[r + 1];
+    col[r] -= acc;
+  }
+}
+
+// In-place Gauss-Jordan inverse of the register block (SPD, no pivoting); the pivot
+// column goes through shared memory pb (one store per entry, broadcast loads).
+template <typename T, int NNX>
+__device__ __forceinline__ void block_invert(T (&col)[NNX], int c, T* pb, double& dmin, double& dmax, int& bad) {
   const int lane = threadIdx.x & 31;
-  const int c = lane < NNX ? lane : NNX - 1;  // idle lanes mirror the last column
-  T col[NNX];
-  dmin = 1e300;
-  dmax = 0.0;
-  bad = 0;
-  for (int y = 0; y < nny; ++y) {
-    const int base = y * NNX;
-    if (y > 0) {
-      // w[b] = sum_{d = c-1..c+1} S_{y-1}^-1[b][d] B_y[c][d]
-      const T bcm = c > 0 ? cdn[3 * (base + c) + 0] : T(0);
-      const T bc0 = cdn[3 * (base + c) + 1];
-      const T bcp = c < NNX - 1 ? cdn[3 * (base + c) + 2] : T(0);
-      T wv[NNX];
 #pragma unroll
-      for (int b = 0; b < NNX; ++b) {
-        const T lft = __shfl_up_sync(0xffffffffu, col[b], 1);
-        const T rgt = __shfl_down_sync(0xffffffffu, col[b], 1);
-        wv[b] = lft * bcm + col[b] * bc0 + rgt * bcp;
-      }
+  for (int k = 0; k < NNX; ++k) {
+    if (lane == k) {
 #pragma unroll
-      for (int r = 0; r < NNX; ++r) {
-        T v = (r == c) ? dg[base + r] : (c == r - 1) ? dl[base + r] : (r == c - 1) ? dl[base + c] : T(0);
-        T acc = cdn[3 * (base + r) + 1] * wv[r];
-        if (r > 0) acc += cdn[3 * (base + r) + 0] * wv[r - 1];
-        if (r < NNX - 1) acc += cdn[3 * (base + r) + 2] * wv[r + 1];
-        col[r] = v - acc;
-      }
-    } else {
-#pragma unroll
-      for (int r = 0; r < NNX; ++r)
-        col[r] = (r == c) ? dg[r] : (c == r - 1) ? dl[r] : (r == c - 1) ? dl[c] : T(0);
+      for (int i = 0; i < NNX; ++i) pb[i] = col[i];
     }
+    __syncwarp();
+    const T d = pb[k];
+    if (!(d > T(0))) bad = 1;
+    dmin = fmin(dmin, (double)d);
+    dmax = fmax(dmax, (double)d);
+    const T inv = pivot_reciprocal(d);
+    const T f = col[k] * inv;
 #pragma unroll
-    for (int k = 0; k < NNX; ++k) {
-      const T d = shfl(col[k], k);
-      if (!(d > T(0))) bad = 1;
-      dmin = fmin(dmin, (double)d);
-      dmax = fmax(dmax, (double)d);
-      const T inv = T(1) / d;
-      const T f = col[k] * inv;
-#pragma unroll
-      for (int i = 0; i < NNX; ++i) {
-        const T pk = shfl(col[i], k);
-        if (i == k) col[i] = (c == k) ? inv : f;
-        else col[i] = (c == k) ? -pk * inv : col[i] - pk * f;
-      }
+    for (int i = 0; i < NNX; ++i) {
+      const T pk = pb[i];
+      if (i == k) col[i] = (c == k) ? inv : f;
+      else col[i] = (c == k) ? -pk * inv : col[i] - pk * f;
     }
-    if (lane < NNX) {
+    __syncwarp();
+  }
+}
+
+template <typename T, int NNX>
+__device__ __forceinline__ void block_store(const T (&col)[NNX], int c, T* dst) {
+  if ((threadIdx.x & 31) < NNX) {
 #pragma unroll
-      for (int r = 0; r < NNX; ++r) sinv[(size_t)y * NNX * NNX + r * NNX + c] = col[r];
+    for (int r = 0; r < NNX; ++r) dst[r * NNX + c] = col[r];
+  }
+}
+
+// Twisted block LDL^T of the line-block operator (lines 0..nny-1, middle line
+// m = (nny-1)/2): warp 0 eliminates lines 0..m-1 top-down (S_y = A_yy - B_y S_{y-1}^-1
+// B_y^T), warp 1 lines nny-1..m+1 bottom-up (T_y = A_yy - B_{y+1}^T T_{y+1}^-1
+// B_{y+1}), then warp 0 the middle line M = A_mm - B_m S_{m-1}^-1 B_m^T -
+// B_{m+1}^T T_{m+1}^-1 B_{m+1}.  The inverses of all blocks land in sinv (row-major,
+// block y at y nnx^2).  Pivot statistics of both warps are merged into stat.
+template <typename T, int NNX>
+__device__ void factor_twisted(int nny, const T* dg, const T* dl, const T* cdn, T* sinv, T* pb, double* stat) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int c = lane < NNX ? lane : NNX - 1;
+  const int m = (nny - 1) / 2;
+  constexpr int nb = NNX * NNX;
+  double dmin = 1e300, dmax = 0.0;
+  int bad = 0;
+  T col[NNX], prev[NNX];
+  if (wid == 0) {
+    for (int y = 0; y < m; ++y) {
+      block_diag<T, NNX>(col, c, y, dg, dl);
+      if (y > 0) sub_from_below<T, NNX>(col, prev, c, y, cdn);
+      block_invert<T, NNX>(col, c, pb, dmin, dmax, bad);
+      block_store<T, NNX>(col, c, sinv + (size_t)y * nb);
+#pragma unroll
+      for (int r = 0; r < NNX; ++r) prev[r] = col[r];
+    }
+  } else if (wid == 1) {
+    for (int y = nny - 1; y > m; --y) {
+      block_diag<T, NNX>(col, c, y, dg, dl);
+      if (y < nny - 1) sub_from_above<T, NNX>(col, prev, c, y, cdn);
+      block_invert<T, NNX>(col, c, pb, dmin, dmax, bad);
+      block_store<T, NNX>(col, c, sinv + (size_t)y * nb);
+#pragma unroll
+      for (int r = 0; r < NNX; ++r) prev[r] = col[r];
+    }
+    if (lane == 0) {
+      stat[0] = dmin;
+      stat[1] = dmax;
+      stat[2] = bad;
     }
   }
+  __syncthreads();
+  if (wid == 0) {
+    block_diag<T, NNX>(col, c, m, dg, dl);
+    if (m > 0) sub_from_below<T, NNX>(col, prev, c, m, cdn);
+    if (m + 1 < nny) {
+      T up[NNX];
+#pragma unroll
+      for (int r = 0; r < NNX; ++r) up[r] = sinv[(size_t)(m + 1) * nb + r * NNX + c];
+      sub_from_above<T, NNX>(col, up, c, m, cdn);
+    }
+    block_invert<T, NNX>(col, c, pb, dmin, dmax, bad);
+    block_store<T, NNX>(col, c, sinv + (size_t)m * nb);
+    if (lane == 0) {
+      stat[0] = fmin(dmin, stat[0]);
+      stat[1] = fmax(dmax, stat[1]);
+      stat[2] = (bad || stat[2] != 0.0) ? 1.0 : 0.0;
+    }
+  }
+  __syncthreads();
 }
 
 // The same factorization by the whole block in shared memory (any line length):
@@ -303,9 +403,11 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
   double* ctil = az + n;
   double* dsc = ctil + n;
   // per-warp column buffers: x (n+1 doubles) and residual / solve vector (n+1 T)
-  const size_t wstride = align16((size_t)np1 * 8) + align16((size_t)np1 * sizeof(T));
+  const size_t wstride = align16((size_t)np1 * 8) + align16((size_t)np1 * sizeof(T)) + 64 * sizeof(T);
   double* xw = reinterpret_cast<double*>(smem + a.off_warp + wid * wstride);
   T* rw = reinterpret_cast<T*>(smem + a.off_warp + wid * wstride + align16((size_t)np1 * 8));
+  T* tb = reinterpret_cast<T*>(smem + a.off_warp + wid * wstride + align16((size_t)np1 * 8) +
+                               align16((size_t)np1 * sizeof(T)));  // 2 x 32 T: broadcast buffers
   double* kel = reinterpret_cast<double*>(smem + a.off_warp);  // aliases the warp buffers
   double* fel = kel + 3 * a.rx * a.ry;
   double* red = reinterpret_cast<double*>(smem + a.off_misc);
@@ -495,15 +597,13 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
     double dmin, dmax;
     int bad;
     if constexpr (NNX > 0) {
-      if (wid == 0) {
-        factor_lines_warp<T, NNX>(nny, dg, dl, cdn, sinv, dmin, dmax, bad);
-        if (lane == 0) {
-          const double eps = (sizeof(T) == 8) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
-          flag[0] = bad ? MHM_CELL_SINGULAR_PIVOT : (dmin <= eps * n * dmax ? MHM_CELL_RANK_DEFICIENT : 0);
-        }
-      }
+      factor_twisted<T, NNX>(nny, dg, dl, cdn, sinv, tb, red);
+      const double eps = (sizeof(T) == 8) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
+      dmin = red[0];
+      dmax = red[1];
+      if (red[2] != 0.0) st = MHM_CELL_SINGULAR_PIVOT;
+      else if (dmin <= eps * n * dmax) st = MHM_CELL_RANK_DEFICIENT;
       __syncthreads();
-      st = flag[0];
     } else {
       factor_lines_block<T>(nnx, nny, dg, dl, cdn, sinv, gj0, gj1, dmin, dmax, bad);
       const double eps = (sizeof(T) == 8) ? 2.220446049250313e-16 : 1.1920928955078125e-07;
@@ -516,6 +616,8 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
   // ---- refinement, one warp per right-hand-side column ---------------------------
   // x += y + (r_n - c.y) / zc, x_n += mu with mu = sum(r) / zc and y = D Apin^-1 D
   // (r - c mu), until ||b - K x|| <= tol ||b|| (columnwise, FP64 residual).
+  // middle line of the twisted factorization (plain top-down for the shared-memory one)
+  const int mid = NNX > 0 ? (nny - 1) / 2 : nny - 1;
   double fz = 0.0;
   for (int i = lane; i < n; i += 32) fz += fvec[i];
   fz = warp_sum(fz);
@@ -540,61 +642,122 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
       for (int i = lane; i < n; i += 32) sum += (double)rw[i];
       const double mu = warp_sum(sum) / zc;
       const double rmu = (double)rw[n];
-      // forward: z_y = S_y^-1 (v_y - B_y z_{y-1}), lane = node of the line
-      T zprev = T(0);
-      for (int y = 0; y < nny; ++y) {
-        const int i = y * nnx + lane;
-        T tv = T(0);
-        if (lane < nnx) tv = T(((double)rw[i] - ctil[i] * mu) * dsc[i]);
-        if (y > 0) {
-          const T zl = __shfl_up_sync(0xffffffffu, zprev, 1);
-          const T zr = __shfl_down_sync(0xffffffffu, zprev, 1);
-          if (lane < nnx) {
-            tv -= cdn[3 * i + 1] * zprev;
-            if (lane > 0) tv -= cdn[3 * i + 0] * zl;
-            if (lane < nnx - 1) tv -= cdn[3 * i + 2] * zr;
+      // Twisted block solve, lane = node of a line; the lines' values are broadcast
+      // through tb, neighbouring lines are read back from rw.  Lines 0..m-1 go forward
+      // top-down, lines nny-1..m+1 bottom-up (interleaved), line m closes, and the
+      // back-substitution runs outward from m.  (m = nny-1: plain top-down.)
+      const int la = lane < nnx ? lane : 0;
+      const int ntop = mid, nbot = nny - 1 - mid, nstep = ntop > nbot ? ntop : nbot;
+      T* tbt = tb;
+      T* tbb = tb + 32;
+      for (int sidx = 0; sidx < nstep; ++sidx) {
+        const bool dt = sidx < ntop, db = sidx < nbot;
+        const int yt = sidx, yb = nny - 1 - sidx;
+        if (lane < nnx) {
+          if (dt) {
+            const int i = yt * nnx + la;
+            T tv = T(((double)rw[i] - ctil[i] * mu) * dsc[i]);
+            if (yt > 0) {
+              const T* zp = rw + (yt - 1) * nnx;
+              tv -= cdn[3 * i + 1] * zp[la];
+              if (la > 0) tv -= cdn[3 * i + 0] * zp[la - 1];
+              if (la < nnx - 1) tv -= cdn[3 * i + 2] * zp[la + 1];
+            }
+            tbt[la] = tv;
+          }
+          if (db) {
+            const int i = yb * nnx + la;
+            T tv = T(((double)rw[i] - ctil[i] * mu) * dsc[i]);
+            if (yb < nny - 1) {
+              const T* zp = rw + (yb + 1) * nnx;
+              const int base = 3 * (yb + 1) * nnx;
+              tv -= cdn[base + 3 * la + 1] * zp[la];
+              if (la + 1 < nnx) tv -= cdn[base + 3 * (la + 1) + 0] * zp[la + 1];
+              if (la > 0) tv -= cdn[base + 3 * (la - 1) + 2] * zp[la - 1];
+            }
+            tbb[la] = tv;
           }
         }
-        const T* S = sinv + (size_t)y * nb + (lane < nnx ? lane : 0) * nnx;
-        T acc0 = T(0), acc1 = T(0);
-        int b = 0;
-        for (; b + 1 < nnx; b += 2) {
-          const T t0 = shfl(tv, b), t1v = shfl(tv, b + 1);
-          acc0 += S[b] * t0;
-          acc1 += S[b + 1] * t1v;
+        __syncwarp();
+        const T* St = sinv + (size_t)yt * nb + la * nnx;
+        const T* Sb = sinv + (size_t)yb * nb + la * nnx;
+        T at = T(0), ab = T(0);
+#pragma unroll 4
+        for (int b = 0; b < nnx; ++b) {
+          if (dt) at += St[b] * tbt[b];
+          if (db) ab += Sb[b] * tbb[b];
         }
-        if (b < nnx) acc0 += S[b] * shfl(tv, b);
-        zprev = acc0 + acc1;
-        if (lane < nnx) rw[i] = zprev;
+        __syncwarp();
+        if (lane < nnx) {
+          if (dt) rw[yt * nnx + la] = at;
+          if (db) rw[yb * nnx + la] = ab;
+        }
+        __syncwarp();
       }
-      // backward: x_y = z_y - S_y^-1 B_{y+1}^T x_{y+1}
-      T xnext = zprev;
-      for (int y = nny - 2; y >= 0; --y) {
-        const T xl = __shfl_up_sync(0xffffffffu, xnext, 1);
-        const T xr = __shfl_down_sync(0xffffffffu, xnext, 1);
-        T u = T(0);
+      {
+        const int i = mid * nnx + la;
         if (lane < nnx) {
-          const int base = 3 * (y + 1) * nnx;
-          u = cdn[base + 3 * lane + 1] * xnext;
-          if (lane + 1 < nnx) u += cdn[base + 3 * (lane + 1) + 0] * xr;
-          if (lane > 0) u += cdn[base + 3 * (lane - 1) + 2] * xl;
+          T tv = T(((double)rw[i] - ctil[i] * mu) * dsc[i]);
+          if (mid > 0) {
+            const T* zp = rw + (mid - 1) * nnx;
+            tv -= cdn[3 * i + 1] * zp[la];
+            if (la > 0) tv -= cdn[3 * i + 0] * zp[la - 1];
+            if (la < nnx - 1) tv -= cdn[3 * i + 2] * zp[la + 1];
+          }
+          if (mid + 1 < nny) {
+            const T* zp = rw + (mid + 1) * nnx;
+            const int base = 3 * (mid + 1) * nnx;
+            tv -= cdn[base + 3 * la + 1] * zp[la];
+            if (la + 1 < nnx) tv -= cdn[base + 3 * (la + 1) + 0] * zp[la + 1];
+            if (la > 0) tv -= cdn[base + 3 * (la - 1) + 2] * zp[la - 1];
+          }
+          tbt[la] = tv;
         }
-        const T* S = sinv + (size_t)y * nb + (lane < nnx ? lane : 0) * nnx;
-        T acc0 = T(0), acc1 = T(0);
-        int b = 0;
-        for (; b + 1 < nnx; b += 2) {
-          const T u0 = shfl(u, b), u1 = shfl(u, b + 1);
-          acc0 += S[b] * u0;
-          acc1 += S[b + 1] * u1;
-        }
-        if (b < nnx) acc0 += S[b] * shfl(u, b);
-        T xv = T(0);
+        __syncwarp();
+        const T* Sm = sinv + (size_t)mid * nb + la * nnx;
+        T acc = T(0);
+#pragma unroll 4
+        for (int b = 0; b < nnx; ++b) acc += Sm[b] * tbt[b];
+        __syncwarp();
+        if (lane < nnx) rw[i] = acc;
+        __syncwarp();
+      }
+      for (int sidx = 0; sidx < nstep; ++sidx) {
+        const bool dt = sidx < ntop, db = sidx < nbot;
+        const int yt = mid - 1 - sidx, yb = mid + 1 + sidx;
         if (lane < nnx) {
-          const int i = y * nnx + lane;
-          xv = rw[i] - (acc0 + acc1);
-          rw[i] = xv;
+          if (dt) {  // B_{yt+1}^T x_{yt+1}
+            const T* xn = rw + (yt + 1) * nnx;
+            const int base = 3 * (yt + 1) * nnx;
+            T u = cdn[base + 3 * la + 1] * xn[la];
+            if (la + 1 < nnx) u += cdn[base + 3 * (la + 1) + 0] * xn[la + 1];
+            if (la > 0) u += cdn[base + 3 * (la - 1) + 2] * xn[la - 1];
+            tbt[la] = u;
+          }
+          if (db) {  // B_yb x_{yb-1}
+            const T* xp = rw + (yb - 1) * nnx;
+            const int i = yb * nnx + la;
+            T u = cdn[3 * i + 1] * xp[la];
+            if (la > 0) u += cdn[3 * i + 0] * xp[la - 1];
+            if (la < nnx - 1) u += cdn[3 * i + 2] * xp[la + 1];
+            tbb[la] = u;
+          }
         }
-        xnext = xv;
+        __syncwarp();
+        const T* St = sinv + (size_t)(dt ? yt : 0) * nb + la * nnx;
+        const T* Sb = sinv + (size_t)(db ? yb : 0) * nb + la * nnx;
+        T at = T(0), ab = T(0);
+#pragma unroll 4
+        for (int b = 0; b < nnx; ++b) {
+          if (dt) at += St[b] * tbt[b];
+          if (db) ab += Sb[b] * tbb[b];
+        }
+        __syncwarp();
+        if (lane < nnx) {
+          if (dt) rw[yt * nnx + la] -= at;
+          if (db) rw[yb * nnx + la] -= ab;
+        }
+        __syncwarp();
       }
       __syncwarp();
       // kernel shift and update
@@ -779,7 +942,7 @@ int fill_args(const mhm_q1_problem* p, int precision, Q1Args& a) {
   a.off_sten = off; off = align16(off + (size_t)5 * a.n * 8);
   a.off_vec = off; off = align16(off + (size_t)4 * a.n * 8);
   a.off_warp = off;
-  const size_t warps = (size_t)(kThreads / 32) * (align16(np1 * 8) + align16(np1 * tsz));
+  const size_t warps = (size_t)(kThreads / 32) * (align16(np1 * 8) + align16(np1 * tsz) + 64 * tsz);
   const size_t asm_tmp = (size_t)7 * a.rx * a.ry * 8;
   off = align16(off + (warps > asm_tmp ? warps : asm_tmp));
   a.off_misc = off; off = align16(off + (32 + (size_t)a.w) * 8 + (2 * (size_t)a.w + 1) * 4);
