@@ -47,6 +47,10 @@ MACRO, LOCAL, FACE_DEGREE = 64, 16, 2
 SIGMA, ELL, SEED = 2.0, 0.05, 20261203
 METRIC = "MHM solves/s (64x64 Q1 Darcy, lognormal kappa), mixed vs FP64 GPU"
 CPU_SAMPLE_CELLS = 1024
+# DRAM bytes (read + write) per launch of this workload's kernels, from the ncu
+# captures summarised in profiles/skeleton_pcg_darcy64_r16_p2.md and
+# profiles/q1_condense_darcy64_r16_p2_mixed.md.
+NCU_DRAM_BYTES = {"skeleton_pcg": 15.4e6, "q1_condense": 92.3e6}
 
 
 def parse():
@@ -208,8 +212,21 @@ def main():
 
     mesh = CartesianMacroMesh(MACRO)
     sk = SkeletonSpace(mesh, (FaceSpace.uniform(FACE_DEGREE),) * len(mesh.faces))
-    plans = {p: CartesianQ1Plan(mesh, sk, LOCAL, precision=p) for p in ("mixed", "fp64")}
     dev = torch.device("cuda", local)
+    if args.profile:
+        # the bench workload's launches only (mixed precision), for ncu: no baselines,
+        # no L2 flush kernels, no host copies
+        plan = CartesianQ1Plan(mesh, sk, LOCAL, precision="mixed")
+        plan.set_device_coefficients(1, torch.from_numpy(np.ascontiguousarray(kappa)).to(dev), (0.0, 0.0, 0.0),
+                                     0, None, 1.0)
+        for _ in range(args.warmup + args.steps):
+            plan.launch(torch.cuda.current_stream())
+        torch.cuda.synchronize()
+        info, _ = plan.check()
+        print(json.dumps({"profile": True, "launches": 4 * (args.warmup + args.steps),
+                          "global_iterations": int(info[1])}), flush=True)
+        return
+    plans = {p: CartesianQ1Plan(mesh, sk, LOCAL, precision=p) for p in ("mixed", "fp64")}
     kappa_host = torch.from_numpy(np.ascontiguousarray(kappa)).pin_memory()
     kappa_dev = kappa_host.to(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -351,13 +368,17 @@ def roofline(plan, kernel, ms, inner_iters, outer):
             peak, source = float(json.load(f)["hbm_gbs"]), "measured"
     p = plan.pattern
     nnz = len(p.indices)
-    nnz_s = int((p.trace_end - p.indptr[:plan.T]).sum())
     M, n, w, T = plan.cells, plan.n, plan.w, plan.T
     if kernel == "skeleton_pcg":
-        # per inner iteration: S values+indices once, ~14 trace vectors, 4 coarse passes over the
-        # (nx x nx) sine transforms and the cell maps; per outer correction one full K SpMV
-        per_iter = nnz_s * 12 + 14 * T * 8 + 4 * (2 * plan.mesh.nx * plan.mesh.nx * 8 + M * 8) + 2 * M * plan.t * 16
-        bytes_ = inner_iters * per_iter + (outer + 2) * (nnz * 12 + 2 * plan.N * 8)
+        # Cell-form projected CG: setup reads the cell blocks and tables once; per inner
+        # iteration each of the two half-steps writes the cells' face partials (M t) and
+        # reads them back on every CTA's local DOFs (~2 T), and each of its two coarse
+        # solves writes and reads the three-part row data (3 M) and the solved rows
+        # (M, read back three rows per CTA); every outer correction sweeps the CSR K.
+        t = plan.t
+        setup = M * (t + 1) * (t + 1) * 8 + M * t * (8 + 8 + 4) + T * 16
+        per_iter = 2 * (M * t * 8 + 2 * T * 8) + 2 * (2 * 3 * M * 8 + M * 8 + 3 * M * 8)
+        bytes_ = setup + inner_iters * per_iter + (outer + 2) * (nnz * 12 + 2 * plan.N * 8)
     elif kernel == "q1_condense":
         bytes_ = plan.nxf * plan.nyf * 8 + M * w * (n + 1) * 8 + M * (plan.t + 1) * (plan.t + 2) * 8
     elif kernel == "q1_reconstruct":
@@ -366,7 +387,7 @@ def roofline(plan, kernel, ms, inner_iters, outer):
         bytes_ = nnz * 24 + plan.N * 24
     achieved = bytes_ / (ms * 1e-3) / 1e9
     return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "algorithmic_bytes": int(bytes_),
+            "frac": achieved / peak, "traffic": NCU_DRAM_BYTES.get(kernel), "algorithmic_bytes": int(bytes_),
             "peak_source": source + " (MEASURED_PEAKS.json hbm_gbs)" if source == "measured" else source}
 
 
