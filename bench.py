@@ -46,7 +46,7 @@ sys.path.insert(0, ROOT)
 MACRO, LOCAL, FACE_DEGREE = 64, 16, 2
 SIGMA, ELL, SEED = 2.0, 0.05, 20261203
 METRIC = "MHM solves/s (64x64 Q1 Darcy, lognormal kappa), mixed vs FP64 GPU"
-CPU_SAMPLE_CELLS = 1024
+CPU_SAMPLE_CELLS = 4096
 # DRAM bytes (read + write) per launch of this workload's kernels, from the ncu
 # captures summarised in profiles/skeleton_pcg_darcy64_r16_p2.md and
 # profiles/q1_condense_darcy64_r16_p2_mixed.md.

@@ -168,7 +168,9 @@ int64_t mhm_skeleton_workspace_bytes(const mhm_skeleton_system* s /* host */, in
  * inner iterations, outer corrections, barrier error flag.  stats (device
  * double[4]): final relative residual ||rhs - K x|| / ||rhs||, the physical
  * certificate ||K x - rhs|| / max(||rhs||, ||load_scale||, || |K||x| ||),
- * first inner relative residual, unused.  The solve runs as one persistent
+ * relative residual after the first outer correction, unused.  rtol bounds the
+ * outer FP64 residual; the first inner solve runs to inner_rtol, each later one
+ * to rtol / (current outer residual), clipped to [1e-12, 0.1].  The solve runs as one persistent
  * cooperative kernel with one CTA per macro row (ny CTAs, all co-resident;
  * MHM_ERR_UNSUPPORTED when they do not fit or a row's tables exceed shared
  * memory); `grid` is accepted for ABI stability and ignored.  workspace is

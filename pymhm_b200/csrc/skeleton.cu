@@ -371,6 +371,67 @@ __device__ void coarse_rows(const Sys& s, const Row& R, const double* W, int lo,
   __syncthreads();
 }
 
+// Start of an inner half-step after a grid barrier: the partial sums in slots
+// [slot, slot + NS), the per-DOF exchange sums Xf + Xs on the G DOFs (into out) and
+// the solved coarse rows r-1 .. r+1 of W (into wrow; rows outside [0, ny) zero)
+// are all loaded in one batch before any of them is used; then the coarse rows Y
+// are formed.  tot receives the partial sums (identical in every CTA).
+template <int NS>
+__device__ void phase_begin(const Sys& s, const Work& w, const Row& R, int slot, double (&tot)[NS], double* sh,
+                            const double* Xf, const double* Xs, double* out, const double* W) {
+  const int nx = s.nx, ny = s.ny, r0 = R.r - 1, tid = threadIdx.x, nth = blockDim.x;
+  __syncthreads();
+  double pv[NS][4];
+  if (tid < 32) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = tid + 32 * q;
+#pragma unroll
+      for (int n = 0; n < NS; ++n) pv[n][q] = i < (int)gridDim.x ? __ldcg(w.part + i * 4 + slot + n) : 0.0;
+    }
+  }
+  double xa[2], xb[2], wv;
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int l = tid + q * nth;
+    const int64_t i = l < R.ng ? R.gdof[l] : 0;
+    xa[q] = l < R.ng ? __ldcg(Xf + i) : 0.0;
+    xb[q] = l < R.ng ? __ldcg(Xs + i) : 0.0;
+  }
+  {
+    const int ir = r0 + tid / nx;
+    wv = (tid < 3 * nx && ir >= 0 && ir < ny) ? __ldcg(W + (size_t)ir * nx + tid % nx) : 0.0;
+  }
+  // remainders (rows wider than the block; not reached for the supported sizes)
+  for (int l = tid + 2 * nth; l < R.ng; l += nth) out[l] = __ldcg(Xf + R.gdof[l]) + __ldcg(Xs + R.gdof[l]);
+  for (int idx = tid + nth; idx < 3 * nx; idx += nth) {
+    const int ir = r0 + idx / nx;
+    R.wrow[idx] = (ir >= 0 && ir < ny) ? __ldcg(W + (size_t)ir * nx + idx % nx) : 0.0;
+  }
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int l = tid + q * nth;
+    if (l < R.ng) out[l] = xa[q] + xb[q];
+  }
+  if (tid < 3 * nx) R.wrow[tid] = wv;
+  if (tid < 32) {
+    for (int i0 = tid + 128; i0 < (int)gridDim.x; i0 += 32)
+#pragma unroll
+      for (int n = 0; n < NS; ++n) pv[n][0] += __ldcg(w.part + i0 * 4 + slot + n);
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      const double a = warp_sum((pv[n][0] + pv[n][1]) + (pv[n][2] + pv[n][3]));
+      if (tid == 0) sh[n] = a;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int n = 0; n < NS; ++n) tot[n] = sh[n];
+  const double* in[3] = {R.wrow, R.wrow + nx, R.wrow + 2 * nx};
+  sine_apply(R, nx, 3, in, [&](int j, int i, double v) { R.yrow[j * nx + i] = v; });
+  __syncthreads();
+}
+
 // Per-cell products cpart[cx][a] = sum_b B_c[a][b] v[cl[cx][b]] (B packed symmetric);
 // returns this thread's sum of v[cl] * cpart (for (u, S u)).
 template <int T>
@@ -774,7 +835,9 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       if (res <= P.rtol) break;
     }
     {
-      const double itol = (outer == 0) ? P.inner_rtol : fmax(P.inner_rtol, 1e-4);
+      // the first inner solve to inner_rtol; a later correction only has to win the
+      // factor between the current outer residual and rtol
+      const double itol = (outer == 0) ? P.inner_rtol : fmin(0.1, fmax(P.rtol / res, 1e-12));
       const Coarse Cx1{w.Ux1, nullptr, nullptr}, Cx2{w.Ux2, nullptr, nullptr};
       // coarse data of r2
       for (int cx = tid; cx < nx; cx += nth) R.col[cx] = w.rfull[s.T + R.c0 + cx];
@@ -818,7 +881,9 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       int k = 0;
       for (;; ++k) {
         // (1) u = P M^-1 r and w = S u (cell partials) on G; gamma, delta
-        const double rn = sqrt(grid_total(w, 0, sh));
+        double rr[1];
+        phase_begin<1>(s, w, R, 0, rr, sh, w.Zf, w.Zs, R.vt, w.Wz);
+        const double rn = sqrt(rr[0]);
         if (!isfinite(rn)) { status = MHM_SOLVE_NONFINITE; break; }
         if (k == 0) {
           r0 = rn;
@@ -827,8 +892,6 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
           break;
         }
         if (k >= P.max_inner) { status = MHM_SOLVE_NOT_CONVERGED; break; }
-        read_exchange(R, w.Zf, w.Zs, R.vt);
-        coarse_rows(s, R, w.Wz, R.r - 1, R.r + 2);
         for (int l = tid; l < R.ng; l += nth) R.vu[l] = R.vt[l] - g0y(R, l);
         double gam = 0.0;
         for (int l = tid; l < R.nown; l += nth) gam = fma(R.vr[l], R.vu[l], gam);
@@ -845,14 +908,12 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
         // (2) step: P S p by recurrence, r -= alpha P S p; preconditioned partials
         {
           double gd[2];
-          grid_totals<2>(w, 1, gd, sh);
+          phase_begin<2>(s, w, R, 1, gd, sh, w.Vf, w.Vs, R.vt, w.Ww);
           const double g = gd[0], d = gd[1];
           const double beta = k > 0 ? g / gam_prev : 0.0;
           const double pq = k > 0 ? d - beta * g / alpha_prev : d;
           if (!(pq > 0.0) || !isfinite(g)) { status = MHM_SOLVE_BREAKDOWN; break; }
           const double alpha = g / pq;
-          read_exchange(R, w.Vf, w.Vs, R.vt);
-          coarse_rows(s, R, w.Ww, R.r - 1, R.r + 2);
           for (int l = tid; l < R.ng; l += nth) {
             const double pw = R.vt[l] - g0y(R, l);
             const double ps = k > 0 ? fma(beta, R.vps[l], pw) : pw;

@@ -219,7 +219,7 @@ class CartesianQ1Plan:
 
     def __init__(self, mesh, skeleton=None, local_refinement=4, *, dirichlet=0.0, quadrature_order=4,
                  degree=1, precision="fp64", device=None, max_refine=None, local_tol=1e-12,
-                 global_rtol=1e-13, inner_rtol=1e-12, max_inner=5000, max_outer=6, grid=0):
+                 global_rtol=1e-13, inner_rtol=1e-10, max_inner=5000, max_outer=6, grid=0):
         import torch
 
         if int(degree) != 1:

@@ -39,7 +39,7 @@ class SkeletonFactorization:
 
     solver = "mhm_b200"
 
-    def __init__(self, matrix, mesh, skeleton=None, *, rtol: float = 1e-10, inner_rtol: float = 1e-12,
+    def __init__(self, matrix, mesh, skeleton=None, *, rtol: float = 1e-10, inner_rtol: float = 1e-10,
                  max_inner: int = 5000, max_outer: int = 8):
         import torch
 
