@@ -9,12 +9,17 @@ cells, f = 1, homogeneous Dirichlet data.  Synthetic, seeded inputs.
 
 A step is one complete MHM solve: local assembly + condensation, ordered
 skeleton reduction, global skeleton solve, reconstruction of fields and
-fluxes.  ``value`` is solves/s with the permeability already resident in HBM
-(mixed precision: binary32 local factors + FP64 refinement; the FP64-factor
-path is reported beside it); ``e2e`` times the public API with the
-permeability copied from pinned host memory and fields, fluxes and skeleton
-unknowns copied back every step.  L2 is flushed (256 MiB write) between timed
-steps, outside the timed region.
+fluxes.  ``value`` is solves/s of a serving loop with the permeability already
+resident in HBM: independent requests alternate between two plans, so two
+solves are in flight and one request's latency-bound global solve (64 of the
+148 SMs, high-priority stream) overlaps the next request's local stage
+(low-priority stream).  Mixed precision: binary32 local factors + FP64
+refinement; the FP64-factor path is reported beside it, and ``sequential``
+gives one-solve-at-a-time latency with the per-kernel split (L2 flushed by a
+256 MiB write between those steps, outside the timed region).  ``e2e`` runs
+the same serving loop through the public API with the permeability copied
+from pinned host memory and fields, fluxes, skeleton unknowns and status
+copied back for every request.
 
 ``--impl reference`` times the CPU restatement of the reference path (the
 oracle) on the host cores instead: each step runs the local stage on a
@@ -182,7 +187,12 @@ def workload_config(args):
     return {"workload": f"darcy-q1-{MACRO}x{MACRO}-r{LOCAL}-p{FACE_DEGREE}-lognormal-s{SIGMA:g}-l{ELL:g}",
             "macrocells": MACRO * MACRO, "local_dofs": (LOCAL + 1) ** 2, "rhs_per_cell": 4 * (FACE_DEGREE + 1) + 1,
             "skeleton_unknowns": None, "fine_cells": (MACRO * LOCAL) ** 2, "seed": SEED,
-            "parallelism": f"replicas x{args.gpus}", "l2": "flushed between timed steps (256 MiB write)"}
+            "parallelism": f"replicas x{args.gpus}",
+            "serving": "value/e2e: two independent solves in flight per GPU (two plans; local stage on "
+                       "low-priority streams, global solve + reconstruction on high-priority streams); "
+                       "'sequential': one solve at a time",
+            "l2": "sequential: flushed between timed steps (256 MiB write); serving loop: no flush, each "
+                  "solve's working set (responses 133 MB + fields/fluxes 26 MB) exceeds the 126 MB L2"}
 
 
 def main():
@@ -226,26 +236,40 @@ def main():
         print(json.dumps({"profile": True, "launches": 4 * (args.warmup + args.steps),
                           "global_iterations": int(info[1])}), flush=True)
         return
-    plans = {p: CartesianQ1Plan(mesh, sk, LOCAL, precision=p) for p in ("mixed", "fp64")}
+    plans = {p: [CartesianQ1Plan(mesh, sk, LOCAL, precision=p) for _ in range(2)] for p in ("mixed", "fp64")}
     kappa_host = torch.from_numpy(np.ascontiguousarray(kappa)).pin_memory()
-    kappa_dev = kappa_host.to(dev)
+    kappa_dev = [kappa_host.to(dev) for _ in range(2)]  # one resident copy per plan
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
+    lo, hi = torch.cuda.Stream.priority_range()
+    local_st = [torch.cuda.Stream(device=dev, priority=lo) for _ in range(2)]
+    global_st = [torch.cuda.Stream(device=dev, priority=hi) for _ in range(2)]
 
     def barrier():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
 
-    results = {}
-    for prec, plan in plans.items():
-        plan.set_device_coefficients(1, kappa_dev, (0.0, 0.0, 0.0), 0, None, 1.0)
+    def fork():
+        for st in local_st + global_st:
+            st.wait_stream(stream)
+
+    def join():
+        for st in local_st + global_st:
+            stream.wait_stream(st)
+
+    seq, pipe = {}, {}
+    for prec, pl in plans.items():
+        for j, plan in enumerate(pl):
+            plan.set_device_coefficients(1, kappa_dev[j], (0.0, 0.0, 0.0), 0, None, 1.0)
+        # (a) back-to-back single solves on one stream: latency and the per-kernel split,
+        #     L2 flushed between steps
+        plan = pl[0]
         for _ in range(args.warmup):
             plan.launch(stream)
         torch.cuda.synchronize()
         plan.check()
         steps, kern = [], []
-        clocks = Clocks(local) if prec == "mixed" else None
         barrier()
         for _ in range(args.steps):
             flush.zero_()
@@ -255,41 +279,87 @@ def main():
             steps.append(ev[0].elapsed_time(ev[4]))
             kern.append([ev[k].elapsed_time(ev[k + 1]) for k in range(4)])
         barrier()
-        clk = clocks.stop() if clocks else None
         info, stats = plan.check()
-        results[prec] = dict(steps=np.array(steps), kern=np.array(kern), info=info, stats=stats, clocks=clk)
-
-    # end to end through the public API: H2D kappa, solve, D2H fields/flux/x/status
-    plan = plans["mixed"]
-    n_out = plan.fields.numel() + plan.flux.numel() + plan.x.numel()
-    host_fields = torch.empty(plan.fields.shape, dtype=torch.float64).pin_memory()
-    host_flux = torch.empty(plan.flux.shape, dtype=torch.float64).pin_memory()
-    host_x = torch.empty(plan.x.shape, dtype=torch.float64).pin_memory()
-    host_status = torch.empty(plan.cell_status.shape, dtype=torch.int32).pin_memory()
-    host_info = torch.empty(4, dtype=torch.int32).pin_memory()
-    e2e_ms = []
-    kdev = torch.empty_like(kappa_dev)
-    plan.set_device_coefficients(1, kdev, (0.0, 0.0, 0.0), 0, None, 1.0)
-    for it in range(args.warmup + args.steps):
-        flush.zero_()
+        seq[prec] = dict(steps=np.array(steps), kern=np.array(kern), info=info, stats=stats)
+        # (b) serving loop: request k on plan k % 2, two solves in flight; the local stage
+        #     runs on low-priority streams, the global solve and the reconstruction on
+        #     high-priority ones, so each solve's latency-bound global stage overlaps the
+        #     next request's local stage
+        fork()
+        for k in range(args.warmup):
+            pl[k % 2].launch(local_st[k % 2], global_stream=global_st[k % 2])
+        join()
         torch.cuda.synchronize()
+        clocks = Clocks(local) if prec == "mixed" else None
+        barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(args.steps)]
         e0.record(stream)
-        kdev.copy_(kappa_host, non_blocking=True)
-        plan.launch(stream)
-        host_fields.copy_(plan.fields, non_blocking=True)
-        host_flux.copy_(plan.flux, non_blocking=True)
-        host_x.copy_(plan.x, non_blocking=True)
-        host_status.copy_(plan.cell_status, non_blocking=True)
-        host_info.copy_(plan.info, non_blocking=True)
+        fork()
+        for k in range(args.steps):
+            pl[k % 2].launch(local_st[k % 2], global_stream=global_st[k % 2], events=evs[k])
+        join()
         e1.record(stream)
-        e1.synchronize()
-        if it >= args.warmup:
-            e2e_ms.append(e0.elapsed_time(e1))
-        if int(host_status.numpy().max()) != 0 or int(host_info[0]) != 0:
+        torch.cuda.synchronize()
+        barrier()
+        clk = clocks.stop() if clocks else None
+        for plan in pl:
+            plan.check()
+        pipe[prec] = dict(total=e0.elapsed_time(e1), lat=np.array([e[0].elapsed_time(e[4]) for e in evs]), clocks=clk)
+
+    # end to end through the public API, same serving loop: H2D kappa, solve, D2H
+    # fields / flux / x / status / info for every request
+    pl = plans["mixed"]
+    plan = pl[0]
+    n_out = plan.fields.numel() + plan.flux.numel() + plan.x.numel()
+    hosts = [dict(fields=torch.empty(plan.fields.shape, dtype=torch.float64).pin_memory(),
+                  flux=torch.empty(plan.flux.shape, dtype=torch.float64).pin_memory(),
+                  x=torch.empty(plan.x.shape, dtype=torch.float64).pin_memory(),
+                  status=torch.empty(plan.cell_status.shape, dtype=torch.int32).pin_memory(),
+                  info=torch.empty(4, dtype=torch.int32).pin_memory()) for _ in range(2)]
+    kdev = [torch.empty_like(kappa_dev[0]) for _ in range(2)]
+    for j in range(2):
+        pl[j].set_device_coefficients(1, kdev[j], (0.0, 0.0, 0.0), 0, None, 1.0)
+
+    def request(k):
+        j = k % 2
+        p_, ls, gs, h = pl[j], local_st[j], global_st[j], hosts[j]
+        if getattr(p_, "_done", None) is not None:
+            ls.wait_event(p_._done)  # the previous request on this plan still reads kappa
+        with torch.cuda.stream(ls):
+            kdev[j].copy_(kappa_host, non_blocking=True)
+        p_.launch(ls, global_stream=gs)
+        with torch.cuda.stream(gs):
+            h["fields"].copy_(p_.fields, non_blocking=True)
+            h["flux"].copy_(p_.flux, non_blocking=True)
+            h["x"].copy_(p_.x, non_blocking=True)
+            h["status"].copy_(p_.cell_status, non_blocking=True)
+            h["info"].copy_(p_.info, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(gs)
+        p_._done = ev
+
+    fork()
+    for k in range(args.warmup):
+        request(k)
+    join()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fork()
+    for k in range(args.steps):
+        request(k)
+    join()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    for h in hosts:
+        if int(h["status"].numpy().max()) != 0 or int(h["info"][0]) != 0:
             raise RuntimeError("end-to-end solve reported a failure")
+    e2e_total = e0.elapsed_time(e1)
     h2d = kappa_host.numel() * 8
-    d2h = n_out * 8 + host_status.numel() * 4 + 16
+    d2h = n_out * 8 + plan.cell_status.numel() * 4 + 16
+    host_fields, host_flux, host_x = hosts[(args.steps - 1) % 2]["fields"], hosts[(args.steps - 1) % 2]["flux"], \
+        hosts[(args.steps - 1) % 2]["x"]
 
     # accuracy against the reference's FP64 solution (golden fixture of the same workload)
     acc = {}
@@ -309,32 +379,40 @@ def main():
     def agg(v):
         return max_over_ranks(v, dist, dev)
 
-    mixed, fp64 = results["mixed"], results["fp64"]
-    ms = agg(float(mixed["steps"].mean()))
-    ms64 = agg(float(fp64["steps"].mean()))
-    ms_e2e = agg(float(np.mean(e2e_ms)))
+    K = args.steps
+    ms = agg(pipe["mixed"]["total"] / K)
+    ms64 = agg(pipe["fp64"]["total"] / K)
+    ms_e2e = agg(e2e_total / K)
+    seq_ms = agg(float(seq["mixed"]["steps"].mean()))
+    seq_ms64 = agg(float(seq["fp64"]["steps"].mean()))
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return
+    mixed, fp64 = seq["mixed"], seq["fp64"]
     kern = mixed["kern"].mean(axis=0)
     names = ["q1_condense", "skeleton_scatter", "skeleton_pcg", "q1_reconstruct"]
     top = int(np.argmax(kern))
     roof = roofline(plan, names[top], kern[top], int(mixed["info"][1]), int(mixed["info"][2]))
-    from pymhm_b200 import darcy as _d  # noqa: F401
+
+    def pct(v, q):
+        return float(np.percentile(v, q))
 
     line = {
         "metric": METRIC, "value": world * 1000.0 / ms, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic (seeded lognormal kappa, f=1)", "config": workload_config(args),
-        "latency_ms": {"p50": float(np.percentile(mixed["steps"], 50)), "p99": float(np.percentile(mixed["steps"], 99))},
+        "latency_ms": {"p50": pct(pipe["mixed"]["lat"], 50), "p99": pct(pipe["mixed"]["lat"], 99)},
         "fp64": {"value": world * 1000.0 / ms64, "ms_per_step": ms64,
-                 "p50": float(np.percentile(fp64["steps"], 50)), "p99": float(np.percentile(fp64["steps"], 99)),
+                 "p50": pct(pipe["fp64"]["lat"], 50), "p99": pct(pipe["fp64"]["lat"], 99),
+                 "sequential_ms": seq_ms64,
                  "kernels_ms": dict(zip(names, map(float, fp64["kern"].mean(axis=0)))),
                  "global_iterations": int(fp64["info"][1])},
         "mixed_over_fp64": ms64 / ms,
+        "sequential": {"ms_per_solve": seq_ms, "p50": pct(mixed["steps"], 50), "p99": pct(mixed["steps"], 99),
+                       "fp64_ms_per_solve": seq_ms64},
         "kernels_ms": dict(zip(names, map(float, kern))),
         "global_iterations": int(mixed["info"][1]), "outer_corrections": int(mixed["info"][2]),
         "residual": float(mixed["stats"][0]), "certificate": float(mixed["stats"][1]),
@@ -342,7 +420,7 @@ def main():
         "e2e": {"value": world * 1000.0 / ms_e2e, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e},
         "gpu_launches": 4 * args.steps,
-        "roofline": roof, "cpu_baseline": cpu, "clocks": mixed["clocks"],
+        "roofline": roof, "cpu_baseline": cpu, "clocks": pipe["mixed"]["clocks"],
     }
     line["config"]["skeleton_unknowns"] = plan.N
     print(json.dumps(line), flush=True)

@@ -347,42 +347,62 @@ class CartesianQ1Plan:
         q.source_mode, q.source, q.source_const = smode, _lib.ptr(source), float(sconst)
         self._keep = (kappa, source)
 
-    def launch(self, stream=None, *, reconstruct=True, events=None):
+    def launch(self, stream=None, *, reconstruct=True, events=None, global_stream=None):
         """Enqueue the four kernels on ``stream`` (no host synchronisation).
 
         ``events``, if given, is a list of at least five ``torch.cuda.Event``s
         recorded before, between and after the kernels (per-kernel timing).
+        ``global_stream``, if given, runs the skeleton solve and the reconstruction
+        after the local stage on that stream instead (ordered by an event), so that
+        a serving loop can put the latency-bound global solve on a higher-priority
+        stream and overlap it with the next request's local stage.
         """
         L, s = self.lib, _lib.stream_handle(stream)
         P = _lib.ptr
         torch = self.torch
         cur = torch.cuda.current_stream() if stream is None else stream
+        gcur = cur if global_stream is None else global_stream
+        gs = s if global_stream is None else _lib.stream_handle(global_stream)
+        if getattr(self, "_done", None) is not None and self._done_stream is not cur:
+            cur.wait_event(self._done)  # the previous solve's global stage still reads the buffers
 
-        def mark(k):
+        def mark(k, st):
             if events is not None:
-                events[k].record(cur)
+                events[k].record(st)
 
-        mark(0)
+        mark(0, cur)
         _lib.check(L.mhm_q1_condense(self.q1, PRECISIONS[self.precision], self.max_refine, self.local_tol,
                                      P(self.solution), P(self.blocks), P(self.loads), P(self.corrected),
                                      P(self.cell_status), P(self.cell_iters), s), "mhm_q1_condense")
-        mark(1)
+        mark(1, cur)
         pat = self.pattern
         _lib.check(L.mhm_skeleton_scatter(len(pat.indices), P(self.d_slot_ptr), P(self.d_contrib),
                                           P(self.blocks), P(self.values), self.N, self.T,
                                           P(self.d_load_ptr), P(self.d_load_contrib), P(self.loads),
                                           P(self.d_boundary), P(self.rhs), P(self.load_scale), s),
                    "mhm_skeleton_scatter")
-        mark(2)
+        mark(2, cur)
+        if global_stream is not None:
+            if not hasattr(self, "_handoff"):
+                self._handoff = torch.cuda.Event()
+            self._handoff.record(cur)
+            global_stream.wait_event(self._handoff)
         _lib.check(L.mhm_skeleton_solve(self.sys, P(self.rhs), P(self.load_scale), P(self.x), self.global_rtol,
                                         self.inner_rtol, self.max_inner, self.max_outer, self.grid,
-                                        P(self.workspace), self.workspace.numel(), P(self.info), P(self.stats), s),
+                                        P(self.workspace), self.workspace.numel(), P(self.info), P(self.stats), gs),
                    "mhm_skeleton_solve")
-        mark(3)
+        mark(3, gcur)
         if reconstruct:
             _lib.check(L.mhm_q1_reconstruct(self.q1, P(self.solution), P(self.d_cell_dofs), self.T, P(self.x),
-                                            P(self.fields), P(self.flux), s), "mhm_q1_reconstruct")
-        mark(4)
+                                            P(self.fields), P(self.flux), gs), "mhm_q1_reconstruct")
+        mark(4, gcur)
+        if global_stream is not None:
+            if getattr(self, "_done", None) is None:
+                self._done = torch.cuda.Event()
+            self._done.record(gcur)
+            self._done_stream = gcur
+        else:
+            self._done = None
 
     def check(self):
         """Synchronise and raise the reference's error for any failed cell or solve."""
