@@ -116,6 +116,37 @@ int mhm_q1_condense(const mhm_q1_problem* p /* host */, int32_t precision, int32
                     double tol, double* solution, double* blocks, double* loads,
                     uint8_t* corrected, int32_t* cell_status, int32_t* cell_iters, void* stream);
 
+/*
+ * Offline / online reuse (replaces OfflineLocalProblem and the local part of
+ * OfflineHybridSystem, core/offline.py:104-313): a condensation that keeps each
+ * cell's factor, and later source responses that reuse it.
+ *
+ * Bytes of the stored factors: cells x (ry+1) x (rx+1)^2 values of the factor
+ * type (binary64 for MHM_PRECISION_FP64, binary32 for MHM_PRECISION_MIXED);
+ * -1 for invalid arguments.
+ */
+int64_t mhm_q1_factor_bytes(const mhm_q1_problem* p /* host */, int32_t precision);
+
+/* mhm_q1_condense that also writes each cell's factor (the inverses of its line
+ * Schur complements) to `factors` (mhm_q1_factor_bytes). */
+int mhm_q1_condense_offline(const mhm_q1_problem* p /* host */, int32_t precision,
+                            int32_t max_refine, double tol, double* solution, double* blocks,
+                            double* loads, uint8_t* corrected, int32_t* cell_status,
+                            int32_t* cell_iters, void* factors, void* stream);
+
+/*
+ * Source response only (OfflineLocalProblem.response, core/offline.py:121-127):
+ * re-assembles every cell with p's source and the offline permeability, reuses
+ * `factors` instead of factoring, refines the source column and writes solution
+ * column 0 (R f) and `loads`.  Solution columns 1..w-1, the Schur blocks and
+ * `corrected` keep what mhm_q1_condense_offline wrote for the same operator; the
+ * caller must not change the permeability in between.
+ */
+int mhm_q1_source_response(const mhm_q1_problem* p /* host */, int32_t precision,
+                           int32_t max_refine, double tol, const void* factors, double* solution,
+                           double* loads, uint8_t* corrected, int32_t* cell_status,
+                           int32_t* cell_iters, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Ordered skeleton reduction                                                 */
 /* ------------------------------------------------------------------------ */

@@ -20,7 +20,7 @@ from .topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
 __all__ = [
     "CartesianMacroMesh", "FaceSpace", "SkeletonSpace", "LinearSolveError", "SolverUnavailableError",
     "solve_darcy_quadrilateral", "CartesianQ1Plan", "BatchedFactorization", "condense_batched",
-    "GpuLocalSolver",
+    "GpuLocalSolver", "SkeletonFactorization", "OfflineQ1System",
 ]
 
 
@@ -33,6 +33,10 @@ def __getattr__(name):
         from . import batched
 
         return getattr(batched, name)
+    if name == "OfflineQ1System":
+        from . import offline
+
+        return offline.OfflineQ1System
     if name == "SkeletonFactorization":
         from . import skeleton
 

@@ -74,6 +74,11 @@ _SIGNATURES = {
     "mhm_q1_rhs_width": (C.c_int32, [C.POINTER(Q1Problem)]),
     "mhm_q1_condense_smem_bytes": (C.c_int64, [C.POINTER(Q1Problem), C.c_int32]),
     "mhm_q1_condense": (C.c_int, [C.POINTER(Q1Problem), C.c_int32, C.c_int32, C.c_double, P, P, P, P, P, P, P]),
+    "mhm_q1_factor_bytes": (C.c_int64, [C.POINTER(Q1Problem), C.c_int32]),
+    "mhm_q1_condense_offline": (C.c_int, [C.POINTER(Q1Problem), C.c_int32, C.c_int32, C.c_double, P, P, P, P, P,
+                                          P, P, P]),
+    "mhm_q1_source_response": (C.c_int, [C.POINTER(Q1Problem), C.c_int32, C.c_int32, C.c_double, P, P, P, P, P,
+                                         P, P]),
     "mhm_skeleton_scatter": (C.c_int, [C.c_int64, P, P, P, P, C.c_int64, C.c_int64, P, P, P, P, P, P, P]),
     "mhm_skeleton_workspace_bytes": (C.c_int64, [C.POINTER(SkeletonSystem), C.c_int32]),
     "mhm_skeleton_solve": (C.c_int, [C.POINTER(SkeletonSystem), P, P, P, C.c_double, C.c_double, C.c_int32,

@@ -55,6 +55,10 @@ struct Q1Args {
   int qorder;
   double gpt[kMaxQuad], gwt[kMaxQuad];
   int max_refine;
+  // 0: condense; 1: condense and store each cell's line-block inverses in factors;
+  // 2: source response only, with the stored factors (columns 0 only, no Schur block)
+  int mode;
+  void* factors;
   double tol;
   double* sol;
   double* blocks;
@@ -593,7 +597,12 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
   if (st == MHM_CELL_OK) st = flag[0];
 
   // ---- block LDL^T of the line blocks ------------------------------------------
-  if (st == MHM_CELL_OK) {
+  if (st == MHM_CELL_OK && a.mode == 2) {
+    // the factor of an earlier condensation of the same operator (offline / online)
+    const T* src = static_cast<const T*>(a.factors) + (size_t)cell * nny * nb;
+    for (int e = tid; e < nny * nb; e += blockDim.x) sinv[e] = src[e];
+    __syncthreads();
+  } else if (st == MHM_CELL_OK) {
     double dmin, dmax;
     int bad;
     if constexpr (NNX > 0) {
@@ -611,6 +620,10 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
       else if (dmin <= eps * n * dmax) st = MHM_CELL_RANK_DEFICIENT;
       __syncthreads();
     }
+    if (a.mode == 1 && st == MHM_CELL_OK) {
+      T* dst = static_cast<T*>(a.factors) + (size_t)cell * nny * nb;
+      for (int e = tid; e < nny * nb; e += blockDim.x) dst[e] = sinv[e];
+    }
   }
 
   // ---- refinement, one warp per right-hand-side column ---------------------------
@@ -622,7 +635,8 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
   for (int i = lane; i < n; i += 32) fz += fvec[i];
   fz = warp_sum(fz);
   const int t1 = t + 1;
-  for (int col = wid; col < w; col += nwarps) {
+  const int ncol = a.mode == 2 ? 1 : w;  // a source response refines the source column only
+  for (int col = wid; col < ncol; col += nwarps) {
     double s2 = 0.0;
     for (int i = lane; i < n; i += 32) {
       const double bv = rhs_value(a, col, i, fvec, az, cb);
@@ -820,7 +834,7 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
   __syncthreads();
   if (tid == 0) {
     int it = 0, ok = 1, nf = 0;
-    for (int col = 0; col < w; ++col) {
+    for (int col = 0; col < ncol; ++col) {
       it = citer[col] > it ? citer[col] : it;
       ok &= (cstat[col] == 1);
       nf |= (cstat[col] == 2);
@@ -988,27 +1002,61 @@ extern "C" int64_t mhm_q1_condense_smem_bytes(const mhm_q1_problem* p, int32_t p
   return (int64_t)a.smem;
 }
 
-extern "C" int mhm_q1_condense(const mhm_q1_problem* p, int32_t precision, int32_t max_refine,
-                               double tol, double* solution, double* blocks, double* loads,
-                               uint8_t* corrected, int32_t* cell_status, int32_t* cell_iters,
-                               void* stream) {
+namespace {
+int run_condense(const mhm_q1_problem* p, int32_t precision, int32_t max_refine, double tol, double* solution,
+                 double* blocks, double* loads, uint8_t* corrected, int32_t* cell_status, int32_t* cell_iters,
+                 int mode, void* factors, void* stream) {
   if (precision != MHM_PRECISION_FP64 && precision != MHM_PRECISION_MIXED) return MHM_ERR_ARGUMENT;
   Q1Args a;
   int rc = fill_args(p, precision, a);
   if (rc != MHM_OK) return rc;
-  if (!solution || !blocks || !loads || !corrected || !cell_status || !cell_iters || max_refine < 1 ||
-      !(tol > 0))
+  if (!solution || (!blocks && mode != 2) || !loads || !corrected || !cell_status || !cell_iters ||
+      max_refine < 1 || !(tol > 0) || (mode != 0 && !factors))
     return MHM_ERR_ARGUMENT;
   if (a.smem > 227 * 1024) return MHM_ERR_UNSUPPORTED;
   a.max_refine = max_refine; a.tol = tol;
   a.sol = solution; a.blocks = blocks; a.loads = loads; a.corrected = corrected;
   a.status = cell_status; a.iters = cell_iters;
+  a.mode = mode; a.factors = factors;
   const int cells = a.nx * a.ny;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int rc2 = precision == MHM_PRECISION_FP64 ? launch_condense<double>(a, cells, s)
                                                   : launch_condense<float>(a, cells, s);
   if (rc2 != MHM_OK) return rc2;
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+}  // namespace
+
+extern "C" int mhm_q1_condense(const mhm_q1_problem* p, int32_t precision, int32_t max_refine,
+                               double tol, double* solution, double* blocks, double* loads,
+                               uint8_t* corrected, int32_t* cell_status, int32_t* cell_iters,
+                               void* stream) {
+  return run_condense(p, precision, max_refine, tol, solution, blocks, loads, corrected, cell_status,
+                      cell_iters, 0, nullptr, stream);
+}
+
+extern "C" int64_t mhm_q1_factor_bytes(const mhm_q1_problem* p, int32_t precision) {
+  if (precision != MHM_PRECISION_FP64 && precision != MHM_PRECISION_MIXED) return -1;
+  Q1Args a;
+  if (fill_args(p, precision, a) != MHM_OK) return -1;
+  const int64_t tsz = precision == MHM_PRECISION_FP64 ? 8 : 4;
+  return (int64_t)a.nx * a.ny * a.nny * a.nnx * a.nnx * tsz;
+}
+
+extern "C" int mhm_q1_condense_offline(const mhm_q1_problem* p, int32_t precision, int32_t max_refine,
+                                       double tol, double* solution, double* blocks, double* loads,
+                                       uint8_t* corrected, int32_t* cell_status, int32_t* cell_iters,
+                                       void* factors, void* stream) {
+  return run_condense(p, precision, max_refine, tol, solution, blocks, loads, corrected, cell_status,
+                      cell_iters, 1, factors, stream);
+}
+
+extern "C" int mhm_q1_source_response(const mhm_q1_problem* p, int32_t precision, int32_t max_refine,
+                                      double tol, const void* factors, double* solution, double* loads,
+                                      uint8_t* corrected, int32_t* cell_status, int32_t* cell_iters,
+                                      void* stream) {
+  return run_condense(p, precision, max_refine, tol, solution, nullptr, loads, corrected, cell_status,
+                      cell_iters, 2, const_cast<void*>(factors), stream);
 }
 
 extern "C" int mhm_q1_reconstruct(const mhm_q1_problem* p, const double* solution,

@@ -347,7 +347,7 @@ class CartesianQ1Plan:
         q.source_mode, q.source, q.source_const = smode, _lib.ptr(source), float(sconst)
         self._keep = (kappa, source)
 
-    def launch(self, stream=None, *, reconstruct=True, events=None, global_stream=None):
+    def launch(self, stream=None, *, reconstruct=True, events=None, global_stream=None, local="condense"):
         """Enqueue the four kernels on ``stream`` (no host synchronisation).
 
         ``events``, if given, is a list of at least five ``torch.cuda.Event``s
@@ -356,6 +356,10 @@ class CartesianQ1Plan:
         after the local stage on that stream instead (ordered by an event), so that
         a serving loop can put the latency-bound global solve on a higher-priority
         stream and overlap it with the next request's local stage.
+        ``local`` selects the local stage: ``"condense"``; ``"offline"`` (condense and
+        keep each cell's factor, see ``prepare_offline``); ``"online"`` (source
+        response only with the kept factors; Schur blocks and the skeleton matrix
+        are reused, only the right-hand side is reduced).
         """
         L, s = self.lib, _lib.stream_handle(stream)
         P = _lib.ptr
@@ -371,12 +375,30 @@ class CartesianQ1Plan:
                 events[k].record(st)
 
         mark(0, cur)
-        _lib.check(L.mhm_q1_condense(self.q1, PRECISIONS[self.precision], self.max_refine, self.local_tol,
-                                     P(self.solution), P(self.blocks), P(self.loads), P(self.corrected),
-                                     P(self.cell_status), P(self.cell_iters), s), "mhm_q1_condense")
+        prec = PRECISIONS[self.precision]
+        if local == "condense":
+            _lib.check(L.mhm_q1_condense(self.q1, prec, self.max_refine, self.local_tol, P(self.solution),
+                                         P(self.blocks), P(self.loads), P(self.corrected), P(self.cell_status),
+                                         P(self.cell_iters), s), "mhm_q1_condense")
+        elif local == "offline":
+            _lib.check(L.mhm_q1_condense_offline(self.q1, prec, self.max_refine, self.local_tol, P(self.solution),
+                                                 P(self.blocks), P(self.loads), P(self.corrected),
+                                                 P(self.cell_status), P(self.cell_iters), P(self.factors), s),
+                       "mhm_q1_condense_offline")
+        elif local == "online":
+            if getattr(self, "factors", None) is None:
+                raise RuntimeError("prepare_offline() must run before online source responses")
+            _lib.check(L.mhm_q1_source_response(self.q1, prec, self.max_refine, self.local_tol, P(self.factors),
+                                                P(self.solution), P(self.loads), P(self.corrected),
+                                                P(self.cell_status), P(self.cell_iters), s),
+                       "mhm_q1_source_response")
+        else:
+            raise ValueError("local must be 'condense', 'offline' or 'online'")
         mark(1, cur)
         pat = self.pattern
-        _lib.check(L.mhm_skeleton_scatter(len(pat.indices), P(self.d_slot_ptr), P(self.d_contrib),
+        # online: the skeleton matrix is unchanged, only the right-hand side is reduced
+        _lib.check(L.mhm_skeleton_scatter(0 if local == "online" else len(pat.indices), P(self.d_slot_ptr),
+                                          P(self.d_contrib),
                                           P(self.blocks), P(self.values), self.N, self.T,
                                           P(self.d_load_ptr), P(self.d_load_contrib), P(self.loads),
                                           P(self.d_boundary), P(self.rhs), P(self.load_scale), s),
@@ -423,6 +445,39 @@ class CartesianQ1Plan:
             raise ValueError("incompatible data: gauge changed physical equations")
         del torch
         return info, stats
+
+    def prepare_offline(self, stream=None):
+        """Offline step of ``OfflineHybridSystem`` (``core/offline.py:148-229``): one full
+        solve with the current coefficients that also keeps every cell's factor in HBM
+        (``mhm_q1_factor_bytes``: 161 MB in FP64, 80 MB with binary32 factors at
+        64x64 x 16x16).  Later ``solve_source`` calls change the source only."""
+        nbytes = int(self.lib.mhm_q1_factor_bytes(self.q1, PRECISIONS[self.precision]))
+        if nbytes <= 0:
+            raise RuntimeError("could not size the factor store")
+        if getattr(self, "factors", None) is None or self.factors.numel() != nbytes:
+            self.factors = self.torch.empty(nbytes, dtype=self.torch.uint8, device=self.device)
+        self.launch(stream, local="offline")
+        self.check()
+
+    def set_source(self, source=0.0, *, non_blocking=False):
+        """Replace the source only (the permeability and the kept factors stay)."""
+        smode, sarr, sconst = source_input(source, self.mesh, self.rx, self.ry, self.order)
+        self.source = None if sarr is None else self.torch.as_tensor(np.array(sarr)).to(
+            self.device, non_blocking=non_blocking)
+        q = self.q1
+        q.source_mode, q.source, q.source_const = smode, _lib.ptr(self.source), float(sconst)
+        self._keep = (self._keep[0], self.source)
+
+    def solve_source(self, source=0.0, stream=None) -> Q1Solution:
+        """Online step (``OfflineHybridSystem.solve``, ``core/offline.py:231-307``): the
+        new source's local responses with the kept factors, the reduced right-hand
+        side, the global solve with the unchanged skeleton matrix, reconstruction."""
+        t0 = time.perf_counter()
+        self.set_source(source)
+        self.launch(stream, local="online")
+        sol = self.result()
+        sol.seconds = time.perf_counter() - t0
+        return sol
 
     def result(self, seconds=0.0) -> Q1Solution:
         info, stats = self.check()

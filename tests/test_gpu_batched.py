@@ -101,3 +101,32 @@ def test_gpu_local_solver_protocol():
     out = GpuLocalSolver()(aug.copy(), rhs.copy())
     assert out.shape == rhs.shape
     assert np.all(np.linalg.norm(aug @ out - rhs, axis=0) <= 1e-10 * np.linalg.norm(rhs, axis=0) + 1e-300)
+
+
+def test_condense_batched_uneven_sizes_keep_order():
+    """A mixed batch (three local sizes and right-hand-side widths, interleaved) is
+    grouped by (augmented size, rhs width) as ``cuda.py:300-305`` does and returned in
+    input order, each cell matching the reference's own lifts and source response."""
+    from types import SimpleNamespace
+
+    from pymhm_b200.batched import condense_batched
+    from tests._cases import load
+
+    cells = []
+    for name in ("poisson_8x8_r4_p1", "darcy_4x4_r16_p2_lognormal", "affine_3x2_rect_r4x5_p1s2"):
+        g = load(name)
+        for c in g["keep_cells"]:
+            cells.append((g[f"cell{c}_aug"], g[f"cell{c}_rhs"], g[f"cell{c}_source"], g[f"cell{c}_lifts"]))
+    order = np.random.default_rng(5).permutation(len(cells))
+    cells = [cells[i] for i in order]
+    assert len({(c[0].shape[0], c[1].shape[1]) for c in cells}) >= 3
+    probs = [SimpleNamespace(condensation_system=lambda aug=aug, rhs=rhs: (aug, rhs),
+                             response_from_solution=lambda s: s) for aug, rhs, _, _ in cells]
+    out = condense_batched(probs)
+    assert len(out) == len(cells)
+    for (aug, rhs, source, lifts), sol in zip(cells, out):
+        n, t = len(source), lifts.shape[1]
+        assert sol.shape == rhs.shape
+        assert np.linalg.norm(sol[:n, 1:1 + t] - lifts) <= 1e-10 * np.linalg.norm(lifts)
+        # some cells carry a numerically zero source response: bound it absolutely too
+        assert np.linalg.norm(sol[:n, 0] - source) <= 1e-10 * np.linalg.norm(source) + 1e-14

@@ -1,0 +1,66 @@
+"""Offline / online reuse (``core/offline.py``): new sources with the kept factors."""
+
+import numpy as np
+import pytest
+
+from tests._cases import CASES, load, rel
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-10, "mixed": 1e-8}
+
+
+def _setup(name):
+    from pymhm_b200.topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
+
+    g = load(name)
+    margs, (deg, sub), ref, perm, src, dr = CASES[name]
+    mesh = CartesianMacroMesh(*margs)
+    sk = SkeletonSpace(mesh, (FaceSpace.uniform(deg, sub),) * len(mesh.faces))
+    return g, mesh, sk, ref, perm(g), src, dr
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", ["darcy_4x4_r16_p2_lognormal", "poisson_8x8_r4_p1"])
+def test_online_source_matches_reference(name, precision):
+    """Prepared with another source, queried with the fixture's: the reference solution."""
+    from pymhm_b200.offline import OfflineQ1System
+
+    g, mesh, sk, ref, perm, src, dr = _setup(name)
+    with OfflineQ1System(mesh, sk, ref, permeability=perm, source=0.37, dirichlet=dr, precision=precision) as off:
+        sol = off.solve(src)
+        tol = TOL[precision]
+        assert rel(sol.trace, g["trace"]) <= tol
+        assert rel(sol.coarse, g["coarse"]) <= tol
+        assert rel(sol.fields, g["fields"]) <= tol
+        assert rel(sol.flux, g["flux"]) <= tol
+        assert sol.residual <= 1e-12
+
+
+def test_online_equals_a_fresh_solve():
+    """Several sources in order (``solve_many``) equal fresh full solves."""
+    from pymhm_b200.darcy import CartesianQ1Plan
+    from pymhm_b200.offline import OfflineQ1System
+
+    g, mesh, sk, ref, perm, src, dr = _setup("darcy_4x4_r16_p2_lognormal")
+    sources = [1.0, lambda x: np.sin(3 * x[:, 0]) * x[:, 1], 2.5]
+    with OfflineQ1System(mesh, sk, ref, permeability=perm, source=0.0, dirichlet=dr) as off:
+        online = off.solve_many(sources)
+    for s, on in zip(sources, online):
+        plan = CartesianQ1Plan(mesh, sk, ref, dirichlet=dr)
+        full = plan.solve(perm, s)
+        assert rel(on.trace, full.trace) <= 1e-11
+        assert rel(on.fields, full.fields) <= 1e-11
+        assert rel(on.flux, full.flux) <= 1e-11
+
+
+def test_online_needs_the_offline_step():
+    from pymhm_b200.darcy import CartesianQ1Plan
+
+    g, mesh, sk, ref, perm, src, dr = _setup("poisson_8x8_r4_p1")
+    plan = CartesianQ1Plan(mesh, sk, ref, dirichlet=dr)
+    plan.set_coefficients(perm, src)
+    with pytest.raises(RuntimeError):
+        plan.launch(local="online")
+    assert plan.lib.mhm_q1_factor_bytes(plan.q1, 0) == 64 * 5 * 5 * 5 * 8
+    assert plan.lib.mhm_q1_factor_bytes(plan.q1, 1) == 64 * 5 * 5 * 5 * 4
