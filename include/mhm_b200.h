@@ -28,6 +28,10 @@
  *   mhm_batched_factor /   replace BatchedFactorization.__init__/solve
  *   mhm_batched_solve      (execution/cuda.py:165-288): equilibrated dense LU
  *                          with FP64 residual refinement.
+ *   mhm_q1_condense_offline / mhm_q1_source_response
+ *                          replace OfflineLocalProblem's factor-once and
+ *                          one-column response (core/offline.py:99-145) for
+ *                          OfflineHybridSystem.solve (core/offline.py:234-307).
  */
 #ifndef MHM_B200_H
 #define MHM_B200_H
