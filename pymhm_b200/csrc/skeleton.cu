@@ -126,7 +126,7 @@ __device__ bool grid_sync(const Work& w, unsigned& epoch) {
   ++epoch;
   if (threadIdx.x == 0) {
     const unsigned target = epoch * gridDim.x;
-    __threadfence();
+    // the release orders every write of the CTA before the bar.sync above
     red_release_add(w.bar, 1u);
     long long spins = 0;
     while (ld_acquire(w.bar) < target) {
@@ -222,9 +222,9 @@ __device__ double csr_entry(const Sys& s, int64_t i, int64_t j) {
   return 0.0;
 }
 
-// Row stride of the shared-memory sine transform: = 8 (mod 16) doubles, so the
-// two half-warps of a transform step read disjoint banks.
-__host__ __device__ inline int q_stride(int nx) { return nx + ((8 - nx % 16) + 16) % 16; }
+// Row stride of the shared-memory sine transform: = 4 (mod 16) doubles, so the four
+// rows that a half-warp reads in one transform step fall in disjoint banks.
+__host__ __device__ inline int q_stride(int nx) { return nx + ((4 - nx % 16) + 16) % 16; }
 
 // Per-CTA state.  CTA r owns macro row r and the DOFs [d0, d1) first met in it.
 // Local DOFs ("G"): l < nown are the owned DOFs d0 + l; l >= nown (rows r > 0)
@@ -237,22 +237,23 @@ struct Row {
   int64_t d0, d1;
   double* Q;      // nx x qs: Q[k][i] = sqrt(2/(nx+1)) sin(pi (k+1)(i+1) / (nx+1))
   double* yrow;   // 3 nx
-  double* col;    // 8 nx: self, bottom, right, top, left sums; then self, up, down columns
+  double* col;    // 12 nx: faces' coarse sums across (1-4) and to the cell (8-11); combined (5)
   double* wrow;   // 3 nx
   double* mcheb;  // nmode (ny + 1): U_m(theta_k)
   double* mcinv;  // nmode: 1 / (ay U_ny(theta_k))
   double* ucol;   // ny
   double *vr, *vps, *vp, *vlam, *vu, *vt;  // G vectors: r, P S p, p, lambda, u, staging
-  double* cpart;  // nx t: per-cell partials
   double* Sb;     // nx np: packed symmetric S_c
   double* Pb;     // nx np: packed symmetric preconditioner block
   double *ga, *gb;  // G: G0 coefficient of the first / second cell
   int16_t *ya, *yb; // G: yrow index of the first / second cell (second: -1 = none)
   int32_t* gdof;    // G: global DOF
-  int16_t* cl;      // nx t: local DOF of each cell slot
-  double* gself;    // nx t: g0 of the cell on its slot
-  double* gnb;      // nx t: g0 of the other cell on the same DOF (0: none)
-  uint8_t* role;    // nx t: bit 0 = the cell is the DOF's second cell, bit 1 = the DOF has two cells
+  // per cell slot, stored [slot][cell] so that the lanes of a warp (one cell each)
+  // read consecutive entries:
+  int16_t* cl;      // t nx: local DOF
+  double* gself;    // t nx: g0 of the cell on the slot
+  double* gnb;      // t nx: g0 of the other cell on the same DOF (0: none)
+  uint8_t* role;    // t nx: bit 0 = the cell is the DOF's second cell, bit 1 = the DOF has two cells
   double* scratch;  // kWarps t t (aliases the G vectors during setup)
 };
 
@@ -265,24 +266,28 @@ __device__ __forceinline__ double g0y(const Row& R, int l) {
 
 // Packed index of (i, j) in a symmetric T x T block stored by upper rows.
 template <int T>
-__device__ __forceinline__ int packed(int a, int b) {
-  const int i = a < b ? a : b, j = a < b ? b : a;
-  return i * T - (i * (i - 1)) / 2 + (j - i);
+__host__ __device__ __forceinline__ constexpr int packed(int a, int b) {
+  return a < b ? a * T - (a * (a - 1)) / 2 + (b - a) : b * T - (b * (b - 1)) / 2 + (a - b);
 }
 
+// Distance between the packed blocks of consecutive cells: T (T + 1) / 2 rounded up
+// to an odd count of doubles, so that the lanes of a warp (one cell each) read
+// distinct shared-memory banks.
+__host__ __device__ __forceinline__ constexpr int block_stride(int t) { return (t * (t + 1) / 2) | 1; }
+
 // out(j, i, v): v = sum_k in[j][k] Q[k][i] for j < nin (in[j] in shared memory),
-// i < nx.  Warp w takes columns 8w .. 8w+7 (repeating every 128); lane bits 3-4
-// split k four ways, reduced by shuffles.
+// i < nx.  Warp w takes columns 4w .. 4w+3 (repeating every 64); lane bits 2-4
+// split k eight ways, reduced by shuffles.
 template <typename F>
 __device__ void sine_apply(const Row& R, int nx, int nin, const double* const* in, F out) {
-  const int lane = threadIdx.x & 31, q = lane >> 3;
-  for (int base = (threadIdx.x >> 5) * 8; base < nx; base += kWarps * 8) {
-    const int i = base + (lane & 7);
+  const int lane = threadIdx.x & 31, q = lane >> 2;
+  for (int base = (threadIdx.x >> 5) * 4; base < nx; base += kWarps * 4) {
+    const int i = base + (lane & 3);
     double acc[3] = {0.0, 0.0, 0.0};
     if (i < nx) {
       const double* qc = R.Q + i;
 #pragma unroll 4
-      for (int k = q; k < nx; k += 4) {
+      for (int k = q; k < nx; k += 8) {
         const double qv = qc[k * R.qs];
 #pragma unroll
         for (int j = 0; j < 3; ++j)
@@ -291,6 +296,7 @@ __device__ void sine_apply(const Row& R, int nx, int nin, const double* const* i
     }
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
+      acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], 4);
       acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], 8);
       acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], 16);
     }
@@ -432,38 +438,68 @@ __device__ void phase_begin(const Sys& s, const Work& w, const Row& R, int slot,
   __syncthreads();
 }
 
-// Per-cell products cpart[cx][a] = sum_b B_c[a][b] v[cl[cx][b]] (B packed symmetric);
-// returns this thread's sum of v[cl] * cpart (for (u, S u)).
-template <int T>
-__device__ double cell_matvec(const Sys& s, const Row& R, const double* B, const double* v) {
-  __syncthreads();
-  constexpr int np = T * (T + 1) / 2;
-  double dot = 0.0;
-  for (int idx = threadIdx.x; idx < s.nx * T; idx += blockDim.x) {
-    const int cx = idx / T, a = idx - cx * T;
-    const double* blk = B + (size_t)cx * np;
-    const int16_t* c = R.cl + cx * T;
-    double bv[T], xv[T];
+// Rows Q FS .. Q FS + FS - 1 (face Q) of one cell's product B_c v_c, with B_c
+// packed symmetric at blk and v_c in xv.  The face's rows go to the per-DOF
+// exchange arrays (first / second cell; skipped for null Xf) and, with `coarse`,
+// into the coarse sums of the face: col[(1 + Q) nx + cx] across the face to the
+// neighbour, col[(8 + Q) nx + cx] to the cell itself.  Returns the face's share of
+// v_c . B_c v_c.
+template <int FS, int Q>
+__device__ __forceinline__ double face_rows(const Row& R, const double* blk, int cx, int nx,
+                                            const double (&xv)[4 * FS], double* Xf, double* Xs, bool coarse) {
+  constexpr int T = 4 * FS;
+  double acc[FS];
 #pragma unroll
-    for (int b = 0; b < T; ++b) {
-      bv[b] = blk[packed<T>(a, b)];
-      xv[b] = v[c[b]];
+  for (int j = 0; j < FS; ++j) {
+    double a = 0.0;
+#pragma unroll
+    for (int b = 0; b < T; ++b) a = fma(blk[packed<T>(Q * FS + j, b)], xv[b], a);
+    acc[j] = a;
+  }
+  double dot = 0.0, self = 0.0, across = 0.0;
+#pragma unroll
+  for (int j = 0; j < FS; ++j) {
+    const int idx = (Q * FS + j) * nx + cx;
+    dot = fma(xv[Q * FS + j], acc[j], dot);
+    if (Xf) ((R.role[idx] & 1) ? Xs : Xf)[R.gdof[R.cl[idx]]] = acc[j];
+    if (coarse) {
+      self = fma(R.gself[idx], acc[j], self);
+      across = fma(R.gnb[idx], acc[j], across);
     }
-    double acc = 0.0;
-#pragma unroll
-    for (int b = 0; b < T; ++b) acc = fma(bv[b], xv[b], acc);
-    R.cpart[idx] = acc;
-    dot = fma(v[c[a]], acc, dot);
+  }
+  if (coarse) {
+    R.col[(1 + Q) * nx + cx] = across;
+    R.col[(8 + Q) * nx + cx] = self;
   }
   return dot;
 }
 
-// Partials of the row's cells to the per-DOF exchange arrays (first / second cell).
-__device__ void write_exchange(const Row& R, int nslot, double* Xf, double* Xs) {
-  for (int idx = threadIdx.x; idx < nslot; idx += blockDim.x) {
-    const int64_t i = R.gdof[R.cl[idx]];
-    ((R.role[idx] & 1) ? Xs : Xf)[i] = R.cpart[idx];
+// B_c v_c for every cell of the row (B packed symmetric, block_stride apart),
+// written to the exchange arrays and, with `coarse`, reduced to the faces' coarse
+// sums (see face_rows).  Warp w computes face w % 4 of cells 32 (w / 4) + lane, so
+// every block index is a compile-time constant within a warp.  Returns this
+// thread's part of sum_c v_c . B_c v_c.
+template <int FS>
+__device__ double cell_apply(const Sys& s, const Row& R, const double* B, const double* v, double* Xf, double* Xs,
+                             bool coarse) {
+  constexpr int T = 4 * FS;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, face = wid & 3, nx = s.nx;
+  const int step = 32 * ((int)(blockDim.x >> 5) >> 2);
+  double dot = 0.0;
+  for (int cx = lane + 32 * (wid >> 2); cx < nx; cx += step) {
+    const double* blk = B + (size_t)cx * block_stride(T);
+    double xv[T];
+#pragma unroll
+    for (int b = 0; b < T; ++b) xv[b] = v[R.cl[b * nx + cx]];
+    switch (face) {
+      case 0: dot += face_rows<FS, 0>(R, blk, cx, nx, xv, Xf, Xs, coarse); break;
+      case 1: dot += face_rows<FS, 1>(R, blk, cx, nx, xv, Xf, Xs, coarse); break;
+      case 2: dot += face_rows<FS, 2>(R, blk, cx, nx, xv, Xf, Xs, coarse); break;
+      default: dot += face_rows<FS, 3>(R, blk, cx, nx, xv, Xf, Xs, coarse); break;
+    }
   }
+  return dot;
 }
 
 // out[l] = Xf + Xs over the G DOFs (four loads of each array in flight per thread).
@@ -485,40 +521,26 @@ __device__ void read_exchange(const Row& R, const double* Xf, const double* Xs, 
   }
 }
 
-// Row-transformed coarse data of sum_c cpart_c (minus G0^T of the G vector
-// `minus`, if given) for this row and, through the shared faces, rows r+1, r-1.
-__device__ void partial_coarse(const Sys& s, const Row& R, const Coarse& U, const double* minus) {
-  const int nx = s.nx, t = s.t, fs = s.fs;
+// Row-transformed coarse data of the cell products of the last cell_apply (with
+// `coarse`), minus G0^T of the G vector `minus` if given, for this row and,
+// through the shared faces, rows r+1 and r-1.
+__device__ void coarse_combine(const Sys& s, const Row& R, const Coarse& U, const double* minus) {
+  const int nx = s.nx, t = s.t;
   __syncthreads();
-  // col[0..5nx): per cell the self sum and the sums across bottom, right, top, left
-  for (int idx = threadIdx.x; idx < 5 * nx; idx += blockDim.x) {
-    const int kind = idx / nx, cx = idx - kind * nx;
-    const double* p = R.cpart + cx * t;
-    double acc = 0.0;
-    if (kind == 0) {
-      const double* g = R.gself + cx * t;
-      for (int a = 0; a < t; ++a) acc = fma(g[a], p[a], acc);
-      if (minus) {
-        double m = 0.0;
-        for (int a = 0; a < t; ++a) m = fma(g[a], minus[R.cl[cx * t + a]], m);
-        acc -= m;
-      }
-    } else {
-      const int a0 = (kind - 1) * fs;
-      const double* g = R.gnb + cx * t;
-      for (int j = 0; j < fs; ++j) acc = fma(g[a0 + j], p[a0 + j], acc);
-    }
-    R.col[idx] = acc;
-  }
-  __syncthreads();
+  const double* own = R.col + 8 * nx;
   for (int cx = threadIdx.x; cx < nx; cx += blockDim.x) {
-    const double from_left = cx > 0 ? R.col[2 * nx + cx - 1] : 0.0;       // right side of cx-1
-    const double from_right = cx + 1 < nx ? R.col[4 * nx + cx + 1] : 0.0;  // left side of cx+1
-    R.col[5 * nx + cx] = (R.col[cx] + from_left) + from_right;
-    R.col[6 * nx + cx] = R.col[3 * nx + cx];  // to row r+1 (top)
-    R.col[7 * nx + cx] = R.col[nx + cx];      // to row r-1 (bottom)
+    double self = (own[cx] + own[nx + cx]) + (own[2 * nx + cx] + own[3 * nx + cx]);
+    if (minus) {
+      double m = 0.0;
+      for (int a = 0; a < t; ++a) m = fma(R.gself[a * nx + cx], minus[R.cl[a * nx + cx]], m);
+      self -= m;
+    }
+    const double from_left = cx > 0 ? R.col[2 * nx + cx - 1] : 0.0;       // right face of cx-1
+    const double from_right = cx + 1 < nx ? R.col[4 * nx + cx + 1] : 0.0;  // left face of cx+1
+    R.col[5 * nx + cx] = (self + from_left) + from_right;
   }
-  const int src[3] = {5, 6, 7};
+  // to row r+1: the top faces' sums; to row r-1: the bottom faces'
+  const int src[3] = {5, 3, 1};
   double* const dst[3] = {U.self, R.r + 1 < s.ny ? U.below : nullptr, R.r > 0 ? U.above : nullptr};
   const int shift[3] = {0, 1, -1};
   coarse_rowfwd(s, R, 3, src, dst, shift);
@@ -532,7 +554,7 @@ __device__ void dof_coarse(const Sys& s, const Row& R, const double* v0, const d
     const int j = idx / nx, cx = idx - j * nx;
     const double* v = j ? v1 : v0;
     double acc = 0.0;
-    for (int a = 0; a < t; ++a) acc = fma(R.gself[cx * t + a], v[R.cl[cx * t + a]], acc);
+    for (int a = 0; a < t; ++a) acc = fma(R.gself[a * nx + cx], v[R.cl[a * nx + cx]], acc);
     R.col[idx] = acc;
   }
 }
@@ -567,7 +589,7 @@ __host__ __device__ size_t smem_layout(int nx, int ny, int fs, int t, int grid, 
   // a row owns at most 3 nx + 1 faces (row 0); later rows own 2 nx + 1 and add the
   // nx bottom faces of their cells
   const size_t g = (size_t)(3 * nx + 1) * fs;
-  const size_t np = (size_t)t * (t + 1) / 2;
+  const size_t np = (size_t)block_stride(t);
   const size_t vec = 6 * g > (size_t)kWarps * t * t ? 6 * g : (size_t)kWarps * t * t;
   const size_t nmode = grid > 0 ? (size_t)((nx + grid - 1) / grid) : 1;
   size_t o = 0;
@@ -578,24 +600,23 @@ __host__ __device__ size_t smem_layout(int nx, int ny, int fs, int t, int grid, 
   };
   take((size_t)nx * q_stride(nx) * 8);   // 0 Q
   take(3 * (size_t)nx * 8);              // 1 yrow
-  take(8 * (size_t)nx * 8);              // 2 col
+  take(12 * (size_t)nx * 8);             // 2 col
   take(3 * (size_t)nx * 8);              // 3 wrow
   take(nmode * (ny + 1) * 8);            // 4 mcheb
   take(nmode * 8);                       // 5 mcinv
   take((size_t)ny * 8);                  // 6 ucol
   take(vec * 8);                         // 7 G vectors (6 g) / setup scratch
-  take((size_t)nx * t * 8);              // 8 cpart
-  take((size_t)nx * np * 8);             // 9 Sb
-  take((size_t)nx * np * 8);             // 10 Pb
-  take(g * 8);                           // 11 ga
-  take(g * 8);                           // 12 gb
-  take(g * 2);                           // 13 ya
-  take(g * 2);                           // 14 yb
-  take(g * 4);                           // 15 gdof
-  take((size_t)nx * t * 2);              // 16 cl
-  take((size_t)nx * t * 8);              // 17 gself
-  take((size_t)nx * t * 8);              // 18 gnb
-  take((size_t)nx * t);                  // 19 role
+  take((size_t)nx * np * 8);             // 8 Sb
+  take((size_t)nx * np * 8);             // 9 Pb
+  take(g * 8);                           // 10 ga
+  take(g * 8);                           // 11 gb
+  take(g * 2);                           // 12 ya
+  take(g * 2);                           // 13 yb
+  take(g * 4);                           // 14 gdof
+  take((size_t)nx * t * 2);              // 15 cl
+  take((size_t)nx * t * 8);              // 16 gself
+  take((size_t)nx * t * 8);              // 17 gnb
+  take((size_t)nx * t);                  // 18 role
   off[k] = o;
   return o;
 }
@@ -603,7 +624,7 @@ __host__ __device__ size_t smem_layout(int nx, int ny, int fs, int t, int grid, 
 template <int FS>
 __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Params P) {
   constexpr int T = 4 * FS;
-  constexpr int np = T * (T + 1) / 2;
+  constexpr int np = block_stride(T);
   const Sys& s = P.s;
   const Work& w = P.w;
   __shared__ double red[64];
@@ -641,18 +662,17 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
     R.vr = v; R.vps = v + g; R.vp = v + 2 * g; R.vlam = v + 3 * g; R.vu = v + 4 * g; R.vt = v + 5 * g;
     R.scratch = v;
   }
-  R.cpart = reinterpret_cast<double*>(dyn + off[8]);
-  R.Sb = reinterpret_cast<double*>(dyn + off[9]);
-  R.Pb = reinterpret_cast<double*>(dyn + off[10]);
-  R.ga = reinterpret_cast<double*>(dyn + off[11]);
-  R.gb = reinterpret_cast<double*>(dyn + off[12]);
-  R.ya = reinterpret_cast<int16_t*>(dyn + off[13]);
-  R.yb = reinterpret_cast<int16_t*>(dyn + off[14]);
-  R.gdof = reinterpret_cast<int32_t*>(dyn + off[15]);
-  R.cl = reinterpret_cast<int16_t*>(dyn + off[16]);
-  R.gself = reinterpret_cast<double*>(dyn + off[17]);
-  R.gnb = reinterpret_cast<double*>(dyn + off[18]);
-  R.role = reinterpret_cast<uint8_t*>(dyn + off[19]);
+  R.Sb = reinterpret_cast<double*>(dyn + off[8]);
+  R.Pb = reinterpret_cast<double*>(dyn + off[9]);
+  R.ga = reinterpret_cast<double*>(dyn + off[10]);
+  R.gb = reinterpret_cast<double*>(dyn + off[11]);
+  R.ya = reinterpret_cast<int16_t*>(dyn + off[12]);
+  R.yb = reinterpret_cast<int16_t*>(dyn + off[13]);
+  R.gdof = reinterpret_cast<int32_t*>(dyn + off[14]);
+  R.cl = reinterpret_cast<int16_t*>(dyn + off[15]);
+  R.gself = reinterpret_cast<double*>(dyn + off[16]);
+  R.gnb = reinterpret_cast<double*>(dyn + off[17]);
+  R.role = reinterpret_cast<uint8_t*>(dyn + off[18]);
   {
     // DOFs are numbered by their first cell: binary search the row boundaries
     auto lower = [&](int cell) {
@@ -718,14 +738,15 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
     const int cx = idx / T, a = idx - cx * T;
     const int c = R.c0 + cx;
     const int64_t i = s.cell_dofs[(size_t)c * T + a];
-    R.cl[idx] = (int16_t)(i >= R.d0 && i < R.d1 ? i - R.d0 : R.nown + cx * FS + a);
+    const int sl = a * nx + cx;
+    R.cl[sl] = (int16_t)(i >= R.d0 && i < R.d1 ? i - R.d0 : R.nown + cx * FS + a);
     const int first = s.dof_cells[2 * i];
     const bool second = first != c;
-    R.role[idx] = (uint8_t)((second ? 1 : 0) | (s.dof_cells[2 * i + 1] >= 0 ? 2 : 0));
-    R.gself[idx] = s.g0[(size_t)c * T + a];
+    R.role[sl] = (uint8_t)((second ? 1 : 0) | (s.dof_cells[2 * i + 1] >= 0 ? 2 : 0));
+    R.gself[sl] = s.g0[(size_t)c * T + a];
     const int other = second ? first : s.dof_cells[2 * i + 1];
     const int oslot = second ? s.dof_slot[2 * i] : s.dof_slot[2 * i + 1];
-    R.gnb[idx] = other >= 0 ? s.g0[(size_t)other * T + oslot] : 0.0;
+    R.gnb[sl] = other >= 0 ? s.g0[(size_t)other * T + oslot] : 0.0;
   }
   // DOFs met by one cell only: their second-cell partials stay zero
   for (int64_t i = R.d0 + tid; i < R.d1; i += nth)
@@ -747,7 +768,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       const int64_t ia = s.cell_dofs[(size_t)c * T + a], ib = s.cell_dofs[(size_t)c * T + b];
       v = 0.5 * (csr_entry(s, ia, ib) + csr_entry(s, ib, ia));
       // an entry between two DOFs of a face shared with another cell is split evenly
-      if (a / FS == b / FS && (R.role[cx * T + a] & 2)) v *= 0.5;
+      if (a / FS == b / FS && (R.role[a * nx + cx] & 2)) v *= 0.5;
     }
     R.Sb[(size_t)cx * np + packed<T>(a, b)] = v;
   }
@@ -849,9 +870,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       coarse_rows(s, R, w.Wx1, R.r - 1, R.r + 2);
       for (int l = tid; l < R.ng; l += nth) R.vlam[l] = -g0y(R, l);
       for (int l = tid; l < R.ng; l += nth) R.vt[l] = __ldcg(w.rfull + R.gdof[l]);
-      cell_matvec<T>(s, R, R.Sb, R.vlam);
-      __syncthreads();
-      write_exchange(R, nx * T, w.Vf, w.Vs);
+      cell_apply<FS>(s, R, R.Sb, R.vlam, w.Vf, w.Vs, false);
       SYNC_OR_EXIT();
       // rhoP = r1 - S lambda0 on G; its coarse data
       read_exchange(R, w.Vf, w.Vs, R.vu);
@@ -868,10 +887,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       {
         double r2 = 0.0;
         for (int l = tid; l < R.nown; l += nth) r2 = fma(R.vr[l], R.vr[l], r2);
-        cell_matvec<T>(s, R, R.Pb, R.vr);
-        __syncthreads();
-        write_exchange(R, nx * T, w.Zf, w.Zs);
-        partial_coarse(s, R, w.Uz, nullptr);
+        cell_apply<FS>(s, R, R.Pb, R.vr, w.Zf, w.Zs, true);
+        coarse_combine(s, R, w.Uz, nullptr);
         put_partial(w, 0, r2, red);
       }
       SYNC_OR_EXIT();
@@ -892,14 +909,13 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
           break;
         }
         if (k >= P.max_inner) { status = MHM_SOLVE_NOT_CONVERGED; break; }
+#pragma unroll 2
         for (int l = tid; l < R.ng; l += nth) R.vu[l] = R.vt[l] - g0y(R, l);
         double gam = 0.0;
         for (int l = tid; l < R.nown; l += nth) gam = fma(R.vr[l], R.vu[l], gam);
         {
-          const double del = cell_matvec<T>(s, R, R.Sb, R.vu);
-          __syncthreads();
-          write_exchange(R, nx * T, w.Vf, w.Vs);
-          partial_coarse(s, R, w.Uw, nullptr);
+          const double del = cell_apply<FS>(s, R, R.Sb, R.vu, w.Vf, w.Vs, true);
+          coarse_combine(s, R, w.Uw, nullptr);
           put_partial2(w, 1, gam, del, red);
         }
         SYNC_OR_EXIT();
@@ -914,6 +930,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
           const double pq = k > 0 ? d - beta * g / alpha_prev : d;
           if (!(pq > 0.0) || !isfinite(g)) { status = MHM_SOLVE_BREAKDOWN; break; }
           const double alpha = g / pq;
+#pragma unroll 2
           for (int l = tid; l < R.ng; l += nth) {
             const double pw = R.vt[l] - g0y(R, l);
             const double ps = k > 0 ? fma(beta, R.vps[l], pw) : pw;
@@ -947,10 +964,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
         {
           double r2 = 0.0;
           for (int l = tid; l < R.nown; l += nth) r2 = fma(R.vr[l], R.vr[l], r2);
-          cell_matvec<T>(s, R, R.Pb, R.vr);
-          __syncthreads();
-          write_exchange(R, nx * T, w.Zf, w.Zs);
-          partial_coarse(s, R, w.Uz, nullptr);
+          cell_apply<FS>(s, R, R.Pb, R.vr, w.Zf, w.Zs, true);
+          coarse_combine(s, R, w.Uz, nullptr);
           put_partial(w, 0, r2, red);
         }
         SYNC_OR_EXIT();
@@ -961,8 +976,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       if (status != MHM_SOLVE_OK) goto finish;
       // c = (G0^T G0)^-1 G0^T (S lambda - r1): cell partials of S lambda, minus r1
       for (int l = tid; l < R.ng; l += nth) R.vt[l] = __ldcg(w.rfull + R.gdof[l]);
-      cell_matvec<T>(s, R, R.Sb, R.vlam);
-      partial_coarse(s, R, w.Uw, R.vt);
+      cell_apply<FS>(s, R, R.Sb, R.vlam, nullptr, nullptr, true);
+      coarse_combine(s, R, w.Uw, R.vt);
       SYNC_OR_EXIT();
       mode_solve(s, R, w.Uw, w.Ww);
       SYNC_OR_EXIT();
