@@ -55,7 +55,7 @@ CPU_SAMPLE_CELLS = 4096
 # DRAM bytes (read + write) per launch of this workload's kernels, from the ncu
 # captures summarised in profiles/skeleton_pcg_darcy64_r16_p2.md and
 # profiles/q1_condense_darcy64_r16_p2_mixed.md.
-NCU_DRAM_BYTES = {"skeleton_pcg": 15.4e6, "q1_condense": 92.3e6}
+NCU_DRAM_BYTES = {"skeleton_pcg": 15.3e6, "q1_condense": 92.3e6}
 
 
 def parse():
