@@ -32,6 +32,11 @@
  *                          replace OfflineLocalProblem's factor-once and
  *                          one-column response (core/offline.py:99-145) for
  *                          OfflineHybridSystem.solve (core/offline.py:234-307).
+ *   mhm_q1_original_defect / mhm_refine_norms / mhm_q1_correction_response /
+ *   mhm_q1_flux / mhm_vector_accumulate
+ *                          replace the residual evaluation and the defect-source
+ *                          correction of refine_hybrid (core/refinement.py:612-800)
+ *                          for the Cartesian Q1 path.
  */
 #ifndef MHM_B200_H
 #define MHM_B200_H
@@ -92,8 +97,10 @@ typedef struct mhm_q1_problem {
     const double* kappa;          /* global fine grid, [gx][gy][comp] (x-major)    */
     double kappa_const[3];        /* kxx, kxy, kyy for kappa_mode 0                */
     int32_t source_mode;          /* 0 constant, 1 per fine cell,
-                                     2 per Gauss point of the fine cell            */
-    const double* source;         /* [gx][gy] or [gx][gy][q] (q = qy*order + qx)   */
+                                     2 per Gauss point of the fine cell,
+                                     3 nodal load vector of each cell              */
+    const double* source;         /* [gx][gy] or [gx][gy][q] (q = qy*order + qx);
+                                     mode 3: [cell][node], node = iy*(rx+1)+ix     */
     double source_const;
     int32_t quad_order;           /* Gauss points per axis for source_mode 2      */
 } mhm_q1_problem;
@@ -150,6 +157,56 @@ int mhm_q1_source_response(const mhm_q1_problem* p /* host */, int32_t precision
                            int32_t max_refine, double tol, const void* factors, double* solution,
                            double* loads, uint8_t* corrected, int32_t* cell_status,
                            int32_t* cell_iters, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Original-equation refinement (core/refinement.py:612-800)                 */
+/* ------------------------------------------------------------------------ */
+/*
+ * Residual of the uncondensed equations at a hybrid solution (x: trace then
+ * coarse unknowns; fields: (cells, n) nodal values), refinement.py:718-738:
+ * defect[cell][i] = f - B lambda - A u (each row in double-double arithmetic),
+ * slot_terms[cell][j] = (B^T u)_j, weak[g] = boundary[g] - the DOF's slot terms
+ * (first cell, then second; boundary may be NULL = 0), and per cell
+ * partial[cell] = {d.d, f.f, sum d}.  p's source and permeability are those of
+ * the original problem.
+ */
+int mhm_q1_original_defect(const mhm_q1_problem* p /* host */, const int64_t* cell_dofs,
+                           int64_t trace_size, const int32_t* dof_cells, const int32_t* dof_slot,
+                           const double* x, const double* fields, const double* boundary,
+                           double* defect, double* slot_terms, double* weak, double* partial,
+                           void* stream);
+
+/*
+ * Norms of one refinement step, summed in a fixed order by one block:
+ * out[0] = ||[defects; weak]||^2, out[1] = ||[loads; boundary]||^2,
+ * out[2] = ||[weak; sum d per cell]||^2 and, if indptr is given, out[3] =
+ * ||rhs||^2 and out[4] = || |K| |x| ||^2 of the assembled CSR system (size rows).
+ */
+int mhm_refine_norms(int32_t cells, const double* partial, int64_t trace_size, const double* weak,
+                     const double* boundary, int64_t size, const int64_t* indptr,
+                     const int32_t* indices, const double* values, const double* x,
+                     const double* rhs, double* out /* 5 */, void* stream);
+
+/*
+ * Correction source responses (refinement.py:779-798): solution column 0 and
+ * `loads` become the response to p's source and its reduced load, as in
+ * mhm_q1_source_response; p carries the defects as nodal loads (source_mode 3).
+ * factors from mhm_q1_condense_offline of the same operator, or NULL to factor
+ * each cell again.  The corrected fields are the old ones plus the
+ * reconstruction (mhm_q1_reconstruct) of this response with the correction's
+ * trace and coarse values.
+ */
+int mhm_q1_correction_response(const mhm_q1_problem* p /* host */, int32_t precision,
+                               int32_t max_refine, double tol, const void* factors,
+                               double* solution, double* loads, uint8_t* corrected,
+                               int32_t* cell_status, int32_t* cell_iters, void* stream);
+
+/* Flux -K grad u at the fine-cell centres from given nodal fields (cells, n):
+ * the flux part of mhm_q1_reconstruct (postprocessing/solutions.py:278-324). */
+int mhm_q1_flux(const mhm_q1_problem* p /* host */, const double* fields, double* flux, void* stream);
+
+/* dst[i] += src[i], i < n (the hybrid unknowns plus a correction). */
+int mhm_vector_accumulate(int64_t n, double* dst, const double* src, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Ordered skeleton reduction                                                 */

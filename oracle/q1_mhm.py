@@ -708,6 +708,61 @@ def solve_darcy_q1(mesh, skeleton, refinement, permeability=1.0, source=0.0, dir
 
 
 # --------------------------------------------------------------------------------------
+# Original-equation refinement: core/refinement.py:612-800 (no fixed DOFs, no moments)
+# --------------------------------------------------------------------------------------
+def refine_q1(mesh, skeleton, refinement, trace, coarse, fields, permeability=1.0, source=0.0, dirichlet=0.0,
+              max_steps=2, min_steps=0, rtol=1e-10, atol=0.0, order=4):
+    """``refine_hybrid`` for the Cartesian Q1 system (``refinement.py:612-800``).
+
+    Residual of the uncondensed equations (``:718-738``): local defects
+    ``f - B lambda - A u`` (accurate residuals, ``:721-727``) and the weak trace rows
+    ``boundary - sum B^T u`` (``:729-731``); acceptance at ``max(atol, rtol ||rhs||)``
+    (``:687-690, :739-765``); each correction solves every cell with its defect as the
+    source, assembles the correction system with the weak residual as boundary load
+    and adds its solution (``:772-800``).
+    """
+    boundary, _ = boundary_data(skeleton, dirichlet, None, order)
+    probs = [local_problem(mesh, skeleton, c, refinement, permeability, source, order)[1]
+             for c in range(len(mesh.cells))]
+    trace = np.array(trace, dtype=float)
+    coarse = np.array(coarse, dtype=float)
+    fields = [np.array(u, dtype=float) for u in fields]
+    rhs_norm = float(np.linalg.norm(np.concatenate([p.load for p in probs] + [boundary])))
+    threshold = max(atol, rtol * rhs_norm)
+    history, step = [], 0
+    while True:
+        defects = []
+        weak = boundary.copy()
+        for p, u in zip(probs, fields):
+            forcing = accurate_residual(sparse.csr_matrix(p.coupling), p.load, trace[p.trace_dofs])
+            defects.append(accurate_residual(p.matrix.tocsr(), forcing, u))
+            np.add.at(weak, p.trace_dofs, -p.coupling.T @ u)
+        residual = float(np.linalg.norm(np.concatenate([*defects, weak])))
+        history.append(residual)
+        if step >= min_steps and np.isfinite(residual) and residual <= threshold:
+            retained = [np.sum(np.asarray(d, dtype=float)) for d in defects]
+            return dict(trace=trace, coarse=coarse, fields=np.array(fields), residual_norms=tuple(history),
+                        rhs_norm=rhs_norm, reduced=float(np.linalg.norm(np.r_[weak, retained])))
+        if step == max_steps or not np.isfinite(residual):
+            raise LinearSolveError(f"original hybrid residual {residual:.6e} exceeds {threshold:.6e} "
+                                   f"after {step} corrections")
+        contribs, responses = [], []
+        for c, (p, d) in enumerate(zip(probs, defects)):
+            resp = condense(LocalProblem(p.matrix, p.coupling, np.asarray(d, dtype=float), p.trace_dofs,
+                                         p.constraints))
+            contribs.append(contribution(resp, skeleton.size + c))
+            responses.append(resp)
+        matrix, rhs, scale = assemble_global(contribs, skeleton.size, weak)
+        x, _ = solve_global(matrix, rhs, scale)
+        dtrace, dcoarse = x[: skeleton.size], x[skeleton.size:]
+        trace += dtrace
+        coarse += dcoarse
+        fields = [u + r.source - r.lifts @ dtrace[r.problem.trace_dofs] + r.retained @ dcoarse[c: c + 1]
+                  for c, (u, r) in enumerate(zip(fields, responses))]
+        step += 1
+
+
+# --------------------------------------------------------------------------------------
 # Timed CPU baseline: the local stage of the oracle over a sample of macrocells
 # --------------------------------------------------------------------------------------
 _SAMPLE_STATE = {}

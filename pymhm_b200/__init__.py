@@ -8,7 +8,10 @@ Public entry points:
   reference's batched GPU local algebra and ``LocalLinearSolver`` protocol
   (``pymhm_b200.batched``);
 * ``SkeletonFactorization`` - a ``LinearFactorization``-style global solver for
-  ``HybridSystem.solve(factorization=...)`` (``pymhm_b200.skeleton``).
+  ``HybridSystem.solve(factorization=...)`` (``pymhm_b200.skeleton``);
+* ``OfflineQ1System`` - factors kept for repeated sources (``pymhm_b200.offline``);
+* ``refine_hybrid`` / ``CartesianQ1Plan.refine`` - defect correction of the original
+  uncondensed equations (``pymhm_b200.darcy``).
 
 Compute runs in ``libmhm_b200.so`` (hand-written sm_100a CUDA behind a C ABI);
 importing this package does not touch the GPU.
@@ -20,12 +23,12 @@ from .topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
 __all__ = [
     "CartesianMacroMesh", "FaceSpace", "SkeletonSpace", "LinearSolveError", "SolverUnavailableError",
     "solve_darcy_quadrilateral", "CartesianQ1Plan", "BatchedFactorization", "condense_batched",
-    "GpuLocalSolver", "SkeletonFactorization", "OfflineQ1System",
+    "GpuLocalSolver", "SkeletonFactorization", "OfflineQ1System", "refine_hybrid", "HybridRefinement",
 ]
 
 
 def __getattr__(name):
-    if name in ("solve_darcy_quadrilateral", "CartesianQ1Plan", "Q1Solution"):
+    if name in ("solve_darcy_quadrilateral", "CartesianQ1Plan", "Q1Solution", "refine_hybrid", "HybridRefinement"):
         from . import darcy
 
         return getattr(darcy, name)

@@ -56,7 +56,8 @@ struct Q1Args {
   double gpt[kMaxQuad], gwt[kMaxQuad];
   int max_refine;
   // 0: condense; 1: condense and store each cell's line-block inverses in factors;
-  // 2: source response only, with the stored factors (columns 0 only, no Schur block)
+  // 2: source response only, with the stored factors (columns 0 only, no Schur block);
+  // 3: source response only, with a fresh factorization
   int mode;
   void* factors;
   double tol;
@@ -385,46 +386,18 @@ struct Occupancy {
 
 // NNX > 0: the factorization runs in one warp's registers for lines of NNX nodes;
 // NNX = 0: any line length, factorization in shared memory by the whole block.
-template <typename T, int NNX>
-__global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_kernel(const Q1Args a) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int cell = blockIdx.x;
-  const int tid = threadIdx.x;
-  const int n = a.n, nnx = NNX > 0 ? NNX : a.nnx, nny = a.nny, w = a.w, t = a.t;
-  const int nb = nnx * nnx, np1 = n + 1;
-  const int lane = tid & 31, wid = tid >> 5, nwarps = blockDim.x >> 5;
-  T* sinv = reinterpret_cast<T*>(smem + a.off_sinv);  // nny blocks of nnx x nnx, row-major
-  T* gj0 = reinterpret_cast<T*>(smem + a.off_gj);     // Gauss-Jordan ping-pong (NNX = 0)
-  T* gj1 = gj0 + nb;
-  T* cdn = reinterpret_cast<T*>(smem + a.off_cpl);    // (n, 3): to (y-1, x-1), (y-1, x), (y-1, x+1)
-  T* dg = cdn + 3 * n;                                // (n): scaled diagonal
-  T* dl = dg + n;                                     // (n): scaled coupling to (y, x-1)
-  double* cb = reinterpret_cast<double*>(smem + a.off_cb);  // (t, kmax) boundary couplings
-  double* zb = cb + (size_t)t * a.kmax;                     // (t): sum of each column's couplings
-  double* sten = reinterpret_cast<double*>(smem + a.off_sten);
-  double* fvec = reinterpret_cast<double*>(smem + a.off_vec);
-  double* az = fvec + n;
-  double* ctil = az + n;
-  double* dsc = ctil + n;
-  // per-warp column buffers: x (n+1 doubles) and residual / solve vector (n+1 T)
-  const size_t wstride = align16((size_t)np1 * 8) + align16((size_t)np1 * sizeof(T)) + 64 * sizeof(T);
-  double* xw = reinterpret_cast<double*>(smem + a.off_warp + wid * wstride);
-  T* rw = reinterpret_cast<T*>(smem + a.off_warp + wid * wstride + align16((size_t)np1 * 8));
-  T* tb = reinterpret_cast<T*>(smem + a.off_warp + wid * wstride + align16((size_t)np1 * 8) +
-                               align16((size_t)np1 * sizeof(T)));  // 2 x 32 T: broadcast buffers
-  double* kel = reinterpret_cast<double*>(smem + a.off_warp);  // aliases the warp buffers
-  double* fel = kel + 3 * a.rx * a.ry;
-  double* red = reinterpret_cast<double*>(smem + a.off_misc);
-  double* rnorm = red + 32;
-  int* cstat = reinterpret_cast<int*>(rnorm + w);  // per column: 1 converged, 2 non-finite
-  int* citer = cstat + w;
-  int* flag = citer + w;
-
+// Local assembly of one macrocell (quadrilateral.py:191-253, cartesian.py:69-83):
+// element coefficients kel (3 ne) and loads fel (4 ne), the trace coupling of every
+// boundary node cb (t kmax) and its column sums zb (t), and node-wise the lower
+// stencil of A sten (5 n), the load f (n) and the constraint c = M 1 (n).  Each
+// thread returns its part of max|A|, ||A||_F^2 and max c.
+__device__ __forceinline__ void assemble_cell(const Q1Args& a, int cell, double* kel, double* fel, double* cb,
+                                              double* zb, double* sten, double* fvec, double* ctil, double& amax,
+                                              double& fro, double& cmax) {
+  const int tid = threadIdx.x, n = a.n, t = a.t, nnx = a.nnx;
   const int cx = cell % a.nx, cy = cell / a.nx;
   const int ne = a.rx * a.ry;
-  double* xg = a.sol + (size_t)cell * w * np1;
-
-  // ---- element coefficients and element loads; boundary coupling table ---------
+  // element coefficients and element loads; boundary coupling table ---------
   for (int e = tid; e < ne; e += blockDim.x) {
     const int ex = e % a.rx, ey = e / a.rx;
     const size_t g = (size_t)(cx * a.rx + ex) * a.NYf + (cy * a.ry + ey);
@@ -438,7 +411,9 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
     }
     kel[3 * e] = kxx; kel[3 * e + 1] = kxy; kel[3 * e + 2] = kyy;
     double fe[4];
-    if (a.smode == 2) {
+    if (a.smode == 3) {
+      fe[0] = fe[1] = fe[2] = fe[3] = 0.0;  // nodal loads are given, see the gather
+    } else if (a.smode == 2) {
       const int Q = a.qorder;
       fe[0] = fe[1] = fe[2] = fe[3] = 0.0;
       for (int qy = 0; qy < Q; ++qy)
@@ -463,7 +438,6 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
     const Side sd = trace_side(a, j);
     cb[idx] = k < side_len(a, sd.s) ? coupling(a, cell, sd.s, k, sd.q) : 0.0;
   }
-  if (tid == 0) flag[0] = 0;
   __syncthreads();
   for (int j = tid; j < t; j += blockDim.x) {
     double acc = 0.0;
@@ -472,9 +446,9 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
     zb[j] = acc;
   }
 
-  // ---- node-wise gather of the lower stencil, load and constraint -------------
+  // node-wise gather of the lower stencil, load and constraint -------------
   const double rxy = a.hy / a.hx, ryx = a.hx / a.hy;
-  double amax = 0.0, fro = 0.0, cmax = 0.0;
+  amax = fro = cmax = 0.0;
   for (int i = tid; i < n; i += blockDim.x) {
     const int ix = i % nnx, iy = i / nnx;
     double sv[5] = {0, 0, 0, 0, 0};
@@ -518,7 +492,7 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
       ++count;
     }
     for (int q = 0; q < 5; ++q) sten[5 * i + q] = sv[q];
-    fvec[i] = f;
+    fvec[i] = a.smode == 3 ? a.src[(size_t)cell * n + i] : f;
     ctil[i] = count * (a.area * 0.25);
     amax = fmax(amax, fabs(sv[0]));
     fro += sv[0] * sv[0];
@@ -529,6 +503,48 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
     cmax = fmax(cmax, ctil[i]);
   }
   __syncthreads();
+}
+
+template <typename T, int NNX>
+__global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_kernel(const Q1Args a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int cell = blockIdx.x;
+  const int tid = threadIdx.x;
+  const int n = a.n, nnx = NNX > 0 ? NNX : a.nnx, nny = a.nny, w = a.w, t = a.t;
+  const int nb = nnx * nnx, np1 = n + 1;
+  const int lane = tid & 31, wid = tid >> 5, nwarps = blockDim.x >> 5;
+  T* sinv = reinterpret_cast<T*>(smem + a.off_sinv);  // nny blocks of nnx x nnx, row-major
+  T* gj0 = reinterpret_cast<T*>(smem + a.off_gj);     // Gauss-Jordan ping-pong (NNX = 0)
+  T* gj1 = gj0 + nb;
+  T* cdn = reinterpret_cast<T*>(smem + a.off_cpl);    // (n, 3): to (y-1, x-1), (y-1, x), (y-1, x+1)
+  T* dg = cdn + 3 * n;                                // (n): scaled diagonal
+  T* dl = dg + n;                                     // (n): scaled coupling to (y, x-1)
+  double* cb = reinterpret_cast<double*>(smem + a.off_cb);  // (t, kmax) boundary couplings
+  double* zb = cb + (size_t)t * a.kmax;                     // (t): sum of each column's couplings
+  double* sten = reinterpret_cast<double*>(smem + a.off_sten);
+  double* fvec = reinterpret_cast<double*>(smem + a.off_vec);
+  double* az = fvec + n;
+  double* ctil = az + n;
+  double* dsc = ctil + n;
+  // per-warp column buffers: x (n+1 doubles) and residual / solve vector (n+1 T)
+  const size_t wstride = align16((size_t)np1 * 8) + align16((size_t)np1 * sizeof(T)) + 64 * sizeof(T);
+  double* xw = reinterpret_cast<double*>(smem + a.off_warp + wid * wstride);
+  T* rw = reinterpret_cast<T*>(smem + a.off_warp + wid * wstride + align16((size_t)np1 * 8));
+  T* tb = reinterpret_cast<T*>(smem + a.off_warp + wid * wstride + align16((size_t)np1 * 8) +
+                               align16((size_t)np1 * sizeof(T)));  // 2 x 32 T: broadcast buffers
+  double* kel = reinterpret_cast<double*>(smem + a.off_warp);  // aliases the warp buffers
+  double* fel = kel + 3 * a.rx * a.ry;
+  double* red = reinterpret_cast<double*>(smem + a.off_misc);
+  double* rnorm = red + 32;
+  int* cstat = reinterpret_cast<int*>(rnorm + w);  // per column: 1 converged, 2 non-finite
+  int* citer = cstat + w;
+  int* flag = citer + w;
+
+  double* xg = a.sol + (size_t)cell * w * np1;
+
+  if (tid == 0) flag[0] = 0;
+  double amax, fro, cmax;
+  assemble_cell(a, cell, kel, fel, cb, zb, sten, fvec, ctil, amax, fro, cmax);
   // retained action A 1 (compensated row sums) and finiteness
   double az2 = 0.0;
   int nonzero = 0, nonfinite = 0;
@@ -635,7 +651,7 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
   for (int i = lane; i < n; i += 32) fz += fvec[i];
   fz = warp_sum(fz);
   const int t1 = t + 1;
-  const int ncol = a.mode == 2 ? 1 : w;  // a source response refines the source column only
+  const int ncol = a.mode >= 2 ? 1 : w;  // a source response refines the source column only
   for (int col = wid; col < ncol; col += nwarps) {
     double s2 = 0.0;
     for (int i = lane; i < n; i += 32) {
@@ -846,6 +862,33 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
   }
 }
 
+// Flux -K grad u at the fine-cell centres of one macrocell from its nodal values u
+// (shared memory), postprocessing/solutions.py:278-324.
+__device__ __forceinline__ void cell_flux(const Q1Args& a, int cell, const double* u, double* flux) {
+  const int tid = threadIdx.x;
+  const int cx = cell % a.nx, cy = cell / a.nx;
+  const int ne = a.rx * a.ry;
+  for (int e = tid; e < ne; e += blockDim.x) {
+    const int ex = e % a.rx, ey = e / a.rx;
+    const int n0 = ey * a.nnx + ex;
+    const double u0 = u[n0], u1 = u[n0 + 1], u2 = u[n0 + a.nnx], u3 = u[n0 + a.nnx + 1];
+    const double gx = (-u0 + u1 - u2 + u3) * (0.5 / a.hx);
+    const double gy = (-u0 - u1 + u2 + u3) * (0.5 / a.hy);
+    const size_t g = (size_t)(cx * a.rx + ex) * a.NYf + (cy * a.ry + ey);
+    double kxx, kxy, kyy;
+    if (a.kmode == 0) {
+      kxx = a.k0; kxy = a.k1; kyy = a.k2;
+    } else if (a.kmode == 1) {
+      kxx = kyy = a.kappa[g]; kxy = 0.0;
+    } else {
+      kxx = a.kappa[3 * g]; kxy = a.kappa[3 * g + 1]; kyy = a.kappa[3 * g + 2];
+    }
+    double* out = flux + ((size_t)cell * ne + e) * 2;
+    out[0] = -(kxx * gx + kxy * gy);
+    out[1] = -(kxy * gx + kyy * gy);
+  }
+}
+
 // Reconstruction u = R f - (R B) lambda_K + (1 - R A 1) c_K and flux -K grad u at
 // fine-cell centres (reconstruction.py:130-141, solutions.py:278-324).
 __global__ void __launch_bounds__(kThreads) q1_reconstruct_kernel(
@@ -869,27 +912,145 @@ __global__ void __launch_bounds__(kThreads) q1_reconstruct_kernel(
   }
   __syncthreads();
   if (flux == nullptr) return;
-  const int cx = cell % a.nx, cy = cell / a.nx;
-  const int ne = a.rx * a.ry;
-  for (int e = tid; e < ne; e += blockDim.x) {
-    const int ex = e % a.rx, ey = e / a.rx;
-    const int n0 = ey * a.nnx + ex;
-    const double u0 = u[n0], u1 = u[n0 + 1], u2 = u[n0 + a.nnx], u3 = u[n0 + a.nnx + 1];
-    const double gx = (-u0 + u1 - u2 + u3) * (0.5 / a.hx);
-    const double gy = (-u0 - u1 + u2 + u3) * (0.5 / a.hy);
-    const size_t g = (size_t)(cx * a.rx + ex) * a.NYf + (cy * a.ry + ey);
-    double kxx, kxy, kyy;
-    if (a.kmode == 0) {
-      kxx = a.k0; kxy = a.k1; kyy = a.k2;
-    } else if (a.kmode == 1) {
-      kxx = kyy = a.kappa[g]; kxy = 0.0;
-    } else {
-      kxx = a.kappa[3 * g]; kxy = a.kappa[3 * g + 1]; kyy = a.kappa[3 * g + 2];
+  cell_flux(a, cell, u, flux);
+}
+
+// Flux of given nodal fields (one CTA per macrocell).
+__global__ void __launch_bounds__(kThreads) q1_flux_kernel(const Q1Args a, const double* fields, double* flux) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* u = reinterpret_cast<double*>(smem);
+  const int cell = blockIdx.x;
+  for (int i = threadIdx.x; i < a.n; i += blockDim.x) u[i] = fields[(size_t)cell * a.n + i];
+  __syncthreads();
+  cell_flux(a, cell, u, flux);
+}
+
+// Original (uncondensed) equations of every cell at a hybrid solution
+// (refinement.py:718-738): the local defect d = f - B lambda - A u per node, each
+// row accumulated in double-double arithmetic as the reference's accurate residual
+// does in extended precision (linalg/linear.py:98-126); the cell's weak-trace terms
+// B^T u per trace slot, also accumulated in double-double; and per cell the sums
+// [d.d, f.f, 1.d].
+__global__ void __launch_bounds__(kThreads) q1_defect_kernel(const Q1Args a, const int64_t* cell_dofs,
+                                                             const double* x, const double* fields,
+                                                             double* defect, double* slot_terms,
+                                                             double* partial) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int n = a.n, t = a.t, nnx = a.nnx, ne = a.rx * a.ry, cell = blockIdx.x, tid = threadIdx.x;
+  double* kel = reinterpret_cast<double*>(smem);
+  double* fel = kel + 3 * ne;
+  double* cb = fel + 4 * ne;
+  double* zb = cb + (size_t)t * a.kmax;
+  double* sten = zb + t;
+  double* fvec = sten + 5 * n;
+  double* ctil = fvec + n;
+  double* u = ctil + n;
+  double* lam = u + n;
+  double* red = lam + t;
+  double amax, fro, cmax;
+  assemble_cell(a, cell, kel, fel, cb, zb, sten, fvec, ctil, amax, fro, cmax);
+  for (int i = tid; i < n; i += blockDim.x) u[i] = fields[(size_t)cell * n + i];
+  for (int j = tid; j < t; j += blockDim.x) lam[j] = x[cell_dofs[(size_t)cell * t + j]];
+  __syncthreads();
+  double d2 = 0.0, f2 = 0.0, d1 = 0.0;
+  for (int i = tid; i < n; i += blockDim.x) {
+    const int ix = i % nnx, iy = i / nnx;
+    double hi = fvec[i], lo = 0.0;
+    for (int j = 0; j < t; ++j) {
+      const double bij = rhs_value(a, 1 + j, i, fvec, nullptr, cb);
+      if (bij != 0.0) dd_fma(hi, lo, -bij, lam[j]);
     }
-    double* out = flux + ((size_t)cell * ne + e) * 2;
-    out[0] = -(kxx * gx + kxy * gy);
-    out[1] = -(kxy * gx + kyy * gy);
+    const double* sv = sten + 5 * i;
+    dd_fma(hi, lo, -sv[0], u[i]);
+    if (ix > 0) dd_fma(hi, lo, -sv[1], u[i - 1]);
+    if (iy > 0 && ix < nnx - 1) dd_fma(hi, lo, -sv[2], u[i - nnx + 1]);
+    if (iy > 0) dd_fma(hi, lo, -sv[3], u[i - nnx]);
+    if (iy > 0 && ix > 0) dd_fma(hi, lo, -sv[4], u[i - nnx - 1]);
+    if (ix < nnx - 1) dd_fma(hi, lo, -sten[5 * (i + 1) + 1], u[i + 1]);
+    if (iy < a.nny - 1) {
+      if (ix > 0) dd_fma(hi, lo, -sten[5 * (i + nnx - 1) + 2], u[i + nnx - 1]);
+      dd_fma(hi, lo, -sten[5 * (i + nnx) + 3], u[i + nnx]);
+      if (ix < nnx - 1) dd_fma(hi, lo, -sten[5 * (i + nnx + 1) + 4], u[i + nnx + 1]);
+    }
+    const double d = hi + lo;
+    defect[(size_t)cell * n + i] = d;
+    d2 = fma(d, d, d2);
+    f2 = fma(fvec[i], fvec[i], f2);
+    d1 += d;
   }
+  for (int j = tid; j < t; j += blockDim.x) {
+    const Side sd = trace_side(a, j);
+    const int len = side_len(a, sd.s);
+    double hi = 0.0, lo = 0.0;
+    for (int k = 0; k < len; ++k) dd_fma(hi, lo, cb[j * a.kmax + k], u[side_node(a, sd.s, k)]);
+    slot_terms[(size_t)cell * t + j] = hi + lo;
+  }
+  d2 = block_sum(d2, red);
+  f2 = block_sum(f2, red);
+  d1 = block_sum(d1, red);
+  if (tid == 0) {
+    partial[3 * (size_t)cell] = d2;
+    partial[3 * (size_t)cell + 1] = f2;
+    partial[3 * (size_t)cell + 2] = d1;
+  }
+}
+
+// Weak-trace residual of the original equations (refinement.py:729-731):
+// weak_i = boundary_i - sum over the DOF's cells (first, then second) of B^T u.
+__global__ void weak_residual_kernel(int64_t trace_size, int t, const int32_t* dof_cells,
+                                     const int32_t* dof_slot, const double* slot_terms,
+                                     const double* boundary, double* weak) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < trace_size;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double hi = boundary ? boundary[i] : 0.0, lo = 0.0;
+    for (int k = 0; k < 2; ++k) {
+      const int c = dof_cells[2 * i + k];
+      if (c >= 0) dd_add(hi, lo, -slot_terms[(size_t)c * t + dof_slot[2 * i + k]]);
+    }
+    weak[i] = hi + lo;
+  }
+}
+
+// Norms of a refinement step, each a sum in a fixed order (one block):
+// out[0] = ||[d; weak]||^2 (original residual), out[1] = ||[f; boundary]||^2
+// (its scale), out[2] = ||[weak; 1.d per cell]||^2 (reduced residual),
+// out[3] = ||rhs||^2 and out[4] = || |K| |x| ||^2 of the assembled system.
+__global__ void __launch_bounds__(1024) refine_norms_kernel(int cells, const double* partial, int64_t trace_size,
+                                                            const double* weak, const double* boundary,
+                                                            int64_t size, const int64_t* indptr,
+                                                            const int32_t* indices, const double* values,
+                                                            const double* x, const double* rhs, double* out) {
+  __shared__ double red[32];
+  double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int c = threadIdx.x; c < cells; c += blockDim.x) {
+    v[0] += partial[3 * (size_t)c];
+    v[1] += partial[3 * (size_t)c + 1];
+    v[2] += partial[3 * (size_t)c + 2] * partial[3 * (size_t)c + 2];
+  }
+  for (int64_t i = threadIdx.x; i < trace_size; i += blockDim.x) {
+    const double w2 = weak[i] * weak[i];
+    v[0] += w2;
+    v[2] += w2;
+    const double b = boundary ? boundary[i] : 0.0;
+    v[1] += b * b;
+  }
+  if (indptr) {
+    for (int64_t r = threadIdx.x; r < size; r += blockDim.x) {
+      double acc = 0.0;
+      for (int64_t e = indptr[r]; e < indptr[r + 1]; ++e) acc = fma(fabs(values[e]), fabs(x[indices[e]]), acc);
+      v[4] = fma(acc, acc, v[4]);
+      v[3] = fma(rhs[r], rhs[r], v[3]);
+    }
+  }
+  for (int k = 0; k < 5; ++k) {
+    const double tot = block_sum(v[k], red);
+    if (threadIdx.x == 0) out[k] = tot;
+  }
+}
+
+__global__ void accumulate_kernel(int64_t n, double* dst, const double* src) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] += src[i];
 }
 
 // Gauss-Legendre nodes/weights on [0,1] by Newton iteration on P_m (host).
@@ -925,7 +1086,7 @@ void gauss01(int m, double* x, double* wts) {
 int fill_args(const mhm_q1_problem* p, int precision, Q1Args& a) {
   if (!p || p->macro_nx < 1 || p->macro_ny < 1 || p->rx < 1 || p->ry < 1) return MHM_ERR_ARGUMENT;
   if (!(p->hx > 0) || !(p->hy > 0) || p->tf_h < 1 || p->tf_v < 1) return MHM_ERR_ARGUMENT;
-  if (p->kappa_mode < 0 || p->kappa_mode > 2 || p->source_mode < 0 || p->source_mode > 2)
+  if (p->kappa_mode < 0 || p->kappa_mode > 2 || p->source_mode < 0 || p->source_mode > 3)
     return MHM_ERR_ARGUMENT;
   if ((p->kappa_mode && !p->kappa) || (p->source_mode && !p->source)) return MHM_ERR_ARGUMENT;
   if (p->source_mode == 2 && (p->quad_order < 1 || p->quad_order > kMaxQuad)) return MHM_ERR_ARGUMENT;
@@ -1010,8 +1171,8 @@ int run_condense(const mhm_q1_problem* p, int32_t precision, int32_t max_refine,
   Q1Args a;
   int rc = fill_args(p, precision, a);
   if (rc != MHM_OK) return rc;
-  if (!solution || (!blocks && mode != 2) || !loads || !corrected || !cell_status || !cell_iters ||
-      max_refine < 1 || !(tol > 0) || (mode != 0 && !factors))
+  if (!solution || (!blocks && mode < 2) || !loads || !corrected || !cell_status || !cell_iters ||
+      max_refine < 1 || !(tol > 0) || ((mode == 1 || mode == 2) && !factors))
     return MHM_ERR_ARGUMENT;
   if (a.smem > 227 * 1024) return MHM_ERR_UNSUPPORTED;
   a.max_refine = max_refine; a.tol = tol;
@@ -1075,5 +1236,69 @@ extern "C" int mhm_q1_reconstruct(const mhm_q1_problem* p, const double* solutio
     return MHM_ERR_LAUNCH;
   q1_reconstruct_kernel<<<a.nx * a.ny, kThreads, smem, static_cast<cudaStream_t>(stream)>>>(
       a, cell_dofs, trace_size, x, fields, flux);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+extern "C" int mhm_q1_correction_response(const mhm_q1_problem* p, int32_t precision, int32_t max_refine,
+                                          double tol, const void* factors, double* solution, double* loads,
+                                          uint8_t* corrected, int32_t* cell_status, int32_t* cell_iters,
+                                          void* stream) {
+  return run_condense(p, precision, max_refine, tol, solution, nullptr, loads, corrected, cell_status,
+                      cell_iters, factors ? 2 : 3, const_cast<void*>(factors), stream);
+}
+
+extern "C" int mhm_q1_original_defect(const mhm_q1_problem* p, const int64_t* cell_dofs, int64_t trace_size,
+                                      const int32_t* dof_cells, const int32_t* dof_slot, const double* x,
+                                      const double* fields, const double* boundary, double* defect,
+                                      double* slot_terms, double* weak, double* partial, void* stream) {
+  Q1Args a;
+  int rc = fill_args(p, MHM_PRECISION_FP64, a);
+  if (rc != MHM_OK) return rc;
+  if (!cell_dofs || trace_size < 1 || !dof_cells || !dof_slot || !x || !fields || !defect || !slot_terms ||
+      !weak || !partial)
+    return MHM_ERR_ARGUMENT;
+  const int ne = a.rx * a.ry;
+  const size_t smem = ((size_t)7 * ne + (size_t)a.t * a.kmax + a.t + 8 * (size_t)a.n + a.t + 32) * 8;
+  if (smem > 227 * 1024) return MHM_ERR_UNSUPPORTED;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(q1_defect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess)
+    return MHM_ERR_LAUNCH;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  q1_defect_kernel<<<a.nx * a.ny, kThreads, smem, st>>>(a, cell_dofs, x, fields, defect, slot_terms, partial);
+  int blocks = (int)((trace_size + 255) / 256);
+  if (blocks > 4096) blocks = 4096;
+  weak_residual_kernel<<<blocks, 256, 0, st>>>(trace_size, a.t, dof_cells, dof_slot, slot_terms, boundary, weak);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+extern "C" int mhm_refine_norms(int32_t cells, const double* partial, int64_t trace_size, const double* weak,
+                                const double* boundary, int64_t size, const int64_t* indptr,
+                                const int32_t* indices, const double* values, const double* x,
+                                const double* rhs, double* out, void* stream) {
+  if (cells < 1 || !partial || trace_size < 0 || (trace_size > 0 && !weak) || !out) return MHM_ERR_ARGUMENT;
+  if (indptr && (size < 1 || !indices || !values || !x || !rhs)) return MHM_ERR_ARGUMENT;
+  refine_norms_kernel<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(
+      cells, partial, trace_size, weak, boundary, size, indptr, indices, values, x, rhs, out);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+extern "C" int mhm_vector_accumulate(int64_t n, double* dst, const double* src, void* stream) {
+  if (n < 0 || (n > 0 && (!dst || !src))) return MHM_ERR_ARGUMENT;
+  if (n == 0) return MHM_OK;
+  int blocks = (int)((n + 255) / 256);
+  if (blocks > 4096) blocks = 4096;
+  accumulate_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(n, dst, src);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+extern "C" int mhm_q1_flux(const mhm_q1_problem* p, const double* fields, double* flux, void* stream) {
+  Q1Args a;
+  int rc = fill_args(p, MHM_PRECISION_FP64, a);
+  if (rc != MHM_OK) return rc;
+  if (!fields || !flux) return MHM_ERR_ARGUMENT;
+  const size_t smem = (size_t)a.n * 8;
+  if (smem > 48 * 1024) return MHM_ERR_UNSUPPORTED;
+  q1_flux_kernel<<<a.nx * a.ny, kThreads, smem, static_cast<cudaStream_t>(stream)>>>(a, fields, flux);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }

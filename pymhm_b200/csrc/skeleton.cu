@@ -857,8 +857,13 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
     }
     {
       // the first inner solve to inner_rtol; a later correction only has to win the
-      // factor between the current outer residual and rtol
+      // factor between the current outer residual and rtol.  Either one also stops
+      // once its residual is below half of what rtol asks of the outer residual
+      // (res bnorm): a right-hand side whose projected part is at rounding level, as
+      // for a correction carried by the coarse unknowns alone, then needs no inner
+      // iteration instead of chasing rounding noise into a breakdown
       const double itol = (outer == 0) ? P.inner_rtol : fmin(0.1, fmax(P.rtol / res, 1e-12));
+      const double afloor = 0.5 * P.rtol * res * bnorm;
       const Coarse Cx1{w.Ux1, nullptr, nullptr}, Cx2{w.Ux2, nullptr, nullptr};
       // coarse data of r2
       for (int cx = tid; cx < nx; cx += nth) R.col[cx] = w.rfull[s.T + R.c0 + cx];
@@ -904,8 +909,8 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
         if (!isfinite(rn)) { status = MHM_SOLVE_NONFINITE; break; }
         if (k == 0) {
           r0 = rn;
-          if (r0 == 0.0) break;
-        } else if (rn <= itol * r0) {
+          if (r0 == 0.0 || r0 <= afloor) break;
+        } else if (rn <= itol * r0 || rn <= afloor) {
           break;
         }
         if (k >= P.max_inner) { status = MHM_SOLVE_NOT_CONVERGED; break; }

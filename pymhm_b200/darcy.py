@@ -20,6 +20,7 @@ Per solve, four kernels run back to back on one stream:
 
 from __future__ import annotations
 
+import math
 import numbers
 import time
 from dataclasses import dataclass, field
@@ -210,6 +211,44 @@ class Q1Solution:
     extra: dict = field(default_factory=dict)
 
 
+@dataclass(frozen=True)
+class HybridRefinement:
+    """Corrected solution and original-equation residual history (``HybridRefinement``,
+    ``core/refinement.py:30-47``).
+
+    ``residual_norms`` holds the residual of the uncondensed local equations and the
+    weak trace equations before the first and after every accepted correction;
+    ``rhs_norm`` is the norm of their right-hand side (local loads and boundary
+    data).  ``solution.residual`` is the reduced residual of the corrected fields.
+    """
+
+    solution: Q1Solution
+    residual_norms: tuple
+    rhs_norm: float
+
+
+def _refinement_steps(steps) -> None:
+    """``_refinement_steps`` (``linalg/linear.py:84-87``)."""
+    if isinstance(steps, (bool, np.bool_)) or not isinstance(steps, (int, np.integer)) or steps < 0:
+        raise ValueError("refinement_steps must be a nonnegative integer")
+
+
+def _step_limits(max_steps, min_steps) -> None:
+    """``_step_limits`` (``core/refinement.py:343-348``)."""
+    _refinement_steps(max_steps)
+    _refinement_steps(min_steps)
+    if min_steps > max_steps:
+        raise ValueError("min_steps must not exceed max_steps")
+
+
+def _tolerances(rtol, atol) -> None:
+    """``_tolerances`` (``linalg/linear.py:76-81``)."""
+    if not np.isfinite(rtol) or not np.isfinite(atol) or min(rtol, atol) < 0:
+        raise ValueError("rtol and atol must be finite and nonnegative")
+    if rtol == 0 and atol == 0:
+        raise ValueError("at least one tolerance must be positive")
+
+
 class CartesianQ1Plan:
     """Device-resident plan: topology, tables, pattern and buffers for one problem shape.
 
@@ -346,6 +385,7 @@ class CartesianQ1Plan:
         q.kappa_const[0], q.kappa_const[1], q.kappa_const[2] = kconst
         q.source_mode, q.source, q.source_const = smode, _lib.ptr(source), float(sconst)
         self._keep = (kappa, source)
+        self._factors_current = False  # factors kept by prepare_offline belong to the old permeability
 
     def launch(self, stream=None, *, reconstruct=True, events=None, global_stream=None, local="condense"):
         """Enqueue the four kernels on ``stream`` (no host synchronisation).
@@ -385,9 +425,12 @@ class CartesianQ1Plan:
                                                  P(self.blocks), P(self.loads), P(self.corrected),
                                                  P(self.cell_status), P(self.cell_iters), P(self.factors), s),
                        "mhm_q1_condense_offline")
+            self._factors_current = True
         elif local == "online":
             if getattr(self, "factors", None) is None:
                 raise RuntimeError("prepare_offline() must run before online source responses")
+            if not getattr(self, "_factors_current", False):
+                raise RuntimeError("the permeability changed since prepare_offline(): the kept factors are stale")
             _lib.check(L.mhm_q1_source_response(self.q1, prec, self.max_refine, self.local_tol, P(self.factors),
                                                 P(self.solution), P(self.loads), P(self.corrected),
                                                 P(self.cell_status), P(self.cell_iters), s),
@@ -479,6 +522,89 @@ class CartesianQ1Plan:
         sol.seconds = time.perf_counter() - t0
         return sol
 
+    def refine(self, *, max_steps=2, min_steps=0, rtol=1e-10, atol=0.0, stream=None) -> HybridRefinement:
+        """Defect correction of the original equations (``refine_hybrid``,
+        ``core/refinement.py:612-800``) applied to the plan's last solve.
+
+        Each step evaluates the uncondensed local residuals d = f - B lambda - A u and
+        the weak trace residual boundary - sum B^T u in double-double arithmetic
+        (``mhm_q1_original_defect``).  It accepts when their norm is at most
+        ``max(atol, rtol * rhs_norm)`` (after at least ``min_steps`` corrections).
+        Otherwise it solves every cell once more with its defect as the source: with
+        the factors kept by ``prepare_offline`` when they belong to the current
+        permeability, else with a fresh factorization.  The reduced loads of those
+        responses and the weak residual form the right-hand side of a global solve
+        with the unchanged skeleton matrix.  The correction's trace and coarse values
+        and its reconstructed fields are added to the current ones, so the fields
+        need not be the reconstruction of the kept responses (the reference accepts
+        any ``HybridSolution``); the fluxes are evaluated again from the corrected
+        fields.  The source column of the local responses
+        then holds the last defect's response.  A residual still above the threshold
+        after ``max_steps`` corrections raises ``LinearSolveError``.
+        """
+        _step_limits(max_steps, min_steps)
+        _tolerances(rtol, atol)
+        torch, L, P = self.torch, self.lib, _lib.ptr
+        s = _lib.stream_handle(stream)
+        cur = torch.cuda.current_stream() if stream is None else stream
+        self.check()
+        M, n, t = self.cells, self.n, self.t
+        if getattr(self, "_refine", None) is None:
+            f64 = dict(dtype=torch.float64, device=self.device)
+            self._refine = dict(defect=torch.empty((M, n), **f64), slots=torch.empty((M, t), **f64),
+                                weak=torch.empty(self.T, **f64), partial=torch.empty((M, 3), **f64),
+                                norms=torch.empty(5, **f64), dx=torch.empty(self.N, **f64),
+                                rhs=torch.empty(self.N, **f64), scale=torch.empty(self.N, **f64),
+                                dfields=torch.empty((M, n), **f64))
+        B = self._refine
+        qd = _lib.Q1Problem.from_buffer_copy(self.q1)
+        qd.source_mode, qd.source, qd.source_const = 3, P(B["defect"]), 0.0
+        factors = self.factors if getattr(self, "_factors_current", False) else None
+        pat = self.pattern
+        history, step = [], 0
+        while True:
+            _lib.check(L.mhm_q1_original_defect(self.q1, P(self.d_cell_dofs), self.T, P(self.d_dof_cells),
+                                                P(self.d_dof_slot), P(self.x), P(self.fields), P(self.d_boundary),
+                                                P(B["defect"]), P(B["slots"]), P(B["weak"]), P(B["partial"]), s),
+                       "mhm_q1_original_defect")
+            _lib.check(L.mhm_refine_norms(M, P(B["partial"]), self.T, P(B["weak"]), P(self.d_boundary), self.N,
+                                          P(self.d_indptr), P(self.d_indices), P(self.values), P(self.x),
+                                          P(self.rhs), P(B["norms"]), s), "mhm_refine_norms")
+            cur.synchronize()
+            norms = B["norms"].cpu().numpy()
+            residual, rhs_norm = math.sqrt(norms[0]), math.sqrt(norms[1])
+            history.append(residual)
+            threshold = max(atol, rtol * rhs_norm)
+            if step >= min_steps and math.isfinite(residual) and residual <= threshold:
+                sol = self.result()
+                scale = max(math.sqrt(norms[3]), math.sqrt(norms[4]), np.finfo(float).tiny)
+                sol.residual = math.sqrt(norms[2]) / scale
+                sol.extra["refinement_steps"] = step
+                return HybridRefinement(sol, tuple(history), rhs_norm)
+            if step == max_steps or not math.isfinite(residual):
+                raise LinearSolveError(f"original hybrid residual {residual:.6e} exceeds {threshold:.6e} "
+                                       f"after {step} corrections")
+            _lib.check(L.mhm_q1_correction_response(qd, PRECISIONS[self.precision], self.max_refine,
+                                                    self.local_tol, P(factors), P(self.solution), P(self.loads),
+                                                    P(self.corrected), P(self.cell_status), P(self.cell_iters), s),
+                       "mhm_q1_correction_response")
+            _lib.check(L.mhm_skeleton_scatter(0, P(self.d_slot_ptr), P(self.d_contrib), P(self.blocks),
+                                              P(self.values), self.N, self.T, P(self.d_load_ptr),
+                                              P(self.d_load_contrib), P(self.loads), P(B["weak"]), P(B["rhs"]),
+                                              P(B["scale"]), s), "mhm_skeleton_scatter")
+            _lib.check(L.mhm_skeleton_solve(self.sys, P(B["rhs"]), P(B["scale"]), P(B["dx"]), self.global_rtol,
+                                            self.inner_rtol, self.max_inner, self.max_outer, self.grid,
+                                            P(self.workspace), self.workspace.numel(), P(self.info), P(self.stats),
+                                            s), "mhm_skeleton_solve")
+            _lib.check(L.mhm_q1_reconstruct(self.q1, P(self.solution), P(self.d_cell_dofs), self.T, P(B["dx"]),
+                                            P(B["dfields"]), None, s), "mhm_q1_reconstruct")
+            for dst, src in ((self.x, B["dx"]), (self.fields, B["dfields"])):
+                _lib.check(L.mhm_vector_accumulate(dst.numel(), P(dst), P(src), s), "mhm_vector_accumulate")
+            _lib.check(L.mhm_q1_flux(self.q1, P(self.fields), P(self.flux), s), "mhm_q1_flux")
+            cur.synchronize()
+            self.check()
+            step += 1
+
     def result(self, seconds=0.0) -> Q1Solution:
         info, stats = self.check()
         x = self.x.cpu().numpy()
@@ -508,18 +634,37 @@ class CartesianQ1Plan:
 def solve_darcy_quadrilateral(mesh, *, permeability=1.0, source=0.0, dirichlet=0.0, neumann=None,
                               skeleton=None, local_refinement=4, degree=1, quadrature_order=4,
                               mean_pressure=0.0, solver="gpu", local_solver="gpu", backend="serial",
-                              workers=None, precision="fp64") -> Q1Solution:
+                              workers=None, precision="fp64", hybrid_refinement_steps=0,
+                              hybrid_refinement_min_steps=0) -> Q1Solution:
     """GPU counterpart of ``solve_darcy_quadrilateral`` (``cartesian.py:86-168``).
 
     Weak Dirichlet data on every boundary face; pure-Neumann gauges and Neumann
     faces are rejected with ``NotImplementedError`` (not on this path).  The
     ``solver``, ``local_solver``, ``backend`` and ``workers`` arguments are
     accepted for signature compatibility: the whole solve runs on the GPU.
+    ``hybrid_refinement_steps`` / ``hybrid_refinement_min_steps`` follow the Darcy
+    driver's keywords (``_legacy/models/darcy/primal.py:191-244, 306-316``): a positive
+    count corrects the original equations after condensation (``refine_hybrid``,
+    relative residual 1e-10) and raises ``LinearSolveError`` if that fails.
     """
+    _refinement_steps(hybrid_refinement_steps)
+    _refinement_steps(hybrid_refinement_min_steps)
+    if hybrid_refinement_min_steps > hybrid_refinement_steps:
+        raise ValueError("hybrid_refinement_min_steps must not exceed hybrid_refinement_steps")
     if neumann:
         raise NotImplementedError("Neumann faces are not on the GPU path")
     del mean_pressure, solver, local_solver, backend, workers
     order = max(int(quadrature_order), int(degree) + 1)
     plan = CartesianQ1Plan(mesh, skeleton, local_refinement, dirichlet=dirichlet, quadrature_order=order,
                            degree=degree, precision=precision)
-    return plan.solve(permeability, source)
+    sol = plan.solve(permeability, source)
+    if hybrid_refinement_steps:
+        sol = plan.refine(max_steps=hybrid_refinement_steps, min_steps=hybrid_refinement_min_steps).solution
+    return sol
+
+
+def refine_hybrid(plan, *, max_steps=2, min_steps=0, rtol=1e-10, atol=0.0, stream=None) -> HybridRefinement:
+    """``refine_hybrid`` (``core/refinement.py:612-800``) for a solved ``CartesianQ1Plan``:
+    the plan holds the system, the solution and the boundary load that the reference
+    passes separately.  See ``CartesianQ1Plan.refine``."""
+    return plan.refine(max_steps=max_steps, min_steps=min_steps, rtol=rtol, atol=atol, stream=stream)
