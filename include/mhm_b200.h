@@ -28,6 +28,9 @@
  *   mhm_batched_factor /   replace BatchedFactorization.__init__/solve
  *   mhm_batched_solve      (execution/cuda.py:165-288): equilibrated dense LU
  *                          with FP64 residual refinement.
+ *   mhm_p1_batch_assemble  replaces assemble_p1_batch (execution/cuda.py:27-105):
+ *                          dense P1 stiffness, mass and load of a batch of
+ *                          triangle or tetrahedron meshes.
  *   mhm_q1_condense_offline / mhm_q1_source_response
  *                          replace OfflineLocalProblem's factor-once and
  *                          one-column response (core/offline.py:99-145) for
@@ -327,6 +330,33 @@ int mhm_batched_solve(int64_t count, int32_t n, int32_t nrhs, const double* matr
 
 /* Library version string (host). */
 const char* mhm_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Batched dense P1 simplex assembly (execution/cuda.py:27-105)               */
+/* ------------------------------------------------------------------------ */
+/*
+ * points (batch, npoints, dim), dim 2 or 3; every batch item shares
+ * cells (ncells, dim+1), which the caller has checked (0 <= index < npoints).
+ * diffusion holds dim x dim tensors: item b, cell e uses tensor
+ * b * diffusion_batch_stride + e * diffusion_cell_stride (strides 0 broadcast);
+ * source likewise holds one value per fine cell.  node_ptr (npoints+1) /
+ * node_contrib list, per node, element * (dim+1) + local index in ascending
+ * element order.  scratch: mhm_p1_batch_scratch_bytes.  Outputs: dense
+ * stiffness and consistent mass (batch, npoints, npoints) and load
+ * (batch, npoints); each entry sums its elements in ascending order.
+ * status[0..3] is set to 1 for non-finite points, a degenerate simplex
+ * (|det J| <= eps prod |J columns|), a diffusion tensor that is not finite,
+ * symmetric (1e-12 relative) and positive definite, or a non-finite source.
+ */
+int mhm_p1_batch_assemble(int64_t batch, int32_t npoints, int32_t dim, const double* points,
+                          int32_t ncells, const int32_t* cells, const double* diffusion,
+                          int64_t diffusion_batch_stride, int64_t diffusion_cell_stride,
+                          const double* source, int64_t source_batch_stride,
+                          int64_t source_cell_stride, const int64_t* node_ptr,
+                          const int32_t* node_contrib, double* scratch, double* stiffness,
+                          double* mass, double* load, int32_t* status /* 4 */, void* stream);
+
+int64_t mhm_p1_batch_scratch_bytes(int64_t batch, int32_t dim, int32_t ncells);
 
 #ifdef __cplusplus
 }

@@ -95,6 +95,9 @@ _SIGNATURES = {
     "mhm_batched_factor": (C.c_int, [C.c_int64, C.c_int32, P, P, P, P, P, P, P]),
     "mhm_batched_solve": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, P, P, P, P, P, P, P, C.c_double,
                                     C.c_double, C.c_int32, P, P]),
+    "mhm_p1_batch_assemble": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, C.c_int32, P, P, C.c_int64,
+                                        C.c_int64, P, C.c_int64, C.c_int64, P, P, P, P, P, P, P, P]),
+    "mhm_p1_batch_scratch_bytes": (C.c_int64, [C.c_int64, C.c_int32, C.c_int32]),
     "mhm_version": (C.c_char_p, []),
 }
 

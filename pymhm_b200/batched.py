@@ -9,8 +9,11 @@
   decodes responses with the problem's own ``response_from_solution``.
 * ``GpuLocalSolver`` implements ``LocalLinearSolver`` (``core/assembly.py:32-47``)
   for ``SolverConfig(local_solver=GpuLocalSolver())``.
+* ``assemble_p1_batch`` mirrors ``cuda.py:27-105``: dense P1 stiffness, mass and
+  load of a batch of triangle or tetrahedron meshes sharing one connectivity.
 
-Compute is ``mhm_batched_factor`` / ``mhm_batched_solve`` from libmhm_b200.so.
+Compute is ``mhm_batched_factor`` / ``mhm_batched_solve`` / ``mhm_p1_batch_assemble``
+from libmhm_b200.so.
 """
 
 from __future__ import annotations
@@ -168,3 +171,105 @@ class GpuLocalSolver:
 
     def close(self) -> None:
         pass
+
+
+_INCIDENCE: dict = {}
+
+
+def _node_incidence(cells: np.ndarray, npoints: int):
+    """Per node, element * (d+1) + local index of every incidence in ascending element
+    order (CSR), cached per connectivity."""
+    key = (cells.shape, npoints, cells.tobytes())
+    hit = _INCIDENCE.get(key)
+    if hit is None:
+        nv = cells.shape[1]
+        flat = cells.ravel().astype(np.int64)
+        codes = np.arange(flat.size, dtype=np.int64)  # element * nv + local, ascending
+        order = np.argsort(flat, kind="stable")
+        ptr = np.zeros(npoints + 1, dtype=np.int64)
+        np.add.at(ptr, flat + 1, 1)
+        hit = (np.cumsum(ptr), codes[order].astype(np.int32))
+        if len(_INCIDENCE) > 16:
+            _INCIDENCE.clear()
+        _INCIDENCE[key] = hit
+    return hit
+
+
+def _broadcast_strides(value, torch, lead, item_shape, dev):
+    """``value`` broadcast to ``lead + item_shape``, lead = (batch, cells), as a
+    contiguous FP64 base holding only the non-broadcast items, with the strides (in
+    items) over batch and cells that address it (0 where broadcast)."""
+    t = torch.as_tensor(value, device=dev)
+    if t.is_complex():
+        raise TypeError("complex coefficient")
+    view = torch.broadcast_to(t, (*lead, *item_shape))
+    nb = lead[0] if view.stride(0) != 0 else 1
+    nc = lead[1] if view.stride(1) != 0 else 1
+    base = view[:nb, :nc].to(torch.float64).contiguous()
+    return base, (nc if nb > 1 else 0), (1 if nc > 1 else 0)
+
+
+def assemble_p1_batch(points, cells, *, diffusion=1.0, source=0.0):
+    """Dense P1 simplex operators of a batch of local meshes on the current CUDA device
+    (``assemble_p1_batch``, ``execution/cuda.py:27-105``).
+
+    ``points`` has shape ``(batch, npoints, d)``, d = 2 or 3; every mesh shares the
+    integer connectivity ``cells[ncells, d+1]``.  ``diffusion`` is a positive scalar
+    or SPD tensors broadcastable to ``(batch, ncells, d, d)``; ``source`` is constant
+    per fine cell, broadcastable to ``(batch, ncells)``.  Returns the dense stiffness,
+    consistent mass ``(batch, npoints, npoints)`` and load ``(batch, npoints)`` as
+    CUDA tensors (the reference returns CuPy arrays).  Each entry sums its elements in
+    ascending element order, so repeated calls give identical bits.  The same
+    ``ValueError`` messages as the reference reject malformed geometry and
+    coefficients.
+    """
+    torch = _torch()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    pts = torch.as_tensor(points, device=dev) if not isinstance(points, torch.Tensor) else points.to(dev)
+    if (pts.dim() != 3 or pts.shape[-1] not in (2, 3) or not pts.shape[0] or not pts.shape[1]
+            or pts.is_complex() or not (pts.dtype.is_floating_point or pts.dtype in (torch.int32, torch.int64))):
+        raise ValueError("points must be finite real arrays shaped (batch,npoints,2 or 3)")
+    count, size, dim = (int(v) for v in pts.shape)
+    conn = cells.cpu().numpy() if isinstance(cells, torch.Tensor) else np.asarray(cells)
+    if (conn.ndim != 2 or conn.shape[1] != dim + 1 or not len(conn) or conn.dtype.kind not in "iu"
+            or np.any(conn < 0) or np.any(conn >= size)):
+        raise ValueError("cells must contain valid simplex node indices")
+    conn = np.ascontiguousarray(conn, dtype=np.int32)
+    ncells = len(conn)
+    pts = pts.to(torch.float64).contiguous()
+    try:
+        raw = torch.as_tensor(diffusion, device=dev)
+        if raw.dim() == 0:
+            raw = raw.to(torch.float64) * torch.eye(dim, dtype=torch.float64, device=dev)
+        kbase, kb, kc = _broadcast_strides(raw, torch, (count, ncells), (dim, dim), dev)
+    except (RuntimeError, TypeError, ValueError):
+        raise ValueError("diffusion must be finite real symmetric positive definite") from None
+    try:
+        sbase, sb, sc = _broadcast_strides(source, torch, (count, ncells), (), dev)
+    except (RuntimeError, TypeError, ValueError):
+        raise ValueError("source must be real finite cell values") from None
+    ptr, contrib = _node_incidence(conn, size)
+    lib = _lib.lib()
+    d_cells = torch.from_numpy(conn).to(dev)
+    d_ptr = torch.from_numpy(ptr).to(dev)
+    d_contrib = torch.from_numpy(contrib).to(dev)
+    nbytes = int(lib.mhm_p1_batch_scratch_bytes(count, dim, ncells))
+    scratch = torch.empty(nbytes // 8, dtype=torch.float64, device=dev)
+    stiffness = torch.empty((count, size, size), dtype=torch.float64, device=dev)
+    mass = torch.empty_like(stiffness)
+    load = torch.empty((count, size), dtype=torch.float64, device=dev)
+    status = torch.empty(4, dtype=torch.int32, device=dev)
+    P = _lib.ptr
+    _lib.check(lib.mhm_p1_batch_assemble(count, size, dim, P(pts), ncells, P(d_cells), P(kbase), kb, kc, P(sbase),
+                                         sb, sc, P(d_ptr), P(d_contrib), P(scratch), P(stiffness), P(mass), P(load),
+                                         P(status), _lib.stream_handle(None)), "mhm_p1_batch_assemble")
+    flags = status.cpu().numpy()
+    if flags[0]:
+        raise ValueError("points must be finite real arrays shaped (batch,npoints,2 or 3)")
+    if flags[1]:
+        raise ValueError("degenerate simplex in resident geometry")
+    if flags[2]:
+        raise ValueError("diffusion must be finite real symmetric positive definite")
+    if flags[3]:
+        raise ValueError("source must be real finite cell values")
+    return stiffness, mass, load

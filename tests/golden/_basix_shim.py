@@ -14,7 +14,10 @@ calls two of its functions:
   (``src/pymhm/fem/reference.py:596-625``) from ``FaceSpace.evaluate``
   (``src/pymhm/fem/traces/interval.py:54-89``).
 
-Both are restated here from their published mathematics: the nodal Lagrange
+The P1 operator fixtures (``make_p1_golden.py``) also need the degree-one
+Lagrange basis on triangles and tetrahedra (barycentric coordinates).
+
+All are restated here from their published mathematics: the nodal Lagrange
 basis on the declared node order (unique polynomial interpolant, obtained by a
 Legendre-Vandermonde solve) with exact Kronecker rows at literal nodes, as the
 reference wrapper enforces (``reference.py:484-488``); and the conventional
@@ -45,11 +48,30 @@ def _interval_lagrange(degree, points, nodes, nderiv):
     return vals, ders
 
 
+def _simplex_p1(bary, nodes, nderiv):
+    """Degree-one Lagrange basis on a triangle or tetrahedron for the declared node
+    order: phi_j = sum_m bary_m C[m, j] with C the inverse of the nodes' barycentric
+    matrix (phi_j(node_k) = delta_jk); gradients in the reference coordinates
+    x = bary[:, 1:] are C[a + 1, j] - C[0, j]; Hessians vanish."""
+    dim = nodes.shape[1] - 1
+    coef = np.linalg.inv(nodes)
+    vals = bary @ coef
+    rows, cols = np.nonzero(np.all(bary[:, None, :] == nodes[None, :, :], axis=2))
+    vals[rows] = 0.0
+    vals[rows, cols] = 1.0
+    grad = np.broadcast_to((coef[1:] - coef[0]).T, (len(bary), nodes.shape[0], dim)).copy()
+    gradient = grad if nderiv else np.empty((*vals.shape, 0))
+    hessian = np.zeros((*vals.shape, dim, dim)) if nderiv == 2 else np.empty((*vals.shape, 0, 0))
+    return vals, gradient, hessian
+
+
 def simplex_lagrange_tabulation(cell, degree, bary, *, nodes, nderiv=2):
-    if cell != "interval":
-        raise NotImplementedError("the fixture shim covers interval tabulation only")
     bary = np.asarray(bary, dtype=float)
     nodes = np.asarray(nodes, dtype=float)
+    if cell in ("triangle", "tetrahedron") and int(degree) == 1:
+        return _simplex_p1(bary, nodes, nderiv)
+    if cell != "interval":
+        raise NotImplementedError("the fixture shim covers intervals and degree-one simplices only")
     vals, ders = _interval_lagrange(int(degree), bary[:, 1], nodes[:, 1], nderiv)
     gradient = ders[:, :, None] if nderiv else np.empty((*vals.shape, 0))
     hessian = np.empty((*vals.shape, 0, 0))

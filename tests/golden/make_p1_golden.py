@@ -1,0 +1,50 @@
+"""Write golden fixtures for dense P1 simplex assembly by running PyMHM's own CPU
+operators, the ones the reference's GPU test compares ``assemble_p1_batch`` with
+(``tests/test_gpu_batch.py``): ``p1_operators`` on ``TriangleMesh.unit_square(3)``
+and ``tetra_operators`` (degree 1) on ``TetraMesh.unit_cube(1).submesh(0, 2)``.
+
+    PYMHM_SRC=/path/to/pymhm/src python tests/golden/make_p1_golden.py
+
+Basix is replaced by ``_basix_shim`` (degree-one simplex basis).
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, os.environ.get("PYMHM_SRC", "/root/reference/src"))
+sys.path.insert(0, str(HERE))
+
+import _basix_shim  # noqa: E402
+
+_basix_shim.install()
+
+from pymhm.fem.scalar.operators import p1_operators  # noqa: E402
+from pymhm.fem.scalar.tetrahedron import tetra_operators  # noqa: E402
+from pymhm.meshes.tetrahedron import TetraMesh  # noqa: E402
+from pymhm.meshes.triangle import TriangleMesh  # noqa: E402
+
+
+def main():
+    out = {}
+    mesh = TriangleMesh.unit_square(3)
+    tensor = np.array([[2.0, 0.2], [0.2, 1.0]])
+    a, m, f = p1_operators(mesh, diffusion=tensor, source=3.0)
+    out.update(tri_points=mesh.points, tri_cells=mesh.cells, tri_tensor=tensor, tri_source=3.0,
+               tri_A=a.toarray(), tri_M=m.toarray(), tri_f=f)
+    tetra = TetraMesh.unit_cube(1).submesh(0, 2)
+    tensor = np.array([[2.0, 0.2, 0.0], [0.2, 1.0, 0.1], [0.0, 0.1, 3.0]])
+    a, m, f = tetra_operators(tetra, degree=1, diffusion=tensor, source=2.5)
+    out.update(tet_points=tetra.points, tet_cells=tetra.cells, tet_tensor=tensor, tet_source=2.5,
+               tet_A=a.toarray(), tet_M=m.toarray(), tet_f=f)
+    np.savez_compressed(HERE / "p1_operators.npz", **out)
+    print("tri", mesh.points.shape, mesh.cells.shape, "tet", tetra.points.shape, tetra.cells.shape)
+
+
+if __name__ == "__main__":
+    main()
