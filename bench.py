@@ -58,6 +58,84 @@ CPU_SAMPLE_CELLS = 4096
 NCU_DRAM_BYTES = {"skeleton_pcg": 15.3e6, "q1_condense": 92.3e6}
 
 
+def triangle_submesh(r):
+    """Uniform refinement of the unit right triangle into r^2 triangles:
+    (r+1)(r+2)/2 P1 nodes (91 for r = 12, 325 for r = 24)."""
+    nodes = [(i, j) for j in range(r + 1) for i in range(r + 1 - j)]
+    index = {p: k for k, p in enumerate(nodes)}
+    cells = []
+    for j in range(r):
+        for i in range(r - j):
+            cells.append([index[(i, j)], index[(i + 1, j)], index[(i, j + 1)]])
+            if i + j < r - 1:
+                cells.append([index[(i + 1, j)], index[(i + 1, j + 1)], index[(i, j + 1)]])
+    return np.array(nodes, dtype=float) / r, np.array(cells, dtype=np.int64)
+
+
+def batched_local_campaign(torch, refinement, batch=64, queries=12, repeats=3):
+    """The reference's resident batched local-stage benchmark (``gpu_campaign``,
+    benchmarks/execution_modes.py:203-290) with this library's kernels: P1 volume
+    assembly of ``batch`` copies of a triangle refined ``refinement`` times, the
+    mean-constrained dense systems, batched LU, a first solve of the source and three
+    trace columns, ``queries`` repeated right-hand sides, download.  Wall clock per
+    phase with a device synchronisation at each boundary, one untimed repetition
+    first; median over ``repeats``."""
+    from pymhm_b200.batched import BatchedFactorization, assemble_p1_batch
+
+    pts, cells = triangle_submesh(refinement)
+    n = len(pts)
+    coords = np.repeat(pts[None], batch, axis=0)
+    dev = torch.device("cuda")
+    diffusion = torch.diag(torch.tensor([3.0, 1.0], dtype=torch.float64, device=dev))
+    records, error = [], 0.0
+    for rep in range(repeats + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        p_dev, c_dev = torch.from_numpy(coords).to(dev), torch.from_numpy(cells).to(dev)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        stiffness, mass, forcing = assemble_p1_batch(p_dev, c_dev, diffusion=diffusion, source=1.0)
+        constrained = torch.zeros((batch, n + 1, n + 1), dtype=torch.float64, device=dev)
+        constrained[:, :n, :n] = stiffness
+        c = mass.sum(dim=2)  # constraint M 1, scaled as the condensation contract scales it
+        scale = torch.clamp(stiffness.abs().amax(dim=(1, 2)) / c.abs().amax(dim=1), max=1.0)
+        means = c * scale[:, None]
+        constrained[:, :n, n] = means
+        constrained[:, n, :n] = means
+        loads = torch.zeros((batch, n + 1, 4), dtype=torch.float64, device=dev)
+        loads[:, :n, 0] = forcing
+        loads[:, 0, 1] = loads[:, 1, 2] = loads[:, 2, 3] = 1.0  # coupling = the first three unit columns
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        with BatchedFactorization(constrained) as fact:
+            torch.cuda.synchronize()
+            t3 = time.perf_counter()
+            first = fact.solve(loads)
+            torch.cuda.synchronize()
+            t4 = time.perf_counter()
+            for factor in np.linspace(0.5, 1.5, queries):
+                repeated = fact.solve(loads * float(factor))
+            torch.cuda.synchronize()
+            t5 = time.perf_counter()
+            host_first = first[:, :n].cpu().numpy()
+            host_last = repeated[:, :n].cpu().numpy()
+            torch.cuda.synchronize()
+            t6 = time.perf_counter()
+        if rep == 0:
+            a0 = constrained[0].cpu().numpy()
+            want = np.linalg.solve(a0, loads[0].cpu().numpy())[:n]
+            error = max(float(np.max(np.abs(host_first[0] - want))),
+                        float(np.max(np.abs(host_last[-1] - 1.5 * want))))
+        else:
+            records.append([t1 - t0, t2 - t1, t3 - t2, t4 - t3, t5 - t4, t6 - t5, t6 - t0])
+    med = np.median(np.array(records), axis=0) * 1e3
+    keys = ["upload", "assembly_and_constrained_systems", "factorization", "first_solve", "repeated_rhs_total",
+            "download", "total"]
+    out = {k: float(v) for k, v in zip(keys, med)}
+    out.update(batch=batch, local_unknowns=n, queries=queries, max_solution_error_vs_numpy=error)
+    return out
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -343,6 +421,16 @@ def main():
                   "note": "refine_hybrid on the mixed solve: original-equation residual, defect source responses "
                           "with a fresh factorization, correction solve, reconstruction; forced one step"}
 
+    # the reference's own batched local-stage benchmark, same phases and sizes
+    campaigns = {f"batched_local_r{r}": batched_local_campaign(torch, r) for r in (12, 24)}
+    campaigns["reference_rtx3060_ms"] = {
+        "batched_local_r12": {"factorization": 3.19, "first_solve": 1.31, "repeated_rhs_total": 16.0, "total": 26.6},
+        "batched_local_r24": {"factorization": 28.0, "first_solve": 5.15, "repeated_rhs_total": 61.6,
+                              "total": 105.6}}
+    campaigns["note"] = ("gpu_campaign of benchmarks/execution_modes.py (64 P1 triangle meshes, 12 queries) with "
+                         "assemble_p1_batch and BatchedFactorization of this library; reference figures: RTX 3060 "
+                         "(benchmarks/results/execution/gpu-r12.json, gpu-r24.json)")
+
     # end to end through the public API, same serving loop: H2D kappa, solve, D2H
     # fields / flux / x / status / info for every request
     pl = plans["mixed"]
@@ -454,6 +542,7 @@ def main():
                               "note": "OfflineQ1System: kept local factors, one query = source responses + "
                                       "right-hand-side reduction + global solve + reconstruction, one at a time"},
         "refinement": refinement,
+        "reference_campaigns": campaigns,
         "global_iterations": int(mixed["info"][1]), "outer_corrections": int(mixed["info"][2]),
         "residual": float(mixed["stats"][0]), "certificate": float(mixed["stats"][1]),
         "error_vs_reference": acc,
