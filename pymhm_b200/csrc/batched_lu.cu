@@ -7,8 +7,13 @@
 //   * rank test min |u_ii| <= eps * n * max |LU| -> "rank deficient" (:132-135)
 //   * solve with the equilibrated factors, FP64 residual on the original matrix,
 //     at most two corrections, columnwise acceptance (:230-255)
-// One CTA owns one matrix; the working matrix lives in shared memory when it
-// fits and in the caller's `factors` array (L2-resident) otherwise.
+// One CTA owns one matrix.  The working matrix lives in shared memory when it fits
+// (n <= 160, unblocked right-looking LU).  Up to n = 640 it lives in the caller's
+// `factors` array (L2-resident) and is factored in blocks of 32 columns: the panel
+// in shared memory with partial pivoting, the trailing matrix updated in 64 x 64
+// tiles.  Larger n use the unblocked algorithm on `factors`.  Solves keep the
+// right-hand sides in shared memory and read the factors in 32-row chunks (one
+// batch of loads per chunk) when they fit, else one warp per column.
 #include <cmath>
 
 #include "mhm_common.cuh"
@@ -224,6 +229,496 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_kernel(
   if (tid == 0) status[m] = MHM_CELL_RESIDUAL;
 }
 
+
+constexpr int kPanel = 32;
+constexpr int kPanelStride = kPanel + 1;  // odd: a column of the panel spans all banks
+constexpr int kTile = 64;
+constexpr int kTileStride = kTile + 1;
+constexpr int kBlockedMaxN = 640;
+
+// Row then column max-equilibration of A into F (cuda.py:201-211); the status of
+// zero rows / columns and non-finite entries.
+__device__ int equilibrate(int n, const double* A, double* F, double* rsc, double* csc) {
+  int st = MHM_CELL_OK;
+  const int tid = threadIdx.x;
+  const size_t nn = (size_t)n * n;
+  int zero_row = 0, nonfinite = 0;
+  for (int i = tid; i < n; i += blockDim.x) {
+    double mx = 0.0;
+#pragma unroll 8
+    for (int j = 0; j < n; ++j) {
+      const double v = A[(size_t)i * n + j];
+      if (!isfinite(v)) nonfinite = 1;
+      mx = fmax(mx, fabs(v));
+    }
+    if (mx == 0.0) zero_row = 1;
+    rsc[i] = (mx > 0.0) ? 1.0 / mx : 0.0;
+  }
+  nonfinite = __syncthreads_or(nonfinite);
+  zero_row = __syncthreads_or(zero_row);
+  if (nonfinite) st = MHM_CELL_NONFINITE;
+  else if (zero_row) st = MHM_CELL_ZERO_ROW;
+  int zero_col = 0;
+  for (int j = tid; j < n; j += blockDim.x) {
+    double mx = 0.0;
+#pragma unroll 8
+    for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(A[(size_t)i * n + j] * rsc[i]));
+    if (mx == 0.0) zero_col = 1;
+    csc[j] = (mx > 0.0) ? 1.0 / mx : 0.0;
+  }
+  zero_col = __syncthreads_or(zero_col);
+  if (st == MHM_CELL_OK && zero_col) st = MHM_CELL_ZERO_COLUMN;
+  for (size_t idx = tid; idx < nn; idx += blockDim.x) {
+    const int i = (int)(idx / n), j = (int)(idx % n);
+    F[idx] = A[idx] * rsc[i] * csc[j];
+  }
+  __syncthreads();
+  return st;
+}
+
+// Blocked right-looking LU with partial pivoting of one matrix held in `factors`
+// (32 < n <= 640).  Per panel of 32 columns: (a) the panel rows kb..n-1 are factored
+// in shared memory, pivots by first maximum as the unblocked kernel; (b) the panel's
+// row swaps are applied to the other columns, a thread per column, in order;
+// (c) U12 = L11^-1 A12, a thread per column; (d) A22 -= L21 U12 in 64 x 64 tiles,
+// 4 x 4 outputs per thread.
+__global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
+    int n, const double* __restrict__ mats, double* __restrict__ factors, int32_t* __restrict__ piv,
+    double* __restrict__ rs, double* __restrict__ cs, int32_t* __restrict__ status) {
+  extern __shared__ __align__(16) double sm[];
+  double* Pn = sm;                                   // (n, kPanelStride) panel
+  double* Ut = Pn + (size_t)n * kPanelStride;        // (kPanel, kTileStride) U12 tile
+  __shared__ double red[32];
+  __shared__ double wbest[32];
+  __shared__ int wrow[32];
+  __shared__ int sperm[kPanel];
+  __shared__ int apos[2 * kPanel], asrc[2 * kPanel];  // rows the panel's swaps move: position <- source
+  __shared__ int naff;
+  const int m = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  const size_t nn = (size_t)n * n;
+  double* F = factors + nn * m;
+  int st = equilibrate(n, mats + nn * m, F, rs + (size_t)n * m, cs + (size_t)n * m);
+  for (int kb = 0; kb < n && st == MHM_CELL_OK; kb += kPanel) {
+    const int w = min(kPanel, n - kb), rows = n - kb;
+    for (int idx = tid; idx < rows * w; idx += blockDim.x) {
+      const int r = idx / w, c = idx - r * w;
+      Pn[r * kPanelStride + c] = F[(size_t)(kb + r) * n + kb + c];
+    }
+    __syncthreads();
+    for (int c = 0; c < w; ++c) {
+      double best = -1.0;
+      int bi = c;
+      for (int r = c + tid; r < rows; r += blockDim.x) {
+        const double v = fabs(Pn[r * kPanelStride + c]);
+        if (v > best) { best = v; bi = r; }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (lane == 0) { wbest[wid] = best; wrow[wid] = bi; }
+      __syncthreads();
+      if (tid == 0) {
+        double b = wbest[0];
+        int r = wrow[0];
+        for (int q = 1; q < nw; ++q)
+          if (wbest[q] > b || (wbest[q] == b && wrow[q] < r)) { b = wbest[q]; r = wrow[q]; }
+        sperm[c] = r;
+      }
+      __syncthreads();
+      const int p = sperm[c];
+      if (p != c)
+        for (int j = tid; j < w; j += blockDim.x) {
+          const double t = Pn[c * kPanelStride + j];
+          Pn[c * kPanelStride + j] = Pn[p * kPanelStride + j];
+          Pn[p * kPanelStride + j] = t;
+        }
+      __syncthreads();
+      const double d = Pn[c * kPanelStride + c];
+      if (d == 0.0) { st = MHM_CELL_SINGULAR_PIVOT; break; }
+      const double inv = 1.0 / d;
+      {
+        // warps stride the rows below the pivot; each lane forms the row's multiplier,
+        // lane 31 stores it, lane k updates panel column c + 1 + k
+        const int j = c + 1 + lane;
+        const double u = j < w ? Pn[c * kPanelStride + j] : 0.0;
+        for (int r = c + 1 + wid; r < rows; r += nw) {
+          const double l = Pn[r * kPanelStride + c] * inv;
+          __syncwarp();
+          if (j < w) Pn[r * kPanelStride + j] = fma(-l, u, Pn[r * kPanelStride + j]);
+          if (lane == 31) Pn[r * kPanelStride + c] = l;
+        }
+      }
+      __syncthreads();
+    }
+    if (st != MHM_CELL_OK) break;
+    for (int idx = tid; idx < rows * w; idx += blockDim.x) {
+      const int r = idx / w, c = idx - r * w;
+      F[(size_t)(kb + r) * n + kb + c] = Pn[r * kPanelStride + c];
+    }
+    for (int c = tid; c < w; c += blockDim.x) piv[(size_t)m * n + kb + c] = kb + sperm[c];
+    if (tid == 0) {
+      // compose the panel's swaps on the rows they touch: position apos[k] receives
+      // the row that started at asrc[k] (panel-relative)
+      int cnt = 0;
+      for (int c = 0; c < w; ++c) {
+        const int p = sperm[c];
+        for (const int r : {c, p}) {
+          bool seen = false;
+          for (int k = 0; k < cnt; ++k) seen |= apos[k] == r;
+          if (!seen) { apos[cnt] = r; asrc[cnt] = r; ++cnt; }
+        }
+      }
+      for (int c = 0; c < w; ++c) {
+        const int p = sperm[c];
+        if (p == c) continue;
+        int kc = 0, kp = 0;
+        for (int k = 0; k < cnt; ++k) {
+          if (apos[k] == c) kc = k;
+          if (apos[k] == p) kp = k;
+        }
+        const int t = asrc[kc];
+        asrc[kc] = asrc[kp];
+        asrc[kp] = t;
+      }
+      naff = cnt;
+    }
+    __syncthreads();
+    // the other columns: every moved entry of a column is loaded before any is stored
+    for (int j = tid; j < n - w; j += blockDim.x) {
+      const int col = j < kb ? j : j + w;
+      double v[2 * kPanel];
+#pragma unroll
+      for (int k = 0; k < 2 * kPanel; ++k) v[k] = k < naff ? F[(size_t)(kb + asrc[k]) * n + col] : 0.0;
+#pragma unroll
+      for (int k = 0; k < 2 * kPanel; ++k)
+        if (k < naff) F[(size_t)(kb + apos[k]) * n + col] = v[k];
+    }
+    __syncthreads();
+    for (int j = kb + w + tid; j < n; j += blockDim.x) {
+      double x[kPanel];
+#pragma unroll
+      for (int r = 0; r < kPanel; ++r) x[r] = r < w ? F[(size_t)(kb + r) * n + j] : 0.0;
+#pragma unroll
+      for (int r = 1; r < kPanel; ++r)
+#pragma unroll
+        for (int q = 0; q < r; ++q) x[r] = fma(-Pn[r * kPanelStride + q], x[q], x[r]);
+#pragma unroll
+      for (int r = 0; r < kPanel; ++r)
+        if (r < w) F[(size_t)(kb + r) * n + j] = x[r];
+    }
+    __syncthreads();
+    const int m2 = n - kb - w, base = kb + w;
+    const int ty = tid >> 4, tx = tid & 15;
+    for (int ti = 0; ti < m2; ti += kTile)
+      for (int tj = 0; tj < m2; tj += kTile) {
+        double acc[4][4];  // the tile's current entries, loaded before the U12 tile is staged
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const int i = ti + ty * 4 + a, j = tj + tx + 16 * b;
+            acc[a][b] = (i < m2 && j < m2) ? F[(size_t)(base + i) * n + base + j] : 0.0;
+          }
+        for (int idx = tid; idx < w * kTile; idx += blockDim.x) {
+          const int r = idx / kTile, c = idx - r * kTile;
+          Ut[r * kTileStride + c] = (tj + c < m2) ? F[(size_t)(kb + r) * n + base + tj + c] : 0.0;
+        }
+        __syncthreads();
+        int prow[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          const int r = w + ti + ty * 4 + a;  // panel row of L21
+          prow[a] = r < rows ? r : rows - 1;
+        }
+        for (int q = 0; q < w; ++q) {
+          double l[4], u[4];
+#pragma unroll
+          for (int a = 0; a < 4; ++a) l[a] = Pn[prow[a] * kPanelStride + q];
+#pragma unroll
+          for (int b = 0; b < 4; ++b) u[b] = Ut[q * kTileStride + tx + 16 * b];
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] = fma(-l[a], u[b], acc[a][b]);
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+          const int i = ti + ty * 4 + a;
+          if (i >= m2) continue;
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const int j = tj + tx + 16 * b;
+            if (j < m2) F[(size_t)(base + i) * n + base + j] = acc[a][b];
+          }
+        }
+        __syncthreads();
+      }
+  }
+  if (st == MHM_CELL_OK) {
+    double dmin = 1e300, amax = 0.0;
+    for (int i = tid; i < n; i += blockDim.x) dmin = fmin(dmin, fabs(F[(size_t)i * n + i]));
+#pragma unroll 8
+    for (size_t idx = tid; idx < nn; idx += blockDim.x) amax = fmax(amax, fabs(F[idx]));
+    dmin = block_min(dmin, red);
+    amax = block_max(amax, red);
+    if (dmin <= 2.220446049250313e-16 * n * amax) st = MHM_CELL_RANK_DEFICIENT;
+  }
+  if (tid == 0) status[m] = st;
+}
+
+// W <- U^-1 L^-1 W for the shared-memory block W (n, nrhs), in place, by chunks of
+// 32 rows (right-looking): the chunk's diagonal block (in Dg) is solved with one
+// warp per column, a lane per row; then every row beyond the chunk subtracts its
+// 32 factor entries times the chunk's solution, a thread per row with the 32
+// loads issued together.  The threads whose rows form the next chunk also load
+// that chunk's diagonal block (into the other half of Dg) in the same pass.
+__device__ void chunked_lu_solve(int n, int nrhs, const double* LU, double* W, double* Dg) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  const int nchunk = (n + 31) / 32;
+  for (int dir = 0; dir < 2; ++dir) {
+    const bool lower = dir == 0;
+    int cur = 0;
+    {  // the first diagonal block
+      const int i0 = lower ? 0 : (nchunk - 1) * 32, h = min(32, n - i0);
+      for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
+        const int r = idx >> 5, c = idx & 31;
+        Dg[r * 33 + c] = (r < h && c < h) ? LU[(size_t)(i0 + r) * n + i0 + c] : 0.0;
+      }
+      __syncthreads();
+    }
+    for (int q = 0; q < nchunk; ++q) {
+      const int i0 = lower ? q * 32 : (nchunk - 1 - q) * 32;
+      const int h = min(32, n - i0);
+      const double* D = Dg + cur * 32 * 33;
+      double* Dn = Dg + (1 - cur) * 32 * 33;
+      for (int c = wid; c < nrhs; c += nw) {
+        double v = lane < h ? W[(size_t)(i0 + lane) * nrhs + c] : 0.0;
+        if (lower) {
+          for (int sidx = 0; sidx < h; ++sidx) {
+            const double xs = __shfl_sync(0xffffffffu, v, sidx);
+            if (lane > sidx && lane < h) v = fma(-D[lane * 33 + sidx], xs, v);
+          }
+        } else {
+          for (int sidx = h - 1; sidx >= 0; --sidx) {
+            if (lane == sidx) v = v / D[sidx * 33 + sidx];
+            const double xs = __shfl_sync(0xffffffffu, v, sidx);
+            if (lane < sidx) v = fma(-D[lane * 33 + sidx], xs, v);
+          }
+        }
+        if (lane < h) W[(size_t)(i0 + lane) * nrhs + c] = v;
+      }
+      __syncthreads();
+      // rows beyond the chunk (below for L, above for U); the next chunk's rows also
+      // stage its diagonal block
+      const int r0 = lower ? i0 + h : 0, r1 = lower ? n : i0;
+      const int n0 = lower ? i0 + h : i0 - 32;  // first row of the next chunk
+      const int hn = lower ? min(32, n - n0) : 32;
+      for (int i = r0 + tid; i < r1; i += blockDim.x) {
+        const double* row = LU + (size_t)i * n;
+        double l[32];
+#pragma unroll
+        for (int sidx = 0; sidx < 32; ++sidx) l[sidx] = sidx < h ? row[i0 + sidx] : 0.0;
+        const int rn = i - n0;
+        double dn[32];
+        const bool stage = q + 1 < nchunk && rn >= 0 && rn < hn;
+        if (stage) {
+#pragma unroll
+          for (int sidx = 0; sidx < 32; ++sidx) dn[sidx] = sidx < hn ? row[n0 + sidx] : 0.0;
+        }
+        for (int c = 0; c < nrhs; ++c) {
+          double acc = 0.0;
+#pragma unroll
+          for (int sidx = 0; sidx < 32; ++sidx) acc = fma(l[sidx], W[(size_t)(i0 + min(sidx, h - 1)) * nrhs + c], acc);
+          W[(size_t)i * nrhs + c] -= acc;
+        }
+        if (stage) {
+#pragma unroll
+          for (int sidx = 0; sidx < 32; ++sidx) Dn[rn * 33 + sidx] = dn[sidx];
+        }
+      }
+      __syncthreads();
+      cur = 1 - cur;
+    }
+  }
+}
+
+// Solve with the right-hand sides in shared memory (n nrhs small enough): the
+// permutation is composed once, every application reads the factors in chunks, the
+// residual B - A X is one warp per row in double-double arithmetic, then the
+// reference's columnwise max-scaled acceptance (cuda.py:230-255).
+template <int NR>
+__global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
+    int n, int nrhs, const double* __restrict__ mats, const double* __restrict__ factors,
+    const int32_t* __restrict__ piv, const double* __restrict__ rs, const double* __restrict__ cs,
+    const double* __restrict__ rhs, double* __restrict__ x, double rtol, double atol, int max_refine,
+    int32_t* __restrict__ status) {
+  extern __shared__ __align__(16) double sm[];
+  double* X = sm;                          // (n, nrhs)
+  double* W = X + (size_t)n * nrhs;        // (n, nrhs)
+  double* Dg = W + (size_t)n * nrhs;       // 2 x 32 x 33
+  double* part = Dg + 2 * 32 * 33;         // 32 x 16
+  double* colr = part + 32 * 16;           // (3, 16): bmax, b2, r2 per column
+  int* perm = reinterpret_cast<int*>(colr + 3 * 16);
+  int* iperm = perm + n;
+  __shared__ int flag;
+  const int m = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  const size_t nn = (size_t)n * n, nb = (size_t)n * nrhs;
+  const double* A = mats + nn * m;
+  const double* LU = factors + nn * m;
+  const double* rsc = rs + (size_t)n * m;
+  const double* csc = cs + (size_t)n * m;
+  const double* B = rhs + nb * m;
+  double* Xg = x + nb * m;
+  if (status[m] != MHM_CELL_OK) return;
+  if (tid == 0) {
+    for (int i = 0; i < n; ++i) perm[i] = i;
+    const int32_t* pv = piv + (size_t)n * m;
+    for (int k = 0; k < n; ++k) {
+      const int p = pv[k];
+      if (p != k) { const int t = perm[k]; perm[k] = perm[p]; perm[p] = t; }
+    }
+    for (int i = 0; i < n; ++i) iperm[perm[i]] = i;
+    flag = 0;
+  }
+  if (tid < 16) colr[tid] = colr[16 + tid] = 0.0;
+  __syncthreads();
+  int nonfinite = 0;
+  for (size_t idx = tid; idx < nb; idx += blockDim.x)
+    if (!isfinite(B[idx])) nonfinite = 1;
+  if (__syncthreads_or(nonfinite)) {
+    for (size_t idx = tid; idx < nb; idx += blockDim.x) Xg[idx] = B[idx];
+    if (tid == 0) status[m] = MHM_CELL_NONFINITE;
+    return;
+  }
+  // per column: max |b| and ||b / scale||^2
+  for (int c = wid; c < nrhs; c += nw) {
+    double bmax = 0.0;
+    for (int i = lane; i < n; i += 32) bmax = fmax(bmax, fabs(B[(size_t)i * nrhs + c]));
+    bmax = warp_max(bmax);
+    double scale = fmax(atol, bmax);
+    if (!(scale > 0.0)) scale = 1.0;
+    double b2 = 0.0;
+    for (int i = lane; i < n; i += 32) {
+      const double bv = B[(size_t)i * nrhs + c] / scale;
+      b2 += bv * bv;
+    }
+    b2 = warp_sum(b2);
+    if (lane == 0) { colr[c] = scale; colr[16 + c] = b2; }
+  }
+  // X = csc .* U^-1 L^-1 P (rsc .* B)
+  for (size_t idx = tid; idx < nb; idx += blockDim.x) {
+    const int i = (int)(idx / nrhs), c = (int)(idx - (size_t)i * nrhs);
+    const int src = perm[i];
+    W[idx] = B[(size_t)src * nrhs + c] * rsc[src];
+  }
+  __syncthreads();
+  chunked_lu_solve(n, nrhs, LU, W, Dg);
+  for (size_t idx = tid; idx < nb; idx += blockDim.x) {
+    const int i = (int)(idx / nrhs);
+    X[idx] = W[idx] * csc[i];
+  }
+  __syncthreads();
+  int result = MHM_CELL_RESIDUAL;
+  for (int pass = 0; pass <= max_refine; ++pass) {
+    int bad = 0;
+    for (size_t idx = tid; idx < nb; idx += blockDim.x)
+      if (!isfinite(X[idx])) bad = 1;
+    if (__syncthreads_or(bad)) { result = MHM_CELL_NONFINITE; break; }
+    // R = B - A X, one warp per row; the scaled residual goes to W at the row's
+    // permuted position (ready for the correction solve); per warp the sums of
+    // (r / scale)^2 per column, added in warp order below
+    double wr2[NR];
+#pragma unroll
+    for (int c = 0; c < NR; ++c) wr2[c] = 0.0;
+    // each lane's (at most 20) entries of the warp's next row are loaded while the
+    // current row is summed
+    constexpr int kPer = kBlockedMaxN / 32;
+    double av[kPer], an[kPer];
+    if (wid < n) {
+      const double* row = A + (size_t)wid * n;
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) av[u] = lane + 32 * u < n ? row[lane + 32 * u] : 0.0;
+    }
+    for (int i = wid; i < n; i += nw) {
+      if (i + nw < n) {
+        const double* nrow = A + (size_t)(i + nw) * n;
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) an[u] = lane + 32 * u < n ? nrow[lane + 32 * u] : 0.0;
+      }
+      double hi[NR], lo[NR];
+#pragma unroll
+      for (int c = 0; c < NR; ++c) hi[c] = lo[c] = 0.0;
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        const int j = lane + 32 * u;
+        if (j < n) {
+#pragma unroll
+          for (int c = 0; c < NR; ++c)
+            if (c < nrhs) dd_fma(hi[c], lo[c], -av[u], X[(size_t)j * nrhs + c]);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < NR; ++c) {
+        if (c >= nrhs) continue;
+        double h = hi[c], l = lo[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const double oh = __shfl_xor_sync(0xffffffffu, h, o);
+          const double ol = __shfl_xor_sync(0xffffffffu, l, o);
+          double sres, e;
+          two_sum(h, oh, sres, e);
+          h = sres;
+          l += ol + e;
+        }
+        if (lane == 0) {
+          double sres, e;
+          two_sum(B[(size_t)i * nrhs + c], h, sres, e);
+          const double r = sres + (e + l);
+          W[(size_t)iperm[i] * nrhs + c] = r * rsc[i];
+          const double rv = r / colr[c];
+          wr2[c] = fma(rv, rv, wr2[c]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) av[u] = an[u];
+    }
+    if (lane == 0)
+#pragma unroll
+      for (int c = 0; c < NR; ++c) part[wid * 16 + c] = wr2[c];
+    __syncthreads();
+    if (tid == 0) {
+      for (int c = 0; c < nrhs; ++c) {
+        double t = 0.0;
+        for (int q = 0; q < nw; ++q) t += part[q * 16 + c];
+        colr[32 + c] = t;
+      }
+      int ok = 1;
+      for (int c = 0; c < nrhs; ++c) {
+        const double scale = colr[c];
+        const double limit = fmax(atol / scale, rtol * sqrt(colr[16 + c]));
+        if (!(sqrt(colr[32 + c]) <= limit)) ok = 0;
+      }
+      flag = ok;
+    }
+    __syncthreads();
+    if (flag) { result = MHM_CELL_OK; break; }
+    if (pass == max_refine) break;
+    chunked_lu_solve(n, nrhs, LU, W, Dg);
+    for (size_t idx = tid; idx < nb; idx += blockDim.x) {
+      const int i = (int)(idx / nrhs);
+      X[idx] += W[idx] * csc[i];
+    }
+    __syncthreads();
+  }
+  for (size_t idx = tid; idx < nb; idx += blockDim.x) Xg[idx] = X[idx];
+  if (tid == 0 && result != MHM_CELL_OK) status[m] = result;
+}
+
+size_t chunked_solve_smem(int n, int nrhs) {
+  return ((size_t)2 * n * nrhs + 2 * 32 * 33 + 32 * 16 + 3 * 16) * 8 + (size_t)2 * n * 4;
+}
 }  // namespace
 }  // namespace mhm
 
@@ -237,12 +732,22 @@ extern "C" int mhm_batched_factor(int64_t count, int32_t n, const double* matric
   if (count > 0x7fffffff) return MHM_ERR_UNSUPPORTED;
   const size_t bytes = (size_t)n * n * 8;
   const int in_smem = bytes <= 200 * 1024;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (!in_smem && n <= kBlockedMaxN) {
+    const size_t smem = ((size_t)n * kPanelStride + (size_t)kPanel * kTileStride) * 8;
+    if (cudaFuncSetAttribute(batched_factor_blocked_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+      return MHM_ERR_LAUNCH;
+    batched_factor_blocked_kernel<<<(unsigned)count, kLuThreads, smem, st>>>(n, matrices, factors, pivots,
+                                                                             row_scale, col_scale, status);
+    return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+  }
   const size_t smem = in_smem ? bytes : 0;
   if (in_smem && smem > 48 * 1024 &&
       cudaFuncSetAttribute(batched_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
     return MHM_ERR_LAUNCH;
-  batched_factor_kernel<<<(unsigned)count, kLuThreads, smem, static_cast<cudaStream_t>(stream)>>>(
+  batched_factor_kernel<<<(unsigned)count, kLuThreads, smem, st>>>(
       n, matrices, factors, pivots, row_scale, col_scale, status, in_smem);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
@@ -256,6 +761,22 @@ extern "C" int mhm_batched_solve(int64_t count, int32_t n, int32_t nrhs, const d
       !col_scale || !rhs || !x || !work || !status || max_refine < 0 || !(rtol >= 0) || !(atol >= 0))
     return MHM_ERR_ARGUMENT;
   if (count > 0x7fffffff) return MHM_ERR_UNSUPPORTED;
+  const size_t smem = chunked_solve_smem(n, nrhs);
+  // the residual's row prefetch covers n <= kBlockedMaxN columns
+  if (n <= kBlockedMaxN && nrhs <= 16 && smem <= 200 * 1024) {
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    auto go = [&](auto kernel) {
+      if (smem > 48 * 1024 &&
+          cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return MHM_ERR_LAUNCH;
+      kernel<<<(unsigned)count, kLuThreads, smem, st>>>(n, nrhs, matrices, factors, pivots, row_scale, col_scale,
+                                                        rhs, x, rtol, atol, max_refine, status);
+      return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+    };
+    if (nrhs <= 4) return go(batched_solve_chunked_kernel<4>);
+    if (nrhs <= 8) return go(batched_solve_chunked_kernel<8>);
+    return go(batched_solve_chunked_kernel<16>);
+  }
   batched_solve_kernel<<<(unsigned)count, kLuThreads, 0, static_cast<cudaStream_t>(stream)>>>(
       n, nrhs, matrices, factors, pivots, row_scale, col_scale, rhs, x, work, rtol, atol, max_refine,
       status);

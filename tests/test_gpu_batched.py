@@ -69,6 +69,40 @@ def test_random_batches_with_refinement():
         assert np.all(r <= 1e-12)
 
 
+@pytest.mark.parametrize("n,nrhs", [(33, 4), (45, 1), (160, 1), (161, 4), (326, 4), (326, 17), (640, 16), (641, 3),
+                                    (1000, 1)])
+def test_factor_and_solve_paths(n, nrhs):
+    """Every factor path (shared memory n <= 160, blocked 161..640, unblocked on the
+    factors array above) and solve path (chunked with the right-hand sides in shared
+    memory for nrhs <= 16, one warp per column otherwise) on matrices that need row
+    pivoting."""
+    from pymhm_b200.batched import BatchedFactorization
+
+    rng = np.random.default_rng(n + nrhs)
+    a = rng.normal(size=(4, n, n))
+    a[:, :, 1] *= 1e5
+    x = rng.normal(size=(4, n, nrhs))
+    b = a @ x
+    with BatchedFactorization(a) as f:
+        got = f.solve(b, host=True)
+        piv = f.pivots.cpu().numpy()
+    assert np.any(piv != np.arange(n))  # pivoting happened
+    r = np.linalg.norm(a @ got - b, axis=1) / np.linalg.norm(b, axis=1)
+    assert np.all(r <= 1e-12)
+    assert np.max(np.abs(got - x)) <= 1e-8 * np.max(np.abs(x))
+
+
+def test_blocked_factor_reports_rank_deficiency():
+    from pymhm_b200.batched import BatchedFactorization
+    from pymhm_b200.errors import LinearSolveError
+
+    rng = np.random.default_rng(5)
+    a = rng.normal(size=(2, 300, 300))
+    a[1, 150] = a[1, 20] * 3.0  # dependent rows in the second matrix only
+    with pytest.raises(LinearSolveError, match="rank deficient|singular pivot"):
+        BatchedFactorization(a)
+
+
 def test_condense_batched_matches_oracle_condensation():
     """Augmented Q1 systems from the fixture, through the generic batched path."""
     from types import SimpleNamespace
