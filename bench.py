@@ -144,7 +144,27 @@ def parse():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true", help="small run for ncu (no baselines, no e2e)")
+    ap.add_argument("--lu-case", type=int, default=0, metavar="N",
+                    help="only factor 64 seeded N x N matrices twice with the batched LU (for ncu)")
     return ap.parse_args()
+
+
+def lu_case(n, batch=64):
+    """The batched dense LU on ``batch`` seeded matrices N(0,1) + n I, factored twice."""
+    import torch
+
+    from pymhm_b200 import _lib
+    from pymhm_b200.batched import BatchedFactorization
+
+    rng = np.random.default_rng(0)
+    a = torch.from_numpy(rng.normal(size=(batch, n, n)) + n * np.eye(n)).to("cuda")
+    f = BatchedFactorization(a)
+    P = _lib.ptr
+    for _ in range(2):
+        _lib.check(f.lib.mhm_batched_factor(batch, n, P(f.matrix), P(f.factors), P(f.pivots), P(f.row_scale),
+                                            P(f.col_scale), P(f.status), None), "mhm_batched_factor")
+    torch.cuda.synchronize()
+    print(json.dumps({"lu_case": n, "batch": batch, "ok": bool((f.status == 0).all())}))
 
 
 def dist_env():
@@ -277,6 +297,9 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.lu_case:
+        lu_case(args.lu_case)
         return
     rank, world, local = dist_env()
     kappa = workload_kappa()
