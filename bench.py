@@ -136,6 +136,61 @@ def batched_local_campaign(torch, refinement, batch=64, queries=12, repeats=3):
     return out
 
 
+SERVING_MACRO = (16, 32, 64)
+SERVING_LOCAL = (4, 8, 16)
+
+
+def serving_campaign(torch, lambdas=(100, 500, 2000), requests=150, precisions=("mixed", "fp64")):
+    """Streamed serving (continuous batching with admission by HBM footprint): Poisson
+    arrivals at each rate in ``lambdas``; per request a macro grid from {16, 32, 64}^2,
+    a local refinement from {4, 8, 16}^2, a seeded log-normal permeability (sigma in
+    [1, 2], correlation length 0.05; drawn from a pool of two fields per fine-grid
+    size, generated before timing) and 1..8 constant sources, the first solved with
+    factors kept, the others through the kept factors.  One untimed warm-up stream
+    creates the slots.  Returns p50/p99 latency (arrival to results in pinned host
+    memory) and solves/s per rate and precision."""
+    from pymhm_b200.serving import DarcyRequest, ServingEngine, summarize
+    from pymhm_b200.workloads import lognormal_permeability
+
+    rng = np.random.default_rng(5)
+    pool = {}
+    for m in SERVING_MACRO:
+        for r in SERVING_LOCAL:
+            n = m * r
+            if n not in pool:
+                pool[n] = [lognormal_permeability(n, n, sigma=float(rng.uniform(1.0, 2.0)), ell=0.05,
+                                                  seed=int(rng.integers(1 << 30))) for _ in range(2)]
+
+    def stream(lam, count, seed):
+        g = np.random.default_rng(seed)
+        t = np.cumsum(g.exponential(1.0 / lam, count)) if lam else np.zeros(count)
+        out = []
+        for i in range(count):
+            m, r = int(g.choice(SERVING_MACRO)), int(g.choice(SERVING_LOCAL))
+            kappa = pool[m * r][int(g.integers(2))]
+            sources = tuple(float(v) for v in g.uniform(0.5, 2.0, int(g.integers(1, 9))))
+            out.append(DarcyRequest(m, r, kappa, sources, arrival=float(t[i])))
+        return out
+
+    result = {}
+    for prec in precisions:
+        engine = ServingEngine(precision=prec, max_in_flight=8)
+        warm = [DarcyRequest(m, r, pool[m * r][0], (1.0, 2.0)) for m in SERVING_MACRO for r in SERVING_LOCAL] * 3
+        engine.run(warm, realtime=False)
+        per = {}
+        for lam in lambdas:
+            per[f"lambda_{lam}"] = summarize(engine.run(stream(lam, requests, lam)))
+        per["slots"] = len(engine.slots)
+        per["peak_device_bytes"] = int(engine.stats.get("peak_bytes", 0))
+        result[prec] = per
+        del engine
+        torch.cuda.empty_cache()
+    result["workload"] = (f"{requests} requests per rate, Poisson arrivals; macro in {SERVING_MACRO}^2, local in "
+                          f"{SERVING_LOCAL}^2, P2 faces, 1..8 constant sources per request (kept factors); "
+                          "HBM budget 150 GB, 8 requests in flight")
+    return result
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -444,6 +499,9 @@ def main():
                   "note": "refine_hybrid on the mixed solve: original-equation residual, defect source responses "
                           "with a fresh factorization, correction solve, reconstruction; forced one step"}
 
+    # streamed serving of independent requests (continuous batching, HBM admission)
+    serving_stream = serving_campaign(torch)
+
     # the reference's own batched local-stage benchmark, same phases and sizes
     campaigns = {f"batched_local_r{r}": batched_local_campaign(torch, r) for r in (12, 24)}
     campaigns["reference_rtx3060_ms"] = {
@@ -566,6 +624,7 @@ def main():
                                       "right-hand-side reduction + global solve + reconstruction, one at a time"},
         "refinement": refinement,
         "reference_campaigns": campaigns,
+        "serving_stream": serving_stream,
         "global_iterations": int(mixed["info"][1]), "outer_corrections": int(mixed["info"][2]),
         "residual": float(mixed["stats"][0]), "certificate": float(mixed["stats"][1]),
         "error_vs_reference": acc,

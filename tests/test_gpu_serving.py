@@ -1,0 +1,85 @@
+"""The serving loop (pymhm_b200.serving): every request's result is the same alone and
+in the mix, agrees with an independent solve, and admission respects the HBM budget."""
+
+import numpy as np
+import pytest
+
+from tests._cases import rel
+
+pytestmark = pytest.mark.gpu
+
+
+def make_requests(count=6, seed=11):
+    from pymhm_b200.serving import DarcyRequest
+    from pymhm_b200.workloads import lognormal_permeability
+
+    rng = np.random.default_rng(seed)
+    shapes = [(4, 4), (8, 4), (4, 8), (8, 8), (4, 16), (8, 16)]
+    reqs = []
+    for i in range(count):
+        macro, ref = shapes[i % len(shapes)]
+        n = macro * ref
+        kappa = lognormal_permeability(n, n, sigma=float(rng.uniform(1, 2)), ell=0.1, seed=int(rng.integers(1 << 30)))
+        sources = tuple(float(v) for v in rng.uniform(0.5, 2.0, int(rng.integers(1, 4))))
+        reqs.append(DarcyRequest(macro, ref, kappa, sources, arrival=0.004 * i))
+    return reqs
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_results_are_the_same_alone_and_in_the_mix(precision):
+    from pymhm_b200.darcy import CartesianQ1Plan
+    from pymhm_b200.serving import ServingEngine
+    from pymhm_b200.topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
+
+    reqs = make_requests()
+    mix = ServingEngine(precision=precision, max_in_flight=4, keep_fields=True)
+    together = mix.run(reqs, realtime=False)
+    assert mix.stats["peak_in_flight"] > 1
+    alone = ServingEngine(precision=precision, max_in_flight=1, keep_fields=True).run(reqs, realtime=False)
+    for req, a, b in zip(reqs, together, alone):
+        assert len(a.x) == len(req.sources)
+        for k in range(len(req.sources)):
+            assert np.array_equal(a.x[k], b.x[k])
+            assert np.array_equal(a.fields[k], b.fields[k])
+            assert np.array_equal(a.flux[k], b.flux[k])
+    # and each agrees with a fresh plan solving the same request source by source
+    tol = 1e-10 if precision == "fp64" else 1e-8
+    for req, res in zip(reqs, together):
+        mesh = CartesianMacroMesh(req.macro)
+        sk = SkeletonSpace(mesh, (FaceSpace.uniform(req.face_degree),) * len(mesh.faces))
+        plan = CartesianQ1Plan(mesh, sk, req.refinement, precision=precision)
+        for k, src in enumerate(req.sources):
+            sol = plan.solve(req.permeability, src)
+            assert rel(res.fields[k], sol.fields) <= tol
+            assert rel(res.x[k][: plan.T], sol.trace) <= tol
+
+
+def test_admission_respects_the_hbm_budget():
+    from pymhm_b200.serving import ServingEngine
+
+    reqs = [r for r in make_requests(8) if (r.macro, r.refinement) == (8, 8)] or make_requests(4)[:2]
+    probe = ServingEngine(max_in_flight=4)
+    probe.run(reqs[:1], realtime=False)
+    one = probe.stats["peak_bytes"]
+    engine = ServingEngine(max_in_flight=4, hbm_budget=1.5 * one, keep_fields=True)
+    out = engine.run(reqs * 3, realtime=False)
+    assert engine.stats["peak_in_flight"] == 1
+    assert engine.stats["peak_bytes"] <= 1.5 * one
+    for a, b in zip(out, out[len(reqs):]):
+        assert np.array_equal(a.fields[0], b.fields[0])
+    with pytest.raises(ValueError, match="HBM budget"):
+        ServingEngine(hbm_budget=one / 2).run(reqs[:1], realtime=False)
+
+
+def test_realtime_arrivals_and_latency():
+    from pymhm_b200.serving import ServingEngine, summarize
+
+    reqs = make_requests(6)
+    out = ServingEngine(max_in_flight=3).run(reqs)
+    for req, res in zip(reqs, out):
+        assert res.admitted >= req.arrival - 1e-6
+        assert res.finished >= res.admitted
+        assert res.latency > 0
+    s = summarize(out)
+    assert s["requests"] == 6 and s["rhs"] == sum(len(r.sources) for r in reqs)
+    assert s["latency_ms"]["p99"] >= s["latency_ms"]["p50"] > 0
