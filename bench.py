@@ -146,8 +146,9 @@ def serving_campaign(torch, lambdas=(100, 500, 2000), requests=150, precisions=(
     a local refinement from {4, 8, 16}^2, a seeded log-normal permeability (sigma in
     [1, 2], correlation length 0.05; drawn from a pool of two fields per fine-grid
     size, generated before timing) and 1..8 constant sources, the first solved with
-    factors kept, the others through the kept factors.  One untimed warm-up stream
-    creates the slots.  Returns p50/p99 latency (arrival to results in pinned host
+    factors kept, the others through the kept factors.  Before timing, four slots per
+    shape are reserved (plans built, both steps captured as CUDA graphs) and one
+    untimed stream warms them.  Returns p50/p99 latency (arrival to results in pinned host
     memory) and solves/s per rate and precision."""
     from pymhm_b200.serving import DarcyRequest, ServingEngine, summarize
     from pymhm_b200.workloads import lognormal_permeability
@@ -175,7 +176,10 @@ def serving_campaign(torch, lambdas=(100, 500, 2000), requests=150, precisions=(
     result = {}
     for prec in precisions:
         engine = ServingEngine(precision=prec, max_in_flight=8)
-        warm = [DarcyRequest(m, r, pool[m * r][0], (1.0, 2.0)) for m in SERVING_MACRO for r in SERVING_LOCAL] * 3
+        for m in SERVING_MACRO:
+            for r in SERVING_LOCAL:
+                engine.reserve((m, r, FACE_DEGREE), 4)
+        warm = [DarcyRequest(m, r, pool[m * r][0], (1.0, 2.0)) for m in SERVING_MACRO for r in SERVING_LOCAL] * 2
         engine.run(warm, realtime=False)
         per = {}
         for lam in lambdas:
@@ -481,7 +485,24 @@ def main():
             steps_on.append(ev[0].elapsed_time(ev[4]))
             kern_on.append(ev[0].elapsed_time(ev[1]))
         plan.check()
-        online[prec] = {"ms_per_solve": float(np.mean(steps_on)), "source_response_ms": float(np.mean(kern_on))}
+        # the same query captured as a CUDA graph and replayed
+        plan.capture_online()
+        for _ in range(args.warmup):
+            gst = plan.replay_online(1.0)
+        torch.cuda.synchronize()
+        steps_g = []
+        for k in range(args.steps):
+            flush.zero_()
+            g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            g0.record(gst)
+            plan.replay_online(1.0 + 0.01 * k, stream=gst)
+            g1.record(gst)
+            torch.cuda.synchronize()
+            steps_g.append(g0.elapsed_time(g1))
+        plan.check()
+        online[prec] = {"ms_per_solve": float(np.mean(steps_on)), "source_response_ms": float(np.mean(kern_on)),
+                        "graph_ms_per_solve": float(np.mean(steps_g))}
+        plan._graphs = None
         plan.factors = None
 
     # original-equation refinement of a mixed-precision solve (refine_hybrid): one

@@ -605,6 +605,78 @@ class CartesianQ1Plan:
             self.check()
             step += 1
 
+    def capture(self, local="online", stream=None):
+        """Capture one solve as a CUDA graph that ``replay`` runs again.
+
+        ``local="offline"`` captures the condensation that keeps every cell's factor,
+        the skeleton reduction, the global solve and the reconstruction
+        (``OfflineHybridSystem``'s offline step); ``"online"`` captures a new source's
+        responses with the kept factors, the right-hand-side reduction, the global
+        solve and the reconstruction.  Kernel arguments are fixed at capture: the
+        permeability buffer must stay where ``set_device_coefficients`` put it, and the
+        source is read from a persistent per-fine-cell device buffer that each replay
+        overwrites first (a constant source gives the same element loads as
+        ``source_mode`` 0).  The graph's launches run once eagerly before the capture."""
+        torch = self.torch
+        if local not in ("offline", "online"):
+            raise ValueError("local must be 'offline' or 'online'")
+        if local == "online" and not getattr(self, "_factors_current", False):
+            raise RuntimeError("prepare_offline() must run before capturing online queries")
+        if local == "offline" and getattr(self, "factors", None) is None:
+            nbytes = int(self.lib.mhm_q1_factor_bytes(self.q1, PRECISIONS[self.precision]))
+            self.factors = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        if getattr(self, "_graph_source", None) is None:
+            self._graph_source = torch.zeros((self.nxf, self.nyf), dtype=torch.float64, device=self.device)
+        q = self.q1
+        q.source_mode, q.source, q.source_const = 1, _lib.ptr(self._graph_source), 0.0
+        self._keep = (self._keep[0], self._graph_source)
+        if getattr(self, "_graphs", None) is None:
+            self._graphs, self._graph_stream = {}, None
+        st = self._graph_stream or (torch.cuda.Stream(device=self.device) if stream is None else stream)
+        self._graph_stream = st
+        st.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(st):
+            self.launch(st, local=local)  # warm-up outside the capture
+        st.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=st):
+            self.launch(st, local=local)
+        self._graphs[local] = graph
+        return graph
+
+    def capture_online(self, stream=None):
+        """``capture("online")``; requires ``prepare_offline``."""
+        return self.capture("online", stream)
+
+    def replay(self, local="online", source=0.0, *, stream=None, after=None):
+        """Run the captured ``local`` solve for ``source`` (a constant or one value per
+        fine cell, shape (nx*rx, ny*ry)), asynchronously on ``stream`` (default: the
+        capture stream) after ``after`` (default: the current stream).  Returns the
+        stream it ran on."""
+        torch = self.torch
+        graph = (getattr(self, "_graphs", None) or {}).get(local)
+        if graph is None:
+            raise RuntimeError(f"capture({local!r}) must run first")
+        st = self._graph_stream if stream is None else stream
+        if after is not st:
+            st.wait_stream(torch.cuda.current_stream() if after is None else after)
+        with torch.cuda.stream(st):
+            if isinstance(source, numbers.Number):
+                self._graph_source.fill_(float(source))
+            else:
+                arr = np.asarray(source, dtype=float)
+                if arr.shape != (self.nxf, self.nyf):
+                    raise ValueError(f"fine-cell source must have shape ({self.nxf}, {self.nyf})")
+                self._graph_source.copy_(torch.as_tensor(arr), non_blocking=False)
+            graph.replay()
+        if local == "offline":
+            self._factors_current = True
+        return st
+
+    def replay_online(self, source=0.0, *, stream=None):
+        """``replay("online", source, after=stream)``."""
+        return self.replay("online", source, after=stream)
+
     def result(self, seconds=0.0) -> Q1Solution:
         info, stats = self.check()
         x = self.x.cpu().numpy()

@@ -6,8 +6,10 @@ permeability field and 1..8 sources.  The engine keeps *slots*: a resident
 permeability buffer and pinned host buffers.  A request is admitted, in arrival
 order, as soon as a slot of its shape is idle or a new one fits both the in-flight
 limit and the HBM budget; otherwise it waits, and idle slots of other shapes are
-released to make room.  An admitted request is enqueued on its slot's stream
-without host synchronisation: the permeability upload, the condensation that keeps
+released to make room.  Each slot captures both steps of a request as CUDA graphs
+when it is created.  An admitted request is enqueued on its slot's stream without
+host synchronisation: the permeability upload, then graph replays of the
+condensation that keeps
 every cell's factor (``OfflineHybridSystem``'s offline step,
 ``core/offline.py:148-229``), the global solve and the reconstruction for the first
 source, then for each further source only the source responses with the kept
@@ -83,9 +85,13 @@ class _Slot:
         nbytes = int(plan.lib.mhm_q1_factor_bytes(plan.q1, PRECISIONS[engine.precision]))
         plan.factors = torch.empty(nbytes, dtype=torch.uint8, device=plan.device)
         n_fine = macro * refinement
-        self.kappa = torch.empty((n_fine, n_fine), dtype=torch.float64, device=plan.device)
+        self.kappa = torch.ones((n_fine, n_fine), dtype=torch.float64, device=plan.device)
         self.kappa_host = torch.empty((n_fine, n_fine), dtype=torch.float64).pin_memory()
         self.stream = torch.cuda.Stream(device=plan.device)
+        # both steps of a request captured once as CUDA graphs on the slot's stream
+        plan.set_device_coefficients(1, self.kappa, (0.0, 0.0, 0.0), 0, None, 1.0)
+        plan.capture("offline", stream=self.stream)
+        plan.capture("online", stream=self.stream)
         self.done = torch.cuda.Event()
         pin = dict(dtype=torch.float64)
         self.x_host = [torch.empty(plan.N, **pin).pin_memory() for _ in range(MAX_SOURCES)]
@@ -118,12 +124,7 @@ class _Slot:
             np.copyto(self.kappa_host.numpy(), request.permeability)
             self.kappa.copy_(self.kappa_host, non_blocking=True)
             for k, src in enumerate(request.sources):
-                if k == 0:
-                    plan.set_device_coefficients(1, self.kappa, (0.0, 0.0, 0.0), 0, None, float(src))
-                    plan.launch(st, local="offline")
-                else:
-                    plan.set_source(float(src))
-                    plan.launch(st, local="online")
+                plan.replay("offline" if k == 0 else "online", float(src), stream=st, after=st)
                 self.x_host[k].copy_(plan.x, non_blocking=True)
                 self.status_host[k].copy_(plan.cell_status, non_blocking=True)
                 self.info_host[k].copy_(plan.info, non_blocking=True)
@@ -217,6 +218,27 @@ class ServingEngine:
         self.stats["slots_created"] = self.stats.get("slots_created", 0) + 1
         self.stats["peak_bytes"] = max(self.stats.get("peak_bytes", 0), self._bytes())
         return slot
+
+    def reserve(self, shape, count=1) -> int:
+        """Create idle slots for ``shape`` (macro, refinement, face degree) until there are
+        ``count`` of them or the budget is reached, so that later requests do not pay
+        for plan construction and graph capture; returns the slots of that shape."""
+        shape = tuple(int(v) for v in shape)
+        have = [s for s in self.slots if s.shape == shape]
+        while len(have) < count:
+            need = self._shape_bytes.get(shape, 0)
+            if (self.max_slots is not None and len(self.slots) >= self.max_slots) or \
+                    self._bytes() + need > self.hbm_budget:
+                break
+            slot = _Slot(self, shape)
+            self._shape_bytes[shape] = slot.bytes
+            if self._bytes() + slot.bytes > self.hbm_budget:
+                break
+            self.slots.append(slot)
+            have.append(slot)
+            self.stats["slots_created"] = self.stats.get("slots_created", 0) + 1
+            self.stats["peak_bytes"] = max(self.stats.get("peak_bytes", 0), self._bytes())
+        return len(have)
 
     def run(self, requests, *, realtime=True) -> list[DarcyResult]:
         """Serve ``requests`` (arrival times relative to the call) and return their

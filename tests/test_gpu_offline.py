@@ -64,3 +64,30 @@ def test_online_needs_the_offline_step():
         plan.launch(local="online")
     assert plan.lib.mhm_q1_factor_bytes(plan.q1, 0) == 64 * 5 * 5 * 5 * 8
     assert plan.lib.mhm_q1_factor_bytes(plan.q1, 1) == 64 * 5 * 5 * 5 * 4
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_captured_online_query_matches_eager(precision):
+    """One online query captured as a CUDA graph gives the eager query's bits, for a
+    constant and for a per-fine-cell source, replay after replay."""
+    import torch
+
+    from tests.test_gpu_darcy import make_plan
+
+    g, plan = make_plan("darcy_4x4_r16_p2_lognormal", precision)
+    plan.prepare_offline()
+    rng = np.random.default_rng(4)
+    cells = rng.uniform(0.5, 2.0, (plan.nxf, plan.nyf))
+    eager = {}
+    for key, src in (("const", 1.75), ("cells", cells)):
+        sol = plan.solve_source(src)
+        eager[key] = (sol.fields.copy(), sol.trace.copy())
+    plan.capture_online()
+    for _ in range(2):
+        for key, src in (("const", 1.75), ("cells", cells)):
+            st = plan.replay_online(src)
+            st.synchronize()
+            plan.check()
+            assert np.array_equal(plan.fields.cpu().numpy(), eager[key][0])
+            assert np.array_equal(plan.x.cpu().numpy()[: plan.T], eager[key][1])
+    torch.cuda.synchronize()
