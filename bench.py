@@ -203,6 +203,8 @@ def parse():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true", help="small run for ncu (no baselines, no e2e)")
+    ap.add_argument("--profile-extras", action="store_true",
+                    help="with --profile: also one refinement step, a P1 batch assembly and a batched LU")
     ap.add_argument("--lu-case", type=int, default=0, metavar="N",
                     help="only factor 64 seeded N x N matrices twice with the batched LU (for ncu)")
     return ap.parse_args()
@@ -393,8 +395,30 @@ def main():
             plan.launch(torch.cuda.current_stream())
         torch.cuda.synchronize()
         info, _ = plan.check()
+        extras = {}
+        if args.profile_extras:
+            # one forced refinement step of this solve, the P1 batch assembly and the
+            # batched LU of the 64 x 325 local-stage campaign
+            ref = plan.refine(max_steps=1, min_steps=1, rtol=1e-9)
+            from pymhm_b200.batched import BatchedFactorization, assemble_p1_batch
+
+            pts, cells = triangle_submesh(24)
+            coords = torch.from_numpy(np.repeat(pts[None], 64, axis=0)).to(dev)
+            stiff, mass, load = assemble_p1_batch(coords, torch.from_numpy(cells).to(dev),
+                                                  diffusion=torch.diag(torch.tensor([3.0, 1.0], device=dev)),
+                                                  source=1.0)
+            n = stiff.shape[1]
+            system = torch.zeros((64, n + 1, n + 1), dtype=torch.float64, device=dev)
+            system[:, :n, :n] = stiff
+            system[:, :n, n] = system[:, n, :n] = mass.sum(dim=2)
+            rhs = torch.zeros((64, n + 1, 4), dtype=torch.float64, device=dev)
+            rhs[:, :n, 0] = load
+            with BatchedFactorization(system) as fact:
+                fact.solve(rhs)
+            torch.cuda.synchronize()
+            extras = {"refinement_residuals": [float(v) for v in ref.residual_norms], "p1_batch": [64, n]}
         print(json.dumps({"profile": True, "launches": 4 * (args.warmup + args.steps),
-                          "global_iterations": int(info[1])}), flush=True)
+                          "global_iterations": int(info[1]), **extras}), flush=True)
         return
     plans = {p: [CartesianQ1Plan(mesh, sk, LOCAL, precision=p) for _ in range(2)] for p in ("mixed", "fp64")}
     kappa_host = torch.from_numpy(np.ascontiguousarray(kappa)).pin_memory()

@@ -180,15 +180,16 @@ int mhm_q1_original_defect(const mhm_q1_problem* p /* host */, const int64_t* ce
                            void* stream);
 
 /*
- * Norms of one refinement step, summed in a fixed order by one block:
+ * Norms of one refinement step, each summed in a fixed order:
  * out[0] = ||[defects; weak]||^2, out[1] = ||[loads; boundary]||^2,
  * out[2] = ||[weak; sum d per cell]||^2 and, if indptr is given, out[3] =
  * ||rhs||^2 and out[4] = || |K| |x| ||^2 of the assembled CSR system (size rows).
+ * out holds 5 + 5 * 256 doubles: the block partials follow the five results.
  */
 int mhm_refine_norms(int32_t cells, const double* partial, int64_t trace_size, const double* weak,
                      const double* boundary, int64_t size, const int64_t* indptr,
                      const int32_t* indices, const double* values, const double* x,
-                     const double* rhs, double* out /* 5 */, void* stream);
+                     const double* rhs, double* out /* 5 + 1280 */, void* stream);
 
 /*
  * Correction source responses (refinement.py:779-798): solution column 0 and

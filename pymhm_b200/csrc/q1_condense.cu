@@ -1011,23 +1011,35 @@ __global__ void weak_residual_kernel(int64_t trace_size, int t, const int32_t* d
   }
 }
 
-// Norms of a refinement step, each a sum in a fixed order (one block):
-// out[0] = ||[d; weak]||^2 (original residual), out[1] = ||[f; boundary]||^2
-// (its scale), out[2] = ||[weak; 1.d per cell]||^2 (reduced residual),
-// out[3] = ||rhs||^2 and out[4] = || |K| |x| ||^2 of the assembled system.
-__global__ void __launch_bounds__(1024) refine_norms_kernel(int cells, const double* partial, int64_t trace_size,
+// Norms of a refinement step: out[0] = ||[d; weak]||^2 (original residual),
+// out[1] = ||[f; boundary]||^2 (its scale), out[2] = ||[weak; 1.d per cell]||^2
+// (reduced residual), out[3] = ||rhs||^2 and out[4] = || |K| |x| ||^2 of the
+// assembled system.  Block b of kNormBlocks sums fixed index ranges of the cells,
+// trace DOFs and rows into partial[b][5]; refine_norms_final adds the partials in
+// block order, so every sum has a fixed order.
+constexpr int kNormBlocks = 256;
+
+__device__ __forceinline__ void block_range(int64_t n, int64_t& lo, int64_t& hi) {
+  lo = n * blockIdx.x / gridDim.x;
+  hi = n * (blockIdx.x + 1) / gridDim.x;
+}
+
+__global__ void __launch_bounds__(256) refine_norms_partial(int cells, const double* partial, int64_t trace_size,
                                                             const double* weak, const double* boundary,
                                                             int64_t size, const int64_t* indptr,
                                                             const int32_t* indices, const double* values,
-                                                            const double* x, const double* rhs, double* out) {
+                                                            const double* x, const double* rhs, double* blocks) {
   __shared__ double red[32];
   double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int c = threadIdx.x; c < cells; c += blockDim.x) {
-    v[0] += partial[3 * (size_t)c];
-    v[1] += partial[3 * (size_t)c + 1];
-    v[2] += partial[3 * (size_t)c + 2] * partial[3 * (size_t)c + 2];
+  int64_t lo, hi;
+  block_range(cells, lo, hi);
+  for (int64_t c = lo + threadIdx.x; c < hi; c += blockDim.x) {
+    v[0] += partial[3 * c];
+    v[1] += partial[3 * c + 1];
+    v[2] += partial[3 * c + 2] * partial[3 * c + 2];
   }
-  for (int64_t i = threadIdx.x; i < trace_size; i += blockDim.x) {
+  block_range(trace_size, lo, hi);
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
     const double w2 = weak[i] * weak[i];
     v[0] += w2;
     v[2] += w2;
@@ -1035,7 +1047,8 @@ __global__ void __launch_bounds__(1024) refine_norms_kernel(int cells, const dou
     v[1] += b * b;
   }
   if (indptr) {
-    for (int64_t r = threadIdx.x; r < size; r += blockDim.x) {
+    block_range(size, lo, hi);
+    for (int64_t r = lo + threadIdx.x; r < hi; r += blockDim.x) {
       double acc = 0.0;
       for (int64_t e = indptr[r]; e < indptr[r + 1]; ++e) acc = fma(fabs(values[e]), fabs(x[indices[e]]), acc);
       v[4] = fma(acc, acc, v[4]);
@@ -1044,8 +1057,18 @@ __global__ void __launch_bounds__(1024) refine_norms_kernel(int cells, const dou
   }
   for (int k = 0; k < 5; ++k) {
     const double tot = block_sum(v[k], red);
-    if (threadIdx.x == 0) out[k] = tot;
+    if (threadIdx.x == 0) blocks[blockIdx.x * 5 + k] = tot;
   }
+}
+
+// Warp k adds the partials of result k (lane-strided, then a fixed shuffle tree).
+__global__ void refine_norms_final(int nblocks, const double* blocks, double* out) {
+  const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (k >= 5) return;
+  double t = 0.0;
+  for (int b = lane; b < nblocks; b += 32) t += blocks[b * 5 + k];
+  t = warp_sum(t);
+  if (lane == 0) out[k] = t;
 }
 
 __global__ void accumulate_kernel(int64_t n, double* dst, const double* src) {
@@ -1278,8 +1301,11 @@ extern "C" int mhm_refine_norms(int32_t cells, const double* partial, int64_t tr
                                 const double* rhs, double* out, void* stream) {
   if (cells < 1 || !partial || trace_size < 0 || (trace_size > 0 && !weak) || !out) return MHM_ERR_ARGUMENT;
   if (indptr && (size < 1 || !indices || !values || !x || !rhs)) return MHM_ERR_ARGUMENT;
-  refine_norms_kernel<<<1, 1024, 0, static_cast<cudaStream_t>(stream)>>>(
-      cells, partial, trace_size, weak, boundary, size, indptr, indices, values, x, rhs, out);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  double* blocks = out + 5;
+  refine_norms_partial<<<kNormBlocks, 256, 0, st>>>(cells, partial, trace_size, weak, boundary, size, indptr, indices,
+                                                    values, x, rhs, blocks);
+  refine_norms_final<<<1, 160, 0, st>>>(kNormBlocks, blocks, out);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
 

@@ -553,7 +553,7 @@ class CartesianQ1Plan:
             f64 = dict(dtype=torch.float64, device=self.device)
             self._refine = dict(defect=torch.empty((M, n), **f64), slots=torch.empty((M, t), **f64),
                                 weak=torch.empty(self.T, **f64), partial=torch.empty((M, 3), **f64),
-                                norms=torch.empty(5, **f64), dx=torch.empty(self.N, **f64),
+                                norms=torch.empty(5 + 5 * 256, **f64), dx=torch.empty(self.N, **f64),
                                 rhs=torch.empty(self.N, **f64), scale=torch.empty(self.N, **f64),
                                 dfields=torch.empty((M, n), **f64))
         B = self._refine
@@ -571,7 +571,7 @@ class CartesianQ1Plan:
                                           P(self.d_indptr), P(self.d_indices), P(self.values), P(self.x),
                                           P(self.rhs), P(B["norms"]), s), "mhm_refine_norms")
             cur.synchronize()
-            norms = B["norms"].cpu().numpy()
+            norms = B["norms"][:5].cpu().numpy()
             residual, rhs_norm = math.sqrt(norms[0]), math.sqrt(norms[1])
             history.append(residual)
             threshold = max(atol, rtol * rhs_norm)
