@@ -421,6 +421,11 @@ class CartesianQ1Plan:
                                          P(self.blocks), P(self.loads), P(self.corrected), P(self.cell_status),
                                          P(self.cell_iters), s), "mhm_q1_condense")
         elif local == "offline":
+            if getattr(self, "factors", None) is None:
+                nbytes = int(L.mhm_q1_factor_bytes(self.q1, prec))
+                if nbytes <= 0:
+                    raise RuntimeError("could not size the factor store")
+                self.factors = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
             _lib.check(L.mhm_q1_condense_offline(self.q1, prec, self.max_refine, self.local_tol, P(self.solution),
                                                  P(self.blocks), P(self.loads), P(self.corrected),
                                                  P(self.cell_status), P(self.cell_iters), P(self.factors), s),

@@ -201,6 +201,8 @@ class ServingEngine:
         if sum(1 for s in self.slots if s.request is not None) >= self.max_in_flight:
             return None
         need = self._shape_bytes.get(shape, 0)
+        if need > self.hbm_budget:
+            raise ValueError(f"a request of shape {shape} needs {need} device bytes, more than the HBM budget")
         while ((self.max_slots is not None and len(self.slots) >= self.max_slots)
                or self._bytes() + need > self.hbm_budget):
             idle = [s for s in self.slots if s.request is None]
@@ -209,11 +211,10 @@ class ServingEngine:
             self.slots.remove(idle[0])
         slot = _Slot(self, shape)
         self._shape_bytes[shape] = slot.bytes
+        if slot.bytes > self.hbm_budget:
+            raise ValueError(f"a request of shape {shape} needs {slot.bytes} device bytes, more than the HBM budget")
         if self._bytes() + slot.bytes > self.hbm_budget:
-            if not self.slots:
-                raise ValueError(f"a request of shape {shape} needs {slot.bytes} device bytes, "
-                                 f"more than the HBM budget")
-            return None  # first slot of this shape: measured, retried once others finish
+            return None  # first slot of this shape, now measured: idle slots make room on the next try
         self.slots.append(slot)
         self.stats["slots_created"] = self.stats.get("slots_created", 0) + 1
         self.stats["peak_bytes"] = max(self.stats.get("peak_bytes", 0), self._bytes())
@@ -273,6 +274,11 @@ class ServingEngine:
             while queue:
                 idx = queue[0]
                 slot = self._slot_for(requests[idx].shape)
+                if slot is None and not running:
+                    # nothing on the device: all slots are idle and can be released
+                    slot = self._slot_for(requests[idx].shape)
+                    if slot is None:
+                        raise RuntimeError(f"request {idx} cannot be admitted within the HBM budget")
                 if slot is None:
                     break
                 queue.popleft()

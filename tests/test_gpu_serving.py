@@ -83,3 +83,50 @@ def test_realtime_arrivals_and_latency():
     s = summarize(out)
     assert s["requests"] == 6 and s["rhs"] == sum(len(r.sources) for r in reqs)
     assert s["latency_ms"]["p99"] >= s["latency_ms"]["p50"] > 0
+
+
+def test_reserved_slots_and_eviction_under_the_budget():
+    """Reserved slots serve later requests without new plans; when the budget is full,
+    idle slots of other shapes make room for a new shape; a shape larger than the
+    whole budget is rejected."""
+    from pymhm_b200.serving import ServingEngine
+
+    reqs = make_requests(6)
+    small_reqs = [r for r in reqs if (r.macro, r.refinement) == (4, 4)]
+    big_reqs = [r for r in reqs if (r.macro, r.refinement) == (8, 4)]
+    engine = ServingEngine(max_in_flight=2, keep_fields=True)
+    assert engine.reserve((4, 4, 2), 2) == 2
+    assert engine.reserve((8, 4, 2), 1) == 1
+    created = engine.stats["slots_created"]
+    engine.run(small_reqs * 2, realtime=False)
+    assert engine.stats["slots_created"] == created
+    small, big = engine._shape_bytes[(4, 4, 2)], engine._shape_bytes[(8, 4, 2)]
+    tight = ServingEngine(max_in_flight=1, hbm_budget=big + 1.2 * small, keep_fields=True)
+    assert tight.reserve((4, 4, 2), 2) == 2
+    out = tight.run(small_reqs + big_reqs, realtime=False)
+    assert all(o is not None for o in out)
+    assert tight._bytes() <= tight.hbm_budget
+    assert any(s.shape == (8, 4, 2) for s in tight.slots)
+    with pytest.raises(ValueError, match="HBM budget"):
+        ServingEngine(hbm_budget=0.5 * big).run(big_reqs, realtime=False)
+
+
+def test_captured_offline_step_matches_eager():
+    """The offline step (factors kept) replayed from its CUDA graph gives the eager
+    launch's bits."""
+    import torch
+
+    from tests.test_gpu_darcy import make_plan
+
+    g, plan = make_plan("darcy_4x4_r16_p2_lognormal", "mixed")
+    kappa = torch.from_numpy(np.ascontiguousarray(g["kappa"])).to(plan.device)
+    plan.set_device_coefficients(1, kappa, (0.0, 0.0, 0.0), 0, None, 1.0)
+    plan.launch(local="offline")
+    plan.check()
+    eager = plan.fields.cpu().numpy().copy()
+    plan.capture("offline")
+    plan.fields.zero_()
+    st = plan.replay("offline", 1.0)
+    st.synchronize()
+    plan.check()
+    assert np.array_equal(plan.fields.cpu().numpy(), eager)
