@@ -1,7 +1,8 @@
 """Write golden fixtures for dense P1 simplex assembly by running PyMHM's own CPU
 operators, the ones the reference's GPU test compares ``assemble_p1_batch`` with
 (``tests/test_gpu_batch.py``): ``p1_operators`` on ``TriangleMesh.unit_square(3)``
-and ``tetra_operators`` (degree 1) on ``TetraMesh.unit_cube(1).submesh(0, 2)``.
+and ``tetra_operators`` (degree 1) on ``TetraMesh.unit_cube(1).submesh(0, 2)`` and on
+``submesh(0, 8)`` (165 nodes, the local mesh of the 3-D configuration).
 
     PYMHM_SRC=/path/to/pymhm/src python tests/golden/make_p1_golden.py
 
@@ -42,6 +43,10 @@ def main():
     a, m, f = tetra_operators(tetra, degree=1, diffusion=tensor, source=2.5)
     out.update(tet_points=tetra.points, tet_cells=tetra.cells, tet_tensor=tensor, tet_source=2.5,
                tet_A=a.toarray(), tet_M=m.toarray(), tet_f=f)
+    # config-4 size: one macro tetrahedron of the unit cube refined with submesh(cell, 8)
+    big = TetraMesh.unit_cube(1).submesh(0, 8)
+    a, m, f = tetra_operators(big, degree=1, diffusion=tensor, source=2.5)
+    out.update(tet8_points=big.points, tet8_cells=big.cells, tet8_A=a.toarray(), tet8_M=m.toarray(), tet8_f=f)
     np.savez_compressed(HERE / "p1_operators.npz", **out)
     print("tri", mesh.points.shape, mesh.cells.shape, "tet", tetra.points.shape, tetra.cells.shape)
 

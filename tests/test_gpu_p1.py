@@ -80,6 +80,24 @@ def test_matches_reference_operators(kind):
         np.testing.assert_allclose(f[b], g[f"{kind}_f"], atol=1e-14)
 
 
+def test_config4_local_mesh_matches_reference():
+    """One macro tetrahedron refined with submesh(cell, 8) (165 P1 nodes, the local mesh
+    of the 3-D configuration): 32 affinely mapped copies, each against the reference's
+    operators mapped the same way (stiffness and mass scale with the map)."""
+    g = load("p1_operators")
+    pts, cells = g["tet8_points"], g["tet8_cells"]
+    rng = np.random.default_rng(8)
+    scales = rng.uniform(0.5, 2.0, 32)
+    shifts = rng.normal(size=(32, 3))
+    coords = np.stack([s * pts + t for s, t in zip(scales, shifts)])
+    a, m, f = gpu(coords, cells, diffusion=g["tet_tensor"], source=float(g["tet_source"]))
+    for b, sc in enumerate(scales):
+        # uniform scaling by sc: stiffness * sc, mass * sc^3, load * sc^3 in three dimensions
+        np.testing.assert_allclose(a[b], sc * g["tet8_A"], atol=1e-12 * sc * np.abs(g["tet8_A"]).max())
+        np.testing.assert_allclose(m[b], sc**3 * g["tet8_M"], atol=1e-14 * sc**3 * np.abs(g["tet8_M"]).max() + 1e-300)
+        np.testing.assert_allclose(f[b], sc**3 * g["tet8_f"], atol=1e-13 * sc**3 * np.abs(g["tet8_f"]).max())
+
+
 @pytest.mark.parametrize("dimension", [2, 3])
 def test_simplex_moments(dimension):
     points = np.vstack((np.zeros(dimension), np.eye(dimension)))

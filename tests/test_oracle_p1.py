@@ -10,12 +10,13 @@ from oracle.p1_batch import assemble_p1_batch
 from tests._cases import load
 
 
-@pytest.mark.parametrize("kind", ["tri", "tet"])
+@pytest.mark.parametrize("kind", ["tri", "tet", "tet8"])
 def test_oracle_matches_reference_operators(kind):
     g = load("p1_operators")
     pts = np.stack([g[f"{kind}_points"]] * 2)
-    a, m, f = assemble_p1_batch(pts, g[f"{kind}_cells"], diffusion=g[f"{kind}_tensor"],
-                                source=float(g[f"{kind}_source"]))
+    coef = "tet" if kind == "tet8" else kind
+    a, m, f = assemble_p1_batch(pts, g[f"{kind}_cells"], diffusion=g[f"{coef}_tensor"],
+                                source=float(g[f"{coef}_source"]))
     for b in range(2):
         np.testing.assert_allclose(a[b], g[f"{kind}_A"], atol=1e-13)
         np.testing.assert_allclose(m[b], g[f"{kind}_M"], atol=1e-14)
