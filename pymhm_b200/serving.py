@@ -135,6 +135,14 @@ class _Slot:
             self.done.record(st)
 
     def collect(self, admitted, finished, keep_fields) -> DarcyResult:
+        """The finished request's results; the slot is free again afterwards, also
+        when a status check raises."""
+        try:
+            return self._collect(admitted, finished, keep_fields)
+        finally:
+            self.request = None
+
+    def _collect(self, admitted, finished, keep_fields) -> DarcyResult:
         from . import _lib
 
         index, request = self.request
@@ -156,7 +164,6 @@ class _Slot:
             if keep_fields:
                 fields.append(self.fields_host[k].numpy().copy())
                 flux.append(self.flux_host[k].numpy().copy())
-        self.request = None
         return DarcyResult(index, xs, fields, flux, request.arrival, admitted, finished, iters)
 
 
@@ -166,8 +173,8 @@ class ServingEngine:
     ``hbm_budget`` bounds the device bytes of all slots together (plans, kept factors,
     permeability buffers); ``max_in_flight`` bounds the requests on the device at
     once; idle slots stay resident for later requests of their shape until the budget
-    (or ``max_slots``, if given) needs their room.  ``keep_fields`` also returns every source's fields and fluxes (pinned
-    buffers of that size per slot and source).
+    (or ``max_slots``, if given) needs their room.  ``keep_fields`` also returns every
+    source's fields and fluxes (pinned buffers of that size per slot and source).
     """
 
     def __init__(self, *, precision="mixed", hbm_budget=150e9, max_in_flight=8, max_slots=None, keep_fields=False,
