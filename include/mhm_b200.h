@@ -15,6 +15,9 @@
  *                          (core/condensation.py:21-122) + local_global_
  *                          contribution (core/contributions.py:14-74) for all
  *                          macrocells of a Cartesian Q1 problem at once.
+ *                          With kappa_mode 3/4 its assembly follows the
+ *                          cut-cell branch of quadrilateral_operators
+ *                          (fem/scalar/quadrilateral.py:136-188, 215-234).
  *   mhm_skeleton_scatter   replaces assemble_hybrid_contributions
  *                          (core/contributions.py:77-195) and the Numba
  *                          leaves core/_assembly.py:10-42.
@@ -96,8 +99,13 @@ typedef struct mhm_q1_problem {
     const int8_t* side_sign;      /* (cells, 4): +-1, sides bottom,right,top,left */
     const int8_t* side_orient;    /* (cells, 4): 0/1 as in coupling_table          */
     int32_t kappa_mode;           /* 0 constant, 1 isotropic per fine cell,
-                                     2 (kxx,kxy,kyy) per fine cell                */
-    const double* kappa;          /* global fine grid, [gx][gy][comp] (x-major)    */
+                                     2 (kxx,kxy,kyy) per fine cell,
+                                     3 isotropic per pixel, 4 (kxx,kxy,kyy) per
+                                     pixel: a pixel field whose lines may cut the
+                                     fine cells, integrated exactly on each
+                                     intersection (quadrilateral.py:136-188)       */
+    const double* kappa;          /* modes 1/2: global fine grid [gx][gy][comp];
+                                     modes 3/4: pixels [px][py][comp] (x-major)    */
     double kappa_const[3];        /* kxx, kxy, kyy for kappa_mode 0                */
     int32_t source_mode;          /* 0 constant, 1 per fine cell,
                                      2 per Gauss point of the fine cell,
@@ -106,6 +114,14 @@ typedef struct mhm_q1_problem {
                                      mode 3: [cell][node], node = iy*(rx+1)+ix     */
     double source_const;
     int32_t quad_order;           /* Gauss points per axis for source_mode 2      */
+    double pixel_origin[2];       /* kappa_mode 3/4: lower-left corner of pixel 0  */
+    double pixel_spacing[2];      /* kappa_mode 3/4: pixel widths                 */
+    int32_t pixel_nx, pixel_ny;   /* kappa_mode 3/4: pixel counts; the field must
+                                     cover the domain                              */
+    double* cut_elements;         /* kappa_mode 3/4: device work buffer of
+                                     (global fine cells) x 16 doubles, [gx][gy][4x4];
+                                     every local entry point first writes each fine
+                                     cell's element stiffness there               */
 } mhm_q1_problem;
 
 /* Width of the per-cell right-hand side block: 1 source + trace + 1 retained. */

@@ -277,10 +277,13 @@ def _neumaier(total, corr, value):
 def diffusion_blocks(weights, gradients, tensors, measure):
     """``diffusion_blocks`` (``_integration.py:43-88``), vectorised over cells.
 
-    Shapes: weights (q,), gradients (q,4,2), tensors (cells,q,2,2), measure scalar.
+    Shapes: weights (q,) or per cell (cells,q), gradients (q,4,2) or (cells,q,4,2),
+    tensors (cells,q,2,2), measure scalar.
     """
     cells, count = tensors.shape[:2]
-    width, dim = gradients.shape[1:]
+    weights = np.broadcast_to(weights, (cells, count))
+    gradients = np.broadcast_to(gradients, (cells, *gradients.shape[-3:]))
+    width, dim = gradients.shape[2:]
     transformed = np.empty((cells, count, width, dim))
     for q in range(count):
         for j in range(width):
@@ -288,7 +291,7 @@ def diffusion_blocks(weights, gradients, tensors, measure):
                 t = np.zeros(cells)
                 c = np.zeros(cells)
                 for b in range(dim):
-                    t, c = _neumaier(t, c, tensors[:, q, a, b] * gradients[q, j, b])
+                    t, c = _neumaier(t, c, tensors[:, q, a, b] * gradients[:, q, j, b])
                 transformed[:, q, j, a] = t + c
     result = np.empty((cells, width, width))
     for i in range(width):
@@ -299,8 +302,8 @@ def diffusion_blocks(weights, gradients, tensors, measure):
                 s = np.zeros(cells)
                 sc = np.zeros(cells)
                 for a in range(dim):
-                    s, sc = _neumaier(s, sc, gradients[q, i, a] * transformed[:, q, j, a])
-                t, c = _neumaier(t, c, (s + sc) * weights[q] * measure)
+                    s, sc = _neumaier(s, sc, gradients[:, q, i, a] * transformed[:, q, j, a])
+                t, c = _neumaier(t, c, (s + sc) * weights[:, q] * measure)
             result[:, i, j] = t + c
     return result
 
@@ -341,17 +344,83 @@ class PixelField:
         return self.values[idx[:, 0], idx[:, 1]]
 
 
+def grid_resolves_material(fine, field):
+    """``grid_resolves_material`` (``quadrilateral.py:116-132``): every pixel line lies on a
+    fine-grid line (pixel spacing an integer multiple of the fine spacing, origin offset
+    an integer number of fine cells), to 64 eps of the compared values."""
+    spacing = np.asarray(fine.spacing, dtype=float)
+    intervals = np.asarray(field.spacing, dtype=float) / spacing
+    bounds = np.asarray(fine.bounds, dtype=float)
+    offsets = (bounds[[0, 2]] - np.asarray(field.origin, dtype=float)) / spacing
+    values = np.r_[intervals, offsets]
+    tolerance = 64 * EPS * max(1.0, float(np.max(np.abs(values))))
+    return bool(np.all(np.abs(values - np.rint(values)) <= tolerance))
+
+
+def rectangle_intersection_quadrature(origins, spacing, field, order):
+    """``rectangle_intersection_quadrature`` (``quadrilateral.py:136-188``): per fine cell,
+    tensor Gauss rules on its exact intersections with the pixels, in the cell's
+    reference coordinates; zero-weight padding to a common point count."""
+    pixel_spacing = np.asarray(field.spacing, dtype=float)
+    pixel_origin = np.asarray(field.origin, dtype=float)
+    shape = np.asarray(field.values.shape[:2])
+    lower = (origins - pixel_origin) / pixel_spacing
+    upper = (origins + spacing - pixel_origin) / pixel_spacing
+    tolerance = 64 * EPS * shape
+    if np.any(lower < -tolerance) or np.any(upper > shape + tolerance):
+        raise ValueError("a fine rectangle lies outside the Cartesian material field")
+    lower = np.where(np.isclose(lower, np.rint(lower), rtol=0, atol=tolerance), np.rint(lower), lower)
+    upper = np.where(np.isclose(upper, np.rint(upper), rtol=0, atol=tolerance), np.rint(upper), upper)
+    first = np.floor(lower).astype(int)
+    last = np.ceil(upper).astype(int) - 1
+    parts = np.max(last - first + 1, axis=0)
+    gauss, weights = leggauss(order)
+    gauss, weights = (gauss + 1) / 2, weights / 2
+    axes, axis_weights = [], []
+    for axis in range(2):
+        indices = first[:, axis, None] + np.arange(parts[axis])
+        physical_lo = pixel_origin[axis] + indices * pixel_spacing[axis]
+        physical_hi = pixel_origin[axis] + (indices + 1) * pixel_spacing[axis]
+        end = origins[:, axis, None] + spacing[axis]
+        lo = np.minimum(np.maximum(physical_lo, origins[:, axis, None]), end)
+        hi = np.maximum(np.minimum(physical_hi, end), lo)
+        a = (lo - origins[:, axis, None]) / spacing[axis]
+        width = (hi - lo) / spacing[axis]
+        axes.append(a[..., None] + width[..., None] * gauss)
+        axis_weights.append(width[..., None] * weights)
+    count = len(origins)
+    x = np.broadcast_to(axes[0][:, None, None, :, :], (count, parts[1], order, parts[0], order))
+    y = np.broadcast_to(axes[1][:, :, :, None, None], x.shape)
+    combined = axis_weights[1][:, :, :, None, None] * axis_weights[0][:, None, None, :, :]
+    reference = np.stack((x, y), axis=-1).reshape(count, -1, 2)
+    return np.clip(reference, 0, 1), combined.reshape(count, -1)
+
+
 def q1_operators(fine, permeability=1.0, source=0.0, order=4):
-    """``quadrilateral_operators`` grid-aligned branch (``quadrilateral.py:191-253``)."""
+    """``quadrilateral_operators`` (``quadrilateral.py:191-253``): the uniform rule, or the
+    cut rule when the pixel lines of a ``PixelField`` cross the fine cells."""
     reference, weights = quadrature(order)
     dofs, nodes = q1_space(fine)
     basis, gradient = q1_basis(reference)
     gradient = gradient / fine.spacing
     area = float(np.prod(fine.spacing))
     n = len(nodes)
+    cuts = isinstance(permeability, PixelField) and not grid_resolves_material(fine, permeability)
     blocks, loads = [], []
     for begin in range(0, len(fine.cells), 256):
         origins = fine.points[fine.cells[begin: begin + 256, 0]]
+        if cuts:
+            cref, cw = rectangle_intersection_quadrature(origins, np.asarray(fine.spacing, float), permeability,
+                                                         order)
+            cb, cg = q1_basis(cref.reshape(-1, 2))
+            cb = cb.reshape(len(origins), -1, 4)
+            cg = cg.reshape(len(origins), -1, 4, 2) / fine.spacing
+            pts = origins[:, None, :] + cref * fine.spacing
+            tensors = tensor_at(permeability, pts.reshape(-1, 2)).reshape(len(origins), -1, 2, 2)
+            force = scalar_at(source, pts.reshape(-1, 2)).reshape(len(origins), -1)
+            blocks.append(diffusion_blocks(cw, cg, tensors, area))
+            loads.append(area * np.einsum("tq,tqi,tq->ti", cw, cb, force))
+            continue
         pts = origins[:, None, :] + reference[None, :, :] * fine.spacing
         tensors = tensor_at(permeability, pts.reshape(-1, 2)).reshape(len(origins), len(weights), 2, 2)
         force = scalar_at(source, pts.reshape(-1, 2)).reshape(len(origins), len(weights))

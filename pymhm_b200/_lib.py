@@ -53,6 +53,8 @@ class Q1Problem(C.Structure):
         ("kappa_mode", C.c_int32), ("kappa", C.c_void_p), ("kappa_const", C.c_double * 3),
         ("source_mode", C.c_int32), ("source", C.c_void_p), ("source_const", C.c_double),
         ("quad_order", C.c_int32),
+        ("pixel_origin", C.c_double * 2), ("pixel_spacing", C.c_double * 2),
+        ("pixel_nx", C.c_int32), ("pixel_ny", C.c_int32), ("cut_elements", C.c_void_p),
     ]
 
 

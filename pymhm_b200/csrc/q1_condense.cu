@@ -49,6 +49,14 @@ struct Q1Args {
   int kmode;
   const double* kappa;
   double k0, k1, k2;
+  // kmode 3/4: pixel field [px][py][comp] whose lines may cut the fine cells; a
+  // pre-pass writes every fine cell's 4x4 element matrix to cut ([gx][gy][16]),
+  // which the node gather reads in place of the per-element tensor (cut_mode)
+  bool cut_mode;
+  double x0, y0;
+  double px0, py0, psx, psy;
+  int pnx, pny;
+  double* cut;
   int smode;
   const double* src;
   double s0;
@@ -86,6 +94,107 @@ __device__ __forceinline__ double elem_k(double kxx, double kxy, double kyy, dou
     v += kxy * (dax * dcy + dcx * day);
   }
   return v;
+}
+
+// Pixel columns [first, last] that the interval [lo, lo + h) overlaps, in the
+// reference's snapped pixel coordinates (quadrilateral.py:152-170): a coordinate
+// within 64 eps * count of an integer is that integer.  Clamped to the field.
+__device__ __forceinline__ void pixel_span(double lo, double h, double origin, double spacing, int count,
+                                           int& first, int& last) {
+  const double tol = 64.0 * 2.220446049250313e-16 * count;
+  double u0 = (lo - origin) / spacing, u1 = (lo + h - origin) / spacing;
+  const double r0 = rint(u0), r1 = rint(u1);
+  if (fabs(u0 - r0) <= tol) u0 = r0;
+  if (fabs(u1 - r1) <= tol) u1 = r1;
+  first = (int)floor(u0);
+  last = (int)ceil(u1) - 1;
+  if (first < 0) first = 0;
+  if (last > count - 1) last = count - 1;
+}
+
+// Reference-coordinate segment of pixel column i inside [lo, lo + h]: midpoint m
+// and width w (both in units of h), as rectangle_intersection_quadrature clips it.
+__device__ __forceinline__ void pixel_segment(double lo, double h, double origin, double spacing, int i,
+                                              double& m, double& w) {
+  const double end = lo + h;
+  const double plo = fmin(fmax(origin + i * spacing, lo), end);
+  const double phi = fmax(fmin(origin + (i + 1) * spacing, end), plo);
+  const double a = fmin(fmax((plo - lo) / h, 0.0), 1.0);
+  w = fmin((phi - plo) / h, 1.0 - a);
+  m = a + 0.5 * w;
+}
+
+// Element matrix of a fine cell cut by pixel lines (kappa_mode 3/4): the sum over
+// its pixel intersections [a,b] x [c,d] (reference coordinates) of the exact Q1
+// integrals with that pixel's constant tensor.  With X_0 = 1 - xi, X_1 = xi,
+// slopes s_0 = -1, s_1 = 1, midpoints m and widths w, every product of two linear
+// factors integrates exactly as w (f(m) g(m) + f' g' w^2 / 12):
+//   K_ac += kxx (hy/hx) s_ax s_cx wx IY(ay,cy) + kyy (hx/hy) s_ay s_cy wy IX(ax,cx)
+//         + kxy (s_ax s_cy JX(cx) JY(ay) + s_ay s_cx JX(ax) JY(cy)),
+// IX(i,j) = wx (X_i X_j (mx) + s_i s_j wx^2/12), JX(i) = wx X_i(mx), likewise in y.
+// This is the reference's per-intersection Gauss sum (exact for these integrands)
+// up to rounding (quadrilateral.py:215-234).
+__device__ void cut_element(const Q1Args& a, double ex0, double ey0, double* km) {
+  const double rxy = a.hy / a.hx, ryx = a.hx / a.hy;
+  for (int q = 0; q < 16; ++q) km[q] = 0.0;
+  int fx, lx, fy, ly;
+  pixel_span(ex0, a.hx, a.px0, a.psx, a.pnx, fx, lx);
+  pixel_span(ey0, a.hy, a.py0, a.psy, a.pny, fy, ly);
+  for (int iy = fy; iy <= ly; ++iy) {
+    double my, wy;
+    pixel_segment(ey0, a.hy, a.py0, a.psy, iy, my, wy);
+    if (!(wy > 0.0)) continue;
+    const double Y[2] = {1.0 - my, my};
+    for (int ix = fx; ix <= lx; ++ix) {
+      double mx, wx;
+      pixel_segment(ex0, a.hx, a.px0, a.psx, ix, mx, wx);
+      if (!(wx > 0.0)) continue;
+      const double X[2] = {1.0 - mx, mx};
+      const size_t g = (size_t)ix * a.pny + iy;
+      double kxx, kxy, kyy;
+      if (a.kmode == 3) {
+        kxx = kyy = a.kappa[g]; kxy = 0.0;
+      } else {
+        kxx = a.kappa[3 * g]; kxy = a.kappa[3 * g + 1]; kyy = a.kappa[3 * g + 2];
+      }
+      const double cx2 = wx * wx / 12.0, cy2 = wy * wy / 12.0;
+      for (int A = 0; A < 4; ++A) {
+        const int ax = A & 1, ay = A >> 1;
+        const double sax = ax ? 1.0 : -1.0, say = ay ? 1.0 : -1.0;
+        for (int Cc = 0; Cc < 4; ++Cc) {
+          const int cx = Cc & 1, cy = Cc >> 1;
+          const double scx = cx ? 1.0 : -1.0, scy = cy ? 1.0 : -1.0;
+          const double iy2 = wy * (Y[ay] * Y[cy] + say * scy * cy2);
+          const double ix2 = wx * (X[ax] * X[cx] + sax * scx * cx2);
+          double v = kxx * rxy * (sax * scx) * wx * iy2 + kyy * ryx * (say * scy) * wy * ix2;
+          if (kxy != 0.0)
+            v += kxy * (sax * scy * (wx * X[cx]) * (wy * Y[ay]) + say * scx * (wx * X[ax]) * (wy * Y[cy]));
+          km[A * 4 + Cc] += v;
+        }
+      }
+    }
+  }
+}
+
+// Pre-pass of the cut-cell modes: thread per global fine cell g = gx * NYf + gy.
+__global__ void __launch_bounds__(256) cut_element_kernel(const Q1Args a) {
+  const int64_t total = (int64_t)a.nx * a.rx * a.NYf;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const int gx = (int)(g / a.NYf), gy = (int)(g - (int64_t)gx * a.NYf);
+    double km[16];
+    cut_element(a, a.x0 + (double)gx * a.hx, a.y0 + (double)gy * a.hy, km);
+    double* out = a.cut + 16 * g;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) out[q] = km[q];
+  }
+}
+
+// Entry (r, c) of an element stiffness: k is the element's 4x4 cut-cell matrix from
+// the pre-pass (cut) or its tensor (kxx, kxy, kyy) for the closed form.
+__device__ __forceinline__ double elem_entry(bool cut, const double* k, double rxy, double ryx, int r, int c) {
+  if (cut) return __ldg(k + 4 * r + c);
+  return elem_k(k[0], k[1], k[2], rxy, ryx, r, c);
 }
 
 struct Side {
@@ -401,15 +510,17 @@ __device__ __forceinline__ void assemble_cell(const Q1Args& a, int cell, double*
   for (int e = tid; e < ne; e += blockDim.x) {
     const int ex = e % a.rx, ey = e / a.rx;
     const size_t g = (size_t)(cx * a.rx + ex) * a.NYf + (cy * a.ry + ey);
-    double kxx, kxy, kyy;
-    if (a.kmode == 0) {
-      kxx = a.k0; kxy = a.k1; kyy = a.k2;
-    } else if (a.kmode == 1) {
-      kxx = kyy = a.kappa[g]; kxy = 0.0;
-    } else {
-      kxx = a.kappa[3 * g]; kxy = a.kappa[3 * g + 1]; kyy = a.kappa[3 * g + 2];
+    if (!a.cut_mode) {
+      double kxx, kxy, kyy;
+      if (a.kmode == 0) {
+        kxx = a.k0; kxy = a.k1; kyy = a.k2;
+      } else if (a.kmode == 1) {
+        kxx = kyy = a.kappa[g]; kxy = 0.0;
+      } else {
+        kxx = a.kappa[3 * g]; kxy = a.kappa[3 * g + 1]; kyy = a.kappa[3 * g + 2];
+      }
+      kel[3 * e] = kxx; kel[3 * e + 1] = kxy; kel[3 * e + 2] = kyy;
     }
-    kel[3 * e] = kxx; kel[3 * e + 1] = kxy; kel[3 * e + 2] = kyy;
     double fe[4];
     if (a.smode == 3) {
       fe[0] = fe[1] = fe[2] = fe[3] = 0.0;  // nodal loads are given, see the gather
@@ -457,37 +568,39 @@ __device__ __forceinline__ void assemble_cell(const Q1Args& a, int cell, double*
     // candidate elements: E00 (ix-1,iy-1) local 3; E10 (ix,iy-1) local 2;
     //                     E01 (ix-1,iy) local 1;   E11 (ix,iy) local 0
     const bool l = ix > 0, r = ix < a.rx, d = iy > 0, u = iy < a.ry;
+    // global fine cell above-right of the node (element E11); used in cut mode only
+    const size_t g11 = (size_t)(cx * a.rx + ix) * a.NYf + (cy * a.ry + iy);
     if (l && d) {
       const int e = (iy - 1) * a.rx + ix - 1;
-      const double* k = kel + 3 * e;
-      sv[0] += elem_k(k[0], k[1], k[2], rxy, ryx, 3, 3);
-      sv[1] += elem_k(k[0], k[1], k[2], rxy, ryx, 3, 2);
-      sv[3] += elem_k(k[0], k[1], k[2], rxy, ryx, 3, 1);
-      sv[4] += elem_k(k[0], k[1], k[2], rxy, ryx, 3, 0);
+      const double* k = a.cut_mode ? a.cut + 16 * (g11 - a.NYf - 1) : kel + 3 * e;
+      sv[0] += elem_entry(a.cut_mode, k, rxy, ryx, 3, 3);
+      sv[1] += elem_entry(a.cut_mode, k, rxy, ryx, 3, 2);
+      sv[3] += elem_entry(a.cut_mode, k, rxy, ryx, 3, 1);
+      sv[4] += elem_entry(a.cut_mode, k, rxy, ryx, 3, 0);
       f += fel[4 * e + 3];
       ++count;
     }
     if (r && d) {
       const int e = (iy - 1) * a.rx + ix;
-      const double* k = kel + 3 * e;
-      sv[0] += elem_k(k[0], k[1], k[2], rxy, ryx, 2, 2);
-      sv[2] += elem_k(k[0], k[1], k[2], rxy, ryx, 2, 1);
-      sv[3] += elem_k(k[0], k[1], k[2], rxy, ryx, 2, 0);
+      const double* k = a.cut_mode ? a.cut + 16 * (g11 - 1) : kel + 3 * e;
+      sv[0] += elem_entry(a.cut_mode, k, rxy, ryx, 2, 2);
+      sv[2] += elem_entry(a.cut_mode, k, rxy, ryx, 2, 1);
+      sv[3] += elem_entry(a.cut_mode, k, rxy, ryx, 2, 0);
       f += fel[4 * e + 2];
       ++count;
     }
     if (l && u) {
       const int e = iy * a.rx + ix - 1;
-      const double* k = kel + 3 * e;
-      sv[0] += elem_k(k[0], k[1], k[2], rxy, ryx, 1, 1);
-      sv[1] += elem_k(k[0], k[1], k[2], rxy, ryx, 1, 0);
+      const double* k = a.cut_mode ? a.cut + 16 * (g11 - a.NYf) : kel + 3 * e;
+      sv[0] += elem_entry(a.cut_mode, k, rxy, ryx, 1, 1);
+      sv[1] += elem_entry(a.cut_mode, k, rxy, ryx, 1, 0);
       f += fel[4 * e + 1];
       ++count;
     }
     if (r && u) {
       const int e = iy * a.rx + ix;
-      const double* k = kel + 3 * e;
-      sv[0] += elem_k(k[0], k[1], k[2], rxy, ryx, 0, 0);
+      const double* k = a.cut_mode ? a.cut + 16 * (g11) : kel + 3 * e;
+      sv[0] += elem_entry(a.cut_mode, k, rxy, ryx, 0, 0);
       f += fel[4 * e + 0];
       ++count;
     }
@@ -862,6 +975,22 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
   }
 }
 
+// Pixel that holds the centre of global fine cell (gx, gy): points on a pixel line
+// (to 4 eps of the coordinate) take the pixel on the positive side, clipped at the
+// field's upper edge (materials/cartesian.py:40-72).
+__device__ __forceinline__ size_t centre_pixel(const Q1Args& a, int gx, int gy) {
+  const double eps = 2.220446049250313e-16;
+  double u = ((a.x0 + (double)gx * a.hx + 0.5 * a.hx) - a.px0) / a.psx;
+  double v = ((a.y0 + (double)gy * a.hy + 0.5 * a.hy) - a.py0) / a.psy;
+  const double ru = rint(u), rv = rint(v);
+  if (fabs(u - ru) <= 4.0 * eps * fmax(1.0, fabs(u))) u = ru;
+  if (fabs(v - rv) <= 4.0 * eps * fmax(1.0, fabs(v))) v = rv;
+  int ix = (int)fmax(u, 0.0), iy = (int)fmax(v, 0.0);
+  if (ix > a.pnx - 1) ix = a.pnx - 1;
+  if (iy > a.pny - 1) iy = a.pny - 1;
+  return (size_t)ix * a.pny + iy;
+}
+
 // Flux -K grad u at the fine-cell centres of one macrocell from its nodal values u
 // (shared memory), postprocessing/solutions.py:278-324.
 __device__ __forceinline__ void cell_flux(const Q1Args& a, int cell, const double* u, double* flux) {
@@ -874,11 +1003,12 @@ __device__ __forceinline__ void cell_flux(const Q1Args& a, int cell, const doubl
     const double u0 = u[n0], u1 = u[n0 + 1], u2 = u[n0 + a.nnx], u3 = u[n0 + a.nnx + 1];
     const double gx = (-u0 + u1 - u2 + u3) * (0.5 / a.hx);
     const double gy = (-u0 - u1 + u2 + u3) * (0.5 / a.hy);
-    const size_t g = (size_t)(cx * a.rx + ex) * a.NYf + (cy * a.ry + ey);
+    size_t g = (size_t)(cx * a.rx + ex) * a.NYf + (cy * a.ry + ey);
+    if (a.cut_mode) g = centre_pixel(a, cx * a.rx + ex, cy * a.ry + ey);
     double kxx, kxy, kyy;
     if (a.kmode == 0) {
       kxx = a.k0; kxy = a.k1; kyy = a.k2;
-    } else if (a.kmode == 1) {
+    } else if (a.kmode == 1 || a.kmode == 3) {
       kxx = kyy = a.kappa[g]; kxy = 0.0;
     } else {
       kxx = a.kappa[3 * g]; kxy = a.kappa[3 * g + 1]; kyy = a.kappa[3 * g + 2];
@@ -1109,7 +1239,11 @@ void gauss01(int m, double* x, double* wts) {
 int fill_args(const mhm_q1_problem* p, int precision, Q1Args& a) {
   if (!p || p->macro_nx < 1 || p->macro_ny < 1 || p->rx < 1 || p->ry < 1) return MHM_ERR_ARGUMENT;
   if (!(p->hx > 0) || !(p->hy > 0) || p->tf_h < 1 || p->tf_v < 1) return MHM_ERR_ARGUMENT;
-  if (p->kappa_mode < 0 || p->kappa_mode > 2 || p->source_mode < 0 || p->source_mode > 3)
+  if (p->kappa_mode < 0 || p->kappa_mode > 4 || p->source_mode < 0 || p->source_mode > 3)
+    return MHM_ERR_ARGUMENT;
+  if (p->kappa_mode >= 3 &&
+      (p->pixel_nx < 1 || p->pixel_ny < 1 || !(p->pixel_spacing[0] > 0) || !(p->pixel_spacing[1] > 0) ||
+       !std::isfinite(p->pixel_origin[0]) || !std::isfinite(p->pixel_origin[1]) || !p->cut_elements))
     return MHM_ERR_ARGUMENT;
   if ((p->kappa_mode && !p->kappa) || (p->source_mode && !p->source)) return MHM_ERR_ARGUMENT;
   if (p->source_mode == 2 && (p->quad_order < 1 || p->quad_order > kMaxQuad)) return MHM_ERR_ARGUMENT;
@@ -1126,6 +1260,14 @@ int fill_args(const mhm_q1_problem* p, int precision, Q1Args& a) {
   a.table = p->coupling_table; a.sign = p->side_sign; a.orient = p->side_orient;
   a.kmode = p->kappa_mode; a.kappa = p->kappa;
   a.k0 = p->kappa_const[0]; a.k1 = p->kappa_const[1]; a.k2 = p->kappa_const[2];
+  a.cut_mode = a.kmode >= 3;
+  a.x0 = p->x0; a.y0 = p->y0;
+  if (a.kmode >= 3) {
+    a.px0 = p->pixel_origin[0]; a.py0 = p->pixel_origin[1];
+    a.psx = p->pixel_spacing[0]; a.psy = p->pixel_spacing[1];
+    a.pnx = p->pixel_nx; a.pny = p->pixel_ny;
+    a.cut = p->cut_elements;
+  }
   a.smode = p->source_mode; a.src = p->source; a.s0 = p->source_const;
   a.qorder = p->quad_order > 0 ? p->quad_order : 1;
   gauss01(a.qorder, a.gpt, a.gwt);
@@ -1187,6 +1329,15 @@ extern "C" int64_t mhm_q1_condense_smem_bytes(const mhm_q1_problem* p, int32_t p
 }
 
 namespace {
+// Cut-cell modes: fill the element-matrix buffer before a local kernel reads it.
+void launch_cut_elements(const Q1Args& a, cudaStream_t s) {
+  if (!a.cut_mode) return;
+  const int64_t total = (int64_t)a.nx * a.rx * a.NYf;
+  int64_t grid = (total + 255) / 256;
+  if (grid > 148 * 16) grid = 148 * 16;
+  cut_element_kernel<<<(int)grid, 256, 0, s>>>(a);
+}
+
 int run_condense(const mhm_q1_problem* p, int32_t precision, int32_t max_refine, double tol, double* solution,
                  double* blocks, double* loads, uint8_t* corrected, int32_t* cell_status, int32_t* cell_iters,
                  int mode, void* factors, void* stream) {
@@ -1204,6 +1355,7 @@ int run_condense(const mhm_q1_problem* p, int32_t precision, int32_t max_refine,
   a.mode = mode; a.factors = factors;
   const int cells = a.nx * a.ny;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  launch_cut_elements(a, s);
   const int rc2 = precision == MHM_PRECISION_FP64 ? launch_condense<double>(a, cells, s)
                                                   : launch_condense<float>(a, cells, s);
   if (rc2 != MHM_OK) return rc2;
@@ -1288,6 +1440,7 @@ extern "C" int mhm_q1_original_defect(const mhm_q1_problem* p, const int64_t* ce
           cudaSuccess)
     return MHM_ERR_LAUNCH;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  launch_cut_elements(a, st);
   q1_defect_kernel<<<a.nx * a.ny, kThreads, smem, st>>>(a, cell_dofs, x, fields, defect, slot_terms, partial);
   int blocks = (int)((trace_size + 255) / 256);
   if (blocks > 4096) blocks = 4096;

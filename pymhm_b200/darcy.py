@@ -110,15 +110,52 @@ def _tensor_components(values: np.ndarray) -> tuple[int, np.ndarray]:
     raise ValueError("fine-cell permeability must have shape (nx, ny) or (nx, ny, 2, 2)")
 
 
-def permeability_input(permeability, mesh: CartesianMacroMesh, rx: int, ry: int, order: int):
-    """Map a permeability description to (mode, fine-grid array | None, constant triple).
+def _pixel_origin(field) -> np.ndarray:
+    origin = getattr(field, "origin", None)
+    return np.zeros(2) if origin is None else np.asarray(origin, dtype=float)
 
-    Accepted: a positive scalar or constant 2x2 tensor; a grid-aligned pixel field
-    with ``values``, ``spacing`` and ``origin`` (``materials/cartesian.py``), whose
-    lines coincide with fine-grid lines; an array of fine-cell values; or a
-    callable that is constant on every fine cell at the Gauss points.  Material
-    lines crossing fine cells need the reference's cut quadrature
-    (``quadrilateral.py:136-188``), which this path does not implement.
+
+def grid_resolves_material(field, mesh: CartesianMacroMesh, rx: int, ry: int) -> bool:
+    """Every pixel line of ``field`` lies on a fine-grid line (``grid_resolves_material``,
+    ``quadrilateral.py:116-132``): the pixel spacing is a whole number of fine cells and
+    the pixel origin sits a whole number of fine cells from the domain corner, each to
+    64 eps of the compared value."""
+    fhx, fhy, _, _, x0, y0 = fine_grid(mesh, rx, ry)
+    spacing = np.asarray(field.spacing, dtype=float)
+    if spacing.shape != (2,):
+        raise ValueError("quadrilateral material integration requires a two-dimensional field")
+    fine = np.array([fhx, fhy])
+    values = np.r_[spacing / fine, (np.array([x0, y0]) - _pixel_origin(field)) / fine]
+    tolerance = 64 * np.finfo(float).eps * max(1.0, float(np.max(np.abs(values))))
+    return bool(np.all(np.abs(values - np.rint(values)) <= tolerance))
+
+
+def pixel_geometry(field, mesh: CartesianMacroMesh, rx: int, ry: int):
+    """(origin, spacing, counts) of a pixel field whose lines cut the fine cells, after
+    the reference's coverage check (``quadrilateral.py:149-158``)."""
+    fhx, fhy, nxf, nyf, x0, y0 = fine_grid(mesh, rx, ry)
+    origin, spacing = _pixel_origin(field), np.asarray(field.spacing, dtype=float)
+    if not (np.all(np.isfinite(origin)) and np.all(np.isfinite(spacing)) and np.all(spacing > 0)):
+        raise ValueError("material field spacing must be positive and its origin finite")
+    shape = np.asarray(np.shape(field.values)[:2])
+    lower = (np.array([x0, y0]) - origin) / spacing
+    upper = (np.array([x0 + nxf * fhx, y0 + nyf * fhy]) - origin) / spacing
+    tolerance = 64 * np.finfo(float).eps * shape
+    if np.any(lower < -tolerance) or np.any(upper > shape + tolerance):
+        raise ValueError("a fine rectangle lies outside the Cartesian material field")
+    return (float(origin[0]), float(origin[1])), (float(spacing[0]), float(spacing[1])), (int(shape[0]), int(shape[1]))
+
+
+def permeability_input(permeability, mesh: CartesianMacroMesh, rx: int, ry: int, order: int):
+    """Map a permeability description to (mode, array | None, constant triple).
+
+    Accepted: a positive scalar or constant 2x2 tensor; a pixel field with
+    ``values``, ``spacing`` and ``origin`` (``materials/cartesian.py``); an array of
+    fine-cell values; or a callable that is constant on every fine cell at the Gauss
+    points.  A pixel field whose lines coincide with fine-grid lines is sampled per
+    fine cell (modes 1/2); one whose lines cut the fine cells is passed as pixels
+    (modes 3/4, geometry from ``pixel_geometry``) and integrated on each fine cell's
+    exact pixel intersections, as ``quadrilateral.py:136-188, 215-234`` does.
     """
     _, _, nxf, nyf, _, _ = fine_grid(mesh, rx, ry)
     if _is_number(permeability):
@@ -136,19 +173,15 @@ def permeability_input(permeability, mesh: CartesianMacroMesh, rx: int, ry: int,
         mode, comp = _tensor_components(arr)
         return mode, comp, (0.0, 0.0, 0.0)
     if hasattr(permeability, "spacing") and hasattr(permeability, "values"):
-        fhx, fhy, _, _, x0, y0 = fine_grid(mesh, rx, ry)
         spacing = np.asarray(permeability.spacing, dtype=float)
-        origin = np.zeros(2) if getattr(permeability, "origin", None) is None else np.asarray(permeability.origin, float)
-        ratio = spacing / np.array([fhx, fhy])
-        offset = (np.array([x0, y0]) - origin) / np.array([fhx, fhy])
-        if (spacing.shape != (2,) or np.any(np.abs(ratio - np.rint(ratio)) > 1e-9 * np.maximum(1, ratio))
-                or np.any(np.abs(offset - np.rint(offset)) > 1e-9 * np.maximum(1, np.abs(offset)))
-                or np.any(np.rint(ratio) < 1)):
-            raise NotImplementedError(
-                "material lines must coincide with fine-grid lines (cut-cell quadrature is not on this path)")
+        origin = _pixel_origin(permeability)
+        vals = np.asarray(permeability.values, dtype=float)
+        if not grid_resolves_material(permeability, mesh, rx, ry):
+            pixel_geometry(permeability, mesh, rx, ry)  # coverage
+            mode, comp = _tensor_components(vals)
+            return mode + 2, comp, (0.0, 0.0, 0.0)
         centres = _fine_centres(mesh, rx, ry)
         idx = np.floor((centres - origin) / spacing).astype(np.int64)
-        vals = np.asarray(permeability.values, dtype=float)
         shape = np.array(vals.shape[:2])
         if np.any(idx < 0) or np.any(idx >= shape):
             raise ValueError("a fine rectangle lies outside the Cartesian material field")
@@ -174,6 +207,15 @@ def permeability_input(permeability, mesh: CartesianMacroMesh, rx: int, ry: int,
             return mode, comp, (0.0, 0.0, 0.0)
         raise ValueError("permeability callable must return scalars or 2x2 tensors per point")
     raise TypeError("unsupported permeability description")
+
+
+def _cut_source_check(smode: int) -> None:
+    """With pixel lines cutting the fine cells the reference integrates the load on the
+    cut rule too; a pointwise source is sampled here on the fine cells' own Gauss
+    points, which is a different quadrature unless the source is constant per cell."""
+    if smode == 2:
+        raise NotImplementedError("a pointwise source with a cut material field needs the cut load quadrature; "
+                                  "pass a constant or per-fine-cell source")
 
 
 def source_input(source, mesh: CartesianMacroMesh, rx: int, ry: int, order: int):
@@ -374,13 +416,27 @@ class CartesianQ1Plan:
         torch = self.torch
         kmode, karr, kconst = permeability_input(permeability, self.mesh, self.rx, self.ry, self.order)
         smode, sarr, sconst = source_input(source, self.mesh, self.rx, self.ry, self.order)
+        pixels = pixel_geometry(permeability, self.mesh, self.rx, self.ry) if kmode >= 3 else None
         self.kappa = None if karr is None else torch.as_tensor(np.array(karr)).to(self.device, non_blocking=non_blocking)
         self.source = None if sarr is None else torch.as_tensor(np.array(sarr)).to(self.device, non_blocking=non_blocking)
-        self.set_device_coefficients(kmode, self.kappa, kconst, smode, self.source, sconst)
+        self.set_device_coefficients(kmode, self.kappa, kconst, smode, self.source, sconst, pixels=pixels)
 
-    def set_device_coefficients(self, kmode, kappa, kconst, smode, source, sconst):
-        """Point the plan at device-resident coefficient tensors (no copies)."""
+    def set_device_coefficients(self, kmode, kappa, kconst, smode, source, sconst, *, pixels=None):
+        """Point the plan at device-resident coefficient tensors (no copies).
+
+        ``pixels`` = (origin, spacing, counts) is required for the cut-cell modes 3/4,
+        where ``kappa`` holds pixel values [px][py][comp]."""
         q = self.q1
+        if kmode >= 3:
+            if pixels is None:
+                raise ValueError("kappa modes 3 and 4 need the pixel geometry")
+            _cut_source_check(smode)
+            (q.pixel_origin[0], q.pixel_origin[1]), (q.pixel_spacing[0], q.pixel_spacing[1]), \
+                (q.pixel_nx, q.pixel_ny) = pixels
+            if getattr(self, "cut_elements", None) is None:
+                self.cut_elements = self.torch.empty(self.nxf * self.nyf * 16, dtype=self.torch.float64,
+                                                     device=self.device)
+            q.cut_elements = _lib.ptr(self.cut_elements)
         q.kappa_mode, q.kappa = kmode, _lib.ptr(kappa)
         q.kappa_const[0], q.kappa_const[1], q.kappa_const[2] = kconst
         q.source_mode, q.source, q.source_const = smode, _lib.ptr(source), float(sconst)
@@ -510,6 +566,8 @@ class CartesianQ1Plan:
     def set_source(self, source=0.0, *, non_blocking=False):
         """Replace the source only (the permeability and the kept factors stay)."""
         smode, sarr, sconst = source_input(source, self.mesh, self.rx, self.ry, self.order)
+        if self.q1.kappa_mode >= 3:
+            _cut_source_check(smode)
         self.source = None if sarr is None else self.torch.as_tensor(np.array(sarr)).to(
             self.device, non_blocking=non_blocking)
         q = self.q1

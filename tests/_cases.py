@@ -38,6 +38,8 @@ CASES = {
     "poisson_8x8_r4_p1": ((8,), (1, 1), (4, 4), lambda g: 1.0, sine_source, 0.0),
     "darcy_4x4_r16_p2_lognormal": ((4,), (2, 1), (16, 16),
                                    lambda g: PixelField(g["kappa"], (1 / 64, 1 / 64)), 1.0, 0.0),
+    "darcy_4x4_r8_p1_cut20": ((4,), (1, 1), (8, 8),
+                              lambda g: PixelField(g["kappa"], (1 / 20, 1 / 20)), 1.0, 0.0),
     "affine_3x2_rect_r4x5_p1s2": ((3, 2, (-1, 2, -2, 2)), (1, 2), (4, 5),
                                   lambda g: PixelField(g["kappa"], (0.25, 0.4), (-1, -2)), quad_source,
                                   affine_dirichlet),

@@ -9,7 +9,8 @@ import numpy as np
 import pytest
 
 from pymhm_b200 import _lib
-from pymhm_b200.darcy import permeability_input, source_input
+from pymhm_b200.darcy import (_cut_source_check, grid_resolves_material, permeability_input, pixel_geometry,
+                               source_input)
 from pymhm_b200.topology import CartesianMacroMesh
 from pymhm_b200.workloads import digest, lognormal_permeability
 from tests._cases import PixelField, load
@@ -37,15 +38,17 @@ def test_struct_layout_matches_header(tmp_path):
     src = tmp_path / "layout.c"
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "mhm_b200.h"\n'
-        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu\\n\", sizeof(mhm_q1_problem),"
+        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu\\n\", sizeof(mhm_q1_problem),"
         " offsetof(mhm_q1_problem, kappa_const), offsetof(mhm_q1_problem, quad_order),"
         " sizeof(mhm_skeleton_system), offsetof(mhm_skeleton_system, nx),"
-        " offsetof(mhm_skeleton_system, coarse_ay)); return 0;}\n")
+        " offsetof(mhm_skeleton_system, coarse_ay), offsetof(mhm_q1_problem, pixel_origin),"
+        " offsetof(mhm_q1_problem, pixel_ny)); return 0;}\n")
     exe = tmp_path / "layout"
     subprocess.run(["gcc", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [ctypes.sizeof(_lib.Q1Problem), _lib.Q1Problem.kappa_const.offset, _lib.Q1Problem.quad_order.offset,
-            ctypes.sizeof(_lib.SkeletonSystem), _lib.SkeletonSystem.nx.offset, _lib.SkeletonSystem.coarse_ay.offset]
+            ctypes.sizeof(_lib.SkeletonSystem), _lib.SkeletonSystem.nx.offset, _lib.SkeletonSystem.coarse_ay.offset,
+            _lib.Q1Problem.pixel_origin.offset, _lib.Q1Problem.pixel_ny.offset]
     assert got == want
 
 
@@ -78,8 +81,26 @@ def test_pixel_field_mapping_and_alignment():
     coarse = np.arange(1, 17, dtype=float).reshape(4, 4)
     mode, arr, _ = permeability_input(PixelField(coarse, (0.25, 0.25)), mesh, 16, 16, 4)
     assert mode == 1 and np.array_equal(arr, np.repeat(np.repeat(coarse, 16, 0), 16, 1))
-    with pytest.raises(NotImplementedError, match="fine-grid lines"):
-        permeability_input(PixelField(coarse, (0.3, 0.25)), mesh, 16, 16, 4)
+    # pixel lines that cut the fine cells: pixels passed as they are (cut-cell modes)
+    mode, arr, _ = permeability_input(PixelField(coarse, (0.3, 0.25)), mesh, 16, 16, 4)
+    assert mode == 3 and np.array_equal(arr, coarse)
+    assert pixel_geometry(PixelField(coarse, (0.3, 0.25)), mesh, 16, 16) == ((0.0, 0.0), (0.3, 0.25), (4, 4))
+    assert not grid_resolves_material(PixelField(coarse, (0.3, 0.25)), mesh, 16, 16)
+    assert grid_resolves_material(PixelField(coarse, (0.25, 0.25), (0.0, -1 / 64)), mesh, 16, 16)
+    # a shifted origin alone also cuts
+    mode, _, _ = permeability_input(PixelField(np.ones((5, 5)), (0.25, 0.25), (-0.01, -0.01)), mesh, 16, 16, 4)
+    assert mode == 3
+    ptens = np.broadcast_to(np.array([[2.0, 0.5], [0.5, 3.0]]), (4, 4, 2, 2))
+    mode, arr, _ = permeability_input(PixelField(ptens, (0.3, 0.3)), mesh, 16, 16, 4)
+    assert mode == 4 and arr.shape == (4, 4, 3) and np.all(arr[..., 1] == 0.5)
+    with pytest.raises(ValueError, match="outside the Cartesian material field"):
+        permeability_input(PixelField(coarse, (0.2, 0.25)), mesh, 16, 16, 4)
+    with pytest.raises(ValueError, match="outside the Cartesian material field"):
+        permeability_input(PixelField(coarse, (0.3, 0.3), (0.01, 0.0)), mesh, 16, 16, 4)
+    with pytest.raises(NotImplementedError, match="cut load quadrature"):
+        _cut_source_check(2)
+    _cut_source_check(0)
+    _cut_source_check(1)
     with pytest.raises(ValueError, match="positive definite"):
         permeability_input(-1.0, mesh, 16, 16, 4)
     with pytest.raises(ValueError, match="positive definite"):
