@@ -235,7 +235,69 @@ def dist_env():
     return rank, world, local
 
 
-class Clocks:
+class NvmlClocks:
+    """SM clock and clock-event reasons read through NVML every 5 ms on a thread during
+    the timed region (read only; the timed region of the default run is tens of ms,
+    shorter than nvidia-smi's sampling period).  The GPU is matched by UUID, so a
+    remapped CUDA_VISIBLE_DEVICES cannot select another board."""
+
+    PERIOD_S = 0.005
+
+    def __init__(self, device_index):
+        import threading
+
+        import pynvml
+
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        uuid = str(__import__("torch").cuda.get_device_properties(device_index).uuid)
+        self.handle = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM))
+        self.bits = {
+            "hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+            "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+            "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+            "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap,
+        }
+        self.sm, self.reasons = [], set()
+        self.done = threading.Event()
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
+
+    def _sample(self):
+        nv = self.nv
+        self.sm.append(float(nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM)))
+        active = nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+        self.reasons.update(name for name, bit in self.bits.items() if active & bit)
+
+    def _run(self):
+        while True:
+            self._sample()
+            if self.done.wait(self.PERIOD_S):
+                return
+
+    def stop(self):
+        self.done.set()
+        self.thread.join(timeout=5)
+        try:
+            self.nv.nvmlShutdown()
+        except Exception:
+            pass
+        if not self.sm:
+            return None
+        return {"sm_mhz": float(np.median(self.sm)), "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.sm), "source": "nvml, 5 ms period"}
+
+
+def Clocks(index):
+    """NVML sampler, or nvidia-smi when NVML is not importable."""
+    try:
+        return NvmlClocks(index)
+    except Exception:
+        return SmiClocks(index)
+
+
+class SmiClocks:
     """nvidia-smi sampling during the timed region (median SM clock, throttle reasons)."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -270,7 +332,7 @@ class Clocks:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi, 200 ms period"}
 
 
 def workload_kappa():
@@ -571,35 +633,58 @@ def main():
     for j in range(2):
         pl[j].set_device_coefficients(1, kdev[j], (0.0, 0.0, 0.0), 0, None, 1.0)
 
+    # results leave on a copy stream per plan: the plan's next local stage waits for
+    # its previous solve's compute only, and its next global stage (which rewrites x,
+    # fields and flux) for the copies, which have long finished by then
+    copy_st = [torch.cuda.Stream(device=dev) for _ in range(2)]
+    copied, status_copied = [None, None], [None, None]
+
     def request(k):
         j = k % 2
-        p_, ls, gs, h = pl[j], local_st[j], global_st[j], hosts[j]
+        p_, ls, gs, cs, h = pl[j], local_st[j], global_st[j], copy_st[j], hosts[j]
         if getattr(p_, "_done", None) is not None:
-            ls.wait_event(p_._done)  # the previous request on this plan still reads kappa
+            ls.wait_event(p_._done)  # the previous solve on this plan still reads kappa and its responses
+        if status_copied[j] is not None:
+            ls.wait_event(status_copied[j])  # the local stage rewrites the cell status words
+        if copied[j] is not None:
+            gs.wait_event(copied[j])
         with torch.cuda.stream(ls):
             kdev[j].copy_(kappa_host, non_blocking=True)
-        p_.launch(ls, global_stream=gs)
-        with torch.cuda.stream(gs):
+        p_.launch(ls, global_stream=gs)  # records p_._done on gs after the reconstruction
+        cs.wait_event(p_._done)
+        with torch.cuda.stream(cs):
+            h["status"].copy_(p_.cell_status, non_blocking=True)
+            status_copied[j] = torch.cuda.Event()
+            status_copied[j].record(cs)
+            h["info"].copy_(p_.info, non_blocking=True)
             h["fields"].copy_(p_.fields, non_blocking=True)
             h["flux"].copy_(p_.flux, non_blocking=True)
             h["x"].copy_(p_.x, non_blocking=True)
-            h["status"].copy_(p_.cell_status, non_blocking=True)
-            h["info"].copy_(p_.info, non_blocking=True)
         ev = torch.cuda.Event()
-        ev.record(gs)
-        p_._done = ev
+        ev.record(cs)
+        copied[j] = ev
 
-    fork()
+    def fork_all():
+        fork()
+        for cs in copy_st:
+            cs.wait_stream(stream)
+
+    def join_all():
+        join()
+        for cs in copy_st:
+            stream.wait_stream(cs)
+
+    fork_all()
     for k in range(args.warmup):
         request(k)
-    join()
+    join_all()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    fork()
+    fork_all()
     for k in range(args.steps):
         request(k)
-    join()
+    join_all()
     e1.record(stream)
     torch.cuda.synchronize()
     for h in hosts:

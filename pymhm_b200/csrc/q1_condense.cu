@@ -500,6 +500,9 @@ struct Occupancy {
 // boundary node cb (t kmax) and its column sums zb (t), and node-wise the lower
 // stencil of A sten (5 n), the load f (n) and the constraint c = M 1 (n).  Each
 // thread returns its part of max|A|, ||A||_F^2 and max c.
+// CUT: the cut-cell modes (kappa_mode 3/4), a compile-time switch so that the
+// aligned modes' kernels carry no trace of the cut path.
+template <bool CUT>
 __device__ __forceinline__ void assemble_cell(const Q1Args& a, int cell, double* kel, double* fel, double* cb,
                                               double* zb, double* sten, double* fvec, double* ctil, double& amax,
                                               double& fro, double& cmax) {
@@ -510,7 +513,7 @@ __device__ __forceinline__ void assemble_cell(const Q1Args& a, int cell, double*
   for (int e = tid; e < ne; e += blockDim.x) {
     const int ex = e % a.rx, ey = e / a.rx;
     const size_t g = (size_t)(cx * a.rx + ex) * a.NYf + (cy * a.ry + ey);
-    if (!a.cut_mode) {
+    if (!CUT) {
       double kxx, kxy, kyy;
       if (a.kmode == 0) {
         kxx = a.k0; kxy = a.k1; kyy = a.k2;
@@ -572,35 +575,35 @@ __device__ __forceinline__ void assemble_cell(const Q1Args& a, int cell, double*
     const size_t g11 = (size_t)(cx * a.rx + ix) * a.NYf + (cy * a.ry + iy);
     if (l && d) {
       const int e = (iy - 1) * a.rx + ix - 1;
-      const double* k = a.cut_mode ? a.cut + 16 * (g11 - a.NYf - 1) : kel + 3 * e;
-      sv[0] += elem_entry(a.cut_mode, k, rxy, ryx, 3, 3);
-      sv[1] += elem_entry(a.cut_mode, k, rxy, ryx, 3, 2);
-      sv[3] += elem_entry(a.cut_mode, k, rxy, ryx, 3, 1);
-      sv[4] += elem_entry(a.cut_mode, k, rxy, ryx, 3, 0);
+      const double* k = CUT ? a.cut + 16 * (g11 - a.NYf - 1) : kel + 3 * e;
+      sv[0] += elem_entry(CUT, k, rxy, ryx, 3, 3);
+      sv[1] += elem_entry(CUT, k, rxy, ryx, 3, 2);
+      sv[3] += elem_entry(CUT, k, rxy, ryx, 3, 1);
+      sv[4] += elem_entry(CUT, k, rxy, ryx, 3, 0);
       f += fel[4 * e + 3];
       ++count;
     }
     if (r && d) {
       const int e = (iy - 1) * a.rx + ix;
-      const double* k = a.cut_mode ? a.cut + 16 * (g11 - 1) : kel + 3 * e;
-      sv[0] += elem_entry(a.cut_mode, k, rxy, ryx, 2, 2);
-      sv[2] += elem_entry(a.cut_mode, k, rxy, ryx, 2, 1);
-      sv[3] += elem_entry(a.cut_mode, k, rxy, ryx, 2, 0);
+      const double* k = CUT ? a.cut + 16 * (g11 - 1) : kel + 3 * e;
+      sv[0] += elem_entry(CUT, k, rxy, ryx, 2, 2);
+      sv[2] += elem_entry(CUT, k, rxy, ryx, 2, 1);
+      sv[3] += elem_entry(CUT, k, rxy, ryx, 2, 0);
       f += fel[4 * e + 2];
       ++count;
     }
     if (l && u) {
       const int e = iy * a.rx + ix - 1;
-      const double* k = a.cut_mode ? a.cut + 16 * (g11 - a.NYf) : kel + 3 * e;
-      sv[0] += elem_entry(a.cut_mode, k, rxy, ryx, 1, 1);
-      sv[1] += elem_entry(a.cut_mode, k, rxy, ryx, 1, 0);
+      const double* k = CUT ? a.cut + 16 * (g11 - a.NYf) : kel + 3 * e;
+      sv[0] += elem_entry(CUT, k, rxy, ryx, 1, 1);
+      sv[1] += elem_entry(CUT, k, rxy, ryx, 1, 0);
       f += fel[4 * e + 1];
       ++count;
     }
     if (r && u) {
       const int e = iy * a.rx + ix;
-      const double* k = a.cut_mode ? a.cut + 16 * (g11) : kel + 3 * e;
-      sv[0] += elem_entry(a.cut_mode, k, rxy, ryx, 0, 0);
+      const double* k = CUT ? a.cut + 16 * (g11) : kel + 3 * e;
+      sv[0] += elem_entry(CUT, k, rxy, ryx, 0, 0);
       f += fel[4 * e + 0];
       ++count;
     }
@@ -618,7 +621,7 @@ __device__ __forceinline__ void assemble_cell(const Q1Args& a, int cell, double*
   __syncthreads();
 }
 
-template <typename T, int NNX>
+template <typename T, int NNX, bool CUT>
 __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_kernel(const Q1Args a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int cell = blockIdx.x;
@@ -657,7 +660,7 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
 
   if (tid == 0) flag[0] = 0;
   double amax, fro, cmax;
-  assemble_cell(a, cell, kel, fel, cb, zb, sten, fvec, ctil, amax, fro, cmax);
+  assemble_cell<CUT>(a, cell, kel, fel, cb, zb, sten, fvec, ctil, amax, fro, cmax);
   // retained action A 1 (compensated row sums) and finiteness
   double az2 = 0.0;
   int nonzero = 0, nonfinite = 0;
@@ -1078,7 +1081,10 @@ __global__ void __launch_bounds__(kThreads) q1_defect_kernel(const Q1Args a, con
   double* lam = u + n;
   double* red = lam + t;
   double amax, fro, cmax;
-  assemble_cell(a, cell, kel, fel, cb, zb, sten, fvec, ctil, amax, fro, cmax);
+  if (a.cut_mode)
+    assemble_cell<true>(a, cell, kel, fel, cb, zb, sten, fvec, ctil, amax, fro, cmax);
+  else
+    assemble_cell<false>(a, cell, kel, fel, cb, zb, sten, fvec, ctil, amax, fro, cmax);
   for (int i = tid; i < n; i += blockDim.x) u[i] = fields[(size_t)cell * n + i];
   for (int j = tid; j < t; j += blockDim.x) lam[j] = x[cell_dofs[(size_t)cell * t + j]];
   __syncthreads();
@@ -1290,13 +1296,18 @@ int fill_args(const mhm_q1_problem* p, int precision, Q1Args& a) {
   return MHM_OK;
 }
 
-template <typename T, int NNX>
-int launch_one(const Q1Args& a, int cells, cudaStream_t s) {
-  if (cudaFuncSetAttribute(q1_condense_kernel<T, NNX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template <typename T, int NNX, bool CUT>
+int launch_variant(const Q1Args& a, int cells, cudaStream_t s) {
+  if (cudaFuncSetAttribute(q1_condense_kernel<T, NNX, CUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)a.smem) != cudaSuccess)
     return MHM_ERR_LAUNCH;
-  q1_condense_kernel<T, NNX><<<cells, kThreads, a.smem, s>>>(a);
+  q1_condense_kernel<T, NNX, CUT><<<cells, kThreads, a.smem, s>>>(a);
   return MHM_OK;
+}
+
+template <typename T, int NNX>
+int launch_one(const Q1Args& a, int cells, cudaStream_t s) {
+  return a.cut_mode ? launch_variant<T, NNX, true>(a, cells, s) : launch_variant<T, NNX, false>(a, cells, s);
 }
 
 // Register-resident factorization for the common line lengths (4, 8 and 16 fine
