@@ -140,6 +140,121 @@ SERVING_MACRO = (16, 32, 64)
 SERVING_LOCAL = (4, 8, 16)
 
 
+def small_poisson_campaign(torch, steps=200, warmup=10):
+    """The 8x8-macrocell Poisson case (4x4 Q1 cells each, P1 faces, kappa = 1,
+    f = 2 pi^2 sin(pi x) sin(pi y), homogeneous Dirichlet): 64 local problems of 25
+    unknowns.  Launch- and latency-bound; reported as solves/s back to back and the
+    latency of one solve at a time (CUDA events), with the error against the
+    reference's FP64 solution of the same case (golden fixture)."""
+    from pymhm_b200.darcy import CartesianQ1Plan
+    from pymhm_b200.topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
+    from pymhm_b200.workloads import sine_source
+
+    mesh = CartesianMacroMesh(8)
+    sk = SkeletonSpace(mesh, (FaceSpace.uniform(1),) * len(mesh.faces))
+    gpath = os.path.join(ROOT, "tests", "golden", "poisson_8x8_r4_p1.npz")
+    g = np.load(gpath) if os.path.exists(gpath) else None
+    out = {}
+    for prec in ("mixed", "fp64"):
+        plan = CartesianQ1Plan(mesh, sk, 4, precision=prec)
+        plan.set_coefficients(1.0, sine_source)
+        st = torch.cuda.Stream()
+        for _ in range(warmup):
+            plan.launch(st)
+        torch.cuda.synchronize()
+        lat = []
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            plan.launch(st)
+            e1.record(st)
+            e1.synchronize()
+            lat.append(e0.elapsed_time(e1))
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(st)
+        for _ in range(steps):
+            plan.launch(st)
+        t1.record(st)
+        torch.cuda.synchronize()
+        eager_s = t0.elapsed_time(t1)
+        # the same fresh solve captured as one CUDA graph (capture("condense"))
+        plan.capture("condense", st)
+        glat = []
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            plan.replay("condense", after=st)
+            e1.record(st)
+            e1.synchronize()
+            glat.append(e0.elapsed_time(e1))
+        t0.record(st)
+        for _ in range(steps):
+            plan.replay("condense", after=st)
+        t1.record(st)
+        torch.cuda.synchronize()
+        sol = plan.result()
+        lat, glat = np.array(lat), np.array(glat)
+        entry = {"solves_per_s": steps * 1000.0 / t0.elapsed_time(t1), "p50_ms": float(np.percentile(glat, 50)),
+                 "p99_ms": float(np.percentile(glat, 99)), "global_iterations": sol.global_iterations,
+                 "eager": {"solves_per_s": steps * 1000.0 / eager_s, "p50_ms": float(np.percentile(lat, 50)),
+                           "p99_ms": float(np.percentile(lat, 99))}}
+        if g is not None:
+            rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+            entry["error_vs_reference"] = {"lambda": rel(sol.trace, g["trace"]), "u": rel(sol.fields, g["fields"]),
+                                           "flux": rel(sol.flux, g["flux"])}
+        out[prec] = entry
+    out["note"] = ("8x8 macrocells x 4x4 Q1, P1 faces, sine source; one fresh solve (four kernels) per CUDA graph "
+                   "replay (capture('condense')); 'eager': the same solve launched from Python each time")
+    return out
+
+
+def cut_material_campaign(torch, steps=5, pixels=1000):
+    """The headline workload's mesh (64x64 macrocells x 16x16 Q1, P2 faces) with a
+    log-normal pixel field of pixels x pixels cells (sigma 2, ell 0.05) whose lines cut
+    the 1024 x 1024 fine cells: every fine cell is integrated on its exact pixel
+    intersections (cut-element pre-pass inside the local stage).  One solve at a time,
+    per-kernel CUDA events; mixed against FP64 on the same input."""
+    from pymhm_b200.darcy import CartesianQ1Plan
+    from pymhm_b200.topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
+    from pymhm_b200.workloads import lognormal_permeability
+
+    class Pixels:
+        def __init__(self, values):
+            self.values, self.spacing, self.origin = values, (1.0 / pixels, 1.0 / pixels), (0.0, 0.0)
+
+    field = Pixels(lognormal_permeability(pixels, pixels, sigma=SIGMA, ell=ELL, seed=SEED + 1))
+    mesh = CartesianMacroMesh(MACRO)
+    sk = SkeletonSpace(mesh, (FaceSpace.uniform(FACE_DEGREE),) * len(mesh.faces))
+    out, fields = {}, {}
+    for prec in ("mixed", "fp64"):
+        plan = CartesianQ1Plan(mesh, sk, LOCAL, precision=prec)
+        plan.set_coefficients(field, 1.0)
+        st = torch.cuda.Stream()
+        plan.launch(st)
+        torch.cuda.synchronize()
+        per = []
+        for _ in range(steps):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+            plan.launch(st, events=ev)
+            torch.cuda.synchronize()
+            per.append([ev[i].elapsed_time(ev[i + 1]) for i in range(4)])
+        sol = plan.result()
+        per = np.array(per)
+        out[prec] = {"ms_per_solve": float(per.sum(1).mean()),
+                     "kernels_ms": {"q1_condense_with_cut_prepass": float(per[:, 0].mean()),
+                                    "skeleton_scatter": float(per[:, 1].mean()),
+                                    "skeleton_pcg": float(per[:, 2].mean()),
+                                    "q1_reconstruct": float(per[:, 3].mean())},
+                     "global_iterations": sol.global_iterations, "kappa_mode": int(plan.q1.kappa_mode)}
+        fields[prec] = sol.fields
+        plan.cut_elements = None
+    out["mixed_vs_fp64_fields"] = float(np.linalg.norm(fields["mixed"] - fields["fp64"]) /
+                                        np.linalg.norm(fields["fp64"]))
+    out["note"] = (f"{pixels}x{pixels} pixel field over the 1024x1024 fine grid (pixel lines cut the fine cells); "
+                   "the condense time includes the cut-element pre-pass")
+    return out
+
+
 def serving_campaign(torch, lambdas=(100, 500, 2000), requests=150, precisions=("mixed", "fp64")):
     """Streamed serving (continuous batching with admission by HBM footprint): Poisson
     arrivals at each rate in ``lambdas``; per request a macro grid from {16, 32, 64}^2,
@@ -207,6 +322,9 @@ def parse():
                     help="with --profile: also one refinement step, a P1 batch assembly and a batched LU")
     ap.add_argument("--lu-case", type=int, default=0, metavar="N",
                     help="only factor 64 seeded N x N matrices twice with the batched LU (for ncu)")
+    ap.add_argument("--cut-case", type=int, default=0, metavar="P",
+                    help="only the 64x64 x 16x16 solve with a P x P pixel field cutting the fine cells, "
+                         "mixed and FP64, two timed solves each (for ncu)")
     return ap.parse_args()
 
 
@@ -424,6 +542,11 @@ def main():
     if args.lu_case:
         lu_case(args.lu_case)
         return
+    if args.cut_case:
+        import torch
+
+        print(json.dumps({"cut_case": cut_material_campaign(torch, steps=2, pixels=args.cut_case)}))
+        return
     rank, world, local = dist_env()
     kappa = workload_kappa()
     # CPU baseline first (spawned pool before any CUDA context exists)
@@ -608,6 +731,8 @@ def main():
 
     # streamed serving of independent requests (continuous batching, HBM admission)
     serving_stream = serving_campaign(torch)
+    small_poisson = small_poisson_campaign(torch)
+    cut_material = cut_material_campaign(torch)
 
     # the reference's own batched local-stage benchmark, same phases and sizes
     campaigns = {f"batched_local_r{r}": batched_local_campaign(torch, r) for r in (12, 24)}
@@ -755,6 +880,8 @@ def main():
         "refinement": refinement,
         "reference_campaigns": campaigns,
         "serving_stream": serving_stream,
+        "poisson_8x8_r4_p1": small_poisson,
+        "cut_material": cut_material,
         "global_iterations": int(mixed["info"][1]), "outer_corrections": int(mixed["info"][2]),
         "residual": float(mixed["stats"][0]), "certificate": float(mixed["stats"][1]),
         "error_vs_reference": acc,

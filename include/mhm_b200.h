@@ -119,9 +119,10 @@ typedef struct mhm_q1_problem {
     int32_t pixel_nx, pixel_ny;   /* kappa_mode 3/4: pixel counts; the field must
                                      cover the domain                              */
     double* cut_elements;         /* kappa_mode 3/4: device work buffer of
-                                     (global fine cells) x 16 doubles, [gx][gy][4x4];
-                                     every local entry point first writes each fine
-                                     cell's element stiffness there               */
+                                     10 x (global fine cells) doubles: the lower
+                                     triangle of each fine cell's element stiffness,
+                                     entry-major [entry][gx][gy]; every local entry
+                                     point first writes it                         */
 } mhm_q1_problem;
 
 /* Width of the per-cell right-hand side block: 1 source + trace + 1 retained. */

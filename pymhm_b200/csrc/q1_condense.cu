@@ -50,9 +50,11 @@ struct Q1Args {
   const double* kappa;
   double k0, k1, k2;
   // kmode 3/4: pixel field [px][py][comp] whose lines may cut the fine cells; a
-  // pre-pass writes every fine cell's 4x4 element matrix to cut ([gx][gy][16]),
-  // which the node gather reads in place of the per-element tensor (cut_mode)
+  // pre-pass writes the lower triangle of every fine cell's element matrix to cut,
+  // entry-major ([entry][gx][gy], entry (r, c), r >= c, at r (r + 1) / 2 + c, stride
+  // cut_stride = fine cells), which the node gather reads in place of the tensor
   bool cut_mode;
+  int64_t cut_stride;
   double x0, y0;
   double px0, py0, psx, psy;
   int pnx, pny;
@@ -124,7 +126,8 @@ __device__ __forceinline__ void pixel_segment(double lo, double h, double origin
   m = a + 0.5 * w;
 }
 
-// Element matrix of a fine cell cut by pixel lines (kappa_mode 3/4): the sum over
+// Lower triangle of the element matrix of a fine cell cut by pixel lines (kappa_mode
+// 3/4, entry (a, c) with a >= c at a (a + 1) / 2 + c): the sum over
 // its pixel intersections [a,b] x [c,d] (reference coordinates) of the exact Q1
 // integrals with that pixel's constant tensor.  With X_0 = 1 - xi, X_1 = xi,
 // slopes s_0 = -1, s_1 = 1, midpoints m and widths w, every product of two linear
@@ -134,9 +137,10 @@ __device__ __forceinline__ void pixel_segment(double lo, double h, double origin
 // IX(i,j) = wx (X_i X_j (mx) + s_i s_j wx^2/12), JX(i) = wx X_i(mx), likewise in y.
 // This is the reference's per-intersection Gauss sum (exact for these integrands)
 // up to rounding (quadrilateral.py:215-234).
-__device__ void cut_element(const Q1Args& a, double ex0, double ey0, double* km) {
+__device__ __forceinline__ void cut_element(const Q1Args& a, double ex0, double ey0, double (&km)[10]) {
   const double rxy = a.hy / a.hx, ryx = a.hx / a.hy;
-  for (int q = 0; q < 16; ++q) km[q] = 0.0;
+#pragma unroll
+  for (int q = 0; q < 10; ++q) km[q] = 0.0;
   int fx, lx, fy, ly;
   pixel_span(ex0, a.hx, a.px0, a.psx, a.pnx, fx, lx);
   pixel_span(ey0, a.hy, a.py0, a.psy, a.pny, fy, ly);
@@ -158,10 +162,12 @@ __device__ void cut_element(const Q1Args& a, double ex0, double ey0, double* km)
         kxx = a.kappa[3 * g]; kxy = a.kappa[3 * g + 1]; kyy = a.kappa[3 * g + 2];
       }
       const double cx2 = wx * wx / 12.0, cy2 = wy * wy / 12.0;
+#pragma unroll
       for (int A = 0; A < 4; ++A) {
         const int ax = A & 1, ay = A >> 1;
         const double sax = ax ? 1.0 : -1.0, say = ay ? 1.0 : -1.0;
-        for (int Cc = 0; Cc < 4; ++Cc) {
+#pragma unroll
+        for (int Cc = 0; Cc <= A; ++Cc) {
           const int cx = Cc & 1, cy = Cc >> 1;
           const double scx = cx ? 1.0 : -1.0, scy = cy ? 1.0 : -1.0;
           const double iy2 = wy * (Y[ay] * Y[cy] + say * scy * cy2);
@@ -169,7 +175,7 @@ __device__ void cut_element(const Q1Args& a, double ex0, double ey0, double* km)
           double v = kxx * rxy * (sax * scx) * wx * iy2 + kyy * ryx * (say * scy) * wy * ix2;
           if (kxy != 0.0)
             v += kxy * (sax * scy * (wx * X[cx]) * (wy * Y[ay]) + say * scx * (wx * X[ax]) * (wy * Y[cy]));
-          km[A * 4 + Cc] += v;
+          km[A * (A + 1) / 2 + Cc] += v;
         }
       }
     }
@@ -182,18 +188,20 @@ __global__ void __launch_bounds__(256) cut_element_kernel(const Q1Args a) {
   for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total;
        g += (int64_t)gridDim.x * blockDim.x) {
     const int gx = (int)(g / a.NYf), gy = (int)(g - (int64_t)gx * a.NYf);
-    double km[16];
+    double km[10];
     cut_element(a, a.x0 + (double)gx * a.hx, a.y0 + (double)gy * a.hy, km);
-    double* out = a.cut + 16 * g;
+    // entry-major: consecutive threads store consecutive fine cells of one entry
 #pragma unroll
-    for (int q = 0; q < 16; ++q) out[q] = km[q];
+    for (int q = 0; q < 10; ++q) a.cut[q * a.cut_stride + g] = km[q];
   }
 }
 
-// Entry (r, c) of an element stiffness: k is the element's 4x4 cut-cell matrix from
-// the pre-pass (cut) or its tensor (kxx, kxy, kyy) for the closed form.
-__device__ __forceinline__ double elem_entry(bool cut, const double* k, double rxy, double ryx, int r, int c) {
-  if (cut) return __ldg(k + 4 * r + c);
+// Entry (r, c), r >= c, of an element stiffness: k points at the element's first
+// cut-cell entry from the pre-pass (entries cut_stride apart), or at its tensor
+// (kxx, kxy, kyy) for the closed form.
+__device__ __forceinline__ double elem_entry(const Q1Args& a, bool cut, const double* k, double rxy, double ryx,
+                                             int r, int c) {
+  if (cut) return __ldg(k + (r * (r + 1) / 2 + c) * a.cut_stride);
   return elem_k(k[0], k[1], k[2], rxy, ryx, r, c);
 }
 
@@ -575,35 +583,35 @@ __device__ __forceinline__ void assemble_cell(const Q1Args& a, int cell, double*
     const size_t g11 = (size_t)(cx * a.rx + ix) * a.NYf + (cy * a.ry + iy);
     if (l && d) {
       const int e = (iy - 1) * a.rx + ix - 1;
-      const double* k = CUT ? a.cut + 16 * (g11 - a.NYf - 1) : kel + 3 * e;
-      sv[0] += elem_entry(CUT, k, rxy, ryx, 3, 3);
-      sv[1] += elem_entry(CUT, k, rxy, ryx, 3, 2);
-      sv[3] += elem_entry(CUT, k, rxy, ryx, 3, 1);
-      sv[4] += elem_entry(CUT, k, rxy, ryx, 3, 0);
+      const double* k = CUT ? a.cut + (g11 - a.NYf - 1) : kel + 3 * e;
+      sv[0] += elem_entry(a, CUT, k, rxy, ryx, 3, 3);
+      sv[1] += elem_entry(a, CUT, k, rxy, ryx, 3, 2);
+      sv[3] += elem_entry(a, CUT, k, rxy, ryx, 3, 1);
+      sv[4] += elem_entry(a, CUT, k, rxy, ryx, 3, 0);
       f += fel[4 * e + 3];
       ++count;
     }
     if (r && d) {
       const int e = (iy - 1) * a.rx + ix;
-      const double* k = CUT ? a.cut + 16 * (g11 - 1) : kel + 3 * e;
-      sv[0] += elem_entry(CUT, k, rxy, ryx, 2, 2);
-      sv[2] += elem_entry(CUT, k, rxy, ryx, 2, 1);
-      sv[3] += elem_entry(CUT, k, rxy, ryx, 2, 0);
+      const double* k = CUT ? a.cut + (g11 - 1) : kel + 3 * e;
+      sv[0] += elem_entry(a, CUT, k, rxy, ryx, 2, 2);
+      sv[2] += elem_entry(a, CUT, k, rxy, ryx, 2, 1);
+      sv[3] += elem_entry(a, CUT, k, rxy, ryx, 2, 0);
       f += fel[4 * e + 2];
       ++count;
     }
     if (l && u) {
       const int e = iy * a.rx + ix - 1;
-      const double* k = CUT ? a.cut + 16 * (g11 - a.NYf) : kel + 3 * e;
-      sv[0] += elem_entry(CUT, k, rxy, ryx, 1, 1);
-      sv[1] += elem_entry(CUT, k, rxy, ryx, 1, 0);
+      const double* k = CUT ? a.cut + (g11 - a.NYf) : kel + 3 * e;
+      sv[0] += elem_entry(a, CUT, k, rxy, ryx, 1, 1);
+      sv[1] += elem_entry(a, CUT, k, rxy, ryx, 1, 0);
       f += fel[4 * e + 1];
       ++count;
     }
     if (r && u) {
       const int e = iy * a.rx + ix;
-      const double* k = CUT ? a.cut + 16 * (g11) : kel + 3 * e;
-      sv[0] += elem_entry(CUT, k, rxy, ryx, 0, 0);
+      const double* k = CUT ? a.cut + (g11) : kel + 3 * e;
+      sv[0] += elem_entry(a, CUT, k, rxy, ryx, 0, 0);
       f += fel[4 * e + 0];
       ++count;
     }
@@ -1273,6 +1281,7 @@ int fill_args(const mhm_q1_problem* p, int precision, Q1Args& a) {
     a.psx = p->pixel_spacing[0]; a.psy = p->pixel_spacing[1];
     a.pnx = p->pixel_nx; a.pny = p->pixel_ny;
     a.cut = p->cut_elements;
+    a.cut_stride = (int64_t)a.nx * a.rx * a.NYf;
   }
   a.smode = p->source_mode; a.src = p->source; a.s0 = p->source_const;
   a.qorder = p->quad_order > 0 ? p->quad_order : 1;

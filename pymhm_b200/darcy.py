@@ -434,7 +434,7 @@ class CartesianQ1Plan:
             (q.pixel_origin[0], q.pixel_origin[1]), (q.pixel_spacing[0], q.pixel_spacing[1]), \
                 (q.pixel_nx, q.pixel_ny) = pixels
             if getattr(self, "cut_elements", None) is None:
-                self.cut_elements = self.torch.empty(self.nxf * self.nyf * 16, dtype=self.torch.float64,
+                self.cut_elements = self.torch.empty(10 * self.nxf * self.nyf, dtype=self.torch.float64,
                                                      device=self.device)
             q.cut_elements = _lib.ptr(self.cut_elements)
         q.kappa_mode, q.kappa = kmode, _lib.ptr(kappa)
@@ -679,10 +679,15 @@ class CartesianQ1Plan:
         permeability buffer must stay where ``set_device_coefficients`` put it, and the
         source is read from a persistent per-fine-cell device buffer that each replay
         overwrites first (a constant source gives the same element loads as
-        ``source_mode`` 0).  The graph's launches run once eagerly before the capture."""
+        ``source_mode`` 0).  ``"condense"`` captures a complete fresh solve with the
+        coefficients exactly as set (pointwise sources included); its replays take no
+        source and refuse to run once ``set_coefficients`` has moved the coefficient
+        buffers.  The graph's launches run once eagerly before the capture."""
         torch = self.torch
-        if local not in ("offline", "online"):
-            raise ValueError("local must be 'offline' or 'online'")
+        if local not in ("offline", "online", "condense"):
+            raise ValueError("local must be 'offline', 'online' or 'condense'")
+        if local == "condense":
+            return self._capture_graph(local, stream, keep=self._keep)
         if local == "online" and not getattr(self, "_factors_current", False):
             raise RuntimeError("prepare_offline() must run before capturing online queries")
         if local == "offline" and getattr(self, "factors", None) is None:
@@ -693,6 +698,10 @@ class CartesianQ1Plan:
         q = self.q1
         q.source_mode, q.source, q.source_const = 1, _lib.ptr(self._graph_source), 0.0
         self._keep = (self._keep[0], self._graph_source)
+        return self._capture_graph(local, stream)
+
+    def _capture_graph(self, local, stream, keep=None):
+        torch = self.torch
         if getattr(self, "_graphs", None) is None:
             self._graphs, self._graph_stream = {}, None
         st = self._graph_stream or (torch.cuda.Stream(device=self.device) if stream is None else stream)
@@ -705,21 +714,38 @@ class CartesianQ1Plan:
         with torch.cuda.graph(graph, stream=st):
             self.launch(st, local=local)
         self._graphs[local] = graph
+        if keep is not None:
+            # the captured kernels read these buffers: hold them, and remember where they were
+            self._graph_keep = (keep, self.q1.kappa, self.q1.source)
         return graph
 
     def capture_online(self, stream=None):
         """``capture("online")``; requires ``prepare_offline``."""
         return self.capture("online", stream)
 
-    def replay(self, local="online", source=0.0, *, stream=None, after=None):
+    def replay(self, local="online", source=None, *, stream=None, after=None):
         """Run the captured ``local`` solve for ``source`` (a constant or one value per
-        fine cell, shape (nx*rx, ny*ry)), asynchronously on ``stream`` (default: the
-        capture stream) after ``after`` (default: the current stream).  Returns the
-        stream it ran on."""
+        fine cell, shape (nx*rx, ny*ry); default 0 for ``"offline"``/``"online"``, none
+        for ``"condense"``), asynchronously on ``stream`` (default: the capture stream)
+        after ``after`` (default: the current stream).  Returns the stream it ran on."""
         torch = self.torch
         graph = (getattr(self, "_graphs", None) or {}).get(local)
         if graph is None:
             raise RuntimeError(f"capture({local!r}) must run first")
+        if local == "condense":
+            if source is not None:
+                raise ValueError("the captured fresh solve reads the coefficients set before capture; "
+                                 "set_coefficients and capture('condense') again to change them")
+            _, kappa_ptr, source_ptr = self._graph_keep
+            if self.q1.kappa != kappa_ptr or self.q1.source != source_ptr:
+                raise RuntimeError("the coefficients changed since capture('condense'); capture again")
+            st = self._graph_stream if stream is None else stream
+            if after is not st:
+                st.wait_stream(torch.cuda.current_stream() if after is None else after)
+            with torch.cuda.stream(st):
+                graph.replay()
+            return st
+        source = 0.0 if source is None else source
         st = self._graph_stream if stream is None else stream
         if after is not st:
             st.wait_stream(torch.cuda.current_stream() if after is None else after)
