@@ -23,7 +23,9 @@
  *                          leaves core/_assembly.py:10-42.
  *   mhm_skeleton_solve     replaces solve_hybrid_system's global solve
  *                          (core/system.py:355-528 -> linalg/linear.py:798)
- *                          for Dirichlet/weak-boundary systems without gauges.
+ *                          for systems without gauges; with
+ *   mhm_skeleton_fixed_rhs its elimination of fixed (Neumann) trace DOFs
+ *                          (core/system.py:421-447) on whole bottom/top sides.
  *   mhm_q1_reconstruct     replaces reconstruct_response (core/reconstruction.py:
  *                          130-141) and the flux samples of
  *                          QuadrilateralDarcySolution.evaluate
@@ -272,9 +274,29 @@ typedef struct mhm_skeleton_system {
      * additive Schwarz over the cells' 12 x 12 principal submatrices.          */
     const double* cell_blocks;
     int32_t block_ld;
+    /* Optional (NULL allowed): fixed trace DOFs, T bytes (1 = fixed), the Neumann
+     * faces' prescribed coefficients (core/system.py:421-447).  The solve then
+     * works on the free DOFs: rhs must hold rhs - K x_fixed with zeros on the
+     * fixed rows (mhm_skeleton_fixed_rhs), x is returned zero on them and the
+     * caller adds x_fixed.  The fixed DOFs must be all DOFs of the faces of the
+     * whole bottom and/or top side, which the coarse operator takes as Neumann
+     * ends of T_y: coarse_neumann bit 0 = bottom (y = y0), bit 1 = top.         */
+    const uint8_t* fixed;
+    int32_t coarse_neumann;
 } mhm_skeleton_system;
 
 int64_t mhm_skeleton_workspace_bytes(const mhm_skeleton_system* s /* host */, int32_t grid);
+
+/*
+ * Elimination of prescribed trace DOFs before mhm_skeleton_solve, in place:
+ * rhs[i] = rhs[i] - sum_j K[i][j] xfixed[j] (double-double row sums) on the free
+ * rows, 0 on the fixed ones.  xfixed (N) holds the prescribed values on the fixed
+ * trace DOFs and zeros elsewhere; fixed (T bytes) marks them.  K is the CSR of
+ * mhm_skeleton_system.
+ */
+int mhm_skeleton_fixed_rhs(int64_t size, int64_t trace_size, const int64_t* indptr,
+                           const int32_t* indices, const double* values, const uint8_t* fixed,
+                           const double* xfixed, double* rhs, void* stream);
 
 /*
  * Solve K x = rhs.  x (N) is output.  info (device int32[4]): status, total

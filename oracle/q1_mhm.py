@@ -702,13 +702,24 @@ def assemble_global(contribs, trace_size, boundary_load=None):
     return matrix, rhs, scale
 
 
-def solve_global(matrix, rhs, load_scale, rtol=1e-10):
-    """``solve_hybrid_system`` without fixed DOFs or gauges (``core/system.py:355-528``)."""
-    x = EquilibratedLU(matrix, rtol).solve(rhs)
-    defect = matrix @ x - rhs
-    action = abs(matrix) @ np.abs(x)
-    phys = max(np.linalg.norm(rhs), np.linalg.norm(load_scale), np.linalg.norm(rhs),
-               np.linalg.norm(action), np.finfo(float).tiny)
+def solve_global(matrix, rhs, load_scale, rtol=1e-10, fixed=None):
+    """``solve_hybrid_system`` without gauges (``core/system.py:355-528``): fixed trace
+    DOFs take their prescribed values and leave the system, whose other rows lose the
+    prescribed action (``:421-447``)."""
+    fixed = {} if fixed is None else fixed
+    n = len(rhs)
+    x = np.zeros(n)
+    idx = np.array(sorted(fixed), dtype=np.int64)
+    x[idx] = [fixed[i] for i in idx]
+    free = np.setdiff1d(np.arange(n), idx)
+    reduced = matrix[free][:, free] if len(idx) else matrix
+    action = (matrix @ x)[free]
+    rrhs = rhs[free] - action
+    x[free] = EquilibratedLU(sparse.csc_matrix(reduced), rtol).solve(rrhs)
+    defect = reduced @ x[free] - rrhs
+    scale = abs(reduced) @ np.abs(x[free])
+    phys = max(np.linalg.norm(rhs[free]), np.linalg.norm(load_scale[free]), np.linalg.norm(action),
+               np.linalg.norm(rrhs), np.linalg.norm(scale), np.finfo(float).tiny)
     residual = float(np.linalg.norm(defect) / phys)
     if residual > 1e-8:
         raise ValueError("incompatible data: gauge changed physical equations")
@@ -754,9 +765,10 @@ def local_problem(mesh, skeleton, cell, refinement, permeability, source, order=
 
 
 def solve_darcy_q1(mesh, skeleton, refinement, permeability=1.0, source=0.0, dirichlet=0.0,
-                   order=4, keep_responses=False, cells=None):
-    """``solve_darcy_quadrilateral`` for degree one and Dirichlet data (``cartesian.py:86-168``)."""
-    boundary, _ = boundary_data(skeleton, dirichlet, None, order)
+                   order=4, keep_responses=False, cells=None, neumann=None):
+    """``solve_darcy_quadrilateral`` for degree one (``cartesian.py:86-168``); Neumann
+    faces fix their trace DOFs (no pure-Neumann gauge)."""
+    boundary, fixed = boundary_data(skeleton, dirichlet, neumann, order)
     responses, contribs, fines = [], [], []
     for cell in range(len(mesh.cells)):
         fine, problem = local_problem(mesh, skeleton, cell, refinement, permeability, source, order)
@@ -765,7 +777,7 @@ def solve_darcy_q1(mesh, skeleton, refinement, permeability=1.0, source=0.0, dir
         responses.append(resp)
         fines.append(fine)
     matrix, rhs, scale = assemble_global(contribs, skeleton.size, boundary)
-    x, residual = solve_global(matrix, rhs, scale)
+    x, residual = solve_global(matrix, rhs, scale, fixed=fixed)
     trace = x[: skeleton.size]
     coarse = x[skeleton.size:]
     fields = np.array([r.source - r.lifts @ trace[r.problem.trace_dofs] + r.retained @ coarse[c: c + 1]

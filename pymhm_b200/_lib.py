@@ -68,6 +68,7 @@ class SkeletonSystem(C.Structure):
         ("dof_slot", C.c_void_p), ("nx", C.c_int32), ("ny", C.c_int32),
         ("coarse_ax", C.c_double), ("coarse_ay", C.c_double),
         ("cell_blocks", C.c_void_p), ("block_ld", C.c_int32),
+        ("fixed", C.c_void_p), ("coarse_neumann", C.c_int32),
     ]
 
 
@@ -86,6 +87,7 @@ _SIGNATURES = {
     "mhm_q1_original_defect": (C.c_int, [C.POINTER(Q1Problem), P, C.c_int64, P, P, P, P, P, P, P, P, P, P]),
     "mhm_refine_norms": (C.c_int, [C.c_int32, P, C.c_int64, P, P, C.c_int64, P, P, P, P, P, P, P]),
     "mhm_vector_accumulate": (C.c_int, [C.c_int64, P, P, P]),
+    "mhm_skeleton_fixed_rhs": (C.c_int, [C.c_int64, C.c_int64, P, P, P, P, P, P, P]),
     "mhm_q1_flux": (C.c_int, [C.POINTER(Q1Problem), P, P, P]),
     "mhm_skeleton_scatter": (C.c_int, [C.c_int64, P, P, P, P, C.c_int64, C.c_int64, P, P, P, P, P, P, P]),
     "mhm_skeleton_workspace_bytes": (C.c_int64, [C.POINTER(SkeletonSystem), C.c_int32]),

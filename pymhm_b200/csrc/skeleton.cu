@@ -75,6 +75,8 @@ struct Sys {
   double ax, ay;
   const double* blocks;
   int ld;
+  const uint8_t* fixed;  // T: 1 = fixed trace DOF (null: none)
+  int yneu;              // coarse T_y ends: bit 0 bottom, bit 1 top Neumann
 };
 
 // Row-transformed coarse data of one quantity, layout [mode][row]:
@@ -239,8 +241,8 @@ struct Row {
   double* yrow;   // 3 nx
   double* col;    // 12 nx: faces' coarse sums across (1-4) and to the cell (8-11); combined (5)
   double* wrow;   // 3 nx
-  double* mcheb;  // nmode (ny + 1): U_m(theta_k)
-  double* mcinv;  // nmode: 1 / (ay U_ny(theta_k))
+  double* mcheb;  // nmode 2 (ny + 1): U_m(theta_k); with Neumann ends u then v (see mode_solve)
+  double* mcinv;  // nmode: 1 / (ay U_ny(theta_k)), or 1 / C
   double* ucol;   // ny
   double *vr, *vps, *vp, *vlam, *vu, *vt;  // G vectors: r, P S p, p, lambda, u, staging
   double* Sb;     // nx np: packed symmetric S_c
@@ -327,7 +329,9 @@ __device__ void coarse_rowfwd1(const Sys& s, const Row& R, double* dst) {
 // After every row's coarse data is written: for each sine mode k this CTA owns,
 // W[ir][k] = sum_iy Tinv_k[ir][iy] U[k][iy] for every row ir, with
 // Tinv_k[i][j] = U_i U_{ny-1-j} / (ay U_ny) for i <= j (U the mode's Chebyshev
-// values; symmetric).
+// values; symmetric).  With Neumann ends (whole bottom / top sides fixed) the end
+// rows of T_k lose one neighbour and Tinv_k[i][j] = u_i v_j / C for i <= j, u and v
+// the solutions of the homogeneous recurrence from the bottom and the top end.
 __device__ void mode_solve(const Sys& s, const Row& R, const Coarse& U, double* W) {
   const int ny = s.ny, nx = s.nx;
   for (int j = 0; j < R.nmode; ++j) {
@@ -341,16 +345,23 @@ __device__ void mode_solve(const Sys& s, const Row& R, const Coarse& U, double* 
       R.ucol[iy] = (v0 + v1) + v2;
     }
     __syncthreads();
-    const double* u = R.mcheb + (size_t)j * (ny + 1);
+    const double* u = R.mcheb + (size_t)j * 2 * (ny + 1);
+    const double* v = u + (ny + 1);
     const double c = R.mcinv[j];
     const int lane8 = threadIdx.x & 7, grp = threadIdx.x >> 3, ngrp = blockDim.x >> 3;
     for (int base = 0; base < ny; base += ngrp) {
       const int ir = base + grp;
       double acc = 0.0;
       if (ir < ny) {
-        const double uir = u[ir], unir = u[ny - 1 - ir];
-        for (int iy = lane8; iy < ny; iy += 8)
-          acc = fma((ir < iy ? uir * u[ny - 1 - iy] : u[iy] * unir), R.ucol[iy], acc);
+        if (s.yneu == 0) {
+          const double uir = u[ir], unir = u[ny - 1 - ir];
+          for (int iy = lane8; iy < ny; iy += 8)
+            acc = fma((ir < iy ? uir * u[ny - 1 - iy] : u[iy] * unir), R.ucol[iy], acc);
+        } else {
+          const double uir = u[ir], vir = v[ir];
+          for (int iy = lane8; iy < ny; iy += 8)
+            acc = fma((ir <= iy ? uir * v[iy] : u[iy] * vir), R.ucol[iy], acc);
+        }
       }
       acc += __shfl_xor_sync(0xffffffffu, acc, 4);
       acc += __shfl_xor_sync(0xffffffffu, acc, 2);
@@ -461,7 +472,7 @@ __device__ __forceinline__ double face_rows(const Row& R, const double* blk, int
   for (int j = 0; j < FS; ++j) {
     const int idx = (Q * FS + j) * nx + cx;
     dot = fma(xv[Q * FS + j], acc[j], dot);
-    if (Xf) ((R.role[idx] & 1) ? Xs : Xf)[R.gdof[R.cl[idx]]] = acc[j];
+    if (Xf) ((R.role[idx] & 1) ? Xs : Xf)[R.gdof[R.cl[idx]]] = (R.role[idx] & 4) ? 0.0 : acc[j];
     if (coarse) {
       self = fma(R.gself[idx], acc[j], self);
       across = fma(R.gnb[idx], acc[j], across);
@@ -602,7 +613,7 @@ __host__ __device__ size_t smem_layout(int nx, int ny, int fs, int t, int grid, 
   take(3 * (size_t)nx * 8);              // 1 yrow
   take(12 * (size_t)nx * 8);             // 2 col
   take(3 * (size_t)nx * 8);              // 3 wrow
-  take(nmode * (ny + 1) * 8);            // 4 mcheb
+  take(nmode * 2 * (ny + 1) * 8);        // 4 mcheb
   take(nmode * 8);                       // 5 mcinv
   take((size_t)ny * 8);                  // 6 ucol
   take(vec * 8);                         // 7 G vectors (6 g) / setup scratch
@@ -697,18 +708,36 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
   // theta_k = 1 + ax lam_k / (2 ay); U_m(theta_k), m = 0..ny
   for (int j = tid; j < R.nmode; j += nth) {
     const int k = blockIdx.x + j * gridDim.x;
-    double* u = R.mcheb + (size_t)j * (ny + 1);
+    double* u = R.mcheb + (size_t)j * 2 * (ny + 1);
     const double lam = 2.0 - 2.0 * cospi((double)(k + 1) / (double)(nx + 1));
     const double two_theta = 2.0 + s.ax * lam / s.ay;
-    double um1 = 0.0, u0 = 1.0;
-    u[0] = 1.0;
-    for (int m = 1; m <= ny; ++m) {
-      const double un = two_theta * u0 - um1;
-      u[m] = un;
-      um1 = u0;
-      u0 = un;
+    if (s.yneu == 0) {
+      double um1 = 0.0, u0 = 1.0;
+      u[0] = 1.0;
+      for (int m = 1; m <= ny; ++m) {
+        const double un = two_theta * u0 - um1;
+        u[m] = un;
+        um1 = u0;
+        u0 = un;
+      }
+      R.mcinv[j] = 1.0 / (s.ay * u[ny]);
+    } else {
+      // rows of T_k / ay: diagonal e_i = 2 theta_k, minus 1 on a Neumann end row
+      double* v = u + (ny + 1);
+      auto e = [&](int i) {
+        double d = two_theta;
+        if (i == 0 && (s.yneu & 1)) d -= 1.0;
+        if (i == ny - 1 && (s.yneu & 2)) d -= 1.0;
+        return d;
+      };
+      u[0] = 1.0;
+      if (ny > 1) u[1] = e(0);
+      for (int m = 1; m + 1 < ny; ++m) u[m + 1] = e(m) * u[m] - u[m - 1];
+      v[ny - 1] = 1.0;
+      if (ny > 1) v[ny - 2] = e(ny - 1);
+      for (int m = ny - 2; m >= 1; --m) v[m - 1] = e(m) * v[m] - v[m + 1];
+      R.mcinv[j] = 1.0 / (s.ay * (e(0) * v[0] - (ny > 1 ? v[1] : 0.0)));
     }
-    R.mcinv[j] = 1.0 / (s.ay * u[ny]);
   }
   // G DOFs
   for (int l = tid; l < R.ng; l += nth) {
@@ -729,6 +758,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
         const int cy = c / nx;
         y = (cy - R.r + 1) * nx + (c - cy * nx);
       }
+      if (s.fixed && s.fixed[i]) g = 0.0;  // fixed DOFs are outside the coarse space
       if (k == 0) { R.ga[l] = g; R.ya[l] = (int16_t)(y < 0 ? 0 : y); }
       else { R.gb[l] = g; R.yb[l] = (int16_t)y; }
     }
@@ -742,11 +772,12 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
     R.cl[sl] = (int16_t)(i >= R.d0 && i < R.d1 ? i - R.d0 : R.nown + cx * FS + a);
     const int first = s.dof_cells[2 * i];
     const bool second = first != c;
-    R.role[sl] = (uint8_t)((second ? 1 : 0) | (s.dof_cells[2 * i + 1] >= 0 ? 2 : 0));
-    R.gself[sl] = s.g0[(size_t)c * T + a];
+    const bool fix = s.fixed && s.fixed[i];
+    R.role[sl] = (uint8_t)((second ? 1 : 0) | (s.dof_cells[2 * i + 1] >= 0 ? 2 : 0) | (fix ? 4 : 0));
+    R.gself[sl] = fix ? 0.0 : s.g0[(size_t)c * T + a];
     const int other = second ? first : s.dof_cells[2 * i + 1];
     const int oslot = second ? s.dof_slot[2 * i] : s.dof_slot[2 * i + 1];
-    R.gnb[sl] = other >= 0 ? s.g0[(size_t)other * T + oslot] : 0.0;
+    R.gnb[sl] = (other >= 0 && !fix) ? s.g0[(size_t)other * T + oslot] : 0.0;
   }
   // DOFs met by one cell only: their second-cell partials stay zero
   for (int64_t i = R.d0 + tid; i < R.d1; i += nth)
@@ -838,7 +869,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
     if (outer > 0) {
       double r2 = 0.0;
       for (int64_t i = R.d0 + tid; i < R.d1; i += nth) {
-        const double v = P.rhs[i] - krow(s, i, P.x);
+        const double v = (s.fixed && s.fixed[i]) ? 0.0 : P.rhs[i] - krow(s, i, P.x);
         w.rfull[i] = v;
         r2 += v * v;
       }
@@ -995,7 +1026,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
   if (outer >= P.max_outer) {
     double r2 = 0.0;
     for (int64_t i = R.d0 + tid; i < R.d1; i += nth) {
-      const double v = P.rhs[i] - krow(s, i, P.x);
+      const double v = (s.fixed && s.fixed[i]) ? 0.0 : P.rhs[i] - krow(s, i, P.x);
       r2 += v * v;
     }
     for (int cx = tid; cx < nx; cx += nth) {
@@ -1027,7 +1058,8 @@ finish:
       const double ls = P.load_scale ? P.load_scale[i] : 0.0;
       l2 += ls * ls;
     };
-    for (int64_t i = R.d0 + tid; i < R.d1; i += nth) row(i);
+    for (int64_t i = R.d0 + tid; i < R.d1; i += nth)
+      if (!(s.fixed && s.fixed[i])) row(i);  // the reduced system's rows only
     for (int cx = tid; cx < nx; cx += nth) row(s.T + R.c0 + cx);
     put_partial(w, 0, d2, red);
     put_partial(w, 1, a2, red);
@@ -1148,7 +1180,8 @@ bool valid(const mhm_skeleton_system* s) {
          s->nx >= 1 && s->ny >= 1 && (int64_t)s->nx * s->ny == s->cells && s->indptr &&
          s->indices && s->values && s->trace_end && s->cell_dofs && s->cell_g0 && s->dof_cells &&
          s->dof_slot && std::isfinite(s->coarse_ax) && std::isfinite(s->coarse_ay) &&
-         s->coarse_ax > 0 && s->coarse_ay > 0 && (!s->cell_blocks || s->block_ld >= s->cell_width);
+         s->coarse_ax > 0 && s->coarse_ay > 0 && (!s->cell_blocks || s->block_ld >= s->cell_width) &&
+         s->coarse_neumann >= 0 && s->coarse_neumann <= 3 && (s->fixed || s->coarse_neumann == 0);
 }
 
 // The Chebyshev values U_m(theta) grow like rho^m, rho = theta + sqrt(theta^2 - 1);
@@ -1190,6 +1223,42 @@ extern "C" int64_t mhm_skeleton_workspace_bytes(const mhm_skeleton_system* s, in
   return (int64_t)layout(s, s->ny).total;
 }
 
+namespace mhm {
+namespace {
+// rhs <- rhs - K xfixed on the free rows (double-double row sums), 0 on the fixed rows
+// (the elimination of prescribed DOFs, core/system.py:421-447).
+__global__ void fixed_rhs_kernel(int64_t size, int64_t trace_size, const int64_t* indptr, const int32_t* indices,
+                                 const double* values, const uint8_t* fixed, const double* xfixed, double* rhs) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < size; i += stride) {
+    if (i < trace_size && fixed[i]) {
+      rhs[i] = 0.0;
+      continue;
+    }
+    double hi = rhs[i], lo = 0.0;
+    for (int64_t e = indptr[i]; e < indptr[i + 1]; ++e) {
+      const double xv = xfixed[indices[e]];
+      if (xv != 0.0) dd_add(hi, lo, -values[e] * xv);
+    }
+    rhs[i] = hi + lo;
+  }
+}
+}  // namespace
+}  // namespace mhm
+
+extern "C" int mhm_skeleton_fixed_rhs(int64_t size, int64_t trace_size, const int64_t* indptr,
+                                      const int32_t* indices, const double* values, const uint8_t* fixed,
+                                      const double* xfixed, double* rhs, void* stream) {
+  if (size < 1 || trace_size < 0 || trace_size > size || !indptr || !indices || !values || !fixed || !xfixed ||
+      !rhs)
+    return MHM_ERR_ARGUMENT;
+  int64_t grid = (size + 255) / 256;
+  if (grid > 148 * 8) grid = 148 * 8;
+  fixed_rhs_kernel<<<(int)grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(size, trace_size, indptr, indices,
+                                                                           values, fixed, xfixed, rhs);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
 extern "C" int mhm_skeleton_solve(const mhm_skeleton_system* s, const double* rhs,
                                   const double* load_scale, double* x, double rtol,
                                   double inner_rtol, int32_t max_inner, int32_t max_outer,
@@ -1209,7 +1278,8 @@ extern "C" int mhm_skeleton_solve(const mhm_skeleton_system* s, const double* rh
   Params P{};
   P.s = Sys{s->size, s->trace_size, s->indptr, s->indices, s->values, s->trace_end, s->faces,
             s->face_size, s->cells, s->cell_width, s->cell_dofs, s->cell_g0, s->dof_cells,
-            s->dof_slot, s->nx, s->ny, s->coarse_ax, s->coarse_ay, s->cell_blocks, s->block_ld};
+            s->dof_slot, s->nx, s->ny, s->coarse_ax, s->coarse_ay, s->cell_blocks, s->block_ld,
+            s->fixed, s->fixed ? s->coarse_neumann : 0};
   auto at = [&](size_t o) { return reinterpret_cast<double*>(base + o); };
   P.w.Zf = at(L.Zf);
   P.w.Zs = at(L.Zs);

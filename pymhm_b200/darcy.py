@@ -35,6 +35,8 @@ from .topology import (
     FaceSpace,
     SkeletonSpace,
     boundary_data,
+    neumann_fixed,
+    neumann_sides,
     coarse_coefficients,
     coupling_tables,
     dof_cell_maps,
@@ -298,8 +300,8 @@ class CartesianQ1Plan:
     (new coefficients or sources on the same mesh) allocate nothing.
     """
 
-    def __init__(self, mesh, skeleton=None, local_refinement=4, *, dirichlet=0.0, quadrature_order=4,
-                 degree=1, precision="fp64", device=None, max_refine=None, local_tol=1e-12,
+    def __init__(self, mesh, skeleton=None, local_refinement=4, *, dirichlet=0.0, neumann=None,
+                 quadrature_order=4, degree=1, precision="fp64", device=None, max_refine=None, local_tol=1e-12,
                  global_rtol=1e-13, inner_rtol=1e-10, max_inner=5000, max_outer=6, grid=0):
         import torch
 
@@ -338,7 +340,11 @@ class CartesianQ1Plan:
         self.pattern = skeleton_pattern(self.cell_dofs_h, self.T)
         dof_cells, dof_slot = dof_cell_maps(self.cell_dofs_h, self.T)
         g0 = geometric_constraint(m, space_h, space_v)
-        self.boundary_h = boundary_data(sk, dirichlet, self.order)
+        # Neumann faces (whole bottom / top sides): their trace DOFs are prescribed
+        # (boundary_data's `fixed`) and eliminated from the global solve
+        self.neumann_bits = neumann_sides(m, neumann)
+        self.boundary_h = boundary_data(sk, dirichlet, self.order, neumann)
+        fixed_dofs, fixed_values = neumann_fixed(sk, neumann, self.order)
         # ---- device constants ---------------------------------------------------------
         dev = self.device
         f64 = dict(dtype=torch.float64, device=dev)
@@ -405,6 +411,14 @@ class CartesianQ1Plan:
         s.nx, s.ny = m.nx, m.ny
         s.coarse_ax, s.coarse_ay = self.coarse_ab
         s.cell_blocks, s.block_ld = _lib.ptr(self.blocks), self.t + 1
+        self.d_fixed = self.d_xfixed = None
+        if self.neumann_bits:
+            mask = np.zeros(self.T, dtype=np.uint8)
+            mask[fixed_dofs] = 1
+            xfixed = np.zeros(self.N)
+            xfixed[fixed_dofs] = fixed_values
+            self.d_fixed, self.d_xfixed = up(mask, torch.uint8), up(xfixed, torch.float64)
+            s.fixed, s.coarse_neumann = _lib.ptr(self.d_fixed), self.neumann_bits
         nbytes = self.lib.mhm_skeleton_workspace_bytes(s, self.grid)
         if nbytes <= 0:
             raise RuntimeError("could not size the skeleton solver workspace")
@@ -507,6 +521,10 @@ class CartesianQ1Plan:
                                           P(self.d_load_ptr), P(self.d_load_contrib), P(self.loads),
                                           P(self.d_boundary), P(self.rhs), P(self.load_scale), s),
                    "mhm_skeleton_scatter")
+        if self.d_fixed is not None:
+            _lib.check(L.mhm_skeleton_fixed_rhs(self.N, self.T, P(self.d_indptr), P(self.d_indices), P(self.values),
+                                                P(self.d_fixed), P(self.d_xfixed), P(self.rhs), s),
+                       "mhm_skeleton_fixed_rhs")
         mark(2, cur)
         if global_stream is not None:
             if not hasattr(self, "_handoff"):
@@ -517,6 +535,8 @@ class CartesianQ1Plan:
                                         self.inner_rtol, self.max_inner, self.max_outer, self.grid,
                                         P(self.workspace), self.workspace.numel(), P(self.info), P(self.stats), gs),
                    "mhm_skeleton_solve")
+        if self.d_xfixed is not None:  # the prescribed Neumann coefficients
+            _lib.check(L.mhm_vector_accumulate(self.N, P(self.x), P(self.d_xfixed), gs), "mhm_vector_accumulate")
         mark(3, gcur)
         if reconstruct:
             _lib.check(L.mhm_q1_reconstruct(self.q1, P(self.solution), P(self.d_cell_dofs), self.T, P(self.x),
@@ -586,6 +606,8 @@ class CartesianQ1Plan:
         return sol
 
     def refine(self, *, max_steps=2, min_steps=0, rtol=1e-10, atol=0.0, stream=None) -> HybridRefinement:
+        if self.d_fixed is not None:
+            raise NotImplementedError("original-equation refinement with Neumann faces is not on the GPU path")
         """Defect correction of the original equations (``refine_hybrid``,
         ``core/refinement.py:612-800``) applied to the plan's last solve.
 
@@ -799,8 +821,10 @@ def solve_darcy_quadrilateral(mesh, *, permeability=1.0, source=0.0, dirichlet=0
                               hybrid_refinement_min_steps=0) -> Q1Solution:
     """GPU counterpart of ``solve_darcy_quadrilateral`` (``cartesian.py:86-168``).
 
-    Weak Dirichlet data on every boundary face; pure-Neumann gauges and Neumann
-    faces are rejected with ``NotImplementedError`` (not on this path).  The
+    Weak Dirichlet data on the faces not listed in ``neumann``; Neumann data (outward
+    normal fluxes) on whole bottom and/or top sides prescribes those faces' trace
+    coefficients, which the global solve eliminates.  Other Neumann face sets,
+    including the pure-Neumann case with its gauge, raise ``NotImplementedError``.  The
     ``solver``, ``local_solver``, ``backend`` and ``workers`` arguments are
     accepted for signature compatibility: the whole solve runs on the GPU.
     ``hybrid_refinement_steps`` / ``hybrid_refinement_min_steps`` follow the Darcy
@@ -812,12 +836,10 @@ def solve_darcy_quadrilateral(mesh, *, permeability=1.0, source=0.0, dirichlet=0
     _refinement_steps(hybrid_refinement_min_steps)
     if hybrid_refinement_min_steps > hybrid_refinement_steps:
         raise ValueError("hybrid_refinement_min_steps must not exceed hybrid_refinement_steps")
-    if neumann:
-        raise NotImplementedError("Neumann faces are not on the GPU path")
     del mean_pressure, solver, local_solver, backend, workers
     order = max(int(quadrature_order), int(degree) + 1)
-    plan = CartesianQ1Plan(mesh, skeleton, local_refinement, dirichlet=dirichlet, quadrature_order=order,
-                           degree=degree, precision=precision)
+    plan = CartesianQ1Plan(mesh, skeleton, local_refinement, dirichlet=dirichlet, neumann=neumann,
+                           quadrature_order=order, degree=degree, precision=precision)
     sol = plan.solve(permeability, source)
     if hybrid_refinement_steps:
         sol = plan.refine(max_steps=hybrid_refinement_steps, min_steps=hybrid_refinement_min_steps).solution

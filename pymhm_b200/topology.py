@@ -343,14 +343,31 @@ def _neumaier_moments(basis: np.ndarray, weights: np.ndarray, values: np.ndarray
     return out
 
 
-def boundary_data(skeleton: SkeletonSpace, dirichlet=0.0, order: int = 4) -> np.ndarray:
-    """Weak Dirichlet trace load (``fem/scalar/operators.py:247-321``, no Neumann faces)."""
+def _neumann_faces(skeleton: SkeletonSpace, neumann) -> dict:
+    neumann = {} if neumann is None else neumann
+    if not isinstance(neumann, dict):
+        raise ValueError("Neumann data must map boundary faces to prescribed fields")
+    boundary = set(int(f) for f in skeleton.mesh.boundary_faces)
+    faces = {}
+    for face, data in neumann.items():
+        if isinstance(face, bool) or not isinstance(face, (int, np.integer)) or int(face) not in boundary:
+            raise ValueError("Neumann data may only be imposed on boundary faces")
+        faces[int(face)] = data
+    return faces
+
+
+def boundary_data(skeleton: SkeletonSpace, dirichlet=0.0, order: int = 4, neumann=None) -> np.ndarray:
+    """Weak Dirichlet trace load on the faces without Neumann data
+    (``fem/scalar/operators.py:247-321``)."""
     load = np.zeros(skeleton.size)
+    neumann = _neumann_faces(skeleton, neumann)
     if not callable(dirichlet) and float(dirichlet) == 0.0:
         return load
     mesh = skeleton.mesh
     lengths = mesh.lengths
     for face in mesh.boundary_faces:
+        if int(face) in neumann:
+            continue
         space = skeleton.faces[face]
         t, w = space.quadrature(max(order, max(space.degrees) + 2))
         start, end = mesh.points[mesh.faces[face]]
@@ -359,6 +376,55 @@ def boundary_data(skeleton: SkeletonSpace, dirichlet=0.0, order: int = 4) -> np.
         vals = np.broadcast_to(np.asarray(vals, dtype=float), (len(pts),))
         load[skeleton.dofs(int(face))] = _neumaier_moments(space.evaluate(t), w, vals) * lengths[face]
     return load
+
+
+def neumann_fixed(skeleton: SkeletonSpace, neumann, order: int = 4) -> tuple[np.ndarray, np.ndarray]:
+    """Prescribed trace coefficients of the Neumann faces (``boundary_data``'s ``fixed``,
+    ``fem/scalar/operators.py:286-316``): the L2 projection of the outward normal flux
+    onto each face's trace basis, with the compensated boundary moments."""
+    neumann = _neumann_faces(skeleton, neumann)
+    dofs, values = [], []
+    mesh = skeleton.mesh
+    for face in mesh.boundary_faces:
+        if int(face) not in neumann:
+            continue
+        space = skeleton.faces[face]
+        t, w = space.quadrature(max(order, max(space.degrees) + 2))
+        start, end = mesh.points[mesh.faces[face]]
+        pts = start + t[:, None] * (end - start)
+        data = neumann[int(face)]
+        vals = np.broadcast_to(np.asarray(data(pts) if callable(data) else data, dtype=float), (len(pts),))
+        if not np.all(np.isfinite(vals)):
+            raise ValueError("scalar coefficient must be finite")
+        basis = space.evaluate(t)
+        moments = _neumaier_moments(basis, w, vals)
+        coef = np.linalg.solve(basis.T @ (w[:, None] * basis), moments)
+        dofs.append(skeleton.dofs(int(face)))
+        values.append(coef)
+    if not dofs:
+        return np.zeros(0, dtype=np.int64), np.zeros(0)
+    return np.concatenate(dofs).astype(np.int64), np.concatenate(values)
+
+
+def neumann_sides(mesh, neumann) -> int:
+    """Which whole sides the Neumann faces cover: bit 0 the bottom (y = y0), bit 1 the
+    top.  The global solver's coarse operator takes those as Neumann ends in y; any
+    other set of Neumann faces (left or right faces, part of a side, every boundary
+    face) is outside this path."""
+    faces = set(int(f) for f in (neumann or {}))
+    if not faces:
+        return 0
+    x0, x1, y0, y1 = mesh.bounds
+    pts = mesh.points[mesh.faces[mesh.boundary_faces]]
+    ys = pts[:, :, 1]
+    bottom = set(int(f) for f in mesh.boundary_faces[np.all(ys == y0, axis=1)])
+    top = set(int(f) for f in mesh.boundary_faces[np.all(ys == y1, axis=1)])
+    bits = (1 if bottom <= faces else 0) | (2 if top <= faces else 0)
+    covered = (bottom if bits & 1 else set()) | (top if bits & 2 else set())
+    if faces != covered:
+        raise NotImplementedError("Neumann data is supported on whole bottom and top sides only "
+                                  "(the global solver's coarse operator takes them as Neumann ends)")
+    return bits
 
 
 # ----------------------------------------------------------------------------------------

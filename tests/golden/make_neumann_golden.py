@@ -1,0 +1,73 @@
+"""Write golden fixtures with Neumann faces on whole bottom/top sides, by running PyMHM
+itself: ``boundary_data`` prescribes those faces' trace coefficients (the L2
+projection of the outward normal flux) and ``HybridSystem.solve(fixed=...)``
+eliminates them, as ``solve_darcy_quadrilateral`` does (``_legacy/models/darcy/
+cartesian.py:122-143``, ``core/system.py:421-447``).
+
+    PYMHM_SRC=/path/to/pymhm/src python tests/golden/make_neumann_golden.py
+
+Reuses the imports of ``make_golden`` (and its Basix shim).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from make_golden import (HERE, CartesianCellField, CartesianMacroMesh, FaceSpace, HybridSystem,
+                         QuadrilateralDarcySolution, SkeletonSpace, _assemble_quad, _QuadTask, boundary_data,
+                         lognormal_permeability, sine_source)
+
+
+def side_faces(mesh, y):
+    faces = [int(f) for f in mesh.boundary_faces if np.all(mesh.points[mesh.faces[f]][:, 1] == y)]
+    return faces
+
+
+def pressure_drop(x):
+    return 1.0 - x[:, 0]
+
+
+def bottom_flux(x):
+    return 0.5 + x[:, 0]
+
+
+def run(name, mesh, face_space, refinement, permeability, source, dirichlet, neumann):
+    sk = SkeletonSpace(mesh, (face_space,) * len(mesh.faces))
+    order = 4
+    boundary, fixed = boundary_data(sk, dirichlet, neumann, order=order)
+    tasks = [_QuadTask(mesh, c, refinement, sk, 1, permeability, source, order) for c in range(len(mesh.cells))]
+    system = HybridSystem.from_local_factory(_assemble_quad, tasks, boundary_load=boundary)
+    hybrid = system.solve(fixed=fixed)
+    fines = [meta[0] for meta in system.local_metadata]
+    sol = QuadrilateralDarcySolution(sk, tuple(fines), hybrid.fields, (), hybrid, permeability, source, 1, order)
+    flux = np.array([sol.evaluate(c, f.points[f.cells].mean(axis=1))[1] for c, f in enumerate(fines)])
+    A = system.matrix.tocsc()
+    keys = np.array(sorted(fixed), dtype=np.int64)
+    return dict(
+        boundary=boundary, fixed_dofs=keys, fixed_values=np.array([fixed[k] for k in keys]),
+        neumann_faces=np.array(sorted(neumann), dtype=np.int64),
+        indptr=A.indptr, indices=A.indices, data=A.data, rhs=system.rhs, load_scale=system.load_scale,
+        trace=hybrid.trace, coarse=np.concatenate(hybrid.coarse), residual=hybrid.residual,
+        fields=np.array(hybrid.fields), flux=flux,
+    ), name
+
+
+def main():
+    mesh = CartesianMacroMesh(4)
+    kap = lognormal_permeability(32, 32, sigma=2.0, ell=0.1, seed=31)
+    field = CartesianCellField(kap, spacing=(1 / 32, 1 / 32))
+    walls = {f: 0.0 for f in side_faces(mesh, 0.0) + side_faces(mesh, 1.0)}
+    out, name = run("darcy_4x4_r8_p2_noflow_tb", mesh, FaceSpace.uniform(2), (8, 8), field, 1.0, pressure_drop,
+                    walls)
+    out["kappa"] = kap
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    print(name, "fixed", len(out["fixed_dofs"]), "residual", out["residual"])
+    flux_bottom = {f: bottom_flux for f in side_faces(mesh, 0.0)}
+    out, name = run("poisson_4x4_r4_p1_flux_bottom", mesh, FaceSpace.uniform(1), (4, 4), 1.0, sine_source, 0.0,
+                    flux_bottom)
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    print(name, "fixed", len(out["fixed_dofs"]), "residual", out["residual"])
+
+
+if __name__ == "__main__":
+    main()

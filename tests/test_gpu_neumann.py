@@ -1,0 +1,73 @@
+"""GPU parity with Neumann faces on whole bottom/top sides: the prescribed trace DOFs
+are eliminated (mhm_skeleton_fixed_rhs + the masked projected CG with Neumann ends
+of the coarse operator) as PyMHM's solve_hybrid_system does with ``fixed``."""
+
+import numpy as np
+import pytest
+
+from tests._cases import PixelField, load, rel
+from tests.test_oracle_neumann import NEUMANN_CASES, neumann_map
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-10, "mixed": 1e-8}
+
+
+def make_plan(name, precision):
+    from pymhm_b200.darcy import CartesianQ1Plan
+    from pymhm_b200.topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
+
+    g = load(name)
+    deg, ref, perm, src, dr, val = NEUMANN_CASES[name]
+    mesh = CartesianMacroMesh(4)
+    sk = SkeletonSpace(mesh, (FaceSpace.uniform(deg),) * len(mesh.faces))
+    plan = CartesianQ1Plan(mesh, sk, ref, dirichlet=dr, neumann=neumann_map(g, val), precision=precision)
+    kap = PixelField(g["kappa"], (1 / 32, 1 / 32)) if "kappa" in g else 1.0
+    plan.set_coefficients(kap, src)
+    return g, plan
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", list(NEUMANN_CASES))
+def test_neumann_solution_matches_reference(name, precision):
+    g, plan = make_plan(name, precision)
+    plan.launch()
+    sol = plan.result()
+    tol = TOL[precision]
+    assert rel(sol.trace, g["trace"]) <= tol
+    assert rel(sol.coarse, g["coarse"]) <= tol
+    assert rel(sol.fields, g["fields"]) <= tol
+    assert rel(sol.flux, g["flux"]) <= tol
+    # the prescribed coefficients come back exactly
+    assert np.array_equal(sol.trace[g["fixed_dofs"]], g["fixed_values"]) or \
+        np.max(np.abs(sol.trace[g["fixed_dofs"]] - g["fixed_values"])) <= 1e-15
+    assert sol.residual <= 1e-12
+
+
+def test_neumann_online_and_captured_paths():
+    g, plan = make_plan("darcy_4x4_r8_p2_noflow_tb", "fp64")
+    plan.prepare_offline()
+    sol = plan.solve_source(1.0)
+    assert rel(sol.fields, g["fields"]) <= 1e-10
+    plan.capture("condense")
+    plan.replay("condense").synchronize()
+    assert rel(plan.result().fields, g["fields"]) <= 1e-10
+    with pytest.raises(NotImplementedError, match="Neumann"):
+        plan.refine(max_steps=1)
+
+
+def test_driver_accepts_neumann_sides():
+    from pymhm_b200.darcy import solve_darcy_quadrilateral
+    from pymhm_b200.topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
+
+    name = "poisson_4x4_r4_p1_flux_bottom"
+    g = load(name)
+    deg, ref, perm, src, dr, val = NEUMANN_CASES[name]
+    mesh = CartesianMacroMesh(4)
+    sk = SkeletonSpace(mesh, (FaceSpace.uniform(deg),) * len(mesh.faces))
+    sol = solve_darcy_quadrilateral(mesh, skeleton=sk, local_refinement=ref, source=src, dirichlet=dr,
+                                    neumann=neumann_map(g, val))
+    assert rel(sol.fields, g["fields"]) <= 1e-10
+    left = {int(f): 0.0 for f in mesh.boundary_faces if np.all(mesh.points[mesh.faces[f]][:, 0] == 0.0)}
+    with pytest.raises(NotImplementedError):
+        solve_darcy_quadrilateral(mesh, skeleton=sk, local_refinement=ref, neumann=left)
