@@ -25,7 +25,7 @@
  *                          (core/system.py:355-528 -> linalg/linear.py:798)
  *                          for systems without gauges; with
  *   mhm_skeleton_fixed_rhs its elimination of fixed (Neumann) trace DOFs
- *                          (core/system.py:421-447) on whole bottom/top sides.
+ *                          (core/system.py:421-447) on whole sides.
  *   mhm_q1_reconstruct     replaces reconstruct_response (core/reconstruction.py:
  *                          130-141) and the flux samples of
  *                          QuadrilateralDarcySolution.evaluate
@@ -279,10 +279,18 @@ typedef struct mhm_skeleton_system {
      * works on the free DOFs: rhs must hold rhs - K x_fixed with zeros on the
      * fixed rows (mhm_skeleton_fixed_rhs), x is returned zero on them and the
      * caller adds x_fixed.  The fixed DOFs must be all DOFs of the faces of the
-     * whole bottom and/or top side, which the coarse operator takes as Neumann
-     * ends of T_y: coarse_neumann bit 0 = bottom (y = y0), bit 1 = top.         */
+     * whole bottom, top, left and/or right sides (not all four), which the coarse
+     * operator takes as Neumann ends of T_y (coarse_neumann bit 0 = bottom y = y0,
+     * bit 1 = top) and of T_x (bit 2 = left x = x0, bit 3 = right).             */
     const uint8_t* fixed;
     int32_t coarse_neumann;
+    /* With coarse_neumann bit 2 (left side x = x0 fixed) or bit 3 (right side):
+     * the eigenvectors and eigenvalues of T_x with those Neumann ends,
+     * coarse_qx[cell][mode] (nx x nx, orthonormal columns) and coarse_lamx[mode]
+     * (nx), which replace the sine basis.  Ignored otherwise (NULL allowed).
+     * All four sides fixed (the pure-Neumann gauge) is not accepted.           */
+    const double* coarse_qx;
+    const double* coarse_lamx;
 } mhm_skeleton_system;
 
 int64_t mhm_skeleton_workspace_bytes(const mhm_skeleton_system* s /* host */, int32_t grid);

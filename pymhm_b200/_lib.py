@@ -69,6 +69,7 @@ class SkeletonSystem(C.Structure):
         ("coarse_ax", C.c_double), ("coarse_ay", C.c_double),
         ("cell_blocks", C.c_void_p), ("block_ld", C.c_int32),
         ("fixed", C.c_void_p), ("coarse_neumann", C.c_int32),
+        ("coarse_qx", C.c_void_p), ("coarse_lamx", C.c_void_p),
     ]
 
 

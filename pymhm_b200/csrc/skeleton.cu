@@ -77,6 +77,8 @@ struct Sys {
   int ld;
   const uint8_t* fixed;  // T: 1 = fixed trace DOF (null: none)
   int yneu;              // coarse T_y ends: bit 0 bottom, bit 1 top Neumann
+  const double* qx;      // nx x nx eigenvectors [k][i] of the coarse T_x (null: the sine basis)
+  const double* lamx;    // nx eigenvalues of T_x (with qx)
 };
 
 // Row-transformed coarse data of one quantity, layout [mode][row]:
@@ -277,10 +279,13 @@ __host__ __device__ __forceinline__ constexpr int packed(int a, int b) {
 // distinct shared-memory banks.
 __host__ __device__ __forceinline__ constexpr int block_stride(int t) { return (t * (t + 1) / 2) | 1; }
 
-// out(j, i, v): v = sum_k in[j][k] Q[k][i] for j < nin (in[j] in shared memory),
-// i < nx.  Warp w takes columns 4w .. 4w+3 (repeating every 64); lane bits 2-4
-// split k eight ways, reduced by shuffles.
-template <typename F>
+// out(j, i, v): v = sum_k in[j][k] Q[k][i] (TR: Q[i][k]) for j < nin (in[j] in
+// shared memory), i < nx.  Q[cell][mode] holds the coarse T_x eigenvectors, so the
+// forward transform reads it as is and the inverse transposed (the sine basis is
+// symmetric; a host table with Neumann x-ends is not).  Warp w takes columns
+// 4w .. 4w+3 (repeating every 64); lane bits 2-4 split k eight ways, reduced by
+// shuffles.
+template <bool TR = false, typename F>
 __device__ void sine_apply(const Row& R, int nx, int nin, const double* const* in, F out) {
   const int lane = threadIdx.x & 31, q = lane >> 2;
   for (int base = (threadIdx.x >> 5) * 4; base < nx; base += kWarps * 4) {
@@ -290,7 +295,7 @@ __device__ void sine_apply(const Row& R, int nx, int nin, const double* const* i
       const double* qc = R.Q + i;
 #pragma unroll 4
       for (int k = q; k < nx; k += 8) {
-        const double qv = qc[k * R.qs];
+        const double qv = TR ? R.Q[i * R.qs + k] : qc[k * R.qs];
 #pragma unroll
         for (int j = 0; j < 3; ++j)
           if (j < nin) acc[j] = fma(in[j][k], qv, acc[j]);
@@ -332,6 +337,9 @@ __device__ void coarse_rowfwd1(const Sys& s, const Row& R, double* dst) {
 // values; symmetric).  With Neumann ends (whole bottom / top sides fixed) the end
 // rows of T_k lose one neighbour and Tinv_k[i][j] = u_i v_j / C for i <= j, u and v
 // the solutions of the homogeneous recurrence from the bottom and the top end.
+// NEU: the solve may have fixed DOFs (compile-time switch; the Dirichlet-only
+// instantiation carries none of their code).
+template <bool NEU>
 __device__ void mode_solve(const Sys& s, const Row& R, const Coarse& U, double* W) {
   const int ny = s.ny, nx = s.nx;
   for (int j = 0; j < R.nmode; ++j) {
@@ -345,7 +353,7 @@ __device__ void mode_solve(const Sys& s, const Row& R, const Coarse& U, double* 
       R.ucol[iy] = (v0 + v1) + v2;
     }
     __syncthreads();
-    const double* u = R.mcheb + (size_t)j * 2 * (ny + 1);
+    const double* u = R.mcheb + (size_t)j * (NEU ? 2 : 1) * (ny + 1);
     const double* v = u + (ny + 1);
     const double c = R.mcinv[j];
     const int lane8 = threadIdx.x & 7, grp = threadIdx.x >> 3, ngrp = blockDim.x >> 3;
@@ -353,7 +361,7 @@ __device__ void mode_solve(const Sys& s, const Row& R, const Coarse& U, double* 
       const int ir = base + grp;
       double acc = 0.0;
       if (ir < ny) {
-        if (s.yneu == 0) {
+        if (!NEU || s.yneu == 0) {
           const double uir = u[ir], unir = u[ny - 1 - ir];
           for (int iy = lane8; iy < ny; iy += 8)
             acc = fma((ir < iy ? uir * u[ny - 1 - iy] : u[iy] * unir), R.ucol[iy], acc);
@@ -373,6 +381,7 @@ __device__ void mode_solve(const Sys& s, const Row& R, const Coarse& U, double* 
 
 // Coarse solution rows [lo, hi) (clipped to the grid, within r-1 .. r+1) from W
 // into yrow; other slots zero.  Y row = W row Q.
+template <bool NEU>
 __device__ void coarse_rows(const Sys& s, const Row& R, const double* W, int lo, int hi) {
   const int ny = s.ny, nx = s.nx, r0 = R.r - 1;
   if (lo < 0) lo = 0;
@@ -384,7 +393,11 @@ __device__ void coarse_rows(const Sys& s, const Row& R, const double* W, int lo,
   }
   __syncthreads();
   const double* in[3] = {R.wrow, R.wrow + nx, R.wrow + 2 * nx};
-  sine_apply(R, nx, 3, in, [&](int j, int i, double v) { R.yrow[j * nx + i] = v; });
+  auto put = [&](int j, int i, double v) { R.yrow[j * nx + i] = v; };
+  if (NEU && s.qx)
+    sine_apply<true>(R, nx, 3, in, put);  // inverse transform
+  else
+    sine_apply<false>(R, nx, 3, in, put);
   __syncthreads();
 }
 
@@ -393,7 +406,7 @@ __device__ void coarse_rows(const Sys& s, const Row& R, const double* W, int lo,
 // the solved coarse rows r-1 .. r+1 of W (into wrow; rows outside [0, ny) zero)
 // are all loaded in one batch before any of them is used; then the coarse rows Y
 // are formed.  tot receives the partial sums (identical in every CTA).
-template <int NS>
+template <int NS, bool NEU>
 __device__ void phase_begin(const Sys& s, const Work& w, const Row& R, int slot, double (&tot)[NS], double* sh,
                             const double* Xf, const double* Xs, double* out, const double* W) {
   const int nx = s.nx, ny = s.ny, r0 = R.r - 1, tid = threadIdx.x, nth = blockDim.x;
@@ -445,7 +458,11 @@ __device__ void phase_begin(const Sys& s, const Work& w, const Row& R, int slot,
 #pragma unroll
   for (int n = 0; n < NS; ++n) tot[n] = sh[n];
   const double* in[3] = {R.wrow, R.wrow + nx, R.wrow + 2 * nx};
-  sine_apply(R, nx, 3, in, [&](int j, int i, double v) { R.yrow[j * nx + i] = v; });
+  auto put = [&](int j, int i, double v) { R.yrow[j * nx + i] = v; };
+  if (NEU && s.qx)
+    sine_apply<true>(R, nx, 3, in, put);  // inverse transform
+  else
+    sine_apply<false>(R, nx, 3, in, put);
   __syncthreads();
 }
 
@@ -455,7 +472,7 @@ __device__ void phase_begin(const Sys& s, const Work& w, const Row& R, int slot,
 // into the coarse sums of the face: col[(1 + Q) nx + cx] across the face to the
 // neighbour, col[(8 + Q) nx + cx] to the cell itself.  Returns the face's share of
 // v_c . B_c v_c.
-template <int FS, int Q>
+template <int FS, int Q, bool NEU>
 __device__ __forceinline__ double face_rows(const Row& R, const double* blk, int cx, int nx,
                                             const double (&xv)[4 * FS], double* Xf, double* Xs, bool coarse) {
   constexpr int T = 4 * FS;
@@ -472,7 +489,7 @@ __device__ __forceinline__ double face_rows(const Row& R, const double* blk, int
   for (int j = 0; j < FS; ++j) {
     const int idx = (Q * FS + j) * nx + cx;
     dot = fma(xv[Q * FS + j], acc[j], dot);
-    if (Xf) ((R.role[idx] & 1) ? Xs : Xf)[R.gdof[R.cl[idx]]] = (R.role[idx] & 4) ? 0.0 : acc[j];
+    if (Xf) ((R.role[idx] & 1) ? Xs : Xf)[R.gdof[R.cl[idx]]] = (NEU && (R.role[idx] & 4)) ? 0.0 : acc[j];
     if (coarse) {
       self = fma(R.gself[idx], acc[j], self);
       across = fma(R.gnb[idx], acc[j], across);
@@ -490,7 +507,7 @@ __device__ __forceinline__ double face_rows(const Row& R, const double* blk, int
 // sums (see face_rows).  Warp w computes face w % 4 of cells 32 (w / 4) + lane, so
 // every block index is a compile-time constant within a warp.  Returns this
 // thread's part of sum_c v_c . B_c v_c.
-template <int FS>
+template <int FS, bool NEU>
 __device__ double cell_apply(const Sys& s, const Row& R, const double* B, const double* v, double* Xf, double* Xs,
                              bool coarse) {
   constexpr int T = 4 * FS;
@@ -504,10 +521,10 @@ __device__ double cell_apply(const Sys& s, const Row& R, const double* B, const 
 #pragma unroll
     for (int b = 0; b < T; ++b) xv[b] = v[R.cl[b * nx + cx]];
     switch (face) {
-      case 0: dot += face_rows<FS, 0>(R, blk, cx, nx, xv, Xf, Xs, coarse); break;
-      case 1: dot += face_rows<FS, 1>(R, blk, cx, nx, xv, Xf, Xs, coarse); break;
-      case 2: dot += face_rows<FS, 2>(R, blk, cx, nx, xv, Xf, Xs, coarse); break;
-      default: dot += face_rows<FS, 3>(R, blk, cx, nx, xv, Xf, Xs, coarse); break;
+      case 0: dot += face_rows<FS, 0, NEU>(R, blk, cx, nx, xv, Xf, Xs, coarse); break;
+      case 1: dot += face_rows<FS, 1, NEU>(R, blk, cx, nx, xv, Xf, Xs, coarse); break;
+      case 2: dot += face_rows<FS, 2, NEU>(R, blk, cx, nx, xv, Xf, Xs, coarse); break;
+      default: dot += face_rows<FS, 3, NEU>(R, blk, cx, nx, xv, Xf, Xs, coarse); break;
     }
   }
   return dot;
@@ -596,7 +613,7 @@ __device__ void warp_invert(double* a, int t) {
 
 constexpr int kSmemArrays = 23;
 
-__host__ __device__ size_t smem_layout(int nx, int ny, int fs, int t, int grid, size_t* off) {
+__host__ __device__ size_t smem_layout(int nx, int ny, int fs, int t, int grid, bool neu, size_t* off) {
   // a row owns at most 3 nx + 1 faces (row 0); later rows own 2 nx + 1 and add the
   // nx bottom faces of their cells
   const size_t g = (size_t)(3 * nx + 1) * fs;
@@ -613,7 +630,7 @@ __host__ __device__ size_t smem_layout(int nx, int ny, int fs, int t, int grid, 
   take(3 * (size_t)nx * 8);              // 1 yrow
   take(12 * (size_t)nx * 8);             // 2 col
   take(3 * (size_t)nx * 8);              // 3 wrow
-  take(nmode * 2 * (ny + 1) * 8);        // 4 mcheb
+  take(nmode * (neu ? 2 : 1) * (ny + 1) * 8);  // 4 mcheb
   take(nmode * 8);                       // 5 mcinv
   take((size_t)ny * 8);                  // 6 ucol
   take(vec * 8);                         // 7 G vectors (6 g) / setup scratch
@@ -632,7 +649,7 @@ __host__ __device__ size_t smem_layout(int nx, int ny, int fs, int t, int grid, 
   return o;
 }
 
-template <int FS>
+template <int FS, bool NEU>
 __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Params P) {
   constexpr int T = 4 * FS;
   constexpr int np = block_stride(T);
@@ -653,7 +670,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
   do {                 \
     if (!grid_sync(w, epoch)) { status = MHM_SOLVE_BARRIER_TIMEOUT; goto done; } \
   } while (0)
-  if (tid == 0) smem_layout(nx, ny, FS, T, gridDim.x, off);
+  if (tid == 0) smem_layout(nx, ny, FS, T, gridDim.x, NEU, off);
   __syncthreads();
   R.r = blockIdx.x;
   R.c0 = R.r * nx;
@@ -702,16 +719,16 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
   for (int e = tid; e < nx * nx; e += nth) {
     const int k = e / nx, i = e - k * nx;
     const int m = ((k + 1) * (i + 1)) % (2 * (nx + 1));
-    R.Q[k * R.qs + i] = sqrt(2.0 / (nx + 1)) * sinpi((double)m / (double)(nx + 1));
+    R.Q[k * R.qs + i] = (NEU && s.qx) ? s.qx[e] : sqrt(2.0 / (nx + 1)) * sinpi((double)m / (double)(nx + 1));
   }
   // Chebyshev values of this CTA's sine modes: T_k = ay tridiag(-1, 2 theta_k, -1),
   // theta_k = 1 + ax lam_k / (2 ay); U_m(theta_k), m = 0..ny
   for (int j = tid; j < R.nmode; j += nth) {
     const int k = blockIdx.x + j * gridDim.x;
-    double* u = R.mcheb + (size_t)j * 2 * (ny + 1);
-    const double lam = 2.0 - 2.0 * cospi((double)(k + 1) / (double)(nx + 1));
+    double* u = R.mcheb + (size_t)j * (NEU ? 2 : 1) * (ny + 1);
+    const double lam = (NEU && s.lamx) ? s.lamx[k] : 2.0 - 2.0 * cospi((double)(k + 1) / (double)(nx + 1));
     const double two_theta = 2.0 + s.ax * lam / s.ay;
-    if (s.yneu == 0) {
+    if (!NEU || s.yneu == 0) {
       double um1 = 0.0, u0 = 1.0;
       u[0] = 1.0;
       for (int m = 1; m <= ny; ++m) {
@@ -758,7 +775,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
         const int cy = c / nx;
         y = (cy - R.r + 1) * nx + (c - cy * nx);
       }
-      if (s.fixed && s.fixed[i]) g = 0.0;  // fixed DOFs are outside the coarse space
+      if (NEU && s.fixed[i]) g = 0.0;  // fixed DOFs are outside the coarse space
       if (k == 0) { R.ga[l] = g; R.ya[l] = (int16_t)(y < 0 ? 0 : y); }
       else { R.gb[l] = g; R.yb[l] = (int16_t)y; }
     }
@@ -772,7 +789,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
     R.cl[sl] = (int16_t)(i >= R.d0 && i < R.d1 ? i - R.d0 : R.nown + cx * FS + a);
     const int first = s.dof_cells[2 * i];
     const bool second = first != c;
-    const bool fix = s.fixed && s.fixed[i];
+    const bool fix = NEU && s.fixed[i];
     R.role[sl] = (uint8_t)((second ? 1 : 0) | (s.dof_cells[2 * i + 1] >= 0 ? 2 : 0) | (fix ? 4 : 0));
     R.gself[sl] = fix ? 0.0 : s.g0[(size_t)c * T + a];
     const int other = second ? first : s.dof_cells[2 * i + 1];
@@ -869,7 +886,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
     if (outer > 0) {
       double r2 = 0.0;
       for (int64_t i = R.d0 + tid; i < R.d1; i += nth) {
-        const double v = (s.fixed && s.fixed[i]) ? 0.0 : P.rhs[i] - krow(s, i, P.x);
+        const double v = (NEU && s.fixed[i]) ? 0.0 : P.rhs[i] - krow(s, i, P.x);
         w.rfull[i] = v;
         r2 += v * v;
       }
@@ -900,13 +917,13 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       for (int cx = tid; cx < nx; cx += nth) R.col[cx] = w.rfull[s.T + R.c0 + cx];
       coarse_rowfwd1(s, R, w.Ux1);
       SYNC_OR_EXIT();
-      mode_solve(s, R, Cx1, w.Wx1);
+      mode_solve<NEU>(s, R, Cx1, w.Wx1);
       SYNC_OR_EXIT();
       // lambda0 = -G0 (G0^T G0)^-1 r2 on G; cell partials of S lambda0; r1 on G
-      coarse_rows(s, R, w.Wx1, R.r - 1, R.r + 2);
+      coarse_rows<NEU>(s, R, w.Wx1, R.r - 1, R.r + 2);
       for (int l = tid; l < R.ng; l += nth) R.vlam[l] = -g0y(R, l);
       for (int l = tid; l < R.ng; l += nth) R.vt[l] = __ldcg(w.rfull + R.gdof[l]);
-      cell_apply<FS>(s, R, R.Sb, R.vlam, w.Vf, w.Vs, false);
+      cell_apply<FS, NEU>(s, R, R.Sb, R.vlam, w.Vf, w.Vs, false);
       SYNC_OR_EXIT();
       // rhoP = r1 - S lambda0 on G; its coarse data
       read_exchange(R, w.Vf, w.Vs, R.vu);
@@ -915,27 +932,27 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       dof_coarse(s, R, R.vr, nullptr);
       coarse_rowfwd1(s, R, w.Ux1);
       SYNC_OR_EXIT();
-      mode_solve(s, R, Cx1, w.Wx1);
+      mode_solve<NEU>(s, R, Cx1, w.Wx1);
       SYNC_OR_EXIT();
       // r0 = P rhoP; preconditioned partials and their coarse data; |r0|^2
-      coarse_rows(s, R, w.Wx1, R.r - 1, R.r + 2);
+      coarse_rows<NEU>(s, R, w.Wx1, R.r - 1, R.r + 2);
       for (int l = tid; l < R.ng; l += nth) R.vr[l] -= g0y(R, l);
       {
         double r2 = 0.0;
         for (int l = tid; l < R.nown; l += nth) r2 = fma(R.vr[l], R.vr[l], r2);
-        cell_apply<FS>(s, R, R.Pb, R.vr, w.Zf, w.Zs, true);
+        cell_apply<FS, NEU>(s, R, R.Pb, R.vr, w.Zf, w.Zs, true);
         coarse_combine(s, R, w.Uz, nullptr);
         put_partial(w, 0, r2, red);
       }
       SYNC_OR_EXIT();
-      mode_solve(s, R, w.Uz, w.Wz);
+      mode_solve<NEU>(s, R, w.Uz, w.Wz);
       SYNC_OR_EXIT();
       double r0 = 0.0, gam_prev = 1.0, alpha_prev = 1.0;
       int k = 0;
       for (;; ++k) {
         // (1) u = P M^-1 r and w = S u (cell partials) on G; gamma, delta
         double rr[1];
-        phase_begin<1>(s, w, R, 0, rr, sh, w.Zf, w.Zs, R.vt, w.Wz);
+        phase_begin<1, NEU>(s, w, R, 0, rr, sh, w.Zf, w.Zs, R.vt, w.Wz);
         const double rn = sqrt(rr[0]);
         if (!isfinite(rn)) { status = MHM_SOLVE_NONFINITE; break; }
         if (k == 0) {
@@ -950,17 +967,17 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
         double gam = 0.0;
         for (int l = tid; l < R.nown; l += nth) gam = fma(R.vr[l], R.vu[l], gam);
         {
-          const double del = cell_apply<FS>(s, R, R.Sb, R.vu, w.Vf, w.Vs, true);
+          const double del = cell_apply<FS, NEU>(s, R, R.Sb, R.vu, w.Vf, w.Vs, true);
           coarse_combine(s, R, w.Uw, nullptr);
           put_partial2(w, 1, gam, del, red);
         }
         SYNC_OR_EXIT();
-        mode_solve(s, R, w.Uw, w.Ww);
+        mode_solve<NEU>(s, R, w.Uw, w.Ww);
         SYNC_OR_EXIT();
         // (2) step: P S p by recurrence, r -= alpha P S p; preconditioned partials
         {
           double gd[2];
-          phase_begin<2>(s, w, R, 1, gd, sh, w.Vf, w.Vs, R.vt, w.Ww);
+          phase_begin<2, NEU>(s, w, R, 1, gd, sh, w.Vf, w.Vs, R.vt, w.Ww);
           const double g = gd[0], d = gd[1];
           const double beta = k > 0 ? g / gam_prev : 0.0;
           const double pq = k > 0 ? d - beta * g / alpha_prev : d;
@@ -989,35 +1006,35 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
             coarse_rowfwd(s, R, 2, src, dst, shift);
           }
           SYNC_OR_EXIT();
-          mode_solve(s, R, Cx1, w.Wx1);
-          mode_solve(s, R, Cx2, w.Wx2);
+          mode_solve<NEU>(s, R, Cx1, w.Wx1);
+          mode_solve<NEU>(s, R, Cx2, w.Wx2);
           SYNC_OR_EXIT();
-          coarse_rows(s, R, w.Wx1, R.r - 1, R.r + 2);
+          coarse_rows<NEU>(s, R, w.Wx1, R.r - 1, R.r + 2);
           for (int l = tid; l < R.ng; l += nth) R.vr[l] -= g0y(R, l);
-          coarse_rows(s, R, w.Wx2, R.r - 1, R.r + 2);
+          coarse_rows<NEU>(s, R, w.Wx2, R.r - 1, R.r + 2);
           for (int l = tid; l < R.ng; l += nth) R.vps[l] -= g0y(R, l);
         }
         {
           double r2 = 0.0;
           for (int l = tid; l < R.nown; l += nth) r2 = fma(R.vr[l], R.vr[l], r2);
-          cell_apply<FS>(s, R, R.Pb, R.vr, w.Zf, w.Zs, true);
+          cell_apply<FS, NEU>(s, R, R.Pb, R.vr, w.Zf, w.Zs, true);
           coarse_combine(s, R, w.Uz, nullptr);
           put_partial(w, 0, r2, red);
         }
         SYNC_OR_EXIT();
-        mode_solve(s, R, w.Uz, w.Wz);
+        mode_solve<NEU>(s, R, w.Uz, w.Wz);
         SYNC_OR_EXIT();
       }
       total_inner += k;
       if (status != MHM_SOLVE_OK) goto finish;
       // c = (G0^T G0)^-1 G0^T (S lambda - r1): cell partials of S lambda, minus r1
       for (int l = tid; l < R.ng; l += nth) R.vt[l] = __ldcg(w.rfull + R.gdof[l]);
-      cell_apply<FS>(s, R, R.Sb, R.vlam, nullptr, nullptr, true);
+      cell_apply<FS, NEU>(s, R, R.Sb, R.vlam, nullptr, nullptr, true);
       coarse_combine(s, R, w.Uw, R.vt);
       SYNC_OR_EXIT();
-      mode_solve(s, R, w.Uw, w.Ww);
+      mode_solve<NEU>(s, R, w.Uw, w.Ww);
       SYNC_OR_EXIT();
-      coarse_rows(s, R, w.Ww, R.r, R.r + 1);
+      coarse_rows<NEU>(s, R, w.Ww, R.r, R.r + 1);
       for (int l = tid; l < R.nown; l += nth) P.x[R.d0 + l] += R.vlam[l];
       for (int cx = tid; cx < nx; cx += nth) P.x[s.T + R.c0 + cx] += R.yrow[nx + cx];
       SYNC_OR_EXIT();
@@ -1026,7 +1043,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
   if (outer >= P.max_outer) {
     double r2 = 0.0;
     for (int64_t i = R.d0 + tid; i < R.d1; i += nth) {
-      const double v = (s.fixed && s.fixed[i]) ? 0.0 : P.rhs[i] - krow(s, i, P.x);
+      const double v = (NEU && s.fixed[i]) ? 0.0 : P.rhs[i] - krow(s, i, P.x);
       r2 += v * v;
     }
     for (int cx = tid; cx < nx; cx += nth) {
@@ -1059,7 +1076,7 @@ finish:
       l2 += ls * ls;
     };
     for (int64_t i = R.d0 + tid; i < R.d1; i += nth)
-      if (!(s.fixed && s.fixed[i])) row(i);  // the reduced system's rows only
+      if (!(NEU && s.fixed[i])) row(i);  // the reduced system's rows only
     for (int cx = tid; cx < nx; cx += nth) row(s.T + R.c0 + cx);
     put_partial(w, 0, d2, red);
     put_partial(w, 1, a2, red);
@@ -1140,15 +1157,19 @@ Layout layout(const mhm_skeleton_system* s, int grid) {
 
 size_t dyn_smem(const mhm_skeleton_system* s, int grid) {
   size_t off[kSmemArrays + 1];
-  return smem_layout(s->nx, s->ny, s->face_size, s->cell_width, grid, off);
+  return smem_layout(s->nx, s->ny, s->face_size, s->cell_width, grid, s->fixed != nullptr, off);
 }
 
-const void* kernel_for(int fs) {
-  switch (fs) {
-    case 1: return (const void*)skeleton_pcg_kernel<1>;
-    case 2: return (const void*)skeleton_pcg_kernel<2>;
-    case 3: return (const void*)skeleton_pcg_kernel<3>;
-    case 4: return (const void*)skeleton_pcg_kernel<4>;
+const void* kernel_for(int fs, bool neu) {
+  switch (fs * 2 + (neu ? 1 : 0)) {
+    case 2: return (const void*)skeleton_pcg_kernel<1, false>;
+    case 3: return (const void*)skeleton_pcg_kernel<1, true>;
+    case 4: return (const void*)skeleton_pcg_kernel<2, false>;
+    case 5: return (const void*)skeleton_pcg_kernel<2, true>;
+    case 6: return (const void*)skeleton_pcg_kernel<3, false>;
+    case 7: return (const void*)skeleton_pcg_kernel<3, true>;
+    case 8: return (const void*)skeleton_pcg_kernel<4, false>;
+    case 9: return (const void*)skeleton_pcg_kernel<4, true>;
     default: return nullptr;
   }
 }
@@ -1157,7 +1178,7 @@ const void* kernel_for(int fs) {
 // Local DOF indices are int16 and the DOF ids int32.
 int resolve_grid(const mhm_skeleton_system* s) {
   int dev = 0, sms = 0, per_sm = 0;
-  const void* kern = kernel_for(s->face_size);
+  const void* kern = kernel_for(s->face_size, s->fixed != nullptr);
   if (!kern) return 0;
   if ((int64_t)(3 * (int64_t)s->nx + 1) * s->face_size > 32767 || s->trace_size > INT32_MAX) return 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return -1;
@@ -1181,7 +1202,8 @@ bool valid(const mhm_skeleton_system* s) {
          s->indices && s->values && s->trace_end && s->cell_dofs && s->cell_g0 && s->dof_cells &&
          s->dof_slot && std::isfinite(s->coarse_ax) && std::isfinite(s->coarse_ay) &&
          s->coarse_ax > 0 && s->coarse_ay > 0 && (!s->cell_blocks || s->block_ld >= s->cell_width) &&
-         s->coarse_neumann >= 0 && s->coarse_neumann <= 3 && (s->fixed || s->coarse_neumann == 0);
+         s->coarse_neumann >= 0 && s->coarse_neumann < 15 && (s->fixed || s->coarse_neumann == 0) &&
+         (!(s->coarse_neumann & 12) || (s->coarse_qx && s->coarse_lamx));
 }
 
 // The Chebyshev values U_m(theta) grow like rho^m, rho = theta + sqrt(theta^2 - 1);
@@ -1279,7 +1301,9 @@ extern "C" int mhm_skeleton_solve(const mhm_skeleton_system* s, const double* rh
   P.s = Sys{s->size, s->trace_size, s->indptr, s->indices, s->values, s->trace_end, s->faces,
             s->face_size, s->cells, s->cell_width, s->cell_dofs, s->cell_g0, s->dof_cells,
             s->dof_slot, s->nx, s->ny, s->coarse_ax, s->coarse_ay, s->cell_blocks, s->block_ld,
-            s->fixed, s->fixed ? s->coarse_neumann : 0};
+            s->fixed, s->fixed ? (s->coarse_neumann & 3) : 0,
+            (s->fixed && (s->coarse_neumann & 12)) ? s->coarse_qx : nullptr,
+            (s->fixed && (s->coarse_neumann & 12)) ? s->coarse_lamx : nullptr};
   auto at = [&](size_t o) { return reinterpret_cast<double*>(base + o); };
   P.w.Zf = at(L.Zf);
   P.w.Zs = at(L.Zs);
@@ -1304,7 +1328,7 @@ extern "C" int mhm_skeleton_solve(const mhm_skeleton_system* s, const double* rh
   if (cudaMemsetAsync(base + L.bar, 0, L.total - L.bar, st) != cudaSuccess) return MHM_ERR_LAUNCH;
   if (cudaMemsetAsync(stats, 0, 4 * sizeof(double), st) != cudaSuccess) return MHM_ERR_LAUNCH;
   void* args[] = {&P};
-  cudaError_t e = cudaLaunchCooperativeKernel(kernel_for(s->face_size), dim3(g), dim3(kSolveThreads),
+  cudaError_t e = cudaLaunchCooperativeKernel(kernel_for(s->face_size, s->fixed != nullptr), dim3(g), dim3(kSolveThreads),
                                               args, dyn_smem(s, g), st);
   return e == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }

@@ -35,6 +35,7 @@ from .topology import (
     FaceSpace,
     SkeletonSpace,
     boundary_data,
+    coarse_x_basis,
     neumann_fixed,
     neumann_sides,
     coarse_coefficients,
@@ -419,6 +420,10 @@ class CartesianQ1Plan:
             xfixed[fixed_dofs] = fixed_values
             self.d_fixed, self.d_xfixed = up(mask, torch.uint8), up(xfixed, torch.float64)
             s.fixed, s.coarse_neumann = _lib.ptr(self.d_fixed), self.neumann_bits
+            if self.neumann_bits & 12:  # Neumann left/right sides: T_x eigenbasis from the host
+                qx, lamx = coarse_x_basis(m.nx, self.neumann_bits)
+                self.d_qx, self.d_lamx = up(qx, torch.float64), up(lamx, torch.float64)
+                s.coarse_qx, s.coarse_lamx = _lib.ptr(self.d_qx), _lib.ptr(self.d_lamx)
         nbytes = self.lib.mhm_skeleton_workspace_bytes(s, self.grid)
         if nbytes <= 0:
             raise RuntimeError("could not size the skeleton solver workspace")
@@ -822,9 +827,9 @@ def solve_darcy_quadrilateral(mesh, *, permeability=1.0, source=0.0, dirichlet=0
     """GPU counterpart of ``solve_darcy_quadrilateral`` (``cartesian.py:86-168``).
 
     Weak Dirichlet data on the faces not listed in ``neumann``; Neumann data (outward
-    normal fluxes) on whole bottom and/or top sides prescribes those faces' trace
-    coefficients, which the global solve eliminates.  Other Neumann face sets,
-    including the pure-Neumann case with its gauge, raise ``NotImplementedError``.  The
+    normal fluxes) on whole sides of the domain prescribes those faces' trace
+    coefficients, which the global solve eliminates.  Parts of sides and the
+    pure-Neumann case with its gauge raise ``NotImplementedError``.  The
     ``solver``, ``local_solver``, ``backend`` and ``workers`` arguments are
     accepted for signature compatibility: the whole solve runs on the GPU.
     ``hybrid_refinement_steps`` / ``hybrid_refinement_min_steps`` follow the Darcy

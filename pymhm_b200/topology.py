@@ -408,23 +408,43 @@ def neumann_fixed(skeleton: SkeletonSpace, neumann, order: int = 4) -> tuple[np.
 
 def neumann_sides(mesh, neumann) -> int:
     """Which whole sides the Neumann faces cover: bit 0 the bottom (y = y0), bit 1 the
-    top.  The global solver's coarse operator takes those as Neumann ends in y; any
-    other set of Neumann faces (left or right faces, part of a side, every boundary
-    face) is outside this path."""
+    top, bit 2 the left (x = x0), bit 3 the right.  The global solver's coarse operator
+    takes those as Neumann ends of its 1-D factors.  Any other set of Neumann faces
+    (part of a side) and the pure-Neumann case (all four sides, which needs the
+    reference's mean-pressure gauge) are outside this path."""
     faces = set(int(f) for f in (neumann or {}))
     if not faces:
         return 0
     x0, x1, y0, y1 = mesh.bounds
     pts = mesh.points[mesh.faces[mesh.boundary_faces]]
-    ys = pts[:, :, 1]
-    bottom = set(int(f) for f in mesh.boundary_faces[np.all(ys == y0, axis=1)])
-    top = set(int(f) for f in mesh.boundary_faces[np.all(ys == y1, axis=1)])
-    bits = (1 if bottom <= faces else 0) | (2 if top <= faces else 0)
-    covered = (bottom if bits & 1 else set()) | (top if bits & 2 else set())
+    xs, ys = pts[:, :, 0], pts[:, :, 1]
+    sides = [set(int(f) for f in mesh.boundary_faces[np.all(c == v, axis=1)])
+             for c, v in ((ys, y0), (ys, y1), (xs, x0), (xs, x1))]
+    bits, covered = 0, set()
+    for bit, side in enumerate(sides):
+        if side <= faces:
+            bits |= 1 << bit
+            covered |= side
     if faces != covered:
-        raise NotImplementedError("Neumann data is supported on whole bottom and top sides only "
+        raise NotImplementedError("Neumann data is supported on whole sides of the domain only "
                                   "(the global solver's coarse operator takes them as Neumann ends)")
+    if bits == 15:
+        raise NotImplementedError("pure-Neumann problems (every boundary face) need the mean-pressure gauge, "
+                                  "which is not on the GPU path")
     return bits
+
+
+def coarse_x_basis(nx: int, bits: int) -> tuple[np.ndarray, np.ndarray]:
+    """Eigenvectors [cell][mode] and eigenvalues of the coarse operator's x factor
+    tridiag(-1, 2, -1) of order nx whose end rows lose a neighbour on a Neumann left
+    (bit 2) or right (bit 3) side."""
+    t = 2.0 * np.eye(nx) - np.eye(nx, k=1) - np.eye(nx, k=-1)
+    if bits & 4:
+        t[0, 0] -= 1.0
+    if bits & 8:
+        t[-1, -1] -= 1.0
+    lam, vec = np.linalg.eigh(t)
+    return np.ascontiguousarray(vec), np.maximum(lam, 0.0)
 
 
 # ----------------------------------------------------------------------------------------

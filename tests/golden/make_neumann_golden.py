@@ -18,9 +18,9 @@ from make_golden import (HERE, CartesianCellField, CartesianMacroMesh, FaceSpace
                          lognormal_permeability, sine_source)
 
 
-def side_faces(mesh, y):
-    faces = [int(f) for f in mesh.boundary_faces if np.all(mesh.points[mesh.faces[f]][:, 1] == y)]
-    return faces
+def side_faces(mesh, y=None, x=None):
+    axis, value = (1, y) if x is None else (0, x)
+    return [int(f) for f in mesh.boundary_faces if np.all(mesh.points[mesh.faces[f]][:, axis] == value)]
 
 
 def pressure_drop(x):
@@ -29,6 +29,14 @@ def pressure_drop(x):
 
 def bottom_flux(x):
     return 0.5 + x[:, 0]
+
+
+def vertical_drop(x):
+    return 1.0 - x[:, 1]
+
+
+def left_flux(x):
+    return 0.3 - 0.2 * x[:, 1]
 
 
 def run(name, mesh, face_space, refinement, permeability, source, dirichlet, neumann):
@@ -65,6 +73,18 @@ def main():
     flux_bottom = {f: bottom_flux for f in side_faces(mesh, 0.0)}
     out, name = run("poisson_4x4_r4_p1_flux_bottom", mesh, FaceSpace.uniform(1), (4, 4), 1.0, sine_source, 0.0,
                     flux_bottom)
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    print(name, "fixed", len(out["fixed_dofs"]), "residual", out["residual"])
+    walls = {f: 0.0 for f in side_faces(mesh, x=0.0) + side_faces(mesh, x=1.0)}
+    out, name = run("darcy_4x4_r8_p2_noflow_lr", mesh, FaceSpace.uniform(2), (8, 8), field, 1.0, vertical_drop,
+                    walls)
+    out["kappa"] = kap
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    print(name, "fixed", len(out["fixed_dofs"]), "residual", out["residual"])
+    mixed = {f: left_flux for f in side_faces(mesh, x=0.0)}
+    mixed.update({f: bottom_flux for f in side_faces(mesh, 0.0)})
+    out, name = run("poisson_4x4_r4_p1_flux_left_bottom", mesh, FaceSpace.uniform(1), (4, 4), 1.0, sine_source,
+                    0.0, mixed)
     np.savez_compressed(HERE / f"{name}.npz", **out)
     print(name, "fixed", len(out["fixed_dofs"]), "residual", out["residual"])
 

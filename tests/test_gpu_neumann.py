@@ -21,7 +21,7 @@ def make_plan(name, precision):
     deg, ref, perm, src, dr, val = NEUMANN_CASES[name]
     mesh = CartesianMacroMesh(4)
     sk = SkeletonSpace(mesh, (FaceSpace.uniform(deg),) * len(mesh.faces))
-    plan = CartesianQ1Plan(mesh, sk, ref, dirichlet=dr, neumann=neumann_map(g, val), precision=precision)
+    plan = CartesianQ1Plan(mesh, sk, ref, dirichlet=dr, neumann=neumann_map(g, val, mesh), precision=precision)
     kap = PixelField(g["kappa"], (1 / 32, 1 / 32)) if "kappa" in g else 1.0
     plan.set_coefficients(kap, src)
     return g, plan
@@ -66,8 +66,8 @@ def test_driver_accepts_neumann_sides():
     mesh = CartesianMacroMesh(4)
     sk = SkeletonSpace(mesh, (FaceSpace.uniform(deg),) * len(mesh.faces))
     sol = solve_darcy_quadrilateral(mesh, skeleton=sk, local_refinement=ref, source=src, dirichlet=dr,
-                                    neumann=neumann_map(g, val))
+                                    neumann=neumann_map(g, val, mesh))
     assert rel(sol.fields, g["fields"]) <= 1e-10
-    left = {int(f): 0.0 for f in mesh.boundary_faces if np.all(mesh.points[mesh.faces[f]][:, 0] == 0.0)}
-    with pytest.raises(NotImplementedError):
-        solve_darcy_quadrilateral(mesh, skeleton=sk, local_refinement=ref, neumann=left)
+    everywhere = {int(f): 0.0 for f in mesh.boundary_faces}
+    with pytest.raises(NotImplementedError, match="pure-Neumann"):
+        solve_darcy_quadrilateral(mesh, skeleton=sk, local_refinement=ref, neumann=everywhere)

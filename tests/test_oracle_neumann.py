@@ -8,16 +8,44 @@ from oracle import q1_mhm as o
 from tests._cases import load, rel
 from pymhm_b200.workloads import sine_source
 
+def _bottom_flux(x):
+    return 0.5 + x[:, 0]
+
+
+def _left_flux(x):
+    return 0.3 - 0.2 * x[:, 1]
+
+
+def _kappa(g):
+    return o.PixelField(g["kappa"], (1 / 32, 1 / 32))
+
+
 NEUMANN_CASES = {
-    # name -> (face degree, refinement, permeability(g), source, dirichlet, neumann value)
-    "darcy_4x4_r8_p2_noflow_tb": (2, (8, 8), lambda g: o.PixelField(g["kappa"], (1 / 32, 1 / 32)), 1.0,
-                                  lambda x: 1.0 - x[:, 0], 0.0),
-    "poisson_4x4_r4_p1_flux_bottom": (1, (4, 4), lambda g: 1.0, sine_source, 0.0, lambda x: 0.5 + x[:, 0]),
+    # name -> (face degree, refinement, permeability(g), source, dirichlet,
+    #          Neumann sides: (axis, coordinate) -> outward flux)
+    "darcy_4x4_r8_p2_noflow_tb": (2, (8, 8), _kappa, 1.0, lambda x: 1.0 - x[:, 0], {(1, 0.0): 0.0, (1, 1.0): 0.0}),
+    "poisson_4x4_r4_p1_flux_bottom": (1, (4, 4), lambda g: 1.0, sine_source, 0.0, {(1, 0.0): _bottom_flux}),
+    "darcy_4x4_r8_p2_noflow_lr": (2, (8, 8), _kappa, 1.0, lambda x: 1.0 - x[:, 1], {(0, 0.0): 0.0, (0, 1.0): 0.0}),
+    "poisson_4x4_r4_p1_flux_left_bottom": (1, (4, 4), lambda g: 1.0, sine_source, 0.0,
+                                           {(0, 0.0): _left_flux, (1, 0.0): _bottom_flux}),
 }
 
+SIDE_BITS = {"darcy_4x4_r8_p2_noflow_tb": 3, "poisson_4x4_r4_p1_flux_bottom": 1, "darcy_4x4_r8_p2_noflow_lr": 12,
+             "poisson_4x4_r4_p1_flux_left_bottom": 5}
 
-def neumann_map(g, value):
-    return {int(f): value for f in g["neumann_faces"]}
+
+def neumann_map(g, sides, mesh=None):
+    """The case's Neumann data per face; the faces are the fixture's."""
+    if mesh is None:
+        mesh = o.cartesian_mesh(4)
+    out = {}
+    for f in mesh.boundary_faces:
+        pts = mesh.points[mesh.faces[f]]
+        for (axis, value), data in sides.items():
+            if np.all(pts[:, axis] == value):
+                out[int(f)] = data
+    assert sorted(out) == [int(f) for f in g["neumann_faces"]]
+    return out
 
 
 @pytest.mark.parametrize("name", list(NEUMANN_CASES))
@@ -50,7 +78,7 @@ def test_host_boundary_data_matches_reference(name):
     order = np.argsort(dofs)
     assert np.array_equal(dofs[order], g["fixed_dofs"])
     assert np.allclose(values[order], g["fixed_values"], rtol=0, atol=1e-15)
-    assert neumann_sides(mesh, neu) == (3 if name.startswith("darcy") else 1)
+    assert neumann_sides(mesh, neu) == SIDE_BITS[name]
 
 
 def test_neumann_side_rules():
@@ -63,9 +91,25 @@ def test_neumann_side_rules():
     left = [int(f) for f, p in zip(mesh.boundary_faces, pts) if np.all(p[:, 0] == 0.0)]
     assert neumann_sides(mesh, None) == 0
     assert neumann_sides(mesh, {f: 0.0 for f in top}) == 2
-    with pytest.raises(NotImplementedError, match="whole bottom and top sides"):
+    assert neumann_sides(mesh, {f: 0.0 for f in left}) == 4
+    with pytest.raises(NotImplementedError, match="whole sides"):
         neumann_sides(mesh, {f: 0.0 for f in bottom[:2]})
-    with pytest.raises(NotImplementedError, match="whole bottom and top sides"):
-        neumann_sides(mesh, {f: 0.0 for f in left})
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(NotImplementedError, match="whole sides"):
+        neumann_sides(mesh, {f: 0.0 for f in left + bottom[1:]})
+    with pytest.raises(NotImplementedError, match="pure-Neumann"):
         neumann_sides(mesh, {int(f): 0.0 for f in mesh.boundary_faces})
+
+
+@pytest.mark.parametrize("bits", [4, 8, 12])
+def test_coarse_x_basis_diagonalises_the_neumann_factor(bits):
+    from pymhm_b200.topology import coarse_x_basis
+
+    nx = 7
+    q, lam = coarse_x_basis(nx, bits)
+    t = 2.0 * np.eye(nx) - np.eye(nx, k=1) - np.eye(nx, k=-1)
+    t[0, 0] -= 1.0 if bits & 4 else 0.0
+    t[-1, -1] -= 1.0 if bits & 8 else 0.0
+    assert np.allclose(q.T @ q, np.eye(nx), atol=1e-14)
+    assert np.allclose(q @ np.diag(lam) @ q.T, t, atol=1e-13)
+    # a zero mode only when both x ends are Neumann (the y ends then carry the solve)
+    assert (lam.min() <= 1e-14) == (bits == 12)
