@@ -1,6 +1,7 @@
-"""GPU parity with Neumann faces on whole bottom/top sides: the prescribed trace DOFs
-are eliminated (mhm_skeleton_fixed_rhs + the masked projected CG with Neumann ends
-of the coarse operator) as PyMHM's solve_hybrid_system does with ``fixed``."""
+"""GPU parity with Neumann faces on whole sides of the domain: the prescribed trace
+DOFs are eliminated (mhm_skeleton_fixed_rhs + the masked projected CG with Neumann
+ends of the coarse operator's 1-D factors) as PyMHM's solve_hybrid_system does with
+``fixed``."""
 
 import numpy as np
 import pytest
