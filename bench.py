@@ -754,28 +754,41 @@ def main():
                   x=torch.empty(plan.x.shape, dtype=torch.float64).pin_memory(),
                   status=torch.empty(plan.cell_status.shape, dtype=torch.int32).pin_memory(),
                   info=torch.empty(4, dtype=torch.int32).pin_memory()) for _ in range(2)]
-    kdev = [torch.empty_like(kappa_dev[0]) for _ in range(2)]
+    # two permeability buffers per plan: request k+2 uploads into the one request k
+    # does not read, on an upload stream, while request k computes
+    kdev = [[torch.empty_like(kappa_dev[0]) for _ in range(2)] for _ in range(2)]
     for j in range(2):
-        pl[j].set_device_coefficients(1, kdev[j], (0.0, 0.0, 0.0), 0, None, 1.0)
+        pl[j].set_device_coefficients(1, kdev[j][0], (0.0, 0.0, 0.0), 0, None, 1.0)
 
     # results leave on a copy stream per plan: the plan's next local stage waits for
     # its previous solve's compute only, and its next global stage (which rewrites x,
     # fields and flux) for the copies, which have long finished by then
     copy_st = [torch.cuda.Stream(device=dev) for _ in range(2)]
+    upload_st = [torch.cuda.Stream(device=dev) for _ in range(2)]
     copied, status_copied = [None, None], [None, None]
+    local_done = [[None, None], [None, None]]  # [plan][buffer]: the local stage that last read it
 
     def request(k):
-        j = k % 2
+        j, b = k % 2, (k // 2) % 2
         p_, ls, gs, cs, h = pl[j], local_st[j], global_st[j], copy_st[j], hosts[j]
+        us = upload_st[j]
+        if local_done[j][b] is not None:
+            us.wait_event(local_done[j][b])
+        with torch.cuda.stream(us):
+            kdev[j][b].copy_(kappa_host, non_blocking=True)
+        uploaded = torch.cuda.Event()
+        uploaded.record(us)
         if getattr(p_, "_done", None) is not None:
-            ls.wait_event(p_._done)  # the previous solve on this plan still reads kappa and its responses
+            ls.wait_event(p_._done)  # the previous solve on this plan still reads its responses
         if status_copied[j] is not None:
             ls.wait_event(status_copied[j])  # the local stage rewrites the cell status words
         if copied[j] is not None:
             gs.wait_event(copied[j])
-        with torch.cuda.stream(ls):
-            kdev[j].copy_(kappa_host, non_blocking=True)
+        ls.wait_event(uploaded)
+        p_.set_device_coefficients(1, kdev[j][b], (0.0, 0.0, 0.0), 0, None, 1.0)
         p_.launch(ls, global_stream=gs)  # records p_._done on gs after the reconstruction
+        local_done[j][b] = torch.cuda.Event()
+        local_done[j][b].record(ls)
         cs.wait_event(p_._done)
         with torch.cuda.stream(cs):
             h["status"].copy_(p_.cell_status, non_blocking=True)
@@ -791,12 +804,12 @@ def main():
 
     def fork_all():
         fork()
-        for cs in copy_st:
+        for cs in copy_st + upload_st:
             cs.wait_stream(stream)
 
     def join_all():
         join()
-        for cs in copy_st:
+        for cs in copy_st + upload_st:
             stream.wait_stream(cs)
 
     fork_all()
