@@ -618,7 +618,8 @@ __host__ __device__ size_t smem_layout(int nx, int ny, int fs, int t, int grid, 
   // nx bottom faces of their cells
   const size_t g = (size_t)(3 * nx + 1) * fs;
   const size_t np = (size_t)block_stride(t);
-  const size_t vec = 6 * g > (size_t)kWarps * t * t ? 6 * g : (size_t)kWarps * t * t;
+  const size_t scratch = (size_t)kWarps * t * (t + 1);  // per warp: a t x t block and t weights
+  const size_t vec = 6 * g > scratch ? 6 * g : scratch;
   const size_t nmode = grid > 0 ? (size_t)((nx + grid - 1) / grid) : 1;
   size_t o = 0;
   int k = 0;
@@ -822,12 +823,23 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
   }
   __syncthreads();
   // preconditioner blocks: D B^-1 D, B = S_c (cell blocks) or the assembled principal
-  // submatrix (D = 1); one warp inverts one cell's block in the setup scratch
+  // submatrix (D = 1); one warp inverts one cell's block in the setup scratch.  The
+  // stiffness weights D of the cell's T slots (a dependent chain of global loads
+  // each) are formed first, one lane per slot.
   {
     const int warp = tid >> 5, lane = tid & 31;
-    double* a = R.scratch + (size_t)warp * T * T;
+    double* a = R.scratch + (size_t)warp * T * (T + 1);
+    double* wts = a + T * T;
     for (int cx = warp; cx < nx; cx += kWarps) {
       const int c = R.c0 + cx;
+      if (s.blocks && lane < T) {
+        const int64_t dof = s.cell_dofs[(size_t)c * T + lane];
+        const int c1 = s.dof_cells[2 * dof], c2 = s.dof_cells[2 * dof + 1];
+        const double d1 = s.blocks[(size_t)c1 * s.ld * s.ld + (size_t)s.dof_slot[2 * dof] * (s.ld + 1)];
+        const double d2 =
+            c2 >= 0 ? s.blocks[(size_t)c2 * s.ld * s.ld + (size_t)s.dof_slot[2 * dof + 1] * (s.ld + 1)] : 0.0;
+        wts[lane] = s.blocks[(size_t)c * s.ld * s.ld + (size_t)lane * (s.ld + 1)] / (d1 + d2);
+      }
       for (int e = lane; e < T * T; e += 32) {
         const int i = e / T, j = e - i * T;
         double v;
@@ -843,19 +855,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
       for (int e = lane; e < T * T; e += 32) {
         const int i = e / T, j = e - i * T;
         if (i > j) continue;
-        double di = 1.0, dj = 1.0;
-        if (s.blocks) {
-          auto weight = [&](int slot) {
-            const int64_t dof = s.cell_dofs[(size_t)c * T + slot];
-            const int c1 = s.dof_cells[2 * dof], c2 = s.dof_cells[2 * dof + 1];
-            const double d1 = s.blocks[(size_t)c1 * s.ld * s.ld + (size_t)s.dof_slot[2 * dof] * (s.ld + 1)];
-            const double d2 =
-                c2 >= 0 ? s.blocks[(size_t)c2 * s.ld * s.ld + (size_t)s.dof_slot[2 * dof + 1] * (s.ld + 1)] : 0.0;
-            return s.blocks[(size_t)c * s.ld * s.ld + (size_t)slot * (s.ld + 1)] / (d1 + d2);
-          };
-          di = weight(i);
-          dj = weight(j);
-        }
+        const double di = s.blocks ? wts[i] : 1.0, dj = s.blocks ? wts[j] : 1.0;
         R.Pb[(size_t)cx * np + packed<T>(i, j)] = di * (0.5 * (a[i * T + j] + a[j * T + i])) * dj;
       }
       __syncwarp();
