@@ -189,14 +189,16 @@ int mhm_q1_source_response(const mhm_q1_problem* p /* host */, int32_t precision
  * defect[cell][i] = f - B lambda - A u (each row in double-double arithmetic),
  * slot_terms[cell][j] = (B^T u)_j, weak[g] = boundary[g] - the DOF's slot terms
  * (first cell, then second; boundary may be NULL = 0), and per cell
- * partial[cell] = {d.d, f.f, sum d}.  p's source and permeability are those of
- * the original problem.
+ * partial[cell] = {d.d, g.g, sum d} with g = f - B lambda_fixed, lambda_fixed
+ * the trace values on the DOFs marked in `fixed` (T bytes; NULL = none, g = f),
+ * refinement.py:704-709.  p's source and permeability are those of the original
+ * problem.
  */
 int mhm_q1_original_defect(const mhm_q1_problem* p /* host */, const int64_t* cell_dofs,
                            int64_t trace_size, const int32_t* dof_cells, const int32_t* dof_slot,
-                           const double* x, const double* fields, const double* boundary,
-                           double* defect, double* slot_terms, double* weak, double* partial,
-                           void* stream);
+                           const uint8_t* fixed, const double* x, const double* fields,
+                           const double* boundary, double* defect, double* slot_terms, double* weak,
+                           double* partial, void* stream);
 
 /*
  * Norms of one refinement step, each summed in a fixed order:
@@ -205,8 +207,9 @@ int mhm_q1_original_defect(const mhm_q1_problem* p /* host */, const int64_t* ce
  * ||rhs||^2 and out[4] = || |K| |x| ||^2 of the assembled CSR system (size rows).
  * out holds 5 + 5 * 256 doubles: the block partials follow the five results.
  */
-int mhm_refine_norms(int32_t cells, const double* partial, int64_t trace_size, const double* weak,
-                     const double* boundary, int64_t size, const int64_t* indptr,
+int mhm_refine_norms(int32_t cells, const double* partial, int64_t trace_size,
+                     const uint8_t* fixed /* NULL: none; fixed DOFs and rows are left out */,
+                     const double* weak, const double* boundary, int64_t size, const int64_t* indptr,
                      const int32_t* indices, const double* values, const double* x,
                      const double* rhs, double* out /* 5 + 1280 */, void* stream);
 
@@ -296,15 +299,15 @@ typedef struct mhm_skeleton_system {
 int64_t mhm_skeleton_workspace_bytes(const mhm_skeleton_system* s /* host */, int32_t grid);
 
 /*
- * Elimination of prescribed trace DOFs before mhm_skeleton_solve, in place:
- * rhs[i] = rhs[i] - sum_j K[i][j] xfixed[j] (double-double row sums) on the free
- * rows, 0 on the fixed ones.  xfixed (N) holds the prescribed values on the fixed
- * trace DOFs and zeros elsewhere; fixed (T bytes) marks them.  K is the CSR of
- * mhm_skeleton_system.
+ * Elimination of prescribed trace DOFs before mhm_skeleton_solve:
+ * reduced[i] = rhs[i] - sum_j K[i][j] xfixed[j] (double-double row sums) on the
+ * free rows, 0 on the fixed ones (reduced may be rhs).  xfixed (N) holds the
+ * prescribed values on the fixed trace DOFs and zeros elsewhere; fixed (T bytes)
+ * marks them.  K is the CSR of mhm_skeleton_system.
  */
 int mhm_skeleton_fixed_rhs(int64_t size, int64_t trace_size, const int64_t* indptr,
                            const int32_t* indices, const double* values, const uint8_t* fixed,
-                           const double* xfixed, double* rhs, void* stream);
+                           const double* xfixed, const double* rhs, double* reduced, void* stream);
 
 /*
  * Solve K x = rhs.  x (N) is output.  info (device int32[4]): status, total

@@ -85,10 +85,10 @@ _SIGNATURES = {
                                          P, P]),
     "mhm_q1_correction_response": (C.c_int, [C.POINTER(Q1Problem), C.c_int32, C.c_int32, C.c_double, P, P, P,
                                              P, P, P, P]),
-    "mhm_q1_original_defect": (C.c_int, [C.POINTER(Q1Problem), P, C.c_int64, P, P, P, P, P, P, P, P, P, P]),
-    "mhm_refine_norms": (C.c_int, [C.c_int32, P, C.c_int64, P, P, C.c_int64, P, P, P, P, P, P, P]),
+    "mhm_q1_original_defect": (C.c_int, [C.POINTER(Q1Problem), P, C.c_int64, P, P, P, P, P, P, P, P, P, P, P]),
+    "mhm_refine_norms": (C.c_int, [C.c_int32, P, C.c_int64, P, P, P, C.c_int64, P, P, P, P, P, P, P]),
     "mhm_vector_accumulate": (C.c_int, [C.c_int64, P, P, P]),
-    "mhm_skeleton_fixed_rhs": (C.c_int, [C.c_int64, C.c_int64, P, P, P, P, P, P, P]),
+    "mhm_skeleton_fixed_rhs": (C.c_int, [C.c_int64, C.c_int64, P, P, P, P, P, P, P, P]),
     "mhm_q1_flux": (C.c_int, [C.POINTER(Q1Problem), P, P, P]),
     "mhm_skeleton_scatter": (C.c_int, [C.c_int64, P, P, P, P, C.c_int64, C.c_int64, P, P, P, P, P, P, P]),
     "mhm_skeleton_workspace_bytes": (C.c_int64, [C.POINTER(SkeletonSystem), C.c_int32]),

@@ -1073,9 +1073,9 @@ __global__ void __launch_bounds__(kThreads) q1_flux_kernel(const Q1Args a, const
 // B^T u per trace slot, also accumulated in double-double; and per cell the sums
 // [d.d, f.f, 1.d].
 __global__ void __launch_bounds__(kThreads) q1_defect_kernel(const Q1Args a, const int64_t* cell_dofs,
-                                                             const double* x, const double* fields,
-                                                             double* defect, double* slot_terms,
-                                                             double* partial) {
+                                                             const uint8_t* fixed, const double* x,
+                                                             const double* fields, double* defect,
+                                                             double* slot_terms, double* partial) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int n = a.n, t = a.t, nnx = a.nnx, ne = a.rx * a.ry, cell = blockIdx.x, tid = threadIdx.x;
   double* kel = reinterpret_cast<double*>(smem);
@@ -1087,22 +1087,31 @@ __global__ void __launch_bounds__(kThreads) q1_defect_kernel(const Q1Args a, con
   double* ctil = fvec + n;
   double* u = ctil + n;
   double* lam = u + n;
-  double* red = lam + t;
+  double* lamf = lam + t;  // lambda on the fixed trace slots, 0 elsewhere
+  double* red = lamf + t;
   double amax, fro, cmax;
   if (a.cut_mode)
     assemble_cell<true>(a, cell, kel, fel, cb, zb, sten, fvec, ctil, amax, fro, cmax);
   else
     assemble_cell<false>(a, cell, kel, fel, cb, zb, sten, fvec, ctil, amax, fro, cmax);
   for (int i = tid; i < n; i += blockDim.x) u[i] = fields[(size_t)cell * n + i];
-  for (int j = tid; j < t; j += blockDim.x) lam[j] = x[cell_dofs[(size_t)cell * t + j]];
+  for (int j = tid; j < t; j += blockDim.x) {
+    const int64_t dof = cell_dofs[(size_t)cell * t + j];
+    lam[j] = x[dof];
+    lamf[j] = (fixed && fixed[dof]) ? x[dof] : 0.0;
+  }
   __syncthreads();
   double d2 = 0.0, f2 = 0.0, d1 = 0.0;
   for (int i = tid; i < n; i += blockDim.x) {
     const int ix = i % nnx, iy = i / nnx;
     double hi = fvec[i], lo = 0.0;
+    double fb = fvec[i];  // the load less the prescribed traces' coupling (refinement.py:704-709)
     for (int j = 0; j < t; ++j) {
       const double bij = rhs_value(a, 1 + j, i, fvec, nullptr, cb);
-      if (bij != 0.0) dd_fma(hi, lo, -bij, lam[j]);
+      if (bij != 0.0) {
+        dd_fma(hi, lo, -bij, lam[j]);
+        fb = fma(-bij, lamf[j], fb);
+      }
     }
     const double* sv = sten + 5 * i;
     dd_fma(hi, lo, -sv[0], u[i]);
@@ -1119,7 +1128,7 @@ __global__ void __launch_bounds__(kThreads) q1_defect_kernel(const Q1Args a, con
     const double d = hi + lo;
     defect[(size_t)cell * n + i] = d;
     d2 = fma(d, d, d2);
-    f2 = fma(fvec[i], fvec[i], f2);
+    f2 = fma(fb, fb, f2);
     d1 += d;
   }
   for (int j = tid; j < t; j += blockDim.x) {
@@ -1169,10 +1178,11 @@ __device__ __forceinline__ void block_range(int64_t n, int64_t& lo, int64_t& hi)
 }
 
 __global__ void __launch_bounds__(256) refine_norms_partial(int cells, const double* partial, int64_t trace_size,
-                                                            const double* weak, const double* boundary,
-                                                            int64_t size, const int64_t* indptr,
-                                                            const int32_t* indices, const double* values,
-                                                            const double* x, const double* rhs, double* blocks) {
+                                                            const uint8_t* fixed, const double* weak,
+                                                            const double* boundary, int64_t size,
+                                                            const int64_t* indptr, const int32_t* indices,
+                                                            const double* values, const double* x,
+                                                            const double* rhs, double* blocks) {
   __shared__ double red[32];
   double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   int64_t lo, hi;
@@ -1184,6 +1194,7 @@ __global__ void __launch_bounds__(256) refine_norms_partial(int cells, const dou
   }
   block_range(trace_size, lo, hi);
   for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    if (fixed && fixed[i]) continue;  // the free trace DOFs' weak equations only
     const double w2 = weak[i] * weak[i];
     v[0] += w2;
     v[2] += w2;
@@ -1193,6 +1204,7 @@ __global__ void __launch_bounds__(256) refine_norms_partial(int cells, const dou
   if (indptr) {
     block_range(size, lo, hi);
     for (int64_t r = lo + threadIdx.x; r < hi; r += blockDim.x) {
+      if (fixed && r < trace_size && fixed[r]) continue;  // active rows
       double acc = 0.0;
       for (int64_t e = indptr[r]; e < indptr[r + 1]; ++e) acc = fma(fabs(values[e]), fabs(x[indices[e]]), acc);
       v[4] = fma(acc, acc, v[4]);
@@ -1443,9 +1455,10 @@ extern "C" int mhm_q1_correction_response(const mhm_q1_problem* p, int32_t preci
 }
 
 extern "C" int mhm_q1_original_defect(const mhm_q1_problem* p, const int64_t* cell_dofs, int64_t trace_size,
-                                      const int32_t* dof_cells, const int32_t* dof_slot, const double* x,
-                                      const double* fields, const double* boundary, double* defect,
-                                      double* slot_terms, double* weak, double* partial, void* stream) {
+                                      const int32_t* dof_cells, const int32_t* dof_slot, const uint8_t* fixed,
+                                      const double* x, const double* fields, const double* boundary,
+                                      double* defect, double* slot_terms, double* weak, double* partial,
+                                      void* stream) {
   Q1Args a;
   int rc = fill_args(p, MHM_PRECISION_FP64, a);
   if (rc != MHM_OK) return rc;
@@ -1453,7 +1466,7 @@ extern "C" int mhm_q1_original_defect(const mhm_q1_problem* p, const int64_t* ce
       !weak || !partial)
     return MHM_ERR_ARGUMENT;
   const int ne = a.rx * a.ry;
-  const size_t smem = ((size_t)7 * ne + (size_t)a.t * a.kmax + a.t + 8 * (size_t)a.n + a.t + 32) * 8;
+  const size_t smem = ((size_t)7 * ne + (size_t)a.t * a.kmax + a.t + 8 * (size_t)a.n + 2 * a.t + 32) * 8;
   if (smem > 227 * 1024) return MHM_ERR_UNSUPPORTED;
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(q1_defect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
@@ -1461,23 +1474,24 @@ extern "C" int mhm_q1_original_defect(const mhm_q1_problem* p, const int64_t* ce
     return MHM_ERR_LAUNCH;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   launch_cut_elements(a, st);
-  q1_defect_kernel<<<a.nx * a.ny, kThreads, smem, st>>>(a, cell_dofs, x, fields, defect, slot_terms, partial);
+  q1_defect_kernel<<<a.nx * a.ny, kThreads, smem, st>>>(a, cell_dofs, fixed, x, fields, defect, slot_terms,
+                                                        partial);
   int blocks = (int)((trace_size + 255) / 256);
   if (blocks > 4096) blocks = 4096;
   weak_residual_kernel<<<blocks, 256, 0, st>>>(trace_size, a.t, dof_cells, dof_slot, slot_terms, boundary, weak);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
 
-extern "C" int mhm_refine_norms(int32_t cells, const double* partial, int64_t trace_size, const double* weak,
-                                const double* boundary, int64_t size, const int64_t* indptr,
+extern "C" int mhm_refine_norms(int32_t cells, const double* partial, int64_t trace_size, const uint8_t* fixed,
+                                const double* weak, const double* boundary, int64_t size, const int64_t* indptr,
                                 const int32_t* indices, const double* values, const double* x,
                                 const double* rhs, double* out, void* stream) {
   if (cells < 1 || !partial || trace_size < 0 || (trace_size > 0 && !weak) || !out) return MHM_ERR_ARGUMENT;
   if (indptr && (size < 1 || !indices || !values || !x || !rhs)) return MHM_ERR_ARGUMENT;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   double* blocks = out + 5;
-  refine_norms_partial<<<kNormBlocks, 256, 0, st>>>(cells, partial, trace_size, weak, boundary, size, indptr, indices,
-                                                    values, x, rhs, blocks);
+  refine_norms_partial<<<kNormBlocks, 256, 0, st>>>(cells, partial, trace_size, fixed, weak, boundary, size, indptr,
+                                                    indices, values, x, rhs, blocks);
   refine_norms_final<<<1, 160, 0, st>>>(kNormBlocks, blocks, out);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }

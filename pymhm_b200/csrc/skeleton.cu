@@ -1247,14 +1247,16 @@ extern "C" int64_t mhm_skeleton_workspace_bytes(const mhm_skeleton_system* s, in
 
 namespace mhm {
 namespace {
-// rhs <- rhs - K xfixed on the free rows (double-double row sums), 0 on the fixed rows
-// (the elimination of prescribed DOFs, core/system.py:421-447).
+// reduced = rhs - K xfixed on the free rows (double-double row sums), 0 on the fixed
+// rows (the elimination of prescribed DOFs, core/system.py:421-447).  One thread per
+// row reads its row before writing it, so reduced may alias rhs.
 __global__ void fixed_rhs_kernel(int64_t size, int64_t trace_size, const int64_t* indptr, const int32_t* indices,
-                                 const double* values, const uint8_t* fixed, const double* xfixed, double* rhs) {
+                                 const double* values, const uint8_t* fixed, const double* xfixed,
+                                 const double* rhs, double* reduced) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < size; i += stride) {
     if (i < trace_size && fixed[i]) {
-      rhs[i] = 0.0;
+      reduced[i] = 0.0;
       continue;
     }
     double hi = rhs[i], lo = 0.0;
@@ -1262,7 +1264,7 @@ __global__ void fixed_rhs_kernel(int64_t size, int64_t trace_size, const int64_t
       const double xv = xfixed[indices[e]];
       if (xv != 0.0) dd_add(hi, lo, -values[e] * xv);
     }
-    rhs[i] = hi + lo;
+    reduced[i] = hi + lo;
   }
 }
 }  // namespace
@@ -1270,14 +1272,14 @@ __global__ void fixed_rhs_kernel(int64_t size, int64_t trace_size, const int64_t
 
 extern "C" int mhm_skeleton_fixed_rhs(int64_t size, int64_t trace_size, const int64_t* indptr,
                                       const int32_t* indices, const double* values, const uint8_t* fixed,
-                                      const double* xfixed, double* rhs, void* stream) {
+                                      const double* xfixed, const double* rhs, double* reduced, void* stream) {
   if (size < 1 || trace_size < 0 || trace_size > size || !indptr || !indices || !values || !fixed || !xfixed ||
-      !rhs)
+      !rhs || !reduced)
     return MHM_ERR_ARGUMENT;
   int64_t grid = (size + 255) / 256;
   if (grid > 148 * 8) grid = 148 * 8;
   fixed_rhs_kernel<<<(int)grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(size, trace_size, indptr, indices,
-                                                                           values, fixed, xfixed, rhs);
+                                                                           values, fixed, xfixed, rhs, reduced);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
 

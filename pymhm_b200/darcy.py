@@ -420,6 +420,7 @@ class CartesianQ1Plan:
             xfixed[fixed_dofs] = fixed_values
             self.d_fixed, self.d_xfixed = up(mask, torch.uint8), up(xfixed, torch.float64)
             s.fixed, s.coarse_neumann = _lib.ptr(self.d_fixed), self.neumann_bits
+            self.rhs_red = torch.empty(self.N, dtype=torch.float64, device=dev)
             if self.neumann_bits & 12:  # Neumann left/right sides: T_x eigenbasis from the host
                 qx, lamx = coarse_x_basis(m.nx, self.neumann_bits)
                 self.d_qx, self.d_lamx = up(qx, torch.float64), up(lamx, torch.float64)
@@ -526,9 +527,9 @@ class CartesianQ1Plan:
                                           P(self.d_load_ptr), P(self.d_load_contrib), P(self.loads),
                                           P(self.d_boundary), P(self.rhs), P(self.load_scale), s),
                    "mhm_skeleton_scatter")
-        if self.d_fixed is not None:
+        if self.d_fixed is not None:  # the global solve sees the reduced right-hand side
             _lib.check(L.mhm_skeleton_fixed_rhs(self.N, self.T, P(self.d_indptr), P(self.d_indices), P(self.values),
-                                                P(self.d_fixed), P(self.d_xfixed), P(self.rhs), s),
+                                                P(self.d_fixed), P(self.d_xfixed), P(self.rhs), P(self.rhs_red), s),
                        "mhm_skeleton_fixed_rhs")
         mark(2, cur)
         if global_stream is not None:
@@ -536,7 +537,8 @@ class CartesianQ1Plan:
                 self._handoff = torch.cuda.Event()
             self._handoff.record(cur)
             global_stream.wait_event(self._handoff)
-        _lib.check(L.mhm_skeleton_solve(self.sys, P(self.rhs), P(self.load_scale), P(self.x), self.global_rtol,
+        _lib.check(L.mhm_skeleton_solve(self.sys, P(self.rhs if self.d_fixed is None else self.rhs_red),
+                                        P(self.load_scale), P(self.x), self.global_rtol,
                                         self.inner_rtol, self.max_inner, self.max_outer, self.grid,
                                         P(self.workspace), self.workspace.numel(), P(self.info), P(self.stats), gs),
                    "mhm_skeleton_solve")
@@ -611,8 +613,6 @@ class CartesianQ1Plan:
         return sol
 
     def refine(self, *, max_steps=2, min_steps=0, rtol=1e-10, atol=0.0, stream=None) -> HybridRefinement:
-        if self.d_fixed is not None:
-            raise NotImplementedError("original-equation refinement with Neumann faces is not on the GPU path")
         """Defect correction of the original equations (``refine_hybrid``,
         ``core/refinement.py:612-800``) applied to the plan's last solve.
 
@@ -630,7 +630,11 @@ class CartesianQ1Plan:
         any ``HybridSolution``); the fluxes are evaluated again from the corrected
         fields.  The source column of the local responses
         then holds the last defect's response.  A residual still above the threshold
-        after ``max_steps`` corrections raises ``LinearSolveError``.
+        after ``max_steps`` corrections raises ``LinearSolveError``.  With Neumann faces
+        the prescribed trace coefficients stay as they are: the right-hand-side norm
+        takes the loads less their coupling and the free DOFs' boundary data, the
+        weak residual counts the free DOFs, and each correction solves with those
+        DOFs held at zero (``refinement.py:676-709, 792``).
         """
         _step_limits(max_steps, min_steps)
         _tolerances(rtol, atol)
@@ -644,6 +648,7 @@ class CartesianQ1Plan:
             self._refine = dict(defect=torch.empty((M, n), **f64), slots=torch.empty((M, t), **f64),
                                 weak=torch.empty(self.T, **f64), partial=torch.empty((M, 3), **f64),
                                 norms=torch.empty(5 + 5 * 256, **f64), dx=torch.empty(self.N, **f64),
+                                zero=torch.zeros(self.N, **f64),
                                 rhs=torch.empty(self.N, **f64), scale=torch.empty(self.N, **f64),
                                 dfields=torch.empty((M, n), **f64))
         B = self._refine
@@ -654,10 +659,12 @@ class CartesianQ1Plan:
         history, step = [], 0
         while True:
             _lib.check(L.mhm_q1_original_defect(self.q1, P(self.d_cell_dofs), self.T, P(self.d_dof_cells),
-                                                P(self.d_dof_slot), P(self.x), P(self.fields), P(self.d_boundary),
-                                                P(B["defect"]), P(B["slots"]), P(B["weak"]), P(B["partial"]), s),
+                                                P(self.d_dof_slot), P(self.d_fixed), P(self.x), P(self.fields),
+                                                P(self.d_boundary), P(B["defect"]), P(B["slots"]), P(B["weak"]),
+                                                P(B["partial"]), s),
                        "mhm_q1_original_defect")
-            _lib.check(L.mhm_refine_norms(M, P(B["partial"]), self.T, P(B["weak"]), P(self.d_boundary), self.N,
+            _lib.check(L.mhm_refine_norms(M, P(B["partial"]), self.T, P(self.d_fixed), P(B["weak"]),
+                                          P(self.d_boundary), self.N,
                                           P(self.d_indptr), P(self.d_indices), P(self.values), P(self.x),
                                           P(self.rhs), P(B["norms"]), s), "mhm_refine_norms")
             cur.synchronize()
@@ -682,6 +689,10 @@ class CartesianQ1Plan:
                                               P(self.values), self.N, self.T, P(self.d_load_ptr),
                                               P(self.d_load_contrib), P(self.loads), P(B["weak"]), P(B["rhs"]),
                                               P(B["scale"]), s), "mhm_skeleton_scatter")
+            if self.d_fixed is not None:  # the correction holds the prescribed DOFs at zero
+                _lib.check(L.mhm_skeleton_fixed_rhs(self.N, self.T, P(self.d_indptr), P(self.d_indices),
+                                                    P(self.values), P(self.d_fixed), P(B["zero"]), P(B["rhs"]),
+                                                    P(B["rhs"]), s), "mhm_skeleton_fixed_rhs")
             _lib.check(L.mhm_skeleton_solve(self.sys, P(B["rhs"]), P(B["scale"]), P(B["dx"]), self.global_rtol,
                                             self.inner_rtol, self.max_inner, self.max_outer, self.grid,
                                             P(self.workspace), self.workspace.numel(), P(self.info), P(self.stats),

@@ -1,8 +1,10 @@
-"""Write golden fixtures with Neumann faces on whole bottom/top sides, by running PyMHM
-itself: ``boundary_data`` prescribes those faces' trace coefficients (the L2
+"""Write golden fixtures with Neumann faces on whole sides of the domain, by running
+PyMHM itself: ``boundary_data`` prescribes those faces' trace coefficients (the L2
 projection of the outward normal flux) and ``HybridSystem.solve(fixed=...)``
 eliminates them, as ``solve_darcy_quadrilateral`` does (``_legacy/models/darcy/
-cartesian.py:122-143``, ``core/system.py:421-447``).
+cartesian.py:122-143``, ``core/system.py:421-447``).  For the left-and-bottom flux
+case it also runs ``refine_hybrid`` with ``fixed`` from a perturbed solution (every
+local field plus 0.002 * (1, ..., n), as the reference's refinement test does).
 
     PYMHM_SRC=/path/to/pymhm/src python tests/golden/make_neumann_golden.py
 
@@ -13,9 +15,12 @@ from __future__ import annotations
 
 import numpy as np
 
+from dataclasses import replace
+
 from make_golden import (HERE, CartesianCellField, CartesianMacroMesh, FaceSpace, HybridSystem,
                          QuadrilateralDarcySolution, SkeletonSpace, _assemble_quad, _QuadTask, boundary_data,
                          lognormal_permeability, sine_source)
+from pymhm.core.refinement import refine_hybrid
 
 
 def side_faces(mesh, y=None, x=None):
@@ -39,13 +44,23 @@ def left_flux(x):
     return 0.3 - 0.2 * x[:, 1]
 
 
-def run(name, mesh, face_space, refinement, permeability, source, dirichlet, neumann):
+def run(name, mesh, face_space, refinement, permeability, source, dirichlet, neumann, refine=False):
     sk = SkeletonSpace(mesh, (face_space,) * len(mesh.faces))
     order = 4
     boundary, fixed = boundary_data(sk, dirichlet, neumann, order=order)
     tasks = [_QuadTask(mesh, c, refinement, sk, 1, permeability, source, order) for c in range(len(mesh.cells))]
     system = HybridSystem.from_local_factory(_assemble_quad, tasks, boundary_load=boundary)
     hybrid = system.solve(fixed=fixed)
+    extra = {}
+    if refine:
+        perturbed = replace(hybrid, fields=tuple(u + 0.002 * np.arange(1, len(u) + 1) for u in hybrid.fields))
+        result = refine_hybrid(system, perturbed, boundary_load=boundary, fixed=fixed, max_steps=2, rtol=1e-10)
+        extra = dict(
+            refine_start_fields=np.array(perturbed.fields), refine_residual_norms=np.array(result.residual_norms),
+            refine_rhs_norm=result.rhs_norm, refine_reduced=result.solution.residual,
+            refine_trace=result.solution.trace, refine_coarse=np.concatenate(result.solution.coarse),
+            refine_fields=np.array(result.solution.fields))
+        print(name, "refinement history", result.residual_norms, "rhs", result.rhs_norm)
     fines = [meta[0] for meta in system.local_metadata]
     sol = QuadrilateralDarcySolution(sk, tuple(fines), hybrid.fields, (), hybrid, permeability, source, 1, order)
     flux = np.array([sol.evaluate(c, f.points[f.cells].mean(axis=1))[1] for c, f in enumerate(fines)])
@@ -56,7 +71,7 @@ def run(name, mesh, face_space, refinement, permeability, source, dirichlet, neu
         neumann_faces=np.array(sorted(neumann), dtype=np.int64),
         indptr=A.indptr, indices=A.indices, data=A.data, rhs=system.rhs, load_scale=system.load_scale,
         trace=hybrid.trace, coarse=np.concatenate(hybrid.coarse), residual=hybrid.residual,
-        fields=np.array(hybrid.fields), flux=flux,
+        fields=np.array(hybrid.fields), flux=flux, **extra,
     ), name
 
 
@@ -84,7 +99,7 @@ def main():
     mixed = {f: left_flux for f in side_faces(mesh, x=0.0)}
     mixed.update({f: bottom_flux for f in side_faces(mesh, 0.0)})
     out, name = run("poisson_4x4_r4_p1_flux_left_bottom", mesh, FaceSpace.uniform(1), (4, 4), 1.0, sine_source,
-                    0.0, mixed)
+                    0.0, mixed, refine=True)
     np.savez_compressed(HERE / f"{name}.npz", **out)
     print(name, "fixed", len(out["fixed_dofs"]), "residual", out["residual"])
 

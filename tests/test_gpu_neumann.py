@@ -53,8 +53,6 @@ def test_neumann_online_and_captured_paths():
     plan.capture("condense")
     plan.replay("condense").synchronize()
     assert rel(plan.result().fields, g["fields"]) <= 1e-10
-    with pytest.raises(NotImplementedError, match="Neumann"):
-        plan.refine(max_steps=1)
 
 
 def test_driver_accepts_neumann_sides():
@@ -72,3 +70,30 @@ def test_driver_accepts_neumann_sides():
     everywhere = {int(f): 0.0 for f in mesh.boundary_faces}
     with pytest.raises(NotImplementedError, match="pure-Neumann"):
         solve_darcy_quadrilateral(mesh, skeleton=sk, local_refinement=ref, neumann=everywhere)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_neumann_refinement_matches_reference(precision):
+    """refine_hybrid with prescribed trace coefficients (core/refinement.py:676-709, 792):
+    the right-hand-side norm takes the loads less the fixed traces' coupling, the weak
+    residual the free DOFs, and the corrections hold the fixed DOFs at zero."""
+    import torch
+
+    name = "poisson_4x4_r4_p1_flux_left_bottom"
+    g, plan = make_plan(name, precision)
+    plan.launch()
+    plan.check()
+    plan.fields.copy_(torch.from_numpy(g["refine_start_fields"].reshape(plan.cells, plan.n)).to(plan.device))
+    out = plan.refine(max_steps=2, rtol=1e-10)
+    hist = np.array(out.residual_norms)
+    ref_hist = g["refine_residual_norms"]
+    assert len(ref_hist) <= len(hist) <= len(ref_hist) + (precision == "mixed")
+    assert abs(hist[0] - ref_hist[0]) <= 1e-12 * ref_hist[0]
+    assert abs(out.rhs_norm - float(g["refine_rhs_norm"])) <= 1e-13 * float(g["refine_rhs_norm"])
+    assert hist[-1] <= 1e-10 * out.rhs_norm
+    sol = out.solution
+    assert rel(sol.trace, g["refine_trace"]) <= 1e-10
+    assert rel(sol.coarse, g["refine_coarse"]) <= 1e-10
+    assert rel(sol.fields, g["refine_fields"]) <= 1e-10
+    # the prescribed coefficients are untouched by the corrections
+    assert np.max(np.abs(sol.trace[g["fixed_dofs"]] - g["fixed_values"])) <= 1e-15

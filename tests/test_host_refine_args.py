@@ -46,10 +46,12 @@ def test_nodal_load_source_mode_and_refinement_entry_points():
     q.source_mode = 4
     assert lib.mhm_q1_condense_smem_bytes(q, 0) == 0
     q.source_mode = 3
-    assert lib.mhm_q1_original_defect(q, None, 1, None, None, None, None, None, None, None, None, None,
+    assert lib.mhm_q1_original_defect(q, None, 1, None, None, None, None, None, None, None, None, None, None,
                                       None) == _lib.MHM_ERR_ARGUMENT
-    assert lib.mhm_refine_norms(0, None, 0, None, None, 0, None, None, None, None, None, None,
+    assert lib.mhm_refine_norms(0, None, 0, None, None, None, 0, None, None, None, None, None, None,
                                 None) == _lib.MHM_ERR_ARGUMENT
+    assert lib.mhm_skeleton_fixed_rhs(0, 0, None, None, None, None, None, None, None,
+                                      None) == _lib.MHM_ERR_ARGUMENT
     assert lib.mhm_vector_accumulate(-1, None, None, None) == _lib.MHM_ERR_ARGUMENT
     assert lib.mhm_vector_accumulate(0, None, None, None) == _lib.MHM_OK
     assert lib.mhm_q1_correction_response(q, 0, 0, 1e-12, None, None, None, None, None, None,
