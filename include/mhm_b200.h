@@ -227,6 +227,18 @@ int mhm_q1_correction_response(const mhm_q1_problem* p /* host */, int32_t preci
                                double* solution, double* loads, uint8_t* corrected,
                                int32_t* cell_status, int32_t* cell_iters, void* stream);
 
+/*
+ * Mean-pressure gauge of a pure-Neumann solve (every boundary side fixed), the
+ * reference's hybrid_mean_constraint with the cells' weights C = M 1
+ * (core/system.py:531-566, _legacy/models/darcy/cartesian.py:136-142): with
+ * s1 = sum_cells C . fields and s2 = sum_cells C . (1 - R A1) (solution column
+ * w-1), adds alpha = (value - s1) / s2 to every coarse unknown x[T + cell].  The
+ * caller reconstructs again.  partial: 2 cells + 1 doubles (the last = alpha).
+ */
+int mhm_q1_mean_gauge(const mhm_q1_problem* p /* host */, const double* solution,
+                      const double* fields, double value, int64_t trace_size, double* x,
+                      double* partial, void* stream);
+
 /* Flux -K grad u at the fine-cell centres from given nodal fields (cells, n):
  * the flux part of mhm_q1_reconstruct (postprocessing/solutions.py:278-324). */
 int mhm_q1_flux(const mhm_q1_problem* p /* host */, const double* fields, double* flux, void* stream);
@@ -282,7 +294,7 @@ typedef struct mhm_skeleton_system {
      * works on the free DOFs: rhs must hold rhs - K x_fixed with zeros on the
      * fixed rows (mhm_skeleton_fixed_rhs), x is returned zero on them and the
      * caller adds x_fixed.  The fixed DOFs must be all DOFs of the faces of the
-     * whole bottom, top, left and/or right sides (not all four), which the coarse
+     * whole bottom, top, left and/or right sides, which the coarse
      * operator takes as Neumann ends of T_y (coarse_neumann bit 0 = bottom y = y0,
      * bit 1 = top) and of T_x (bit 2 = left x = x0, bit 3 = right).             */
     const uint8_t* fixed;
@@ -290,10 +302,14 @@ typedef struct mhm_skeleton_system {
     /* With coarse_neumann bit 2 (left side x = x0 fixed) or bit 3 (right side):
      * the eigenvectors and eigenvalues of T_x with those Neumann ends,
      * coarse_qx[cell][mode] (nx x nx, orthonormal columns) and coarse_lamx[mode]
-     * (nx), which replace the sine basis.  Ignored otherwise (NULL allowed).
-     * All four sides fixed (the pure-Neumann gauge) is not accepted.           */
+     * (nx), which replace the sine basis.  Ignored otherwise (NULL allowed).  */
     const double* coarse_qx;
     const double* coarse_lamx;
+    /* With all four sides fixed (coarse_neumann 15, pure Neumann): the ny x ny
+     * pseudo-inverse of mode 0's T_y (row-major), the constant coarse mode being
+     * the kernel of G0^T G0.  The solve then returns coarse unknowns without that
+     * mode; mhm_q1_mean_gauge fixes it from the mean-pressure condition.        */
+    const double* coarse_pinv0;
 } mhm_skeleton_system;
 
 int64_t mhm_skeleton_workspace_bytes(const mhm_skeleton_system* s /* host */, int32_t grid);

@@ -702,10 +702,23 @@ def assemble_global(contribs, trace_size, boundary_load=None):
     return matrix, rhs, scale
 
 
-def solve_global(matrix, rhs, load_scale, rtol=1e-10, fixed=None):
-    """``solve_hybrid_system`` without gauges (``core/system.py:355-528``): fixed trace
-    DOFs take their prescribed values and leave the system, whose other rows lose the
-    prescribed action (``:421-447``)."""
+def mean_constraint(responses, trace_size, weights, value):
+    """``hybrid_mean_constraint`` (``core/system.py:531-566``): the row r and target b
+    of sum_cells w_c . u_c = value, u_c = source - lifts lambda + retained c."""
+    row = np.zeros(trace_size + len(responses))
+    target = float(value)
+    for c, (r, w) in enumerate(zip(responses, weights)):
+        np.add.at(row, r.problem.trace_dofs, -r.lifts.T @ w)
+        row[trace_size + c] = (r.retained.T @ w)[0]
+        target -= w @ r.source
+    return row, target
+
+
+def solve_global(matrix, rhs, load_scale, rtol=1e-10, fixed=None, constraints=None):
+    """``solve_hybrid_system`` (``core/system.py:355-528``): fixed trace DOFs take their
+    prescribed values and leave the system, whose other rows lose the prescribed
+    action (``:421-447``); constraint rows r.x = b border it with multipliers
+    (``:448-457``), the residual check reading the physical rows only."""
     fixed = {} if fixed is None else fixed
     n = len(rhs)
     x = np.zeros(n)
@@ -715,7 +728,14 @@ def solve_global(matrix, rhs, load_scale, rtol=1e-10, fixed=None):
     reduced = matrix[free][:, free] if len(idx) else matrix
     action = (matrix @ x)[free]
     rrhs = rhs[free] - action
-    x[free] = EquilibratedLU(sparse.csc_matrix(reduced), rtol).solve(rrhs)
+    if constraints:
+        rows = np.array([row for row, _ in constraints])
+        targets = np.array([t for _, t in constraints]) - rows @ x
+        bordered = sparse.bmat([[sparse.csc_matrix(reduced), sparse.csc_matrix(rows[:, free].T)],
+                                [sparse.csc_matrix(rows[:, free]), None]], format="csc")
+        x[free] = EquilibratedLU(bordered, rtol).solve(np.r_[rrhs, targets])[: len(free)]
+    else:
+        x[free] = EquilibratedLU(sparse.csc_matrix(reduced), rtol).solve(rrhs)
     defect = reduced @ x[free] - rrhs
     scale = abs(reduced) @ np.abs(x[free])
     phys = max(np.linalg.norm(rhs[free]), np.linalg.norm(load_scale[free]), np.linalg.norm(action),
@@ -765,9 +785,10 @@ def local_problem(mesh, skeleton, cell, refinement, permeability, source, order=
 
 
 def solve_darcy_q1(mesh, skeleton, refinement, permeability=1.0, source=0.0, dirichlet=0.0,
-                   order=4, keep_responses=False, cells=None, neumann=None):
+                   order=4, keep_responses=False, cells=None, neumann=None, mean_pressure=0.0):
     """``solve_darcy_quadrilateral`` for degree one (``cartesian.py:86-168``); Neumann
-    faces fix their trace DOFs (no pure-Neumann gauge)."""
+    faces fix their trace DOFs, and with every boundary face Neumann the mean of the
+    pressure is ``mean_pressure`` (``:136-142``)."""
     boundary, fixed = boundary_data(skeleton, dirichlet, neumann, order)
     responses, contribs, fines = [], [], []
     for cell in range(len(mesh.cells)):
@@ -777,7 +798,12 @@ def solve_darcy_q1(mesh, skeleton, refinement, permeability=1.0, source=0.0, dir
         responses.append(resp)
         fines.append(fine)
     matrix, rhs, scale = assemble_global(contribs, skeleton.size, boundary)
-    x, residual = solve_global(matrix, rhs, scale, fixed=fixed)
+    constraints = None
+    if neumann and set(neumann) == set(int(f) for f in mesh.boundary_faces):
+        x0, x1, y0, y1 = mesh.bounds
+        weights = [r.problem.constraints[:, 0] for r in responses]
+        constraints = [mean_constraint(responses, skeleton.size, weights, mean_pressure * (x1 - x0) * (y1 - y0))]
+    x, residual = solve_global(matrix, rhs, scale, fixed=fixed, constraints=constraints)
     trace = x[: skeleton.size]
     coarse = x[skeleton.size:]
     fields = np.array([r.source - r.lifts @ trace[r.problem.trace_dofs] + r.retained @ coarse[c: c + 1]

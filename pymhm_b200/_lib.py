@@ -69,7 +69,7 @@ class SkeletonSystem(C.Structure):
         ("coarse_ax", C.c_double), ("coarse_ay", C.c_double),
         ("cell_blocks", C.c_void_p), ("block_ld", C.c_int32),
         ("fixed", C.c_void_p), ("coarse_neumann", C.c_int32),
-        ("coarse_qx", C.c_void_p), ("coarse_lamx", C.c_void_p),
+        ("coarse_qx", C.c_void_p), ("coarse_lamx", C.c_void_p), ("coarse_pinv0", C.c_void_p),
     ]
 
 
@@ -88,6 +88,7 @@ _SIGNATURES = {
     "mhm_q1_original_defect": (C.c_int, [C.POINTER(Q1Problem), P, C.c_int64, P, P, P, P, P, P, P, P, P, P, P]),
     "mhm_refine_norms": (C.c_int, [C.c_int32, P, C.c_int64, P, P, P, C.c_int64, P, P, P, P, P, P, P]),
     "mhm_vector_accumulate": (C.c_int, [C.c_int64, P, P, P]),
+    "mhm_q1_mean_gauge": (C.c_int, [C.POINTER(Q1Problem), P, P, C.c_double, C.c_int64, P, P, P]),
     "mhm_skeleton_fixed_rhs": (C.c_int, [C.c_int64, C.c_int64, P, P, P, P, P, P, P, P]),
     "mhm_q1_flux": (C.c_int, [C.POINTER(Q1Problem), P, P, P]),
     "mhm_skeleton_scatter": (C.c_int, [C.c_int64, P, P, P, P, C.c_int64, C.c_int64, P, P, P, P, P, P, P]),

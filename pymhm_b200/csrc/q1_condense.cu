@@ -1505,6 +1505,64 @@ extern "C" int mhm_vector_accumulate(int64_t n, double* dst, const double* src, 
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
 
+namespace mhm {
+namespace {
+// Mean-pressure gauge of a pure-Neumann solve (hybrid_mean_constraint,
+// core/system.py:531-566, with the weights C = M 1 of every cell): per cell
+// s1 = C . u and s2 = C . (1 - R A1), C_i = area / 4 times the elements at node i.
+__global__ void __launch_bounds__(kThreads) gauge_partial_kernel(const Q1Args a, const double* fields,
+                                                                 double* partial) {
+  __shared__ double red[32];
+  const int cell = blockIdx.x, n = a.n, np1 = n + 1;
+  const double* ra1 = a.sol + ((size_t)cell * a.w + (a.w - 1)) * np1;
+  double s1 = 0.0, s2 = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int ix = i % a.nnx, iy = i / a.nnx;
+    const double c = ((ix == 0 || ix == a.rx) ? 1.0 : 2.0) * ((iy == 0 || iy == a.ry) ? 1.0 : 2.0) * (a.area * 0.25);
+    s1 = fma(c, fields[(size_t)cell * n + i], s1);
+    s2 = fma(c, 1.0 - ra1[i], s2);
+  }
+  s1 = block_sum(s1, red);
+  s2 = block_sum(s2, red);
+  if (threadIdx.x == 0) {
+    partial[2 * (size_t)cell] = s1;
+    partial[2 * (size_t)cell + 1] = s2;
+  }
+}
+
+// One block: alpha = (value - sum s1) / sum s2 (fixed-order sums), then every coarse
+// unknown += alpha, so that sum_cells C . u = value once the fields are reconstructed.
+__global__ void __launch_bounds__(256) gauge_apply_kernel(int cells, const double* partial, double value,
+                                                         int64_t trace_size, double* x, double* alpha_out) {
+  __shared__ double red[32];
+  double s1 = 0.0, s2 = 0.0;
+  for (int c = threadIdx.x; c < cells; c += blockDim.x) {
+    s1 += partial[2 * (size_t)c];
+    s2 += partial[2 * (size_t)c + 1];
+  }
+  s1 = block_sum(s1, red);
+  s2 = block_sum(s2, red);
+  const double alpha = (value - s1) / s2;
+  if (threadIdx.x == 0) alpha_out[0] = alpha;
+  for (int c = threadIdx.x; c < cells; c += blockDim.x) x[trace_size + c] += alpha;
+}
+}  // namespace
+}  // namespace mhm
+
+extern "C" int mhm_q1_mean_gauge(const mhm_q1_problem* p, const double* solution, const double* fields,
+                                 double value, int64_t trace_size, double* x, double* partial, void* stream) {
+  Q1Args a;
+  int rc = fill_args(p, MHM_PRECISION_FP64, a);
+  if (rc != MHM_OK) return rc;
+  if (!solution || !fields || trace_size < 0 || !x || !partial || !std::isfinite(value)) return MHM_ERR_ARGUMENT;
+  a.sol = const_cast<double*>(solution);
+  const int cells = a.nx * a.ny;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  gauge_partial_kernel<<<cells, kThreads, 0, st>>>(a, fields, partial);
+  gauge_apply_kernel<<<1, 256, 0, st>>>(cells, partial, value, trace_size, x, partial + 2 * (size_t)cells);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
 extern "C" int mhm_q1_flux(const mhm_q1_problem* p, const double* fields, double* flux, void* stream) {
   Q1Args a;
   int rc = fill_args(p, MHM_PRECISION_FP64, a);

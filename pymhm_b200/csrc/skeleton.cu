@@ -79,6 +79,7 @@ struct Sys {
   int yneu;              // coarse T_y ends: bit 0 bottom, bit 1 top Neumann
   const double* qx;      // nx x nx eigenvectors [k][i] of the coarse T_x (null: the sine basis)
   const double* lamx;    // nx eigenvalues of T_x (with qx)
+  const double* pinv0;   // ny x ny pseudo-inverse of mode 0's T_y when every side is fixed (else null)
 };
 
 // Row-transformed coarse data of one quantity, layout [mode][row]:
@@ -361,7 +362,10 @@ __device__ void mode_solve(const Sys& s, const Row& R, const Coarse& U, double* 
       const int ir = base + grp;
       double acc = 0.0;
       if (ir < ny) {
-        if (!NEU || s.yneu == 0) {
+        if (NEU && s.pinv0 && k == 0) {
+          const double* prow = s.pinv0 + (size_t)ir * ny;
+          for (int iy = lane8; iy < ny; iy += 8) acc = fma(__ldg(prow + iy), R.ucol[iy], acc);
+        } else if (!NEU || s.yneu == 0) {
           const double uir = u[ir], unir = u[ny - 1 - ir];
           for (int iy = lane8; iy < ny; iy += 8)
             acc = fma((ir < iy ? uir * u[ny - 1 - iy] : u[iy] * unir), R.ucol[iy], acc);
@@ -729,7 +733,9 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
     double* u = R.mcheb + (size_t)j * (NEU ? 2 : 1) * (ny + 1);
     const double lam = (NEU && s.lamx) ? s.lamx[k] : 2.0 - 2.0 * cospi((double)(k + 1) / (double)(nx + 1));
     const double two_theta = 2.0 + s.ax * lam / s.ay;
-    if (!NEU || s.yneu == 0) {
+    if (NEU && s.pinv0 && k == 0) {
+      R.mcinv[j] = 1.0;  // the singular constant mode: mode_solve applies pinv0
+    } else if (!NEU || s.yneu == 0) {
       double um1 = 0.0, u0 = 1.0;
       u[0] = 1.0;
       for (int m = 1; m <= ny; ++m) {
@@ -1202,8 +1208,9 @@ bool valid(const mhm_skeleton_system* s) {
          s->indices && s->values && s->trace_end && s->cell_dofs && s->cell_g0 && s->dof_cells &&
          s->dof_slot && std::isfinite(s->coarse_ax) && std::isfinite(s->coarse_ay) &&
          s->coarse_ax > 0 && s->coarse_ay > 0 && (!s->cell_blocks || s->block_ld >= s->cell_width) &&
-         s->coarse_neumann >= 0 && s->coarse_neumann < 15 && (s->fixed || s->coarse_neumann == 0) &&
-         (!(s->coarse_neumann & 12) || (s->coarse_qx && s->coarse_lamx));
+         s->coarse_neumann >= 0 && s->coarse_neumann <= 15 && (s->fixed || s->coarse_neumann == 0) &&
+         (!(s->coarse_neumann & 12) || (s->coarse_qx && s->coarse_lamx)) &&
+         (s->coarse_neumann != 15 || s->coarse_pinv0);
 }
 
 // The Chebyshev values U_m(theta) grow like rho^m, rho = theta + sqrt(theta^2 - 1);
@@ -1305,7 +1312,8 @@ extern "C" int mhm_skeleton_solve(const mhm_skeleton_system* s, const double* rh
             s->dof_slot, s->nx, s->ny, s->coarse_ax, s->coarse_ay, s->cell_blocks, s->block_ld,
             s->fixed, s->fixed ? (s->coarse_neumann & 3) : 0,
             (s->fixed && (s->coarse_neumann & 12)) ? s->coarse_qx : nullptr,
-            (s->fixed && (s->coarse_neumann & 12)) ? s->coarse_lamx : nullptr};
+            (s->fixed && (s->coarse_neumann & 12)) ? s->coarse_lamx : nullptr,
+            (s->fixed && s->coarse_neumann == 15) ? s->coarse_pinv0 : nullptr};
   auto at = [&](size_t o) { return reinterpret_cast<double*>(base + o); };
   P.w.Zf = at(L.Zf);
   P.w.Zs = at(L.Zs);

@@ -35,6 +35,7 @@ from .topology import (
     FaceSpace,
     SkeletonSpace,
     boundary_data,
+    coarse_mode0_pinv,
     coarse_x_basis,
     neumann_fixed,
     neumann_sides,
@@ -301,7 +302,7 @@ class CartesianQ1Plan:
     (new coefficients or sources on the same mesh) allocate nothing.
     """
 
-    def __init__(self, mesh, skeleton=None, local_refinement=4, *, dirichlet=0.0, neumann=None,
+    def __init__(self, mesh, skeleton=None, local_refinement=4, *, dirichlet=0.0, neumann=None, mean_pressure=0.0,
                  quadrature_order=4, degree=1, precision="fp64", device=None, max_refine=None, local_tol=1e-12,
                  global_rtol=1e-13, inner_rtol=1e-10, max_inner=5000, max_outer=6, grid=0):
         import torch
@@ -425,6 +426,17 @@ class CartesianQ1Plan:
                 qx, lamx = coarse_x_basis(m.nx, self.neumann_bits)
                 self.d_qx, self.d_lamx = up(qx, torch.float64), up(lamx, torch.float64)
                 s.coarse_qx, s.coarse_lamx = _lib.ptr(self.d_qx), _lib.ptr(self.d_lamx)
+        # pure Neumann: the mean-pressure condition sum_cells C . u = mean_pressure |domain|
+        # fixes the constant coarse mode (cartesian.py:136-142)
+        self.pure_neumann = self.neumann_bits == 15
+        if self.pure_neumann:
+            x0, x1, y0, y1 = m.bounds
+            self.mean_value = float(mean_pressure) * (x1 - x0) * (y1 - y0)
+            if not np.isfinite(self.mean_value):
+                raise ValueError("mean_pressure must be finite")
+            self.d_pinv0 = up(coarse_mode0_pinv(m.ny, self.coarse_ab[1]), torch.float64)
+            s.coarse_pinv0 = _lib.ptr(self.d_pinv0)
+            self.gauge = torch.empty(2 * self.cells + 1, dtype=torch.float64, device=dev)
         nbytes = self.lib.mhm_skeleton_workspace_bytes(s, self.grid)
         if nbytes <= 0:
             raise RuntimeError("could not size the skeleton solver workspace")
@@ -545,6 +557,11 @@ class CartesianQ1Plan:
         if self.d_xfixed is not None:  # the prescribed Neumann coefficients
             _lib.check(L.mhm_vector_accumulate(self.N, P(self.x), P(self.d_xfixed), gs), "mhm_vector_accumulate")
         mark(3, gcur)
+        if self.pure_neumann:  # fields of the gauge-free solve, then the mean-pressure shift
+            _lib.check(L.mhm_q1_reconstruct(self.q1, P(self.solution), P(self.d_cell_dofs), self.T, P(self.x),
+                                            P(self.fields), None, gs), "mhm_q1_reconstruct")
+            _lib.check(L.mhm_q1_mean_gauge(self.q1, P(self.solution), P(self.fields), self.mean_value, self.T,
+                                           P(self.x), P(self.gauge), gs), "mhm_q1_mean_gauge")
         if reconstruct:
             _lib.check(L.mhm_q1_reconstruct(self.q1, P(self.solution), P(self.d_cell_dofs), self.T, P(self.x),
                                             P(self.fields), P(self.flux), gs), "mhm_q1_reconstruct")
@@ -636,6 +653,9 @@ class CartesianQ1Plan:
         weak residual counts the free DOFs, and each correction solves with those
         DOFs held at zero (``refinement.py:676-709, 792``).
         """
+        if self.pure_neumann:
+            raise NotImplementedError("original-equation refinement of a pure-Neumann solve needs its physical "
+                                      "moments (refinement.py:676-703), which are not on the GPU path")
         _step_limits(max_steps, min_steps)
         _tolerances(rtol, atol)
         torch, L, P = self.torch, self.lib, _lib.ptr
@@ -839,8 +859,9 @@ def solve_darcy_quadrilateral(mesh, *, permeability=1.0, source=0.0, dirichlet=0
 
     Weak Dirichlet data on the faces not listed in ``neumann``; Neumann data (outward
     normal fluxes) on whole sides of the domain prescribes those faces' trace
-    coefficients, which the global solve eliminates.  Parts of sides and the
-    pure-Neumann case with its gauge raise ``NotImplementedError``.  The
+    coefficients, which the global solve eliminates; with every side Neumann the
+    pressure mean over the domain is ``mean_pressure`` (the reference's gauge).  Neumann
+    data on part of a side raises ``NotImplementedError``.  The
     ``solver``, ``local_solver``, ``backend`` and ``workers`` arguments are
     accepted for signature compatibility: the whole solve runs on the GPU.
     ``hybrid_refinement_steps`` / ``hybrid_refinement_min_steps`` follow the Darcy
@@ -852,10 +873,10 @@ def solve_darcy_quadrilateral(mesh, *, permeability=1.0, source=0.0, dirichlet=0
     _refinement_steps(hybrid_refinement_min_steps)
     if hybrid_refinement_min_steps > hybrid_refinement_steps:
         raise ValueError("hybrid_refinement_min_steps must not exceed hybrid_refinement_steps")
-    del mean_pressure, solver, local_solver, backend, workers
+    del solver, local_solver, backend, workers
     order = max(int(quadrature_order), int(degree) + 1)
     plan = CartesianQ1Plan(mesh, skeleton, local_refinement, dirichlet=dirichlet, neumann=neumann,
-                           quadrature_order=order, degree=degree, precision=precision)
+                           mean_pressure=mean_pressure, quadrature_order=order, degree=degree, precision=precision)
     sol = plan.solve(permeability, source)
     if hybrid_refinement_steps:
         sol = plan.refine(max_steps=hybrid_refinement_steps, min_steps=hybrid_refinement_min_steps).solution

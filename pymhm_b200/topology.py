@@ -409,9 +409,9 @@ def neumann_fixed(skeleton: SkeletonSpace, neumann, order: int = 4) -> tuple[np.
 def neumann_sides(mesh, neumann) -> int:
     """Which whole sides the Neumann faces cover: bit 0 the bottom (y = y0), bit 1 the
     top, bit 2 the left (x = x0), bit 3 the right.  The global solver's coarse operator
-    takes those as Neumann ends of its 1-D factors.  Any other set of Neumann faces
-    (part of a side) and the pure-Neumann case (all four sides, which needs the
-    reference's mean-pressure gauge) are outside this path."""
+    takes those as Neumann ends of its 1-D factors (all four: the pure-Neumann case,
+    whose constant coarse mode the mean-pressure condition fixes).  Neumann data on
+    part of a side is outside this path."""
     faces = set(int(f) for f in (neumann or {}))
     if not faces:
         return 0
@@ -428,9 +428,6 @@ def neumann_sides(mesh, neumann) -> int:
     if faces != covered:
         raise NotImplementedError("Neumann data is supported on whole sides of the domain only "
                                   "(the global solver's coarse operator takes them as Neumann ends)")
-    if bits == 15:
-        raise NotImplementedError("pure-Neumann problems (every boundary face) need the mean-pressure gauge, "
-                                  "which is not on the GPU path")
     return bits
 
 
@@ -444,7 +441,23 @@ def coarse_x_basis(nx: int, bits: int) -> tuple[np.ndarray, np.ndarray]:
     if bits & 8:
         t[-1, -1] -= 1.0
     lam, vec = np.linalg.eigh(t)
-    return np.ascontiguousarray(vec), np.maximum(lam, 0.0)
+    lam = np.maximum(lam, 0.0)
+    if bits & 12 == 12:  # both ends Neumann: the constant mode, exactly
+        lam[0] = 0.0
+        vec[:, 0] = 1.0 / np.sqrt(nx)
+    return np.ascontiguousarray(vec), lam
+
+
+def coarse_mode0_pinv(ny: int, ay: float) -> np.ndarray:
+    """Pseudo-inverse of ay tridiag(-1, 2, -1) of order ny with both end rows Neumann
+    (the coarse operator's constant x mode when every side is fixed): the constant
+    vector spans its kernel."""
+    t = 2.0 * np.eye(ny) - np.eye(ny, k=1) - np.eye(ny, k=-1)
+    t[0, 0] -= 1.0
+    t[-1, -1] -= 1.0
+    lam, vec = np.linalg.eigh(t)
+    keep = np.arange(ny) > 0  # the smallest eigenvalue is the constant mode's zero
+    return np.ascontiguousarray((vec[:, keep] / lam[keep]) @ vec[:, keep].T / ay)
 
 
 # ----------------------------------------------------------------------------------------

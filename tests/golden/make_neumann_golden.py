@@ -44,13 +44,18 @@ def left_flux(x):
     return 0.3 - 0.2 * x[:, 1]
 
 
-def run(name, mesh, face_space, refinement, permeability, source, dirichlet, neumann, refine=False):
+def run(name, mesh, face_space, refinement, permeability, source, dirichlet, neumann, refine=False,
+        mean_pressure=None):
     sk = SkeletonSpace(mesh, (face_space,) * len(mesh.faces))
     order = 4
     boundary, fixed = boundary_data(sk, dirichlet, neumann, order=order)
     tasks = [_QuadTask(mesh, c, refinement, sk, 1, permeability, source, order) for c in range(len(mesh.cells))]
     system = HybridSystem.from_local_factory(_assemble_quad, tasks, boundary_load=boundary)
-    hybrid = system.solve(fixed=fixed)
+    constraints = None
+    if mean_pressure is not None:  # pure Neumann: the driver's mean-pressure row (cartesian.py:135-142)
+        _, means = zip(*system.local_metadata)
+        constraints = [system.mean_constraint(means, mean_pressure * float(np.sum(mesh.areas)))]
+    hybrid = system.solve(fixed=fixed, constraints=constraints)
     extra = {}
     if refine:
         perturbed = replace(hybrid, fields=tuple(u + 0.002 * np.arange(1, len(u) + 1) for u in hybrid.fields))
@@ -100,6 +105,12 @@ def main():
     mixed.update({f: bottom_flux for f in side_faces(mesh, 0.0)})
     out, name = run("poisson_4x4_r4_p1_flux_left_bottom", mesh, FaceSpace.uniform(1), (4, 4), 1.0, sine_source,
                     0.0, mixed, refine=True)
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    print(name, "fixed", len(out["fixed_dofs"]), "residual", out["residual"])
+    everywhere = {int(f): 0.25 for f in mesh.boundary_faces}  # outward flux 4 x 0.25 = the source's 1
+    out, name = run("darcy_4x4_r8_p1_pure_neumann", mesh, FaceSpace.uniform(1), (8, 8), field, 1.0, 0.0,
+                    everywhere, mean_pressure=0.3)
+    out["kappa"] = kap
     np.savez_compressed(HERE / f"{name}.npz", **out)
     print(name, "fixed", len(out["fixed_dofs"]), "residual", out["residual"])
 

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from tests._cases import PixelField, load, rel
-from tests.test_oracle_neumann import NEUMANN_CASES, neumann_map
+from tests.test_oracle_neumann import MEAN_PRESSURE, NEUMANN_CASES, neumann_map
 
 pytestmark = pytest.mark.gpu
 
@@ -22,7 +22,8 @@ def make_plan(name, precision):
     deg, ref, perm, src, dr, val = NEUMANN_CASES[name]
     mesh = CartesianMacroMesh(4)
     sk = SkeletonSpace(mesh, (FaceSpace.uniform(deg),) * len(mesh.faces))
-    plan = CartesianQ1Plan(mesh, sk, ref, dirichlet=dr, neumann=neumann_map(g, val, mesh), precision=precision)
+    plan = CartesianQ1Plan(mesh, sk, ref, dirichlet=dr, neumann=neumann_map(g, val, mesh),
+                           mean_pressure=MEAN_PRESSURE.get(name, 0.0), precision=precision)
     kap = PixelField(g["kappa"], (1 / 32, 1 / 32)) if "kappa" in g else 1.0
     plan.set_coefficients(kap, src)
     return g, plan
@@ -67,9 +68,10 @@ def test_driver_accepts_neumann_sides():
     sol = solve_darcy_quadrilateral(mesh, skeleton=sk, local_refinement=ref, source=src, dirichlet=dr,
                                     neumann=neumann_map(g, val, mesh))
     assert rel(sol.fields, g["fields"]) <= 1e-10
-    everywhere = {int(f): 0.0 for f in mesh.boundary_faces}
-    with pytest.raises(NotImplementedError, match="pure-Neumann"):
-        solve_darcy_quadrilateral(mesh, skeleton=sk, local_refinement=ref, neumann=everywhere)
+    part = {int(f): 0.0 for f in mesh.boundary_faces if np.all(mesh.points[mesh.faces[f]][:, 0] == 0.0)}
+    part.pop(min(part))
+    with pytest.raises(NotImplementedError, match="whole sides"):
+        solve_darcy_quadrilateral(mesh, skeleton=sk, local_refinement=ref, neumann=part)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
@@ -97,3 +99,20 @@ def test_neumann_refinement_matches_reference(precision):
     assert rel(sol.fields, g["refine_fields"]) <= 1e-10
     # the prescribed coefficients are untouched by the corrections
     assert np.max(np.abs(sol.trace[g["fixed_dofs"]] - g["fixed_values"])) <= 1e-15
+
+
+def test_pure_neumann_mean_pressure_and_refinement_guard():
+    """Every side Neumann: the pressure mean over the domain is the requested one (the
+    reference's gauge row), and original-equation refinement, which would need the
+    solve's physical moments, is refused."""
+    g, plan = make_plan("darcy_4x4_r8_p1_pure_neumann", "fp64")
+    plan.launch()
+    sol = plan.result()
+    fine_area = (0.25 / 8) ** 2
+    nodes = 9
+    ix, iy = np.meshgrid(np.arange(nodes), np.arange(nodes), indexing="xy")
+    weights = (np.where((ix == 0) | (ix == 8), 1.0, 2.0) * np.where((iy == 0) | (iy == 8), 1.0, 2.0)).ravel()
+    mean = float(np.sum(sol.fields * weights[None, :]) * fine_area / 4)
+    assert abs(mean - 0.3) <= 1e-12
+    with pytest.raises(NotImplementedError, match="physical"):
+        plan.refine(max_steps=1)

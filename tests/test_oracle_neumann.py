@@ -28,10 +28,15 @@ NEUMANN_CASES = {
     "darcy_4x4_r8_p2_noflow_lr": (2, (8, 8), _kappa, 1.0, lambda x: 1.0 - x[:, 1], {(0, 0.0): 0.0, (0, 1.0): 0.0}),
     "poisson_4x4_r4_p1_flux_left_bottom": (1, (4, 4), lambda g: 1.0, sine_source, 0.0,
                                            {(0, 0.0): _left_flux, (1, 0.0): _bottom_flux}),
+    # every side Neumann (outward flux 0.25, balancing the unit source): the mean-pressure gauge
+    "darcy_4x4_r8_p1_pure_neumann": (1, (8, 8), _kappa, 1.0, 0.0,
+                                     {(1, 0.0): 0.25, (1, 1.0): 0.25, (0, 0.0): 0.25, (0, 1.0): 0.25}),
 }
 
+MEAN_PRESSURE = {"darcy_4x4_r8_p1_pure_neumann": 0.3}
+
 SIDE_BITS = {"darcy_4x4_r8_p2_noflow_tb": 3, "poisson_4x4_r4_p1_flux_bottom": 1, "darcy_4x4_r8_p2_noflow_lr": 12,
-             "poisson_4x4_r4_p1_flux_left_bottom": 5}
+             "poisson_4x4_r4_p1_flux_left_bottom": 5, "darcy_4x4_r8_p1_pure_neumann": 15}
 
 
 def neumann_map(g, sides, mesh=None):
@@ -57,7 +62,8 @@ def test_oracle_matches_reference(name):
     _, fixed = o.boundary_data(sk, dr, neumann_map(g, val))
     assert np.array_equal(np.array(sorted(fixed)), g["fixed_dofs"])
     assert np.allclose([fixed[k] for k in sorted(fixed)], g["fixed_values"], rtol=0, atol=1e-15)
-    sol = o.solve_darcy_q1(mesh, sk, ref, perm(g), src, dr, neumann=neumann_map(g, val))
+    sol = o.solve_darcy_q1(mesh, sk, ref, perm(g), src, dr, neumann=neumann_map(g, val),
+                           mean_pressure=MEAN_PRESSURE.get(name, 0.0))
     for key, val_ in (("trace", sol.trace), ("coarse", sol.coarse), ("fields", sol.fields), ("flux", sol.flux)):
         assert rel(val_, g[key]) <= 1e-12, key
     assert np.array_equal(sol.trace[g["fixed_dofs"]], g["trace"][g["fixed_dofs"]])
@@ -96,12 +102,13 @@ def test_neumann_side_rules():
         neumann_sides(mesh, {f: 0.0 for f in bottom[:2]})
     with pytest.raises(NotImplementedError, match="whole sides"):
         neumann_sides(mesh, {f: 0.0 for f in left + bottom[1:]})
-    with pytest.raises(NotImplementedError, match="pure-Neumann"):
-        neumann_sides(mesh, {int(f): 0.0 for f in mesh.boundary_faces})
+    assert neumann_sides(mesh, {int(f): 0.0 for f in mesh.boundary_faces}) == 15
 
 
 @pytest.mark.parametrize("bits", [4, 8, 12])
 def test_coarse_x_basis_diagonalises_the_neumann_factor(bits):
+    """The host eigenbasis of the coarse x factor; with both ends Neumann its first
+    mode is exactly the constant."""
     from pymhm_b200.topology import coarse_x_basis
 
     nx = 7
@@ -113,3 +120,15 @@ def test_coarse_x_basis_diagonalises_the_neumann_factor(bits):
     assert np.allclose(q @ np.diag(lam) @ q.T, t, atol=1e-13)
     # a zero mode only when both x ends are Neumann (the y ends then carry the solve)
     assert (lam.min() <= 1e-14) == (bits == 12)
+
+
+def test_mode0_pseudo_inverse():
+    from pymhm_b200.topology import coarse_mode0_pinv
+
+    ny, ay = 6, 0.7
+    t = ay * (2.0 * np.eye(ny) - np.eye(ny, k=1) - np.eye(ny, k=-1))
+    t[0, 0] -= ay
+    t[-1, -1] -= ay
+    p = coarse_mode0_pinv(ny, ay)
+    assert np.allclose(p, np.linalg.pinv(t), atol=1e-13)
+    assert np.allclose(p @ np.ones(ny), 0.0, atol=1e-13)
