@@ -261,8 +261,9 @@ def serving_campaign(torch, lambdas=(100, 500, 2000), requests=150, precisions=(
     a local refinement from {4, 8, 16}^2, a seeded log-normal permeability (sigma in
     [1, 2], correlation length 0.05; drawn from a pool of two fields per fine-grid
     size, generated before timing) and 1..8 constant sources, the first solved with
-    factors kept, the others through the kept factors.  Before timing, four slots per
-    shape are reserved (plans built, both steps captured as CUDA graphs) and one
+    factors kept, the others through the kept factors.  Before timing, as many slots per
+    shape as requests may be in flight (8) are reserved (plans built, both steps
+    captured as CUDA graphs), so that no slot is built inside a timed stream, and one
     untimed stream warms them.  Returns p50/p99 latency (arrival to results in pinned host
     memory) and solves/s per rate and precision."""
     from pymhm_b200.serving import DarcyRequest, ServingEngine, summarize
@@ -293,7 +294,7 @@ def serving_campaign(torch, lambdas=(100, 500, 2000), requests=150, precisions=(
         engine = ServingEngine(precision=prec, max_in_flight=8)
         for m in SERVING_MACRO:
             for r in SERVING_LOCAL:
-                engine.reserve((m, r, FACE_DEGREE), 4)
+                engine.reserve((m, r, FACE_DEGREE), engine.max_in_flight)
         warm = [DarcyRequest(m, r, pool[m * r][0], (1.0, 2.0)) for m in SERVING_MACRO for r in SERVING_LOCAL] * 2
         engine.run(warm, realtime=False)
         per = {}
