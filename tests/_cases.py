@@ -29,17 +29,27 @@ def affine_dirichlet(x):
     return 0.7 + x[:, 0] - 2 * x[:, 1]
 
 
+def face_space(cls, face):
+    """The face space of a case: ``cls.uniform`` of its (degree, subdivisions[, continuous])."""
+    degree, subdivisions, *rest = face
+    return cls.uniform(degree, subdivisions, continuous=bool(rest and rest[0]))
+
+
 def load(name):
     return np.load(GOLDEN / f"{name}.npz")
 
 
-# name -> (macro args, (face degree, subdivisions), refinement, permeability(g), source, dirichlet)
+# name -> (macro args, (face degree, subdivisions[, continuous]), refinement, permeability(g), source,
+#          dirichlet)
 CASES = {
     "poisson_8x8_r4_p1": ((8,), (1, 1), (4, 4), lambda g: 1.0, sine_source, 0.0),
     "darcy_4x4_r16_p2_lognormal": ((4,), (2, 1), (16, 16),
                                    lambda g: PixelField(g["kappa"], (1 / 64, 1 / 64)), 1.0, 0.0),
     "darcy_4x4_r8_p1_cut20": ((4,), (1, 1), (8, 8),
                               lambda g: PixelField(g["kappa"], (1 / 20, 1 / 20)), 1.0, 0.0),
+    # continuous piecewise-linear traces on two segments per face (3 DOFs a face)
+    "darcy_4x4_r8_p1c2_lognormal": ((4,), (1, 2, True), (8, 8),
+                                    lambda g: PixelField(g["kappa"], (1 / 32, 1 / 32)), 1.0, 0.0),
     "affine_3x2_rect_r4x5_p1s2": ((3, 2, (-1, 2, -2, 2)), (1, 2), (4, 5),
                                   lambda g: PixelField(g["kappa"], (0.25, 0.4), (-1, -2)), quad_source,
                                   affine_dirichlet),

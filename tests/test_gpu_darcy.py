@@ -3,7 +3,7 @@
 import numpy as np
 import pytest
 
-from tests._cases import CASES, load, rel
+from tests._cases import face_space, CASES, load, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -16,9 +16,9 @@ def make_plan(name, precision, **kw):
     from pymhm_b200.topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
 
     g = load(name)
-    margs, (deg, sub), ref, perm, src, dr = CASES[name]
+    margs, face, ref, perm, src, dr = CASES[name]
     mesh = CartesianMacroMesh(*margs)
-    sk = SkeletonSpace(mesh, (FaceSpace.uniform(deg, sub),) * len(mesh.faces))
+    sk = SkeletonSpace(mesh, (face_space(FaceSpace, face),) * len(mesh.faces))
     plan = CartesianQ1Plan(mesh, sk, ref, dirichlet=dr, precision=precision, **kw)
     plan.set_coefficients(perm(g), src)
     return g, plan

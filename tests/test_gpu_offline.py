@@ -3,7 +3,7 @@
 import numpy as np
 import pytest
 
-from tests._cases import CASES, load, rel
+from tests._cases import face_space, CASES, load, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -14,9 +14,9 @@ def _setup(name):
     from pymhm_b200.topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
 
     g = load(name)
-    margs, (deg, sub), ref, perm, src, dr = CASES[name]
+    margs, face, ref, perm, src, dr = CASES[name]
     mesh = CartesianMacroMesh(*margs)
-    sk = SkeletonSpace(mesh, (FaceSpace.uniform(deg, sub),) * len(mesh.faces))
+    sk = SkeletonSpace(mesh, (face_space(FaceSpace, face),) * len(mesh.faces))
     return g, mesh, sk, ref, perm(g), src, dr
 
 

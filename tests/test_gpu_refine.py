@@ -4,7 +4,7 @@ against fixtures written by PyMHM's own refinement (tests/golden/make_refine_gol
 import numpy as np
 import pytest
 
-from tests._cases import load, rel
+from tests._cases import face_space, load, rel
 from tests.test_gpu_darcy import make_plan
 
 pytestmark = pytest.mark.gpu
@@ -92,9 +92,9 @@ def test_driver_keyword_refines():
 
     name = "darcy_4x4_r16_p2_lognormal"
     g = load(name)
-    margs, (deg, sub), ref, perm, src, dr = CASES[name]
+    margs, face, ref, perm, src, dr = CASES[name]
     mesh = CartesianMacroMesh(*margs)
-    sk = SkeletonSpace(mesh, (FaceSpace.uniform(deg, sub),) * len(mesh.faces))
+    sk = SkeletonSpace(mesh, (face_space(FaceSpace, face),) * len(mesh.faces))
     sol = solve_darcy_quadrilateral(mesh, permeability=perm(g), source=src, skeleton=sk, local_refinement=ref,
                                     precision="mixed", hybrid_refinement_steps=2)
     assert rel(sol.fields, g["fields"]) <= 1e-10

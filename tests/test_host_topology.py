@@ -5,13 +5,13 @@ import pytest
 
 from oracle import q1_mhm as o
 from pymhm_b200 import topology as tp
-from tests._cases import CASES, load
+from tests._cases import face_space, CASES, load
 
 
 def product_case(name):
-    margs, (deg, sub), ref, *_ = CASES[name]
+    margs, face, ref, *_ = CASES[name]
     mesh = tp.CartesianMacroMesh(*margs)
-    sk = tp.SkeletonSpace(mesh, (tp.FaceSpace.uniform(deg, sub),) * len(mesh.faces))
+    sk = tp.SkeletonSpace(mesh, (face_space(tp.FaceSpace, face),) * len(mesh.faces))
     return mesh, sk, ref
 
 

@@ -5,7 +5,7 @@ import pytest
 from scipy import sparse
 
 from oracle import q1_mhm as o
-from tests._cases import CASES, load, rel
+from tests._cases import face_space, CASES, load, rel
 
 # Cases whose fine cells are cut by pixel lines: the reference evaluates the Q1 basis at
 # per-cell intersection points through its tabulation backend, so operator entries agree
@@ -16,9 +16,9 @@ ROUNDED_PATTERN = ("darcy_4x4_r8_p1_cut20",)
 
 def oracle_case(name):
     g = load(name)
-    margs, (deg, sub), ref, perm, src, dr = CASES[name]
+    margs, face, ref, perm, src, dr = CASES[name]
     mesh = o.cartesian_mesh(*margs)
-    sk = o.Skeleton(mesh, (o.FaceSpace.uniform(deg, sub),) * len(mesh.faces))
+    sk = o.Skeleton(mesh, (face_space(o.FaceSpace, face),) * len(mesh.faces))
     p = perm(g)
     if hasattr(p, "values"):
         p = o.PixelField(p.values, p.spacing, p.origin)
