@@ -310,6 +310,16 @@ typedef struct mhm_skeleton_system {
      * the kernel of G0^T G0.  The solve then returns coarse unknowns without that
      * mode; mhm_q1_mean_gauge fixes it from the mean-pressure condition.        */
     const double* coarse_pinv0;
+    /* Fixed DOFs on part of a side (Neumann faces that do not cover it): the
+     * coarse operator above (those sides counted as Dirichlet) less a_y (a_x)
+     * on the diagonal of each cell with such a horizontal (vertical) face.
+     * coarse_partial = m cells (0: none; at most 2 (nx + ny)),
+     * coarse_partial_cells[m] their indices, coarse_partial_R (cells x m,
+     * row-major) = A_sep^-1 E (D^-1 - E^T A_sep^-1 E)^-1 (the Woodbury factor;
+     * topology.coarse_partial_correction computes it).                        */
+    int32_t coarse_partial;
+    const int32_t* coarse_partial_cells;
+    const double* coarse_partial_R;
 } mhm_skeleton_system;
 
 int64_t mhm_skeleton_workspace_bytes(const mhm_skeleton_system* s /* host */, int32_t grid);

@@ -70,6 +70,7 @@ class SkeletonSystem(C.Structure):
         ("cell_blocks", C.c_void_p), ("block_ld", C.c_int32),
         ("fixed", C.c_void_p), ("coarse_neumann", C.c_int32),
         ("coarse_qx", C.c_void_p), ("coarse_lamx", C.c_void_p), ("coarse_pinv0", C.c_void_p),
+        ("coarse_partial", C.c_int32), ("coarse_partial_cells", C.c_void_p), ("coarse_partial_R", C.c_void_p),
     ]
 
 

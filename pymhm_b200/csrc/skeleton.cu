@@ -80,6 +80,11 @@ struct Sys {
   const double* qx;      // nx x nx eigenvectors [k][i] of the coarse T_x (null: the sine basis)
   const double* lamx;    // nx eigenvalues of T_x (with qx)
   const double* pinv0;   // ny x ny pseudo-inverse of mode 0's T_y when every side is fixed (else null)
+  // Neumann faces on part of a side: the coarse operator is the separable one less
+  // E D E^T on wbm boundary cells; y = A_sep^-1 r is corrected by wbR (E^T y)
+  int wbm;
+  const int32_t* wbcell;  // wbm cells
+  const double* wbR;      // cells x wbm, [cell][l]
 };
 
 // Row-transformed coarse data of one quantity, layout [mode][row]:
@@ -259,6 +264,7 @@ struct Row {
   double* gself;    // t nx: g0 of the cell on the slot
   double* gnb;      // t nx: g0 of the other cell on the same DOF (0: none)
   uint8_t* role;    // t nx: bit 0 = the cell is the DOF's second cell, bit 1 = the DOF has two cells
+  double* wbe;      // fixed-DOF instantiation: y at the Woodbury cells (2 (nx + ny))
   double* scratch;  // kWarps t t (aliases the G vectors during setup)
 };
 
@@ -383,6 +389,36 @@ __device__ void mode_solve(const Sys& s, const Row& R, const Coarse& U, double* 
   }
 }
 
+// Neumann faces on part of a side (fixed-DOF instantiation): the coarse operator is
+// A = A_sep - E D E^T, A_sep the separable operator with those sides taken as
+// Dirichlet and E the wbm boundary cells that lose a face.  By the Woodbury identity
+// A^-1 r = y + wbR (E^T y), y = A_sep^-1 r, wbR = A_sep^-1 E (D^-1 - E^T A_sep^-1 E)^-1.
+// Every CTA forms E^T y from the solved mode data W itself (y at a cell is its row of
+// W through the inverse transform), so no grid barrier is added; it then corrects its
+// coarse rows [lo, hi) in yrow.
+template <bool NEU>
+__device__ void woodbury_rows(const Sys& s, const Row& R, const double* W, int lo, int hi) {
+  if (!NEU || s.wbm == 0) return;
+  const int nx = s.nx, r0 = R.r - 1;
+  for (int l = threadIdx.x; l < s.wbm; l += blockDim.x) {
+    const int c = s.wbcell[l], ir = c / nx, ix = c - ir * nx;
+    const double* wr = W + (size_t)ir * nx;
+    double acc = 0.0;
+    for (int k = 0; k < nx; ++k) acc = fma(__ldcg(wr + k), s.qx ? R.Q[ix * R.qs + k] : R.Q[k * R.qs + ix], acc);
+    R.wbe[l] = acc;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < 3 * nx; idx += blockDim.x) {
+    const int ir = r0 + idx / nx;
+    if (ir < lo || ir >= hi) continue;
+    const double* rr = s.wbR + ((size_t)ir * nx + idx % nx) * s.wbm;
+    double acc = 0.0;
+    for (int l = 0; l < s.wbm; ++l) acc = fma(__ldg(rr + l), R.wbe[l], acc);
+    R.yrow[idx] += acc;
+  }
+  __syncthreads();
+}
+
 // Coarse solution rows [lo, hi) (clipped to the grid, within r-1 .. r+1) from W
 // into yrow; other slots zero.  Y row = W row Q.
 template <bool NEU>
@@ -403,6 +439,7 @@ __device__ void coarse_rows(const Sys& s, const Row& R, const double* W, int lo,
   else
     sine_apply<false>(R, nx, 3, in, put);
   __syncthreads();
+  woodbury_rows<NEU>(s, R, W, lo, hi);
 }
 
 // Start of an inner half-step after a grid barrier: the partial sums in slots
@@ -468,6 +505,7 @@ __device__ void phase_begin(const Sys& s, const Work& w, const Row& R, int slot,
   else
     sine_apply<false>(R, nx, 3, in, put);
   __syncthreads();
+  woodbury_rows<NEU>(s, R, W, 0, ny);
 }
 
 // Rows Q FS .. Q FS + FS - 1 (face Q) of one cell's product B_c v_c, with B_c
@@ -650,6 +688,7 @@ __host__ __device__ size_t smem_layout(int nx, int ny, int fs, int t, int grid, 
   take((size_t)nx * t * 8);              // 16 gself
   take((size_t)nx * t * 8);              // 17 gnb
   take((size_t)nx * t);                  // 18 role
+  if (neu) take(2 * (size_t)(nx + ny) * 8);  // 19 wbe
   off[k] = o;
   return o;
 }
@@ -706,6 +745,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) skeleton_pcg_kernel(const Pa
   R.gself = reinterpret_cast<double*>(dyn + off[16]);
   R.gnb = reinterpret_cast<double*>(dyn + off[17]);
   R.role = reinterpret_cast<uint8_t*>(dyn + off[18]);
+  R.wbe = NEU ? reinterpret_cast<double*>(dyn + off[19]) : nullptr;
   {
     // DOFs are numbered by their first cell: binary search the row boundaries
     auto lower = [&](int cell) {
@@ -1210,7 +1250,10 @@ bool valid(const mhm_skeleton_system* s) {
          s->coarse_ax > 0 && s->coarse_ay > 0 && (!s->cell_blocks || s->block_ld >= s->cell_width) &&
          s->coarse_neumann >= 0 && s->coarse_neumann <= 15 && (s->fixed || s->coarse_neumann == 0) &&
          (!(s->coarse_neumann & 12) || (s->coarse_qx && s->coarse_lamx)) &&
-         (s->coarse_neumann != 15 || s->coarse_pinv0);
+         (s->coarse_neumann != 15 || s->coarse_pinv0) &&
+         (s->coarse_partial == 0 || (s->fixed && s->coarse_partial > 0 &&
+                                     s->coarse_partial <= 2 * (s->nx + s->ny) && s->coarse_partial_cells &&
+                                     s->coarse_partial_R));
 }
 
 // The Chebyshev values U_m(theta) grow like rho^m, rho = theta + sqrt(theta^2 - 1);
@@ -1313,7 +1356,9 @@ extern "C" int mhm_skeleton_solve(const mhm_skeleton_system* s, const double* rh
             s->fixed, s->fixed ? (s->coarse_neumann & 3) : 0,
             (s->fixed && (s->coarse_neumann & 12)) ? s->coarse_qx : nullptr,
             (s->fixed && (s->coarse_neumann & 12)) ? s->coarse_lamx : nullptr,
-            (s->fixed && s->coarse_neumann == 15) ? s->coarse_pinv0 : nullptr};
+            (s->fixed && s->coarse_neumann == 15) ? s->coarse_pinv0 : nullptr,
+            s->fixed ? s->coarse_partial : 0, s->fixed ? s->coarse_partial_cells : nullptr,
+            s->fixed ? s->coarse_partial_R : nullptr};
   auto at = [&](size_t o) { return reinterpret_cast<double*>(base + o); };
   P.w.Zf = at(L.Zf);
   P.w.Zs = at(L.Zs);

@@ -37,8 +37,9 @@ from .topology import (
     boundary_data,
     coarse_mode0_pinv,
     coarse_x_basis,
+    coarse_partial_correction,
     neumann_fixed,
-    neumann_sides,
+    neumann_layout,
     coarse_coefficients,
     coupling_tables,
     dof_cell_maps,
@@ -344,7 +345,7 @@ class CartesianQ1Plan:
         g0 = geometric_constraint(m, space_h, space_v)
         # Neumann faces (whole bottom / top sides): their trace DOFs are prescribed
         # (boundary_data's `fixed`) and eliminated from the global solve
-        self.neumann_bits = neumann_sides(m, neumann)
+        self.neumann_bits, neumann_partial = neumann_layout(m, neumann)
         self.boundary_h = boundary_data(sk, dirichlet, self.order, neumann)
         fixed_dofs, fixed_values = neumann_fixed(sk, neumann, self.order)
         # ---- device constants ---------------------------------------------------------
@@ -422,13 +423,18 @@ class CartesianQ1Plan:
             self.d_fixed, self.d_xfixed = up(mask, torch.uint8), up(xfixed, torch.float64)
             s.fixed, s.coarse_neumann = _lib.ptr(self.d_fixed), self.neumann_bits
             self.rhs_red = torch.empty(self.N, dtype=torch.float64, device=dev)
+            if neumann_partial:  # Neumann faces on part of a side: Woodbury factor of the coarse operator
+                cells, factor = coarse_partial_correction(m, self.neumann_bits, neumann_partial, *self.coarse_ab)
+                self.d_wb_cells, self.d_wb_R = up(cells, torch.int32), up(factor, torch.float64)
+                s.coarse_partial = len(cells)
+                s.coarse_partial_cells, s.coarse_partial_R = _lib.ptr(self.d_wb_cells), _lib.ptr(self.d_wb_R)
             if self.neumann_bits & 12:  # Neumann left/right sides: T_x eigenbasis from the host
                 qx, lamx = coarse_x_basis(m.nx, self.neumann_bits)
                 self.d_qx, self.d_lamx = up(qx, torch.float64), up(lamx, torch.float64)
                 s.coarse_qx, s.coarse_lamx = _lib.ptr(self.d_qx), _lib.ptr(self.d_lamx)
         # pure Neumann: the mean-pressure condition sum_cells C . u = mean_pressure |domain|
         # fixes the constant coarse mode (cartesian.py:136-142)
-        self.pure_neumann = self.neumann_bits == 15
+        self.pure_neumann = self.neumann_bits == 15 and not neumann_partial
         if self.pure_neumann:
             x0, x1, y0, y1 = m.bounds
             self.mean_value = float(mean_pressure) * (x1 - x0) * (y1 - y0)
@@ -858,10 +864,9 @@ def solve_darcy_quadrilateral(mesh, *, permeability=1.0, source=0.0, dirichlet=0
     """GPU counterpart of ``solve_darcy_quadrilateral`` (``cartesian.py:86-168``).
 
     Weak Dirichlet data on the faces not listed in ``neumann``; Neumann data (outward
-    normal fluxes) on whole sides of the domain prescribes those faces' trace
-    coefficients, which the global solve eliminates; with every side Neumann the
-    pressure mean over the domain is ``mean_pressure`` (the reference's gauge).  Neumann
-    data on part of a side raises ``NotImplementedError``.  The
+    normal fluxes) on any set of boundary faces prescribes those faces' trace
+    coefficients, which the global solve eliminates; with every face Neumann the
+    pressure mean over the domain is ``mean_pressure`` (the reference's gauge).  The
     ``solver``, ``local_solver``, ``backend`` and ``workers`` arguments are
     accepted for signature compatibility: the whole solve runs on the GPU.
     ``hybrid_refinement_steps`` / ``hybrid_refinement_min_steps`` follow the Darcy

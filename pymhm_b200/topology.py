@@ -406,15 +406,13 @@ def neumann_fixed(skeleton: SkeletonSpace, neumann, order: int = 4) -> tuple[np.
     return np.concatenate(dofs).astype(np.int64), np.concatenate(values)
 
 
-def neumann_sides(mesh, neumann) -> int:
-    """Which whole sides the Neumann faces cover: bit 0 the bottom (y = y0), bit 1 the
-    top, bit 2 the left (x = x0), bit 3 the right.  The global solver's coarse operator
-    takes those as Neumann ends of its 1-D factors (all four: the pure-Neumann case,
-    whose constant coarse mode the mean-pressure condition fixes).  Neumann data on
-    part of a side is outside this path."""
+def neumann_layout(mesh, neumann) -> tuple[int, list]:
+    """(bits, partial): the whole sides the Neumann faces cover (bit 0 the bottom
+    y = y0, bit 1 the top, bit 2 the left x = x0, bit 3 the right) and the Neumann
+    faces left over, on sides they cover only in part."""
     faces = set(int(f) for f in (neumann or {}))
     if not faces:
-        return 0
+        return 0, []
     x0, x1, y0, y1 = mesh.bounds
     pts = mesh.points[mesh.faces[mesh.boundary_faces]]
     xs, ys = pts[:, :, 0], pts[:, :, 1]
@@ -425,10 +423,47 @@ def neumann_sides(mesh, neumann) -> int:
         if side <= faces:
             bits |= 1 << bit
             covered |= side
-    if faces != covered:
-        raise NotImplementedError("Neumann data is supported on whole sides of the domain only "
-                                  "(the global solver's coarse operator takes them as Neumann ends)")
-    return bits
+    return bits, sorted(faces - covered)
+
+
+def coarse_partial_correction(mesh, bits: int, partial, ax: float, ay: float) -> tuple[np.ndarray, np.ndarray]:
+    """Woodbury factor of the coarse operator with Neumann faces on part of a side.
+
+    A_sep = ay (T_y (x) I) + ax (I (x) T_x) takes the whole Neumann sides in ``bits``
+    as Neumann ends and every other side as Dirichlet; each face in ``partial`` takes
+    its a_y (horizontal face) or a_x (vertical face) off its cell's diagonal:
+    A = A_sep - E D E^T.  Returns the m affected cells and R = A_sep^-1 E
+    (D^-1 - E^T A_sep^-1 E)^-1 (cells x m), so that A^-1 r = y + R (E^T y) with
+    y = A_sep^-1 r."""
+    from scipy import sparse
+    from scipy.sparse import linalg as splinalg
+
+    nx, ny = mesh.nx, mesh.ny
+
+    def factor(n, lo, hi):
+        t = sparse.diags([-np.ones(n - 1), 2.0 * np.ones(n), -np.ones(n - 1)], [-1, 0, 1], format="lil")
+        if lo:
+            t[0, 0] -= 1.0
+        if hi:
+            t[n - 1, n - 1] -= 1.0
+        return t.tocsr()
+
+    tx = factor(nx, bits & 4, bits & 8)
+    ty = factor(ny, bits & 1, bits & 2)
+    a_sep = (ay * sparse.kron(ty, sparse.identity(nx)) + ax * sparse.kron(sparse.identity(ny), tx)).tocsc()
+    weight = {}
+    for f in partial:
+        c = int(mesh.face_cells[f, 0])
+        p = mesh.points[mesh.faces[f]]
+        horizontal = p[0, 1] == p[1, 1]
+        weight[c] = weight.get(c, 0.0) + (ay if horizontal else ax)
+    cells = np.array(sorted(weight), dtype=np.int32)
+    d = np.array([weight[c] for c in cells])
+    e = np.zeros((nx * ny, len(cells)))
+    e[cells, np.arange(len(cells))] = 1.0
+    z = splinalg.splu(a_sep).solve(e)
+    cap = np.diag(1.0 / d) - z[cells]
+    return cells, np.ascontiguousarray(np.linalg.solve(cap.T, z.T).T)
 
 
 def coarse_x_basis(nx: int, bits: int) -> tuple[np.ndarray, np.ndarray]:

@@ -107,6 +107,14 @@ def main():
                     0.0, mixed, refine=True)
     np.savez_compressed(HERE / f"{name}.npz", **out)
     print(name, "fixed", len(out["fixed_dofs"]), "residual", out["residual"])
+    # Neumann data on part of two sides: an inflow through the middle of the left side,
+    # no flow through the first half of the bottom and the whole top, Dirichlet 0 elsewhere
+    partial = {f: -1.0 for f in side_faces(mesh, x=0.0)[1:3]}
+    partial.update({f: 0.0 for f in side_faces(mesh, 0.0)[:2] + side_faces(mesh, 1.0)})
+    out, name = run("darcy_4x4_r8_p2_partial_sides", mesh, FaceSpace.uniform(2), (8, 8), field, 0.0, 0.0, partial)
+    out["kappa"] = kap
+    np.savez_compressed(HERE / f"{name}.npz", **out)
+    print(name, "fixed", len(out["fixed_dofs"]), "residual", out["residual"])
     everywhere = {int(f): 0.25 for f in mesh.boundary_faces}  # outward flux 4 x 0.25 = the source's 1
     out, name = run("darcy_4x4_r8_p1_pure_neumann", mesh, FaceSpace.uniform(1), (8, 8), field, 1.0, 0.0,
                     everywhere, mean_pressure=0.3)

@@ -1,7 +1,7 @@
-"""GPU parity with Neumann faces on whole sides of the domain: the prescribed trace
-DOFs are eliminated (mhm_skeleton_fixed_rhs + the masked projected CG with Neumann
-ends of the coarse operator's 1-D factors) as PyMHM's solve_hybrid_system does with
-``fixed``."""
+"""GPU parity with Neumann faces: the prescribed trace DOFs are eliminated
+(mhm_skeleton_fixed_rhs + the masked projected CG, whose coarse operator takes whole
+Neumann sides as Neumann ends of its 1-D factors and corrects faces on parts of sides
+by a Woodbury factor) as PyMHM's solve_hybrid_system does with ``fixed``."""
 
 import numpy as np
 import pytest
@@ -68,10 +68,8 @@ def test_driver_accepts_neumann_sides():
     sol = solve_darcy_quadrilateral(mesh, skeleton=sk, local_refinement=ref, source=src, dirichlet=dr,
                                     neumann=neumann_map(g, val, mesh))
     assert rel(sol.fields, g["fields"]) <= 1e-10
-    part = {int(f): 0.0 for f in mesh.boundary_faces if np.all(mesh.points[mesh.faces[f]][:, 0] == 0.0)}
-    part.pop(min(part))
-    with pytest.raises(NotImplementedError, match="whole sides"):
-        solve_darcy_quadrilateral(mesh, skeleton=sk, local_refinement=ref, neumann=part)
+    with pytest.raises(ValueError, match="boundary faces"):
+        solve_darcy_quadrilateral(mesh, skeleton=sk, local_refinement=ref, neumann={int(mesh.faces.shape[0]) + 5: 0.0})
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])

@@ -16,6 +16,16 @@ def _left_flux(x):
     return 0.3 - 0.2 * x[:, 1]
 
 
+def _side(mesh, axis, value):
+    return [int(f) for f in mesh.boundary_faces if np.all(mesh.points[mesh.faces[f]][:, axis] == value)]
+
+
+def _partial_sides(mesh):
+    out = {f: -1.0 for f in _side(mesh, 0, 0.0)[1:3]}
+    out.update({f: 0.0 for f in _side(mesh, 1, 0.0)[:2] + _side(mesh, 1, 1.0)})
+    return out
+
+
 def _kappa(g):
     return o.PixelField(g["kappa"], (1 / 32, 1 / 32))
 
@@ -28,6 +38,9 @@ NEUMANN_CASES = {
     "darcy_4x4_r8_p2_noflow_lr": (2, (8, 8), _kappa, 1.0, lambda x: 1.0 - x[:, 1], {(0, 0.0): 0.0, (0, 1.0): 0.0}),
     "poisson_4x4_r4_p1_flux_left_bottom": (1, (4, 4), lambda g: 1.0, sine_source, 0.0,
                                            {(0, 0.0): _left_flux, (1, 0.0): _bottom_flux}),
+    # part of two sides (the middle of the left side, the first half of the bottom) and the
+    # whole top: the coarse operator's Woodbury correction
+    "darcy_4x4_r8_p2_partial_sides": (2, (8, 8), _kappa, 0.0, 0.0, lambda mesh: _partial_sides(mesh)),
     # every side Neumann (outward flux 0.25, balancing the unit source): the mean-pressure gauge
     "darcy_4x4_r8_p1_pure_neumann": (1, (8, 8), _kappa, 1.0, 0.0,
                                      {(1, 0.0): 0.25, (1, 1.0): 0.25, (0, 0.0): 0.25, (0, 1.0): 0.25}),
@@ -36,13 +49,18 @@ NEUMANN_CASES = {
 MEAN_PRESSURE = {"darcy_4x4_r8_p1_pure_neumann": 0.3}
 
 SIDE_BITS = {"darcy_4x4_r8_p2_noflow_tb": 3, "poisson_4x4_r4_p1_flux_bottom": 1, "darcy_4x4_r8_p2_noflow_lr": 12,
-             "poisson_4x4_r4_p1_flux_left_bottom": 5, "darcy_4x4_r8_p1_pure_neumann": 15}
+             "poisson_4x4_r4_p1_flux_left_bottom": 5, "darcy_4x4_r8_p1_pure_neumann": 15,
+             "darcy_4x4_r8_p2_partial_sides": 2}
 
 
 def neumann_map(g, sides, mesh=None):
     """The case's Neumann data per face; the faces are the fixture's."""
     if mesh is None:
         mesh = o.cartesian_mesh(4)
+    if callable(sides):
+        out = sides(mesh)
+        assert sorted(out) == [int(f) for f in g["neumann_faces"]]
+        return out
     out = {}
     for f in mesh.boundary_faces:
         pts = mesh.points[mesh.faces[f]]
@@ -72,7 +90,7 @@ def test_oracle_matches_reference(name):
 @pytest.mark.parametrize("name", list(NEUMANN_CASES))
 def test_host_boundary_data_matches_reference(name):
     from pymhm_b200.topology import (CartesianMacroMesh, FaceSpace, SkeletonSpace, boundary_data, neumann_fixed,
-                                     neumann_sides)
+                                     neumann_layout)
 
     g = load(name)
     deg, ref, perm, src, dr, val = NEUMANN_CASES[name]
@@ -84,25 +102,23 @@ def test_host_boundary_data_matches_reference(name):
     order = np.argsort(dofs)
     assert np.array_equal(dofs[order], g["fixed_dofs"])
     assert np.allclose(values[order], g["fixed_values"], rtol=0, atol=1e-15)
-    assert neumann_sides(mesh, neu) == SIDE_BITS[name]
+    assert neumann_layout(mesh, neu)[0] == SIDE_BITS[name]
 
 
 def test_neumann_side_rules():
-    from pymhm_b200.topology import CartesianMacroMesh, neumann_sides
+    from pymhm_b200.topology import CartesianMacroMesh, neumann_layout
 
     mesh = CartesianMacroMesh(4)
     pts = mesh.points[mesh.faces[mesh.boundary_faces]]
     bottom = [int(f) for f, p in zip(mesh.boundary_faces, pts) if np.all(p[:, 1] == 0.0)]
     top = [int(f) for f, p in zip(mesh.boundary_faces, pts) if np.all(p[:, 1] == 1.0)]
     left = [int(f) for f, p in zip(mesh.boundary_faces, pts) if np.all(p[:, 0] == 0.0)]
-    assert neumann_sides(mesh, None) == 0
-    assert neumann_sides(mesh, {f: 0.0 for f in top}) == 2
-    assert neumann_sides(mesh, {f: 0.0 for f in left}) == 4
-    with pytest.raises(NotImplementedError, match="whole sides"):
-        neumann_sides(mesh, {f: 0.0 for f in bottom[:2]})
-    with pytest.raises(NotImplementedError, match="whole sides"):
-        neumann_sides(mesh, {f: 0.0 for f in left + bottom[1:]})
-    assert neumann_sides(mesh, {int(f): 0.0 for f in mesh.boundary_faces}) == 15
+    assert neumann_layout(mesh, None) == (0, [])
+    assert neumann_layout(mesh, {f: 0.0 for f in top}) == (2, [])
+    assert neumann_layout(mesh, {f: 0.0 for f in left}) == (4, [])
+    assert neumann_layout(mesh, {f: 0.0 for f in bottom[:2]}) == (0, sorted(bottom[:2]))
+    assert neumann_layout(mesh, {f: 0.0 for f in left + bottom[1:]}) == (4, sorted(bottom[1:]))
+    assert neumann_layout(mesh, {int(f): 0.0 for f in mesh.boundary_faces}) == (15, [])
 
 
 @pytest.mark.parametrize("bits", [4, 8, 12])
@@ -132,3 +148,38 @@ def test_mode0_pseudo_inverse():
     p = coarse_mode0_pinv(ny, ay)
     assert np.allclose(p, np.linalg.pinv(t), atol=1e-13)
     assert np.allclose(p @ np.ones(ny), 0.0, atol=1e-13)
+
+
+def test_partial_side_correction_inverts_the_masked_coarse_operator():
+    """The Woodbury factor reproduces the inverse of G0^T G0 restricted to the free
+    DOFs (the coarse operator the skeleton solve projects with) for Neumann faces on
+    parts of sides."""
+    from pymhm_b200 import topology as tp
+
+    mesh = tp.CartesianMacroMesh(5, 4)
+    sk = tp.SkeletonSpace(mesh, (tp.FaceSpace.uniform(2),) * len(mesh.faces))
+    sh, sv = sk.uniform_by_orientation()
+    g0 = tp.geometric_constraint(mesh, sh, sv)
+    ax, ay = tp.coarse_coefficients(mesh, sh, sv)
+    cells = len(mesh.cells)
+    G = np.zeros((sk.size, cells))
+    for c in range(cells):
+        np.add.at(G[:, c], sk.cell_dof_array[c], g0[c])
+    neu = {f: 0.0 for f in _side(mesh, 1, 0.0)[:2] + _side(mesh, 0, 0.0)[1:3] + _side(mesh, 1, 1.0)}
+    bits, partial = tp.neumann_layout(mesh, neu)
+    assert bits == 2 and len(partial) == 4
+    fixed = np.concatenate([sk.dofs(f) for f in neu])
+    G[fixed] = 0.0
+    wb_cells, factor = tp.coarse_partial_correction(mesh, bits, partial, ax, ay)
+
+    def tri(n, lo, hi):
+        t = 2.0 * np.eye(n) - np.eye(n, k=1) - np.eye(n, k=-1)
+        t[0, 0] -= 1.0 if lo else 0.0
+        t[-1, -1] -= 1.0 if hi else 0.0
+        return t
+
+    a_sep = ay * np.kron(tri(4, bits & 1, bits & 2), np.eye(5)) + ax * np.kron(np.eye(4), tri(5, bits & 4, bits & 8))
+    r = np.random.default_rng(3).normal(size=cells)
+    y = np.linalg.solve(a_sep, r)
+    exact = np.linalg.solve(G.T @ G, r)
+    assert np.max(np.abs(y + factor @ y[wb_cells] - exact)) <= 1e-13 * np.max(np.abs(exact))
