@@ -25,7 +25,7 @@
  *                          (core/system.py:355-528 -> linalg/linear.py:798)
  *                          for systems without gauges; with
  *   mhm_skeleton_fixed_rhs its elimination of fixed (Neumann) trace DOFs
- *                          (core/system.py:421-447) on whole sides.
+ *                          (core/system.py:421-447).
  *   mhm_q1_reconstruct     replaces reconstruct_response (core/reconstruction.py:
  *                          130-141) and the flux samples of
  *                          QuadrilateralDarcySolution.evaluate
@@ -293,10 +293,10 @@ typedef struct mhm_skeleton_system {
      * faces' prescribed coefficients (core/system.py:421-447).  The solve then
      * works on the free DOFs: rhs must hold rhs - K x_fixed with zeros on the
      * fixed rows (mhm_skeleton_fixed_rhs), x is returned zero on them and the
-     * caller adds x_fixed.  The fixed DOFs must be all DOFs of the faces of the
-     * whole bottom, top, left and/or right sides, which the coarse
-     * operator takes as Neumann ends of T_y (coarse_neumann bit 0 = bottom y = y0,
-     * bit 1 = top) and of T_x (bit 2 = left x = x0, bit 3 = right).             */
+     * caller adds x_fixed.  The fixed DOFs are all DOFs of their faces.  Whole
+     * fixed sides are Neumann ends of T_y (coarse_neumann bit 0 = bottom y = y0,
+     * bit 1 = top) and of T_x (bit 2 = left x = x0, bit 3 = right); faces on
+     * parts of sides go through coarse_partial below.                           */
     const uint8_t* fixed;
     int32_t coarse_neumann;
     /* With coarse_neumann bit 2 (left side x = x0 fixed) or bit 3 (right side):

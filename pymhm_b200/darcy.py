@@ -343,7 +343,7 @@ class CartesianQ1Plan:
         self.pattern = skeleton_pattern(self.cell_dofs_h, self.T)
         dof_cells, dof_slot = dof_cell_maps(self.cell_dofs_h, self.T)
         g0 = geometric_constraint(m, space_h, space_v)
-        # Neumann faces (whole bottom / top sides): their trace DOFs are prescribed
+        # Neumann faces: their trace DOFs are prescribed
         # (boundary_data's `fixed`) and eliminated from the global solve
         self.neumann_bits, neumann_partial = neumann_layout(m, neumann)
         self.boundary_h = boundary_data(sk, dirichlet, self.order, neumann)
