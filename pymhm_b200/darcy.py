@@ -30,21 +30,20 @@ from numpy.polynomial.legendre import leggauss
 
 from . import _lib
 from .errors import LinearSolveError
+from .skeleton import attach_fixed
 from .topology import (
     CartesianMacroMesh,
     FaceSpace,
     SkeletonSpace,
     boundary_data,
-    coarse_mode0_pinv,
-    coarse_x_basis,
-    coarse_partial_correction,
-    neumann_fixed,
-    neumann_layout,
     coarse_coefficients,
     coupling_tables,
     dof_cell_maps,
+    fixed_coarse_data,
     geometric_constraint,
     mesh_arrays,
+    neumann_fixed,
+    neumann_layout,
     side_orientation,
     skeleton_pattern,
 )
@@ -415,23 +414,13 @@ class CartesianQ1Plan:
         s.coarse_ax, s.coarse_ay = self.coarse_ab
         s.cell_blocks, s.block_ld = _lib.ptr(self.blocks), self.t + 1
         self.d_fixed = self.d_xfixed = None
-        if self.neumann_bits:
-            mask = np.zeros(self.T, dtype=np.uint8)
-            mask[fixed_dofs] = 1
+        if neumann:  # any Neumann face, on whole sides or on parts of them
+            self._fixed_keep = attach_fixed(s, fixed_coarse_data(m, sk, neumann, *self.coarse_ab), up)
+            self.d_fixed = self._fixed_keep["mask"]
             xfixed = np.zeros(self.N)
             xfixed[fixed_dofs] = fixed_values
-            self.d_fixed, self.d_xfixed = up(mask, torch.uint8), up(xfixed, torch.float64)
-            s.fixed, s.coarse_neumann = _lib.ptr(self.d_fixed), self.neumann_bits
+            self.d_xfixed = up(xfixed, torch.float64)
             self.rhs_red = torch.empty(self.N, dtype=torch.float64, device=dev)
-            if neumann_partial:  # Neumann faces on part of a side: Woodbury factor of the coarse operator
-                cells, factor = coarse_partial_correction(m, self.neumann_bits, neumann_partial, *self.coarse_ab)
-                self.d_wb_cells, self.d_wb_R = up(cells, torch.int32), up(factor, torch.float64)
-                s.coarse_partial = len(cells)
-                s.coarse_partial_cells, s.coarse_partial_R = _lib.ptr(self.d_wb_cells), _lib.ptr(self.d_wb_R)
-            if self.neumann_bits & 12:  # Neumann left/right sides: T_x eigenbasis from the host
-                qx, lamx = coarse_x_basis(m.nx, self.neumann_bits)
-                self.d_qx, self.d_lamx = up(qx, torch.float64), up(lamx, torch.float64)
-                s.coarse_qx, s.coarse_lamx = _lib.ptr(self.d_qx), _lib.ptr(self.d_lamx)
         # pure Neumann: the mean-pressure condition sum_cells C . u = mean_pressure |domain|
         # fixes the constant coarse mode (cartesian.py:136-142)
         self.pure_neumann = self.neumann_bits == 15 and not neumann_partial
@@ -440,8 +429,6 @@ class CartesianQ1Plan:
             self.mean_value = float(mean_pressure) * (x1 - x0) * (y1 - y0)
             if not np.isfinite(self.mean_value):
                 raise ValueError("mean_pressure must be finite")
-            self.d_pinv0 = up(coarse_mode0_pinv(m.ny, self.coarse_ab[1]), torch.float64)
-            s.coarse_pinv0 = _lib.ptr(self.d_pinv0)
             self.gauge = torch.empty(2 * self.cells + 1, dtype=torch.float64, device=dev)
         nbytes = self.lib.mhm_skeleton_workspace_bytes(s, self.grid)
         if nbytes <= 0:

@@ -495,6 +495,27 @@ def coarse_mode0_pinv(ny: int, ay: float) -> np.ndarray:
     return np.ascontiguousarray((vec[:, keep] / lam[keep]) @ vec[:, keep].T / ay)
 
 
+def fixed_coarse_data(mesh, skeleton: SkeletonSpace, fixed_faces, ax: float, ay: float) -> dict:
+    """Host data of a skeleton solve whose trace DOFs on ``fixed_faces`` (boundary
+    faces) are prescribed: the DOF mask, the whole fixed sides (``neumann_layout``
+    bits), the x eigenbasis when the left or right side is fixed, the mode-0
+    pseudo-inverse when every side is, and the Woodbury factor of faces on parts of
+    sides (None where not needed)."""
+    faces = sorted(set(int(f) for f in fixed_faces))
+    bits, partial = neumann_layout(mesh, {f: 0.0 for f in faces})
+    mask = np.zeros(skeleton.size, dtype=np.uint8)
+    for f in faces:
+        mask[skeleton.dofs(f)] = 1
+    out = dict(mask=mask, bits=bits, qx=None, lamx=None, pinv0=None, wb_cells=None, wb_R=None)
+    if bits & 12:
+        out["qx"], out["lamx"] = coarse_x_basis(mesh.nx, bits)
+    if bits == 15 and not partial:
+        out["pinv0"] = coarse_mode0_pinv(mesh.ny, ay)
+    if partial:
+        out["wb_cells"], out["wb_R"] = coarse_partial_correction(mesh, bits, partial, ax, ay)
+    return out
+
+
 # ----------------------------------------------------------------------------------------
 # Global pattern and solver maps
 # ----------------------------------------------------------------------------------------

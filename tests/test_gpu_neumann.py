@@ -114,3 +114,59 @@ def test_pure_neumann_mean_pressure_and_refinement_guard():
     assert abs(mean - 0.3) <= 1e-12
     with pytest.raises(NotImplementedError, match="physical"):
         plan.refine(max_steps=1)
+
+
+def test_neumann_faces_on_parts_of_sides_only():
+    """No whole side Neumann: the prescribed faces still leave the solve (the plan keys
+    the fixed-DOF set-up on any Neumann face, not on whole sides)."""
+    from oracle import q1_mhm as o
+    from pymhm_b200.darcy import CartesianQ1Plan
+    from pymhm_b200.topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
+    from pymhm_b200.workloads import sine_source
+
+    mesh = CartesianMacroMesh(4)
+    bottom = [int(f) for f in mesh.boundary_faces if np.all(mesh.points[mesh.faces[f]][:, 1] == 0.0)]
+    right = [int(f) for f in mesh.boundary_faces if np.all(mesh.points[mesh.faces[f]][:, 0] == 1.0)]
+    neumann = {bottom[1]: 0.4, bottom[2]: 0.4, right[3]: -0.2}
+    sk = SkeletonSpace(mesh, (FaceSpace.uniform(1),) * len(mesh.faces))
+    plan = CartesianQ1Plan(mesh, sk, (4, 4), neumann=neumann)
+    assert plan.neumann_bits == 0 and plan.d_fixed is not None
+    plan.set_coefficients(1.0, sine_source)
+    plan.launch()
+    sol = plan.result()
+    om = o.cartesian_mesh(4)
+    osk = o.Skeleton(om, (o.FaceSpace.uniform(1),) * len(om.faces))
+    ref = o.solve_darcy_q1(om, osk, (4, 4), 1.0, sine_source, neumann=neumann)
+    assert rel(sol.trace, ref.trace) <= 1e-10
+    assert rel(sol.fields, ref.fields) <= 1e-10
+    assert rel(sol.flux, ref.flux) <= 1e-10
+
+
+def test_skeleton_factorization_serves_the_reduced_system():
+    """SkeletonFactorization(fixed=...) behind solve_hybrid_system(fixed=...): it matches
+    the system with the fixed rows and columns removed and solves it
+    (core/system.py:421-457), here on the reference's own partial-sides system."""
+    from scipy import sparse
+
+    from pymhm_b200 import SkeletonFactorization
+    from pymhm_b200.topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
+
+    g = load("darcy_4x4_r8_p2_partial_sides")
+    mesh = CartesianMacroMesh(4)
+    sk = SkeletonSpace(mesh, (FaceSpace.uniform(2),) * len(mesh.faces))
+    n = len(g["rhs"])
+    matrix = sparse.csc_matrix((g["data"], g["indices"], g["indptr"]), shape=(n, n))
+    fixed = g["fixed_dofs"]
+    x = np.zeros(n)
+    x[fixed] = g["fixed_values"]
+    free = np.setdiff1d(np.arange(n), fixed)
+    reduced = matrix[free][:, free]
+    rhs = g["rhs"][free] - (matrix @ x)[free]
+    with SkeletonFactorization(matrix, mesh, sk, fixed=fixed) as fact:
+        assert fact.matches(reduced) and not fact.matches(matrix)
+        x[free] = fact.solve(rhs)
+    t = sk.size
+    assert rel(x[:t], g["trace"]) <= 1e-10
+    assert rel(x[t:], g["coarse"]) <= 1e-10
+    with pytest.raises(NotImplementedError, match="all trace DOFs"):
+        SkeletonFactorization(matrix, mesh, sk, fixed=fixed[:-1])
