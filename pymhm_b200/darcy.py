@@ -644,11 +644,12 @@ class CartesianQ1Plan:
         the prescribed trace coefficients stay as they are: the right-hand-side norm
         takes the loads less their coupling and the free DOFs' boundary data, the
         weak residual counts the free DOFs, and each correction solves with those
-        DOFs held at zero (``refinement.py:676-709, 792``).
+        DOFs held at zero (``refinement.py:676-709, 792``).  A pure-Neumann solve carries
+        its mean-pressure moment as the reference's ``moments``: the residual includes
+        the moment defect value - sum_cells C . u, the right-hand-side norm the value,
+        and each correction is gauged to the moment defect (``refinement.py:690-700,
+        725-733, 787-797``).
         """
-        if self.pure_neumann:
-            raise NotImplementedError("original-equation refinement of a pure-Neumann solve needs its physical "
-                                      "moments (refinement.py:676-703), which are not on the GPU path")
         _step_limits(max_steps, min_steps)
         _tolerances(rtol, atol)
         torch, L, P = self.torch, self.lib, _lib.ptr
@@ -661,7 +662,8 @@ class CartesianQ1Plan:
             self._refine = dict(defect=torch.empty((M, n), **f64), slots=torch.empty((M, t), **f64),
                                 weak=torch.empty(self.T, **f64), partial=torch.empty((M, 3), **f64),
                                 norms=torch.empty(5 + 5 * 256, **f64), dx=torch.empty(self.N, **f64),
-                                zero=torch.zeros(self.N, **f64),
+                                zero=torch.zeros(self.N, **f64), gauge_x=torch.zeros(self.N, **f64),
+                                gauge_partial=torch.zeros(2 * M + 1, **f64), shift=torch.zeros(self.N, **f64),
                                 rhs=torch.empty(self.N, **f64), scale=torch.empty(self.N, **f64),
                                 dfields=torch.empty((M, n), **f64))
         B = self._refine
@@ -680,8 +682,16 @@ class CartesianQ1Plan:
                                           P(self.d_boundary), self.N,
                                           P(self.d_indptr), P(self.d_indices), P(self.values), P(self.x),
                                           P(self.rhs), P(B["norms"]), s), "mhm_refine_norms")
+            moment_defect = 0.0
+            if self.pure_neumann:  # sum_cells C . u from the gauge kernel's per-cell partials
+                _lib.check(L.mhm_q1_mean_gauge(self.q1, P(self.solution), P(self.fields), 0.0, self.T,
+                                               P(B["gauge_x"]), P(B["gauge_partial"]), s), "mhm_q1_mean_gauge")
             cur.synchronize()
             norms = B["norms"][:5].cpu().numpy()
+            if self.pure_neumann:
+                moment_defect = self.mean_value - float(np.sum(B["gauge_partial"][0:2 * M:2].cpu().numpy()))
+                norms[0] += moment_defect * moment_defect
+                norms[1] += self.mean_value * self.mean_value
             residual, rhs_norm = math.sqrt(norms[0]), math.sqrt(norms[1])
             history.append(residual)
             threshold = max(atol, rtol * rhs_norm)
@@ -706,10 +716,24 @@ class CartesianQ1Plan:
                 _lib.check(L.mhm_skeleton_fixed_rhs(self.N, self.T, P(self.d_indptr), P(self.d_indices),
                                                     P(self.values), P(self.d_fixed), P(B["zero"]), P(B["rhs"]),
                                                     P(B["rhs"]), s), "mhm_skeleton_fixed_rhs")
+            if self.pure_neumann:
+                # The correction's loads come from binary64 defects, so their component
+                # along the kernel of the system (a uniform shift of the coarse unknowns)
+                # is rounding of the defects, not of the data.  The reference's bordered
+                # solve absorbs it in its multiplier; here it leaves the right-hand side.
+                cur.synchronize()
+                mean = float(np.mean(B["rhs"][self.T:].cpu().numpy()))
+                B["shift"][self.T:].fill_(-mean)
+                _lib.check(L.mhm_vector_accumulate(self.N, P(B["rhs"]), P(B["shift"]), s), "mhm_vector_accumulate")
             _lib.check(L.mhm_skeleton_solve(self.sys, P(B["rhs"]), P(B["scale"]), P(B["dx"]), self.global_rtol,
                                             self.inner_rtol, self.max_inner, self.max_outer, self.grid,
                                             P(self.workspace), self.workspace.numel(), P(self.info), P(self.stats),
                                             s), "mhm_skeleton_solve")
+            if self.pure_neumann:  # the correction carries the moment defect (its gauge row)
+                _lib.check(L.mhm_q1_reconstruct(self.q1, P(self.solution), P(self.d_cell_dofs), self.T, P(B["dx"]),
+                                                P(B["dfields"]), None, s), "mhm_q1_reconstruct")
+                _lib.check(L.mhm_q1_mean_gauge(self.q1, P(self.solution), P(B["dfields"]), moment_defect, self.T,
+                                               P(B["dx"]), P(B["gauge_partial"]), s), "mhm_q1_mean_gauge")
             _lib.check(L.mhm_q1_reconstruct(self.q1, P(self.solution), P(self.d_cell_dofs), self.T, P(B["dx"]),
                                             P(B["dfields"]), None, s), "mhm_q1_reconstruct")
             for dst, src in ((self.x, B["dx"]), (self.fields, B["dfields"])):

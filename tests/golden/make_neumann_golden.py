@@ -3,8 +3,9 @@ PyMHM itself: ``boundary_data`` prescribes those faces' trace coefficients (the 
 projection of the outward normal flux) and ``HybridSystem.solve(fixed=...)``
 eliminates them, as ``solve_darcy_quadrilateral`` does (``_legacy/models/darcy/
 cartesian.py:122-143``, ``core/system.py:421-447``).  For the left-and-bottom flux
-case it also runs ``refine_hybrid`` with ``fixed`` from a perturbed solution (every
-local field plus 0.002 * (1, ..., n), as the reference's refinement test does).
+case and the pure-Neumann case it also runs ``refine_hybrid`` with ``fixed`` (and, for
+the latter, the mean-pressure moment) from a perturbed solution (every local field
+plus 0.002 * (1, ..., n), as the reference's refinement test does).
 
     PYMHM_SRC=/path/to/pymhm/src python tests/golden/make_neumann_golden.py
 
@@ -51,15 +52,17 @@ def run(name, mesh, face_space, refinement, permeability, source, dirichlet, neu
     boundary, fixed = boundary_data(sk, dirichlet, neumann, order=order)
     tasks = [_QuadTask(mesh, c, refinement, sk, 1, permeability, source, order) for c in range(len(mesh.cells))]
     system = HybridSystem.from_local_factory(_assemble_quad, tasks, boundary_load=boundary)
-    constraints = None
+    constraints, moments = None, ()
     if mean_pressure is not None:  # pure Neumann: the driver's mean-pressure row (cartesian.py:135-142)
         _, means = zip(*system.local_metadata)
         constraints = [system.mean_constraint(means, mean_pressure * float(np.sum(mesh.areas)))]
+        moments = ((means, mean_pressure * float(np.sum(mesh.areas))),)
     hybrid = system.solve(fixed=fixed, constraints=constraints)
     extra = {}
     if refine:
         perturbed = replace(hybrid, fields=tuple(u + 0.002 * np.arange(1, len(u) + 1) for u in hybrid.fields))
-        result = refine_hybrid(system, perturbed, boundary_load=boundary, fixed=fixed, max_steps=2, rtol=1e-10)
+        result = refine_hybrid(system, perturbed, boundary_load=boundary, fixed=fixed, moments=moments,
+                               max_steps=2, rtol=1e-10)
         extra = dict(
             refine_start_fields=np.array(perturbed.fields), refine_residual_norms=np.array(result.residual_norms),
             refine_rhs_norm=result.rhs_norm, refine_reduced=result.solution.residual,
@@ -117,7 +120,7 @@ def main():
     print(name, "fixed", len(out["fixed_dofs"]), "residual", out["residual"])
     everywhere = {int(f): 0.25 for f in mesh.boundary_faces}  # outward flux 4 x 0.25 = the source's 1
     out, name = run("darcy_4x4_r8_p1_pure_neumann", mesh, FaceSpace.uniform(1), (8, 8), field, 1.0, 0.0,
-                    everywhere, mean_pressure=0.3)
+                    everywhere, mean_pressure=0.3, refine=True)
     out["kappa"] = kap
     np.savez_compressed(HERE / f"{name}.npz", **out)
     print(name, "fixed", len(out["fixed_dofs"]), "residual", out["residual"])
