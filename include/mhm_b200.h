@@ -105,9 +105,15 @@ typedef struct mhm_q1_problem {
                                      3 isotropic per pixel, 4 (kxx,kxy,kyy) per
                                      pixel: a pixel field whose lines may cut the
                                      fine cells, integrated exactly on each
-                                     intersection (quadrilateral.py:136-188)       */
+                                     intersection (quadrilateral.py:136-188),
+                                     5 isotropic / 6 (kxx,kxy,kyy) per Gauss point
+                                     of every fine cell (quad_order points a side),
+                                     integrated by that rule                       */
     const double* kappa;          /* modes 1/2: global fine grid [gx][gy][comp];
-                                     modes 3/4: pixels [px][py][comp] (x-major)    */
+                                     modes 3/4: pixels [px][py][comp] (x-major);
+                                     modes 5/6: [gx][gy][Q*Q + 1][comp], point
+                                     qy*Q + qx, the last one the fine-cell centre
+                                     (for the flux)                                */
     double kappa_const[3];        /* kxx, kxy, kyy for kappa_mode 0                */
     int32_t source_mode;          /* 0 constant, 1 per fine cell,
                                      2 per Gauss point of the fine cell,
@@ -120,7 +126,7 @@ typedef struct mhm_q1_problem {
     double pixel_spacing[2];      /* kappa_mode 3/4: pixel widths                 */
     int32_t pixel_nx, pixel_ny;   /* kappa_mode 3/4: pixel counts; the field must
                                      cover the domain                              */
-    double* cut_elements;         /* kappa_mode 3/4: device work buffer of
+    double* cut_elements;         /* kappa_mode 3-6: device work buffer of
                                      10 x (global fine cells) doubles: the lower
                                      triangle of each fine cell's element stiffness,
                                      entry-major [entry][gx][gy]; every local entry

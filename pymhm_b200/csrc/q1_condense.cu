@@ -183,6 +183,47 @@ __device__ __forceinline__ void cut_element(const Q1Args& a, double ex0, double 
 }
 
 // Pre-pass of the cut-cell modes: thread per global fine cell g = gx * NYf + gy.
+// Pre-pass of the quadrature modes (kappa_mode 5/6, a permeability that varies inside
+// the fine cells, given at the Gauss points): thread per global fine cell, the lower
+// triangle of sum_q w_q area grad(phi_a) . K_q grad(phi_c), the reference's tensor
+// Gauss rule (quadrilateral.py:191-253, _integration.py:43-88), in the cut-cell
+// layout.  kappa: [gx][gy][Q*Q + 1][comp], point q = qy Q + qx, the last one the centre.
+__global__ void __launch_bounds__(256) quad_element_kernel(const Q1Args a) {
+  const int64_t total = (int64_t)a.nx * a.rx * a.NYf;
+  const int Q = a.qorder, qq = Q * Q;
+  const int comp = a.kmode == 5 ? 1 : 3;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    double km[10];
+#pragma unroll
+    for (int q = 0; q < 10; ++q) km[q] = 0.0;
+    const double* kg = a.kappa + (size_t)g * (qq + 1) * comp;
+    for (int qy = 0; qy < Q; ++qy)
+      for (int qx = 0; qx < Q; ++qx) {
+        const double xi = a.gpt[qx], eta = a.gpt[qy], wq = a.gwt[qx] * a.gwt[qy] * a.area;
+        const double* k = kg + (size_t)(qy * Q + qx) * comp;
+        const double kxx = k[0], kxy = comp == 3 ? k[1] : 0.0, kyy = comp == 3 ? k[2] : k[0];
+        const double X[2] = {1.0 - xi, xi}, Y[2] = {1.0 - eta, eta};
+        double gxv[4], gyv[4];
+#pragma unroll
+        for (int A = 0; A < 4; ++A) {
+          const int ax = A & 1, ay = A >> 1;
+          gxv[A] = (ax ? 1.0 : -1.0) * Y[ay] / a.hx;
+          gyv[A] = X[ax] * (ay ? 1.0 : -1.0) / a.hy;
+        }
+#pragma unroll
+        for (int A = 0; A < 4; ++A)
+#pragma unroll
+          for (int C = 0; C <= A; ++C) {
+            const double kc_x = kxx * gxv[C] + kxy * gyv[C], kc_y = kxy * gxv[C] + kyy * gyv[C];
+            km[A * (A + 1) / 2 + C] += wq * (gxv[A] * kc_x + gyv[A] * kc_y);
+          }
+      }
+#pragma unroll
+    for (int q = 0; q < 10; ++q) a.cut[q * a.cut_stride + g] = km[q];
+  }
+}
+
 __global__ void __launch_bounds__(256) cut_element_kernel(const Q1Args a) {
   const int64_t total = (int64_t)a.nx * a.rx * a.NYf;
   for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total;
@@ -1015,11 +1056,14 @@ __device__ __forceinline__ void cell_flux(const Q1Args& a, int cell, const doubl
     const double gx = (-u0 + u1 - u2 + u3) * (0.5 / a.hx);
     const double gy = (-u0 - u1 + u2 + u3) * (0.5 / a.hy);
     size_t g = (size_t)(cx * a.rx + ex) * a.NYf + (cy * a.ry + ey);
-    if (a.cut_mode) g = centre_pixel(a, cx * a.rx + ex, cy * a.ry + ey);
+    if (a.kmode >= 5)  // quadrature modes: the value stored after the Gauss points
+      g = g * (size_t)(a.qorder * a.qorder + 1) + (size_t)(a.qorder * a.qorder);
+    else if (a.cut_mode)
+      g = centre_pixel(a, cx * a.rx + ex, cy * a.ry + ey);
     double kxx, kxy, kyy;
     if (a.kmode == 0) {
       kxx = a.k0; kxy = a.k1; kyy = a.k2;
-    } else if (a.kmode == 1 || a.kmode == 3) {
+    } else if (a.kmode == 1 || a.kmode == 3 || a.kmode == 5) {
       kxx = kyy = a.kappa[g]; kxy = 0.0;
     } else {
       kxx = a.kappa[3 * g]; kxy = a.kappa[3 * g + 1]; kyy = a.kappa[3 * g + 2];
@@ -1265,9 +1309,11 @@ void gauss01(int m, double* x, double* wts) {
 int fill_args(const mhm_q1_problem* p, int precision, Q1Args& a) {
   if (!p || p->macro_nx < 1 || p->macro_ny < 1 || p->rx < 1 || p->ry < 1) return MHM_ERR_ARGUMENT;
   if (!(p->hx > 0) || !(p->hy > 0) || p->tf_h < 1 || p->tf_v < 1) return MHM_ERR_ARGUMENT;
-  if (p->kappa_mode < 0 || p->kappa_mode > 4 || p->source_mode < 0 || p->source_mode > 3)
+  if (p->kappa_mode < 0 || p->kappa_mode > 6 || p->source_mode < 0 || p->source_mode > 3)
     return MHM_ERR_ARGUMENT;
-  if (p->kappa_mode >= 3 &&
+  if (p->kappa_mode >= 5 && (p->quad_order < 1 || p->quad_order > kMaxQuad || !p->cut_elements))
+    return MHM_ERR_ARGUMENT;
+  if ((p->kappa_mode == 3 || p->kappa_mode == 4) &&
       (p->pixel_nx < 1 || p->pixel_ny < 1 || !(p->pixel_spacing[0] > 0) || !(p->pixel_spacing[1] > 0) ||
        !std::isfinite(p->pixel_origin[0]) || !std::isfinite(p->pixel_origin[1]) || !p->cut_elements))
     return MHM_ERR_ARGUMENT;
@@ -1289,9 +1335,11 @@ int fill_args(const mhm_q1_problem* p, int precision, Q1Args& a) {
   a.cut_mode = a.kmode >= 3;
   a.x0 = p->x0; a.y0 = p->y0;
   if (a.kmode >= 3) {
-    a.px0 = p->pixel_origin[0]; a.py0 = p->pixel_origin[1];
-    a.psx = p->pixel_spacing[0]; a.psy = p->pixel_spacing[1];
-    a.pnx = p->pixel_nx; a.pny = p->pixel_ny;
+    if (a.kmode <= 4) {
+      a.px0 = p->pixel_origin[0]; a.py0 = p->pixel_origin[1];
+      a.psx = p->pixel_spacing[0]; a.psy = p->pixel_spacing[1];
+      a.pnx = p->pixel_nx; a.pny = p->pixel_ny;
+    }
     a.cut = p->cut_elements;
     a.cut_stride = (int64_t)a.nx * a.rx * a.NYf;
   }
@@ -1367,7 +1415,10 @@ void launch_cut_elements(const Q1Args& a, cudaStream_t s) {
   const int64_t total = (int64_t)a.nx * a.rx * a.NYf;
   int64_t grid = (total + 255) / 256;
   if (grid > 148 * 16) grid = 148 * 16;
-  cut_element_kernel<<<(int)grid, 256, 0, s>>>(a);
+  if (a.kmode >= 5)
+    quad_element_kernel<<<(int)grid, 256, 0, s>>>(a);
+  else
+    cut_element_kernel<<<(int)grid, 256, 0, s>>>(a);
 }
 
 int run_condense(const mhm_q1_problem* p, int32_t precision, int32_t max_refine, double tol, double* solution,

@@ -194,21 +194,29 @@ def permeability_input(permeability, mesh: CartesianMacroMesh, rx: int, ry: int,
         mode, comp = _tensor_components(sampled)
         return mode, comp, (0.0, 0.0, 0.0)
     if callable(permeability):
+        # at the Gauss points of every fine cell: one value per cell if it is constant
+        # there (modes 1/2), else every point plus the centre for the flux (modes 5/6)
         pts = _quad_points(mesh, rx, ry, order)
         raw = np.asarray(permeability(pts), dtype=float)
         q = order * order
         if raw.shape == (len(pts),):
             per = raw.reshape(nxf, nyf, q)
-            if np.any(per != per[..., :1]):
-                raise NotImplementedError("permeability must be constant on each fine cell")
-            mode, comp = _tensor_components(per[..., 0])
-            return mode, comp, (0.0, 0.0, 0.0)
+            if np.all(per == per[..., :1]):
+                mode, comp = _tensor_components(per[..., 0])
+                return mode, comp, (0.0, 0.0, 0.0)
+            centre = np.asarray(permeability(_fine_centres(mesh, rx, ry)), dtype=float).reshape(nxf, nyf, 1)
+            full = np.concatenate((per, centre), axis=2)
+            mode, comp = _tensor_components(full.reshape(nxf, nyf * (q + 1)))
+            return 5, comp.reshape(nxf, nyf, q + 1), (0.0, 0.0, 0.0)
         if raw.shape == (len(pts), 2, 2):
             per = raw.reshape(nxf, nyf, q, 2, 2)
-            if np.any(per != per[:, :, :1]):
-                raise NotImplementedError("permeability must be constant on each fine cell")
-            mode, comp = _tensor_components(per[:, :, 0])
-            return mode, comp, (0.0, 0.0, 0.0)
+            if np.all(per == per[:, :, :1]):
+                mode, comp = _tensor_components(per[:, :, 0])
+                return mode, comp, (0.0, 0.0, 0.0)
+            centre = np.asarray(permeability(_fine_centres(mesh, rx, ry)), dtype=float).reshape(nxf, nyf, 1, 2, 2)
+            full = np.concatenate((per, centre), axis=2)
+            mode, comp = _tensor_components(full.reshape(nxf, nyf * (q + 1), 2, 2))
+            return 6, comp.reshape(nxf, nyf, q + 1, 3), (0.0, 0.0, 0.0)
         raise ValueError("permeability callable must return scalars or 2x2 tensors per point")
     raise TypeError("unsupported permeability description")
 
@@ -441,7 +449,7 @@ class CartesianQ1Plan:
         torch = self.torch
         kmode, karr, kconst = permeability_input(permeability, self.mesh, self.rx, self.ry, self.order)
         smode, sarr, sconst = source_input(source, self.mesh, self.rx, self.ry, self.order)
-        pixels = pixel_geometry(permeability, self.mesh, self.rx, self.ry) if kmode >= 3 else None
+        pixels = pixel_geometry(permeability, self.mesh, self.rx, self.ry) if kmode in (3, 4) else None
         self.kappa = None if karr is None else torch.as_tensor(np.array(karr)).to(self.device, non_blocking=non_blocking)
         self.source = None if sarr is None else torch.as_tensor(np.array(sarr)).to(self.device, non_blocking=non_blocking)
         self.set_device_coefficients(kmode, self.kappa, kconst, smode, self.source, sconst, pixels=pixels)
@@ -450,14 +458,16 @@ class CartesianQ1Plan:
         """Point the plan at device-resident coefficient tensors (no copies).
 
         ``pixels`` = (origin, spacing, counts) is required for the cut-cell modes 3/4,
-        where ``kappa`` holds pixel values [px][py][comp]."""
+        where ``kappa`` holds pixel values [px][py][comp]; modes 5/6 hold the values at
+        the fine cells' Gauss points and centres [gx][gy][Q*Q + 1][comp]."""
         q = self.q1
-        if kmode >= 3:
+        if kmode in (3, 4):
             if pixels is None:
                 raise ValueError("kappa modes 3 and 4 need the pixel geometry")
             _cut_source_check(smode)
             (q.pixel_origin[0], q.pixel_origin[1]), (q.pixel_spacing[0], q.pixel_spacing[1]), \
                 (q.pixel_nx, q.pixel_ny) = pixels
+        if kmode >= 3:  # element matrices from a pre-pass
             if getattr(self, "cut_elements", None) is None:
                 self.cut_elements = self.torch.empty(10 * self.nxf * self.nyf, dtype=self.torch.float64,
                                                      device=self.device)

@@ -21,6 +21,15 @@ class PixelField:
         return OP(self.values, self.spacing, self.origin)(pts)
 
 
+def smooth_tensor(x):
+    """The anisotropic test field of the smooth-tensor fixture (make_quadrature_golden.py):
+    K = [[exp(sin 2 pi x cos 2 pi y), 0.3 sin(pi x y)], [0.3 sin(pi x y), 1 + x y]]."""
+    k1 = np.exp(np.sin(2 * np.pi * x[:, 0]) * np.cos(2 * np.pi * x[:, 1]))
+    k2 = 1.0 + x[:, 0] * x[:, 1]
+    k12 = 0.3 * np.sin(np.pi * x[:, 0] * x[:, 1])
+    return np.stack((np.stack((k1, k12), -1), np.stack((k12, k2), -1)), -2)
+
+
 def quad_source(x):
     return 1.0 + x[:, 0] * x[:, 1]
 
@@ -47,6 +56,8 @@ CASES = {
                                    lambda g: PixelField(g["kappa"], (1 / 64, 1 / 64)), 1.0, 0.0),
     "darcy_4x4_r8_p1_cut20": ((4,), (1, 1), (8, 8),
                               lambda g: PixelField(g["kappa"], (1 / 20, 1 / 20)), 1.0, 0.0),
+    # a permeability that varies inside the fine cells (Gauss-point values, kappa mode 6)
+    "darcy_4x4_r8_p1_smooth_tensor": ((4,), (1, 1), (8, 8), lambda g: smooth_tensor, 1.0, 0.0),
     # continuous piecewise-linear traces on two segments per face (3 DOFs a face)
     "darcy_4x4_r8_p1c2_lognormal": ((4,), (1, 2, True), (8, 8),
                                     lambda g: PixelField(g["kappa"], (1 / 32, 1 / 32)), 1.0, 0.0),

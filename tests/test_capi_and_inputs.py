@@ -116,8 +116,16 @@ def test_callable_inputs():
     mesh = CartesianMacroMesh(2)
     mode, arr, _ = permeability_input(lambda p: 1.0 + (p[:, 0] > 0.5), mesh, 4, 4, 4)
     assert mode == 1 and arr.shape == (8, 8) and arr[0, 0] == 1.0 and arr[7, 0] == 2.0
-    with pytest.raises(NotImplementedError, match="constant on each fine cell"):
-        permeability_input(lambda p: 1.0 + p[:, 0], mesh, 4, 4, 4)
+    # varying inside the fine cells: every Gauss point plus the centre (modes 5/6)
+    mode, arr, _ = permeability_input(lambda p: 1.0 + p[:, 0], mesh, 4, 4, 4)
+    assert mode == 5 and arr.shape == (8, 8, 17)
+    assert np.isclose(arr[0, 0, 16], 1.0 + 1 / 16) and np.isclose(arr[7, 0, 16], 1.0 + 15 / 16)
+    tens = lambda p: np.stack((np.stack((1.0 + p[:, 0], 0.1 * p[:, 1]), -1),
+                               np.stack((0.1 * p[:, 1], 2.0 + p[:, 1]), -1)), -2)
+    mode, arr, _ = permeability_input(tens, mesh, 4, 4, 4)
+    assert mode == 6 and arr.shape == (8, 8, 17, 3)
+    with pytest.raises(ValueError, match="positive definite"):
+        permeability_input(lambda p: p[:, 0] - 0.5, mesh, 4, 4, 4)
     mode, arr, _ = source_input(lambda p: p[:, 0] + 10 * p[:, 1], mesh, 4, 4, 4)
     assert mode == 2 and arr.shape == (8, 8, 16)
     from numpy.polynomial.legendre import leggauss
