@@ -22,13 +22,14 @@ from pinned host memory and fields, fluxes, skeleton unknowns and status
 copied back for every request.
 
 ``--impl reference`` times the CPU restatement of the reference path (the
-oracle) on the host cores instead: each step runs the local stage on a
-bounded sample of macrocells in a spawn process pool and scales to the full
-4096-cell solve.
+oracle) on the host cores instead: each step is one whole solve of the same
+workload (the 4096 local problems on a spawn process pool of one BLAS thread
+per process, then skeleton assembly, the global SuperLU solve and the
+reconstruction of fields and fluxes).
 
 Multi-GPU: replicas only (one independent solve per rank, no collective in
 the data path); torch.distributed is used for barriers and the max-over-ranks
-timing.
+timing.  ``--gpus N`` without a torchrun environment starts the N ranks itself.
 """
 
 from __future__ import annotations
@@ -51,11 +52,10 @@ sys.path.insert(0, ROOT)
 MACRO, LOCAL, FACE_DEGREE = 64, 16, 2
 SIGMA, ELL, SEED = 2.0, 0.05, 20261203
 METRIC = "MHM solves/s (64x64 Q1 Darcy, lognormal kappa), mixed vs FP64 GPU"
-CPU_SAMPLE_CELLS = 4096
-# DRAM bytes (read + write) per launch of this workload's kernels, from the ncu
-# captures summarised in profiles/skeleton_pcg_darcy64_r16_p2.md and
-# profiles/q1_condense_darcy64_r16_p2_mixed.md.
-NCU_DRAM_BYTES = {"skeleton_pcg": 15.3e6, "q1_condense": 92.3e6}
+CPU_RUNS, SERIAL_SAMPLE_CELLS = 3, 48
+# DRAM bytes per launch of this workload's kernels from one ncu capture each, with the
+# command that produced them
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dram_traffic.json")
 
 
 def triangle_submesh(r):
@@ -326,7 +326,73 @@ def parse():
     ap.add_argument("--cut-case", type=int, default=0, metavar="P",
                     help="only the 64x64 x 16x16 solve with a P x P pixel field cutting the fine cells, "
                          "mixed and FP64, two timed solves each (for ncu)")
+    ap.add_argument("--launch-check", action="store_true",
+                    help="start the ranks, time an empty step with the barrier and max-over-ranks reduction, "
+                         "print the line's rank fields and exit (no GPU work; gloo without a GPU)")
     return ap.parse_args()
+
+
+def launch_ranks(args):
+    """Start ``--gpus`` ranks when this process is not one already (no WORLD_SIZE in the
+    environment): re-run this script under torch.distributed.run on 127.0.0.1 and
+    exit with its status.  A rank whose WORLD_SIZE differs from ``--gpus`` stops with
+    an error.  Returns True when this process only launched the ranks."""
+    if args.gpus < 1:
+        raise SystemExit("--gpus must be at least 1")
+    world = os.environ.get("WORLD_SIZE")
+    if world is not None:
+        if int(world) != args.gpus:
+            raise SystemExit(f"WORLD_SIZE={world} but --gpus {args.gpus}: launch one rank per GPU")
+        return False
+    if args.gpus == 1:
+        return False
+    import socket
+
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        port = sock.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *sys.argv[1:]]
+    rc = subprocess.call(cmd)
+    if rc:
+        raise SystemExit(rc)
+    return True
+
+
+def init_dist(world, backend):
+    """Process group of the replicas (None for one rank), with a short timeout so that
+    ranks waiting on a rank that died end with an error."""
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as td
+
+    td.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return td
+
+
+def launch_check(args):
+    """The rank plumbing of a run without GPU work: barrier, a timed empty step per rank
+    (one rank sleeps longer), max over ranks, rank 0 prints the rank fields."""
+    import torch
+
+    rank, world, _ = dist_env()
+    gpu = torch.cuda.is_available()
+    dist = init_dist(world, "nccl" if gpu else "gloo")
+    device = torch.device("cuda", rank) if gpu else torch.device("cpu")
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    time.sleep(0.01 * (1 + rank))
+    mine = (time.perf_counter() - t0) * 1e3
+    slowest = max_over_ranks(mine, dist, device)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({"launch_check": True, "n_gpus": world, "ms_per_step": slowest,
+                          "parallelism": f"replicas x{world}", "rank0_ms": mine}), flush=True)
 
 
 def lu_case(n, batch=64):
@@ -460,64 +526,70 @@ def workload_kappa():
     return lognormal_permeability(MACRO * LOCAL, MACRO * LOCAL, sigma=SIGMA, ell=ELL, seed=SEED)
 
 
-def cpu_rate(kappa, cells, workers):
-    from oracle.q1_mhm import local_stage_rate
+def cpu_baseline_entry(kappa, runs=CPU_RUNS, serial_cells=SERIAL_SAMPLE_CELLS):
+    """The oracle's whole solve of the workload on the host cores, median of ``runs``;
+    beside it the local stage in one process with one BLAS thread on a sample of
+    cells.  Returns the baseline entry and the median run's solution (the checker of
+    the GPU fields)."""
+    from oracle.q1_mhm import CartesianSolve, serial_local_rate
 
-    rng = np.random.default_rng(0)
-    sample = np.sort(rng.choice(MACRO * MACRO, size=cells, replace=False))
-    rate, seconds = local_stage_rate(MACRO, LOCAL, FACE_DEGREE, kappa, 1.0, sample, workers)
-    return rate, seconds
-
-
-def cpu_baseline_entry(kappa, cells=CPU_SAMPLE_CELLS):
     workers = os.cpu_count() or 1
-    rate, seconds = cpu_rate(kappa, cells, workers)
-    return {
-        "value": rate / (MACRO * MACRO), "unit": "solves/s", "cores": workers, "kind": "port",
-        "sample": (f"oracle local stage (Q1 assembly + equilibrated SuperLU condensation + Schur block) on "
-                   f"{cells} of {MACRO * MACRO} macrocells in {workers} spawn processes, {seconds:.1f} s wall; "
-                   f"scaled to 4096 cells; global SuperLU solve (about 1% of the reference's time at this size) "
-                   f"not included"),
+    with CartesianSolve(MACRO, LOCAL, FACE_DEGREE, kappa, 1.0, workers=workers) as solver:
+        results = [solver.solve() for _ in range(runs)]
+    totals = [r["phases"]["total_s"] for r in results]
+    sol = results[int(np.argsort(totals)[len(totals) // 2])]
+    sample = np.sort(np.random.default_rng(0).choice(MACRO * MACRO, serial_cells, replace=False))
+    rate, seconds = serial_local_rate(MACRO, LOCAL, FACE_DEGREE, kappa, 1.0, sample)
+    ph = sol["phases"]
+    serial_s = MACRO * MACRO / rate + ph["assembly_s"] + ph["global_solve_s"] + ph["reconstruction_s"]
+    entry = {
+        "value": 1.0 / ph["total_s"], "unit": "solves/s", "cores": workers, "kind": "port",
+        "sample": (f"whole solve of the same workload (4096 local problems on {workers} spawn processes of one "
+                   f"BLAS thread, skeleton assembly, global SuperLU solve, reconstruction of fields and fluxes), "
+                   f"median of {runs} runs"),
+        "runs_s": totals, "phases_s": ph,
+        "serial_one_blas_thread": {
+            "local_cells_per_s": rate, "sample_cells": serial_cells, "sample_s": seconds,
+            "estimated_solve_s": serial_s,
+            "note": "local stage of the sampled cells in one process, scaled to 4096 cells, plus the measured "
+                    "assembly, global solve and reconstruction phases"},
     }
+    return entry, sol
 
 
 def run_reference(args):
+    """Reference arm: the oracle's whole solve per step on all host cores (rank 0)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
+    from oracle.q1_mhm import CartesianSolve
+
     kappa = workload_kappa()
     workers = os.cpu_count() or 1
-    import multiprocessing as mp
-
-    from oracle.q1_mhm import _sample_cells, _sample_init
-
-    pool = mp.get_context("spawn").Pool(workers, initializer=_sample_init,
-                                        initargs=(MACRO, LOCAL, FACE_DEGREE, kappa, 1.0))
-    from oracle.q1_mhm import local_stage_rate
-
-    rng = np.random.default_rng(1)
-    cells_per_step = max(workers * 8, 64)
-    pool.map(_sample_cells, [[c] for c in range(workers)])
-    for _ in range(args.warmup):
-        local_stage_rate(MACRO, LOCAL, FACE_DEGREE, kappa, 1.0, rng.choice(MACRO * MACRO, cells_per_step, False),
-                         workers, pool)
-    times = []
-    for _ in range(args.steps):
-        rate, _ = local_stage_rate(MACRO, LOCAL, FACE_DEGREE, kappa, 1.0,
-                                   rng.choice(MACRO * MACRO, cells_per_step, False), workers, pool)
-        times.append(MACRO * MACRO / rate)
-    pool.close()
-    pool.join()
-    ms = 1000.0 * float(np.mean(times))
+    with CartesianSolve(MACRO, LOCAL, FACE_DEGREE, kappa, 1.0, workers=workers) as solver:
+        for _ in range(args.warmup):
+            solver.solve()
+        phases = []
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            sol = solver.solve()
+            phases.append(sol["phases"])
+        elapsed = time.perf_counter() - t0
+    ms = 1000.0 * elapsed / args.steps
     value = 1000.0 / ms
+    split = {k: float(np.median([p[k] for p in phases])) for k in phases[0]}
+    config = workload_config(args)
+    config["skeleton_unknowns"] = len(sol["rhs"])
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lognormal kappa)",
-        "config": workload_config(args), "impl": "reference",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lognormal kappa, f=1)",
+        "config": config, "impl": "reference",
+        "phases_median_s": split, "residual": float(sol["residual"]),
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers, "kind": "port",
-                         "sample": f"oracle local stage on {cells_per_step} random macrocells per step, "
-                                   f"{workers} spawn processes, scaled to 4096 cells (global solve excluded)"},
+                         "sample": f"whole solve per step: 4096 local problems on {workers} spawn processes of one "
+                                   f"BLAS thread (the pool started once, before timing), skeleton assembly, global "
+                                   f"SuperLU solve, reconstruction of fields and fluxes"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -527,7 +599,7 @@ def workload_config(args):
     return {"workload": f"darcy-q1-{MACRO}x{MACRO}-r{LOCAL}-p{FACE_DEGREE}-lognormal-s{SIGMA:g}-l{ELL:g}",
             "macrocells": MACRO * MACRO, "local_dofs": (LOCAL + 1) ** 2, "rhs_per_cell": 4 * (FACE_DEGREE + 1) + 1,
             "skeleton_unknowns": None, "fine_cells": (MACRO * LOCAL) ** 2, "seed": SEED,
-            "parallelism": f"replicas x{args.gpus}",
+            "parallelism": f"replicas x{int(os.environ.get('WORLD_SIZE', args.gpus))}",
             "serving": "value/e2e: two independent solves in flight per GPU (two plans; local stage on "
                        "low-priority streams, global solve + reconstruction on high-priority streams); "
                        "'sequential': one solve at a time",
@@ -548,23 +620,21 @@ def main():
 
         print(json.dumps({"cut_case": cut_material_campaign(torch, steps=2, pixels=args.cut_case)}))
         return
+    if launch_ranks(args):
+        return
     rank, world, local = dist_env()
+    if args.launch_check:
+        launch_check(args)
+        return
     kappa = workload_kappa()
     # CPU baseline first (spawned pool before any CUDA context exists)
-    cpu = None
-    if rank == 0 and world >= 1 and args.gpus == 1 and not args.no_cpu_baseline and not args.profile:
-        cpu = cpu_baseline_entry(kappa)
+    cpu, ref_sol = None, None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.profile:
+        cpu, ref_sol = cpu_baseline_entry(kappa)
     import torch
 
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as td
-
-        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        dist = td
+    dist = init_dist(world, "nccl")
     from pymhm_b200.darcy import CartesianQ1Plan
     from pymhm_b200.topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
 
@@ -835,20 +905,30 @@ def main():
     host_fields, host_flux, host_x = hosts[(args.steps - 1) % 2]["fields"], hosts[(args.steps - 1) % 2]["flux"], \
         hosts[(args.steps - 1) % 2]["x"]
 
-    # accuracy against the reference's FP64 solution (golden fixture of the same workload)
+    # accuracy: lambda and c against the reference's FP64 solution (golden fixture of the
+    # same workload); u and the flux, relative L2 over all cells, against the CPU
+    # baseline's oracle solve (which reproduces the reference's matrix and unknowns)
     acc = {}
     gpath = os.path.join(ROOT, "tests", "golden", "darcy_64x64_r16_p2_lognormal.npz")
     if os.path.exists(gpath):
         g = np.load(gpath)
-        x = host_x.numpy()
         T = plan.T
         rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
-        acc = {"lambda": rel(x[:T], g["trace"]), "coarse": rel(x[T:], g["coarse"]),
-               "u_norm": abs(float(np.linalg.norm(host_fields.numpy())) / float(g["fields_norm"]) - 1),
-               "flux_norm": abs(float(np.linalg.norm(host_flux.numpy())) / float(g["flux_norm"]) - 1)}
-        keep = list(g["keep_cells"])
-        acc["u_cells"] = rel(host_fields.numpy()[keep], g["fields_cells"])
-        acc["flux_cells"] = rel(host_flux.numpy()[keep], g["flux_cells"])
+        fp64_plan = plans["fp64"][0]
+        fp64_plan.launch(stream)
+        torch.cuda.synchronize()
+        fp64_out = (fp64_plan.x.cpu().numpy(), fp64_plan.fields.cpu().numpy(), fp64_plan.flux.cpu().numpy())
+        for name, (x, fields, flux) in (("mixed", (host_x.numpy(), host_fields.numpy(), host_flux.numpy())),
+                                        ("fp64", fp64_out)):
+            e = {"lambda": rel(x[:T], g["trace"]), "coarse": rel(x[T:], g["coarse"])}
+            if ref_sol is not None:
+                e["u"] = rel(fields, ref_sol["fields"])
+                e["flux"] = rel(flux, ref_sol["flux"])
+            acc[name] = e
+        acc["note"] = ("relative L2 errors; lambda, coarse: against the reference's solution (fixture); u, flux: "
+                       "all 4096 cells against the oracle's solve in the CPU baseline" if ref_sol is not None else
+                       "relative L2 errors against the reference's solution (fixture); u and flux need the CPU "
+                       "baseline's solve, which this run skipped")
 
     def agg(v):
         return max_over_ranks(v, dist, dev)
@@ -919,8 +999,26 @@ def max_over_ranks(value, dist, device):
     return float(t.item())
 
 
+def profile_traffic(kernel):
+    """DRAM bytes per launch (read + write) of ``kernel`` from the committed ncu summary,
+    with the command that measured them; None when that kernel was not captured."""
+    if not os.path.exists(TRAFFIC_FILE):
+        return None, None
+    with open(TRAFFIC_FILE) as f:
+        entry = json.load(f).get(kernel)
+    if not entry:
+        return None, None
+    return float(entry["dram_bytes_read"]) + float(entry["dram_bytes_write"]), entry
+
+
 def roofline(plan, kernel, ms, inner_iters, outer):
-    """Algorithmic bytes of the dominant kernel per launch over its measured time."""
+    """Algorithmic bytes of the dominant kernel per launch over its measured time.
+
+    Global CG: per inner iteration one sweep of the CSR matrix (12 bytes per stored
+    entry: value and column index) and six vectors of N doubles, nnz*12 + 6*N*8, times
+    the measured inner iterations.  The kernel's own model of what it moves (cell
+    blocks and tables once, per iteration the exchanged face partials and coarse row
+    data, one CSR sweep per outer correction) is reported beside it."""
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peak, source = 6650.0, "fallback"
     if os.path.exists(peaks_path):
@@ -928,27 +1026,36 @@ def roofline(plan, kernel, ms, inner_iters, outer):
             peak, source = float(json.load(f)["hbm_gbs"]), "measured"
     p = plan.pattern
     nnz = len(p.indices)
-    M, n, w, T = plan.cells, plan.n, plan.w, plan.T
+    M, n, w, T, N = plan.cells, plan.n, plan.w, plan.T, plan.N
+    model = None
     if kernel == "skeleton_pcg":
-        # Cell-form projected CG: setup reads the cell blocks and tables once; per inner
-        # iteration each of the two half-steps writes the cells' face partials (M t) and
-        # reads them back on every CTA's local DOFs (~2 T), and each of its two coarse
-        # solves writes and reads the three-part row data (3 M) and the solved rows
-        # (M, read back three rows per CTA); every outer correction sweeps the CSR K.
         t = plan.t
+        per_iter = nnz * 12 + 6 * N * 8
+        bytes_ = inner_iters * per_iter
         setup = M * (t + 1) * (t + 1) * 8 + M * t * (8 + 8 + 4) + T * 16
-        per_iter = 2 * (M * t * 8 + 2 * T * 8) + 2 * (2 * 3 * M * 8 + M * 8 + 3 * M * 8)
-        bytes_ = setup + inner_iters * per_iter + (outer + 2) * (nnz * 12 + 2 * plan.N * 8)
+        kernel_iter = 2 * (M * t * 8 + 2 * T * 8) + 2 * (2 * 3 * M * 8 + M * 8 + 3 * M * 8)
+        model = setup + inner_iters * kernel_iter + (outer + 2) * (nnz * 12 + 2 * N * 8)
+        basis = f"{inner_iters} inner iterations x (nnz*12 + 6*N*8) = {inner_iters} x {per_iter} bytes"
     elif kernel == "q1_condense":
         bytes_ = plan.nxf * plan.nyf * 8 + M * w * (n + 1) * 8 + M * (plan.t + 1) * (plan.t + 2) * 8
+        basis = "kappa read + responses and Schur blocks / loads written"
     elif kernel == "q1_reconstruct":
         bytes_ = M * w * (n + 1) * 8 + plan.nxf * plan.nyf * 8 + M * n * 8 + M * plan.nfine * 16
+        basis = "responses and kappa read + fields and fluxes written"
     else:
-        bytes_ = nnz * 24 + plan.N * 24
+        bytes_ = nnz * 24 + N * 24
+        basis = "contributor maps and blocks read + values written"
     achieved = bytes_ / (ms * 1e-3) / 1e9
-    return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": NCU_DRAM_BYTES.get(kernel), "algorithmic_bytes": int(bytes_),
-            "peak_source": source + " (MEASURED_PEAKS.json hbm_gbs)" if source == "measured" else source}
+    traffic, prof = profile_traffic(kernel)
+    out = {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": int(bytes_), "basis": basis,
+           "ms_per_launch": float(ms),
+           "peak_source": source + " (MEASURED_PEAKS.json hbm_gbs)" if source == "measured" else source}
+    if model is not None:
+        out["kernel_model_bytes"] = int(model)
+    if prof is not None:
+        out["traffic_source"] = {k: prof[k] for k in ("command", "case") if k in prof}
+    return out
 
 
 if __name__ == "__main__":

@@ -266,6 +266,19 @@ int mhm_skeleton_scatter(int64_t nnz, const int64_t* slot_ptr, const int64_t* co
                          const int64_t* load_ptr, const int64_t* load_contrib, const double* loads,
                          const double* boundary, double* rhs, double* load_scale, void* stream);
 
+/*
+ * The assembled matrix as the reference hands it on: CSC, entries whose sum is
+ * exactly zero (either sign) dropped.  Replaces `coo_matrix(...).tocsc()` and
+ * `matrix.eliminate_zeros()` (core/contributions.py:184-185).  Input: the
+ * structural CSR (indptr size+1, indices sorted per row) with the values of
+ * mhm_skeleton_scatter, and transpose[k] = the CSR slot of (i, j) for the CSR
+ * slot k of (j, i) (the pattern is symmetric).  Output: csc_indptr (size+1),
+ * csc_indices / csc_data (at least nnz entries; csc_indptr[size] are used).
+ */
+int mhm_skeleton_export_csc(int64_t size, const int64_t* indptr, const int32_t* indices,
+                            const int64_t* transpose, const double* vals, int64_t* csc_indptr,
+                            int32_t* csc_indices, double* csc_data, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Global skeleton solve: projected PCG with an outer FP64 defect correction  */
 /* ------------------------------------------------------------------------ */

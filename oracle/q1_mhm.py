@@ -870,47 +870,141 @@ def refine_q1(mesh, skeleton, refinement, trace, coarse, fields, permeability=1.
 
 
 # --------------------------------------------------------------------------------------
-# Timed CPU baseline: the local stage of the oracle over a sample of macrocells
+# The whole Cartesian solve with the local stage on a process pool (checker at full size
+# and the timed CPU baseline)
 # --------------------------------------------------------------------------------------
-_SAMPLE_STATE = {}
+_POOL_STATE = {}
 
 
-def _sample_init(macro, local, face_degree, kappa, source):
+def _pool_init(macro, local, face_degree, kappa, source, blas_threads):
+    """Worker set-up: one BLAS thread (the reference's process-backend policy,
+    ``execution/cpu.py:97-101``) and the mesh, skeleton and coefficients."""
+    from threadpoolctl import threadpool_limits
+
+    _POOL_STATE["limits"] = threadpool_limits(blas_threads)
     mesh = cartesian_mesh(macro)
     sk = Skeleton(mesh, (FaceSpace.uniform(face_degree),) * len(mesh.faces))
     nf = macro * local
     perm = PixelField(kappa, (1.0 / nf, 1.0 / nf)) if kappa is not None else 1.0
-    _SAMPLE_STATE.update(mesh=mesh, sk=sk, local=local, perm=perm, source=source)
+    _POOL_STATE.update(mesh=mesh, sk=sk, local=local, perm=perm, source=source)
 
 
-def _sample_cells(cells):
-    st = _SAMPLE_STATE
+def _pool_cells(cells):
+    """Assembly, condensation and contribution of the given macrocells (the per-cell
+    loop of ``solve_darcy_q1``); returns what the parent assembles and reconstructs."""
+    st = _POOL_STATE
+    out = []
     for cell in cells:
         _, problem = local_problem(st["mesh"], st["sk"], int(cell), (st["local"], st["local"]), st["perm"],
                                    st["source"])
-        contribution(condense(problem), st["sk"].size + int(cell))
-    return len(cells)
+        resp = condense(problem)
+        idx, block, load = contribution(resp, st["sk"].size + int(cell))
+        out.append((idx, block, load, resp.source, resp.lifts, resp.retained[:, 0]))
+    return out
 
 
-def local_stage_rate(macro, local, face_degree, kappa, source, cells, workers, pool=None):
-    """Macrocells per second of the oracle's assembly + condensation + contribution.
+def cartesian_flux(mesh, refinement, fields, permeability):
+    """``cell_flux`` of every macrocell at once: the same gradient formula and
+    fine-cell centres (``postprocessing/solutions.py:278-324``) over all cells."""
+    r = refinement
+    lower = mesh.points[mesh.cells[:, 0]]
+    upper = mesh.points[mesh.cells[:, 2]]
+    xs = np.linspace(lower[:, 0], upper[:, 0], r + 1)  # (r+1, cells), as each submesh's linspace
+    ys = np.linspace(lower[:, 1], upper[:, 1], r + 1)
+    hx = (upper[:, 0] - lower[:, 0]) / r
+    hy = (upper[:, 1] - lower[:, 1]) / r
+    ix, iy = np.tile(np.arange(r), r), np.repeat(np.arange(r), r)  # fine cells x-fastest
+    origin = iy * (r + 1) + ix
+    u = np.asarray(fields)
+    c0, c1, c2, c3 = (u[:, origin + k] for k in (0, 1, r + 1, r + 2))
+    gx = (-c0 + c1 - c2 + c3) * 0.5 / hx[:, None]
+    gy = (-c0 - c1 + c2 + c3) * 0.5 / hy[:, None]
+    cx = xs[ix].T + 0.5 * hx[:, None]
+    cy = ys[iy].T + 0.5 * hy[:, None]
+    k = tensor_at(permeability, np.column_stack((cx.ravel(), cy.ravel())))
+    grad = np.column_stack((gx.ravel(), gy.ravel()))
+    return -np.einsum("qab,qb->qa", k, grad).reshape(len(u), r * r, 2)
 
-    ``cells`` is the sampled list of macrocell ids, split over ``workers``
-    spawn processes (each owns its own copy of the mesh and coefficients).
+
+class CartesianSolve:
+    """``solve_darcy_q1`` of a uniform Cartesian workload (``macro`` x ``macro`` cells,
+    ``local`` x ``local`` Q1, uniform Legendre faces of ``face_degree``, pixel
+    permeability ``kappa`` on the fine cells or 1, constant or callable ``source``,
+    homogeneous Dirichlet data) with the per-cell local stage on ``workers`` spawn
+    processes of one BLAS thread each.  Assembly, the global SuperLU solve and the
+    reconstruction run in the calling process.  ``solve()`` times each phase.
+
+    Start it before any CUDA context exists in the calling process, or keep the
+    default spawn context: a pool forked from a CUDA process can hang.
     """
-    import multiprocessing as mp
+
+    def __init__(self, macro, local, face_degree, kappa=None, source=1.0, workers=None, chunks_per_worker=4):
+        import multiprocessing as mp
+        import os
+
+        self.workers = int(workers or os.cpu_count() or 1)
+        self.macro, self.local = macro, local
+        self.mesh = cartesian_mesh(macro)
+        self.sk = Skeleton(self.mesh, (FaceSpace.uniform(face_degree),) * len(self.mesh.faces))
+        nf = macro * local
+        self.perm = PixelField(kappa, (1.0 / nf, 1.0 / nf)) if kappa is not None else 1.0
+        self.boundary, _ = boundary_data(self.sk, 0.0, None, 4)
+        cells = len(self.mesh.cells)
+        self.dofs = np.array([self.sk.cell_dofs(c) for c in range(cells)])
+        self.chunks = [c for c in np.array_split(np.arange(cells), self.workers * chunks_per_worker) if len(c)]
+        self.pool = mp.get_context("spawn").Pool(self.workers, initializer=_pool_init,
+                                                 initargs=(macro, local, face_degree, kappa, source, 1))
+        self.pool.map(_pool_cells, [[0]] * self.workers)  # imports and caches, untimed
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def solve(self):
+        import time
+
+        t0 = time.perf_counter()
+        parts = self.pool.map(_pool_cells, self.chunks)
+        t1 = time.perf_counter()
+        res = [r for p in parts for r in p]
+        matrix, rhs, scale = assemble_global([r[:3] for r in res], self.sk.size, self.boundary)
+        t2 = time.perf_counter()
+        x, residual = solve_global(matrix, rhs, scale)
+        t3 = time.perf_counter()
+        T = self.sk.size
+        trace, coarse = x[:T], x[T:]
+        fields = np.array([src - lifts @ trace[self.dofs[c]] + ret * coarse[c]
+                           for c, (_, _, _, src, lifts, ret) in enumerate(res)])
+        flux = cartesian_flux(self.mesh, self.local, fields, self.perm)
+        t4 = time.perf_counter()
+        phases = {"local_stage_s": t1 - t0, "assembly_s": t2 - t1, "global_solve_s": t3 - t2,
+                  "reconstruction_s": t4 - t3, "total_s": t4 - t0}
+        return dict(trace=trace, coarse=coarse, fields=fields, flux=flux, matrix=matrix, rhs=rhs,
+                    residual=residual, phases=phases)
+
+
+def serial_local_rate(macro, local, face_degree, kappa, source, cells):
+    """Macrocells per second of the local stage in this process with one BLAS thread
+    (the reference's ``backend="serial"`` policy), over the given cell ids."""
     import time
 
-    chunks = [c for c in np.array_split(np.asarray(cells), workers) if len(c)]
-    own = pool is None
-    if own:
-        pool = mp.get_context("spawn").Pool(workers, initializer=_sample_init,
-                                            initargs=(macro, local, face_degree, kappa, source))
-        pool.map(_sample_cells, [c[:1] for c in chunks])  # warm imports and caches
-    t0 = time.perf_counter()
-    done = sum(pool.map(_sample_cells, chunks))
-    dt = time.perf_counter() - t0
-    if own:
-        pool.close()
-        pool.join()
-    return done / dt, dt
+    from threadpoolctl import threadpool_limits
+
+    mesh = cartesian_mesh(macro)
+    sk = Skeleton(mesh, (FaceSpace.uniform(face_degree),) * len(mesh.faces))
+    nf = macro * local
+    perm = PixelField(kappa, (1.0 / nf, 1.0 / nf)) if kappa is not None else 1.0
+    with threadpool_limits(1):
+        local_problem(mesh, sk, int(cells[0]), (local, local), perm, source)  # warm caches
+        t0 = time.perf_counter()
+        for cell in cells:
+            _, problem = local_problem(mesh, sk, int(cell), (local, local), perm, source)
+            contribution(condense(problem), sk.size + int(cell))
+        dt = time.perf_counter() - t0
+    return len(cells) / dt, dt

@@ -93,6 +93,7 @@ _SIGNATURES = {
     "mhm_skeleton_fixed_rhs": (C.c_int, [C.c_int64, C.c_int64, P, P, P, P, P, P, P, P]),
     "mhm_q1_flux": (C.c_int, [C.POINTER(Q1Problem), P, P, P]),
     "mhm_skeleton_scatter": (C.c_int, [C.c_int64, P, P, P, P, C.c_int64, C.c_int64, P, P, P, P, P, P, P]),
+    "mhm_skeleton_export_csc": (C.c_int, [C.c_int64, P, P, P, P, P, P, P, P]),
     "mhm_skeleton_workspace_bytes": (C.c_int64, [C.POINTER(SkeletonSystem), C.c_int32]),
     "mhm_skeleton_solve": (C.c_int, [C.POINTER(SkeletonSystem), P, P, P, C.c_double, C.c_double, C.c_int32,
                                      C.c_int32, C.c_int32, P, C.c_int64, P, P, P]),

@@ -1175,6 +1175,64 @@ __global__ void scatter_kernel(int64_t nnz, const int64_t* slot_ptr, const int64
   }
 }
 
+// CSC export with exact zeros dropped.  The structural pattern is symmetric, so column
+// j of the CSC matrix lists the same indices as CSR row j; its entry in row i is the
+// CSR value of slot (i, j) = vals[transpose[k]] for the CSR slot k of (j, i).
+__global__ void csc_count_kernel(int64_t size, const int64_t* indptr, const int64_t* transpose,
+                                 const double* vals, int64_t* csc_indptr) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < size; j += stride) {
+    int64_t c = 0;
+    for (int64_t k = indptr[j]; k < indptr[j + 1]; ++k) c += vals[transpose[k]] != 0.0;
+    csc_indptr[j + 1] = c;
+    if (j == 0) csc_indptr[0] = 0;
+  }
+}
+
+// In-place inclusive scan of ptr[1..size] in one block: each thread sums a contiguous
+// chunk, the chunk totals are scanned in shared memory, and each thread rewrites its
+// chunk from its prefix.  Sums of int64 counts: order-free and exact.
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) csc_scan_kernel(int64_t size, int64_t* ptr) {
+  __shared__ int64_t part[kScanThreads];
+  const int tid = threadIdx.x;
+  const int64_t chunk = (size + kScanThreads - 1) / kScanThreads;
+  const int64_t lo = 1 + tid * chunk;
+  const int64_t hi = lo + chunk < size + 1 ? lo + chunk : size + 1;
+  int64_t s = 0;
+  for (int64_t i = lo; i < hi; ++i) s += ptr[i];
+  part[tid] = s;
+  __syncthreads();
+  for (int off = 1; off < kScanThreads; off <<= 1) {
+    const int64_t v = tid >= off ? part[tid - off] : 0;
+    __syncthreads();
+    part[tid] += v;
+    __syncthreads();
+  }
+  int64_t run = tid ? part[tid - 1] : 0;
+  for (int64_t i = lo; i < hi; ++i) {
+    run += ptr[i];
+    ptr[i] = run;
+  }
+}
+
+__global__ void csc_write_kernel(int64_t size, const int64_t* indptr, const int32_t* indices,
+                                 const int64_t* transpose, const double* vals,
+                                 const int64_t* csc_indptr, int32_t* csc_indices, double* csc_data) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < size; j += stride) {
+    int64_t out = csc_indptr[j];
+    for (int64_t k = indptr[j]; k < indptr[j + 1]; ++k) {
+      const double v = vals[transpose[k]];
+      if (v != 0.0) {
+        csc_indices[out] = indices[k];
+        csc_data[out] = v;
+        ++out;
+      }
+    }
+  }
+}
+
 struct Layout {
   size_t Zf, Zs, Vf, Vs, U[12], rfull, part, bar, err, total;
 };
@@ -1286,6 +1344,23 @@ extern "C" int mhm_skeleton_scatter(int64_t nnz, const int64_t* slot_ptr, const 
   scatter_kernel<<<blocks_n, 256, 0, static_cast<cudaStream_t>(stream)>>>(
       nnz, slot_ptr, contrib, blocks, vals, size, trace_size, load_ptr, load_contrib, loads,
       boundary, rhs, load_scale);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+extern "C" int mhm_skeleton_export_csc(int64_t size, const int64_t* indptr, const int32_t* indices,
+                                       const int64_t* transpose, const double* vals,
+                                       int64_t* csc_indptr, int32_t* csc_indices, double* csc_data,
+                                       void* stream) {
+  if (size < 1 || !indptr || !indices || !transpose || !vals || !csc_indptr || !csc_indices ||
+      !csc_data)
+    return MHM_ERR_ARGUMENT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int blocks_n = (int)((size + 255) / 256);
+  if (blocks_n > 4096) blocks_n = 4096;
+  csc_count_kernel<<<blocks_n, 256, 0, st>>>(size, indptr, transpose, vals, csc_indptr);
+  csc_scan_kernel<<<1, kScanThreads, 0, st>>>(size, csc_indptr);
+  csc_write_kernel<<<blocks_n, 256, 0, st>>>(size, indptr, indices, transpose, vals, csc_indptr,
+                                              csc_indices, csc_data);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
 

@@ -46,6 +46,7 @@ from .topology import (
     neumann_layout,
     side_orientation,
     skeleton_pattern,
+    transpose_slots,
 )
 
 PRECISIONS = {"fp64": _lib.PRECISION_FP64, "mixed": _lib.PRECISION_MIXED}
@@ -868,12 +869,37 @@ class CartesianQ1Plan:
         sol.seconds = time.perf_counter() - t0
         return sol
 
+    def export_csc(self, stream=None):
+        """The assembled skeleton matrix as the reference hands it on, on the device:
+        CSC with the entries whose sum is exactly zero dropped (``coo_matrix(...).tocsc()``
+        then ``eliminate_zeros()``, ``core/contributions.py:184-185``).  Returns
+        ``(indptr int64 (N+1), indices int32, data float64)`` device tensors trimmed to
+        the kept entries; the solver keeps using the structural pattern."""
+        torch = self.torch
+        if getattr(self, "_csc", None) is None:
+            p = self.pattern
+            nnz = len(p.indices)
+            self._csc = dict(
+                transpose=torch.as_tensor(transpose_slots(p.indptr, p.indices)).to(self.device),
+                indptr=torch.empty(self.N + 1, dtype=torch.int64, device=self.device),
+                indices=torch.empty(nnz, dtype=torch.int32, device=self.device),
+                data=torch.empty(nnz, dtype=torch.float64, device=self.device))
+        c = self._csc
+        P = _lib.ptr
+        _lib.check(self.lib.mhm_skeleton_export_csc(self.N, P(self.d_indptr), P(self.d_indices), P(c["transpose"]),
+                                                    P(self.values), P(c["indptr"]), P(c["indices"]), P(c["data"]),
+                                                    _lib.stream_handle(stream)), "mhm_skeleton_export_csc")
+        kept = int(c["indptr"][-1])
+        return c["indptr"], c["indices"][:kept], c["data"][:kept]
+
     def matrix(self):
-        """Host CSR copy of the assembled skeleton matrix (structural pattern)."""
+        """Host copy of the assembled skeleton matrix in the reference's form
+        (``export_csc``): a SciPy CSC matrix whose ``indptr`` / ``indices`` follow the
+        reference's rule for which entries are stored."""
         from scipy import sparse
 
-        p = self.pattern
-        return sparse.csr_matrix((self.values.cpu().numpy(), p.indices.astype(np.int64), p.indptr),
+        indptr, indices, data = self.export_csc()
+        return sparse.csc_matrix((data.cpu().numpy(), indices.cpu().numpy(), indptr.cpu().numpy()),
                                  shape=(self.N, self.N))
 
 

@@ -573,6 +573,17 @@ def skeleton_pattern(cell_dofs: np.ndarray, trace_size: int) -> SkeletonPattern:
                            lflat[lorder], trace_end)
 
 
+def transpose_slots(indptr: np.ndarray, indices: np.ndarray) -> np.ndarray:
+    """For a CSR pattern that is symmetric, ``out[k]`` = the slot of (i, j) for the slot
+    k of (j, i).  Sorting the slots by (column, row) lists them in the CSR order of the
+    transpose, which is the same pattern."""
+    rows = np.repeat(np.arange(len(indptr) - 1, dtype=np.int64), np.diff(indptr))
+    order = np.lexsort((rows, indices.astype(np.int64)))
+    if not (np.array_equal(indices[order], rows) and np.array_equal(rows[order], indices)):
+        raise ValueError("the pattern is not symmetric")
+    return order.astype(np.int64)
+
+
 def dof_cell_maps(cell_dofs: np.ndarray, trace_size: int) -> tuple[np.ndarray, np.ndarray]:
     """(T, 2) cells containing each trace DOF (cell order, -1 padded) and the DOF's slot."""
     cells, t = cell_dofs.shape

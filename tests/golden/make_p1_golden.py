@@ -18,7 +18,9 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-sys.path.insert(0, os.environ.get("PYMHM_SRC", "/root/reference/src"))
+if not os.environ.get("PYMHM_SRC"):
+    sys.exit("set PYMHM_SRC to the src/ directory of a PyMHM 1.3.2 checkout")
+sys.path.insert(0, os.environ["PYMHM_SRC"])
 sys.path.insert(0, str(HERE))
 
 import _basix_shim  # noqa: E402

@@ -116,3 +116,39 @@ def test_oracle_condensation_matches_monolithic_solve():
     n = len(g["cell0_source"])
     assert np.allclose(x[:n, 0], g["cell0_source"], atol=1e-13)
     assert np.allclose(x[:n, 1:1 + g["cell0_lifts"].shape[1]], g["cell0_lifts"], atol=1e-13)
+
+
+def test_full_size_oracle_is_the_reference():
+    """At 64x64 x 16x16 the oracle's parallel solve reproduces the reference: the
+    skeleton matrix's SHA-256 digests (indptr, indices, data after eliminate_zeros),
+    its trace and coarse unknowns exactly, and the norms and kept cells of the fields
+    and fluxes.  This pins the oracle as the checker of the full-size GPU solve."""
+    from pymhm_b200.workloads import digest
+    from tests._full_size import oracle_solution
+
+    g = load("darcy_64x64_r16_p2_lognormal")
+    sol = oracle_solution()
+    m = sol["matrix"]
+    assert digest(m.indptr) == str(g["indptr_sha256"])
+    assert digest(m.indices) == str(g["indices_sha256"])
+    assert digest(m.data) == str(g["data_sha256"])
+    assert np.array_equal(sol["trace"], g["trace"])
+    assert np.array_equal(sol["coarse"], g["coarse"])
+    assert np.array_equal(sol["rhs"], g["rhs"])
+    assert np.linalg.norm(sol["fields"]) == pytest.approx(float(g["fields_norm"]), rel=1e-15)
+    assert np.linalg.norm(sol["flux"]) == pytest.approx(float(g["flux_norm"]), rel=1e-15)
+    keep = list(g["keep_cells"])
+    assert rel(sol["fields"][keep], g["fields_cells"]) <= 1e-15
+    # the gradient's differences amplify the reconstruction's rounding
+    assert rel(sol["flux"][keep], g["flux_cells"]) <= 1e-13
+
+
+def test_vectorised_flux_equals_cell_flux():
+    """``cartesian_flux`` (all cells at once) is ``cell_flux`` cell by cell, bit for bit."""
+    mesh = o.cartesian_mesh(3, 2, (-1.0, 2.0, -2.0, 2.0))
+    rng = np.random.default_rng(3)
+    fields = rng.normal(size=(6, 5 * 5))
+    kappa = o.PixelField(np.exp(rng.normal(size=(12, 10))), (0.25, 0.4), (-1.0, -2.0))
+    flux = o.cartesian_flux(mesh, 4, fields, kappa)
+    for c in range(6):
+        assert np.array_equal(flux[c], o.cell_flux(mesh.submesh(c, 4), fields[c], kappa))
