@@ -915,6 +915,8 @@ def main():
         T = plan.T
         rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
         fp64_plan = plans["fp64"][0]
+        # the online campaign's replays left another source on this plan
+        fp64_plan.set_device_coefficients(1, kappa_dev[0], (0.0, 0.0, 0.0), 0, None, 1.0)
         fp64_plan.launch(stream)
         torch.cuda.synchronize()
         fp64_out = (fp64_plan.x.cpu().numpy(), fp64_plan.fields.cpu().numpy(), fp64_plan.flux.cpu().numpy())

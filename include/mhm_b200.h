@@ -394,6 +394,55 @@ int mhm_skeleton_solve_static(const mhm_skeleton_system* s /* host */, const dou
                               double* stats, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Global skeleton solve on any macro mesh (tetrahedra, polygons, ...)        */
+/* ------------------------------------------------------------------------ */
+/*
+ * Replaces solve_hybrid_system's global solve (core/system.py:355-528 ->
+ * linalg/linear.py:798, SuperLU at rtol 1e-10) for macro meshes without the
+ * Cartesian structure mhm_skeleton_solve relies on.  The caller describes the
+ * assembled system K = [[S, -G], [-G^T, -C]] (the structural CSR of
+ * mhm_skeleton_scatter) and the exact geometric constraint G0 = B^T 1 of every
+ * cell, together with the dense inverse of the coarse operator G0^T G0, which
+ * depends on the mesh only.  All pointers are device pointers; the struct itself
+ * is read on the host.
+ */
+typedef struct mhm_general_system {
+    int64_t size;                 /* N = trace_size + cells                         */
+    int64_t trace_size;           /* T                                              */
+    const int64_t* indptr;        /* CSR of K (N+1), columns sorted per row         */
+    const int32_t* indices;
+    const double* values;
+    int32_t faces;                /* skeleton faces                                  */
+    int32_t max_face_size;        /* largest DOF count of a face (1..8)             */
+    const int64_t* face_ptr;      /* (faces+1): face f owns DOFs face_ptr[f]..[f+1]-1 */
+    int32_t cells;
+    const int64_t* cell_ptr;      /* (cells+1) into cell_dofs / cell_g0            */
+    const int64_t* cell_dofs;     /* trace DOFs of every cell, in its local order   */
+    const double* cell_g0;        /* G0 entry of each (cell, local DOF)              */
+    const int32_t* dof_cells;     /* (T, 2): the cells holding each DOF (-1: none)  */
+    const int64_t* dof_entry;     /* (T, 2): its index in cell_dofs / cell_g0       */
+    const double* coarse_inverse; /* (cells, cells) row-major (G0^T G0)^-1           */
+} mhm_general_system;
+
+/* Workspace bytes of mhm_general_solve on the current device (-1: invalid). */
+int64_t mhm_general_workspace_bytes(const mhm_general_system* s /* host */);
+
+/*
+ * x (N) = K^-1 rhs (N): outer FP64 defect correction on K until
+ * ||rhs - K x|| <= rtol ||rhs||, each correction by projected CG on
+ * [[S, -G0], [-G0^T, 0]] with block-Jacobi preconditioning over the faces
+ * (inner tolerance inner_rtol, at most max_inner CG iterations in total and
+ * max_outer corrections).  One persistent cooperative launch (one CTA per SM).
+ * info (4 int32, device): status (MHM_SOLVE_*), inner iterations, outer
+ * corrections, barrier error flag; stats (2 doubles, device): final relative
+ * residual, ||rhs||.  Every grid barrier is bounded.
+ */
+int mhm_general_solve(const mhm_general_system* s /* host */, const double* rhs, double* x,
+                      void* workspace, int64_t workspace_bytes, double rtol, double inner_rtol,
+                      int32_t max_inner, int32_t max_outer, int32_t* info, double* stats,
+                      void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Reconstruction u_K = R f - (R B) lambda_K + E c_K and flux -K grad u       */
 /* ------------------------------------------------------------------------ */
 int mhm_q1_reconstruct(const mhm_q1_problem* p /* host */, const double* solution,

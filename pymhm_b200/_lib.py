@@ -74,6 +74,16 @@ class SkeletonSystem(C.Structure):
     ]
 
 
+class GeneralSystem(C.Structure):
+    _fields_ = [
+        ("size", C.c_int64), ("trace_size", C.c_int64),
+        ("indptr", C.c_void_p), ("indices", C.c_void_p), ("values", C.c_void_p),
+        ("faces", C.c_int32), ("max_face_size", C.c_int32), ("face_ptr", C.c_void_p),
+        ("cells", C.c_int32), ("cell_ptr", C.c_void_p), ("cell_dofs", C.c_void_p), ("cell_g0", C.c_void_p),
+        ("dof_cells", C.c_void_p), ("dof_entry", C.c_void_p), ("coarse_inverse", C.c_void_p),
+    ]
+
+
 P = C.c_void_p
 _SIGNATURES = {
     "mhm_q1_rhs_width": (C.c_int32, [C.POINTER(Q1Problem)]),
@@ -99,6 +109,9 @@ _SIGNATURES = {
                                      C.c_int32, C.c_int32, P, C.c_int64, P, P, P]),
     "mhm_skeleton_solve_static": (C.c_int, [C.POINTER(SkeletonSystem), P, P, P, C.c_double, C.c_double,
                                             C.c_int32, C.c_int32, C.c_int32, P, P, P]),
+    "mhm_general_workspace_bytes": (C.c_int64, [C.POINTER(GeneralSystem)]),
+    "mhm_general_solve": (C.c_int, [C.POINTER(GeneralSystem), P, P, P, C.c_int64, C.c_double, C.c_double,
+                                    C.c_int32, C.c_int32, P, P, P]),
     "mhm_q1_reconstruct": (C.c_int, [C.POINTER(Q1Problem), P, P, C.c_int64, P, P, P, P]),
     "mhm_batched_factor": (C.c_int, [C.c_int64, C.c_int32, P, P, P, P, P, P, P]),
     "mhm_batched_solve": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, P, P, P, P, P, P, P, C.c_double,

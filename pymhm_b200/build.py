@@ -14,7 +14,8 @@ from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
-SOURCES = ["q1_condense.cu", "skeleton.cu", "skeleton_static.cu", "batched_lu.cu", "p1_assembly.cu"]
+SOURCES = ["q1_condense.cu", "skeleton.cu", "skeleton_static.cu", "batched_lu.cu", "p1_assembly.cu",
+           "general_pcg.cu"]
 LIBRARY = PKG / "libmhm_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -26,23 +27,41 @@ def nvcc() -> str:
     return cand
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    srcs = [PKG / "csrc" / s for s in SOURCES]
-    deps = srcs + [PKG / "csrc" / "mhm_common.cuh", ROOT / "include" / "mhm_b200.h"]
-    if LIBRARY.exists() and not force:
-        built = LIBRARY.stat().st_mtime
-        if all(p.stat().st_mtime <= built for p in deps):
-            return LIBRARY
-    tmp = LIBRARY.with_suffix(".so.tmp")
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           f"-I{ROOT / 'include'}", "-diag-suppress", "177", "-o", str(tmp), *map(str, srcs)]
+def _compile(src: Path, obj: Path, verbose: bool) -> str:
+    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", f"-I{ROOT / 'include'}",
+           "-diag-suppress", "177", "-c", str(src), "-o", str(obj)]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     proc = subprocess.run(cmd, capture_output=True, text=True)
     if proc.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + proc.stdout + proc.stderr)
+        raise RuntimeError(f"nvcc failed on {src.name}:\n" + proc.stdout + proc.stderr)
+    return proc.stderr
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compile every source to an object in ``_build/`` (in parallel, only the ones whose
+    source or headers changed) and link ``libmhm_b200.so``."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    srcs = [PKG / "csrc" / s for s in SOURCES]
+    headers = [PKG / "csrc" / "mhm_common.cuh", ROOT / "include" / "mhm_b200.h"]
+    objdir = ROOT / "_build"
+    objdir.mkdir(exist_ok=True)
+    objs = [objdir / (p.stem + ".o") for p in srcs]
+    newest_header = max(h.stat().st_mtime for h in headers)
+    stale = [(s, o) for s, o in zip(srcs, objs)
+             if force or not o.exists() or o.stat().st_mtime < max(s.stat().st_mtime, newest_header)]
+    if not stale and LIBRARY.exists() and all(o.stat().st_mtime <= LIBRARY.stat().st_mtime for o in objs):
+        return LIBRARY
+    with ThreadPoolExecutor(max_workers=max(1, min(len(stale), os.cpu_count() or 1))) as pool:
+        logs = list(pool.map(lambda so: _compile(so[0], so[1], verbose), stale))
     if verbose:
-        sys.stderr.write(proc.stderr)
+        for log in logs:
+            sys.stderr.write(log)
+    tmp = LIBRARY.with_suffix(".so.tmp")
+    proc = subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs)], capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError("nvcc link failed:\n" + proc.stdout + proc.stderr)
     os.replace(tmp, LIBRARY)
     return LIBRARY
 

@@ -573,6 +573,50 @@ def skeleton_pattern(cell_dofs: np.ndarray, trace_size: int) -> SkeletonPattern:
                            lflat[lorder], trace_end)
 
 
+def block_offsets(cell_dofs) -> tuple[np.ndarray, np.ndarray]:
+    """Flat offsets of every cell's (t_K + 1)^2 block and (t_K + 1) load when the
+    cells' contributions are stored one after another (cells may differ in size)."""
+    t1 = np.array([len(d) + 1 for d in cell_dofs], dtype=np.int64)
+    bofs = np.zeros(len(t1) + 1, dtype=np.int64)
+    bofs[1:] = np.cumsum(t1 * t1)
+    lofs = np.zeros(len(t1) + 1, dtype=np.int64)
+    lofs[1:] = np.cumsum(t1)
+    return bofs, lofs
+
+
+def skeleton_pattern_ragged(cell_dofs, trace_size: int) -> SkeletonPattern:
+    """``skeleton_pattern`` for cells with different numbers of trace DOFs (polygons):
+    cell K's block over ``[cell_dofs[K], T + K]`` is stored at ``block_offsets`` and
+    its entry (a, b) is ``offset_K + a (t_K + 1) + b``."""
+    bofs, lofs = block_offsets(cell_dofs)
+    cells = len(cell_dofs)
+    idx = [np.r_[np.asarray(d, dtype=np.int64), trace_size + k] for k, d in enumerate(cell_dofs)]
+    rows = np.concatenate([np.repeat(i, len(i)) for i in idx]) if cells else np.zeros(0, np.int64)
+    cols = np.concatenate([np.tile(i, len(i)) for i in idx]) if cells else np.zeros(0, np.int64)
+    flat = np.arange(bofs[-1], dtype=np.int64)
+    order = np.lexsort((flat, cols, rows))
+    r, c, f = rows[order], cols[order], flat[order]
+    new = np.ones(len(r), dtype=bool)
+    new[1:] = (r[1:] != r[:-1]) | (c[1:] != c[:-1])
+    slot_start = np.flatnonzero(new)
+    size = trace_size + cells
+    indices = c[slot_start].astype(np.int32)
+    indptr = np.zeros(size + 1, dtype=np.int64)
+    np.add.at(indptr, r[slot_start] + 1, 1)
+    indptr = np.cumsum(indptr)
+    slot_ptr = np.r_[slot_start, len(r)].astype(np.int64)
+    lrows = np.concatenate(idx) if cells else np.zeros(0, np.int64)
+    lflat = np.arange(lofs[-1], dtype=np.int64)
+    lorder = np.lexsort((lflat, lrows))
+    load_ptr = np.zeros(size + 1, dtype=np.int64)
+    np.add.at(load_ptr, lrows + 1, 1)
+    load_ptr = np.cumsum(load_ptr)
+    for_row = indices < trace_size
+    counts = np.add.reduceat(for_row.astype(np.int64), indptr[:-1]) if len(indices) else np.zeros(size, np.int64)
+    trace_end = indptr[:trace_size] + counts[:trace_size]
+    return SkeletonPattern(size, trace_size, indptr, indices, slot_ptr, f, load_ptr, lflat[lorder], trace_end)
+
+
 def transpose_slots(indptr: np.ndarray, indices: np.ndarray) -> np.ndarray:
     """For a CSR pattern that is symmetric, ``out[k]`` = the slot of (i, j) for the slot
     k of (j, i).  Sorting the slots by (column, row) lists them in the CSR order of the

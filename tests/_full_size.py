@@ -32,13 +32,26 @@ def oracle_solution():
     return _CACHE["sol"]
 
 
+def stored_values(m, rows, cols):
+    """Values of the stored entries (row, col) of a CSR matrix, 0 where none is stored."""
+    out = np.zeros(len(rows))
+    for k, (i, j) in enumerate(zip(rows, cols)):
+        lo, hi = m.indptr[i], m.indptr[i + 1]
+        p = lo + np.searchsorted(m.indices[lo:hi], j)
+        if p < hi and m.indices[p] == j:
+            out[k] = m.data[p]
+    return out
+
+
 def pattern_differences(mine, ref):
     """Entries stored by exactly one of two sparse matrices: (rows, cols, |mine|, |ref|)."""
     a = sparse.csr_matrix(mine)
     b = sparse.csr_matrix(ref)
+    a.sort_indices()
+    b.sort_indices()
     ones_a, ones_b = a.copy(), b.copy()
     ones_a.data[:] = 1.0
     ones_b.data[:] = 1.0
     only = (ones_a - ones_a.multiply(ones_b)) + (ones_b - ones_b.multiply(ones_a))
     r, c = only.nonzero()
-    return r, c, np.abs(np.asarray(a[r, c]).ravel()), np.abs(np.asarray(b[r, c]).ravel())
+    return r, c, np.abs(stored_values(a, r, c)), np.abs(stored_values(b, r, c))
