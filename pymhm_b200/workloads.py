@@ -49,6 +49,41 @@ def lognormal_permeability(cells_x: int, cells_y: int | None = None, *, sigma: f
     return np.exp(field)
 
 
+def layered_lognormal_permeability(layers: int = 40, pixels: int = 64, *, sigma: float = 3.0, ell: float = 0.1,
+                                   contrast: float = 1e6, seed: int = DEFAULT_SEED) -> np.ndarray:
+    """``(layers, pixels, pixels)`` permeability of a layered unit cube: layer k (of
+    equal thickness along z) holds its own ``lognormal_permeability`` of the
+    ``pixels`` x ``pixels`` cell centres in (x, y) (seed ``seed + k``), log-values
+    clipped to +-log(contrast)/2 so that max / min <= contrast."""
+    half = 0.5 * np.log(contrast)
+    out = np.empty((layers, pixels, pixels))
+    for k in range(layers):
+        g = np.log(lognormal_permeability(pixels, pixels, sigma=sigma, ell=ell, seed=seed + k))
+        out[k] = np.exp(np.clip(g, -half, half))
+    return out
+
+
+class LayeredField:
+    """Piecewise-constant scalar permeability of the unit cube on a layered pixel
+    grid: point (x, y, z) takes ``values[min(floor(z L), L-1), min(floor(x P), P-1),
+    min(floor(y P), P-1)]`` (coordinates clipped to [0, 1]).  Callable on (n, 3)
+    points, as the reference's material callables are."""
+
+    def __init__(self, values: np.ndarray):
+        self.values = np.ascontiguousarray(values, dtype=float)
+
+    def index(self, points: np.ndarray) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        L, P, Q = self.values.shape
+        p = np.clip(np.asarray(points, dtype=float), 0.0, 1.0)
+        k = np.minimum((p[:, 2] * L).astype(np.int64), L - 1)
+        i = np.minimum((p[:, 0] * P).astype(np.int64), P - 1)
+        j = np.minimum((p[:, 1] * Q).astype(np.int64), Q - 1)
+        return k, i, j
+
+    def __call__(self, points: np.ndarray) -> np.ndarray:
+        return self.values[self.index(points)]
+
+
 def sine_source(points: np.ndarray) -> np.ndarray:
     """Manufactured source ``2 pi^2 sin(pi x) sin(pi y)``."""
     return 2 * np.pi ** 2 * np.sin(np.pi * points[:, 0]) * np.sin(np.pi * points[:, 1])
@@ -67,5 +102,7 @@ def digest(array: np.ndarray) -> str:
 # Workload descriptions used by bench.py and the parity tests.
 POISSON_8x8 = dict(name="poisson-q1-8x8-r4-p1", macro=8, local=4, face_degree=1,
                    permeability="one", source="sine")
+TETRA_8 = dict(name="darcy-p1-tetra-cube8-r8-p1faces-layered", cube=8, local=8, face_degree=1, layers=40,
+               pixels=64, sigma=3.0, ell=0.1, contrast=1e6, seed=DEFAULT_SEED)
 DARCY_64x64 = dict(name="darcy-q1-64x64-r16-p2-lognormal", macro=64, local=16, face_degree=2,
                    permeability="lognormal", source="one", sigma=2.0, ell=0.05, seed=DEFAULT_SEED)

@@ -17,6 +17,9 @@ calls two of its functions:
 The P1 operator fixtures (``make_p1_golden.py``) also need the degree-one
 Lagrange basis on triangles and tetrahedra (barycentric coordinates).
 
+The tetrahedral fixtures (``make_tetra_golden.py``) need the Bernstein basis of the
+triangular skeleton faces too.
+
 All are restated here from their published mathematics: the nodal Lagrange
 basis on the declared node order (unique polynomial interpolant, obtained by a
 Legendre-Vandermonde solve) with exact Kronecker rows at literal nodes, as the
@@ -95,6 +98,34 @@ def legendre_values(points, degree):
     return legendre_tabulation(points, degree)[0]
 
 
+def bernstein_tabulation(points, exponents):
+    """Simplex Bernstein polynomials B_alpha = (k! / alpha!) prod_a lambda_a^alpha_a of
+    degree k = |alpha| in the declared exponent order, lambda = (1 - sum x, x) for the
+    reference coordinates x; values (points, modes) and Cartesian gradients
+    (points, modes, dim).  Replaces ``pymhm.fem.reference.bernstein_tabulation``
+    (``reference.py:744-760``), which tabulates the same basis through Basix."""
+    from math import factorial
+
+    x = np.asarray(points, dtype=float)
+    lam = np.column_stack((1 - x.sum(axis=1), x))
+    dim = x.shape[1]
+    vals = np.empty((len(x), len(exponents)))
+    grads = np.zeros((len(x), len(exponents), dim))
+    for m, alpha in enumerate(exponents):
+        k = sum(alpha)
+        coef = factorial(k) / np.prod([factorial(a) for a in alpha])
+        vals[:, m] = coef * np.prod([lam[:, a] ** p for a, p in enumerate(alpha)], axis=0)
+        # d lambda_0 / d x_i = -1, d lambda_{i+1} / d x_i = 1
+        dl = np.zeros((len(x), dim + 1))
+        for a, p in enumerate(alpha):
+            if p == 0:
+                continue
+            rest = np.prod([lam[:, b] ** q for b, q in enumerate(alpha) if b != a], axis=0)
+            dl[:, a] = coef * p * lam[:, a] ** (p - 1) * rest
+        grads[:, m, :] = dl[:, 1:] - dl[:, :1]
+    return vals, grads
+
+
 def install():
     """Patch the reference modules in place (idempotent)."""
     import pymhm.fem.reference as ref
@@ -103,4 +134,5 @@ def install():
     ref.simplex_lagrange_tabulation = simplex_lagrange_tabulation
     ref.legendre_tabulation = legendre_tabulation
     ref.legendre_values = legendre_values
+    ref.bernstein_tabulation = bernstein_tabulation
     quad.simplex_lagrange_tabulation = simplex_lagrange_tabulation
