@@ -255,6 +255,62 @@ def cut_material_campaign(torch, steps=5, pixels=1000):
     return out
 
 
+def tetra_campaign(torch, steps=5, warmup=2, cube=8, local=8, cpu_cells=16):
+    """3D Primal-MHM Darcy (config 4): the unit cube split into cube^3 x 6 macro
+    tetrahedra (3072 at cube = 8), each red-refined to local^3 fine tetrahedra (165 P1
+    nodes at local = 8), Bernstein P1 modes on every macroface (3 per face: the
+    constant and the linear modes), 40 horizontal layers of log-normal permeability
+    (sigma 3, correlation length 0.1, contrast 1e6, on 64 x 64 pixels), f = 1,
+    homogeneous Dirichlet data, FP64.  One solve at a time with CUDA events per stage;
+    the oracle's local stage on a sample of cells in this process beside it."""
+    from pymhm_b200.tetra import TetraMesh, TriangularSkeleton
+    from pymhm_b200.tetra_darcy import TetraP1Plan
+    from pymhm_b200.workloads import LayeredField, layered_lognormal_permeability
+
+    t0 = time.perf_counter()
+    mesh = TetraMesh.unit_cube(cube)
+    sk = TriangularSkeleton(mesh, 1)
+    field = LayeredField(layered_lognormal_permeability(40, 64, sigma=3.0, ell=0.1, contrast=1e6, seed=SEED))
+    plan = TetraP1Plan(mesh, sk, local)
+    plan.set_coefficients(field, 1.0)
+    plan_s = time.perf_counter() - t0
+    st = torch.cuda.current_stream()
+    for _ in range(warmup):
+        plan.launch(st)
+    torch.cuda.synchronize()
+    plan.check()
+    per = []
+    for _ in range(steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        plan.launch(st, events=ev)
+        torch.cuda.synchronize()
+        per.append([ev[k].elapsed_time(ev[k + 1]) for k in range(4)])
+    sol = plan.result()
+    per = np.array(per)
+    ms = float(per.sum(axis=1).mean())
+    out = {"solves_per_s": 1000.0 / ms, "ms_per_solve": ms,
+           "stages_ms": {"local_stage": float(per[:, 0].mean()), "skeleton_scatter": float(per[:, 1].mean()),
+                         "general_pcg": float(per[:, 2].mean()), "reconstruct": float(per[:, 3].mean())},
+           "macrocells": plan.M, "local_nodes": plan.n, "trace_per_cell": plan.t, "skeleton_unknowns": plan.N,
+           "global_iterations": sol.global_iterations, "outer_corrections": sol.outer_corrections,
+           "residual": sol.residual, "plan_build_s": plan_s}
+    if cpu_cells:
+        from oracle import tetra_mhm as ot
+        from oracle.q1_mhm import condense, contribution
+
+        cells = np.linspace(0, plan.M - 1, cpu_cells).astype(int)
+        c0 = time.perf_counter()
+        for c in cells:
+            _, prob = ot.local_problem(mesh, sk, int(c), local, field, 1.0)
+            contribution(condense(prob), sk.size + int(c))
+        rate = len(cells) / (time.perf_counter() - c0)
+        out["cpu_oracle_local_cells_per_s"] = {"value": rate, "cores": 1, "sample": f"{len(cells)} of {plan.M} "
+                                               "macrocells, local operators + condensation + contribution"}
+    del plan
+    torch.cuda.empty_cache()
+    return out
+
+
 def serving_campaign(torch, lambdas=(100, 500, 2000), requests=150, precisions=("mixed", "fp64")):
     """Streamed serving (continuous batching with admission by HBM footprint): Poisson
     arrivals at each rate in ``lambdas``; per request a macro grid from {16, 32, 64}^2,
@@ -804,6 +860,7 @@ def main():
     serving_stream = serving_campaign(torch)
     small_poisson = small_poisson_campaign(torch)
     cut_material = cut_material_campaign(torch)
+    tetra = tetra_campaign(torch)
 
     # the reference's own batched local-stage benchmark, same phases and sizes
     campaigns = {f"batched_local_r{r}": batched_local_campaign(torch, r) for r in (12, 24)}
@@ -978,6 +1035,7 @@ def main():
         "serving_stream": serving_stream,
         "poisson_8x8_r4_p1": small_poisson,
         "cut_material": cut_material,
+        "tetra_3d": tetra,
         "global_iterations": int(mixed["info"][1]), "outer_corrections": int(mixed["info"][2]),
         "residual": float(mixed["stats"][0]), "certificate": float(mixed["stats"][1]),
         "error_vs_reference": acc,

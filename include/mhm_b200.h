@@ -443,6 +443,55 @@ int mhm_general_solve(const mhm_general_system* s /* host */, const double* rhs,
                       void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Dense local problems (tetrahedral macrocells)                             */
+/* ------------------------------------------------------------------------ */
+/*
+ * Material pre-pass of tetra_operators (fem/scalar/tetrahedron.py:41-52,
+ * 157-190) for a layered voxel permeability: for every macrocell (vertices
+ * macro_vertices (cells, 4, 3)) and fine tetrahedron e of its refinement
+ * (fine_cells (nfine, 4) into ref_bary (npoints, 4)), the quadrature average
+ * sum_q w_q kappa(x_q) over quad_bary / quad_weights (nquad), kappa the voxel
+ * value voxels[layer(z)][ix(x)][iy(y)] (layers x px x py over the unit cube).
+ * Writes the isotropic tensors diffusion (cells, nfine, 3, 3).
+ */
+int mhm_tet_kappa(int64_t cells, const double* macro_vertices, int32_t npoints, const double* ref_bary,
+                  int32_t nfine, const int32_t* fine_cells, int32_t nquad, const double* quad_bary,
+                  const double* quad_weights, int32_t layers, int32_t px, int32_t py,
+                  const double* voxels, double* diffusion, void* stream);
+
+/*
+ * Local contract and augmented systems of `count` dense local problems
+ * (LocalProblem.__init__, core/contracts.py:92-211, with kernel 1 and
+ * constraint M 1; local_condensation_system, core/condensation.py:125-174):
+ * stiffness / mass (count, n, n), load (count, n), coupling (count, n, t),
+ * t <= 12.  Writes aug (count, n+1, n+1) = [[A, c~], [c~^T, 0]] with
+ * c~ = M 1 min(1, max|A| / max|M 1|), rhs (count, n+1, t+2) = [f | B | A 1]
+ * (the last column zero when the cell is not corrected), action (count, 2, n)
+ * = A 1 and A^T 1 (double-double sums), corrected (count) and status (count:
+ * MHM_CELL_KERNEL when the constant is not a left and right kernel at 1e-10).
+ */
+int mhm_dense_systems(int64_t count, int32_t n, int32_t t, const double* stiffness, const double* mass,
+                      const double* load, const double* coupling, double* aug, double* rhs,
+                      double* action, uint8_t* corrected, int32_t* status, void* stream);
+
+/*
+ * Oriented Schur block (count, t+1, t+1) and reduced load (count, t+1) of each
+ * cell from its solved augmented system solution (count, n+1, t+2) =
+ * [R f | R B | R A 1] (local_global_contribution, core/contributions.py:14-74;
+ * local_condensed_load, core/reconstruction.py:91-127).  The products run on
+ * the tensor cores (FP64 mma.sync).
+ */
+int mhm_dense_contributions(int64_t count, int32_t n, int32_t t, const double* solution,
+                            const double* coupling, const double* action, const double* load,
+                            double* blocks, double* loads, void* stream);
+
+/* u_K = R f - (R B) lambda_K + (1 - R A 1) c_K for dense cells (core/reconstruction.py:
+ * 130-141): fields (count, n); cell_dofs (count, t); x = trace then coarse unknowns. */
+int mhm_dense_reconstruct(int64_t count, int32_t n, int32_t t, const double* solution,
+                          const int64_t* cell_dofs, int64_t trace_size, const double* x, double* fields,
+                          void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Reconstruction u_K = R f - (R B) lambda_K + E c_K and flux -K grad u       */
 /* ------------------------------------------------------------------------ */
 int mhm_q1_reconstruct(const mhm_q1_problem* p /* host */, const double* solution,

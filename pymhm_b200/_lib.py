@@ -112,6 +112,11 @@ _SIGNATURES = {
     "mhm_general_workspace_bytes": (C.c_int64, [C.POINTER(GeneralSystem)]),
     "mhm_general_solve": (C.c_int, [C.POINTER(GeneralSystem), P, P, P, C.c_int64, C.c_double, C.c_double,
                                     C.c_int32, C.c_int32, P, P, P]),
+    "mhm_tet_kappa": (C.c_int, [C.c_int64, P, C.c_int32, P, C.c_int32, P, C.c_int32, P, P, C.c_int32, C.c_int32,
+                                C.c_int32, P, P, P]),
+    "mhm_dense_systems": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, P, P, P, P, P, P, P, P, P]),
+    "mhm_dense_contributions": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, P, P, P, P, P, P]),
+    "mhm_dense_reconstruct": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, P, C.c_int64, P, P, P]),
     "mhm_q1_reconstruct": (C.c_int, [C.POINTER(Q1Problem), P, P, C.c_int64, P, P, P, P]),
     "mhm_batched_factor": (C.c_int, [C.c_int64, C.c_int32, P, P, P, P, P, P, P]),
     "mhm_batched_solve": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, P, P, P, P, P, P, P, C.c_double,
@@ -157,8 +162,13 @@ def check(rc: int, what: str) -> None:
 
 
 def ptr(t) -> int:
-    """Device pointer of a torch tensor (None -> NULL)."""
-    return 0 if t is None else int(t.data_ptr())
+    """Device pointer of a torch tensor (None -> NULL).  The kernels index dense
+    row-major arrays, so a tensor whose strides are not row-major is refused."""
+    if t is None:
+        return 0
+    if not t.is_contiguous():
+        raise ValueError("device arrays passed to the library must be contiguous (row-major)")
+    return int(t.data_ptr())
 
 
 def stream_handle(stream) -> int:

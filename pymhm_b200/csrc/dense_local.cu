@@ -1,0 +1,329 @@
+// Local stage of macro meshes whose local problems are stored dense (tetrahedra and
+// other unstructured local meshes): the material pre-pass of the layered permeability,
+// the local contract and augmented systems, the condensation products on the tensor
+// cores, and the reconstruction.  The factorization and solves in between are the
+// batched equilibrated LU (batched_lu.cu).
+//
+// Reference (PyMHM 1.3.2, src/pymhm/):
+//   material quadrature  fem/scalar/tetrahedron.py:41-52, 157-190 (Duffy rule, points
+//                        einsum("qi,tij->tqj", bary, vertices))
+//   local contract       core/contracts.py:92-211 (kernel 1, constraint M 1, the
+//                        retained and test actions A 1 and A^T 1, corrected flag)
+//   augmented system     core/condensation.py:125-174 (scaling min(1, max|A|/max|C|))
+//   contributions        core/contributions.py:14-74, core/reconstruction.py:91-127
+//   reconstruction       core/reconstruction.py:130-141
+#include <cmath>
+#include <cstdint>
+
+#include "mhm_common.cuh"
+
+namespace mhm {
+namespace {
+
+// ---------------------------------------------------------------------------------
+// Material pre-pass: for every (macrocell, fine tetrahedron) the Duffy-rule average
+// sum_q w_q kappa(x_q) of a layered voxel field, written as the isotropic tensor the
+// P1 assembly reads.  The fine vertices are bary @ macro vertices (the submesh), each
+// quadrature point ((b0 p0 + b1 p1) + b2 p2) + b3 p3 with separate roundings, which is
+// the order NumPy's einsum uses, so that points on either side of a voxel face select
+// the same voxel as the reference's evaluation.
+// ---------------------------------------------------------------------------------
+__global__ void tet_kappa_kernel(int64_t cells, const double* __restrict__ macro, int npoints,
+                                 const double* __restrict__ ref_bary, int nfine, const int32_t* __restrict__ fine_cells,
+                                 int nquad, const double* __restrict__ qbary, const double* __restrict__ qw,
+                                 int layers, int px, int py, const double* __restrict__ voxels,
+                                 double* __restrict__ diffusion) {
+  const int64_t total = cells * (int64_t)nfine;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < total; id += stride) {
+    const int64_t cell = id / nfine;
+    const int e = (int)(id - cell * nfine);
+    const double* X = macro + cell * 12;
+    double p[4][3];
+    for (int v = 0; v < 4; ++v) {
+      const double* b = ref_bary + (int64_t)fine_cells[4 * e + v] * 4;
+      for (int j = 0; j < 3; ++j) {
+        double acc = __dmul_rn(b[0], X[j]);
+        acc = __dadd_rn(acc, __dmul_rn(b[1], X[3 + j]));
+        acc = __dadd_rn(acc, __dmul_rn(b[2], X[6 + j]));
+        p[v][j] = __dadd_rn(acc, __dmul_rn(b[3], X[9 + j]));
+      }
+    }
+    double kbar = 0.0;
+    for (int q = 0; q < nquad; ++q) {
+      const double* b = qbary + 4 * q;
+      double x[3];
+      for (int j = 0; j < 3; ++j) {
+        double acc = __dmul_rn(b[0], p[0][j]);
+        acc = __dadd_rn(acc, __dmul_rn(b[1], p[1][j]));
+        acc = __dadd_rn(acc, __dmul_rn(b[2], p[2][j]));
+        x[j] = __dadd_rn(acc, __dmul_rn(b[3], p[3][j]));
+      }
+      const double cx = fmin(fmax(x[0], 0.0), 1.0), cy = fmin(fmax(x[1], 0.0), 1.0),
+                   cz = fmin(fmax(x[2], 0.0), 1.0);
+      long long k = (long long)(cz * layers), i = (long long)(cx * px), j = (long long)(cy * py);
+      if (k > layers - 1) k = layers - 1;
+      if (i > px - 1) i = px - 1;
+      if (j > py - 1) j = py - 1;
+      kbar = fma(qw[q], __ldg(voxels + (k * px + i) * py + j), kbar);
+    }
+    double* D = diffusion + id * 9;
+    for (int a = 0; a < 9; ++a) D[a] = (a % 4 == 0) ? kbar : 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// Local contract and augmented systems, one CTA per cell.
+// ---------------------------------------------------------------------------------
+constexpr int kDThreads = 256;
+
+__global__ void __launch_bounds__(kDThreads) dense_system_kernel(int n, int t, const double* __restrict__ stiffness,
+                                                                  const double* __restrict__ mass,
+                                                                  const double* __restrict__ load,
+                                                                  const double* __restrict__ coupling,
+                                                                  double* __restrict__ aug, double* __restrict__ rhs,
+                                                                  double* __restrict__ action,
+                                                                  uint8_t* __restrict__ corrected,
+                                                                  int32_t* __restrict__ status) {
+  __shared__ double red[32];
+  __shared__ int nonzero;
+  const int64_t cell = blockIdx.x;
+  const int tid = threadIdx.x;
+  const double* A = stiffness + cell * (int64_t)n * n;
+  const double* Mm = mass + cell * (int64_t)n * n;
+  const int n1 = n + 1, w = t + 2;
+  double* K = aug + cell * (int64_t)n1 * n1;
+  double* R = rhs + cell * (int64_t)n1 * w;
+  double* act = action + cell * 2 * (int64_t)n;
+  if (tid == 0) nonzero = 0;
+  // max |A| and ||A||_F^2, the retained action A 1 and the test action A^T 1 (double-double
+  // sums, the reference's extended-precision _matrix_action), and the plain products
+  // A 1 that the kernel check reads
+  double amax = 0.0, fro = 0.0, r2 = 0.0, l2 = 0.0, cmax = 0.0;
+  __syncthreads();
+  for (int i = tid; i < n; i += blockDim.x) {
+    double hi = 0.0, lo = 0.0, plain = 0.0, chi = 0.0, clo = 0.0, cplain = 0.0;
+    for (int j = 0; j < n; ++j) {
+      const double a = A[(int64_t)i * n + j];
+      amax = fmax(amax, fabs(a));
+      fro = fma(a, a, fro);
+      dd_add(hi, lo, a);
+      plain += a;
+      const double b = A[(int64_t)j * n + i];
+      dd_add(chi, clo, b);
+      cplain += b;
+    }
+    const double ai = hi + lo, ti = chi + clo;
+    act[i] = ai;
+    act[n + i] = ti;
+    if (ai != 0.0 || ti != 0.0) nonzero = 1;
+    r2 = fma(plain, plain, r2);
+    l2 = fma(cplain, cplain, l2);
+    double c = 0.0;
+    for (int j = 0; j < n; ++j) c += Mm[(int64_t)i * n + j];
+    cmax = fmax(cmax, fabs(c));
+  }
+  amax = block_max(amax, red);
+  fro = block_sum(fro, red);
+  r2 = block_sum(r2, red);
+  l2 = block_sum(l2, red);
+  cmax = block_max(cmax, red);
+  __syncthreads();
+  const int corr = nonzero;
+  // declared kernel: ||A 1|| and ||A^T 1|| <= 1e-10 ||A||_F sqrt(n) (both scaled by max|A|)
+  int st = MHM_CELL_OK;
+  if (amax > 0.0 && (sqrt(r2) > 1e-10 * sqrt(fro) * sqrt((double)n) ||
+                     sqrt(l2) > 1e-10 * sqrt(fro) * sqrt((double)n)))
+    st = MHM_CELL_KERNEL;
+  const double scale = (cmax > 0.0) ? fmin(1.0, (amax > 0.0 ? amax : 1.0) / cmax) : 1.0;
+  for (int64_t k = tid; k < (int64_t)n1 * n1; k += blockDim.x) {
+    const int i = (int)(k / n1), j = (int)(k - (int64_t)i * n1);
+    double v;
+    if (i < n && j < n) v = A[(int64_t)i * n + j];
+    else if (i == n && j == n) v = 0.0;
+    else {
+      const int r = (i < n) ? i : j;
+      double c = 0.0;
+      for (int m = 0; m < n; ++m) c += Mm[(int64_t)r * n + m];
+      v = c * scale;
+    }
+    K[k] = v;
+  }
+  for (int64_t k = tid; k < (int64_t)n1 * w; k += blockDim.x) {
+    const int i = (int)(k / w), col = (int)(k - (int64_t)i * w);
+    double v = 0.0;
+    if (i < n) {
+      if (col == 0) v = load[cell * n + i];
+      else if (col <= t) v = coupling[(cell * n + i) * t + (col - 1)];
+      else v = corr ? act[i] : 0.0;
+    }
+    R[k] = v;
+  }
+  if (tid == 0) {
+    corrected[cell] = (uint8_t)corr;
+    status[cell] = st;
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// Condensation products on the tensor cores.  Per cell one GEMM P = L^T X with
+//   L = [B | A^T 1 | 1]          (n x (t+2): the t trace columns, the test action, ones)
+//   X = [R f | R B | E | 1 | f]  (n x (t+4), E = 1 - R (A 1))
+// in FP64 mma.sync m8n8k4 tiles (P is at most 16 x 16: t <= 12), one warp per 8 x 8
+// output tile over k-steps of 4 rows, operands staged in shared memory.  Then
+//   block[a][b] = P[a][1+b],  block[a][t] = -P[a][t+1]              (B^T lifts, -B^T E)
+//   block[t][b] = -(P[b][t+2] - P[t][1+b]),  block[t][t] = -P[t][t+1]
+//   load[a] = P[a][0],  load[t] = P[t][0] - P[t+1][t+3]
+// (contributions.py:40-47, reconstruction.py:91-127, corrected branch; with A 1 = 0
+// the test action is zero, E = 1 and these are the uncorrected formulas).
+// ---------------------------------------------------------------------------------
+constexpr int kTile = 16;
+constexpr int kKChunk = 64;
+
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(128) dense_contrib_kernel(int n, int t, const double* __restrict__ solution,
+                                                            const double* __restrict__ coupling,
+                                                            const double* __restrict__ action,
+                                                            const double* __restrict__ load,
+                                                            double* __restrict__ blocks, double* __restrict__ loads) {
+  __shared__ double Ls[kKChunk][kTile + 1];  // L rows (k) x columns (m)
+  __shared__ double Xs[kKChunk][kTile + 1];  // X rows (k) x columns (n)
+  __shared__ double Ps[kTile][kTile + 1];
+  const int64_t cell = blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int n1 = n + 1, w = t + 2, t1 = t + 1;
+  const double* X = solution + cell * (int64_t)n1 * w;
+  const double* Bm = coupling + cell * (int64_t)n * t;
+  const double* tact = action + cell * 2 * (int64_t)n + n;
+  const double* f = load + cell * (int64_t)n;
+  const int tm = warp >> 1, tn = warp & 1;  // this warp's 8 x 8 output tile
+  double d0 = 0.0, d1 = 0.0;
+  for (int k0 = 0; k0 < n; k0 += kKChunk) {
+    __syncthreads();
+    for (int e = tid; e < kKChunk * kTile; e += blockDim.x) {
+      const int k = e / kTile, c = e - k * kTile;
+      const int i = k0 + k;
+      double lv = 0.0, xv = 0.0;
+      if (i < n) {
+        if (c < t) lv = Bm[(int64_t)i * t + c];
+        else if (c == t) lv = tact[i];
+        else if (c == t + 1) lv = 1.0;
+        const double* xr = X + (int64_t)i * w;
+        if (c == 0) xv = xr[0];
+        else if (c <= t) xv = xr[c];
+        else if (c == t + 1) xv = 1.0 - xr[w - 1];
+        else if (c == t + 2) xv = 1.0;
+        else if (c == t + 3) xv = f[i];
+      }
+      Ls[k][c] = lv;
+      Xs[k][c] = xv;
+    }
+    __syncthreads();
+    const int kend = (n - k0 < kKChunk) ? (n - k0) : kKChunk;
+    for (int k = 0; k < kend; k += 4) {
+      // A fragment (row-major 8 x 4): row = lane / 4, col = lane % 4 -> L^T[m][k] = L[k][m]
+      const double a = Ls[k + (lane & 3)][tm * 8 + (lane >> 2)];
+      // B fragment (col-major 4 x 8): row = lane % 4, col = lane / 4 -> X[k][n]
+      const double b = Xs[k + (lane & 3)][tn * 8 + (lane >> 2)];
+      dmma_8x8x4(d0, d1, a, b);
+    }
+  }
+  // C fragment: row = lane / 4, columns 2 (lane % 4) and 2 (lane % 4) + 1
+  {
+    const int r = tm * 8 + (lane >> 2), c = tn * 8 + 2 * (lane & 3);
+    Ps[r][c] = d0;
+    Ps[r][c + 1] = d1;
+  }
+  __syncthreads();
+  double* blk = blocks + cell * (int64_t)t1 * t1;
+  double* ld = loads + cell * (int64_t)t1;
+  for (int e = tid; e < t1 * t1; e += blockDim.x) {
+    const int a = e / t1, b = e - a * t1;
+    double v;
+    if (a < t && b < t) v = Ps[a][1 + b];
+    else if (a < t) v = -Ps[a][t + 1];
+    else if (b < t) v = -(Ps[b][t + 2] - Ps[t][1 + b]);
+    else v = -Ps[t][t + 1];
+    blk[e] = v;
+  }
+  for (int a = tid; a < t1; a += blockDim.x) ld[a] = (a < t) ? Ps[a][0] : Ps[t][0] - Ps[t + 1][t + 3];
+}
+
+// u = R f - (R B) lambda_K + E c_K, thread per (cell, node).
+__global__ void dense_reconstruct_kernel(int64_t cells, int n, int t, const double* __restrict__ solution,
+                                         const int64_t* __restrict__ cell_dofs, int64_t trace_size,
+                                         const double* __restrict__ x, double* __restrict__ fields) {
+  const int64_t total = cells * (int64_t)n;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int w = t + 2;
+  for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < total; id += stride) {
+    const int64_t cell = id / n;
+    const int i = (int)(id - cell * n);
+    const double* xr = solution + (cell * (n + 1) + i) * w;
+    double u = xr[0];
+    for (int b = 0; b < t; ++b) u = fma(-xr[1 + b], x[cell_dofs[cell * t + b]], u);
+    u = fma(1.0 - xr[w - 1], x[trace_size + cell], u);
+    fields[id] = u;
+  }
+}
+
+int grid_for(int64_t work) {
+  int64_t b = (work + 255) / 256;
+  if (b > 65535) b = 65535;
+  return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+}  // namespace mhm
+
+using namespace mhm;
+
+extern "C" int mhm_tet_kappa(int64_t cells, const double* macro_vertices, int32_t npoints, const double* ref_bary,
+                             int32_t nfine, const int32_t* fine_cells, int32_t nquad, const double* quad_bary,
+                             const double* quad_weights, int32_t layers, int32_t px, int32_t py,
+                             const double* voxels, double* diffusion, void* stream) {
+  if (cells < 1 || npoints < 4 || nfine < 1 || nquad < 1 || layers < 1 || px < 1 || py < 1 || !macro_vertices ||
+      !ref_bary || !fine_cells || !quad_bary || !quad_weights || !voxels || !diffusion)
+    return MHM_ERR_ARGUMENT;
+  tet_kappa_kernel<<<grid_for(cells * nfine), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      cells, macro_vertices, npoints, ref_bary, nfine, fine_cells, nquad, quad_bary, quad_weights, layers, px, py,
+      voxels, diffusion);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+extern "C" int mhm_dense_systems(int64_t count, int32_t n, int32_t t, const double* stiffness, const double* mass,
+                                 const double* load, const double* coupling, double* aug, double* rhs,
+                                 double* action, uint8_t* corrected, int32_t* status, void* stream) {
+  if (count < 1 || count > INT32_MAX || n < 1 || t < 1 || t > kTile - 4 || !stiffness || !mass || !load ||
+      !coupling || !aug || !rhs || !action || !corrected || !status)
+    return MHM_ERR_ARGUMENT;
+  dense_system_kernel<<<(unsigned)count, kDThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      n, t, stiffness, mass, load, coupling, aug, rhs, action, corrected, status);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+extern "C" int mhm_dense_contributions(int64_t count, int32_t n, int32_t t, const double* solution,
+                                       const double* coupling, const double* action, const double* load,
+                                       double* blocks, double* loads, void* stream) {
+  if (count < 1 || count > INT32_MAX || n < 1 || t < 1 || t > kTile - 4 || !solution || !coupling || !action ||
+      !load || !blocks || !loads)
+    return MHM_ERR_ARGUMENT;
+  dense_contrib_kernel<<<(unsigned)count, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+      n, t, solution, coupling, action, load, blocks, loads);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+extern "C" int mhm_dense_reconstruct(int64_t count, int32_t n, int32_t t, const double* solution,
+                                     const int64_t* cell_dofs, int64_t trace_size, const double* x, double* fields,
+                                     void* stream) {
+  if (count < 1 || n < 1 || t < 1 || trace_size < 1 || !solution || !cell_dofs || !x || !fields)
+    return MHM_ERR_ARGUMENT;
+  dense_reconstruct_kernel<<<grid_for(count * n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      count, n, t, solution, cell_dofs, trace_size, x, fields);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}

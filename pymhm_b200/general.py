@@ -103,7 +103,7 @@ class GeneralSkeleton:
         qinv = coarse_inverse(self.cell_ptr, self.flat_dofs, self.flat_g0, self.T)
 
         def up(a, dtype):
-            return torch.as_tensor(np.array(a, copy=True), dtype=dtype).to(self.device)
+            return torch.as_tensor(np.array(a, order="C", copy=True), dtype=dtype).to(self.device)
 
         self._keep = dict(
             indptr=up(indptr, torch.int64), indices=up(indices, torch.int32), face_ptr=up(face_ptr, torch.int64),
