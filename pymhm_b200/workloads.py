@@ -84,6 +84,38 @@ class LayeredField:
         return self.values[self.index(points)]
 
 
+def disc_inclusions(count: int = 300, *, rmin: float = 0.01, rmax: float = 0.03,
+                    seed: int = DEFAULT_SEED) -> tuple[np.ndarray, np.ndarray]:
+    """``count`` discs with PCG64-uniform centres in the unit square and radii uniform
+    in [rmin, rmax]: (centres (count, 2), radii (count,))."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    centres = rng.uniform(0.0, 1.0, size=(count, 2))
+    radii = rng.uniform(rmin, rmax, size=count)
+    return centres, radii
+
+
+class DiscInclusions:
+    """Piecewise-constant scalar permeability: ``inside`` in the union of the discs,
+    ``outside`` elsewhere.  A point is inside a disc when
+    (x - cx)^2 + (y - cy)^2 <= r^2, each square and the sum rounded separately.
+    Callable on (n, 2) points, as the reference's material callables are."""
+
+    def __init__(self, centres, radii, inside: float = 1e4, outside: float = 1.0):
+        self.centres = np.ascontiguousarray(centres, dtype=float)
+        self.radii = np.ascontiguousarray(radii, dtype=float)
+        self.r2 = self.radii * self.radii
+        self.inside, self.outside = float(inside), float(outside)
+
+    def __call__(self, points: np.ndarray) -> np.ndarray:
+        p = np.asarray(points, dtype=float)
+        hit = np.zeros(len(p), dtype=bool)
+        for (cx, cy), r2 in zip(self.centres, self.r2):
+            dx = p[:, 0] - cx
+            dy = p[:, 1] - cy
+            hit |= (dx * dx + dy * dy) <= r2
+        return np.where(hit, self.inside, self.outside)
+
+
 def sine_source(points: np.ndarray) -> np.ndarray:
     """Manufactured source ``2 pi^2 sin(pi x) sin(pi y)``."""
     return 2 * np.pi ** 2 * np.sin(np.pi * points[:, 0]) * np.sin(np.pi * points[:, 1])

@@ -68,13 +68,51 @@ def _simplex_p1(bary, nodes, nderiv):
     return vals, gradient, hessian
 
 
+def _triangle_lagrange(degree, bary, nodes, nderiv):
+    """Degree-k nodal Lagrange basis on a triangle for the declared nodes (barycentric
+    rows): the unique polynomial interpolant, from a monomial Vandermonde solve in the
+    reference coordinates (x, y) = (lambda_1, lambda_2), with exact Kronecker rows at the
+    nodes; gradients and Hessians in (x, y)."""
+    powers = [(i, j) for i in range(degree + 1) for j in range(degree + 1 - i)]
+    nx, ny = nodes[:, 1], nodes[:, 2]
+    vand = np.array([[x ** i * y ** j for (i, j) in powers] for x, y in zip(nx, ny)])
+    coef = np.linalg.solve(vand, np.eye(len(powers)))  # column m: coefficients of phi_m
+    x, y = bary[:, 1], bary[:, 2]
+
+    def mono(dx, dy):
+        out = np.zeros((len(x), len(powers)))
+        for k, (i, j) in enumerate(powers):
+            if i < dx or j < dy:
+                continue
+            ci = np.prod(range(i - dx + 1, i + 1)) if dx else 1.0
+            cj = np.prod(range(j - dy + 1, j + 1)) if dy else 1.0
+            out[:, k] = ci * cj * x ** (i - dx) * y ** (j - dy)
+        return out
+
+    vals = mono(0, 0) @ coef
+    rows, cols = np.nonzero(np.all(bary[:, None, :] == nodes[None, :, :], axis=2))
+    vals[rows] = 0.0
+    vals[rows, cols] = 1.0
+    grad = np.stack((mono(1, 0) @ coef, mono(0, 1) @ coef), axis=-1) if nderiv else np.empty((*vals.shape, 0))
+    if nderiv == 2:
+        hess = np.empty((*vals.shape, 2, 2))
+        hess[..., 0, 0] = mono(2, 0) @ coef
+        hess[..., 0, 1] = hess[..., 1, 0] = mono(1, 1) @ coef
+        hess[..., 1, 1] = mono(0, 2) @ coef
+    else:
+        hess = np.empty((*vals.shape, 0, 0))
+    return vals, grad, hess
+
+
 def simplex_lagrange_tabulation(cell, degree, bary, *, nodes, nderiv=2):
     bary = np.asarray(bary, dtype=float)
     nodes = np.asarray(nodes, dtype=float)
     if cell in ("triangle", "tetrahedron") and int(degree) == 1:
         return _simplex_p1(bary, nodes, nderiv)
+    if cell == "triangle":
+        return _triangle_lagrange(int(degree), bary, nodes, nderiv)
     if cell != "interval":
-        raise NotImplementedError("the fixture shim covers intervals and degree-one simplices only")
+        raise NotImplementedError("the fixture shim covers intervals, triangles and degree-one tetrahedra")
     vals, ders = _interval_lagrange(int(degree), bary[:, 1], nodes[:, 1], nderiv)
     gradient = ders[:, :, None] if nderiv else np.empty((*vals.shape, 0))
     hessian = np.empty((*vals.shape, 0, 0))
