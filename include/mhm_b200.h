@@ -462,34 +462,70 @@ int mhm_tet_kappa(int64_t cells, const double* macro_vertices, int32_t npoints, 
 /*
  * Local contract and augmented systems of `count` dense local problems
  * (LocalProblem.__init__, core/contracts.py:92-211, with kernel 1 and
- * constraint M 1; local_condensation_system, core/condensation.py:125-174):
- * stiffness / mass (count, n, n), load (count, n), coupling (count, n, t),
- * t <= 12.  Writes aug (count, n+1, n+1) = [[A, c~], [c~^T, 0]] with
- * c~ = M 1 min(1, max|A| / max|M 1|), rhs (count, n+1, t+2) = [f | B | A 1]
- * (the last column zero when the cell is not corrected), action (count, 2, n)
- * = A 1 and A^T 1 (double-double sums), corrected (count) and status (count:
+ * constraint M 1, divided by 1^T M 1 when `normalize` is set as the 2D primal
+ * driver does, _legacy/models/darcy/primal.py:69-71; local_condensation_system,
+ * core/condensation.py:125-174).  Cell k has n_of[k] unknowns and t_of[k] <= 28
+ * trace columns; its stiffness and mass are rows of lds doubles at
+ * k * lds * lds, its load at k * lds, its coupling (lds x tld) at k * lds * tld.
+ * Writes aug (count, nb, nb), nb >= n + 1: [[A, c~], [c~^T, 0]] with
+ * c~ = C min(1, max|A| / max|C|) and an identity block past n + 1; rhs
+ * (count, nb, w), w >= t + 2: [f | B | A 1] (the A 1 column zero when the cell
+ * is not corrected, zero rows past n); action (count, 3, nb) = A 1, A^T 1
+ * (double-double sums) and M 1; corrected (count); status (count:
  * MHM_CELL_KERNEL when the constant is not a left and right kernel at 1e-10).
  */
-int mhm_dense_systems(int64_t count, int32_t n, int32_t t, const double* stiffness, const double* mass,
+int mhm_dense_systems(int64_t count, int32_t lds, int32_t tld, int32_t nb, int32_t w, int32_t normalize,
+                      const int32_t* n_of, const int32_t* t_of, const double* stiffness, const double* mass,
                       const double* load, const double* coupling, double* aug, double* rhs,
                       double* action, uint8_t* corrected, int32_t* status, void* stream);
 
 /*
- * Oriented Schur block (count, t+1, t+1) and reduced load (count, t+1) of each
- * cell from its solved augmented system solution (count, n+1, t+2) =
- * [R f | R B | R A 1] (local_global_contribution, core/contributions.py:14-74;
+ * Oriented Schur block ((t+1) x (t+1), at blocks + block_off[k]) and reduced
+ * load (t+1, at loads + load_off[k]) of each cell from its solved augmented
+ * system solution (count, nb, w) = [R f | R B | R A 1]
+ * (local_global_contribution, core/contributions.py:14-74;
  * local_condensed_load, core/reconstruction.py:91-127).  The products run on
- * the tensor cores (FP64 mma.sync).
+ * the tensor cores (FP64 mma.sync); max_t is the largest t_of (at most 28).
  */
-int mhm_dense_contributions(int64_t count, int32_t n, int32_t t, const double* solution,
+int mhm_dense_contributions(int64_t count, int32_t lds, int32_t tld, int32_t nb, int32_t w, int32_t max_t,
+                            const int32_t* n_of, const int32_t* t_of, const double* solution,
                             const double* coupling, const double* action, const double* load,
-                            double* blocks, double* loads, void* stream);
+                            const int64_t* block_off, const int64_t* load_off, double* blocks,
+                            double* loads, void* stream);
+
+/*
+ * P2 triangle operators of polygonal macrocells (scalar_operators,
+ * fem/scalar/triangle.py:208-257, degree 2, a scalar permeability sampled at the
+ * Duffy rule's points, constant source), dense per cell.  Every fine triangle of
+ * every cell is one element: triangles (elements, 3) index points (x, y pairs).
+ * The permeability is `inside` in the union of the discs (centres (D, 2), squared
+ * radii radii2), else `outside`; grid > 0 gives a grid x grid cell list over the
+ * unit square (grid_ptr (grid^2 + 1) into grid_discs, cell gx * grid + gy, every
+ * disc meeting the cell listed); grid = 0 means a constant `outside`.
+ * element_scratch: mhm_p2_element_bytes.  Node g of all cells is row node_row[g]
+ * of cell node_cell[g]: its element incidences inc[inc_ptr[g] ..] (element * 6 +
+ * local index, ascending), elem_dofs (elements, 6) the cell-local DOFs; the cell's
+ * dense stiffness and mass start at dense_off[cell] with rows of ld_of[cell]
+ * doubles and its load at load_off[cell].  Rows are summed in element order.
+ */
+int64_t mhm_p2_element_bytes(int64_t elements);
+int mhm_p2_assemble(int64_t elements, const double* points, const int64_t* triangles, int32_t nquad,
+                    const double* quad_bary, const double* quad_weights, int32_t grid,
+                    const int32_t* grid_ptr, const int32_t* grid_discs, const double* centres,
+                    const double* radii2, double inside, double outside, double source,
+                    double* element_scratch, int64_t nodes, const int32_t* node_cell,
+                    const int32_t* node_row, const int64_t* inc_ptr, const int64_t* inc,
+                    const int32_t* elem_dofs, const int64_t* dense_off, const int32_t* ld_of,
+                    const int64_t* load_off, double* stiffness, double* mass, double* load,
+                    void* stream);
 
 /* u_K = R f - (R B) lambda_K + (1 - R A 1) c_K for dense cells (core/reconstruction.py:
- * 130-141): fields (count, n); cell_dofs (count, t); x = trace then coarse unknowns. */
-int mhm_dense_reconstruct(int64_t count, int32_t n, int32_t t, const double* solution,
-                          const int64_t* cell_dofs, int64_t trace_size, const double* x, double* fields,
-                          void* stream);
+ * 130-141): cell k's n_of[k] values go to fields + field_off[k]; its trace DOFs
+ * are cell_dofs[dof_off[k] ...], its coarse unknown x[trace_size + cell_id[k]]. */
+int mhm_dense_reconstruct(int64_t count, int32_t nb, int32_t w, const int32_t* n_of, const int32_t* t_of,
+                          const double* solution, const int64_t* cell_dofs, const int64_t* dof_off,
+                          const int32_t* cell_id, int64_t trace_size, const double* x,
+                          const int64_t* field_off, double* fields, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Reconstruction u_K = R f - (R B) lambda_K + E c_K and flux -K grad u       */

@@ -114,9 +114,15 @@ _SIGNATURES = {
                                     C.c_int32, C.c_int32, P, P, P]),
     "mhm_tet_kappa": (C.c_int, [C.c_int64, P, C.c_int32, P, C.c_int32, P, C.c_int32, P, P, C.c_int32, C.c_int32,
                                 C.c_int32, P, P, P]),
-    "mhm_dense_systems": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, P, P, P, P, P, P, P, P, P]),
-    "mhm_dense_contributions": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, P, P, P, P, P, P]),
-    "mhm_dense_reconstruct": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, P, C.c_int64, P, P, P]),
+    "mhm_dense_systems": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, P, P,
+                                    P, P, P, P, P, P, P, P]),
+    "mhm_dense_contributions": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P,
+                                          P, P, P, P, P, P, P, P, P, P]),
+    "mhm_dense_reconstruct": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, P, P, P, P, P, C.c_int64, P, P, P,
+                                        P]),
+    "mhm_p2_element_bytes": (C.c_int64, [C.c_int64]),
+    "mhm_p2_assemble": (C.c_int, [C.c_int64, P, P, C.c_int32, P, P, C.c_int32, P, P, P, P, C.c_double, C.c_double,
+                                  C.c_double, P, C.c_int64, P, P, P, P, P, P, P, P, P, P, P, P]),
     "mhm_q1_reconstruct": (C.c_int, [C.POINTER(Q1Problem), P, P, C.c_int64, P, P, P, P]),
     "mhm_batched_factor": (C.c_int, [C.c_int64, C.c_int32, P, P, P, P, P, P, P]),
     "mhm_batched_solve": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, P, P, P, P, P, P, P, C.c_double,

@@ -15,7 +15,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 SOURCES = ["q1_condense.cu", "skeleton.cu", "skeleton_static.cu", "batched_lu.cu", "p1_assembly.cu",
-           "general_pcg.cu", "dense_local.cu"]
+           "general_pcg.cu", "dense_local.cu", "p2_local.cu"]
 LIBRARY = PKG / "libmhm_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -73,60 +73,69 @@ __global__ void tet_kappa_kernel(int64_t cells, const double* __restrict__ macro
 }
 
 // ---------------------------------------------------------------------------------
-// Local contract and augmented systems, one CTA per cell.
+// Local contract and augmented systems, one CTA per cell.  Cells of one launch share
+// the storage strides but may differ in size: cell k has n = n_of[k] unknowns and
+// t = t_of[k] trace columns; its stiffness, mass (rows of lds), load (lds) and
+// coupling (lds x tld) sit at k times their strides; its augmented matrix is nb x nb
+// (nb >= n + 1) and its right-hand sides nb x w (w >= t + 2).  Rows and columns past
+// n + 1 are an identity block with zero right-hand sides (solution zero there).
 // ---------------------------------------------------------------------------------
 constexpr int kDThreads = 256;
 
-__global__ void __launch_bounds__(kDThreads) dense_system_kernel(int n, int t, const double* __restrict__ stiffness,
-                                                                  const double* __restrict__ mass,
-                                                                  const double* __restrict__ load,
-                                                                  const double* __restrict__ coupling,
-                                                                  double* __restrict__ aug, double* __restrict__ rhs,
-                                                                  double* __restrict__ action,
-                                                                  uint8_t* __restrict__ corrected,
-                                                                  int32_t* __restrict__ status) {
+__global__ void __launch_bounds__(kDThreads) dense_system_kernel(
+    int lds, int tld, int nb, int w, int normalize, const int32_t* __restrict__ n_of,
+    const int32_t* __restrict__ t_of,
+    const double* __restrict__ stiffness, const double* __restrict__ mass, const double* __restrict__ load,
+    const double* __restrict__ coupling, double* __restrict__ aug, double* __restrict__ rhs,
+    double* __restrict__ action, uint8_t* __restrict__ corrected, int32_t* __restrict__ status) {
   __shared__ double red[32];
   __shared__ int nonzero;
   const int64_t cell = blockIdx.x;
   const int tid = threadIdx.x;
-  const double* A = stiffness + cell * (int64_t)n * n;
-  const double* Mm = mass + cell * (int64_t)n * n;
-  const int n1 = n + 1, w = t + 2;
-  double* K = aug + cell * (int64_t)n1 * n1;
-  double* R = rhs + cell * (int64_t)n1 * w;
-  double* act = action + cell * 2 * (int64_t)n;
+  const int n = n_of[cell], t = t_of[cell];
+  const double* A = stiffness + cell * (int64_t)lds * lds;
+  const double* Mm = mass + cell * (int64_t)lds * lds;
+  double* K = aug + cell * (int64_t)nb * nb;
+  double* R = rhs + cell * (int64_t)nb * w;
+  double* act = action + cell * 3 * (int64_t)nb;  // rows: A 1, A^T 1, the constraint
   if (tid == 0) nonzero = 0;
   // max |A| and ||A||_F^2, the retained action A 1 and the test action A^T 1 (double-double
-  // sums, the reference's extended-precision _matrix_action), and the plain products
-  // A 1 that the kernel check reads
-  double amax = 0.0, fro = 0.0, r2 = 0.0, l2 = 0.0, cmax = 0.0;
+  // sums, the reference's extended-precision _matrix_action), the plain products A 1
+  // that the kernel check reads, and the constraint C = M 1
+  double amax = 0.0, fro = 0.0, r2 = 0.0, l2 = 0.0, cmax = 0.0, csum = 0.0;
   __syncthreads();
   for (int i = tid; i < n; i += blockDim.x) {
     double hi = 0.0, lo = 0.0, plain = 0.0, chi = 0.0, clo = 0.0, cplain = 0.0;
     for (int j = 0; j < n; ++j) {
-      const double a = A[(int64_t)i * n + j];
+      const double a = A[(int64_t)i * lds + j];
       amax = fmax(amax, fabs(a));
       fro = fma(a, a, fro);
       dd_add(hi, lo, a);
       plain += a;
-      const double b = A[(int64_t)j * n + i];
+      const double b = A[(int64_t)j * lds + i];
       dd_add(chi, clo, b);
       cplain += b;
     }
     const double ai = hi + lo, ti = chi + clo;
     act[i] = ai;
-    act[n + i] = ti;
+    act[nb + i] = ti;
     if (ai != 0.0 || ti != 0.0) nonzero = 1;
     r2 = fma(plain, plain, r2);
     l2 = fma(cplain, cplain, l2);
     double c = 0.0;
-    for (int j = 0; j < n; ++j) c += Mm[(int64_t)i * n + j];
-    cmax = fmax(cmax, fabs(c));
+    for (int j = 0; j < n; ++j) c += Mm[(int64_t)i * lds + j];
+    act[2 * nb + i] = c;
+    csum += c;
   }
   amax = block_max(amax, red);
   fro = block_sum(fro, red);
   r2 = block_sum(r2, red);
   l2 = block_sum(l2, red);
+  csum = block_sum(csum, red);
+  // the 2D primal driver divides the constraint by its total, the cell's area
+  // (primal.py:69-71); the 3D driver keeps M 1 (primal_3d.py:58-65)
+  const double cdiv = normalize ? csum : 1.0;
+  for (int i = tid; i < n; i += blockDim.x) cmax = fmax(cmax, fabs(act[2 * nb + i] / cdiv));
   cmax = block_max(cmax, red);
   __syncthreads();
   const int corr = nonzero;
@@ -136,26 +145,22 @@ __global__ void __launch_bounds__(kDThreads) dense_system_kernel(int n, int t, c
                      sqrt(l2) > 1e-10 * sqrt(fro) * sqrt((double)n)))
     st = MHM_CELL_KERNEL;
   const double scale = (cmax > 0.0) ? fmin(1.0, (amax > 0.0 ? amax : 1.0) / cmax) : 1.0;
-  for (int64_t k = tid; k < (int64_t)n1 * n1; k += blockDim.x) {
-    const int i = (int)(k / n1), j = (int)(k - (int64_t)i * n1);
+  for (int64_t k = tid; k < (int64_t)nb * nb; k += blockDim.x) {
+    const int i = (int)(k / nb), j = (int)(k - (int64_t)i * nb);
     double v;
-    if (i < n && j < n) v = A[(int64_t)i * n + j];
+    if (i < n && j < n) v = A[(int64_t)i * lds + j];
+    else if (i > n || j > n) v = (i == j) ? 1.0 : 0.0;
     else if (i == n && j == n) v = 0.0;
-    else {
-      const int r = (i < n) ? i : j;
-      double c = 0.0;
-      for (int m = 0; m < n; ++m) c += Mm[(int64_t)r * n + m];
-      v = c * scale;
-    }
+    else v = (act[2 * nb + ((i < n) ? i : j)] / cdiv) * scale;
     K[k] = v;
   }
-  for (int64_t k = tid; k < (int64_t)n1 * w; k += blockDim.x) {
+  for (int64_t k = tid; k < (int64_t)nb * w; k += blockDim.x) {
     const int i = (int)(k / w), col = (int)(k - (int64_t)i * w);
     double v = 0.0;
     if (i < n) {
-      if (col == 0) v = load[cell * n + i];
-      else if (col <= t) v = coupling[(cell * n + i) * t + (col - 1)];
-      else v = corr ? act[i] : 0.0;
+      if (col == 0) v = load[cell * lds + i];
+      else if (col <= t) v = coupling[(cell * lds + i) * tld + (col - 1)];
+      else if (col == t + 1) v = corr ? act[i] : 0.0;
     }
     R[k] = v;
   }
@@ -169,16 +174,16 @@ __global__ void __launch_bounds__(kDThreads) dense_system_kernel(int n, int t, c
 // Condensation products on the tensor cores.  Per cell one GEMM P = L^T X with
 //   L = [B | A^T 1 | 1]          (n x (t+2): the t trace columns, the test action, ones)
 //   X = [R f | R B | E | 1 | f]  (n x (t+4), E = 1 - R (A 1))
-// in FP64 mma.sync m8n8k4 tiles (P is at most 16 x 16: t <= 12), one warp per 8 x 8
-// output tile over k-steps of 4 rows, operands staged in shared memory.  Then
+// in FP64 mma.sync m8n8k4 tiles over a TILE x TILE output (t + 4 <= TILE), one warp
+// per 8 x 8 output tile over k-steps of 4 rows, operands staged in shared memory.  Then
 //   block[a][b] = P[a][1+b],  block[a][t] = -P[a][t+1]              (B^T lifts, -B^T E)
 //   block[t][b] = -(P[b][t+2] - P[t][1+b]),  block[t][t] = -P[t][t+1]
 //   load[a] = P[a][0],  load[t] = P[t][0] - P[t+1][t+3]
 // (contributions.py:40-47, reconstruction.py:91-127, corrected branch; with A 1 = 0
-// the test action is zero, E = 1 and these are the uncorrected formulas).
+// the test action is zero, E = 1 and these are the uncorrected formulas).  The block
+// and load of cell k go to blocks + block_off[k] and loads + load_off[k].
 // ---------------------------------------------------------------------------------
-constexpr int kTile = 16;
-constexpr int kKChunk = 64;
+constexpr int kKChunk = 32;
 
 __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
@@ -186,37 +191,39 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
                : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(128) dense_contrib_kernel(int n, int t, const double* __restrict__ solution,
-                                                            const double* __restrict__ coupling,
-                                                            const double* __restrict__ action,
-                                                            const double* __restrict__ load,
-                                                            double* __restrict__ blocks, double* __restrict__ loads) {
-  __shared__ double Ls[kKChunk][kTile + 1];  // L rows (k) x columns (m)
-  __shared__ double Xs[kKChunk][kTile + 1];  // X rows (k) x columns (n)
-  __shared__ double Ps[kTile][kTile + 1];
+template <int TILE>
+__global__ void __launch_bounds__(TILE * TILE / 2) dense_contrib_kernel(
+    int lds, int tld, int nb, int w, const int32_t* __restrict__ n_of, const int32_t* __restrict__ t_of,
+    const double* __restrict__ solution, const double* __restrict__ coupling, const double* __restrict__ action,
+    const double* __restrict__ load, const int64_t* __restrict__ block_off, const int64_t* __restrict__ load_off,
+    double* __restrict__ blocks, double* __restrict__ loads) {
+  constexpr int kTilesPerSide = TILE / 8;
+  __shared__ double Ls[kKChunk][TILE + 1];  // L rows (k) x columns (m)
+  __shared__ double Xs[kKChunk][TILE + 1];  // X rows (k) x columns (n)
+  __shared__ double Ps[TILE][TILE + 1];
   const int64_t cell = blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int n1 = n + 1, w = t + 2, t1 = t + 1;
-  const double* X = solution + cell * (int64_t)n1 * w;
-  const double* Bm = coupling + cell * (int64_t)n * t;
-  const double* tact = action + cell * 2 * (int64_t)n + n;
-  const double* f = load + cell * (int64_t)n;
-  const int tm = warp >> 1, tn = warp & 1;  // this warp's 8 x 8 output tile
+  const int n = n_of[cell], t = t_of[cell];
+  const double* X = solution + cell * (int64_t)nb * w;
+  const double* Bm = coupling + cell * (int64_t)lds * tld;
+  const double* tact = action + cell * 3 * (int64_t)nb + nb;
+  const double* f = load + cell * (int64_t)lds;
+  const int tm = warp / kTilesPerSide, tn = warp % kTilesPerSide;  // this warp's 8 x 8 output tile
   double d0 = 0.0, d1 = 0.0;
   for (int k0 = 0; k0 < n; k0 += kKChunk) {
     __syncthreads();
-    for (int e = tid; e < kKChunk * kTile; e += blockDim.x) {
-      const int k = e / kTile, c = e - k * kTile;
+    for (int e = tid; e < kKChunk * TILE; e += blockDim.x) {
+      const int k = e / TILE, c = e - k * TILE;
       const int i = k0 + k;
       double lv = 0.0, xv = 0.0;
       if (i < n) {
-        if (c < t) lv = Bm[(int64_t)i * t + c];
+        if (c < t) lv = Bm[(int64_t)i * tld + c];
         else if (c == t) lv = tact[i];
         else if (c == t + 1) lv = 1.0;
         const double* xr = X + (int64_t)i * w;
         if (c == 0) xv = xr[0];
         else if (c <= t) xv = xr[c];
-        else if (c == t + 1) xv = 1.0 - xr[w - 1];
+        else if (c == t + 1) xv = 1.0 - xr[t + 1];
         else if (c == t + 2) xv = 1.0;
         else if (c == t + 3) xv = f[i];
       }
@@ -240,8 +247,9 @@ __global__ void __launch_bounds__(128) dense_contrib_kernel(int n, int t, const 
     Ps[r][c + 1] = d1;
   }
   __syncthreads();
-  double* blk = blocks + cell * (int64_t)t1 * t1;
-  double* ld = loads + cell * (int64_t)t1;
+  const int t1 = t + 1;
+  double* blk = blocks + block_off[cell];
+  double* ld = loads + load_off[cell];
   for (int e = tid; e < t1 * t1; e += blockDim.x) {
     const int a = e / t1, b = e - a * t1;
     double v;
@@ -254,21 +262,28 @@ __global__ void __launch_bounds__(128) dense_contrib_kernel(int n, int t, const 
   for (int a = tid; a < t1; a += blockDim.x) ld[a] = (a < t) ? Ps[a][0] : Ps[t][0] - Ps[t + 1][t + 3];
 }
 
-// u = R f - (R B) lambda_K + E c_K, thread per (cell, node).
-__global__ void dense_reconstruct_kernel(int64_t cells, int n, int t, const double* __restrict__ solution,
-                                         const int64_t* __restrict__ cell_dofs, int64_t trace_size,
-                                         const double* __restrict__ x, double* __restrict__ fields) {
-  const int64_t total = cells * (int64_t)n;
+// u = R f - (R B) lambda_K + E c_K, thread per (cell, node i < tile of rows); fields of
+// cell k at fields + field_off[k], its trace DOFs at cell_dofs + dof_off[k], its coarse
+// unknown x[trace_size + cell_id[k]].
+__global__ void dense_reconstruct_kernel(int64_t cells, int nb, int w, const int32_t* __restrict__ n_of,
+                                         const int32_t* __restrict__ t_of, const double* __restrict__ solution,
+                                         const int64_t* __restrict__ cell_dofs, const int64_t* __restrict__ dof_off,
+                                         const int32_t* __restrict__ cell_id, int64_t trace_size,
+                                         const double* __restrict__ x, const int64_t* __restrict__ field_off,
+                                         double* __restrict__ fields) {
+  const int64_t total = cells * (int64_t)nb;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const int w = t + 2;
   for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < total; id += stride) {
-    const int64_t cell = id / n;
-    const int i = (int)(id - cell * n);
-    const double* xr = solution + (cell * (n + 1) + i) * w;
+    const int64_t cell = id / nb;
+    const int i = (int)(id - cell * nb);
+    const int n = n_of[cell], t = t_of[cell];
+    if (i >= n) continue;
+    const double* xr = solution + (cell * nb + i) * w;
+    const int64_t* dofs = cell_dofs + dof_off[cell];
     double u = xr[0];
-    for (int b = 0; b < t; ++b) u = fma(-xr[1 + b], x[cell_dofs[cell * t + b]], u);
-    u = fma(1.0 - xr[w - 1], x[trace_size + cell], u);
-    fields[id] = u;
+    for (int b = 0; b < t; ++b) u = fma(-xr[1 + b], x[dofs[b]], u);
+    u = fma(1.0 - xr[t + 1], x[trace_size + cell_id[cell]], u);
+    fields[field_off[cell] + i] = u;
   }
 }
 
@@ -296,34 +311,46 @@ extern "C" int mhm_tet_kappa(int64_t cells, const double* macro_vertices, int32_
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
 
-extern "C" int mhm_dense_systems(int64_t count, int32_t n, int32_t t, const double* stiffness, const double* mass,
-                                 const double* load, const double* coupling, double* aug, double* rhs,
-                                 double* action, uint8_t* corrected, int32_t* status, void* stream) {
-  if (count < 1 || count > INT32_MAX || n < 1 || t < 1 || t > kTile - 4 || !stiffness || !mass || !load ||
-      !coupling || !aug || !rhs || !action || !corrected || !status)
+extern "C" int mhm_dense_systems(int64_t count, int32_t lds, int32_t tld, int32_t nb, int32_t w,
+                                 int32_t normalize, const int32_t* n_of, const int32_t* t_of, const double* stiffness,
+                                 const double* mass, const double* load, const double* coupling, double* aug,
+                                 double* rhs, double* action, uint8_t* corrected, int32_t* status, void* stream) {
+  if (count < 1 || count > INT32_MAX || lds < 1 || tld < 1 || nb < 2 || nb > lds + 64 || w < 3 || !n_of ||
+      !t_of || !stiffness || !mass || !load || !coupling || !aug || !rhs || !action || !corrected || !status)
     return MHM_ERR_ARGUMENT;
   dense_system_kernel<<<(unsigned)count, kDThreads, 0, static_cast<cudaStream_t>(stream)>>>(
-      n, t, stiffness, mass, load, coupling, aug, rhs, action, corrected, status);
+      lds, tld, nb, w, normalize, n_of, t_of, stiffness, mass, load, coupling, aug, rhs, action, corrected,
+      status);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
 
-extern "C" int mhm_dense_contributions(int64_t count, int32_t n, int32_t t, const double* solution,
-                                       const double* coupling, const double* action, const double* load,
+extern "C" int mhm_dense_contributions(int64_t count, int32_t lds, int32_t tld, int32_t nb, int32_t w,
+                                       int32_t max_t, const int32_t* n_of, const int32_t* t_of,
+                                       const double* solution, const double* coupling, const double* action,
+                                       const double* load, const int64_t* block_off, const int64_t* load_off,
                                        double* blocks, double* loads, void* stream) {
-  if (count < 1 || count > INT32_MAX || n < 1 || t < 1 || t > kTile - 4 || !solution || !coupling || !action ||
-      !load || !blocks || !loads)
+  if (count < 1 || count > INT32_MAX || lds < 1 || tld < 1 || nb < 2 || w < 3 || max_t < 1 || max_t > 28 ||
+      !n_of || !t_of || !solution || !coupling || !action || !load || !block_off || !load_off || !blocks ||
+      !loads)
     return MHM_ERR_ARGUMENT;
-  dense_contrib_kernel<<<(unsigned)count, 128, 0, static_cast<cudaStream_t>(stream)>>>(
-      n, t, solution, coupling, action, load, blocks, loads);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (max_t + 4 <= 16)
+    dense_contrib_kernel<16><<<(unsigned)count, 128, 0, st>>>(lds, tld, nb, w, n_of, t_of, solution, coupling,
+                                                               action, load, block_off, load_off, blocks, loads);
+  else
+    dense_contrib_kernel<32><<<(unsigned)count, 512, 0, st>>>(lds, tld, nb, w, n_of, t_of, solution, coupling,
+                                                               action, load, block_off, load_off, blocks, loads);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
 
-extern "C" int mhm_dense_reconstruct(int64_t count, int32_t n, int32_t t, const double* solution,
-                                     const int64_t* cell_dofs, int64_t trace_size, const double* x, double* fields,
-                                     void* stream) {
-  if (count < 1 || n < 1 || t < 1 || trace_size < 1 || !solution || !cell_dofs || !x || !fields)
+extern "C" int mhm_dense_reconstruct(int64_t count, int32_t nb, int32_t w, const int32_t* n_of,
+                                     const int32_t* t_of, const double* solution, const int64_t* cell_dofs,
+                                     const int64_t* dof_off, const int32_t* cell_id, int64_t trace_size,
+                                     const double* x, const int64_t* field_off, double* fields, void* stream) {
+  if (count < 1 || nb < 2 || w < 3 || trace_size < 1 || !n_of || !t_of || !solution || !cell_dofs || !dof_off ||
+      !cell_id || !x || !field_off || !fields)
     return MHM_ERR_ARGUMENT;
-  dense_reconstruct_kernel<<<grid_for(count * n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      count, n, t, solution, cell_dofs, trace_size, x, fields);
+  dense_reconstruct_kernel<<<grid_for(count * nb), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      count, nb, w, n_of, t_of, solution, cell_dofs, dof_off, cell_id, trace_size, x, field_off, fields);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }

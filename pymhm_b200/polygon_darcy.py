@@ -1,0 +1,409 @@
+"""Primal P2 Darcy on polygonal macro meshes (config 3), on the GPU.
+
+GPU counterpart of ``solve_darcy`` (PyMHM 1.3.2, ``src/pymhm/_legacy/models/darcy/
+primal.py:173-344``) for degree-two local spaces on every macrocell's own refinement
+(``PolygonMesh.submesh``, uneven sizes), one ``FaceSpace`` per polygon edge, homogeneous
+Dirichlet data, a constant source and a constant or disc-inclusion permeability.
+
+Local problems differ in size, so cells are binned by their augmented size rounded up
+to ``bin_width``: each bin is one launch of the dense kernels with uniform strides, the
+cells padded with an identity block (their solution is zero there).  One solve:
+
+1. ``mhm_p2_assemble``: P2 element operators and the dense rows of every cell;
+2. per bin: ``mhm_dense_systems`` (local contract, constraint M 1 / 1^T M 1 as the 2D
+   driver normalises it), ``mhm_batched_factor`` / ``mhm_batched_solve`` (checked
+   equilibrated LU), ``mhm_dense_contributions`` (tensor-core products);
+3. ``mhm_skeleton_scatter`` (ordered, ragged blocks) and ``mhm_general_solve``;
+4. per bin: ``mhm_dense_reconstruct``.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .errors import LinearSolveError
+from .general import GeneralSkeleton
+from .polygon import EdgeSkeleton, PolygonMesh, p2_nodal_space, p2_trace_coupling
+from .topology import block_offsets, skeleton_pattern_ragged, transpose_slots
+from .workloads import DiscInclusions
+
+MAX_AUGMENTED = 640  # the batched LU's blocked shared-memory panel
+
+
+def triangle_rule(order: int):
+    """``triangle_quadrature`` (``fem/scalar/operators.py:63-69``): Duffy-product Gauss
+    points (barycentric) and weights summing to one."""
+    t, w = np.polynomial.legendre.leggauss(order)
+    t, w = (t + 1) / 2, w / 2
+    bary = np.array([(1 - a - (1 - a) * b, a, (1 - a) * b) for a in t for b in t])
+    weights = np.array([2 * wa * wb * (1 - a) for a, wa in zip(t, w) for wb in w])
+    return bary, weights
+
+
+def disc_grid(field: DiscInclusions, grid: int = 64):
+    """Cell lists of the discs over a grid x grid partition of the unit square: every
+    disc is listed in each cell its bounding box meets."""
+    lists = [[] for _ in range(grid * grid)]
+    for d, ((cx, cy), r) in enumerate(zip(field.centres, field.radii)):
+        x0, x1 = np.clip([(cx - r) * grid, (cx + r) * grid], 0, grid - 1).astype(int)
+        y0, y1 = np.clip([(cy - r) * grid, (cy + r) * grid], 0, grid - 1).astype(int)
+        for gx in range(x0, x1 + 1):
+            for gy in range(y0, y1 + 1):
+                lists[gx * grid + gy].append(d)
+    ptr = np.r_[0, np.cumsum([len(l) for l in lists])].astype(np.int32)
+    flat = np.array([d for l in lists for d in l], dtype=np.int32)
+    return ptr, flat if len(flat) else np.zeros(1, np.int32)
+
+
+def refinement_for_sizes(mesh: PolygonMesh, lo: int = 200, hi: int = MAX_AUGMENTED - 1, seed: int = 0):
+    """Per-cell subdivision counts with P2 sizes drawn uniformly in [lo, hi]: for a
+    target size, the largest count whose local space stays within it (at least 1)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = np.empty(len(mesh.cells), dtype=np.int64)
+    for c in range(len(mesh.cells)):
+        _, base = mesh.base_triangles(c)
+        m = len(base)
+        target = rng.uniform(lo, hi)
+        r = 1
+        while True:  # P2 nodes of m refined base triangles sharing their edges: grows like 2 m r^2
+            n_next = len(p2_nodal_space(mesh.submesh(c, r + 1))[1]) if m * (r + 1) ** 2 * 2 < 2 * hi else hi + 1
+            if n_next > target or n_next > hi:
+                break
+            r += 1
+        out[c] = r
+    return out
+
+
+@dataclass
+class PolygonSolution:
+    trace: np.ndarray
+    coarse: np.ndarray
+    fields: list  # per cell, its P2 nodal values
+    residual: float
+    corrected: np.ndarray
+    global_iterations: int
+    outer_corrections: int
+    seconds: float = 0.0
+
+
+class PolygonP2Plan:
+    """Device-resident plan of one polygonal problem shape (mesh, skeleton, per-cell
+    refinement): local meshes, couplings, bins, sparsity and every buffer."""
+
+    def __init__(self, mesh: PolygonMesh, skeleton: EdgeSkeleton | None = None, refinements=2, *, order=4,
+                 bin_width=32, device=None, global_rtol=1e-13, inner_rtol=1e-10, max_inner=20000, max_outer=8):
+        import torch
+
+        self.torch = torch
+        self.lib = _lib.lib()
+        self.device = torch.device("cuda" if device is None else device)
+        self.mesh = mesh
+        self.skeleton = EdgeSkeleton(mesh) if skeleton is None else skeleton
+        self.global_rtol, self.inner_rtol = float(global_rtol), float(inner_rtol)
+        self.max_inner, self.max_outer = int(max_inner), int(max_outer)
+        M = len(mesh.cells)
+        self.M = M
+        rs = np.broadcast_to(np.asarray(refinements, dtype=np.int64), (M,))
+        sk = self.skeleton
+        self.T, self.N = sk.size, sk.size + M
+        fines = [mesh.submesh(c, int(rs[c])) for c in range(M)]
+        spaces = [p2_nodal_space(f) for f in fines]
+        self.n_cells = np.array([len(nodes) for _, nodes in spaces], dtype=np.int64)
+        cell_dofs = [sk.cell_dofs(c) for c in range(M)]
+        self.t_cells = np.array([len(d) for d in cell_dofs], dtype=np.int64)
+        if self.n_cells.max() + 1 > MAX_AUGMENTED:
+            raise NotImplementedError(f"local P2 spaces up to {MAX_AUGMENTED - 1} unknowns on this path")
+        if self.t_cells.max() > 28:
+            raise NotImplementedError("at most 28 trace DOFs per cell")
+        couplings = [p2_trace_coupling(mesh, c, fines[c], sk) for c in range(M)]
+        # ---- bins by padded augmented size -------------------------------------------
+        nb_c = ((self.n_cells + 1 + bin_width - 1) // bin_width) * bin_width
+        nb_c = np.minimum(nb_c, MAX_AUGMENTED)
+        order_cells = np.argsort(nb_c, kind="stable")
+        self.order = order_cells
+        self.bins = []
+        dense_base = rhs_base = cpl_base = load_base = act_base = vec_base = 0
+        pos = 0
+        for nb in np.unique(nb_c):
+            members = order_cells[nb_c[order_cells] == nb]
+            k = len(members)
+            tld = int(self.t_cells[members].max())
+            w = tld + 2
+            self.bins.append(dict(nb=int(nb), tld=tld, w=w, k=k, cells=members, pos=pos, dense=dense_base,
+                                  rhs=rhs_base, cpl=cpl_base, load=load_base, act=act_base, vec=vec_base))
+            dense_base += k * nb * nb
+            rhs_base += k * nb * w
+            cpl_base += k * nb * tld
+            load_base += k * nb
+            act_base += k * 3 * nb
+            vec_base += k * nb
+            pos += k
+        # ---- flattened elements and node incidences (cells in bin order) -------------
+        pts, tris, edofs, node_cell, node_row, inc_ptr, incs = [], [], [], [], [], [0], []
+        dense_off = np.empty(M, dtype=np.int64)
+        load_off = np.empty(M, dtype=np.int64)
+        ld_of = np.empty(M, dtype=np.int32)
+        p_base = e_base = 0
+        for b in self.bins:
+            for j, c in enumerate(b["cells"]):
+                fine = fines[c]
+                dofs, _ = spaces[c]
+                slot = b["pos"] + j
+                dense_off[slot] = b["dense"] + j * b["nb"] * b["nb"]
+                load_off[slot] = b["load"] + j * b["nb"]
+                ld_of[slot] = b["nb"]
+                pts.append(fine.points)
+                tris.append(fine.cells + p_base)
+                edofs.append(dofs.astype(np.int32))
+                n = int(self.n_cells[c])
+                flat = dofs.ravel()
+                code = (e_base + np.arange(len(dofs)))[:, None] * 6 + np.arange(6)[None, :]
+                srt = np.lexsort((code.ravel(), flat))
+                counts = np.bincount(flat, minlength=n)
+                incs.append(code.ravel()[srt])
+                inc_ptr.extend((inc_ptr[-1] + np.cumsum(counts)).tolist())
+                node_cell.append(np.full(n, slot, dtype=np.int32))
+                node_row.append(np.arange(n, dtype=np.int32))
+                p_base += len(fine.points)
+                e_base += len(dofs)
+        self.elements, self.nodes = e_base, int(sum(self.n_cells))
+        # ---- skeleton reduction and global solve -------------------------------------
+        self.cell_dofs_list = cell_dofs
+        self.pattern = skeleton_pattern_ragged(cell_dofs, self.T)
+        bofs, lofs = block_offsets(cell_dofs)
+        flat_dofs = np.concatenate(cell_dofs)
+        dofs_off = np.r_[0, np.cumsum(self.t_cells)][:-1]
+        field_off = np.r_[0, np.cumsum(self.n_cells)][:-1]
+        self.field_off_h = np.r_[field_off, self.nodes]
+        self.general = GeneralSkeleton(cell_dofs, [sk.geometric_constraint(c) for c in range(M)], sk.offsets,
+                                       self.T, self.pattern.indptr, self.pattern.indices, device=self.device)
+        qbary, qw = triangle_rule(max(int(order), 4))
+        dev = self.device
+        f64 = dict(dtype=torch.float64, device=dev)
+
+        def up(a, dtype):
+            return torch.as_tensor(np.array(a, order="C", copy=True), dtype=dtype).to(dev)
+
+        # per bin-order slot: sizes and output offsets
+        o = self.order
+        self.d = dict(
+            points=up(np.concatenate(pts), torch.float64), tris=up(np.concatenate(tris), torch.int64),
+            edofs=up(np.concatenate(edofs), torch.int32), node_cell=up(np.concatenate(node_cell), torch.int32),
+            node_row=up(np.concatenate(node_row), torch.int32), inc_ptr=up(np.asarray(inc_ptr), torch.int64),
+            inc=up(np.concatenate(incs), torch.int64), dense_off=up(dense_off, torch.int64),
+            ld_of=up(ld_of, torch.int32), load_off=up(load_off, torch.int64),
+            qbary=up(qbary, torch.float64), qw=up(qw, torch.float64),
+            n_of=up(self.n_cells[o], torch.int32), t_of=up(self.t_cells[o], torch.int32),
+            block_off=up(bofs[:-1][o], torch.int64), lofs=up(lofs[:-1][o], torch.int64),
+            dof_off=up(dofs_off[o], torch.int64), cell_id=up(o, torch.int32), field_off=up(field_off[o], torch.int64),
+            flat_dofs=up(flat_dofs, torch.int64),
+            slot_ptr=up(self.pattern.slot_ptr, torch.int64), contrib=up(self.pattern.contrib, torch.int64),
+            load_ptr=up(self.pattern.load_ptr, torch.int64), load_contrib=up(self.pattern.load_contrib, torch.int64),
+            indptr=up(self.pattern.indptr, torch.int64), indices=up(self.pattern.indices, torch.int32))
+        cpl = np.zeros(cpl_base)
+        for b in self.bins:
+            for j, c in enumerate(b["cells"]):
+                base = b["cpl"] + j * b["nb"] * b["tld"]
+                B = couplings[c]
+                view = cpl[base: base + b["nb"] * b["tld"]].reshape(b["nb"], b["tld"])
+                view[: B.shape[0], : B.shape[1]] = B
+        self.d["coupling"] = up(cpl, torch.float64)
+        self.elem = torch.empty(int(self.lib.mhm_p2_element_bytes(self.elements)) // 8, **f64)
+        self.stiffness = torch.empty(dense_base, **f64)
+        self.mass = torch.empty(dense_base, **f64)
+        self.load = torch.empty(load_base, **f64)
+        self.aug = torch.empty(dense_base, **f64)
+        self.factors = torch.empty(dense_base, **f64)
+        self.rhs = torch.empty(rhs_base, **f64)
+        self.solution = torch.empty(rhs_base, **f64)
+        self.work = torch.empty(rhs_base, **f64)
+        self.action = torch.empty(act_base, **f64)
+        self.pivots = torch.empty(vec_base, dtype=torch.int32, device=dev)
+        self.row_scale = torch.empty(vec_base, **f64)
+        self.col_scale = torch.empty(vec_base, **f64)
+        self.corrected = torch.empty(M, dtype=torch.uint8, device=dev)
+        self.cell_status = torch.empty(M, dtype=torch.int32, device=dev)
+        self.factor_status = torch.empty(M, dtype=torch.int32, device=dev)
+        self.solve_status = torch.empty(M, dtype=torch.int32, device=dev)
+        self.blocks = torch.empty(int(bofs[-1]), **f64)
+        self.loads = torch.empty(int(lofs[-1]), **f64)
+        self.values = torch.empty(len(self.pattern.indices), **f64)
+        self.grhs = torch.empty(self.N, **f64)
+        self.load_scale = torch.empty(self.N, **f64)
+        self.d_boundary = torch.zeros(self.T, **f64)
+        self.x = torch.empty(self.N, **f64)
+        self.fields = torch.empty(self.nodes, **f64)
+        self.field = None
+        self.source = 0.0
+
+    def set_coefficients(self, permeability=1.0, source=0.0):
+        """A ``DiscInclusions`` field or a positive constant permeability; a constant source."""
+        torch = self.torch
+        if isinstance(permeability, DiscInclusions):
+            ptr, flat = disc_grid(permeability)
+            self.field = dict(grid=int(np.sqrt(len(ptr) - 1)), ptr=torch.as_tensor(ptr).to(self.device),
+                              flat=torch.as_tensor(flat).to(self.device),
+                              centres=torch.as_tensor(np.ascontiguousarray(permeability.centres)).to(self.device),
+                              r2=torch.as_tensor(np.ascontiguousarray(permeability.r2)).to(self.device),
+                              inside=permeability.inside, outside=permeability.outside)
+        elif np.ndim(permeability) == 0 and float(permeability) > 0:
+            self.field = dict(grid=0, ptr=None, flat=None, centres=None, r2=None, inside=float(permeability),
+                              outside=float(permeability))
+        else:
+            raise NotImplementedError("permeability: DiscInclusions or a positive constant")
+        if np.ndim(source) != 0 or not np.isfinite(float(source)):
+            raise NotImplementedError("the GPU polygon path takes a constant source")
+        self.source = float(source)
+
+    def _bin_views(self, b):
+        """Sub-tensors of one bin (contiguous slices of the flat buffers)."""
+        k, nb, w, tld = b["k"], b["nb"], b["w"], b["tld"]
+        s = slice(b["pos"], b["pos"] + k)
+        d = self.d
+        return dict(
+            stiffness=self.stiffness[b["dense"]: b["dense"] + k * nb * nb],
+            mass=self.mass[b["dense"]: b["dense"] + k * nb * nb],
+            aug=self.aug[b["dense"]: b["dense"] + k * nb * nb],
+            factors=self.factors[b["dense"]: b["dense"] + k * nb * nb],
+            load=self.load[b["load"]: b["load"] + k * nb],
+            coupling=d["coupling"][b["cpl"]: b["cpl"] + k * nb * tld],
+            rhs=self.rhs[b["rhs"]: b["rhs"] + k * nb * w], solution=self.solution[b["rhs"]: b["rhs"] + k * nb * w],
+            work=self.work[b["rhs"]: b["rhs"] + k * nb * w], action=self.action[b["act"]: b["act"] + k * 3 * nb],
+            pivots=self.pivots[b["vec"]: b["vec"] + k * nb], rs=self.row_scale[b["vec"]: b["vec"] + k * nb],
+            cs=self.col_scale[b["vec"]: b["vec"] + k * nb], n_of=d["n_of"][s], t_of=d["t_of"][s],
+            block_off=d["block_off"][s], lofs=d["lofs"][s], dof_off=d["dof_off"][s], cell_id=d["cell_id"][s],
+            field_off=d["field_off"][s], corrected=self.corrected[s], cell_status=self.cell_status[s],
+            factor_status=self.factor_status[s], solve_status=self.solve_status[s])
+
+    def launch(self, stream=None, *, events=None):
+        """Enqueue one complete solve on ``stream`` (no host synchronisation).  ``events``:
+        five CUDA events around the local stage, reduction, global solve and reconstruction."""
+        torch = self.torch
+        P, lib, sh = _lib.ptr, self.lib, _lib.stream_handle(stream)
+        st = torch.cuda.current_stream() if stream is None else stream
+        d, fld = self.d, self.field
+
+        def mark(k):
+            if events is not None:
+                events[k].record(st)
+
+        mark(0)
+        _lib.check(lib.mhm_p2_assemble(self.elements, P(d["points"]), P(d["tris"]), len(d["qw"]), P(d["qbary"]),
+                                       P(d["qw"]), fld["grid"], P(fld["ptr"]), P(fld["flat"]), P(fld["centres"]),
+                                       P(fld["r2"]), fld["inside"], fld["outside"], self.source, P(self.elem),
+                                       self.nodes, P(d["node_cell"]), P(d["node_row"]), P(d["inc_ptr"]), P(d["inc"]),
+                                       P(d["edofs"]), P(d["dense_off"]), P(d["ld_of"]), P(d["load_off"]),
+                                       P(self.stiffness), P(self.mass), P(self.load), sh), "mhm_p2_assemble")
+        for b in self.bins:
+            v = self._bin_views(b)
+            k, nb, w, tld = b["k"], b["nb"], b["w"], b["tld"]
+            _lib.check(lib.mhm_dense_systems(k, nb, tld, nb, w, 1, P(v["n_of"]), P(v["t_of"]), P(v["stiffness"]),
+                                             P(v["mass"]), P(v["load"]), P(v["coupling"]), P(v["aug"]), P(v["rhs"]),
+                                             P(v["action"]), P(v["corrected"]), P(v["cell_status"]), sh),
+                       "mhm_dense_systems")
+            _lib.check(lib.mhm_batched_factor(k, nb, P(v["aug"]), P(v["factors"]), P(v["pivots"]), P(v["rs"]),
+                                              P(v["cs"]), P(v["factor_status"]), sh), "mhm_batched_factor")
+            with torch.cuda.stream(st):
+                v["solve_status"].copy_(v["factor_status"])
+            _lib.check(lib.mhm_batched_solve(k, nb, w, P(v["aug"]), P(v["factors"]), P(v["pivots"]), P(v["rs"]),
+                                             P(v["cs"]), P(v["rhs"]), P(v["solution"]), P(v["work"]), 1e-10, 0.0,
+                                             2, P(v["solve_status"]), sh), "mhm_batched_solve")
+            _lib.check(lib.mhm_dense_contributions(k, nb, tld, nb, w, tld, P(v["n_of"]), P(v["t_of"]),
+                                                   P(v["solution"]), P(v["coupling"]), P(v["action"]),
+                                                   P(v["load"]), P(v["block_off"]), P(v["lofs"]), P(self.blocks),
+                                                   P(self.loads), sh), "mhm_dense_contributions")
+        mark(1)
+        p = self.pattern
+        _lib.check(lib.mhm_skeleton_scatter(len(p.indices), P(d["slot_ptr"]), P(d["contrib"]), P(self.blocks),
+                                            P(self.values), self.N, self.T, P(d["load_ptr"]), P(d["load_contrib"]),
+                                            P(self.loads), P(self.d_boundary), P(self.grhs), P(self.load_scale), sh),
+                   "mhm_skeleton_scatter")
+        mark(2)
+        self.general.launch(self.values, self.grhs, self.x, rtol=self.global_rtol, inner_rtol=self.inner_rtol,
+                            max_inner=self.max_inner, max_outer=self.max_outer, stream=stream)
+        mark(3)
+        for b in self.bins:
+            v = self._bin_views(b)
+            _lib.check(lib.mhm_dense_reconstruct(b["k"], b["nb"], b["w"], P(v["n_of"]), P(v["t_of"]),
+                                                 P(v["solution"]), P(d["flat_dofs"]), P(v["dof_off"]),
+                                                 P(v["cell_id"]), self.T, P(self.x), P(v["field_off"]),
+                                                 P(self.fields), sh), "mhm_dense_reconstruct")
+        mark(4)
+
+    def check(self):
+        """Raise the reference's error for any failed stage (synchronises)."""
+        for arr in (self.cell_status, self.solve_status):
+            stv = arr.cpu().numpy()
+            bad = np.flatnonzero(stv)
+            if len(bad):
+                raise LinearSolveError(f"{_lib.CELL_MESSAGES.get(int(stv[bad[0]]), 'cell failed')} "
+                                       f"(macrocell {int(self.order[bad[0]])})")
+        return self.general.check()
+
+    def result(self, seconds=0.0) -> PolygonSolution:
+        info, stats = self.check()
+        x = self.x.cpu().numpy()
+        f = self.fields.cpu().numpy()
+        fields = [f[self.field_off_h[c]: self.field_off_h[c + 1]] for c in range(self.M)]
+        corrected = np.empty(self.M, dtype=bool)
+        corrected[self.order] = self.corrected.cpu().numpy().astype(bool)
+        return PolygonSolution(trace=x[: self.T].copy(), coarse=x[self.T:].copy(), fields=fields,
+                               residual=float(stats[0]), corrected=corrected, global_iterations=int(info[1]),
+                               outer_corrections=int(info[2]), seconds=seconds)
+
+    def solve(self, permeability=1.0, source=0.0, stream=None) -> PolygonSolution:
+        t0 = time.perf_counter()
+        self.set_coefficients(permeability, source)
+        self.launch(stream)
+        sol = self.result()
+        sol.seconds = time.perf_counter() - t0
+        return sol
+
+    def cell_block(self, cell: int) -> np.ndarray:
+        """The oriented Schur block of a cell (global cell id), for checks."""
+        bofs, _ = block_offsets(self.cell_dofs_list)
+        t1 = int(self.t_cells[cell]) + 1
+        return self.blocks[int(bofs[cell]): int(bofs[cell]) + t1 * t1].cpu().numpy().reshape(t1, t1)
+
+    def matrix(self):
+        """Host copy of the assembled skeleton matrix in the reference's CSC form, exact
+        zeros dropped (``core/contributions.py:184-185``)."""
+        from scipy import sparse
+
+        torch = self.torch
+        p = self.pattern
+        if getattr(self, "_csc", None) is None:
+            self._csc = dict(transpose=torch.as_tensor(transpose_slots(p.indptr, p.indices)).to(self.device),
+                             indptr=torch.empty(self.N + 1, dtype=torch.int64, device=self.device),
+                             indices=torch.empty(len(p.indices), dtype=torch.int32, device=self.device),
+                             data=torch.empty(len(p.indices), dtype=torch.float64, device=self.device))
+        c = self._csc
+        P = _lib.ptr
+        _lib.check(self.lib.mhm_skeleton_export_csc(self.N, P(self.d["indptr"]), P(self.d["indices"]),
+                                                    P(c["transpose"]), P(self.values), P(c["indptr"]),
+                                                    P(c["indices"]), P(c["data"]), _lib.stream_handle(None)),
+                   "mhm_skeleton_export_csc")
+        kept = int(c["indptr"][-1])
+        return sparse.csc_matrix((c["data"][:kept].cpu().numpy(), c["indices"][:kept].cpu().numpy(),
+                                  c["indptr"].cpu().numpy()), shape=(self.N, self.N))
+
+
+def solve_darcy(mesh: PolygonMesh, *, permeability=1.0, source=0.0, dirichlet=0.0, neumann=None,
+                skeleton: EdgeSkeleton | None = None, local_refinement=4, local_meshes=None, quadrature_order=4,
+                formulation="primal", degree=1, **_ignored) -> PolygonSolution:
+    """GPU counterpart of ``solve_darcy`` (``primal.py:173-344``) on a ``PolygonMesh`` for
+    ``degree=2``, homogeneous Dirichlet data, a constant source and a constant or
+    ``DiscInclusions`` permeability.  ``local_refinement`` may be one count or one per
+    cell (the uneven local sizes of a polygon batch)."""
+    if int(degree) != 2 or formulation != "primal":
+        raise NotImplementedError("the GPU polygon path implements the primal degree-two formulation")
+    if local_meshes is not None or neumann:
+        raise NotImplementedError("explicit local meshes and Neumann data are not on the GPU polygon path")
+    if np.ndim(dirichlet) != 0 or float(dirichlet) != 0.0:
+        raise NotImplementedError("the GPU polygon path takes homogeneous Dirichlet data")
+    plan = PolygonP2Plan(mesh, skeleton, local_refinement, order=max(int(quadrature_order), 4))
+    return plan.solve(permeability, source)

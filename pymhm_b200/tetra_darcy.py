@@ -114,7 +114,13 @@ class TetraP1Plan:
         self.p1_status = torch.zeros(4, dtype=torch.int32, device=dev)
         self.aug = torch.empty((M, n1, n1), **f64)
         self.rhs = torch.empty((M, n1, w), **f64)
-        self.action = torch.empty((M, 2, n), **f64)
+        self.action = torch.empty((M, 3, n1), **f64)
+        self.n_of = torch.full((M,), n, dtype=torch.int32, device=dev)
+        self.t_of = torch.full((M,), t, dtype=torch.int32, device=dev)
+        cells = torch.arange(M, dtype=torch.int64, device=dev)
+        self.block_off, self.load_off = cells * (t + 1) * (t + 1), cells * (t + 1)
+        self.dof_off, self.field_off = cells * t, cells * n
+        self.cell_id = cells.to(torch.int32)
         self.corrected = torch.empty(M, dtype=torch.uint8, device=dev)
         self.cell_status = torch.empty(M, dtype=torch.int32, device=dev)
         self.factors = torch.empty_like(self.aug)
@@ -176,10 +182,11 @@ class TetraP1Plan:
                                              P(self.source), 0, 0, P(self.d_node_ptr), P(self.d_node_contrib),
                                              P(self.scratch), P(self.stiffness), P(self.mass), P(self.load),
                                              P(self.p1_status), sh), "mhm_p1_batch_assemble")
-        _lib.check(lib.mhm_dense_systems(M, n, t, P(self.stiffness), P(self.mass), P(self.load), P(self.d_coupling),
-                                         P(self.aug), P(self.rhs), P(self.action), P(self.corrected),
-                                         P(self.cell_status), sh), "mhm_dense_systems")
         n1, w = n + 1, t + 2
+        _lib.check(lib.mhm_dense_systems(M, n, t, n1, w, 0, P(self.n_of), P(self.t_of), P(self.stiffness),
+                                         P(self.mass), P(self.load), P(self.d_coupling), P(self.aug), P(self.rhs),
+                                         P(self.action), P(self.corrected), P(self.cell_status), sh),
+                   "mhm_dense_systems")
         _lib.check(lib.mhm_batched_factor(M, n1, P(self.aug), P(self.factors), P(self.pivots), P(self.row_scale),
                                           P(self.col_scale), P(self.factor_status), sh), "mhm_batched_factor")
         with self.torch.cuda.stream(st):
@@ -187,8 +194,9 @@ class TetraP1Plan:
         _lib.check(lib.mhm_batched_solve(M, n1, w, P(self.aug), P(self.factors), P(self.pivots), P(self.row_scale),
                                          P(self.col_scale), P(self.rhs), P(self.solution), P(self.work), 1e-10, 0.0,
                                          2, P(self.solve_status), sh), "mhm_batched_solve")
-        _lib.check(lib.mhm_dense_contributions(M, n, t, P(self.solution), P(self.d_coupling), P(self.action),
-                                               P(self.load), P(self.blocks), P(self.loads), sh),
+        _lib.check(lib.mhm_dense_contributions(M, n, t, n1, w, t, P(self.n_of), P(self.t_of), P(self.solution),
+                                               P(self.d_coupling), P(self.action), P(self.load), P(self.block_off),
+                                               P(self.load_off), P(self.blocks), P(self.loads), sh),
                    "mhm_dense_contributions")
         p = self.pattern
         mark(1)
@@ -200,8 +208,9 @@ class TetraP1Plan:
         self.general.launch(self.values, self.grhs, self.x, rtol=self.global_rtol, inner_rtol=self.inner_rtol,
                             max_inner=self.max_inner, max_outer=self.max_outer, stream=stream)
         mark(3)
-        _lib.check(lib.mhm_dense_reconstruct(M, n, t, P(self.solution), P(self.d_cell_dofs), self.T, P(self.x),
-                                             P(self.fields), sh), "mhm_dense_reconstruct")
+        _lib.check(lib.mhm_dense_reconstruct(M, n1, w, P(self.n_of), P(self.t_of), P(self.solution),
+                                             P(self.d_cell_dofs), P(self.dof_off), P(self.cell_id), self.T, P(self.x),
+                                             P(self.field_off), P(self.fields), sh), "mhm_dense_reconstruct")
         mark(4)
 
     def check(self):

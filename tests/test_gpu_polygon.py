@@ -1,0 +1,70 @@
+"""GPU parity of the polygonal P2 path (config 3) against fixtures written by the
+reference (``make_polygon_golden.py``) and against the oracle on a larger mesh."""
+
+import numpy as np
+import pytest
+
+from tests._cases import rel
+from tests.test_oracle_polygon import POLYGON_CASES, polygon_case
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", POLYGON_CASES)
+def test_polygon_solution_matches_reference(name):
+    from pymhm_b200.polygon_darcy import PolygonP2Plan
+
+    g, mesh, sk, fines, field = polygon_case(name)
+    plan = PolygonP2Plan(mesh, sk, g["refinements"])
+    sol = plan.solve(field, 1.0)
+    assert rel(sol.trace, g["trace"]) <= 1e-10
+    assert rel(sol.coarse, g["coarse"]) <= 1e-10
+    assert rel(np.concatenate(sol.fields), g["fields"]) <= 1e-10
+    assert sol.residual <= 1e-12
+    assert np.array_equal(sol.corrected, g["corrected"])
+    for c in g["keep_cells"]:
+        blk, ref = plan.cell_block(int(c)), g[f"cell{c}_block"]
+        assert np.max(np.abs(blk - ref)) <= 1e-9 * np.max(np.abs(ref))
+    # bitwise reproducible
+    x0 = plan.x.clone()
+    plan.launch()
+    plan.check()
+    assert bool((plan.x == x0).all())
+
+
+@pytest.mark.parametrize("name", POLYGON_CASES)
+def test_polygon_matrix_against_reference(name):
+    from scipy import sparse
+
+    from pymhm_b200.polygon_darcy import PolygonP2Plan
+    from tests._full_size import pattern_differences
+
+    g, mesh, sk, fines, field = polygon_case(name)
+    plan = PolygonP2Plan(mesh, sk, g["refinements"])
+    plan.solve(field, 1.0)
+    A = plan.matrix()
+    N = plan.N
+    ref = sparse.csc_matrix((g["data"], g["indices"], g["indptr"]), shape=(N, N))
+    scale = np.max(np.abs(ref.data))
+    # the coarse-coarse entries are rounding residues of A^T 1 (see test_oracle_polygon)
+    assert np.max(np.abs((A - ref).toarray())) <= 1e-8 * scale
+    r, c, mine, theirs = pattern_differences(A, ref)
+    assert np.all(mine <= 1e-8 * scale) and np.all(theirs <= 1e-8 * scale)
+
+
+def test_polygon_larger_mesh_against_oracle():
+    """200 Voronoi cells, per-cell refinements 1..3, 120 discs: the oracle's solve."""
+    from oracle import polygon_mhm as op
+    from pymhm_b200.polygon import EdgeSkeleton, voronoi_mesh
+    from pymhm_b200.polygon_darcy import PolygonP2Plan
+    from pymhm_b200.workloads import DiscInclusions, disc_inclusions
+
+    mesh = voronoi_mesh(200, 17)
+    sk = EdgeSkeleton(mesh)
+    rs = np.random.default_rng(17).integers(1, 4, size=200)
+    field = DiscInclusions(*disc_inclusions(120, rmin=0.01, rmax=0.03, seed=18))
+    ref = op.solve_darcy_p2(mesh, sk, [mesh.submesh(c, int(rs[c])) for c in range(200)], field, 1.0)
+    sol = PolygonP2Plan(mesh, sk, rs).solve(field, 1.0)
+    assert rel(sol.trace, ref["trace"]) <= 1e-10
+    assert rel(sol.coarse, ref["coarse"]) <= 1e-10
+    assert rel(np.concatenate(sol.fields), np.concatenate(ref["fields"])) <= 1e-10
