@@ -422,6 +422,16 @@ typedef struct mhm_general_system {
     const int32_t* dof_cells;     /* (T, 2): the cells holding each DOF (-1: none)  */
     const int64_t* dof_entry;     /* (T, 2): its index in cell_dofs / cell_g0       */
     const double* coarse_inverse; /* (cells, cells) row-major (G0^T G0)^-1           */
+    int64_t cell_entries;         /* cell_ptr[cells]                                 */
+    /* Optional (cell_blocks NULL: face block-Jacobi preconditioner).  The cells'
+       condensed (t+1) x (t+1) blocks, row-major at block_off[c] (t = the cell's
+       DOF count <= max_cell_dofs <= 32, local order of cell_dofs; the last row and
+       column are the coarse unknown), select the cell-Dirichlet preconditioner.
+       The workspace holds its buffers whenever block_off is set.               */
+    const double* cell_blocks;
+    const int64_t* block_off;     /* (cells)                                         */
+    int64_t blocks_size;          /* doubles spanned by the blocks                   */
+    int32_t max_cell_dofs;
 } mhm_general_system;
 
 /* Workspace bytes of mhm_general_solve on the current device (-1: invalid). */
@@ -429,13 +439,16 @@ int64_t mhm_general_workspace_bytes(const mhm_general_system* s /* host */);
 
 /*
  * x (N) = K^-1 rhs (N): outer FP64 defect correction on K until
- * ||rhs - K x|| <= rtol ||rhs||, each correction by projected CG on
- * [[S, -G0], [-G0^T, 0]] with block-Jacobi preconditioning over the faces
- * (inner tolerance inner_rtol, at most max_inner CG iterations in total and
- * max_outer corrections).  One persistent cooperative launch (one CTA per SM).
+ * ||rhs - K x|| <= rtol ||rhs|| and every row's residual is within rtol of
+ * |rhs_i| + sum_j |K_ij| |x_j| (or that componentwise error stopped improving),
+ * each correction by projected CG on [[S, -G0], [-G0^T, 0]], preconditioned by
+ * face block-Jacobi or, with cell_blocks, by the cells' D S_c^-1 D, until the
+ * preconditioned residual norm fell by inner_rtol (at most max_inner CG
+ * iterations in total and max_outer corrections).  Setup kernels, then one
+ * persistent cooperative launch (one CTA per SM).
  * info (4 int32, device): status (MHM_SOLVE_*), inner iterations, outer
- * corrections, barrier error flag; stats (2 doubles, device): final relative
- * residual, ||rhs||.  Every grid barrier is bounded.
+ * corrections, barrier error flag; stats (3 doubles, device): final relative
+ * residual, ||rhs||, componentwise backward error.  Every grid barrier is bounded.
  */
 int mhm_general_solve(const mhm_general_system* s /* host */, const double* rhs, double* x,
                       void* workspace, int64_t workspace_bytes, double rtol, double inner_rtol,
@@ -447,15 +460,15 @@ int mhm_general_solve(const mhm_general_system* s /* host */, const double* rhs,
 /* ------------------------------------------------------------------------ */
 /*
  * Material pre-pass of tetra_operators (fem/scalar/tetrahedron.py:41-52,
- * 157-190) for a layered voxel permeability: for every macrocell (vertices
- * macro_vertices (cells, 4, 3)) and fine tetrahedron e of its refinement
- * (fine_cells (nfine, 4) into ref_bary (npoints, 4)), the quadrature average
+ * 157-190) for a layered voxel permeability: for every macrocell (its refined
+ * vertices points (cells, npoints, 3), as TetraMesh.submesh computes them) and
+ * fine tetrahedron e (fine_cells (nfine, 4)), the quadrature average
  * sum_q w_q kappa(x_q) over quad_bary / quad_weights (nquad), kappa the voxel
  * value voxels[layer(z)][ix(x)][iy(y)] (layers x px x py over the unit cube).
  * Writes the isotropic tensors diffusion (cells, nfine, 3, 3).
  */
-int mhm_tet_kappa(int64_t cells, const double* macro_vertices, int32_t npoints, const double* ref_bary,
-                  int32_t nfine, const int32_t* fine_cells, int32_t nquad, const double* quad_bary,
+int mhm_tet_kappa(int64_t cells, const double* points, int32_t npoints, int32_t nfine,
+                  const int32_t* fine_cells, int32_t nquad, const double* quad_bary,
                   const double* quad_weights, int32_t layers, int32_t px, int32_t py,
                   const double* voxels, double* diffusion, void* stream);
 

@@ -81,6 +81,8 @@ class GeneralSystem(C.Structure):
         ("faces", C.c_int32), ("max_face_size", C.c_int32), ("face_ptr", C.c_void_p),
         ("cells", C.c_int32), ("cell_ptr", C.c_void_p), ("cell_dofs", C.c_void_p), ("cell_g0", C.c_void_p),
         ("dof_cells", C.c_void_p), ("dof_entry", C.c_void_p), ("coarse_inverse", C.c_void_p),
+        ("cell_entries", C.c_int64), ("cell_blocks", C.c_void_p), ("block_off", C.c_void_p),
+        ("blocks_size", C.c_int64), ("max_cell_dofs", C.c_int32),
     ]
 
 
@@ -112,7 +114,7 @@ _SIGNATURES = {
     "mhm_general_workspace_bytes": (C.c_int64, [C.POINTER(GeneralSystem)]),
     "mhm_general_solve": (C.c_int, [C.POINTER(GeneralSystem), P, P, P, C.c_int64, C.c_double, C.c_double,
                                     C.c_int32, C.c_int32, P, P, P]),
-    "mhm_tet_kappa": (C.c_int, [C.c_int64, P, C.c_int32, P, C.c_int32, P, C.c_int32, P, P, C.c_int32, C.c_int32,
+    "mhm_tet_kappa": (C.c_int, [C.c_int64, P, C.c_int32, C.c_int32, P, C.c_int32, P, P, C.c_int32, C.c_int32,
                                 C.c_int32, P, P, P]),
     "mhm_dense_systems": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, P, P,
                                     P, P, P, P, P, P, P, P]),

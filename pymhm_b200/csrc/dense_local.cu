@@ -23,32 +23,25 @@ namespace {
 // ---------------------------------------------------------------------------------
 // Material pre-pass: for every (macrocell, fine tetrahedron) the Duffy-rule average
 // sum_q w_q kappa(x_q) of a layered voxel field, written as the isotropic tensor the
-// P1 assembly reads.  The fine vertices are bary @ macro vertices (the submesh), each
-// quadrature point ((b0 p0 + b1 p1) + b2 p2) + b3 p3 with separate roundings, which is
-// the order NumPy's einsum uses, so that points on either side of a voxel face select
-// the same voxel as the reference's evaluation.
+// P1 assembly reads.  The fine vertices come from the host, computed as the
+// reference's submesh computes them; each quadrature point is
+// ((b0 p0 + b1 p1) + b2 p2) + b3 p3 with separate roundings, the order NumPy's einsum
+// uses, so that points on either side of a voxel face select the same voxel as the
+// reference's evaluation.
 // ---------------------------------------------------------------------------------
-__global__ void tet_kappa_kernel(int64_t cells, const double* __restrict__ macro, int npoints,
-                                 const double* __restrict__ ref_bary, int nfine, const int32_t* __restrict__ fine_cells,
-                                 int nquad, const double* __restrict__ qbary, const double* __restrict__ qw,
-                                 int layers, int px, int py, const double* __restrict__ voxels,
-                                 double* __restrict__ diffusion) {
+__global__ void tet_kappa_kernel(int64_t cells, const double* __restrict__ points, int npoints, int nfine,
+                                 const int32_t* __restrict__ fine_cells, int nquad, const double* __restrict__ qbary,
+                                 const double* __restrict__ qw, int layers, int px, int py,
+                                 const double* __restrict__ voxels, double* __restrict__ diffusion) {
   const int64_t total = cells * (int64_t)nfine;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < total; id += stride) {
     const int64_t cell = id / nfine;
     const int e = (int)(id - cell * nfine);
-    const double* X = macro + cell * 12;
+    const double* X = points + cell * (int64_t)npoints * 3;
     double p[4][3];
-    for (int v = 0; v < 4; ++v) {
-      const double* b = ref_bary + (int64_t)fine_cells[4 * e + v] * 4;
-      for (int j = 0; j < 3; ++j) {
-        double acc = __dmul_rn(b[0], X[j]);
-        acc = __dadd_rn(acc, __dmul_rn(b[1], X[3 + j]));
-        acc = __dadd_rn(acc, __dmul_rn(b[2], X[6 + j]));
-        p[v][j] = __dadd_rn(acc, __dmul_rn(b[3], X[9 + j]));
-      }
-    }
+    for (int v = 0; v < 4; ++v)
+      for (int j = 0; j < 3; ++j) p[v][j] = X[(int64_t)fine_cells[4 * e + v] * 3 + j];
     double kbar = 0.0;
     for (int q = 0; q < nquad; ++q) {
       const double* b = qbary + 4 * q;
@@ -298,16 +291,15 @@ int grid_for(int64_t work) {
 
 using namespace mhm;
 
-extern "C" int mhm_tet_kappa(int64_t cells, const double* macro_vertices, int32_t npoints, const double* ref_bary,
-                             int32_t nfine, const int32_t* fine_cells, int32_t nquad, const double* quad_bary,
+extern "C" int mhm_tet_kappa(int64_t cells, const double* points, int32_t npoints, int32_t nfine,
+                             const int32_t* fine_cells, int32_t nquad, const double* quad_bary,
                              const double* quad_weights, int32_t layers, int32_t px, int32_t py,
                              const double* voxels, double* diffusion, void* stream) {
-  if (cells < 1 || npoints < 4 || nfine < 1 || nquad < 1 || layers < 1 || px < 1 || py < 1 || !macro_vertices ||
-      !ref_bary || !fine_cells || !quad_bary || !quad_weights || !voxels || !diffusion)
+  if (cells < 1 || npoints < 4 || nfine < 1 || nquad < 1 || layers < 1 || px < 1 || py < 1 || !points ||
+      !fine_cells || !quad_bary || !quad_weights || !voxels || !diffusion)
     return MHM_ERR_ARGUMENT;
   tet_kappa_kernel<<<grid_for(cells * nfine), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      cells, macro_vertices, npoints, ref_bary, nfine, fine_cells, nquad, quad_bary, quad_weights, layers, px, py,
-      voxels, diffusion);
+      cells, points, npoints, nfine, fine_cells, nquad, quad_bary, quad_weights, layers, px, py, voxels, diffusion);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
 

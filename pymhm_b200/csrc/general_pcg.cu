@@ -12,17 +12,21 @@
 //
 //   lambda0 = G0 Q (-r_c),  Q = (G0^T G0)^-1 (dense, built once per mesh);
 //   P S P mu = P (r_lambda - S lambda0),  P = I - G0 Q G0^T,
-//   preconditioner P M^-1 P with M^-1 = block Jacobi over the skeleton faces;
+//   preconditioner P M^-1 P, M^-1 either block Jacobi over the skeleton faces or,
+//   when the caller passes the cells' condensed blocks, the cell-Dirichlet sum
+//   sum_c R_c^T D_c S_c^-1 D_c R_c (S_c the cell's trace-trace block, D_c the
+//   stiffness weights S_c,aa / S_aa), the FETI Dirichlet preconditioner with the
+//   roles of the Neumann and Dirichlet operators exchanged (S_c maps fluxes to
+//   traces here);
 //   c = Q G0^T (S lambda - r_lambda),  lambda = lambda0 + mu.
 //
 // One persistent cooperative launch does everything.  Vectors live in the caller's
 // workspace; the trace-trace block S is read from the CSR rows (columns < T).  Every
 // sum runs in a fixed order (per-CTA partials summed identically in every CTA), so
-// results are bitwise reproducible.  Six grid barriers per CG iteration: the residual
-// and the search direction are double-buffered so that values another CTA still reads
-// are never overwritten in the same phase, and quantities a phase needs from other
-// CTAs' DOFs (the updated residual in the cell sums, the preconditioned residual of
-// a shared face) are recomputed where they are read, with the same arithmetic.  Every
+// results are bitwise reproducible.  Seven grid barriers per CG iteration: the
+// residual and the search direction are double-buffered so that values another CTA
+// still reads are never overwritten in the same phase, and the updated residual that
+// the cell sums need is recomputed where it is read, with the same arithmetic.  Every
 // barrier is bounded: a CTA that waits too long sets the error flag, and all return.
 #include <cmath>
 #include <cstdint>
@@ -33,7 +37,6 @@ namespace mhm {
 namespace {
 
 constexpr int kGThreads = 512;
-constexpr int kGWarps = kGThreads / 32;
 constexpr long long kGSpinLimit = 1ll << 26;
 constexpr int kMaxFace = 8;  // DOFs per skeleton face
 constexpr int kSlots = 4;    // reduction slots per CTA
@@ -53,6 +56,10 @@ struct GWork {
   double* v2;
   double* rfull;
   double* finv;
+  double* dof_g;   // (T, 2): G0 entry of the DOF in its first and second cell
+  double* ypart;   // (cell entries): a cell's preconditioned residual on its DOFs
+  double* dsum;    // (T): sum of the DOF's diagonal entries over its cells' blocks
+  double* cinv;    // (cell entries^2 ragged): D S_c^-1 D of every cell
   double* part;
   unsigned* bar;
   int* err;
@@ -67,7 +74,6 @@ struct GParams {
   int max_inner, max_outer;
   int* info;
   double* stats;
-  int32_t* dof_face;
 };
 
 __device__ __forceinline__ unsigned g_ld_acquire(const unsigned* p) {
@@ -108,13 +114,23 @@ __device__ void g_partial(const GWork& w, int slot, double v, double* red) {
   if (threadIdx.x == 0) w.part[blockIdx.x * kSlots + slot] = v;
 }
 
-// Totals of slots [0, n) over all CTAs, in CTA order (the same bits in every CTA).
-__device__ void g_totals(const GWork& w, int n, double* out, double* sh) {
+__device__ void g_partial_max(const GWork& w, int slot, double v, double* red) {
+  v = block_max(v, red);
+  if (threadIdx.x == 0) w.part[blockIdx.x * kSlots + slot] = v;
+}
+
+// Totals of slots [0, n) over all CTAs, in CTA order (the same bits in every CTA); the
+// slots whose bit is set in max_mask are combined by maximum instead of sum.
+__device__ void g_totals(const GWork& w, int n, double* out, double* sh, unsigned max_mask = 0u) {
   if (threadIdx.x < 32) {
     for (int k = 0; k < n; ++k) {
+      const bool mx = (max_mask >> k) & 1u;
       double a = 0.0;
-      for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) a += __ldcg(w.part + i * kSlots + k);
-      a = warp_sum(a);
+      for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) {
+        const double v = __ldcg(w.part + i * kSlots + k);
+        a = mx ? fmax(a, v) : a + v;
+      }
+      a = mx ? warp_max(a) : warp_sum(a);
       if (threadIdx.x == 0) sh[k] = a;
     }
   }
@@ -123,14 +139,13 @@ __device__ void g_totals(const GWork& w, int n, double* out, double* sh) {
   __syncthreads();
 }
 
-// (G0 v)_i: the DOF's entries in its (at most two) cells, first cell then second.
-__device__ __forceinline__ double g0_apply(const mhm_general_system& s, int64_t i, const double* v) {
-  double acc = 0.0;
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const int c = s.dof_cells[2 * i + k];
-    if (c >= 0) acc = fma(s.cell_g0[s.dof_entry[2 * i + k]], __ldcg(v + c), acc);
-  }
+// (G0 v)_i: the DOF's entries in its (at most two) cells, first cell then second
+// (dof_g holds the entries, 0 for a missing second cell).
+__device__ __forceinline__ double g0_apply(const mhm_general_system& s, const double* dof_g, int64_t i,
+                                           const double* v) {
+  const int2 c = reinterpret_cast<const int2*>(s.dof_cells)[i];
+  double acc = dof_g[2 * i] * __ldcg(v + c.x);
+  if (c.y >= 0) acc = fma(dof_g[2 * i + 1], __ldcg(v + c.y), acc);
   return acc;
 }
 
@@ -149,22 +164,49 @@ __device__ void q_gemv(const mhm_general_system& s, const double* xin, double* y
   }
 }
 
-// Projected, preconditioned residual entry of DOF i: r = rt - G0 v on its face, then
-// z0_i = (M_f^-1 r_f)_i.  Also returns r_i.
-__device__ __forceinline__ double dof_z0(const GParams& P, int64_t i, const double* rt, const double* v,
-                                         double& ri) {
+// Face block-Jacobi: z0 on the DOFs of face f from the projected residual rt - G0 v.
+__device__ __forceinline__ void face_apply(const GParams& P, int64_t f, const double* rt, const double* v,
+                                           double* z0) {
   const mhm_general_system& s = P.s;
-  const int f = P.dof_face[i];
   const int64_t f0 = s.face_ptr[f];
   const int fs = (int)(s.face_ptr[f + 1] - f0);
-  const double* inv = P.w.finv + (int64_t)f * kMaxFace * kMaxFace + (i - f0) * kMaxFace;
-  double acc = 0.0;
-  ri = 0.0;
-  for (int j = 0; j < fs; ++j) {
-    const double rj = __ldcg(rt + f0 + j) - g0_apply(s, f0 + j, v);
-    if (f0 + j == i) ri = rj;
-    acc = fma(inv[j], rj, acc);
+  double rv[kMaxFace];
+  for (int j = 0; j < fs; ++j) rv[j] = __ldcg(rt + f0 + j) - g0_apply(s, P.w.dof_g, f0 + j, v);
+  const double* inv = P.w.finv + f * kMaxFace * kMaxFace;
+  for (int i = 0; i < fs; ++i) {
+    double acc = 0.0;
+    for (int j = 0; j < fs; ++j) acc = fma(inv[i * kMaxFace + j], rv[j], acc);
+    z0[f0 + i] = acc;
   }
+}
+
+// Cell-Dirichlet: y_c = D S_c^-1 D r_c on the cell's DOFs, r = rt - G0 v, one warp per
+// cell (lane a computes row a; t <= 32).
+__device__ __forceinline__ void cell_apply(const GParams& P, int64_t c, const double* rt, const double* v,
+                                           int lane) {
+  const mhm_general_system& s = P.s;
+  const int64_t e0 = s.cell_ptr[c];
+  const int t = (int)(s.cell_ptr[c + 1] - e0);
+  double ra = 0.0;
+  if (lane < t) {
+    const int64_t i = s.cell_dofs[e0 + lane];
+    ra = __ldcg(rt + i) - g0_apply(s, P.w.dof_g, i, v);
+  }
+  const double* W = P.w.cinv + s.block_off[c];
+  double acc = 0.0;
+  for (int b = 0; b < t; ++b) {
+    const double rb = __shfl_sync(0xffffffffu, ra, b);
+    if (lane < t) acc = fma(W[lane * t + b], rb, acc);
+  }
+  if (lane < t) P.w.ypart[e0 + lane] = acc;
+}
+
+// The DOF's preconditioned value: the sum of its cells' parts, first cell then second.
+__device__ __forceinline__ double dof_gather(const GParams& P, int64_t i) {
+  const mhm_general_system& s = P.s;
+  const int2 c = reinterpret_cast<const int2*>(s.dof_cells)[i];
+  double acc = __ldcg(P.w.ypart + s.dof_entry[2 * i]);
+  if (c.y >= 0) acc += __ldcg(P.w.ypart + s.dof_entry[2 * i + 1]);
   return acc;
 }
 
@@ -211,6 +253,110 @@ __device__ void face_inverse(const mhm_general_system& s, int f, double* out) {
   }
 }
 
+// D S_c^-1 D of one cell, by one warp: S_c is the top-left t x t of the cell's block
+// (row length t + 1); Gauss-Jordan in place on W (lane j owns column j; SPD, no
+// pivoting), then the stiffness weights D_a = S_aa / (sum over the DOF's cells).
+__device__ void cell_inverse(const GParams& P, int64_t c, int lane) {
+  const mhm_general_system& s = P.s;
+  const int64_t e0 = s.cell_ptr[c];
+  const int t = (int)(s.cell_ptr[c + 1] - e0);
+  const double* S = s.cell_blocks + s.block_off[c];
+  double* W = P.w.cinv + s.block_off[c];
+  if (lane < t)
+    for (int i = 0; i < t; ++i) W[i * t + lane] = S[i * (t + 1) + lane];
+  __syncwarp();
+  for (int k = 0; k < t; ++k) {
+    const double a = 1.0 / W[k * t + k];
+    __syncwarp();
+    if (lane < t && lane != k) W[k * t + lane] *= a;
+    __syncwarp();
+    // column k is left untouched until its own update below
+    if (lane < t && lane != k)
+      for (int i = 0; i < t; ++i)
+        if (i != k) W[i * t + lane] = fma(-W[i * t + k], W[k * t + lane], W[i * t + lane]);
+    __syncwarp();
+    if (lane == k) {
+      for (int i = 0; i < t; ++i)
+        if (i != k) W[i * t + k] = -W[i * t + k] * a;
+      W[k * t + k] = a;
+    }
+    __syncwarp();
+  }
+  double d = 0.0;
+  if (lane < t) d = S[lane * (t + 1) + lane] / __ldcg(P.w.dsum + s.cell_dofs[e0 + lane]);
+  for (int i = 0; i < t; ++i) {
+    const double di = __shfl_sync(0xffffffffu, d, i);
+    if (lane < t) W[i * t + lane] *= di * d;
+  }
+  __syncwarp();
+}
+
+// r = rt - G0 v on every DOF; z0 = M^-1 r (face blocks, or the cells' D S^-1 D summed
+// per DOF); w2 = G0^T z0 per cell.  Two grid barriers; false when one timed out.
+__device__ __noinline__ bool precondition(const GParams& P, const double* rt, unsigned& epoch) {
+  const mhm_general_system& s = P.s;
+  const GWork& w = P.w;
+  const int64_t T = s.trace_size;
+  const int M = s.cells;
+  const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
+  const bool cellmode = s.cell_blocks != nullptr;
+  for (int64_t i = gtid; i < T; i += gstride) w.r[i] = __ldcg(rt + i) - g0_apply(s, w.dof_g, i, w.v);
+  if (cellmode) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t c = gtid >> 5; c < M; c += gstride >> 5) cell_apply(P, c, rt, w.v, lane);
+  } else {
+    for (int64_t f = gtid; f < s.faces; f += gstride) face_apply(P, f, rt, w.v, w.z0);
+  }
+  if (!g_sync(w, epoch)) return false;
+  if (cellmode)
+    for (int64_t i = gtid; i < T; i += gstride) w.z0[i] = dof_gather(P, i);
+  for (int64_t c = gtid; c < M; c += gstride) {
+    double acc = 0.0;
+    for (int64_t e = s.cell_ptr[c]; e < s.cell_ptr[c + 1]; ++e) {
+      const int64_t i = s.cell_dofs[e];
+      acc = fma(s.cell_g0[e], cellmode ? dof_gather(P, i) : __ldcg(w.z0 + i), acc);
+    }
+    w.w2[c] = acc;
+  }
+  return g_sync(w, epoch);
+}
+
+// Per-DOF setup: the DOF's G0 entries, and the sum of its diagonal entries over its
+// cells' blocks (cell-Dirichlet) or, per face, the face block inverses.
+__global__ void general_setup_kernel(const GParams P) {
+  const mhm_general_system& s = P.s;
+  const GWork& w = P.w;
+  const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
+  const bool cellmode = s.cell_blocks != nullptr;
+  for (int64_t i = gtid; i < s.trace_size; i += gstride) {
+    const int2 c = reinterpret_cast<const int2*>(s.dof_cells)[i];
+    w.dof_g[2 * i] = s.cell_g0[s.dof_entry[2 * i]];
+    w.dof_g[2 * i + 1] = c.y >= 0 ? s.cell_g0[s.dof_entry[2 * i + 1]] : 0.0;
+    if (cellmode) {
+      double d = 0.0;
+      for (int k = 0; k < 2; ++k) {
+        const int cc = k ? c.y : c.x;
+        if (cc < 0) continue;
+        const int64_t a = s.dof_entry[2 * i + k] - s.cell_ptr[cc];
+        const int tc = (int)(s.cell_ptr[cc + 1] - s.cell_ptr[cc]);
+        d += s.cell_blocks[s.block_off[cc] + a * (tc + 1) + a];
+      }
+      w.dsum[i] = d;
+    }
+  }
+  if (!cellmode)
+    for (int64_t f = gtid; f < s.faces; f += gstride) face_inverse(s, (int)f, w.finv + f * kMaxFace * kMaxFace);
+}
+
+// One warp per cell: D S_c^-1 D (after general_setup_kernel's DOF sums).
+__global__ void general_cell_inverse_kernel(const GParams P) {
+  const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t c = gtid >> 5; c < P.s.cells; c += nwarps) cell_inverse(P, c, threadIdx.x & 31);
+}
+
 __global__ void __launch_bounds__(kGThreads, 1) general_pcg_kernel(const GParams P) {
   __shared__ double red[32];
   __shared__ double sh[kSlots];
@@ -224,13 +370,18 @@ __global__ void __launch_bounds__(kGThreads, 1) general_pcg_kernel(const GParams
   int status = MHM_SOLVE_OK;
   int total_inner = 0, outer = 0;
   double tot[kSlots];
-  double bnorm = 0.0, res = 0.0;
+  double bnorm = 0.0, res = 0.0, omega = INFINITY;
 #define GSYNC()                                                              \
   do {                                                                       \
     if (!g_sync(w, epoch)) { status = MHM_SOLVE_BARRIER_TIMEOUT; goto done; } \
   } while (0)
-
-  for (int64_t f = gtid; f < s.faces; f += gstride) face_inverse(s, (int)f, w.finv + f * kMaxFace * kMaxFace);
+#define PRECONDITION(RT)                                          \
+  do {                                                            \
+    if (!precondition(P, (RT), epoch)) {                          \
+      status = MHM_SOLVE_BARRIER_TIMEOUT;                         \
+      goto done;                                                  \
+    }                                                             \
+  } while (0)
   {
     double b2 = 0.0;
     for (int64_t i = gtid; i < N; i += gstride) {
@@ -248,23 +399,37 @@ __global__ void __launch_bounds__(kGThreads, 1) general_pcg_kernel(const GParams
     goto done;
   }
   for (;;) {
-    // ---- outer residual rfull = b - K x over all rows ------------------------------
+    // ---- outer residual rfull = b - K x over all rows, its norm and the componentwise
+    //      backward error max_i |r_i| / (|b_i| + sum_j |K_ij| |x_j|) ----------------------
     {
-      double r2 = 0.0;
+      double r2 = 0.0, om = 0.0;
       for (int64_t i = gtid; i < N; i += gstride) {
-        double acc = P.rhs[i];
-        for (int64_t k = s.indptr[i]; k < s.indptr[i + 1]; ++k)
+        const double b = P.rhs[i];
+        double acc = b, den = fabs(b);
+        for (int64_t k = s.indptr[i]; k < s.indptr[i + 1]; ++k) {
+          const double t = s.values[k] * __ldcg(P.x + s.indices[k]);
           acc = fma(-s.values[k], __ldcg(P.x + s.indices[k]), acc);
+          den += fabs(t);
+        }
         w.rfull[i] = acc;
         r2 = fma(acc, acc, r2);
+        om = fmax(om, den > 0.0 ? fabs(acc) / den : (acc != 0.0 ? INFINITY : 0.0));
       }
       g_partial(w, 0, r2, red);
+      g_partial_max(w, 1, om, red);
     }
     GSYNC();
-    g_totals(w, 1, tot, sh);
+    g_totals(w, 2, tot, sh, 2u);
     res = sqrt(tot[0]) / bnorm;
     if (!isfinite(res)) { status = MHM_SOLVE_NONFINITE; goto done; }
-    if (res <= P.rtol) break;
+    // Converged when the normwise residual meets rtol and every row's residual is
+    // within rtol of that row's scale (rows of short faces have tiny entries that a
+    // normwise test alone leaves unresolved), or the latter stopped improving.
+    if (res <= P.rtol && (tot[1] <= P.rtol || tot[1] > 0.5 * omega)) {
+      omega = tot[1];
+      break;
+    }
+    omega = tot[1];
     if (outer >= P.max_outer || total_inner >= P.max_inner) { status = MHM_SOLVE_NOT_CONVERGED; goto done; }
     ++outer;
     // ---- lambda0 = G0 Q (-r_c) ---------------------------------------------------
@@ -273,7 +438,7 @@ __global__ void __launch_bounds__(kGThreads, 1) general_pcg_kernel(const GParams
     q_gemv(s, w.w, w.v);
     GSYNC();
     for (int64_t i = gtid; i < T; i += gstride) {
-      w.lam0[i] = g0_apply(s, i, w.v);
+      w.lam0[i] = g0_apply(s, w.dof_g, i, w.v);
       w.mu[i] = 0.0;
       w.p[0][i] = 0.0;
     }
@@ -298,27 +463,14 @@ __global__ void __launch_bounds__(kGThreads, 1) general_pcg_kernel(const GParams
     GSYNC();
     q_gemv(s, w.w, w.v);
     GSYNC();
-    for (int64_t i = gtid; i < T; i += gstride) {
-      double ri;
-      w.z0[i] = dof_z0(P, i, w.rt[0], w.v, ri);
-      w.r[i] = ri;
-    }
-    for (int64_t c = gtid; c < M; c += gstride) {
-      double acc = 0.0;
-      for (int64_t e = s.cell_ptr[c]; e < s.cell_ptr[c + 1]; ++e) {
-        double ri;
-        acc = fma(s.cell_g0[e], dof_z0(P, s.cell_dofs[e], w.rt[0], w.v, ri), acc);
-      }
-      w.w2[c] = acc;
-    }
-    GSYNC();
+    PRECONDITION(w.rt[0]);
     q_gemv(s, w.w2, w.v2);
     GSYNC();
     double gamma, rr0;
     {
       double rz = 0.0, rr = 0.0;
       for (int64_t i = gtid; i < T; i += gstride) {
-        const double zi = __ldcg(w.z0 + i) - g0_apply(s, i, w.v2);
+        const double zi = __ldcg(w.z0 + i) - g0_apply(s, w.dof_g, i, w.v2);
         w.z[i] = zi;
         const double ri = __ldcg(w.r + i);
         rz = fma(ri, zi, rz);
@@ -332,14 +484,12 @@ __global__ void __launch_bounds__(kGThreads, 1) general_pcg_kernel(const GParams
     gamma = tot[0];
     rr0 = tot[1];
     {
-      // stop at the inner tolerance, or once the inner residual is below half of what
-      // the outer tolerance asks of the whole system
-      const double floor_abs = 0.5 * P.rtol * bnorm;
-      const double target = fmax(P.inner_rtol * sqrt(rr0), floor_abs);
+      // stop once the preconditioned residual norm (r, z)^1/2 fell by inner_rtol
+      const double target = P.inner_rtol * sqrt(fmax(gamma, 0.0));
       double beta = 0.0;
       int cur = 0;
       double rr = rr0;
-      while (sqrt(rr) > target && total_inner < P.max_inner) {
+      while (sqrt(fmax(gamma, 0.0)) > target && total_inner < P.max_inner) {
         if (!(gamma > 0.0)) { status = MHM_SOLVE_BREAKDOWN; goto done; }
         const int nxt = cur ^ 1;
         // P1: direction p = z + beta p_prev, q = S p
@@ -379,21 +529,8 @@ __global__ void __launch_bounds__(kGThreads, 1) general_pcg_kernel(const GParams
         // P3: v = Q G0^T rt
         q_gemv(s, w.w, w.v);
         GSYNC();
-        // P4: r = P rt, z0 = M^-1 r (face blocks); the cells' G0^T z0
-        for (int64_t i = gtid; i < T; i += gstride) {
-          double ri;
-          w.z0[i] = dof_z0(P, i, w.rt[nxt], w.v, ri);
-          w.r[i] = ri;
-        }
-        for (int64_t c = gtid; c < M; c += gstride) {
-          double acc = 0.0;
-          for (int64_t e = s.cell_ptr[c]; e < s.cell_ptr[c + 1]; ++e) {
-            double ri;
-            acc = fma(s.cell_g0[e], dof_z0(P, s.cell_dofs[e], w.rt[nxt], w.v, ri), acc);
-          }
-          w.w2[c] = acc;
-        }
-        GSYNC();
+        // P4: r = P rt, z0 = M^-1 r; the cells' G0^T z0 (two barriers)
+        PRECONDITION(w.rt[nxt]);
         // P5: v2 = Q G0^T z0
         q_gemv(s, w.w2, w.v2);
         GSYNC();
@@ -401,7 +538,7 @@ __global__ void __launch_bounds__(kGThreads, 1) general_pcg_kernel(const GParams
         {
           double rz = 0.0, r2 = 0.0;
           for (int64_t i = gtid; i < T; i += gstride) {
-            const double zi = __ldcg(w.z0 + i) - g0_apply(s, i, w.v2);
+            const double zi = __ldcg(w.z0 + i) - g0_apply(s, w.dof_g, i, w.v2);
             w.z[i] = zi;
             const double ri = __ldcg(w.r + i);
             rz = fma(ri, zi, rz);
@@ -451,12 +588,15 @@ done:
     P.info[3] = *reinterpret_cast<volatile int*>(w.err);
     P.stats[0] = res;
     P.stats[1] = bnorm;
+    P.stats[2] = omega;
   }
 #undef GSYNC
+#undef PRECONDITION
 }
 
 struct GLayout {
-  size_t mu, rt0, rt1, p0, p1, q, r, z0, z, lam0, w, v, w2, v2, rfull, finv, dof_face, part, bar, err, total;
+  size_t mu, rt0, rt1, p0, p1, q, r, z0, z, lam0, w, v, w2, v2, rfull, finv, dof_g, ypart, dsum, cinv, part,
+      bar, err, total;
 };
 
 GLayout g_layout(const mhm_general_system* s, int grid) {
@@ -484,7 +624,10 @@ GLayout g_layout(const mhm_general_system* s, int grid) {
   L.v2 = take(M * 8);
   L.rfull = take(N * 8);
   L.finv = take((size_t)s->faces * kMaxFace * kMaxFace * 8);
-  L.dof_face = take(T * 4);
+  L.dof_g = take(T * 2 * 8);
+  L.ypart = take((size_t)s->cell_entries * 8);
+  L.dsum = take(T * 8);
+  L.cinv = take((size_t)(s->block_off ? s->blocks_size : 1) * 8);
   L.part = take((size_t)grid * kSlots * 8);
   L.bar = take(2 * sizeof(unsigned));
   L.err = take(sizeof(int));
@@ -492,18 +635,14 @@ GLayout g_layout(const mhm_general_system* s, int grid) {
   return L;
 }
 
-__global__ void dof_face_kernel(int64_t faces, const int64_t* face_ptr, int32_t* dof_face) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; f < faces; f += stride)
-    for (int64_t i = face_ptr[f]; i < face_ptr[f + 1]; ++i) dof_face[i] = (int32_t)f;
-}
-
 // The layout (everything but the matrix values, which change from solve to solve).
 bool g_valid_layout(const mhm_general_system* s) {
   return s && s->trace_size >= 1 && s->cells >= 1 && s->size == s->trace_size + s->cells && s->faces >= 1 &&
          s->indptr && s->indices && s->face_ptr && s->cell_ptr && s->cell_dofs && s->cell_g0 && s->dof_cells &&
          s->dof_entry && s->coarse_inverse && s->max_face_size >= 1 && s->max_face_size <= kMaxFace &&
-         s->trace_size <= INT32_MAX;
+         s->trace_size <= INT32_MAX && s->cell_entries >= 1 &&
+         (!s->block_off || (s->blocks_size >= 1 && s->max_cell_dofs >= 1 && s->max_cell_dofs <= 32)) &&
+         (!s->cell_blocks || s->block_off);
 }
 
 int g_grid() {
@@ -560,10 +699,13 @@ extern "C" int mhm_general_solve(const mhm_general_system* s, const double* rhs,
   P.w.v2 = d(L.v2);
   P.w.rfull = d(L.rfull);
   P.w.finv = d(L.finv);
+  P.w.dof_g = d(L.dof_g);
+  P.w.ypart = d(L.ypart);
+  P.w.dsum = d(L.dsum);
+  P.w.cinv = d(L.cinv);
   P.w.part = d(L.part);
   P.w.bar = reinterpret_cast<unsigned*>(base + L.bar);
   P.w.err = reinterpret_cast<int*>(base + L.err);
-  P.dof_face = reinterpret_cast<int32_t*>(base + L.dof_face);
   P.rhs = rhs;
   P.x = x;
   P.rtol = rtol;
@@ -573,9 +715,8 @@ extern "C" int mhm_general_solve(const mhm_general_system* s, const double* rhs,
   P.info = info;
   P.stats = stats;
   if (cudaMemsetAsync(base + L.bar, 0, L.total - L.bar, st) != cudaSuccess) return MHM_ERR_LAUNCH;
-  int blocks = (int)((s->faces + 255) / 256);
-  if (blocks > 4096) blocks = 4096;
-  dof_face_kernel<<<blocks, 256, 0, st>>>(s->faces, s->face_ptr, P.dof_face);
+  general_setup_kernel<<<grid * 2, 256, 0, st>>>(P);
+  if (s->cell_blocks) general_cell_inverse_kernel<<<grid * 2, 256, 0, st>>>(P);
   void* args[] = {&P};
   if (cudaLaunchCooperativeKernel((const void*)general_pcg_kernel, grid, kGThreads, args, 0, st) != cudaSuccess)
     return MHM_ERR_LAUNCH;

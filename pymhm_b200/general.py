@@ -7,6 +7,9 @@ cells' trace DOFs (ragged: a polygon has as many faces as edges), the exact geom
 constraint G0 = B^T 1 of every (cell, DOF), the DOF -> cell maps, the skeleton faces
 that group the DOFs for the block-Jacobi preconditioner, and the dense inverse of the
 coarse operator G0^T G0, which depends on the mesh only and is formed once here.
+Callers that hold the cells' condensed blocks on the device (the local stage writes
+them) pass them to ``launch``; the solver then preconditions with the cells'
+D S_c^-1 D (cell-Dirichlet), which needs far fewer iterations than the face blocks.
 
 ``GeneralSkeleton.solve`` replaces the global solve of ``solve_hybrid_system``
 (``core/system.py:355-528``) for systems without fixed DOFs or gauge rows;
@@ -21,8 +24,10 @@ from scipy import sparse
 
 from . import _lib
 from .errors import LinearSolveError
+from .topology import block_offsets
 
 MAX_FACE_DOFS = 8
+MAX_CELL_DOFS_DIRICHLET = 32
 
 
 def ragged(cell_dofs, cell_g0):
@@ -54,6 +59,8 @@ def dof_maps(cell_ptr, flat_dofs, trace_size):
     dof_entry = np.zeros((trace_size, 2), dtype=np.int64)
     dof_cells[d, k] = c
     dof_entry[d, k] = e
+    if np.any(dof_cells[:, 0] < 0):
+        raise ValueError("every trace DOF must belong to at least one cell")
     return dof_cells, dof_entry
 
 
@@ -79,7 +86,8 @@ class GeneralSkeleton:
     ``face_ptr`` (faces + 1): face f owns the trace DOFs ``face_ptr[f]..face_ptr[f+1]-1``
     (at most 8); ``indptr`` / ``indices``: the structural CSR of the whole reduced
     system (trace DOFs first, then one coarse unknown per cell), as the ordered scatter
-    fills it.
+    fills it.  ``block_off`` (cells + 1, from ``topology.block_offsets``) locates the
+    cells' (t + 1)^2 condensed blocks in the flat array ``launch`` may be given.
     """
 
     def __init__(self, cell_dofs, cell_g0, face_ptr, trace_size, indptr, indices, *, device=None):
@@ -119,16 +127,35 @@ class GeneralSkeleton:
         s.cell_dofs, s.cell_g0 = _lib.ptr(k["cell_dofs"]), _lib.ptr(k["cell_g0"])
         s.dof_cells, s.dof_entry = _lib.ptr(k["dof_cells"]), _lib.ptr(k["dof_entry"])
         s.coarse_inverse = _lib.ptr(k["qinv"])
+        s.cell_entries = int(self.cell_ptr[-1])
+        widths = np.diff(self.cell_ptr)
+        bofs, _ = block_offsets([np.empty(int(t)) for t in widths])
+        self.block_off = bofs
+        self.cell_dirichlet = bool(widths.max() <= MAX_CELL_DOFS_DIRICHLET)
+        if self.cell_dirichlet:
+            k["block_off"] = up(bofs[:-1], torch.int64)
+            s.block_off, s.blocks_size, s.max_cell_dofs = _lib.ptr(k["block_off"]), int(bofs[-1]), int(widths.max())
         nbytes = int(self.lib.mhm_general_workspace_bytes(s))
         if nbytes <= 0:
             raise RuntimeError("could not size the general skeleton workspace")
         self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
         self.info = torch.zeros(4, dtype=torch.int32, device=self.device)
-        self.stats = torch.zeros(2, dtype=torch.float64, device=self.device)
+        self.stats = torch.zeros(3, dtype=torch.float64, device=self.device)
 
-    def launch(self, values, rhs, x, *, rtol=1e-13, inner_rtol=1e-10, max_inner=20000, max_outer=8, stream=None):
-        """Enqueue x = K^-1 rhs for the CSR ``values`` (device tensors, no host sync)."""
+    def launch(self, values, rhs, x, *, blocks=None, rtol=1e-13, inner_rtol=1e-10, max_inner=20000, max_outer=8,
+               stream=None):
+        """Enqueue x = K^-1 rhs for the CSR ``values`` (device tensors, no host sync).
+
+        ``blocks``: the cells' condensed blocks (flat, at ``block_off``) whose ordered
+        scatter gave ``values``; with them (and cells of at most 32 DOFs) the solve
+        uses the cell-Dirichlet preconditioner, else face block-Jacobi."""
         self.sys.values = _lib.ptr(values)
+        if blocks is not None and self.cell_dirichlet:
+            if blocks.numel() < int(self.block_off[-1]) or blocks.dtype != self.torch.float64:
+                raise ValueError("blocks must hold every cell's (t + 1)^2 float64 block")
+            self.sys.cell_blocks = _lib.ptr(blocks)
+        else:
+            self.sys.cell_blocks = 0
         P = _lib.ptr
         _lib.check(self.lib.mhm_general_solve(self.sys, P(rhs), P(x), P(self.workspace), self.workspace.numel(),
                                               float(rtol), float(inner_rtol), int(max_inner), int(max_outer),

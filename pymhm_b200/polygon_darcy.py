@@ -59,20 +59,25 @@ def disc_grid(field: DiscInclusions, grid: int = 64):
     return ptr, flat if len(flat) else np.zeros(1, np.int32)
 
 
+def p2_size(mesh: PolygonMesh, cell: int, r: int) -> int:
+    """P2 unknowns of ``mesh.submesh(cell, r)``: 1 + m r (2 r + 1) for a fan of m
+    triangles around the cell's centroid (every convex cell), else counted."""
+    _, base = mesh.base_triangles(cell)
+    centre = len(base)
+    if np.all(base[:, 2] == centre) and len(base) == len(mesh.cells[cell]):
+        return 1 + len(base) * r * (2 * r + 1)
+    return len(p2_nodal_space(mesh.submesh(cell, r))[1])
+
+
 def refinement_for_sizes(mesh: PolygonMesh, lo: int = 200, hi: int = MAX_AUGMENTED - 1, seed: int = 0):
-    """Per-cell subdivision counts with P2 sizes drawn uniformly in [lo, hi]: for a
-    target size, the largest count whose local space stays within it (at least 1)."""
+    """Per-cell subdivision counts for P2 sizes drawn uniformly in [lo, hi]: for each
+    cell's target size, the largest count whose local space stays within it (at least 1)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     out = np.empty(len(mesh.cells), dtype=np.int64)
     for c in range(len(mesh.cells)):
-        _, base = mesh.base_triangles(c)
-        m = len(base)
         target = rng.uniform(lo, hi)
         r = 1
-        while True:  # P2 nodes of m refined base triangles sharing their edges: grows like 2 m r^2
-            n_next = len(p2_nodal_space(mesh.submesh(c, r + 1))[1]) if m * (r + 1) ** 2 * 2 < 2 * hi else hi + 1
-            if n_next > target or n_next > hi:
-                break
+        while p2_size(mesh, c, r + 1) <= target:
             r += 1
         out[c] = r
     return out
@@ -95,7 +100,8 @@ class PolygonP2Plan:
     refinement): local meshes, couplings, bins, sparsity and every buffer."""
 
     def __init__(self, mesh: PolygonMesh, skeleton: EdgeSkeleton | None = None, refinements=2, *, order=4,
-                 bin_width=32, device=None, global_rtol=1e-13, inner_rtol=1e-10, max_inner=20000, max_outer=8):
+                 bin_width=32, device=None, global_rtol=1e-13, inner_rtol=1e-10, max_inner=20000, max_outer=8,
+                 preconditioner="cell"):
         import torch
 
         self.torch = torch
@@ -105,6 +111,9 @@ class PolygonP2Plan:
         self.skeleton = EdgeSkeleton(mesh) if skeleton is None else skeleton
         self.global_rtol, self.inner_rtol = float(global_rtol), float(inner_rtol)
         self.max_inner, self.max_outer = int(max_inner), int(max_outer)
+        if preconditioner not in ("cell", "face"):
+            raise ValueError("preconditioner must be 'cell' (the cells' D S^-1 D) or 'face' (face blocks)")
+        self.preconditioner = preconditioner
         M = len(mesh.cells)
         self.M = M
         rs = np.broadcast_to(np.asarray(refinements, dtype=np.int64), (M,))
@@ -324,7 +333,8 @@ class PolygonP2Plan:
                    "mhm_skeleton_scatter")
         mark(2)
         self.general.launch(self.values, self.grhs, self.x, rtol=self.global_rtol, inner_rtol=self.inner_rtol,
-                            max_inner=self.max_inner, max_outer=self.max_outer, stream=stream)
+                            max_inner=self.max_inner, max_outer=self.max_outer, stream=stream,
+                            blocks=self.blocks if self.preconditioner == "cell" else None)
         mark(3)
         for b in self.bins:
             v = self._bin_views(b)
@@ -333,6 +343,12 @@ class PolygonP2Plan:
                                                  P(v["cell_id"]), self.T, P(self.x), P(v["field_off"]),
                                                  P(self.fields), sh), "mhm_dense_reconstruct")
         mark(4)
+
+    def failed_cells(self) -> np.ndarray:
+        """Macrocells (global ids) whose local stage failed the reference's contract
+        in the last launch (synchronises)."""
+        bad = np.flatnonzero(self.cell_status.cpu().numpy() | self.solve_status.cpu().numpy())
+        return np.sort(self.order[bad])
 
     def check(self):
         """Raise the reference's error for any failed stage (synchronises)."""

@@ -54,7 +54,8 @@ class TetraP1Plan:
     refinement): topology, tables, sparsity and every buffer of the launch sequence."""
 
     def __init__(self, mesh: TetraMesh, skeleton: TriangularSkeleton | None = None, local_refinement: int = 2, *,
-                 device=None, global_rtol=1e-13, inner_rtol=1e-10, max_inner=20000, max_outer=8):
+                 device=None, global_rtol=1e-13, inner_rtol=1e-10, max_inner=20000, max_outer=8,
+                 preconditioner="cell"):
         import torch
 
         self.torch = torch
@@ -67,6 +68,9 @@ class TetraP1Plan:
         self.r = int(local_refinement)
         self.global_rtol, self.inner_rtol = float(global_rtol), float(inner_rtol)
         self.max_inner, self.max_outer = int(max_inner), int(max_outer)
+        if preconditioner not in ("cell", "face"):
+            raise ValueError("preconditioner must be 'cell' (the cells' D S^-1 D) or 'face' (face blocks)")
+        self.preconditioner = preconditioner
         bary, conn = reference_refinement(self.r)
         fine_cells = TetraMesh(bary @ UNIT_TET, conn).cells  # oriented as in every positive macrocell
         self.n, self.E = len(bary), len(fine_cells)
@@ -77,7 +81,9 @@ class TetraP1Plan:
         if self.t > 12:
             raise NotImplementedError("at most 12 trace DOFs per cell")
         macro = mesh.points[mesh.cells]  # (cells, 4, 3), positively oriented
-        points = np.einsum("pv,cvj->cpj", bary, macro)  # the submeshes' vertices
+        # the submeshes' vertices, each computed as TetraMesh.submesh does (bary @ X):
+        # the material pre-pass must see the same coordinates as the reference
+        points = np.stack([bary @ X for X in macro])
         coupling = trace_coupling(mesh, sk, self.r)
         self.cell_dofs_h = sk.cell_dof_array
         self.pattern = skeleton_pattern(self.cell_dofs_h, self.T)
@@ -88,8 +94,6 @@ class TetraP1Plan:
         def up(a, dtype):
             return torch.as_tensor(np.array(a, order="C", copy=True), dtype=dtype).to(dev)
 
-        self.d_macro = up(macro, torch.float64)
-        self.d_ref_bary = up(bary, torch.float64)
         self.d_fine_cells = up(fine_cells, torch.int32)
         self.d_qbary, self.d_qw = up(qbary, torch.float64), up(qw, torch.float64)
         self.d_points = up(points, torch.float64)
@@ -172,9 +176,9 @@ class TetraP1Plan:
         mark(0)
         if self.kappa is not None:
             L, px, py = self.kappa.shape
-            _lib.check(lib.mhm_tet_kappa(M, P(self.d_macro), n, P(self.d_ref_bary), E, P(self.d_fine_cells),
-                                         len(self.d_qw), P(self.d_qbary), P(self.d_qw), L, px, py, P(self.kappa),
-                                         P(self.diffusion), sh), "mhm_tet_kappa")
+            _lib.check(lib.mhm_tet_kappa(M, P(self.d_points), n, E, P(self.d_fine_cells), len(self.d_qw),
+                                         P(self.d_qbary), P(self.d_qw), L, px, py, P(self.kappa), P(self.diffusion),
+                                         sh), "mhm_tet_kappa")
             kbase, kb, kc = self.diffusion, E, 1
         else:
             kbase, kb, kc = self.kconst, 0, 0
@@ -206,7 +210,8 @@ class TetraP1Plan:
                                             P(self.load_scale), sh), "mhm_skeleton_scatter")
         mark(2)
         self.general.launch(self.values, self.grhs, self.x, rtol=self.global_rtol, inner_rtol=self.inner_rtol,
-                            max_inner=self.max_inner, max_outer=self.max_outer, stream=stream)
+                            max_inner=self.max_inner, max_outer=self.max_outer, stream=stream,
+                            blocks=self.blocks if self.preconditioner == "cell" else None)
         mark(3)
         _lib.check(lib.mhm_dense_reconstruct(M, n1, w, P(self.n_of), P(self.t_of), P(self.solution),
                                              P(self.d_cell_dofs), P(self.dof_off), P(self.cell_id), self.T, P(self.x),

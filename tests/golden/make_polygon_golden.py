@@ -93,7 +93,7 @@ def run_case(name, count, seed, low, high, discs, keep_cells):
 
 def main():
     for name, case in (run_case("polygon_voronoi12_p2_discs", 12, 3, 2, 4, 25, keep_cells=(0, 7)),
-                       run_case("polygon_voronoi40_p2_discs", 40, 21, 1, 3, 60, keep_cells=(3,))):
+                       run_case("polygon_voronoi40_p2_discs", 40, 21, 2, 3, 60, keep_cells=(3,))):
         np.savez_compressed(HERE / f"{name}.npz", **case)
         print(name, "cells", case["count"], "N", len(case["rhs"]), "local sizes",
               int(np.diff(case["field_ptr"]).min()), int(np.diff(case["field_ptr"]).max()))
