@@ -432,22 +432,24 @@ typedef struct mhm_general_system {
     const int64_t* block_off;     /* (cells)                                         */
     int64_t blocks_size;          /* doubles spanned by the blocks                   */
     int32_t max_cell_dofs;
+    int32_t max_trace_row;        /* most trace columns (< T) in one row of the CSR  */
 } mhm_general_system;
 
 /* Workspace bytes of mhm_general_solve on the current device (-1: invalid). */
 int64_t mhm_general_workspace_bytes(const mhm_general_system* s /* host */);
 
 /*
- * x (N) = K^-1 rhs (N): outer FP64 defect correction on K until
- * ||rhs - K x|| <= rtol ||rhs|| and every row's residual is within rtol of
- * |rhs_i| + sum_j |K_ij| |x_j| (or that componentwise error stopped improving),
- * each correction by projected CG on [[S, -G0], [-G0^T, 0]], preconditioned by
- * face block-Jacobi or, with cell_blocks, by the cells' D S_c^-1 D, until the
+ * x (N) = K^-1 rhs (N): flexible GMRES on K in FP64 (cycles of at most 8
+ * steps, each restarted from the true residual) until ||rhs - K x|| <= rtol
+ * ||rhs|| and every row's residual is within rtol of |rhs_i| + sum_j |K_ij|
+ * |x_j| (or that componentwise error stopped improving).  Each step solves
+ * with [[S, -G0], [-G0^T, 0]] by projected CG, preconditioned by face
+ * block-Jacobi or, with cell_blocks, by the cells' D S_c^-1 D, until the
  * preconditioned residual norm fell by inner_rtol (at most max_inner CG
- * iterations in total and max_outer corrections).  Setup kernels, then one
+ * iterations in total and max_outer such solves).  Setup kernels, then one
  * persistent cooperative launch (one CTA per SM).
- * info (4 int32, device): status (MHM_SOLVE_*), inner iterations, outer
- * corrections, barrier error flag; stats (3 doubles, device): final relative
+ * info (4 int32, device): status (MHM_SOLVE_*), inner iterations, inner
+ * solves, barrier error flag; stats (3 doubles, device): final relative
  * residual, ||rhs||, componentwise backward error.  Every grid barrier is bounded.
  */
 int mhm_general_solve(const mhm_general_system* s /* host */, const double* rhs, double* x,

@@ -82,7 +82,7 @@ class GeneralSystem(C.Structure):
         ("cells", C.c_int32), ("cell_ptr", C.c_void_p), ("cell_dofs", C.c_void_p), ("cell_g0", C.c_void_p),
         ("dof_cells", C.c_void_p), ("dof_entry", C.c_void_p), ("coarse_inverse", C.c_void_p),
         ("cell_entries", C.c_int64), ("cell_blocks", C.c_void_p), ("block_off", C.c_void_p),
-        ("blocks_size", C.c_int64), ("max_cell_dofs", C.c_int32),
+        ("blocks_size", C.c_int64), ("max_cell_dofs", C.c_int32), ("max_trace_row", C.c_int32),
     ]
 
 

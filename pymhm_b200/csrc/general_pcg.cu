@@ -5,10 +5,14 @@
 //
 //   K = [[S, -G], [-G^T, -C]]   (trace unknowns lambda, one coarse unknown per cell)
 //
-// is solved by an outer FP64 defect correction x += K0^-1 (b - K x) on the assembled
-// CSR matrix, with K0 = [[S, -G0], [-G0^T, 0]] and G0 = B^T 1 the exact geometric
-// net-flux operator (K - K0 is at rounding level).  K0 is solved by projected CG
-// (the FETI natural coarse space):
+// is solved by flexible GMRES on the assembled CSR matrix in FP64, right-preconditioned
+// by solves with K0 = [[S, -G0], [-G0^T, 0]], G0 = B^T 1 the exact geometric net-flux
+// operator.  K - K0 is at rounding level for most cells, where GMRES takes the two
+// steps of a plain defect correction; cells whose retained basis was corrected
+// (A 1 != 0) carry G != G0 and a coarse term C, and K0^-1 K is then the identity plus
+// a low-rank term, which GMRES resolves in a few more steps (a defect correction
+// alone diverges once that term exceeds one).  K0 is solved by projected CG (the FETI
+// natural coarse space):
 //
 //   lambda0 = G0 Q (-r_c),  Q = (G0^T G0)^-1 (dense, built once per mesh);
 //   P S P mu = P (r_lambda - S lambda0),  P = I - G0 Q G0^T,
@@ -21,9 +25,11 @@
 //   c = Q G0^T (S lambda - r_lambda),  lambda = lambda0 + mu.
 //
 // One persistent cooperative launch does everything.  Vectors live in the caller's
-// workspace; the trace-trace block S is read from the CSR rows (columns < T).  Every
-// sum runs in a fixed order (per-CTA partials summed identically in every CTA), so
-// results are bitwise reproducible.  Seven grid barriers per CG iteration: the
+// workspace.  Every sum runs in a fixed order (per-CTA partials summed identically in
+// every CTA, the small least-squares problem solved the same way in every CTA), so
+// results are bitwise reproducible.  The trace-trace block is re-laid as column-major
+// ELL at setup, the coarse vector of each Q product is staged in shared memory, and
+// per-cell sums run a warp per cell.  Seven grid barriers per CG iteration: the
 // residual and the search direction are double-buffered so that values another CTA
 // still reads are never overwritten in the same phase, and the updated residual that
 // the cell sums need is recomputed where it is read, with the same arithmetic.  Every
@@ -36,10 +42,11 @@
 namespace mhm {
 namespace {
 
-constexpr int kGThreads = 512;
+constexpr int kGThreads = 256;
 constexpr long long kGSpinLimit = 1ll << 26;
 constexpr int kMaxFace = 8;  // DOFs per skeleton face
-constexpr int kSlots = 4;    // reduction slots per CTA
+constexpr int kMaxKrylov = 8;  // flexible GMRES steps per cycle
+constexpr int kSlots = 8;      // reduction slots per CTA (>= kMaxKrylov)
 
 struct GWork {
   double* mu;
@@ -54,12 +61,19 @@ struct GWork {
   double* v;
   double* w2;
   double* v2;
-  double* rfull;
+  double* kv;  // (kMaxKrylov, N): Krylov basis; v_0 holds the cycle's residual unscaled
+  double* kz;  // (kMaxKrylov, N): the inner solves' results z_j = K0^-1 v_j
+  double* ku;  // (N): K z_j during its orthogonalisation
   double* finv;
   double* dof_g;   // (T, 2): G0 entry of the DOF in its first and second cell
   double* ypart;   // (cell entries): a cell's preconditioned residual on its DOFs
   double* dsum;    // (T): sum of the DOF's diagonal entries over its cells' blocks
   double* cinv;    // (cell entries^2 ragged): D S_c^-1 D of every cell
+  int32_t* ell_cols;  // (max_trace_row, T): trace-trace block of S, column-major ELL
+  double* ell_vals;   //   (padding: the row's own column with value 0)
+  int2* ent_cells;    // (cell entries): the entry's DOF's first and second cell
+  double2* ent_g;     //   its G0 entries in those cells
+  int2* ent_pair;     //   its flat entries in those cells (-1: none)
   double* part;
   unsigned* bar;
   int* err;
@@ -74,6 +88,8 @@ struct GParams {
   int max_inner, max_outer;
   int* info;
   double* stats;
+  int qvec;  // Q rows 16-byte aligned with an even length: double2 loads
+  int qsmem; // the coarse vector of a Q product is staged in shared memory
 };
 
 __device__ __forceinline__ unsigned g_ld_acquire(const unsigned* p) {
@@ -149,19 +165,97 @@ __device__ __forceinline__ double g0_apply(const mhm_general_system& s, const do
   return acc;
 }
 
-// y = Q x, one warp per row, lanes over the columns (fixed order).
-__device__ void q_gemv(const mhm_general_system& s, const double* xin, double* yout) {
+// y = Q x, one warp per row, lanes over the columns (fixed order).  With qsmem the
+// CTA first copies x into shared memory; with qvec each lane streams its columns
+// as double2, four loads in flight.
+__device__ void q_gemv(const GParams& P, const double* xin, double* yout) {
+  extern __shared__ double2 xs2[];
+  const mhm_general_system& s = P.s;
   const int M = s.cells;
   const int lane = threadIdx.x & 31;
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  if (P.qsmem) {
+    double* xs = reinterpret_cast<double*>(xs2);
+    for (int d = threadIdx.x; d < M; d += blockDim.x) xs[d] = __ldcg(xin + d);
+    __syncthreads();
+  }
+  if (P.qsmem && P.qvec) {
+    const int H = M >> 1;
+    for (int64_t c = wid; c < M; c += nw) {
+      const double2* row = reinterpret_cast<const double2*>(s.coarse_inverse + c * (int64_t)M);
+      double acc = 0.0;
+      int d = lane;
+      for (; d + 96 < H; d += 128) {
+        const double2 q0 = __ldg(row + d), q1 = __ldg(row + d + 32), q2 = __ldg(row + d + 64),
+                      q3 = __ldg(row + d + 96);
+        const double2 x0 = xs2[d], x1 = xs2[d + 32], x2 = xs2[d + 64], x3 = xs2[d + 96];
+        acc = fma(q0.x, x0.x, acc);
+        acc = fma(q0.y, x0.y, acc);
+        acc = fma(q1.x, x1.x, acc);
+        acc = fma(q1.y, x1.y, acc);
+        acc = fma(q2.x, x2.x, acc);
+        acc = fma(q2.y, x2.y, acc);
+        acc = fma(q3.x, x3.x, acc);
+        acc = fma(q3.y, x3.y, acc);
+      }
+      for (; d < H; d += 32) {
+        const double2 q0 = __ldg(row + d), x0 = xs2[d];
+        acc = fma(q0.x, x0.x, acc);
+        acc = fma(q0.y, x0.y, acc);
+      }
+      acc = warp_sum(acc);
+      if (lane == 0) yout[c] = acc;
+    }
+    return;
+  }
+  const double* xs = reinterpret_cast<const double*>(xs2);
   for (int64_t c = wid; c < M; c += nw) {
     const double* row = s.coarse_inverse + c * (int64_t)M;
     double acc = 0.0;
-    for (int d = lane; d < M; d += 32) acc = fma(__ldg(row + d), __ldcg(xin + d), acc);
+    if (P.qsmem)
+      for (int d = lane; d < M; d += 32) acc = fma(__ldg(row + d), xs[d], acc);
+    else
+      for (int d = lane; d < M; d += 32) acc = fma(__ldg(row + d), __ldcg(xin + d), acc);
     acc = warp_sum(acc);
     if (lane == 0) yout[c] = acc;
   }
+}
+
+// q_i = sum_k S_ik y_k over the trace-trace ELL row of DOF i, y = z + beta p, in
+// the CSR column order (chunks of eight: the loads of a chunk are all in flight).
+__device__ __forceinline__ double ell_row(const GParams& P, int64_t i, double beta, const double* pc,
+                                          const double* z) {
+  const int64_t T = P.s.trace_size;
+  const int W = P.s.max_trace_row;
+  double qi = 0.0;
+  for (int k0 = 0; k0 < W; k0 += 8) {
+    int col[8];
+    double val[8], y[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (k0 + u < W) {
+        col[u] = P.w.ell_cols[(int64_t)(k0 + u) * T + i];
+        val[u] = P.w.ell_vals[(int64_t)(k0 + u) * T + i];
+      }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (k0 + u < W) y[u] = fma(beta, __ldcg(pc + col[u]), __ldcg(z + col[u]));
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (k0 + u < W) qi = fma(val[u], y[u], qi);
+  }
+  return qi;
+}
+
+// sum over the cell's entries e of cell_g0[e] * value(e, DOF), one warp per cell
+// (lanes over the entries, then a warp sum): the same bits in every call.
+template <class F>
+__device__ __forceinline__ double cell_reduce(const mhm_general_system& s, int64_t c, int lane, F value) {
+  const int64_t e0 = s.cell_ptr[c], e1 = s.cell_ptr[c + 1];
+  double acc = 0.0;
+  for (int64_t e = e0 + lane; e < e1; e += 32) acc = fma(s.cell_g0[e], value(e, s.cell_dofs[e]), acc);
+  return warp_sum(acc);
 }
 
 // Face block-Jacobi: z0 on the DOFs of face f from the projected residual rt - G0 v.
@@ -189,8 +283,14 @@ __device__ __forceinline__ void cell_apply(const GParams& P, int64_t c, const do
   const int t = (int)(s.cell_ptr[c + 1] - e0);
   double ra = 0.0;
   if (lane < t) {
-    const int64_t i = s.cell_dofs[e0 + lane];
-    ra = __ldcg(rt + i) - g0_apply(s, P.w.dof_g, i, v);
+    // r_i = rt_i - (G0 v)_i with the DOF's cells and entries in g0_apply's order
+    const int64_t e = e0 + lane;
+    const int64_t i = s.cell_dofs[e];
+    const int2 cc = P.w.ent_cells[e];
+    const double2 g = P.w.ent_g[e];
+    double gv = g.x * __ldcg(v + cc.x);
+    if (cc.y >= 0) gv = fma(g.y, __ldcg(v + cc.y), gv);
+    ra = __ldcg(rt + i) - gv;
   }
   const double* W = P.w.cinv + s.block_off[c];
   double acc = 0.0;
@@ -311,13 +411,18 @@ __device__ __noinline__ bool precondition(const GParams& P, const double* rt, un
   if (!g_sync(w, epoch)) return false;
   if (cellmode)
     for (int64_t i = gtid; i < T; i += gstride) w.z0[i] = dof_gather(P, i);
-  for (int64_t c = gtid; c < M; c += gstride) {
-    double acc = 0.0;
-    for (int64_t e = s.cell_ptr[c]; e < s.cell_ptr[c + 1]; ++e) {
-      const int64_t i = s.cell_dofs[e];
-      acc = fma(s.cell_g0[e], cellmode ? dof_gather(P, i) : __ldcg(w.z0 + i), acc);
+  {
+    const int lane = threadIdx.x & 31;
+    for (int64_t c = gtid >> 5; c < M; c += gstride >> 5) {
+      const double acc = cellmode ? cell_reduce(s, c, lane, [&](int64_t e, int64_t) {
+        const int2 pr = w.ent_pair[e];
+        double y = __ldcg(w.ypart + pr.x);
+        if (pr.y >= 0) y += __ldcg(w.ypart + pr.y);
+        return y;
+      })
+                                  : cell_reduce(s, c, lane, [&](int64_t, int64_t i) { return __ldcg(w.z0 + i); });
+      if (lane == 0) w.w2[c] = acc;
     }
-    w.w2[c] = acc;
   }
   return g_sync(w, epoch);
 }
@@ -346,6 +451,32 @@ __global__ void general_setup_kernel(const GParams P) {
       w.dsum[i] = d;
     }
   }
+  // the trace-trace block as column-major ELL, in CSR column order
+  const int64_t T = s.trace_size;
+  const int W = s.max_trace_row;
+  for (int64_t i = gtid; i < T; i += gstride) {
+    int k = 0;
+    for (int64_t q = s.indptr[i]; q < s.indptr[i + 1]; ++q) {
+      const int32_t j = s.indices[q];
+      if (j < T && k < W) {
+        w.ell_cols[(int64_t)k * T + i] = j;
+        w.ell_vals[(int64_t)k * T + i] = s.values[q];
+        ++k;
+      }
+    }
+    for (; k < W; ++k) {
+      w.ell_cols[(int64_t)k * T + i] = (int32_t)i;
+      w.ell_vals[(int64_t)k * T + i] = 0.0;
+    }
+  }
+  // per cell entry: its DOF's cells, G0 entries and flat entries (g0_apply's order)
+  for (int64_t e = gtid; e < s.cell_entries; e += gstride) {
+    const int64_t i = s.cell_dofs[e];
+    const int2 c = reinterpret_cast<const int2*>(s.dof_cells)[i];
+    w.ent_cells[e] = c;
+    w.ent_g[e] = make_double2(s.cell_g0[s.dof_entry[2 * i]], c.y >= 0 ? s.cell_g0[s.dof_entry[2 * i + 1]] : 0.0);
+    w.ent_pair[e] = make_int2((int)s.dof_entry[2 * i], c.y >= 0 ? (int)s.dof_entry[2 * i + 1] : -1);
+  }
   if (!cellmode)
     for (int64_t f = gtid; f < s.faces; f += gstride) face_inverse(s, (int)f, w.finv + f * kMaxFace * kMaxFace);
 }
@@ -357,20 +488,23 @@ __global__ void general_cell_inverse_kernel(const GParams P) {
   for (int64_t c = gtid >> 5; c < P.s.cells; c += nwarps) cell_inverse(P, c, threadIdx.x & 31);
 }
 
-__global__ void __launch_bounds__(kGThreads, 1) general_pcg_kernel(const GParams P) {
+// z = K0^-1 v (v = ib * isc): lambda0 = G0 Q (-v_c), projected PCG on the trace part,
+// c = Q G0^T (S lambda - v_lambda).  Returns the solve status (barrier timeouts and
+// breakdowns end it early).
+__device__ __forceinline__ int inner_solve(const GParams& P, const double* ib, double isc, double* zj, double need,
+                                        unsigned& epoch, int& total_inner) {
   __shared__ double red[32];
   __shared__ double sh[kSlots];
   const mhm_general_system& s = P.s;
   const GWork& w = P.w;
-  const int64_t T = s.trace_size, N = s.size;
+  const int64_t T = s.trace_size;
   const int M = s.cells;
   const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
-  unsigned epoch = 0;
-  int status = MHM_SOLVE_OK;
-  int total_inner = 0, outer = 0;
+  const int lane = threadIdx.x & 31;
+  const int64_t gwarp = gtid >> 5, nwarps = gstride >> 5;
   double tot[kSlots];
-  double bnorm = 0.0, res = 0.0, omega = INFINITY;
+  int status = MHM_SOLVE_OK;
 #define GSYNC()                                                              \
   do {                                                                       \
     if (!g_sync(w, epoch)) { status = MHM_SOLVE_BARRIER_TIMEOUT; goto done; } \
@@ -381,6 +515,205 @@ __global__ void __launch_bounds__(kGThreads, 1) general_pcg_kernel(const GParams
       status = MHM_SOLVE_BARRIER_TIMEOUT;                         \
       goto done;                                                  \
     }                                                             \
+  } while (0)
+  // ---- inner solve z_j = K0^-1 v_j: lambda0 = G0 Q (-v_c) ------------------------
+  for (int64_t c = gtid; c < M; c += gstride) w.w[c] = -__ldcg(ib + T + c) * isc;
+  GSYNC();
+  q_gemv(P, w.w, w.v);
+  GSYNC();
+  for (int64_t i = gtid; i < T; i += gstride) {
+    w.lam0[i] = g0_apply(s, w.dof_g, i, w.v);
+    w.mu[i] = 0.0;
+    w.p[0][i] = 0.0;
+  }
+  GSYNC();
+  // initial residual rt = v_lambda - S lambda0 (trace-trace block of K)
+  for (int64_t i = gtid; i < T; i += gstride) w.rt[0][i] = __ldcg(ib + i) * isc - ell_row(P, i, 0.0, w.lam0, w.lam0);
+  GSYNC();
+  // projection and preconditioning of the initial residual
+  for (int64_t c = gwarp; c < M; c += nwarps) {
+    const double acc = cell_reduce(s, c, lane, [&](int64_t, int64_t i) { return __ldcg(w.rt[0] + i); });
+    if (lane == 0) w.w[c] = acc;
+  }
+  GSYNC();
+  q_gemv(P, w.w, w.v);
+  GSYNC();
+  PRECONDITION(w.rt[0]);
+  q_gemv(P, w.w2, w.v2);
+  GSYNC();
+  double gamma;
+  {
+    double rz = 0.0;
+    for (int64_t i = gtid; i < T; i += gstride) {
+      const double zi = __ldcg(w.z0 + i) - g0_apply(s, w.dof_g, i, w.v2);
+      w.z[i] = zi;
+      rz = fma(__ldcg(w.r + i), zi, rz);
+    }
+    g_partial(w, 0, rz, red);
+  }
+  GSYNC();
+  g_totals(w, 1, tot, sh);
+  gamma = tot[0];
+  {
+    // stop once the preconditioned residual norm (r, z)^1/2 fell by inner_rtol, or
+    // by `need` (inexact Krylov: later steps need less)
+    const double target = fmax(P.inner_rtol, need) * sqrt(fmax(gamma, 0.0));
+    double beta = 0.0;
+    int cur = 0;
+    while (sqrt(fmax(gamma, 0.0)) > target && total_inner < P.max_inner) {
+      if (!(gamma > 0.0)) { status = MHM_SOLVE_BREAKDOWN; goto done; }
+      const int nxt = cur ^ 1;
+      // P1: direction p = z + beta p_prev, q = S p
+      {
+        double pq = 0.0;
+        for (int64_t i = gtid; i < T; i += gstride) {
+          const double pi = fma(beta, __ldcg(w.p[cur] + i), __ldcg(w.z + i));
+          const double qi = ell_row(P, i, beta, w.p[cur], w.z);
+          w.p[nxt][i] = pi;
+          w.q[i] = qi;
+          pq = fma(pi, qi, pq);
+        }
+        g_partial(w, 0, pq, red);
+      }
+      GSYNC();
+      g_totals(w, 1, tot, sh);
+      if (!(tot[0] > 0.0)) { status = isfinite(tot[0]) ? MHM_SOLVE_BREAKDOWN : MHM_SOLVE_NONFINITE; goto done; }
+      const double alpha = gamma / tot[0];
+      // P2: mu += alpha p, rt_next = rt - alpha q; the cells' G0^T rt_next
+      for (int64_t i = gtid; i < T; i += gstride) {
+        w.mu[i] = fma(alpha, __ldcg(w.p[nxt] + i), w.mu[i]);
+        w.rt[nxt][i] = fma(-alpha, __ldcg(w.q + i), __ldcg(w.rt[cur] + i));
+      }
+      for (int64_t c = gwarp; c < M; c += nwarps) {
+        const double acc = cell_reduce(s, c, lane, [&](int64_t, int64_t i) {
+          return fma(-alpha, __ldcg(w.q + i), __ldcg(w.rt[cur] + i));
+        });
+        if (lane == 0) w.w[c] = acc;
+      }
+      GSYNC();
+      // P3: v = Q G0^T rt
+      q_gemv(P, w.w, w.v);
+      GSYNC();
+      // P4: r = P rt, z0 = M^-1 r; the cells' G0^T z0 (two barriers)
+      PRECONDITION(w.rt[nxt]);
+      // P5: v2 = Q G0^T z0
+      q_gemv(P, w.w2, w.v2);
+      GSYNC();
+      // P6: z = P z0; (r, z)
+      {
+        double rz = 0.0;
+        for (int64_t i = gtid; i < T; i += gstride) {
+          const double zi = __ldcg(w.z0 + i) - g0_apply(s, w.dof_g, i, w.v2);
+          w.z[i] = zi;
+          rz = fma(__ldcg(w.r + i), zi, rz);
+        }
+        g_partial(w, 0, rz, red);
+      }
+      GSYNC();
+      g_totals(w, 1, tot, sh);
+      beta = tot[0] / gamma;
+      gamma = tot[0];
+      if (!isfinite(gamma)) { status = MHM_SOLVE_NONFINITE; goto done; }
+      cur = nxt;
+      ++total_inner;
+    }
+  }
+  // coarse unknowns c = Q G0^T (S lambda - v_lambda); z_j = (lambda0 + mu, c)
+  for (int64_t i = gtid; i < T; i += gstride) {
+    const double li = __ldcg(w.lam0 + i) + __ldcg(w.mu + i);
+    w.q[i] = ell_row(P, i, 1.0, w.mu, w.lam0) - __ldcg(ib + i) * isc;
+    zj[i] = li;
+  }
+  GSYNC();
+  for (int64_t c = gwarp; c < M; c += nwarps) {
+    const double acc = cell_reduce(s, c, lane, [&](int64_t, int64_t i) { return __ldcg(w.q + i); });
+    if (lane == 0) w.w[c] = acc;
+  }
+  GSYNC();
+  q_gemv(P, w.w, w.v);
+  GSYNC();
+  for (int64_t c = gtid; c < M; c += gstride) zj[T + c] = __ldcg(w.v + c);
+  GSYNC();
+done:
+  return status;
+#undef GSYNC
+#undef PRECONDITION
+}
+
+// u = K z_j over all rows, then classical Gram-Schmidt of u against v_0..v_j, twice
+// (v_0 scaled by 1 / beta0 on read); h[0..j] the projections, h[j+1] = ||u||, u left
+// in ku.  False when a grid barrier timed out.
+__device__ __noinline__ bool orthogonalise(const GParams& P, const double* zj, int j, double beta0, double* h,
+                                           unsigned& epoch) {
+  __shared__ double red[32];
+  __shared__ double sh[kSlots];
+  const mhm_general_system& s = P.s;
+  const GWork& w = P.w;
+  const int64_t N = s.size;
+  const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
+  double tot[kSlots];
+#define GSYNC()                          \
+  do {                                   \
+    if (!g_sync(w, epoch)) return false; \
+  } while (0)
+  // ---- u = K z_j (all rows), then classical Gram-Schmidt against v_0..v_j, twice --
+  for (int64_t i = gtid; i < N; i += gstride) {
+    double acc = 0.0;
+    for (int64_t k = s.indptr[i]; k < s.indptr[i + 1]; ++k)
+      acc = fma(s.values[k], __ldcg(zj + s.indices[k]), acc);
+    w.ku[i] = acc;
+  }
+  GSYNC();
+  for (int k = 0; k <= j + 1; ++k) h[k] = 0.0;
+  for (int pass = 0; pass < 2; ++pass) {
+    {
+      double d[kMaxKrylov];
+      for (int k = 0; k <= j; ++k) d[k] = 0.0;
+      for (int64_t i = gtid; i < N; i += gstride) {
+        const double u = __ldcg(w.ku + i);
+        for (int k = 0; k <= j; ++k) d[k] = fma(__ldcg(w.kv + (int64_t)k * N + i) * (k == 0 ? 1.0 / beta0 : 1.0), u, d[k]);
+      }
+      for (int k = 0; k <= j; ++k) g_partial(w, k, d[k], red);
+    }
+    GSYNC();
+    g_totals(w, j + 1, tot, sh);
+    for (int k = 0; k <= j; ++k) h[k] += tot[k];
+    {
+      double n2 = 0.0;
+      for (int64_t i = gtid; i < N; i += gstride) {
+        double u = __ldcg(w.ku + i);
+        for (int k = 0; k <= j; ++k)
+          u = fma(-tot[k], __ldcg(w.kv + (int64_t)k * N + i) * (k == 0 ? 1.0 / beta0 : 1.0), u);
+        w.ku[i] = u;
+        n2 = fma(u, u, n2);
+      }
+      if (pass == 1) g_partial(w, 0, n2, red);
+    }
+    GSYNC();
+  }
+  g_totals(w, 1, tot, sh);
+  h[j + 1] = sqrt(tot[0]);
+  return true;
+#undef GSYNC
+}
+
+__global__ void __launch_bounds__(kGThreads, 1) general_pcg_kernel(const GParams P) {
+  __shared__ double red[32];
+  __shared__ double sh[kSlots];
+  const mhm_general_system& s = P.s;
+  const GWork& w = P.w;
+  const int64_t N = s.size;
+  const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
+  unsigned epoch = 0;
+  int status = MHM_SOLVE_OK;
+  int total_inner = 0, outer = 0;
+  double tot[kSlots];
+  double bnorm = 0.0, res = 0.0, omega = INFINITY;
+#define GSYNC()                                                              \
+  do {                                                                       \
+    if (!g_sync(w, epoch)) { status = MHM_SOLVE_BARRIER_TIMEOUT; goto done; } \
   } while (0)
   {
     double b2 = 0.0;
@@ -398,8 +731,17 @@ __global__ void __launch_bounds__(kGThreads, 1) general_pcg_kernel(const GParams
     if (!isfinite(bnorm)) status = MHM_SOLVE_NONFINITE;
     goto done;
   }
+  // ---- flexible GMRES on K, right-preconditioned by inner solves of K0 -----------
+  // Each cycle starts from the true residual; step j solves K0 z_j = v_j by projected
+  // PCG, orthogonalises K z_j against the basis (classical Gram-Schmidt, twice) and
+  // updates the Givens-rotated least-squares problem.  Where K - K0 is at rounding
+  // level this takes the two steps the plain defect correction took; where a few
+  // cells' coupling or coarse terms differ from G0 and 0 (corrected cells), K0^-1 K
+  // is the identity plus a low-rank term and the cycle still converges.
+  __shared__ double kr[kMaxKrylov + 1][kMaxKrylov];  // R (upper triangle) of the cycle
+  __shared__ double kcs[kMaxKrylov], ksn[kMaxKrylov], kg[kMaxKrylov + 1], ky[kMaxKrylov];
   for (;;) {
-    // ---- outer residual rfull = b - K x over all rows, its norm and the componentwise
+    // ---- true residual v0 = b - K x over all rows, its norm and the componentwise
     //      backward error max_i |r_i| / (|b_i| + sum_j |K_ij| |x_j|) ----------------------
     {
       double r2 = 0.0, om = 0.0;
@@ -411,7 +753,7 @@ __global__ void __launch_bounds__(kGThreads, 1) general_pcg_kernel(const GParams
           acc = fma(-s.values[k], __ldcg(P.x + s.indices[k]), acc);
           den += fabs(t);
         }
-        w.rfull[i] = acc;
+        w.kv[i] = acc;
         r2 = fma(acc, acc, r2);
         om = fmax(om, den > 0.0 ? fabs(acc) / den : (acc != 0.0 ? INFINITY : 0.0));
       }
@@ -431,153 +773,70 @@ __global__ void __launch_bounds__(kGThreads, 1) general_pcg_kernel(const GParams
     }
     omega = tot[1];
     if (outer >= P.max_outer || total_inner >= P.max_inner) { status = MHM_SOLVE_NOT_CONVERGED; goto done; }
-    ++outer;
-    // ---- lambda0 = G0 Q (-r_c) ---------------------------------------------------
-    for (int64_t c = gtid; c < M; c += gstride) w.w[c] = -w.rfull[T + c];
-    GSYNC();
-    q_gemv(s, w.w, w.v);
-    GSYNC();
-    for (int64_t i = gtid; i < T; i += gstride) {
-      w.lam0[i] = g0_apply(s, w.dof_g, i, w.v);
-      w.mu[i] = 0.0;
-      w.p[0][i] = 0.0;
+    const double beta0 = sqrt(tot[0]);
+    if (threadIdx.x == 0) {
+      kg[0] = beta0;
+      for (int k = 1; k <= kMaxKrylov; ++k) kg[k] = 0.0;
     }
-    GSYNC();
-    // ---- initial residual rt = r_lambda - S lambda0 (trace-trace block of K) ------
-    for (int64_t i = gtid; i < T; i += gstride) {
-      double acc = w.rfull[i];
-      for (int64_t k = s.indptr[i]; k < s.indptr[i + 1]; ++k) {
-        const int64_t j = s.indices[k];
-        if (j < T) acc = fma(-s.values[k], __ldcg(w.lam0 + j), acc);
+    __syncthreads();
+    int steps = 0;
+    for (int j = 0; j < kMaxKrylov; ++j) {
+      const double* ib = w.kv + (int64_t)j * N;  // v_j (v_0 scaled by 1 / beta0 on read)
+      const double isc = j == 0 ? 1.0 / beta0 : 1.0;
+      double* zj = w.kz + (int64_t)j * N;
+      const double est = fabs(kg[j]);
+      ++outer;
+      ++steps;
+      {
+        const double need = 0.1 * fmin(P.rtol * bnorm / est, P.rtol / omega);
+        status = inner_solve(P, ib, isc, zj, need, epoch, total_inner);
+        if (status != MHM_SOLVE_OK) goto done;
       }
-      w.rt[0][i] = acc;
-    }
-    GSYNC();
-    // ---- projection and preconditioning of the initial residual ------------------
-    for (int64_t c = gtid; c < M; c += gstride) {
-      double acc = 0.0;
-      for (int64_t e = s.cell_ptr[c]; e < s.cell_ptr[c + 1]; ++e)
-        acc = fma(s.cell_g0[e], __ldcg(w.rt[0] + s.cell_dofs[e]), acc);
-      w.w[c] = acc;
-    }
-    GSYNC();
-    q_gemv(s, w.w, w.v);
-    GSYNC();
-    PRECONDITION(w.rt[0]);
-    q_gemv(s, w.w2, w.v2);
-    GSYNC();
-    double gamma, rr0;
-    {
-      double rz = 0.0, rr = 0.0;
-      for (int64_t i = gtid; i < T; i += gstride) {
-        const double zi = __ldcg(w.z0 + i) - g0_apply(s, w.dof_g, i, w.v2);
-        w.z[i] = zi;
-        const double ri = __ldcg(w.r + i);
-        rz = fma(ri, zi, rz);
-        rr = fma(ri, ri, rr);
+      double h[kMaxKrylov + 1];
+      if (!orthogonalise(P, zj, j, beta0, h, epoch)) { status = MHM_SOLVE_BARRIER_TIMEOUT; goto done; }
+      if (!isfinite(h[j + 1])) { status = MHM_SOLVE_NONFINITE; goto done; }
+      // ---- Givens rotations of the new column (every CTA, the same bits) ---------------
+      if (threadIdx.x == 0) {
+        for (int k = 0; k < j; ++k) {
+          const double a = kcs[k] * h[k] + ksn[k] * h[k + 1];
+          h[k + 1] = -ksn[k] * h[k] + kcs[k] * h[k + 1];
+          h[k] = a;
+        }
+        const double den = hypot(h[j], h[j + 1]);
+        kcs[j] = den > 0.0 ? h[j] / den : 1.0;
+        ksn[j] = den > 0.0 ? h[j + 1] / den : 0.0;
+        for (int k = 0; k < j; ++k) kr[k][j] = h[k];
+        kr[j][j] = den;
+        kg[j + 1] = -ksn[j] * kg[j];
+        kg[j] = kcs[j] * kg[j];
       }
-      g_partial(w, 0, rz, red);
-      g_partial(w, 1, rr, red);
+      __syncthreads();
+      const double next = fabs(kg[j + 1]);
+      const bool last = next <= 0.1 * P.rtol * bnorm || !(h[j + 1] > 0.0) || j + 1 == kMaxKrylov ||
+                        outer >= P.max_outer || total_inner >= P.max_inner;
+      if (!last) {
+        double* vn = w.kv + (int64_t)(j + 1) * N;
+        const double inv = 1.0 / h[j + 1];
+        for (int64_t i = gtid; i < N; i += gstride) vn[i] = __ldcg(w.ku + i) * inv;
+        GSYNC();
+        continue;
+      }
+      break;
     }
-    GSYNC();
-    g_totals(w, 2, tot, sh);
-    gamma = tot[0];
-    rr0 = tot[1];
-    {
-      // stop once the preconditioned residual norm (r, z)^1/2 fell by inner_rtol
-      const double target = P.inner_rtol * sqrt(fmax(gamma, 0.0));
-      double beta = 0.0;
-      int cur = 0;
-      double rr = rr0;
-      while (sqrt(fmax(gamma, 0.0)) > target && total_inner < P.max_inner) {
-        if (!(gamma > 0.0)) { status = MHM_SOLVE_BREAKDOWN; goto done; }
-        const int nxt = cur ^ 1;
-        // P1: direction p = z + beta p_prev, q = S p
-        {
-          double pq = 0.0;
-          for (int64_t i = gtid; i < T; i += gstride) {
-            const double pi = fma(beta, __ldcg(w.p[cur] + i), __ldcg(w.z + i));
-            double qi = 0.0;
-            for (int64_t k = s.indptr[i]; k < s.indptr[i + 1]; ++k) {
-              const int64_t j = s.indices[k];
-              if (j < T) qi = fma(s.values[k], fma(beta, __ldcg(w.p[cur] + j), __ldcg(w.z + j)), qi);
-            }
-            w.p[nxt][i] = pi;
-            w.q[i] = qi;
-            pq = fma(pi, qi, pq);
-          }
-          g_partial(w, 0, pq, red);
-        }
-        GSYNC();
-        g_totals(w, 1, tot, sh);
-        if (!(tot[0] > 0.0)) { status = isfinite(tot[0]) ? MHM_SOLVE_BREAKDOWN : MHM_SOLVE_NONFINITE; goto done; }
-        const double alpha = gamma / tot[0];
-        // P2: mu += alpha p, rt_next = rt - alpha q; the cells' G0^T rt_next
-        for (int64_t i = gtid; i < T; i += gstride) {
-          w.mu[i] = fma(alpha, __ldcg(w.p[nxt] + i), w.mu[i]);
-          w.rt[nxt][i] = fma(-alpha, __ldcg(w.q + i), __ldcg(w.rt[cur] + i));
-        }
-        for (int64_t c = gtid; c < M; c += gstride) {
-          double acc = 0.0;
-          for (int64_t e = s.cell_ptr[c]; e < s.cell_ptr[c + 1]; ++e) {
-            const int64_t i = s.cell_dofs[e];
-            acc = fma(s.cell_g0[e], fma(-alpha, __ldcg(w.q + i), __ldcg(w.rt[cur] + i)), acc);
-          }
-          w.w[c] = acc;
-        }
-        GSYNC();
-        // P3: v = Q G0^T rt
-        q_gemv(s, w.w, w.v);
-        GSYNC();
-        // P4: r = P rt, z0 = M^-1 r; the cells' G0^T z0 (two barriers)
-        PRECONDITION(w.rt[nxt]);
-        // P5: v2 = Q G0^T z0
-        q_gemv(s, w.w2, w.v2);
-        GSYNC();
-        // P6: z = P z0; (r, z) and (r, r)
-        {
-          double rz = 0.0, r2 = 0.0;
-          for (int64_t i = gtid; i < T; i += gstride) {
-            const double zi = __ldcg(w.z0 + i) - g0_apply(s, w.dof_g, i, w.v2);
-            w.z[i] = zi;
-            const double ri = __ldcg(w.r + i);
-            rz = fma(ri, zi, rz);
-            r2 = fma(ri, ri, r2);
-          }
-          g_partial(w, 0, rz, red);
-          g_partial(w, 1, r2, red);
-        }
-        GSYNC();
-        g_totals(w, 2, tot, sh);
-        beta = tot[0] / gamma;
-        gamma = tot[0];
-        rr = tot[1];
-        if (!isfinite(rr) || !isfinite(gamma)) { status = MHM_SOLVE_NONFINITE; goto done; }
-        cur = nxt;
-        ++total_inner;
+    // ---- x += Z y with R y = g (back substitution, every CTA) ------------------------
+    if (threadIdx.x == 0) {
+      for (int k = steps - 1; k >= 0; --k) {
+        double a = kg[k];
+        for (int l = k + 1; l < steps; ++l) a = fma(-kr[k][l], ky[l], a);
+        ky[k] = kr[k][k] != 0.0 ? a / kr[k][k] : 0.0;
       }
     }
-    // ---- coarse unknowns c = Q G0^T (S lambda - r_lambda), then the update -----------
-    for (int64_t i = gtid; i < T; i += gstride) {
-      double acc = -w.rfull[i];
-      for (int64_t k = s.indptr[i]; k < s.indptr[i + 1]; ++k) {
-        const int64_t j = s.indices[k];
-        if (j < T) acc = fma(s.values[k], __ldcg(w.lam0 + j) + __ldcg(w.mu + j), acc);
-      }
-      w.q[i] = acc;
+    __syncthreads();
+    for (int64_t i = gtid; i < N; i += gstride) {
+      double a = P.x[i];
+      for (int k = 0; k < steps; ++k) a = fma(ky[k], __ldcg(w.kz + (int64_t)k * N + i), a);
+      P.x[i] = a;
     }
-    GSYNC();
-    for (int64_t c = gtid; c < M; c += gstride) {
-      double acc = 0.0;
-      for (int64_t e = s.cell_ptr[c]; e < s.cell_ptr[c + 1]; ++e)
-        acc = fma(s.cell_g0[e], __ldcg(w.q + s.cell_dofs[e]), acc);
-      w.w[c] = acc;
-    }
-    GSYNC();
-    q_gemv(s, w.w, w.v);
-    GSYNC();
-    for (int64_t i = gtid; i < T; i += gstride) P.x[i] += __ldcg(w.lam0 + i) + __ldcg(w.mu + i);
-    for (int64_t c = gtid; c < M; c += gstride) P.x[T + c] += __ldcg(w.v + c);
     GSYNC();
   }
 done:
@@ -591,12 +850,11 @@ done:
     P.stats[2] = omega;
   }
 #undef GSYNC
-#undef PRECONDITION
 }
 
 struct GLayout {
-  size_t mu, rt0, rt1, p0, p1, q, r, z0, z, lam0, w, v, w2, v2, rfull, finv, dof_g, ypart, dsum, cinv, part,
-      bar, err, total;
+  size_t mu, rt0, rt1, p0, p1, q, r, z0, z, lam0, w, v, w2, v2, kv, kz, ku, finv, dof_g, ypart, dsum, cinv, ell_cols,
+      ell_vals, ent_cells, ent_g, ent_pair, part, bar, err, total;
 };
 
 GLayout g_layout(const mhm_general_system* s, int grid) {
@@ -622,12 +880,19 @@ GLayout g_layout(const mhm_general_system* s, int grid) {
   L.v = take(M * 8);
   L.w2 = take(M * 8);
   L.v2 = take(M * 8);
-  L.rfull = take(N * 8);
+  L.kv = take(N * 8 * kMaxKrylov);
+  L.kz = take(N * 8 * kMaxKrylov);
+  L.ku = take(N * 8);
   L.finv = take((size_t)s->faces * kMaxFace * kMaxFace * 8);
   L.dof_g = take(T * 2 * 8);
   L.ypart = take((size_t)s->cell_entries * 8);
   L.dsum = take(T * 8);
   L.cinv = take((size_t)(s->block_off ? s->blocks_size : 1) * 8);
+  L.ell_cols = take((size_t)s->max_trace_row * T * 4);
+  L.ell_vals = take((size_t)s->max_trace_row * T * 8);
+  L.ent_cells = take((size_t)s->cell_entries * 8);
+  L.ent_g = take((size_t)s->cell_entries * 16);
+  L.ent_pair = take((size_t)s->cell_entries * 8);
   L.part = take((size_t)grid * kSlots * 8);
   L.bar = take(2 * sizeof(unsigned));
   L.err = take(sizeof(int));
@@ -640,16 +905,27 @@ bool g_valid_layout(const mhm_general_system* s) {
   return s && s->trace_size >= 1 && s->cells >= 1 && s->size == s->trace_size + s->cells && s->faces >= 1 &&
          s->indptr && s->indices && s->face_ptr && s->cell_ptr && s->cell_dofs && s->cell_g0 && s->dof_cells &&
          s->dof_entry && s->coarse_inverse && s->max_face_size >= 1 && s->max_face_size <= kMaxFace &&
-         s->trace_size <= INT32_MAX && s->cell_entries >= 1 &&
+         s->trace_size <= INT32_MAX && s->cell_entries >= 1 && s->cell_entries <= INT32_MAX &&
+         s->max_trace_row >= 1 && s->max_trace_row <= 1024 &&
          (!s->block_off || (s->blocks_size >= 1 && s->max_cell_dofs >= 1 && s->max_cell_dofs <= 32)) &&
          (!s->cell_blocks || s->block_off);
 }
 
-int g_grid() {
+// Dynamic shared memory of the solve: the coarse vector of a Q product, when it fits.
+constexpr size_t kQSmemMax = 192 * 1024;
+size_t g_smem(const mhm_general_system* s) {
+  const size_t bytes = (size_t)s->cells * sizeof(double);
+  return bytes <= kQSmemMax ? bytes : 0;
+}
+
+int g_grid(size_t smem) {
   int dev = 0, sms = 0, per_sm = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return -1;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, general_pcg_kernel, kGThreads, 0) != cudaSuccess)
+  if (cudaFuncSetAttribute(general_pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return -1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, general_pcg_kernel, kGThreads, smem) != cudaSuccess)
     return -1;
   if (per_sm < 1) return 0;
   return sms;  // one CTA per SM: all co-resident for the cooperative launch
@@ -662,7 +938,7 @@ using namespace mhm;
 
 extern "C" int64_t mhm_general_workspace_bytes(const mhm_general_system* s) {
   if (!g_valid_layout(s)) return -1;
-  const int grid = g_grid();
+  const int grid = g_grid(g_smem(s));
   if (grid <= 0) return -1;
   return (int64_t)g_layout(s, grid).total;
 }
@@ -673,7 +949,8 @@ extern "C" int mhm_general_solve(const mhm_general_system* s, const double* rhs,
   if (!g_valid_layout(s) || !s->values || !rhs || !x || !workspace || !info || !stats || !(rtol > 0.0) || !(inner_rtol > 0.0) ||
       max_inner < 1 || max_outer < 1)
     return MHM_ERR_ARGUMENT;
-  const int grid = g_grid();
+  const size_t smem = g_smem(s);
+  const int grid = g_grid(smem);
   if (grid < 0) return MHM_ERR_LAUNCH;
   if (grid == 0) return MHM_ERR_UNSUPPORTED;
   const GLayout L = g_layout(s, grid);
@@ -697,12 +974,19 @@ extern "C" int mhm_general_solve(const mhm_general_system* s, const double* rhs,
   P.w.v = d(L.v);
   P.w.w2 = d(L.w2);
   P.w.v2 = d(L.v2);
-  P.w.rfull = d(L.rfull);
+  P.w.kv = d(L.kv);
+  P.w.kz = d(L.kz);
+  P.w.ku = d(L.ku);
   P.w.finv = d(L.finv);
   P.w.dof_g = d(L.dof_g);
   P.w.ypart = d(L.ypart);
   P.w.dsum = d(L.dsum);
   P.w.cinv = d(L.cinv);
+  P.w.ell_cols = reinterpret_cast<int32_t*>(base + L.ell_cols);
+  P.w.ell_vals = d(L.ell_vals);
+  P.w.ent_cells = reinterpret_cast<int2*>(base + L.ent_cells);
+  P.w.ent_g = reinterpret_cast<double2*>(base + L.ent_g);
+  P.w.ent_pair = reinterpret_cast<int2*>(base + L.ent_pair);
   P.w.part = d(L.part);
   P.w.bar = reinterpret_cast<unsigned*>(base + L.bar);
   P.w.err = reinterpret_cast<int*>(base + L.err);
@@ -714,11 +998,13 @@ extern "C" int mhm_general_solve(const mhm_general_system* s, const double* rhs,
   P.max_outer = max_outer;
   P.info = info;
   P.stats = stats;
+  P.qsmem = smem > 0;
+  P.qvec = (s->cells % 2 == 0) && (reinterpret_cast<uintptr_t>(s->coarse_inverse) % 16 == 0);
   if (cudaMemsetAsync(base + L.bar, 0, L.total - L.bar, st) != cudaSuccess) return MHM_ERR_LAUNCH;
   general_setup_kernel<<<grid * 2, 256, 0, st>>>(P);
   if (s->cell_blocks) general_cell_inverse_kernel<<<grid * 2, 256, 0, st>>>(P);
   void* args[] = {&P};
-  if (cudaLaunchCooperativeKernel((const void*)general_pcg_kernel, grid, kGThreads, args, 0, st) != cudaSuccess)
+  if (cudaLaunchCooperativeKernel((const void*)general_pcg_kernel, grid, kGThreads, args, smem, st) != cudaSuccess)
     return MHM_ERR_LAUNCH;
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }

@@ -128,6 +128,9 @@ class GeneralSkeleton:
         s.dof_cells, s.dof_entry = _lib.ptr(k["dof_cells"]), _lib.ptr(k["dof_entry"])
         s.coarse_inverse = _lib.ptr(k["qinv"])
         s.cell_entries = int(self.cell_ptr[-1])
+        rows = np.repeat(np.arange(self.N), np.diff(indptr))
+        trace_cols = np.asarray(indices) < self.T
+        s.max_trace_row = int(np.bincount(rows[trace_cols], minlength=self.N).max())
         widths = np.diff(self.cell_ptr)
         bofs, _ = block_offsets([np.empty(int(t)) for t in widths])
         self.block_off = bofs

@@ -44,7 +44,7 @@ def test_struct_layout_matches_header(tmp_path):
         " offsetof(mhm_skeleton_system, coarse_ay), offsetof(mhm_q1_problem, pixel_origin),"
         " offsetof(mhm_q1_problem, pixel_ny), sizeof(mhm_general_system), offsetof(mhm_general_system, cells),"
         " offsetof(mhm_general_system, coarse_inverse), offsetof(mhm_general_system, block_off),"
-        " offsetof(mhm_general_system, max_cell_dofs)); return 0;}\n")
+        " offsetof(mhm_general_system, max_trace_row)); return 0;}\n")
     exe = tmp_path / "layout"
     subprocess.run(["gcc", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
@@ -52,7 +52,7 @@ def test_struct_layout_matches_header(tmp_path):
             ctypes.sizeof(_lib.SkeletonSystem), _lib.SkeletonSystem.nx.offset, _lib.SkeletonSystem.coarse_ay.offset,
             _lib.Q1Problem.pixel_origin.offset, _lib.Q1Problem.pixel_ny.offset, ctypes.sizeof(_lib.GeneralSystem),
             _lib.GeneralSystem.cells.offset, _lib.GeneralSystem.coarse_inverse.offset,
-            _lib.GeneralSystem.block_off.offset, _lib.GeneralSystem.max_cell_dofs.offset]
+            _lib.GeneralSystem.block_off.offset, _lib.GeneralSystem.max_trace_row.offset]
     assert got == want
 
 
