@@ -387,6 +387,37 @@ def polygon_campaign(torch, steps=3, warmup=1, count=2000, cpu_cells=8, precondi
     return out
 
 
+def profile_case(torch, cube=0, count=0):
+    """One short run of the 3D or polygon workload for ncu: plan, coefficients, solves,
+    status check; returns the global solve's iterations and residual."""
+    from pymhm_b200.workloads import DiscInclusions, LayeredField, disc_inclusions, layered_lognormal_permeability
+
+    if cube:
+        from pymhm_b200.tetra import TetraMesh, TriangularSkeleton
+        from pymhm_b200.tetra_darcy import TetraP1Plan
+
+        mesh = TetraMesh.unit_cube(cube)
+        plan = TetraP1Plan(mesh, TriangularSkeleton(mesh, 1), 8)
+        plan.set_coefficients(LayeredField(layered_lognormal_permeability(40, 64, sigma=3.0, ell=0.1,
+                                                                          contrast=1e6, seed=SEED)), 1.0)
+        launches = 2
+    else:
+        from pymhm_b200.polygon import EdgeSkeleton, voronoi_mesh
+        from pymhm_b200.polygon_darcy import PolygonP2Plan, refinement_for_sizes
+
+        mesh = voronoi_mesh(count, SEED)
+        plan = PolygonP2Plan(mesh, EdgeSkeleton(mesh), refinement_for_sizes(mesh, seed=SEED + 1))
+        plan.set_coefficients(DiscInclusions(*disc_inclusions(300, rmin=0.01, rmax=0.03, seed=SEED + 2),
+                                             inside=30.0), 1.0)
+        launches = 1
+    for _ in range(launches):
+        plan.launch()
+    torch.cuda.synchronize()
+    info, stats = plan.check()
+    return {"case": f"tetra cube {cube}" if cube else f"polygon {count} cells", "launches": launches,
+            "global_iterations": int(info[1]), "inner_solves": int(info[2]), "residual": float(stats[0])}
+
+
 def serving_campaign(torch, lambdas=(100, 500, 2000), requests=150, precisions=("mixed", "fp64")):
     """Streamed serving (continuous batching with admission by HBM footprint): Poisson
     arrivals at each rate in ``lambdas``; per request a macro grid from {16, 32, 64}^2,
@@ -458,6 +489,15 @@ def parse():
     ap.add_argument("--cut-case", type=int, default=0, metavar="P",
                     help="only the 64x64 x 16x16 solve with a P x P pixel field cutting the fine cells, "
                          "mixed and FP64, two timed solves each (for ncu)")
+    ap.add_argument("--tetra-case", type=int, default=0, metavar="C",
+                    help="only two solves of the 3D workload on the unit cube split into C^3 x 6 macro tetrahedra "
+                         "(local refinement 8, the 40-layer field), for ncu")
+    ap.add_argument("--polygon-case", type=int, default=0, metavar="M",
+                    help="only one solve of the polygon workload with M Voronoi cells (P2 sizes 200-639, "
+                         "disc permeability 30), for ncu")
+    ap.add_argument("--serving-full", action="store_true",
+                    help="only the streamed-serving workload at its full size: 2000 requests at each of "
+                         "50, 100, 200, 500, 1000 and 2000 arrivals/s, mixed and FP64")
     ap.add_argument("--launch-check", action="store_true",
                     help="start the ranks, time an empty step with the barrier and max-over-ranks reduction, "
                          "print the line's rank fields and exit (no GPU work; gloo without a GPU)")
@@ -751,6 +791,17 @@ def main():
         import torch
 
         print(json.dumps({"cut_case": cut_material_campaign(torch, steps=2, pixels=args.cut_case)}))
+        return
+    if args.tetra_case or args.polygon_case:
+        import torch
+
+        print(json.dumps(profile_case(torch, args.tetra_case, args.polygon_case)))
+        return
+    if args.serving_full:
+        import torch
+
+        print(json.dumps({"serving_stream_full": serving_campaign(torch, lambdas=(50, 100, 200, 500, 1000, 2000),
+                                                                  requests=2000)}))
         return
     if launch_ranks(args):
         return

@@ -235,6 +235,15 @@ constexpr int kPanelStride = kPanel + 1;  // odd: a column of the panel spans al
 constexpr int kTile = 64;
 constexpr int kTileStride = kTile + 1;
 constexpr int kBlockedMaxN = 640;
+constexpr int kListed = 1 << 30;  // marks a listed position in the swap composition
+
+// D = A B + D on one 8 x 8 x 4 FP64 tensor-core step (fragments as documented at the
+// call site).
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
 
 // Row then column max-equilibration of A into F (cuda.py:201-211); the status of
 // zero rows / columns and non-finite entries.
@@ -294,6 +303,7 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
   __shared__ int sperm[kPanel];
   __shared__ int apos[2 * kPanel], asrc[2 * kPanel];  // rows the panel's swaps move: position <- source
   __shared__ int naff;
+  __shared__ int srcrow[kBlockedMaxN];
   const int m = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
   const size_t nn = (size_t)n * n;
   double* F = factors + nn * m;
@@ -339,16 +349,17 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
       if (d == 0.0) { st = MHM_CELL_SINGULAR_PIVOT; break; }
       const double inv = 1.0 / d;
       {
-        // warps stride the rows below the pivot; each lane forms the row's multiplier,
-        // lane 31 stores it, lane k updates panel column c + 1 + k
-        const int j = c + 1 + lane;
-        const double u = j < w ? Pn[c * kPanelStride + j] : 0.0;
-        for (int r = c + 1 + wid; r < rows; r += nw) {
+        // every (row below the pivot, panel column right of it) pair is independent:
+        // threads stride them (the multiplier l = a_rc / d formed where used), then the
+        // multipliers replace column c after a barrier
+        const int wc = w - c - 1, below = rows - c - 1;
+        for (int idx = tid; idx < below * wc; idx += blockDim.x) {
+          const int r = c + 1 + idx / wc, j = c + 1 + idx % wc;
           const double l = Pn[r * kPanelStride + c] * inv;
-          __syncwarp();
-          if (j < w) Pn[r * kPanelStride + j] = fma(-l, u, Pn[r * kPanelStride + j]);
-          if (lane == 31) Pn[r * kPanelStride + c] = l;
+          Pn[r * kPanelStride + j] = fma(-l, Pn[c * kPanelStride + j], Pn[r * kPanelStride + j]);
         }
+        __syncthreads();
+        for (int r = c + 1 + tid; r < rows; r += blockDim.x) Pn[r * kPanelStride + c] *= inv;
       }
       __syncthreads();
     }
@@ -358,29 +369,34 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
       F[(size_t)(kb + r) * n + kb + c] = Pn[r * kPanelStride + c];
     }
     for (int c = tid; c < w; c += blockDim.x) piv[(size_t)m * n + kb + c] = kb + sperm[c];
+    // compose the panel's swaps: srcrow[r] = the panel row that ends at position r; the
+    // moved positions (at most 2 w) are listed with their sources
+    for (int r = tid; r < rows; r += blockDim.x) srcrow[r] = r;
+    __syncthreads();
     if (tid == 0) {
-      // compose the panel's swaps on the rows they touch: position apos[k] receives
-      // the row that started at asrc[k] (panel-relative)
-      int cnt = 0;
       for (int c = 0; c < w; ++c) {
         const int p = sperm[c];
-        for (const int r : {c, p}) {
-          bool seen = false;
-          for (int k = 0; k < cnt; ++k) seen |= apos[k] == r;
-          if (!seen) { apos[cnt] = r; asrc[cnt] = r; ++cnt; }
+        if (p != c) {
+          const int t = srcrow[c];
+          srcrow[c] = srcrow[p];
+          srcrow[p] = t;
         }
       }
+      int cnt = 0;
+      for (int c = 0; c < w; ++c)
+        if (srcrow[c] != c) {
+          apos[cnt] = c;
+          asrc[cnt] = srcrow[c];
+          ++cnt;
+        }
       for (int c = 0; c < w; ++c) {
         const int p = sperm[c];
-        if (p == c) continue;
-        int kc = 0, kp = 0;
-        for (int k = 0; k < cnt; ++k) {
-          if (apos[k] == c) kc = k;
-          if (apos[k] == p) kp = k;
+        if (p >= w && !(srcrow[p] & kListed) && srcrow[p] != p) {
+          apos[cnt] = p;
+          asrc[cnt] = srcrow[p];
+          srcrow[p] |= kListed;
+          ++cnt;
         }
-        const int t = asrc[kc];
-        asrc[kc] = asrc[kp];
-        asrc[kp] = t;
       }
       naff = cnt;
     }
@@ -410,48 +426,46 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
     }
     __syncthreads();
     const int m2 = n - kb - w, base = kb + w;
-    const int ty = tid >> 4, tx = tid & 15;
+    // A22 -= L21 U12 on the tensor cores: 64 x 64 tiles, warp wid owns the tile's
+    // 8-row block row wid and its eight 8 x 8 blocks, FP64 mma.sync m8n8k4 over the
+    // panel's columns in steps of 4 (A = -L21 from the panel, B = U12 from Ut; columns
+    // past w are masked to 0).  Fragments: A[lane/4][lane%4], B[lane%4][lane/4],
+    // C[lane/4][2 (lane%4) + {0, 1}].
+    const int fr = lane >> 2, fc = lane & 3;
     for (int ti = 0; ti < m2; ti += kTile)
       for (int tj = 0; tj < m2; tj += kTile) {
-        double acc[4][4];  // the tile's current entries, loaded before the U12 tile is staged
+        const int i = ti + 8 * wid + fr;  // this lane's output row in the trailing block
+        double acc[8][2];                 // loaded before the U12 tile is staged
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 8; ++b)
 #pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            const int i = ti + ty * 4 + a, j = tj + tx + 16 * b;
-            acc[a][b] = (i < m2 && j < m2) ? F[(size_t)(base + i) * n + base + j] : 0.0;
+          for (int e = 0; e < 2; ++e) {
+            const int j = tj + 8 * b + 2 * fc + e;
+            acc[b][e] = (i < m2 && j < m2) ? F[(size_t)(base + i) * n + base + j] : 0.0;
           }
         for (int idx = tid; idx < w * kTile; idx += blockDim.x) {
           const int r = idx / kTile, c = idx - r * kTile;
           Ut[r * kTileStride + c] = (tj + c < m2) ? F[(size_t)(kb + r) * n + base + tj + c] : 0.0;
         }
         __syncthreads();
-        int prow[4];
+        const int prow = w + (i < m2 ? i : m2 - 1);  // panel row of L21 (clamped rows are not stored)
+        for (int q0 = 0; q0 < w; q0 += 4) {
+          const int q = q0 + fc;
+          const double av = q < w ? -Pn[prow * kPanelStride + q] : 0.0;
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          const int r = w + ti + ty * 4 + a;  // panel row of L21
-          prow[a] = r < rows ? r : rows - 1;
-        }
-        for (int q = 0; q < w; ++q) {
-          double l[4], u[4];
-#pragma unroll
-          for (int a = 0; a < 4; ++a) l[a] = Pn[prow[a] * kPanelStride + q];
-#pragma unroll
-          for (int b = 0; b < 4; ++b) u[b] = Ut[q * kTileStride + tx + 16 * b];
-#pragma unroll
-          for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) acc[a][b] = fma(-l[a], u[b], acc[a][b]);
-        }
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          const int i = ti + ty * 4 + a;
-          if (i >= m2) continue;
-#pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            const int j = tj + tx + 16 * b;
-            if (j < m2) F[(size_t)(base + i) * n + base + j] = acc[a][b];
+          for (int b = 0; b < 8; ++b) {
+            const double bv = q < w ? Ut[q * kTileStride + 8 * b + fr] : 0.0;
+            dmma_8x8x4(acc[b][0], acc[b][1], av, bv);
           }
+        }
+        if (i < m2) {
+#pragma unroll
+          for (int b = 0; b < 8; ++b)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int j = tj + 8 * b + 2 * fc + e;
+              if (j < m2) F[(size_t)(base + i) * n + base + j] = acc[b][e];
+            }
         }
         __syncthreads();
       }
@@ -510,34 +524,56 @@ __device__ void chunked_lu_solve(int n, int nrhs, const double* LU, double* W, d
         if (lane < h) W[(size_t)(i0 + lane) * nrhs + c] = v;
       }
       __syncthreads();
-      // rows beyond the chunk (below for L, above for U); the next chunk's rows also
-      // stage its diagonal block
+      // rows beyond the chunk (below for L, above for U):
+      //   W[i] -= LU[i][i0 .. i0 + h) W[i0 .. i0 + h)
+      // on the tensor cores, a warp per block of 8 rows, the chunk's columns in steps of
+      // 4 (past h masked to 0), the right-hand sides in blocks of 8 (FP64 mma.sync
+      // m8n8k4; fragments A[lane/4][lane%4], B[lane%4][lane/4], C[lane/4][2 (lane%4) +
+      // {0, 1}]).  The next chunk's diagonal block is staged beside it.
       const int r0 = lower ? i0 + h : 0, r1 = lower ? n : i0;
       const int n0 = lower ? i0 + h : i0 - 32;  // first row of the next chunk
       const int hn = lower ? min(32, n - n0) : 32;
-      for (int i = r0 + tid; i < r1; i += blockDim.x) {
-        const double* row = LU + (size_t)i * n;
-        double l[32];
+      const int fr = lane >> 2, fc = lane & 3;
+      const int ncb = (nrhs + 7) >> 3;
+      for (int rb = r0 + 8 * wid; rb < r1; rb += 8 * nw) {
+        const int i = rb + fr;
+        const bool iv = i < r1;
+        double acc[2][2];
 #pragma unroll
-        for (int sidx = 0; sidx < 32; ++sidx) l[sidx] = sidx < h ? row[i0 + sidx] : 0.0;
-        const int rn = i - n0;
-        double dn[32];
-        const bool stage = q + 1 < nchunk && rn >= 0 && rn < hn;
-        if (stage) {
+        for (int cb = 0; cb < 2; ++cb)
 #pragma unroll
-          for (int sidx = 0; sidx < 32; ++sidx) dn[sidx] = sidx < hn ? row[n0 + sidx] : 0.0;
+          for (int e = 0; e < 2; ++e) {
+            const int col = 8 * cb + 2 * fc + e;
+            acc[cb][e] = (cb < ncb && iv && col < nrhs) ? W[(size_t)i * nrhs + col] : 0.0;
+          }
+        const double* row = LU + (size_t)(iv ? i : rb) * n + i0;
+#pragma unroll
+        for (int k0 = 0; k0 < 32; k0 += 4) {
+          const int k = k0 + fc;
+          const double av = (iv && k < h) ? -row[k] : 0.0;
+#pragma unroll
+          for (int cb = 0; cb < 2; ++cb) {
+            if (cb >= ncb) break;
+            const int col = 8 * cb + fr;
+            const double bv = (k < h && col < nrhs) ? W[(size_t)(i0 + k) * nrhs + col] : 0.0;
+            dmma_8x8x4(acc[cb][0], acc[cb][1], av, bv);
+          }
         }
-        for (int c = 0; c < nrhs; ++c) {
-          double acc = 0.0;
+        if (iv) {
 #pragma unroll
-          for (int sidx = 0; sidx < 32; ++sidx) acc = fma(l[sidx], W[(size_t)(i0 + min(sidx, h - 1)) * nrhs + c], acc);
-          W[(size_t)i * nrhs + c] -= acc;
-        }
-        if (stage) {
+          for (int cb = 0; cb < 2; ++cb)
 #pragma unroll
-          for (int sidx = 0; sidx < 32; ++sidx) Dn[rn * 33 + sidx] = dn[sidx];
+            for (int e = 0; e < 2; ++e) {
+              const int col = 8 * cb + 2 * fc + e;
+              if (cb < ncb && col < nrhs) W[(size_t)i * nrhs + col] = acc[cb][e];
+            }
         }
       }
+      if (q + 1 < nchunk)
+        for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
+          const int r = idx >> 5, c = idx & 31;
+          Dn[r * 33 + c] = (r < hn && c < hn) ? LU[(size_t)(n0 + r) * n + n0 + c] : 0.0;
+        }
       __syncthreads();
       cur = 1 - cur;
     }
@@ -550,7 +586,7 @@ __device__ void chunked_lu_solve(int n, int nrhs, const double* LU, double* W, d
 // reference's columnwise max-scaled acceptance (cuda.py:230-255).
 template <int NR>
 __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
-    int n, int nrhs, const double* __restrict__ mats, const double* __restrict__ factors,
+    int n, int nrhs, int ldr, int c0, const double* __restrict__ mats, const double* __restrict__ factors,
     const int32_t* __restrict__ piv, const double* __restrict__ rs, const double* __restrict__ cs,
     const double* __restrict__ rhs, double* __restrict__ x, double rtol, double atol, int max_refine,
     int32_t* __restrict__ status) {
@@ -569,8 +605,9 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
   const double* LU = factors + nn * m;
   const double* rsc = rs + (size_t)n * m;
   const double* csc = cs + (size_t)n * m;
-  const double* B = rhs + nb * m;
-  double* Xg = x + nb * m;
+  // columns c0 .. c0 + nrhs - 1 of (n, ldr) row-major right-hand sides and solutions
+  const double* B = rhs + (size_t)n * ldr * m + c0;
+  double* Xg = x + (size_t)n * ldr * m + c0;
   if (status[m] != MHM_CELL_OK) return;
   if (tid == 0) {
     for (int i = 0; i < n; ++i) perm[i] = i;
@@ -586,22 +623,25 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
   __syncthreads();
   int nonfinite = 0;
   for (size_t idx = tid; idx < nb; idx += blockDim.x)
-    if (!isfinite(B[idx])) nonfinite = 1;
+    if (!isfinite(B[(idx / nrhs) * ldr + idx % nrhs])) nonfinite = 1;
   if (__syncthreads_or(nonfinite)) {
-    for (size_t idx = tid; idx < nb; idx += blockDim.x) Xg[idx] = B[idx];
+    for (size_t idx = tid; idx < nb; idx += blockDim.x) {
+      const size_t g = (idx / nrhs) * ldr + idx % nrhs;
+      Xg[g] = B[g];
+    }
     if (tid == 0) status[m] = MHM_CELL_NONFINITE;
     return;
   }
   // per column: max |b| and ||b / scale||^2
   for (int c = wid; c < nrhs; c += nw) {
     double bmax = 0.0;
-    for (int i = lane; i < n; i += 32) bmax = fmax(bmax, fabs(B[(size_t)i * nrhs + c]));
+    for (int i = lane; i < n; i += 32) bmax = fmax(bmax, fabs(B[(size_t)i * ldr + c]));
     bmax = warp_max(bmax);
     double scale = fmax(atol, bmax);
     if (!(scale > 0.0)) scale = 1.0;
     double b2 = 0.0;
     for (int i = lane; i < n; i += 32) {
-      const double bv = B[(size_t)i * nrhs + c] / scale;
+      const double bv = B[(size_t)i * ldr + c] / scale;
       b2 += bv * bv;
     }
     b2 = warp_sum(b2);
@@ -611,7 +651,7 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
   for (size_t idx = tid; idx < nb; idx += blockDim.x) {
     const int i = (int)(idx / nrhs), c = (int)(idx - (size_t)i * nrhs);
     const int src = perm[i];
-    W[idx] = B[(size_t)src * nrhs + c] * rsc[src];
+    W[idx] = B[(size_t)src * ldr + c] * rsc[src];
   }
   __syncthreads();
   chunked_lu_solve(n, nrhs, LU, W, Dg);
@@ -674,7 +714,7 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
         }
         if (lane == 0) {
           double sres, e;
-          two_sum(B[(size_t)i * nrhs + c], h, sres, e);
+          two_sum(B[(size_t)i * ldr + c], h, sres, e);
           const double r = sres + (e + l);
           W[(size_t)iperm[i] * nrhs + c] = r * rsc[i];
           const double rv = r / colr[c];
@@ -712,7 +752,7 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
     }
     __syncthreads();
   }
-  for (size_t idx = tid; idx < nb; idx += blockDim.x) Xg[idx] = X[idx];
+  for (size_t idx = tid; idx < nb; idx += blockDim.x) Xg[(idx / nrhs) * ldr + idx % nrhs] = X[idx];
   if (tid == 0 && result != MHM_CELL_OK) status[m] = result;
 }
 
@@ -761,21 +801,29 @@ extern "C" int mhm_batched_solve(int64_t count, int32_t n, int32_t nrhs, const d
       !col_scale || !rhs || !x || !work || !status || max_refine < 0 || !(rtol >= 0) || !(atol >= 0))
     return MHM_ERR_ARGUMENT;
   if (count > 0x7fffffff) return MHM_ERR_UNSUPPORTED;
-  const size_t smem = chunked_solve_smem(n, nrhs);
   // the residual's row prefetch covers n <= kBlockedMaxN columns
-  if (n <= kBlockedMaxN && nrhs <= 16 && smem <= 200 * 1024) {
+  // more than 16 right-hand sides: column groups of 16 (each column's acceptance is
+  // its own, and a matrix that failed in one group is skipped by the next)
+  const int group = nrhs <= 16 ? nrhs : 16;
+  if (n <= kBlockedMaxN && chunked_solve_smem(n, group) <= 200 * 1024) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    auto go = [&](auto kernel) {
-      if (smem > 48 * 1024 &&
-          cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    auto go = [&](auto kernel, int c0, int cols) {
+      const size_t sm = chunked_solve_smem(n, cols);
+      if (sm > 48 * 1024 &&
+          cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
         return MHM_ERR_LAUNCH;
-      kernel<<<(unsigned)count, kLuThreads, smem, st>>>(n, nrhs, matrices, factors, pivots, row_scale, col_scale,
-                                                        rhs, x, rtol, atol, max_refine, status);
+      kernel<<<(unsigned)count, kLuThreads, sm, st>>>(n, cols, nrhs, c0, matrices, factors, pivots, row_scale,
+                                                      col_scale, rhs, x, rtol, atol, max_refine, status);
       return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
     };
-    if (nrhs <= 4) return go(batched_solve_chunked_kernel<4>);
-    if (nrhs <= 8) return go(batched_solve_chunked_kernel<8>);
-    return go(batched_solve_chunked_kernel<16>);
+    for (int c0 = 0; c0 < nrhs; c0 += group) {
+      const int cols = nrhs - c0 < group ? nrhs - c0 : group;
+      const int rc = cols <= 4 ? go(batched_solve_chunked_kernel<4>, c0, cols)
+                     : cols <= 8 ? go(batched_solve_chunked_kernel<8>, c0, cols)
+                                 : go(batched_solve_chunked_kernel<16>, c0, cols);
+      if (rc != MHM_OK) return rc;
+    }
+    return MHM_OK;
   }
   batched_solve_kernel<<<(unsigned)count, kLuThreads, 0, static_cast<cudaStream_t>(stream)>>>(
       n, nrhs, matrices, factors, pivots, row_scale, col_scale, rhs, x, work, rtol, atol, max_refine,

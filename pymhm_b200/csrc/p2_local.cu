@@ -9,7 +9,7 @@
 // Two passes, both deterministic:
 //   p2_element_kernel  one thread per fine triangle of every cell: the 6 x 6 stiffness
 //                      sum_q w_q area kappa(x_q) grad(phi_i).grad(phi_j), mass and load;
-//   p2_dense_kernel    one thread per (cell, node): the node's rows of the dense
+//   p2_dense_kernel    one warp per (cell, node): the node's rows of the dense
 //                      stiffness and mass and its load, summing its elements in
 //                      ascending element order (the reference sums COO duplicates).
 // kappa(x) is a union of discs (value `inside`, else `outside`); a point is inside when
@@ -109,35 +109,55 @@ __global__ void p2_element_kernel(int64_t elements, const double* __restrict__ p
 // stiffness / mass start at dense_off[cell] with row length ld_of[cell] and whose load
 // starts at load_off[cell]; inc[inc_ptr[g] .. inc_ptr[g+1]) lists element * 6 + local
 // index in ascending order; elem_dofs (elements, 6) are the cell-local P2 DOFs.
-__global__ void p2_dense_kernel(int64_t nodes, const int32_t* __restrict__ node_cell,
-                                const int32_t* __restrict__ node_row, const int64_t* __restrict__ inc_ptr,
-                                const int64_t* __restrict__ inc, const int32_t* __restrict__ elem_dofs,
-                                const double* __restrict__ elem, const int64_t* __restrict__ dense_off,
-                                const int32_t* __restrict__ ld_of, const int64_t* __restrict__ load_off,
-                                double* __restrict__ stiffness, double* __restrict__ mass,
-                                double* __restrict__ load) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < nodes; g += stride) {
+// A warp per node: the two rows are built in shared memory (rows up to kMaxRow; longer
+// rows directly in global memory), element by element in ascending order, lanes 0..5
+// adding one element's six (distinct) columns, then written out coalesced.
+constexpr int kDenseWarps = 8;
+constexpr int kMaxRow = 640;
+
+__global__ void __launch_bounds__(kDenseWarps * 32) p2_dense_kernel(
+    int64_t nodes, const int32_t* __restrict__ node_cell, const int32_t* __restrict__ node_row,
+    const int64_t* __restrict__ inc_ptr, const int64_t* __restrict__ inc, const int32_t* __restrict__ elem_dofs,
+    const double* __restrict__ elem, const int64_t* __restrict__ dense_off, const int32_t* __restrict__ ld_of,
+    const int64_t* __restrict__ load_off, double* __restrict__ stiffness, double* __restrict__ mass,
+    double* __restrict__ load) {
+  extern __shared__ double rows_smem[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double* sA = rows_smem + (size_t)wid * 2 * kMaxRow;
+  double* sM = sA + kMaxRow;
+  const int64_t nwarps = (int64_t)gridDim.x * kDenseWarps;
+  for (int64_t g = (int64_t)blockIdx.x * kDenseWarps + wid; g < nodes; g += nwarps) {
     const int c = node_cell[g], i = node_row[g], ld = ld_of[c];
-    double* A = stiffness + dense_off[c] + (int64_t)i * ld;
-    double* Mm = mass + dense_off[c] + (int64_t)i * ld;
-    for (int j = 0; j < ld; ++j) {
+    double* gA = stiffness + dense_off[c] + (int64_t)i * ld;
+    double* gM = mass + dense_off[c] + (int64_t)i * ld;
+    const bool staged = ld <= kMaxRow;
+    double* A = staged ? sA : gA;
+    double* Mm = staged ? sM : gM;
+    for (int j = lane; j < ld; j += 32) {
       A[j] = 0.0;
       Mm[j] = 0.0;
     }
+    __syncwarp();
     double f = 0.0;
     for (int64_t k = inc_ptr[g]; k < inc_ptr[g + 1]; ++k) {
       const int64_t e = inc[k] / 6;
       const int a = (int)(inc[k] - e * 6);
       const double* el = elem + e * kElemStride;
-      for (int b = 0; b < 6; ++b) {
-        const int j = elem_dofs[6 * e + b];
-        A[j] += el[a * 6 + b];
-        Mm[j] += el[36 + a * 6 + b];
+      if (lane < 6) {
+        const int j = elem_dofs[6 * e + lane];
+        A[j] += el[a * 6 + lane];
+        Mm[j] += el[36 + a * 6 + lane];
       }
       f += el[72 + a];
+      __syncwarp();
     }
-    load[load_off[c] + i] = f;
+    if (staged)
+      for (int j = lane; j < ld; j += 32) {
+        gA[j] = sA[j];
+        gM[j] = sM[j];
+      }
+    if (lane == 0) load[load_off[c] + i] = f;
+    __syncwarp();
   }
 }
 
@@ -174,8 +194,13 @@ extern "C" int mhm_p2_assemble(int64_t elements, const double* points, const int
   p2_element_kernel<<<blocks_for(elements), 256, 0, st>>>(elements, points, triangles, nquad, quad_bary,
                                                           quad_weights, grid, grid_ptr, grid_discs, centres, radii2,
                                                           inside, outside, source, element_scratch);
-  p2_dense_kernel<<<blocks_for(nodes), 256, 0, st>>>(nodes, node_cell, node_row, inc_ptr, inc, elem_dofs,
-                                                     element_scratch, dense_off, ld_of, load_off, stiffness, mass,
-                                                     load);
+  const size_t smem = (size_t)kDenseWarps * 2 * kMaxRow * sizeof(double);
+  if (cudaFuncSetAttribute(p2_dense_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return MHM_ERR_LAUNCH;
+  int64_t dblocks = (nodes + kDenseWarps - 1) / kDenseWarps;
+  if (dblocks > 148 * 16) dblocks = 148 * 16;
+  p2_dense_kernel<<<(unsigned)dblocks, kDenseWarps * 32, smem, st>>>(nodes, node_cell, node_row, inc_ptr, inc,
+                                                                     elem_dofs, element_scratch, dense_off, ld_of,
+                                                                     load_off, stiffness, mass, load);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }

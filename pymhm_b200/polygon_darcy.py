@@ -100,8 +100,8 @@ class PolygonP2Plan:
     refinement): local meshes, couplings, bins, sparsity and every buffer."""
 
     def __init__(self, mesh: PolygonMesh, skeleton: EdgeSkeleton | None = None, refinements=2, *, order=4,
-                 bin_width=32, device=None, global_rtol=1e-13, inner_rtol=1e-10, max_inner=20000, max_outer=8,
-                 preconditioner="cell"):
+                 bin_width=32, streams=4, device=None, global_rtol=1e-13, inner_rtol=1e-10, max_inner=20000,
+                 max_outer=8, preconditioner="cell"):
         import torch
 
         self.torch = torch
@@ -129,6 +129,40 @@ class PolygonP2Plan:
         if self.t_cells.max() > 28:
             raise NotImplementedError("at most 28 trace DOFs per cell")
         couplings = [p2_trace_coupling(mesh, c, fines[c], sk) for c in range(M)]
+        self.nodes = int(sum(self.n_cells))
+        # ---- skeleton reduction and global solve -------------------------------------
+        self.cell_dofs_list = cell_dofs
+        self.pattern = skeleton_pattern_ragged(cell_dofs, self.T)
+        bofs, lofs = block_offsets(cell_dofs)
+        flat_dofs = np.concatenate(cell_dofs)
+        dofs_off = np.r_[0, np.cumsum(self.t_cells)][:-1]
+        field_off = np.r_[0, np.cumsum(self.n_cells)][:-1]
+        self.field_off_h = np.r_[field_off, self.nodes]
+        self.general = GeneralSkeleton(cell_dofs, [sk.geometric_constraint(c) for c in range(M)], sk.offsets,
+                                       self.T, self.pattern.indptr, self.pattern.indices, device=self.device)
+        self._quad = triangle_rule(max(int(order), 4))
+        self._fines, self._spaces, self._couplings = fines, spaces, couplings
+        self._offsets = (bofs, lofs, flat_dofs, dofs_off, field_off)
+        self.field = None
+        self.source = 0.0
+        self.streams = max(1, int(streams))
+        self._layout(int(bin_width))
+
+    def _layout(self, bin_width: int):
+        """Bins by padded augmented size (n + 1 rounded up to a multiple of ``bin_width``),
+        the flattened elements and node incidences in bin order, and every buffer whose
+        layout follows the bins."""
+        torch = self.torch
+        M, dev = self.M, self.device
+        fines, spaces, couplings = self._fines, self._spaces, self._couplings
+        bofs, lofs, flat_dofs, dofs_off, field_off = self._offsets
+        qbary, qw = self._quad
+        f64 = dict(dtype=torch.float64, device=dev)
+
+        def up(a, dtype):
+            return torch.as_tensor(np.array(a, order="C", copy=True), dtype=dtype).to(dev)
+
+        self.bin_width = bin_width
         # ---- bins by padded augmented size -------------------------------------------
         nb_c = ((self.n_cells + 1 + bin_width - 1) // bin_width) * bin_width
         nb_c = np.minimum(nb_c, MAX_AUGMENTED)
@@ -179,24 +213,7 @@ class PolygonP2Plan:
                 node_row.append(np.arange(n, dtype=np.int32))
                 p_base += len(fine.points)
                 e_base += len(dofs)
-        self.elements, self.nodes = e_base, int(sum(self.n_cells))
-        # ---- skeleton reduction and global solve -------------------------------------
-        self.cell_dofs_list = cell_dofs
-        self.pattern = skeleton_pattern_ragged(cell_dofs, self.T)
-        bofs, lofs = block_offsets(cell_dofs)
-        flat_dofs = np.concatenate(cell_dofs)
-        dofs_off = np.r_[0, np.cumsum(self.t_cells)][:-1]
-        field_off = np.r_[0, np.cumsum(self.n_cells)][:-1]
-        self.field_off_h = np.r_[field_off, self.nodes]
-        self.general = GeneralSkeleton(cell_dofs, [sk.geometric_constraint(c) for c in range(M)], sk.offsets,
-                                       self.T, self.pattern.indptr, self.pattern.indices, device=self.device)
-        qbary, qw = triangle_rule(max(int(order), 4))
-        dev = self.device
-        f64 = dict(dtype=torch.float64, device=dev)
-
-        def up(a, dtype):
-            return torch.as_tensor(np.array(a, order="C", copy=True), dtype=dtype).to(dev)
-
+        self.elements = e_base
         # per bin-order slot: sizes and output offsets
         o = self.order
         self.d = dict(
@@ -236,6 +253,7 @@ class PolygonP2Plan:
         self.col_scale = torch.empty(vec_base, **f64)
         self.corrected = torch.empty(M, dtype=torch.uint8, device=dev)
         self.cell_status = torch.empty(M, dtype=torch.int32, device=dev)
+        self.bin_streams = [torch.cuda.Stream(device=dev) for _ in range(min(self.streams, len(self.bins)))]
         self.factor_status = torch.empty(M, dtype=torch.int32, device=dev)
         self.solve_status = torch.empty(M, dtype=torch.int32, device=dev)
         self.blocks = torch.empty(int(bofs[-1]), **f64)
@@ -246,8 +264,41 @@ class PolygonP2Plan:
         self.d_boundary = torch.zeros(self.T, **f64)
         self.x = torch.empty(self.N, **f64)
         self.fields = torch.empty(self.nodes, **f64)
-        self.field = None
-        self.source = 0.0
+
+    def autotune(self, permeability=1.0, source=0.0, *, widths=(16, 32, 64, 128), streams=(1, 4), repeats=2,
+                 cache=None):
+        """Choose the bin width and the number of bin streams by timing the local stage
+        (CUDA events, after one warm-up launch per candidate) on this device, keep the
+        fastest layout and return the choice with every timing.  ``cache``: a JSON file
+        recording choices per device and size signature (``autotune.choose``)."""
+        from . import autotune as at
+
+        torch = self.torch
+        self.set_coefficients(permeability, source)
+        cands = [(int(w), int(k)) for w in widths for k in streams if int(w) >= 8 and int(k) >= 1]
+
+        def measure(c):
+            w, k = c
+            if (w, k) != (self.bin_width, self.streams):
+                self.streams = k
+                self._layout(w)
+            st = torch.cuda.current_stream()
+            self.launch(st)
+            times = []
+            for _ in range(repeats):
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+                self.launch(st, events=ev)
+                torch.cuda.synchronize()
+                times.append(ev[0].elapsed_time(ev[1]))
+            self.check()
+            return float(np.median(times))
+
+        key = at.shape_key(torch.cuda.get_device_name(self.device), self.n_cells, self.t_cells)
+        best, info = at.choose(cands, measure, key=key, cache=cache)
+        if tuple(best) != (self.bin_width, self.streams):
+            self.streams = int(best[1])
+            self._layout(int(best[0]))
+        return {"bin_width": self.bin_width, "streams": self.streams, **info}
 
     def set_coefficients(self, permeability=1.0, source=0.0):
         """A ``DiscInclusions`` field or a positive constant permeability; a constant source."""
@@ -307,24 +358,38 @@ class PolygonP2Plan:
                                        self.nodes, P(d["node_cell"]), P(d["node_row"]), P(d["inc_ptr"]), P(d["inc"]),
                                        P(d["edofs"]), P(d["dense_off"]), P(d["ld_of"]), P(d["load_off"]),
                                        P(self.stiffness), P(self.mass), P(self.load), sh), "mhm_p2_assemble")
-        for b in self.bins:
+        # the bins' chains are independent until the scatter: fork them over side
+        # streams (largest bins first) so that one bin's last wave overlaps the next's
+        fork = torch.cuda.Event()
+        fork.record(st)
+        used = []
+        for idx, b in enumerate(reversed(self.bins)):
+            bs = self.bin_streams[idx % len(self.bin_streams)]
+            if idx < len(self.bin_streams):
+                bs.wait_event(fork)
+                used.append(bs)
+            shb = _lib.stream_handle(bs)
             v = self._bin_views(b)
             k, nb, w, tld = b["k"], b["nb"], b["w"], b["tld"]
             _lib.check(lib.mhm_dense_systems(k, nb, tld, nb, w, 1, P(v["n_of"]), P(v["t_of"]), P(v["stiffness"]),
                                              P(v["mass"]), P(v["load"]), P(v["coupling"]), P(v["aug"]), P(v["rhs"]),
-                                             P(v["action"]), P(v["corrected"]), P(v["cell_status"]), sh),
+                                             P(v["action"]), P(v["corrected"]), P(v["cell_status"]), shb),
                        "mhm_dense_systems")
             _lib.check(lib.mhm_batched_factor(k, nb, P(v["aug"]), P(v["factors"]), P(v["pivots"]), P(v["rs"]),
-                                              P(v["cs"]), P(v["factor_status"]), sh), "mhm_batched_factor")
-            with torch.cuda.stream(st):
+                                              P(v["cs"]), P(v["factor_status"]), shb), "mhm_batched_factor")
+            with torch.cuda.stream(bs):
                 v["solve_status"].copy_(v["factor_status"])
             _lib.check(lib.mhm_batched_solve(k, nb, w, P(v["aug"]), P(v["factors"]), P(v["pivots"]), P(v["rs"]),
                                              P(v["cs"]), P(v["rhs"]), P(v["solution"]), P(v["work"]), 1e-10, 0.0,
-                                             2, P(v["solve_status"]), sh), "mhm_batched_solve")
+                                             2, P(v["solve_status"]), shb), "mhm_batched_solve")
             _lib.check(lib.mhm_dense_contributions(k, nb, tld, nb, w, tld, P(v["n_of"]), P(v["t_of"]),
                                                    P(v["solution"]), P(v["coupling"]), P(v["action"]),
                                                    P(v["load"]), P(v["block_off"]), P(v["lofs"]), P(self.blocks),
-                                                   P(self.loads), sh), "mhm_dense_contributions")
+                                                   P(self.loads), shb), "mhm_dense_contributions")
+        for bs in used:
+            join = torch.cuda.Event()
+            join.record(bs)
+            st.wait_event(join)
         mark(1)
         p = self.pattern
         _lib.check(lib.mhm_skeleton_scatter(len(p.indices), P(d["slot_ptr"]), P(d["contrib"]), P(self.blocks),

@@ -112,3 +112,27 @@ def test_polygon_preconditioners_agree():
     assert rel(sols["cell"].trace, sols["face"].trace) <= 1e-11
     assert rel(np.concatenate(sols["cell"].fields), np.concatenate(sols["face"].fields)) <= 1e-11
     assert sols["cell"].global_iterations < sols["face"].global_iterations
+
+
+def test_polygon_autotune_keeps_the_solution(tmp_path):
+    """The autotuner's choice (bin width, bin streams) changes the schedule only: the
+    solution equals the default layout's to rounding, and a cached choice is replayed."""
+    from pymhm_b200.polygon import EdgeSkeleton, voronoi_mesh
+    from pymhm_b200.polygon_darcy import PolygonP2Plan
+    from pymhm_b200.workloads import DiscInclusions, disc_inclusions
+
+    mesh = voronoi_mesh(80, 23)
+    sk = EdgeSkeleton(mesh)
+    rs = np.random.default_rng(23).integers(2, 5, size=80)
+    field = DiscInclusions(*disc_inclusions(40, rmin=0.01, rmax=0.03, seed=24), inside=30.0)
+    ref = PolygonP2Plan(mesh, sk, rs).solve(field, 1.0)
+    plan = PolygonP2Plan(mesh, sk, rs)
+    cache = tmp_path / "tune.json"
+    out = plan.autotune(field, 1.0, widths=(16, 64), streams=(1, 2), cache=cache)
+    assert (out["bin_width"], out["streams"]) in {(16, 1), (16, 2), (64, 1), (64, 2)}
+    assert len(out["timings_ms"]) == 4 and not out["cached"]
+    sol = plan.solve(field, 1.0)
+    assert rel(sol.trace, ref.trace) <= 1e-11
+    assert rel(np.concatenate(sol.fields), np.concatenate(ref.fields)) <= 1e-11
+    again = PolygonP2Plan(mesh, sk, rs).autotune(field, 1.0, widths=(16, 64), streams=(1, 2), cache=cache)
+    assert again["cached"] and (again["bin_width"], again["streams"]) == (out["bin_width"], out["streams"])
