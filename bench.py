@@ -314,9 +314,9 @@ def tetra_campaign(torch, steps=5, warmup=2, cube=8, local=8, cpu_cells=16, prec
 def polygon_campaign(torch, steps=3, warmup=1, count=2000, cpu_cells=8, preconditioner="cell", inside=30.0,
                      contract_inside=1e4):
     """Polygonal P2 Darcy (config 3 at local sizes up to 639): the Voronoi cells of
-    2000 seeded points in the unit square, each refined with its own subdivision count
-    so that its P2 space has a size drawn uniformly in [200, 639] (the batched LU's
-    blocked range; the configuration's 640-3000 sizes are not built), one Legendre P1
+    2000 seeded points in the unit square, each refined with the largest subdivision
+    count whose P2 space stays within a size drawn uniformly in [200, 639] (the batched
+    LU's blocked range; the configuration's 640-3000 sizes are not built), one Legendre P1
     face space per edge (4-10 edges, 8-20 trace DOFs per cell), 300 seeded discs of
     radius 0.01-0.03 with permeability ``inside`` in a background of 1, f = 1,
     homogeneous Dirichlet data, FP64.  One solve at a time with CUDA events per stage;

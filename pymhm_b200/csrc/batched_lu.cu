@@ -232,8 +232,6 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_kernel(
 
 constexpr int kPanel = 32;
 constexpr int kPanelStride = kPanel + 1;  // odd: a column of the panel spans all banks
-constexpr int kTile = 64;
-constexpr int kTileStride = kTile + 1;
 constexpr int kBlockedMaxN = 640;
 constexpr int kListed = 1 << 30;  // marks a listed position in the swap composition
 
@@ -250,18 +248,21 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
 __device__ int equilibrate(int n, const double* A, double* F, double* rsc, double* csc) {
   int st = MHM_CELL_OK;
   const int tid = threadIdx.x;
-  const size_t nn = (size_t)n * n;
   int zero_row = 0, nonfinite = 0;
-  for (int i = tid; i < n; i += blockDim.x) {
+  // row maxima: a warp per row, lanes over the columns (coalesced)
+  const int lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  for (int i = wid; i < n; i += nw) {
     double mx = 0.0;
-#pragma unroll 8
-    for (int j = 0; j < n; ++j) {
+    for (int j = lane; j < n; j += 32) {
       const double v = A[(size_t)i * n + j];
       if (!isfinite(v)) nonfinite = 1;
       mx = fmax(mx, fabs(v));
     }
-    if (mx == 0.0) zero_row = 1;
-    rsc[i] = (mx > 0.0) ? 1.0 / mx : 0.0;
+    mx = warp_max(mx);
+    if (lane == 0) {
+      if (mx == 0.0) zero_row = 1;
+      rsc[i] = (mx > 0.0) ? 1.0 / mx : 0.0;
+    }
   }
   nonfinite = __syncthreads_or(nonfinite);
   zero_row = __syncthreads_or(zero_row);
@@ -277,9 +278,10 @@ __device__ int equilibrate(int n, const double* A, double* F, double* rsc, doubl
   }
   zero_col = __syncthreads_or(zero_col);
   if (st == MHM_CELL_OK && zero_col) st = MHM_CELL_ZERO_COLUMN;
-  for (size_t idx = tid; idx < nn; idx += blockDim.x) {
-    const int i = (int)(idx / n), j = (int)(idx % n);
-    F[idx] = A[idx] * rsc[i] * csc[j];
+  // a warp per row (no index division)
+  for (int i = wid; i < n; i += nw) {
+    const double ri = rsc[i];
+    for (int j = lane; j < n; j += 32) F[(size_t)i * n + j] = A[(size_t)i * n + j] * ri * csc[j];
   }
   __syncthreads();
   return st;
@@ -289,14 +291,13 @@ __device__ int equilibrate(int n, const double* A, double* F, double* rsc, doubl
 // (32 < n <= 640).  Per panel of 32 columns: (a) the panel rows kb..n-1 are factored
 // in shared memory, pivots by first maximum as the unblocked kernel; (b) the panel's
 // row swaps are applied to the other columns, a thread per column, in order;
-// (c) U12 = L11^-1 A12, a thread per column; (d) A22 -= L21 U12 in 64 x 64 tiles,
-// 4 x 4 outputs per thread.
+// (c) U12 = L11^-1 A12, a thread per column; (d) A22 -= L21 U12 on the FP64 tensor
+// cores, a warp per 8-row block, without a CTA barrier inside.
 __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
     int n, const double* __restrict__ mats, double* __restrict__ factors, int32_t* __restrict__ piv,
     double* __restrict__ rs, double* __restrict__ cs, int32_t* __restrict__ status) {
   extern __shared__ __align__(16) double sm[];
   double* Pn = sm;                                   // (n, kPanelStride) panel
-  double* Ut = Pn + (size_t)n * kPanelStride;        // (kPanel, kTileStride) U12 tile
   __shared__ double red[32];
   __shared__ double wbest[32];
   __shared__ int wrow[32];
@@ -310,10 +311,8 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
   int st = equilibrate(n, mats + nn * m, F, rs + (size_t)n * m, cs + (size_t)n * m);
   for (int kb = 0; kb < n && st == MHM_CELL_OK; kb += kPanel) {
     const int w = min(kPanel, n - kb), rows = n - kb;
-    for (int idx = tid; idx < rows * w; idx += blockDim.x) {
-      const int r = idx / w, c = idx - r * w;
-      Pn[r * kPanelStride + c] = F[(size_t)(kb + r) * n + kb + c];
-    }
+    for (int r = wid; r < rows; r += nw)
+      if (lane < w) Pn[r * kPanelStride + lane] = F[(size_t)(kb + r) * n + kb + lane];
     __syncthreads();
     for (int c = 0; c < w; ++c) {
       double best = -1.0;
@@ -349,14 +348,27 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
       if (d == 0.0) { st = MHM_CELL_SINGULAR_PIVOT; break; }
       const double inv = 1.0 / d;
       {
-        // every (row below the pivot, panel column right of it) pair is independent:
-        // threads stride them (the multiplier l = a_rc / d formed where used), then the
-        // multipliers replace column c after a barrier
-        const int wc = w - c - 1, below = rows - c - 1;
-        for (int idx = tid; idx < below * wc; idx += blockDim.x) {
-          const int r = c + 1 + idx / wc, j = c + 1 + idx % wc;
-          const double l = Pn[r * kPanelStride + c] * inv;
-          Pn[r * kPanelStride + j] = fma(-l, Pn[c * kPanelStride + j], Pn[r * kPanelStride + j]);
+        // every (row below the pivot, panel column right of it) pair is independent (the
+        // multiplier l = a_rc / d formed where used); the multipliers replace column c
+        // after a barrier
+        // a warp per row, a lane per panel column; four rows' loads before their stores
+        const int j = c + 1 + lane;
+        const bool jv = j < w;
+        const double u = jv ? Pn[c * kPanelStride + j] : 0.0;
+        for (int r = c + 1 + wid; r < rows; r += 4 * nw) {
+          double l[4], a[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const int rk = r + k * nw;
+            const bool ok = rk < rows && jv;
+            l[k] = ok ? Pn[rk * kPanelStride + c] * inv : 0.0;
+            a[k] = ok ? Pn[rk * kPanelStride + j] : 0.0;
+          }
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const int rk = r + k * nw;
+            if (rk < rows && jv) Pn[rk * kPanelStride + j] = fma(-l[k], u, a[k]);
+          }
         }
         __syncthreads();
         for (int r = c + 1 + tid; r < rows; r += blockDim.x) Pn[r * kPanelStride + c] *= inv;
@@ -364,10 +376,8 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
       __syncthreads();
     }
     if (st != MHM_CELL_OK) break;
-    for (int idx = tid; idx < rows * w; idx += blockDim.x) {
-      const int r = idx / w, c = idx - r * w;
-      F[(size_t)(kb + r) * n + kb + c] = Pn[r * kPanelStride + c];
-    }
+    for (int r = wid; r < rows; r += nw)
+      if (lane < w) F[(size_t)(kb + r) * n + kb + lane] = Pn[r * kPanelStride + lane];
     for (int c = tid; c < w; c += blockDim.x) piv[(size_t)m * n + kb + c] = kb + sperm[c];
     // compose the panel's swaps: srcrow[r] = the panel row that ends at position r; the
     // moved positions (at most 2 w) are listed with their sources
@@ -426,16 +436,37 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
     }
     __syncthreads();
     const int m2 = n - kb - w, base = kb + w;
-    // A22 -= L21 U12 on the tensor cores: 64 x 64 tiles, warp wid owns the tile's
-    // 8-row block row wid and its eight 8 x 8 blocks, FP64 mma.sync m8n8k4 over the
-    // panel's columns in steps of 4 (A = -L21 from the panel, B = U12 from Ut; columns
-    // past w are masked to 0).  Fragments: A[lane/4][lane%4], B[lane%4][lane/4],
-    // C[lane/4][2 (lane%4) + {0, 1}].
+    // A22 -= L21 U12 on the tensor cores with no CTA barrier inside: warp wid takes the
+    // 8-row blocks wid, wid + nw, ... of the trailing matrix and walks its columns in
+    // blocks of 64 (eight 8 x 8 outputs, FP64 mma.sync m8n8k4 over the panel's columns
+    // in steps of 4).  A = -L21 comes from the panel in shared memory once per row
+    // block; all B = U12 fragments of a column block are loaded from global memory (L2)
+    // before its tensor-core steps, so their latency is paid once.  Fragments:
+    // A[lane/4][lane%4], B[lane%4][lane/4], C[lane/4][2 (lane%4) + {0, 1}]; panel
+    // columns past w are masked to 0.
     const int fr = lane >> 2, fc = lane & 3;
-    for (int ti = 0; ti < m2; ti += kTile)
-      for (int tj = 0; tj < m2; tj += kTile) {
-        const int i = ti + 8 * wid + fr;  // this lane's output row in the trailing block
-        double acc[8][2];                 // loaded before the U12 tile is staged
+    const int ksteps = (w + 3) >> 2;
+    for (int rb = 8 * wid; rb < m2; rb += 8 * nw) {
+      const int i = rb + fr;  // this lane's A / C row in the trailing block
+      const int prow = w + (i < m2 ? i : m2 - 1);  // panel row of L21 (clamped rows are not stored)
+      double av[kPanel / 4];
+#pragma unroll
+      for (int s = 0; s < kPanel / 4; ++s) {
+        const int q = 4 * s + fc;
+        av[s] = q < w ? -Pn[prow * kPanelStride + q] : 0.0;
+      }
+      for (int tj = 0; tj < m2; tj += 64) {
+        double bv[kPanel / 4][8];
+#pragma unroll
+        for (int s = 0; s < kPanel / 4; ++s) {
+          const int q = 4 * s + fc;
+#pragma unroll
+          for (int b = 0; b < 8; ++b) {
+            const int col = tj + 8 * b + fr;
+            bv[s][b] = (q < w && col < m2) ? F[(size_t)(kb + q) * n + base + col] : 0.0;
+          }
+        }
+        double acc[8][2];
 #pragma unroll
         for (int b = 0; b < 8; ++b)
 #pragma unroll
@@ -443,20 +474,11 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
             const int j = tj + 8 * b + 2 * fc + e;
             acc[b][e] = (i < m2 && j < m2) ? F[(size_t)(base + i) * n + base + j] : 0.0;
           }
-        for (int idx = tid; idx < w * kTile; idx += blockDim.x) {
-          const int r = idx / kTile, c = idx - r * kTile;
-          Ut[r * kTileStride + c] = (tj + c < m2) ? F[(size_t)(kb + r) * n + base + tj + c] : 0.0;
-        }
-        __syncthreads();
-        const int prow = w + (i < m2 ? i : m2 - 1);  // panel row of L21 (clamped rows are not stored)
-        for (int q0 = 0; q0 < w; q0 += 4) {
-          const int q = q0 + fc;
-          const double av = q < w ? -Pn[prow * kPanelStride + q] : 0.0;
 #pragma unroll
-          for (int b = 0; b < 8; ++b) {
-            const double bv = q < w ? Ut[q * kTileStride + 8 * b + fr] : 0.0;
-            dmma_8x8x4(acc[b][0], acc[b][1], av, bv);
-          }
+        for (int s = 0; s < kPanel / 4; ++s) {
+          if (s >= ksteps) break;
+#pragma unroll
+          for (int b = 0; b < 8; ++b) dmma_8x8x4(acc[b][0], acc[b][1], av[s], bv[s][b]);
         }
         if (i < m2) {
 #pragma unroll
@@ -467,8 +489,9 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
               if (j < m2) F[(size_t)(base + i) * n + base + j] = acc[b][e];
             }
         }
-        __syncthreads();
       }
+    }
+    __syncthreads();
   }
   if (st == MHM_CELL_OK) {
     double dmin = 1e300, amax = 0.0;
@@ -488,7 +511,8 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
 // 32 factor entries times the chunk's solution, a thread per row with the 32
 // loads issued together.  The threads whose rows form the next chunk also load
 // that chunk's diagonal block (into the other half of Dg) in the same pass.
-__device__ void chunked_lu_solve(int n, int nrhs, const double* LU, double* W, double* Dg) {
+// W (n, nrhs) with row stride ws.
+__device__ void chunked_lu_solve(int n, int nrhs, int ws, const double* LU, double* W, double* Dg) {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
   const int nchunk = (n + 31) / 32;
   for (int dir = 0; dir < 2; ++dir) {
@@ -508,7 +532,7 @@ __device__ void chunked_lu_solve(int n, int nrhs, const double* LU, double* W, d
       const double* D = Dg + cur * 32 * 33;
       double* Dn = Dg + (1 - cur) * 32 * 33;
       for (int c = wid; c < nrhs; c += nw) {
-        double v = lane < h ? W[(size_t)(i0 + lane) * nrhs + c] : 0.0;
+        double v = lane < h ? W[(size_t)(i0 + lane) * ws + c] : 0.0;
         if (lower) {
           for (int sidx = 0; sidx < h; ++sidx) {
             const double xs = __shfl_sync(0xffffffffu, v, sidx);
@@ -521,7 +545,7 @@ __device__ void chunked_lu_solve(int n, int nrhs, const double* LU, double* W, d
             if (lane < sidx) v = fma(-D[lane * 33 + sidx], xs, v);
           }
         }
-        if (lane < h) W[(size_t)(i0 + lane) * nrhs + c] = v;
+        if (lane < h) W[(size_t)(i0 + lane) * ws + c] = v;
       }
       __syncthreads();
       // rows beyond the chunk (below for L, above for U):
@@ -544,7 +568,7 @@ __device__ void chunked_lu_solve(int n, int nrhs, const double* LU, double* W, d
 #pragma unroll
           for (int e = 0; e < 2; ++e) {
             const int col = 8 * cb + 2 * fc + e;
-            acc[cb][e] = (cb < ncb && iv && col < nrhs) ? W[(size_t)i * nrhs + col] : 0.0;
+            acc[cb][e] = (cb < ncb && iv && col < nrhs) ? W[(size_t)i * ws + col] : 0.0;
           }
         const double* row = LU + (size_t)(iv ? i : rb) * n + i0;
 #pragma unroll
@@ -555,7 +579,7 @@ __device__ void chunked_lu_solve(int n, int nrhs, const double* LU, double* W, d
           for (int cb = 0; cb < 2; ++cb) {
             if (cb >= ncb) break;
             const int col = 8 * cb + fr;
-            const double bv = (k < h && col < nrhs) ? W[(size_t)(i0 + k) * nrhs + col] : 0.0;
+            const double bv = (k < h && col < nrhs) ? W[(size_t)(i0 + k) * ws + col] : 0.0;
             dmma_8x8x4(acc[cb][0], acc[cb][1], av, bv);
           }
         }
@@ -565,7 +589,7 @@ __device__ void chunked_lu_solve(int n, int nrhs, const double* LU, double* W, d
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
               const int col = 8 * cb + 2 * fc + e;
-              if (cb < ncb && col < nrhs) W[(size_t)i * nrhs + col] = acc[cb][e];
+              if (cb < ncb && col < nrhs) W[(size_t)i * ws + col] = acc[cb][e];
             }
         }
       }
@@ -591,16 +615,19 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
     const double* __restrict__ rhs, double* __restrict__ x, double rtol, double atol, int max_refine,
     int32_t* __restrict__ status) {
   extern __shared__ __align__(16) double sm[];
-  double* X = sm;                          // (n, nrhs)
-  double* W = X + (size_t)n * nrhs;        // (n, nrhs)
-  double* Dg = W + (size_t)n * nrhs;       // 2 x 32 x 33
+  // X and W are (n, nrhs) with an odd row stride ws = nrhs | 1, so that lanes reading
+  // consecutive rows of one column hit distinct shared-memory banks
+  const int ws = nrhs | 1;
+  double* X = sm;                          // (n, ws)
+  double* W = X + (size_t)n * ws;          // (n, ws)
+  double* Dg = W + (size_t)n * ws;         // 2 x 32 x 33
   double* part = Dg + 2 * 32 * 33;         // 32 x 16
   double* colr = part + 32 * 16;           // (3, 16): bmax, b2, r2 per column
   int* perm = reinterpret_cast<int*>(colr + 3 * 16);
   int* iperm = perm + n;
   __shared__ int flag;
   const int m = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
-  const size_t nn = (size_t)n * n, nb = (size_t)n * nrhs;
+  const size_t nn = (size_t)n * n;
   const double* A = mats + nn * m;
   const double* LU = factors + nn * m;
   const double* rsc = rs + (size_t)n * m;
@@ -622,11 +649,14 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
   if (tid < 16) colr[tid] = colr[16 + tid] = 0.0;
   __syncthreads();
   int nonfinite = 0;
-  for (size_t idx = tid; idx < nb; idx += blockDim.x)
-    if (!isfinite(B[(idx / nrhs) * ldr + idx % nrhs])) nonfinite = 1;
+  // (row, column) loops run over n x NR slots (NR a power of two: shift and mask, no
+  // division), skipping the columns past nrhs
+  for (int idx = tid; idx < n * NR; idx += blockDim.x)
+    if (idx % NR < nrhs && !isfinite(B[(size_t)(idx / NR) * ldr + idx % NR])) nonfinite = 1;
   if (__syncthreads_or(nonfinite)) {
-    for (size_t idx = tid; idx < nb; idx += blockDim.x) {
-      const size_t g = (idx / nrhs) * ldr + idx % nrhs;
+    for (int idx = tid; idx < n * NR; idx += blockDim.x) {
+      if (idx % NR >= nrhs) continue;
+      const size_t g = (size_t)(idx / NR) * ldr + idx % NR;
       Xg[g] = B[g];
     }
     if (tid == 0) status[m] = MHM_CELL_NONFINITE;
@@ -648,23 +678,24 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
     if (lane == 0) { colr[c] = scale; colr[16 + c] = b2; }
   }
   // X = csc .* U^-1 L^-1 P (rsc .* B)
-  for (size_t idx = tid; idx < nb; idx += blockDim.x) {
-    const int i = (int)(idx / nrhs), c = (int)(idx - (size_t)i * nrhs);
+  for (int idx = tid; idx < n * NR; idx += blockDim.x) {
+    const int i = idx / NR, c = idx % NR;
+    if (c >= nrhs) continue;
     const int src = perm[i];
-    W[idx] = B[(size_t)src * ldr + c] * rsc[src];
+    W[i * ws + c] = B[(size_t)src * ldr + c] * rsc[src];
   }
   __syncthreads();
-  chunked_lu_solve(n, nrhs, LU, W, Dg);
-  for (size_t idx = tid; idx < nb; idx += blockDim.x) {
-    const int i = (int)(idx / nrhs);
-    X[idx] = W[idx] * csc[i];
+  chunked_lu_solve(n, nrhs, ws, LU, W, Dg);
+  for (int idx = tid; idx < n * NR; idx += blockDim.x) {
+    const int i = idx / NR, c = idx % NR;
+    if (c < nrhs) X[i * ws + c] = W[i * ws + c] * csc[i];
   }
   __syncthreads();
   int result = MHM_CELL_RESIDUAL;
   for (int pass = 0; pass <= max_refine; ++pass) {
     int bad = 0;
-    for (size_t idx = tid; idx < nb; idx += blockDim.x)
-      if (!isfinite(X[idx])) bad = 1;
+    for (int idx = tid; idx < n * NR; idx += blockDim.x)
+      if (idx % NR < nrhs && !isfinite(X[(idx / NR) * ws + idx % NR])) bad = 1;
     if (__syncthreads_or(bad)) { result = MHM_CELL_NONFINITE; break; }
     // R = B - A X, one warp per row; the scaled residual goes to W at the row's
     // permuted position (ready for the correction solve); per warp the sums of
@@ -696,7 +727,7 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
         if (j < n) {
 #pragma unroll
           for (int c = 0; c < NR; ++c)
-            if (c < nrhs) dd_fma(hi[c], lo[c], -av[u], X[(size_t)j * nrhs + c]);
+            if (c < nrhs) dd_fma(hi[c], lo[c], -av[u], X[(size_t)j * ws + c]);
         }
       }
 #pragma unroll
@@ -716,7 +747,7 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
           double sres, e;
           two_sum(B[(size_t)i * ldr + c], h, sres, e);
           const double r = sres + (e + l);
-          W[(size_t)iperm[i] * nrhs + c] = r * rsc[i];
+          W[(size_t)iperm[i] * ws + c] = r * rsc[i];
           const double rv = r / colr[c];
           wr2[c] = fma(rv, rv, wr2[c]);
         }
@@ -745,19 +776,22 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
     __syncthreads();
     if (flag) { result = MHM_CELL_OK; break; }
     if (pass == max_refine) break;
-    chunked_lu_solve(n, nrhs, LU, W, Dg);
-    for (size_t idx = tid; idx < nb; idx += blockDim.x) {
-      const int i = (int)(idx / nrhs);
-      X[idx] += W[idx] * csc[i];
+    chunked_lu_solve(n, nrhs, ws, LU, W, Dg);
+    for (int idx = tid; idx < n * NR; idx += blockDim.x) {
+      const int i = idx / NR, c = idx % NR;
+      if (c < nrhs) X[i * ws + c] += W[i * ws + c] * csc[i];
     }
     __syncthreads();
   }
-  for (size_t idx = tid; idx < nb; idx += blockDim.x) Xg[(idx / nrhs) * ldr + idx % nrhs] = X[idx];
+  for (int idx = tid; idx < n * NR; idx += blockDim.x) {
+    const int i = idx / NR, c = idx % NR;
+    if (c < nrhs) Xg[(size_t)i * ldr + c] = X[i * ws + c];
+  }
   if (tid == 0 && result != MHM_CELL_OK) status[m] = result;
 }
 
 size_t chunked_solve_smem(int n, int nrhs) {
-  return ((size_t)2 * n * nrhs + 2 * 32 * 33 + 32 * 16 + 3 * 16) * 8 + (size_t)2 * n * 4;
+  return ((size_t)2 * n * (nrhs | 1) + 2 * 32 * 33 + 32 * 16 + 3 * 16) * 8 + (size_t)2 * n * 4;
 }
 }  // namespace
 }  // namespace mhm
@@ -774,7 +808,7 @@ extern "C" int mhm_batched_factor(int64_t count, int32_t n, const double* matric
   const int in_smem = bytes <= 200 * 1024;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (!in_smem && n <= kBlockedMaxN) {
-    const size_t smem = ((size_t)n * kPanelStride + (size_t)kPanel * kTileStride) * 8;
+    const size_t smem = (size_t)n * kPanelStride * 8;
     if (cudaFuncSetAttribute(batched_factor_blocked_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess)
       return MHM_ERR_LAUNCH;
