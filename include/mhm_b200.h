@@ -40,8 +40,8 @@
  *                          replace OfflineLocalProblem's factor-once and
  *                          one-column response (core/offline.py:99-145) for
  *                          OfflineHybridSystem.solve (core/offline.py:234-307).
- *   mhm_q1_original_defect / mhm_refine_norms / mhm_q1_correction_response /
- *   mhm_q1_flux / mhm_vector_accumulate
+ *   mhm_q1_original_defect(_dd) / mhm_refine_norms / mhm_q1_correction_response /
+ *   mhm_q1_flux / mhm_vector_accumulate(_dd)
  *                          replace the residual evaluation and the defect-source
  *                          correction of refine_hybrid (core/refinement.py:612-800)
  *                          for the Cartesian Q1 path.
@@ -207,6 +207,19 @@ int mhm_q1_original_defect(const mhm_q1_problem* p /* host */, const int64_t* ce
                            double* partial, void* stream);
 
 /*
+ * The same for a double-double solution (x + x_lo, fields + fields_lo): the
+ * extended correction storage of refine_hybrid(refinement_precision="extended")
+ * (core/refinement.py:636-643, a wider NumPy type there).  Both low parts are
+ * required.
+ */
+int mhm_q1_original_defect_dd(const mhm_q1_problem* p /* host */, const int64_t* cell_dofs,
+                              int64_t trace_size, const int32_t* dof_cells, const int32_t* dof_slot,
+                              const uint8_t* fixed, const double* x, const double* x_lo,
+                              const double* fields, const double* fields_lo, const double* boundary,
+                              double* defect, double* slot_terms, double* weak, double* partial,
+                              void* stream);
+
+/*
  * Norms of one refinement step, each summed in a fixed order:
  * out[0] = ||[defects; weak]||^2, out[1] = ||[loads; boundary]||^2,
  * out[2] = ||[weak; sum d per cell]||^2 and, if indptr is given, out[3] =
@@ -251,6 +264,10 @@ int mhm_q1_flux(const mhm_q1_problem* p /* host */, const double* fields, double
 
 /* dst[i] += src[i], i < n (the hybrid unknowns plus a correction). */
 int mhm_vector_accumulate(int64_t n, double* dst, const double* src, void* stream);
+
+/* (hi[i], lo[i]) += src[i] in double-double arithmetic, i < n (a correction added
+ * to a double-double solution). */
+int mhm_vector_accumulate_dd(int64_t n, double* hi, double* lo, const double* src, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Ordered skeleton reduction                                                 */

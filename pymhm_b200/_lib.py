@@ -101,6 +101,9 @@ _SIGNATURES = {
     "mhm_q1_original_defect": (C.c_int, [C.POINTER(Q1Problem), P, C.c_int64, P, P, P, P, P, P, P, P, P, P, P]),
     "mhm_refine_norms": (C.c_int, [C.c_int32, P, C.c_int64, P, P, P, C.c_int64, P, P, P, P, P, P, P]),
     "mhm_vector_accumulate": (C.c_int, [C.c_int64, P, P, P]),
+    "mhm_vector_accumulate_dd": (C.c_int, [C.c_int64, P, P, P, P]),
+    "mhm_q1_original_defect_dd": (C.c_int, [C.POINTER(Q1Problem), P, C.c_int64, P, P, P, P, P, P, P, P, P, P, P,
+                                            P, P]),
     "mhm_q1_mean_gauge": (C.c_int, [C.POINTER(Q1Problem), P, P, C.c_double, C.c_int64, P, P, P]),
     "mhm_skeleton_fixed_rhs": (C.c_int, [C.c_int64, C.c_int64, P, P, P, P, P, P, P, P]),
     "mhm_q1_flux": (C.c_int, [C.POINTER(Q1Problem), P, P, P]),

@@ -697,6 +697,71 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
     for (int idx = tid; idx < n * NR; idx += blockDim.x)
       if (idx % NR < nrhs && !isfinite(X[(idx / NR) * ws + idx % NR])) bad = 1;
     if (__syncthreads_or(bad)) { result = MHM_CELL_NONFINITE; break; }
+    // As the reference's _checked (linalg/linear.py:132-152): first the plain binary64
+    // residual, here on the FP64 tensor cores (a warp per 8-row block, A fragments from
+    // global memory, X fragments from shared memory; fragments A[lane/4][lane%4],
+    // B[lane%4][lane/4], C[lane/4][2 (lane%4) + {0, 1}]), with per lane the sums of
+    // (r / scale)^2 of its columns; only when it fails the acceptance, the accurate
+    // residual below, which also feeds the correction.
+    {
+      const int fr = lane >> 2, fc = lane & 3;
+      const int ncb = (nrhs + 7) >> 3;
+      double s2[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+      for (int rb = 8 * wid; rb < n; rb += 8 * nw) {
+        const int i = rb + fr;
+        const bool iv = i < n;
+        const double* arow = A + (size_t)(iv ? i : rb) * n;
+        double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll 8
+        for (int k0 = 0; k0 < n; k0 += 4) {
+          const int kk = k0 + fc;
+          const double a = (iv && kk < n) ? arow[kk] : 0.0;
+#pragma unroll
+          for (int cb = 0; cb < 2; ++cb) {
+            if (cb >= ncb) break;
+            const int col = 8 * cb + fr;
+            const double bx = (kk < n && col < nrhs) ? X[(size_t)kk * ws + col] : 0.0;
+            dmma_8x8x4(acc[cb][0], acc[cb][1], a, bx);
+          }
+        }
+        if (iv) {
+#pragma unroll
+          for (int cb = 0; cb < 2; ++cb)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int col = 8 * cb + 2 * fc + e;
+              if (cb < ncb && col < nrhs) {
+                const double rv = (B[(size_t)i * ldr + col] - acc[cb][e]) / colr[col];
+                s2[cb][e] = fma(rv, rv, s2[cb][e]);
+              }
+            }
+        }
+      }
+#pragma unroll
+      for (int cb = 0; cb < 2; ++cb)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          double v = s2[cb][e];
+          v += __shfl_xor_sync(0xffffffffu, v, 4);
+          v += __shfl_xor_sync(0xffffffffu, v, 8);
+          v += __shfl_xor_sync(0xffffffffu, v, 16);
+          const int col = 8 * cb + 2 * fc + e;
+          if (fr == 0 && cb < ncb && col < nrhs) part[wid * 16 + col] = v;
+        }
+      __syncthreads();
+      if (tid == 0) {
+        int ok = 1;
+        for (int c = 0; c < nrhs; ++c) {
+          double t = 0.0;
+          for (int q = 0; q < nw; ++q) t += part[q * 16 + c];
+          const double limit = fmax(atol / colr[c], rtol * sqrt(colr[16 + c]));
+          if (!(sqrt(t) <= limit)) ok = 0;
+        }
+        flag = ok;
+      }
+      __syncthreads();
+      if (flag) { result = MHM_CELL_OK; break; }
+    }
     // R = B - A X, one warp per row; the scaled residual goes to W at the row's
     // permuted position (ready for the correction solve); per warp the sums of
     // (r / scale)^2 per column, added in warp order below

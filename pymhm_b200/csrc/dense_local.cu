@@ -138,24 +138,29 @@ __global__ void __launch_bounds__(kDThreads) dense_system_kernel(
                      sqrt(l2) > 1e-10 * sqrt(fro) * sqrt((double)n)))
     st = MHM_CELL_KERNEL;
   const double scale = (cmax > 0.0) ? fmin(1.0, (amax > 0.0 ? amax : 1.0) / cmax) : 1.0;
-  for (int64_t k = tid; k < (int64_t)nb * nb; k += blockDim.x) {
-    const int i = (int)(k / nb), j = (int)(k - (int64_t)i * nb);
-    double v;
-    if (i < n && j < n) v = A[(int64_t)i * lds + j];
-    else if (i > n || j > n) v = (i == j) ? 1.0 : 0.0;
-    else if (i == n && j == n) v = 0.0;
-    else v = (act[2 * nb + ((i < n) ? i : j)] / cdiv) * scale;
-    K[k] = v;
-  }
-  for (int64_t k = tid; k < (int64_t)nb * w; k += blockDim.x) {
-    const int i = (int)(k / w), col = (int)(k - (int64_t)i * w);
-    double v = 0.0;
+  // the augmented matrix and the right-hand sides, a warp per row (no index division)
+  const int lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  for (int i = wid; i < nb; i += nw) {
+    double* Ki = K + (int64_t)i * nb;
     if (i < n) {
-      if (col == 0) v = load[cell * lds + i];
-      else if (col <= t) v = coupling[(cell * lds + i) * tld + (col - 1)];
-      else if (col == t + 1) v = corr ? act[i] : 0.0;
+      const double* Ai = A + (int64_t)i * lds;
+      const double ci = (act[2 * nb + i] / cdiv) * scale;
+      for (int j = lane; j < nb; j += 32) Ki[j] = j < n ? Ai[j] : (j == n ? ci : 0.0);
+    } else if (i == n) {
+      for (int j = lane; j < nb; j += 32) Ki[j] = j < n ? (act[2 * nb + j] / cdiv) * scale : 0.0;
+    } else {
+      for (int j = lane; j < nb; j += 32) Ki[j] = (i == j) ? 1.0 : 0.0;
     }
-    R[k] = v;
+    double* Ri = R + (int64_t)i * w;
+    for (int col = lane; col < w; col += 32) {
+      double v = 0.0;
+      if (i < n) {
+        if (col == 0) v = load[cell * lds + i];
+        else if (col <= t) v = coupling[(cell * lds + i) * tld + (col - 1)];
+        else if (col == t + 1) v = corr ? act[i] : 0.0;
+      }
+      Ri[col] = v;
+    }
   }
   if (tid == 0) {
     corrected[cell] = (uint8_t)corr;

@@ -1116,9 +1116,12 @@ __global__ void __launch_bounds__(kThreads) q1_flux_kernel(const Q1Args a, const
 // does in extended precision (linalg/linear.py:98-126); the cell's weak-trace terms
 // B^T u per trace slot, also accumulated in double-double; and per cell the sums
 // [d.d, f.f, 1.d].
+// x_lo / fields_lo (nullable): low parts of a double-double solution (extended
+// refinement storage); their terms enter the same double-double sums.
 __global__ void __launch_bounds__(kThreads) q1_defect_kernel(const Q1Args a, const int64_t* cell_dofs,
                                                              const uint8_t* fixed, const double* x,
-                                                             const double* fields, double* defect,
+                                                             const double* x_lo, const double* fields,
+                                                             const double* fields_lo, double* defect,
                                                              double* slot_terms, double* partial) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int n = a.n, t = a.t, nnx = a.nnx, ne = a.rx * a.ry, cell = blockIdx.x, tid = threadIdx.x;
@@ -1132,16 +1135,23 @@ __global__ void __launch_bounds__(kThreads) q1_defect_kernel(const Q1Args a, con
   double* u = ctil + n;
   double* lam = u + n;
   double* lamf = lam + t;  // lambda on the fixed trace slots, 0 elsewhere
-  double* red = lamf + t;
+  double* ulo = lamf + t;  // low parts (zero without them)
+  double* lamlo = ulo + n;
+  double* red = lamlo + t;
   double amax, fro, cmax;
   if (a.cut_mode)
     assemble_cell<true>(a, cell, kel, fel, cb, zb, sten, fvec, ctil, amax, fro, cmax);
   else
     assemble_cell<false>(a, cell, kel, fel, cb, zb, sten, fvec, ctil, amax, fro, cmax);
-  for (int i = tid; i < n; i += blockDim.x) u[i] = fields[(size_t)cell * n + i];
+  const bool has_lo = x_lo && fields_lo;
+  for (int i = tid; i < n; i += blockDim.x) {
+    u[i] = fields[(size_t)cell * n + i];
+    ulo[i] = has_lo ? fields_lo[(size_t)cell * n + i] : 0.0;
+  }
   for (int j = tid; j < t; j += blockDim.x) {
     const int64_t dof = cell_dofs[(size_t)cell * t + j];
     lam[j] = x[dof];
+    lamlo[j] = has_lo ? x_lo[dof] : 0.0;
     lamf[j] = (fixed && fixed[dof]) ? x[dof] : 0.0;
   }
   __syncthreads();
@@ -1154,20 +1164,24 @@ __global__ void __launch_bounds__(kThreads) q1_defect_kernel(const Q1Args a, con
       const double bij = rhs_value(a, 1 + j, i, fvec, nullptr, cb);
       if (bij != 0.0) {
         dd_fma(hi, lo, -bij, lam[j]);
+        if (has_lo) dd_fma(hi, lo, -bij, lamlo[j]);
         fb = fma(-bij, lamf[j], fb);
       }
     }
     const double* sv = sten + 5 * i;
-    dd_fma(hi, lo, -sv[0], u[i]);
-    if (ix > 0) dd_fma(hi, lo, -sv[1], u[i - 1]);
-    if (iy > 0 && ix < nnx - 1) dd_fma(hi, lo, -sv[2], u[i - nnx + 1]);
-    if (iy > 0) dd_fma(hi, lo, -sv[3], u[i - nnx]);
-    if (iy > 0 && ix > 0) dd_fma(hi, lo, -sv[4], u[i - nnx - 1]);
-    if (ix < nnx - 1) dd_fma(hi, lo, -sten[5 * (i + 1) + 1], u[i + 1]);
-    if (iy < a.nny - 1) {
-      if (ix > 0) dd_fma(hi, lo, -sten[5 * (i + nnx - 1) + 2], u[i + nnx - 1]);
-      dd_fma(hi, lo, -sten[5 * (i + nnx) + 3], u[i + nnx]);
-      if (ix < nnx - 1) dd_fma(hi, lo, -sten[5 * (i + nnx + 1) + 4], u[i + nnx + 1]);
+    for (int part = 0; part < (has_lo ? 2 : 1); ++part) {
+      const double* v = part ? ulo : u;
+      dd_fma(hi, lo, -sv[0], v[i]);
+      if (ix > 0) dd_fma(hi, lo, -sv[1], v[i - 1]);
+      if (iy > 0 && ix < nnx - 1) dd_fma(hi, lo, -sv[2], v[i - nnx + 1]);
+      if (iy > 0) dd_fma(hi, lo, -sv[3], v[i - nnx]);
+      if (iy > 0 && ix > 0) dd_fma(hi, lo, -sv[4], v[i - nnx - 1]);
+      if (ix < nnx - 1) dd_fma(hi, lo, -sten[5 * (i + 1) + 1], v[i + 1]);
+      if (iy < a.nny - 1) {
+        if (ix > 0) dd_fma(hi, lo, -sten[5 * (i + nnx - 1) + 2], v[i + nnx - 1]);
+        dd_fma(hi, lo, -sten[5 * (i + nnx) + 3], v[i + nnx]);
+        if (ix < nnx - 1) dd_fma(hi, lo, -sten[5 * (i + nnx + 1) + 4], v[i + nnx + 1]);
+      }
     }
     const double d = hi + lo;
     defect[(size_t)cell * n + i] = d;
@@ -1180,6 +1194,8 @@ __global__ void __launch_bounds__(kThreads) q1_defect_kernel(const Q1Args a, con
     const int len = side_len(a, sd.s);
     double hi = 0.0, lo = 0.0;
     for (int k = 0; k < len; ++k) dd_fma(hi, lo, cb[j * a.kmax + k], u[side_node(a, sd.s, k)]);
+    if (has_lo)
+      for (int k = 0; k < len; ++k) dd_fma(hi, lo, cb[j * a.kmax + k], ulo[side_node(a, sd.s, k)]);
     slot_terms[(size_t)cell * t + j] = hi + lo;
   }
   d2 = block_sum(d2, red);
@@ -1505,19 +1521,20 @@ extern "C" int mhm_q1_correction_response(const mhm_q1_problem* p, int32_t preci
                       cell_iters, factors ? 2 : 3, const_cast<void*>(factors), stream);
 }
 
-extern "C" int mhm_q1_original_defect(const mhm_q1_problem* p, const int64_t* cell_dofs, int64_t trace_size,
-                                      const int32_t* dof_cells, const int32_t* dof_slot, const uint8_t* fixed,
-                                      const double* x, const double* fields, const double* boundary,
-                                      double* defect, double* slot_terms, double* weak, double* partial,
-                                      void* stream) {
+namespace mhm {
+namespace {
+int original_defect(const mhm_q1_problem* p, const int64_t* cell_dofs, int64_t trace_size, const int32_t* dof_cells,
+                    const int32_t* dof_slot, const uint8_t* fixed, const double* x, const double* x_lo,
+                    const double* fields, const double* fields_lo, const double* boundary, double* defect,
+                    double* slot_terms, double* weak, double* partial, void* stream) {
   Q1Args a;
   int rc = fill_args(p, MHM_PRECISION_FP64, a);
   if (rc != MHM_OK) return rc;
   if (!cell_dofs || trace_size < 1 || !dof_cells || !dof_slot || !x || !fields || !defect || !slot_terms ||
-      !weak || !partial)
+      !weak || !partial || (!x_lo) != (!fields_lo))
     return MHM_ERR_ARGUMENT;
   const int ne = a.rx * a.ry;
-  const size_t smem = ((size_t)7 * ne + (size_t)a.t * a.kmax + a.t + 8 * (size_t)a.n + 2 * a.t + 32) * 8;
+  const size_t smem = ((size_t)7 * ne + (size_t)a.t * a.kmax + a.t + 9 * (size_t)a.n + 3 * a.t + 32) * 8;
   if (smem > 227 * 1024) return MHM_ERR_UNSUPPORTED;
   if (smem > 48 * 1024 &&
       cudaFuncSetAttribute(q1_defect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
@@ -1525,11 +1542,54 @@ extern "C" int mhm_q1_original_defect(const mhm_q1_problem* p, const int64_t* ce
     return MHM_ERR_LAUNCH;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   launch_cut_elements(a, st);
-  q1_defect_kernel<<<a.nx * a.ny, kThreads, smem, st>>>(a, cell_dofs, fixed, x, fields, defect, slot_terms,
-                                                        partial);
+  q1_defect_kernel<<<a.nx * a.ny, kThreads, smem, st>>>(a, cell_dofs, fixed, x, x_lo, fields, fields_lo, defect,
+                                                        slot_terms, partial);
   int blocks = (int)((trace_size + 255) / 256);
   if (blocks > 4096) blocks = 4096;
   weak_residual_kernel<<<blocks, 256, 0, st>>>(trace_size, a.t, dof_cells, dof_slot, slot_terms, boundary, weak);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+// (hi, lo) += src elementwise in double-double (two-sum, then renormalised).
+__global__ void accumulate_dd_kernel(int64_t n, double* hi, double* lo, const double* src) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double s, e;
+    two_sum(hi[i], src[i], s, e);
+    e += lo[i];
+    double h, l;
+    two_sum(s, e, h, l);
+    hi[i] = h;
+    lo[i] = l;
+  }
+}
+}  // namespace
+}  // namespace mhm
+
+extern "C" int mhm_q1_original_defect(const mhm_q1_problem* p, const int64_t* cell_dofs, int64_t trace_size,
+                                      const int32_t* dof_cells, const int32_t* dof_slot, const uint8_t* fixed,
+                                      const double* x, const double* fields, const double* boundary,
+                                      double* defect, double* slot_terms, double* weak, double* partial,
+                                      void* stream) {
+  return original_defect(p, cell_dofs, trace_size, dof_cells, dof_slot, fixed, x, nullptr, fields, nullptr,
+                         boundary, defect, slot_terms, weak, partial, stream);
+}
+
+extern "C" int mhm_q1_original_defect_dd(const mhm_q1_problem* p, const int64_t* cell_dofs, int64_t trace_size,
+                                         const int32_t* dof_cells, const int32_t* dof_slot, const uint8_t* fixed,
+                                         const double* x, const double* x_lo, const double* fields,
+                                         const double* fields_lo, const double* boundary, double* defect,
+                                         double* slot_terms, double* weak, double* partial, void* stream) {
+  if (!x_lo || !fields_lo) return MHM_ERR_ARGUMENT;
+  return original_defect(p, cell_dofs, trace_size, dof_cells, dof_slot, fixed, x, x_lo, fields, fields_lo,
+                         boundary, defect, slot_terms, weak, partial, stream);
+}
+
+extern "C" int mhm_vector_accumulate_dd(int64_t n, double* hi, double* lo, const double* src, void* stream) {
+  if (n < 0 || (n > 0 && (!hi || !lo || !src))) return MHM_ERR_ARGUMENT;
+  if (n == 0) return MHM_OK;
+  int blocks = (int)((n + 255) / 256);
+  if (blocks > 4096) blocks = 4096;
+  accumulate_dd_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(n, hi, lo, src);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
 

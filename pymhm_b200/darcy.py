@@ -633,7 +633,8 @@ class CartesianQ1Plan:
         sol.seconds = time.perf_counter() - t0
         return sol
 
-    def refine(self, *, max_steps=2, min_steps=0, rtol=1e-10, atol=0.0, stream=None) -> HybridRefinement:
+    def refine(self, *, max_steps=2, min_steps=0, rtol=1e-10, atol=0.0, stream=None,
+               refinement_precision="double") -> HybridRefinement:
         """Defect correction of the original equations (``refine_hybrid``,
         ``core/refinement.py:612-800``) applied to the plan's last solve.
 
@@ -660,7 +661,18 @@ class CartesianQ1Plan:
         the moment defect value - sum_cells C . u, the right-hand-side norm the value,
         and each correction is gauged to the moment defect (``refinement.py:690-700,
         725-733, 787-797``).
+
+        ``refinement_precision="extended"`` keeps the solution as double-double values
+        (the reference stores it in a wider NumPy type, ``refinement.py:636-643``): the
+        defects are evaluated from both parts and each correction is added in
+        double-double arithmetic, so the residual can fall below the binary64 floor of
+        the stored solution.  The returned fields and unknowns are the high parts; the
+        low parts are in ``extra["trace_lo"]``, ``extra["coarse_lo"]`` and
+        ``extra["fields_lo"]``.
         """
+        if refinement_precision not in ("double", "extended"):
+            raise ValueError("refinement_precision must be double or extended")
+        extended = refinement_precision == "extended"
         _step_limits(max_steps, min_steps)
         _tolerances(rtol, atol)
         torch, L, P = self.torch, self.lib, _lib.ptr
@@ -678,17 +690,28 @@ class CartesianQ1Plan:
                                 rhs=torch.empty(self.N, **f64), scale=torch.empty(self.N, **f64),
                                 dfields=torch.empty((M, n), **f64))
         B = self._refine
+        if extended:
+            B["x_lo"] = torch.zeros_like(self.x)
+            B["fields_lo"] = torch.zeros_like(self.fields)
         qd = _lib.Q1Problem.from_buffer_copy(self.q1)
         qd.source_mode, qd.source, qd.source_const = 3, P(B["defect"]), 0.0
         factors = self.factors if getattr(self, "_factors_current", False) else None
         pat = self.pattern
         history, step = [], 0
         while True:
-            _lib.check(L.mhm_q1_original_defect(self.q1, P(self.d_cell_dofs), self.T, P(self.d_dof_cells),
-                                                P(self.d_dof_slot), P(self.d_fixed), P(self.x), P(self.fields),
-                                                P(self.d_boundary), P(B["defect"]), P(B["slots"]), P(B["weak"]),
-                                                P(B["partial"]), s),
-                       "mhm_q1_original_defect")
+            if extended:
+                _lib.check(L.mhm_q1_original_defect_dd(self.q1, P(self.d_cell_dofs), self.T, P(self.d_dof_cells),
+                                                       P(self.d_dof_slot), P(self.d_fixed), P(self.x),
+                                                       P(B["x_lo"]), P(self.fields), P(B["fields_lo"]),
+                                                       P(self.d_boundary), P(B["defect"]), P(B["slots"]),
+                                                       P(B["weak"]), P(B["partial"]), s),
+                           "mhm_q1_original_defect_dd")
+            else:
+                _lib.check(L.mhm_q1_original_defect(self.q1, P(self.d_cell_dofs), self.T, P(self.d_dof_cells),
+                                                    P(self.d_dof_slot), P(self.d_fixed), P(self.x), P(self.fields),
+                                                    P(self.d_boundary), P(B["defect"]), P(B["slots"]),
+                                                    P(B["weak"]), P(B["partial"]), s),
+                           "mhm_q1_original_defect")
             _lib.check(L.mhm_refine_norms(M, P(B["partial"]), self.T, P(self.d_fixed), P(B["weak"]),
                                           P(self.d_boundary), self.N,
                                           P(self.d_indptr), P(self.d_indices), P(self.values), P(self.x),
@@ -711,6 +734,10 @@ class CartesianQ1Plan:
                 scale = max(math.sqrt(norms[3]), math.sqrt(norms[4]), np.finfo(float).tiny)
                 sol.residual = math.sqrt(norms[2]) / scale
                 sol.extra["refinement_steps"] = step
+                if extended:
+                    xl = B["x_lo"].cpu().numpy()
+                    sol.extra["trace_lo"], sol.extra["coarse_lo"] = xl[: self.T].copy(), xl[self.T:].copy()
+                    sol.extra["fields_lo"] = B["fields_lo"].cpu().numpy()
                 return HybridRefinement(sol, tuple(history), rhs_norm)
             if step == max_steps or not math.isfinite(residual):
                 raise LinearSolveError(f"original hybrid residual {residual:.6e} exceeds {threshold:.6e} "
@@ -747,8 +774,12 @@ class CartesianQ1Plan:
                                                P(B["dx"]), P(B["gauge_partial"]), s), "mhm_q1_mean_gauge")
             _lib.check(L.mhm_q1_reconstruct(self.q1, P(self.solution), P(self.d_cell_dofs), self.T, P(B["dx"]),
                                             P(B["dfields"]), None, s), "mhm_q1_reconstruct")
-            for dst, src in ((self.x, B["dx"]), (self.fields, B["dfields"])):
-                _lib.check(L.mhm_vector_accumulate(dst.numel(), P(dst), P(src), s), "mhm_vector_accumulate")
+            for dst, lo, src in ((self.x, "x_lo", B["dx"]), (self.fields, "fields_lo", B["dfields"])):
+                if extended:
+                    _lib.check(L.mhm_vector_accumulate_dd(dst.numel(), P(dst), P(B[lo]), P(src), s),
+                               "mhm_vector_accumulate_dd")
+                else:
+                    _lib.check(L.mhm_vector_accumulate(dst.numel(), P(dst), P(src), s), "mhm_vector_accumulate")
             _lib.check(L.mhm_q1_flux(self.q1, P(self.fields), P(self.flux), s), "mhm_q1_flux")
             cur.synchronize()
             self.check()
@@ -935,8 +966,10 @@ def solve_darcy_quadrilateral(mesh, *, permeability=1.0, source=0.0, dirichlet=0
     return sol
 
 
-def refine_hybrid(plan, *, max_steps=2, min_steps=0, rtol=1e-10, atol=0.0, stream=None) -> HybridRefinement:
+def refine_hybrid(plan, *, max_steps=2, min_steps=0, rtol=1e-10, atol=0.0, stream=None,
+                  refinement_precision="double") -> HybridRefinement:
     """``refine_hybrid`` (``core/refinement.py:612-800``) for a solved ``CartesianQ1Plan``:
     the plan holds the system, the solution and the boundary load that the reference
     passes separately.  See ``CartesianQ1Plan.refine``."""
-    return plan.refine(max_steps=max_steps, min_steps=min_steps, rtol=rtol, atol=atol, stream=stream)
+    return plan.refine(max_steps=max_steps, min_steps=min_steps, rtol=rtol, atol=atol, stream=stream,
+                       refinement_precision=refinement_precision)

@@ -129,3 +129,37 @@ def test_refinement_at_full_size():
         del plan
         torch.cuda.empty_cache()
     assert rel(fields["mixed"], fields["fp64"]) <= 1e-10
+
+
+def test_extended_refinement_certifies_the_default_tolerance_at_full_size():
+    """The same workload with the double-double solution store of
+    ``refinement_precision="extended"`` (the reference's wider NumPy type): the
+    binary64 store stagnates near 4e-10 of the right-hand-side norm, the extended one
+    reaches the reference's default rtol = 1e-10, and its fields agree with the
+    binary64 solve's."""
+    import torch
+
+    from pymhm_b200.darcy import CartesianQ1Plan
+    from pymhm_b200.topology import CartesianMacroMesh, FaceSpace, SkeletonSpace
+    from pymhm_b200.workloads import lognormal_permeability
+
+    mesh = CartesianMacroMesh(64)
+    sk = SkeletonSpace(mesh, (FaceSpace.uniform(2),) * len(mesh.faces))
+    kappa = lognormal_permeability(1024, 1024, sigma=2.0, ell=0.05, seed=20261203)
+    plan = CartesianQ1Plan(mesh, sk, 16, precision="fp64")
+    plan.set_coefficients(kappa, 1.0)
+    plan.launch()
+    base = plan.result()
+    out = plan.refine(max_steps=3, rtol=1e-10, refinement_precision="extended")
+    hist = out.residual_norms
+    assert hist[-1] <= 1e-10 * out.rhs_norm
+    assert hist[-1] < hist[0]
+    sol = out.solution
+    assert rel(sol.fields, base.fields) <= 1e-8
+    lo = sol.extra["fields_lo"]
+    assert lo.shape == np.asarray(sol.fields).shape
+    assert np.max(np.abs(lo)) <= 1e-15 * np.max(np.abs(sol.fields))
+    with pytest.raises(ValueError):
+        plan.refine(refinement_precision="quad")
+    del plan
+    torch.cuda.empty_cache()
