@@ -315,6 +315,12 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
       if (lane < w) Pn[r * kPanelStride + lane] = F[(size_t)(kb + r) * n + kb + lane];
     __syncthreads();
     for (int c = 0; c < w; ++c) {
+      // pivot search on column c; the previous column's multipliers are scaled in the
+      // same phase (its elimination ended at the last barrier; columns differ)
+      if (c > 0) {
+        const double pinv = 1.0 / Pn[(c - 1) * kPanelStride + (c - 1)];
+        for (int r = c + tid; r < rows; r += blockDim.x) Pn[r * kPanelStride + c - 1] *= pinv;
+      }
       double best = -1.0;
       int bi = c;
       for (int r = c + tid; r < rows; r += blockDim.x) {
@@ -328,15 +334,14 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
       }
       if (lane == 0) { wbest[wid] = best; wrow[wid] = bi; }
       __syncthreads();
-      if (tid == 0) {
+      // every thread reduces the warps' candidates (first maximum) itself
+      int p = wrow[0];
+      {
         double b = wbest[0];
-        int r = wrow[0];
         for (int q = 1; q < nw; ++q)
-          if (wbest[q] > b || (wbest[q] == b && wrow[q] < r)) { b = wbest[q]; r = wrow[q]; }
-        sperm[c] = r;
+          if (wbest[q] > b || (wbest[q] == b && wrow[q] < p)) { b = wbest[q]; p = wrow[q]; }
       }
-      __syncthreads();
-      const int p = sperm[c];
+      if (tid == 0) sperm[c] = p;
       if (p != c)
         for (int j = tid; j < w; j += blockDim.x) {
           const double t = Pn[c * kPanelStride + j];
@@ -349,9 +354,9 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
       const double inv = 1.0 / d;
       {
         // every (row below the pivot, panel column right of it) pair is independent (the
-        // multiplier l = a_rc / d formed where used); the multipliers replace column c
-        // after a barrier
-        // a warp per row, a lane per panel column; four rows' loads before their stores
+        // multiplier l = a_rc / d formed where used; column c is scaled in the next
+        // column's first phase): a warp per row, a lane per panel column, four rows'
+        // loads before their stores
         const int j = c + 1 + lane;
         const bool jv = j < w;
         const double u = jv ? Pn[c * kPanelStride + j] : 0.0;
@@ -370,9 +375,12 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
             if (rk < rows && jv) Pn[rk * kPanelStride + j] = fma(-l[k], u, a[k]);
           }
         }
-        __syncthreads();
-        for (int r = c + 1 + tid; r < rows; r += blockDim.x) Pn[r * kPanelStride + c] *= inv;
       }
+      __syncthreads();
+    }
+    if (st == MHM_CELL_OK) {  // the last column's multipliers
+      const double pinv = 1.0 / Pn[(w - 1) * kPanelStride + (w - 1)];
+      for (int r = w + tid; r < rows; r += blockDim.x) Pn[r * kPanelStride + w - 1] *= pinv;
       __syncthreads();
     }
     if (st != MHM_CELL_OK) break;
