@@ -70,6 +70,7 @@ extern "C" {
 #define MHM_CELL_NONFINITE 5       /* non-finite input or result                   */
 #define MHM_CELL_ZERO_ROW 6        /* equilibration met a zero row                  */
 #define MHM_CELL_ZERO_COLUMN 7     /* equilibration met a zero column               */
+#define MHM_CELL_SIZE 8            /* a ragged batch's matrix exceeds the launch maximum */
 
 /* Global solve status (mhm_skeleton_solve `info` array, entry 0). */
 #define MHM_SOLVE_OK 0
@@ -589,6 +590,42 @@ int mhm_batched_solve(int64_t count, int32_t n, int32_t nrhs, const double* matr
                       const double* col_scale, const double* rhs, double* x, double* work,
                       double rtol, double atol, int32_t max_refine, int32_t* status,
                       void* stream);
+
+/*
+ * Ragged batches: matrices of different orders in one launch (polygon cells binned
+ * by padded size).  Matrix k has order n (its rows and columns, row-major, at
+ * matrices / factors + mat_off), pivots and row / column scales at + vec_off,
+ * nrhs right-hand sides and solutions (n, nrhs) row-major at rhs / x + rhs_off,
+ * and its status word at status[slot].
+ */
+typedef struct mhm_ragged_matrix {
+    int64_t mat_off;
+    int64_t vec_off;
+    int64_t rhs_off;
+    int32_t n;
+    int32_t nrhs;
+    int32_t slot;
+    int32_t reserved;
+} mhm_ragged_matrix;
+
+/*
+ * mhm_batched_factor over count ragged matrices in one launch (descriptors on the
+ * device; every n <= max_n <= 640, larger ones get MHM_CELL_SIZE).  CTAs start in
+ * descriptor order, so listing the largest matrices first balances the SMs.
+ */
+int mhm_batched_factor_ragged(int64_t count, const mhm_ragged_matrix* desc, int32_t max_n,
+                              const double* matrices, double* factors, int32_t* pivots,
+                              double* row_scale, double* col_scale, int32_t* status, void* stream);
+
+/*
+ * mhm_batched_solve over count ragged systems (nrhs <= max_nrhs columns each), one
+ * launch per group of 16 columns, with the same acceptance per column.
+ */
+int mhm_batched_solve_ragged(int64_t count, const mhm_ragged_matrix* desc, int32_t max_n,
+                             int32_t max_nrhs, const double* matrices, const double* factors,
+                             const int32_t* pivots, const double* row_scale, const double* col_scale,
+                             const double* rhs, double* x, double rtol, double atol, int32_t max_refine,
+                             int32_t* status, void* stream);
 
 /* Library version string (host). */
 const char* mhm_version(void);

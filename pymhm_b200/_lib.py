@@ -15,6 +15,7 @@ LIBRARY = Path(__file__).resolve().parent / "libmhm_b200.so"
 MHM_OK, MHM_ERR_ARGUMENT, MHM_ERR_LAUNCH, MHM_ERR_UNSUPPORTED = 0, 1, 2, 3
 CELL_OK, CELL_KERNEL, CELL_SINGULAR_PIVOT, CELL_RANK_DEFICIENT = 0, 1, 2, 3
 CELL_RESIDUAL, CELL_NONFINITE, CELL_ZERO_ROW, CELL_ZERO_COLUMN = 4, 5, 6, 7
+CELL_SIZE = 8
 SOLVE_OK, SOLVE_NOT_CONVERGED, SOLVE_BREAKDOWN, SOLVE_BARRIER_TIMEOUT, SOLVE_NONFINITE = 0, 1, 2, 3, 4
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 
@@ -34,6 +35,7 @@ CELL_MESSAGES = {
     CELL_NONFINITE: "batched solver returned nonfinite coefficients",
     CELL_ZERO_ROW: "batched matrix contains a zero row",
     CELL_ZERO_COLUMN: "batched matrix contains a zero column",
+    CELL_SIZE: "a ragged batch's matrix exceeds the launch's largest order",
 }
 
 SOLVE_MESSAGES = {
@@ -72,6 +74,11 @@ class SkeletonSystem(C.Structure):
         ("coarse_qx", C.c_void_p), ("coarse_lamx", C.c_void_p), ("coarse_pinv0", C.c_void_p),
         ("coarse_partial", C.c_int32), ("coarse_partial_cells", C.c_void_p), ("coarse_partial_R", C.c_void_p),
     ]
+
+
+class RaggedMatrix(C.Structure):
+    _fields_ = [("mat_off", C.c_int64), ("vec_off", C.c_int64), ("rhs_off", C.c_int64), ("n", C.c_int32),
+                ("nrhs", C.c_int32), ("slot", C.c_int32), ("reserved", C.c_int32)]
 
 
 class GeneralSystem(C.Structure):
@@ -130,6 +137,9 @@ _SIGNATURES = {
                                   C.c_double, P, C.c_int64, P, P, P, P, P, P, P, P, P, P, P, P]),
     "mhm_q1_reconstruct": (C.c_int, [C.POINTER(Q1Problem), P, P, C.c_int64, P, P, P, P]),
     "mhm_batched_factor": (C.c_int, [C.c_int64, C.c_int32, P, P, P, P, P, P, P]),
+    "mhm_batched_factor_ragged": (C.c_int, [C.c_int64, P, C.c_int32, P, P, P, P, P, P, P]),
+    "mhm_batched_solve_ragged": (C.c_int, [C.c_int64, P, C.c_int32, C.c_int32, P, P, P, P, P, P, P, C.c_double,
+                                           C.c_double, C.c_int32, P, P]),
     "mhm_batched_solve": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, P, P, P, P, P, P, P, C.c_double,
                                     C.c_double, C.c_int32, P, P]),
     "mhm_p1_batch_assemble": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, C.c_int32, P, P, C.c_int64,

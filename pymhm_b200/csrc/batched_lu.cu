@@ -293,9 +293,12 @@ __device__ int equilibrate(int n, const double* A, double* F, double* rsc, doubl
 // row swaps are applied to the other columns, a thread per column, in order;
 // (c) U12 = L11^-1 A12, a thread per column; (d) A22 -= L21 U12 on the FP64 tensor
 // cores, a warp per 8-row block, without a CTA barrier inside.
+// With desc (ragged batches), CTA m factors the matrix desc[m] describes (its order,
+// offsets and status word); matrices larger than max_n get MHM_CELL_SIZE.
 __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
-    int n, const double* __restrict__ mats, double* __restrict__ factors, int32_t* __restrict__ piv,
-    double* __restrict__ rs, double* __restrict__ cs, int32_t* __restrict__ status) {
+    int n_uniform, const double* __restrict__ mats, double* __restrict__ factors, int32_t* __restrict__ piv,
+    double* __restrict__ rs, double* __restrict__ cs, int32_t* __restrict__ status,
+    const mhm_ragged_matrix* __restrict__ desc, int max_n) {
   extern __shared__ __align__(16) double sm[];
   double* Pn = sm;                                   // (n, kPanelStride) panel
   __shared__ double red[32];
@@ -306,9 +309,21 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
   __shared__ int naff;
   __shared__ int srcrow[kBlockedMaxN];
   const int m = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
-  const size_t nn = (size_t)n * n;
-  double* F = factors + nn * m;
-  int st = equilibrate(n, mats + nn * m, F, rs + (size_t)n * m, cs + (size_t)n * m);
+  int n = n_uniform, sidx = m;
+  size_t moff = (size_t)n_uniform * n_uniform * m, voff = (size_t)n_uniform * m;
+  if (desc) {
+    const mhm_ragged_matrix d = desc[m];
+    n = d.n;
+    sidx = d.slot;
+    moff = (size_t)d.mat_off;
+    voff = (size_t)d.vec_off;
+    if (n < 1 || n > max_n) {
+      if (tid == 0) status[sidx] = MHM_CELL_SIZE;
+      return;
+    }
+  }
+  double* F = factors + moff;
+  int st = equilibrate(n, mats + moff, F, rs + voff, cs + voff);
   for (int kb = 0; kb < n && st == MHM_CELL_OK; kb += kPanel) {
     const int w = min(kPanel, n - kb), rows = n - kb;
     for (int r = wid; r < rows; r += nw)
@@ -386,7 +401,7 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
     if (st != MHM_CELL_OK) break;
     for (int r = wid; r < rows; r += nw)
       if (lane < w) F[(size_t)(kb + r) * n + kb + lane] = Pn[r * kPanelStride + lane];
-    for (int c = tid; c < w; c += blockDim.x) piv[(size_t)m * n + kb + c] = kb + sperm[c];
+    for (int c = tid; c < w; c += blockDim.x) piv[voff + kb + c] = kb + sperm[c];
     // compose the panel's swaps: srcrow[r] = the panel row that ends at position r; the
     // moved positions (at most 2 w) are listed with their sources
     for (int r = tid; r < rows; r += blockDim.x) srcrow[r] = r;
@@ -504,13 +519,13 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
   if (st == MHM_CELL_OK) {
     double dmin = 1e300, amax = 0.0;
     for (int i = tid; i < n; i += blockDim.x) dmin = fmin(dmin, fabs(F[(size_t)i * n + i]));
-#pragma unroll 8
-    for (size_t idx = tid; idx < nn; idx += blockDim.x) amax = fmax(amax, fabs(F[idx]));
+    for (int i = wid; i < n; i += nw)
+      for (int j = lane; j < n; j += 32) amax = fmax(amax, fabs(F[(size_t)i * n + j]));
     dmin = block_min(dmin, red);
     amax = block_max(amax, red);
     if (dmin <= 2.220446049250313e-16 * n * amax) st = MHM_CELL_RANK_DEFICIENT;
   }
-  if (tid == 0) status[m] = st;
+  if (tid == 0) status[sidx] = st;
 }
 
 // W <- U^-1 L^-1 W for the shared-memory block W (n, nrhs), in place, by chunks of
@@ -617,12 +632,33 @@ __device__ void chunked_lu_solve(int n, int nrhs, int ws, const double* LU, doub
 // residual B - A X is one warp per row in double-double arithmetic, then the
 // reference's columnwise max-scaled acceptance (cuda.py:230-255).
 template <int NR>
+// With desc (ragged batches), CTA m solves columns c0 .. c0 + NR - 1 of the system
+// desc[m] describes (order n, nrhs columns, offsets, status word); a system with no
+// column in that range is skipped.
 __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
-    int n, int nrhs, int ldr, int c0, const double* __restrict__ mats, const double* __restrict__ factors,
-    const int32_t* __restrict__ piv, const double* __restrict__ rs, const double* __restrict__ cs,
-    const double* __restrict__ rhs, double* __restrict__ x, double rtol, double atol, int max_refine,
-    int32_t* __restrict__ status) {
+    int n_uniform, int nrhs_uniform, int ldr_uniform, int c0, const double* __restrict__ mats,
+    const double* __restrict__ factors, const int32_t* __restrict__ piv, const double* __restrict__ rs,
+    const double* __restrict__ cs, const double* __restrict__ rhs, double* __restrict__ x, double rtol, double atol,
+    int max_refine, int32_t* __restrict__ status, const mhm_ragged_matrix* __restrict__ desc, int max_n) {
   extern __shared__ __align__(16) double sm[];
+  int n = n_uniform, nrhs = nrhs_uniform, ldr = ldr_uniform, sidx = blockIdx.x;
+  size_t moff = (size_t)n_uniform * n_uniform * blockIdx.x, voff = (size_t)n_uniform * blockIdx.x,
+         roff = (size_t)n_uniform * ldr_uniform * blockIdx.x;
+  if (desc) {
+    const mhm_ragged_matrix d = desc[blockIdx.x];
+    n = d.n;
+    ldr = d.nrhs;
+    nrhs = min(NR, d.nrhs - c0);
+    sidx = d.slot;
+    moff = (size_t)d.mat_off;
+    voff = (size_t)d.vec_off;
+    roff = (size_t)d.rhs_off;
+    if (n < 1 || n > max_n) {
+      if (threadIdx.x == 0 && c0 == 0) status[sidx] = MHM_CELL_SIZE;
+      return;
+    }
+    if (nrhs < 1) return;
+  }
   // X and W are (n, nrhs) with an odd row stride ws = nrhs | 1, so that lanes reading
   // consecutive rows of one column hit distinct shared-memory banks
   const int ws = nrhs | 1;
@@ -634,19 +670,18 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
   int* perm = reinterpret_cast<int*>(colr + 3 * 16);
   int* iperm = perm + n;
   __shared__ int flag;
-  const int m = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
-  const size_t nn = (size_t)n * n;
-  const double* A = mats + nn * m;
-  const double* LU = factors + nn * m;
-  const double* rsc = rs + (size_t)n * m;
-  const double* csc = cs + (size_t)n * m;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  const double* A = mats + moff;
+  const double* LU = factors + moff;
+  const double* rsc = rs + voff;
+  const double* csc = cs + voff;
   // columns c0 .. c0 + nrhs - 1 of (n, ldr) row-major right-hand sides and solutions
-  const double* B = rhs + (size_t)n * ldr * m + c0;
-  double* Xg = x + (size_t)n * ldr * m + c0;
-  if (status[m] != MHM_CELL_OK) return;
+  const double* B = rhs + roff + c0;
+  double* Xg = x + roff + c0;
+  if (status[sidx] != MHM_CELL_OK) return;
   if (tid == 0) {
     for (int i = 0; i < n; ++i) perm[i] = i;
-    const int32_t* pv = piv + (size_t)n * m;
+    const int32_t* pv = piv + voff;
     for (int k = 0; k < n; ++k) {
       const int p = pv[k];
       if (p != k) { const int t = perm[k]; perm[k] = perm[p]; perm[p] = t; }
@@ -667,7 +702,7 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
       const size_t g = (size_t)(idx / NR) * ldr + idx % NR;
       Xg[g] = B[g];
     }
-    if (tid == 0) status[m] = MHM_CELL_NONFINITE;
+    if (tid == 0) status[sidx] = MHM_CELL_NONFINITE;
     return;
   }
   // per column: max |b| and ||b / scale||^2
@@ -860,7 +895,7 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
     const int i = idx / NR, c = idx % NR;
     if (c < nrhs) Xg[(size_t)i * ldr + c] = X[i * ws + c];
   }
-  if (tid == 0 && result != MHM_CELL_OK) status[m] = result;
+  if (tid == 0 && result != MHM_CELL_OK) status[sidx] = result;
 }
 
 size_t chunked_solve_smem(int n, int nrhs) {
@@ -886,7 +921,8 @@ extern "C" int mhm_batched_factor(int64_t count, int32_t n, const double* matric
                              (int)smem) != cudaSuccess)
       return MHM_ERR_LAUNCH;
     batched_factor_blocked_kernel<<<(unsigned)count, kLuThreads, smem, st>>>(n, matrices, factors, pivots,
-                                                                             row_scale, col_scale, status);
+                                                                             row_scale, col_scale, status,
+                                                                             nullptr, n);
     return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
   }
   const size_t smem = in_smem ? bytes : 0;
@@ -920,7 +956,8 @@ extern "C" int mhm_batched_solve(int64_t count, int32_t n, int32_t nrhs, const d
           cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
         return MHM_ERR_LAUNCH;
       kernel<<<(unsigned)count, kLuThreads, sm, st>>>(n, cols, nrhs, c0, matrices, factors, pivots, row_scale,
-                                                      col_scale, rhs, x, rtol, atol, max_refine, status);
+                                                      col_scale, rhs, x, rtol, atol, max_refine, status, nullptr,
+                                                      n);
       return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
     };
     for (int c0 = 0; c0 < nrhs; c0 += group) {
@@ -936,6 +973,48 @@ extern "C" int mhm_batched_solve(int64_t count, int32_t n, int32_t nrhs, const d
       n, nrhs, matrices, factors, pivots, row_scale, col_scale, rhs, x, work, rtol, atol, max_refine,
       status);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+extern "C" int mhm_batched_factor_ragged(int64_t count, const mhm_ragged_matrix* desc, int32_t max_n,
+                                         const double* matrices, double* factors, int32_t* pivots,
+                                         double* row_scale, double* col_scale, int32_t* status, void* stream) {
+  if (count < 1 || !desc || max_n < 1 || max_n > kBlockedMaxN || !matrices || !factors || !pivots || !row_scale ||
+      !col_scale || !status)
+    return MHM_ERR_ARGUMENT;
+  if (count > 0x7fffffff) return MHM_ERR_UNSUPPORTED;
+  const size_t smem = (size_t)max_n * kPanelStride * 8;
+  if (cudaFuncSetAttribute(batched_factor_blocked_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return MHM_ERR_LAUNCH;
+  batched_factor_blocked_kernel<<<(unsigned)count, kLuThreads, smem, static_cast<cudaStream_t>(stream)>>>(
+      max_n, matrices, factors, pivots, row_scale, col_scale, status, desc, max_n);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+extern "C" int mhm_batched_solve_ragged(int64_t count, const mhm_ragged_matrix* desc, int32_t max_n,
+                                        int32_t max_nrhs, const double* matrices, const double* factors,
+                                        const int32_t* pivots, const double* row_scale, const double* col_scale,
+                                        const double* rhs, double* x, double rtol, double atol, int32_t max_refine,
+                                        int32_t* status, void* stream) {
+  if (count < 1 || !desc || max_n < 1 || max_n > kBlockedMaxN || max_nrhs < 1 || !matrices || !factors ||
+      !pivots || !row_scale || !col_scale || !rhs || !x || !status || max_refine < 0 || !(rtol >= 0) ||
+      !(atol >= 0))
+    return MHM_ERR_ARGUMENT;
+  if (count > 0x7fffffff) return MHM_ERR_UNSUPPORTED;
+  const int group = max_nrhs < 16 ? max_nrhs : 16;
+  const size_t sm = chunked_solve_smem(max_n, group);
+  if (sm > 200 * 1024) return MHM_ERR_UNSUPPORTED;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaFuncSetAttribute(batched_solve_chunked_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
+      cudaSuccess)
+    return MHM_ERR_LAUNCH;
+  for (int c0 = 0; c0 < max_nrhs; c0 += 16) {
+    batched_solve_chunked_kernel<16><<<(unsigned)count, kLuThreads, sm, st>>>(
+        max_n, group, group, c0, matrices, factors, pivots, row_scale, col_scale, rhs, x, rtol, atol, max_refine,
+        status, desc, max_n);
+    if (cudaGetLastError() != cudaSuccess) return MHM_ERR_LAUNCH;
+  }
+  return MHM_OK;
 }
 
 extern "C" const char* mhm_version(void) { return "mhm_b200 0.1.0 (sm_100a)"; }

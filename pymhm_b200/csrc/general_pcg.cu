@@ -167,7 +167,7 @@ __device__ __forceinline__ double g0_apply(const mhm_general_system& s, const do
 
 // y = Q x, one warp per row, lanes over the columns (fixed order).  With qsmem the
 // CTA first copies x into shared memory; with qvec each lane streams its columns
-// as double2, eight loads in flight.
+// as double2, four loads in flight.
 __device__ void q_gemv(const GParams& P, const double* xin, double* yout) {
   extern __shared__ double2 xs2[];
   const mhm_general_system& s = P.s;
@@ -186,17 +186,6 @@ __device__ void q_gemv(const GParams& P, const double* xin, double* yout) {
       const double2* row = reinterpret_cast<const double2*>(s.coarse_inverse + c * (int64_t)M);
       double acc = 0.0;
       int d = lane;
-      for (; d + 224 < H; d += 256) {  // eight loads in flight per lane
-        double2 q[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) q[u] = __ldg(row + d + 32 * u);
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const double2 x = xs2[d + 32 * u];
-          acc = fma(q[u].x, x.x, acc);
-          acc = fma(q[u].y, x.y, acc);
-        }
-      }
       for (; d + 96 < H; d += 128) {
         const double2 q0 = __ldg(row + d), q1 = __ldg(row + d + 32), q2 = __ldg(row + d + 64),
                       q3 = __ldg(row + d + 96);

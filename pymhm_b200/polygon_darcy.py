@@ -100,8 +100,8 @@ class PolygonP2Plan:
     refinement): local meshes, couplings, bins, sparsity and every buffer."""
 
     def __init__(self, mesh: PolygonMesh, skeleton: EdgeSkeleton | None = None, refinements=2, *, order=4,
-                 bin_width=32, streams=4, device=None, global_rtol=1e-13, inner_rtol=1e-10, max_inner=20000,
-                 max_outer=8, preconditioner="cell"):
+                 bin_width=32, streams=4, ragged=True, device=None, global_rtol=1e-13, inner_rtol=1e-10,
+                 max_inner=20000, max_outer=8, preconditioner="cell"):
         import torch
 
         self.torch = torch
@@ -146,6 +146,7 @@ class PolygonP2Plan:
         self.field = None
         self.source = 0.0
         self.streams = max(1, int(streams))
+        self.ragged = bool(ragged)
         self._layout(int(bin_width))
 
     def _layout(self, bin_width: int):
@@ -254,6 +255,18 @@ class PolygonP2Plan:
         self.corrected = torch.empty(M, dtype=torch.uint8, device=dev)
         self.cell_status = torch.empty(M, dtype=torch.int32, device=dev)
         self.bin_streams = [torch.cuda.Stream(device=dev) for _ in range(min(self.streams, len(self.bins)))]
+        # one ragged descriptor per cell for the single-launch factor and solve, the
+        # largest systems first (CTAs start in this order)
+        desc = []
+        for b in reversed(self.bins):
+            nb, w = b["nb"], b["w"]
+            for j in range(b["k"]):
+                desc.append((b["dense"] + j * nb * nb, b["vec"] + j * nb, b["rhs"] + j * nb * w, nb, w, b["pos"] + j, 0))
+        rec = np.array(desc, dtype=[("mat_off", "<i8"), ("vec_off", "<i8"), ("rhs_off", "<i8"), ("n", "<i4"),
+                                    ("nrhs", "<i4"), ("slot", "<i4"), ("reserved", "<i4")])
+        self.d_ragged = torch.as_tensor(rec.view(np.uint8).copy()).to(dev)
+        self.ragged_max_n = int(max(b["nb"] for b in self.bins))
+        self.ragged_max_nrhs = int(max(b["w"] for b in self.bins))
         self.factor_status = torch.empty(M, dtype=torch.int32, device=dev)
         self.solve_status = torch.empty(M, dtype=torch.int32, device=dev)
         self.blocks = torch.empty(int(bofs[-1]), **f64)
@@ -265,23 +278,30 @@ class PolygonP2Plan:
         self.x = torch.empty(self.N, **f64)
         self.fields = torch.empty(self.nodes, **f64)
 
-    def autotune(self, permeability=1.0, source=0.0, *, widths=(16, 32, 64, 128), streams=(1, 4), repeats=2,
-                 cache=None):
-        """Choose the bin width and the number of bin streams by timing the local stage
-        (CUDA events, after one warm-up launch per candidate) on this device, keep the
-        fastest layout and return the choice with every timing.  ``cache``: a JSON file
-        recording choices per device and size signature (``autotune.choose``)."""
+    def autotune(self, permeability=1.0, source=0.0, *, widths=(16, 32, 64, 128), streams=(1, 4),
+                 ragged=(True, False), repeats=2, cache=None):
+        """Choose the bin width, the number of bin streams and whether the bins' LU
+        factorizations and checked solves run as one ragged launch each, by timing the
+        local stage (CUDA events, after one warm-up launch per candidate) on this
+        device; keep the fastest layout and return the choice with every timing.
+        ``cache``: a JSON file recording choices per device and size signature
+        (``autotune.choose``)."""
         from . import autotune as at
 
         torch = self.torch
         self.set_coefficients(permeability, source)
-        cands = [(int(w), int(k)) for w in widths for k in streams if int(w) >= 8 and int(k) >= 1]
+        cands = [(int(w), int(k), bool(g)) for w in widths for k in streams for g in ragged
+                 if int(w) >= 8 and int(k) >= 1]
 
-        def measure(c):
-            w, k = c
+        def apply(c):
+            w, k, g = c
+            self.ragged = bool(g)
             if (w, k) != (self.bin_width, self.streams):
                 self.streams = k
                 self._layout(w)
+
+        def measure(c):
+            apply(c)
             st = torch.cuda.current_stream()
             self.launch(st)
             times = []
@@ -295,10 +315,8 @@ class PolygonP2Plan:
 
         key = at.shape_key(torch.cuda.get_device_name(self.device), self.n_cells, self.t_cells)
         best, info = at.choose(cands, measure, key=key, cache=cache)
-        if tuple(best) != (self.bin_width, self.streams):
-            self.streams = int(best[1])
-            self._layout(int(best[0]))
-        return {"bin_width": self.bin_width, "streams": self.streams, **info}
+        apply(tuple(best))
+        return {"bin_width": self.bin_width, "streams": self.streams, "ragged": self.ragged, **info}
 
     def set_coefficients(self, permeability=1.0, source=0.0):
         """A ``DiscInclusions`` field or a positive constant permeability; a constant source."""
@@ -359,22 +377,33 @@ class PolygonP2Plan:
                                        P(d["edofs"]), P(d["dense_off"]), P(d["ld_of"]), P(d["load_off"]),
                                        P(self.stiffness), P(self.mass), P(self.load), sh), "mhm_p2_assemble")
         # the bins' chains are independent until the scatter: fork them over side
-        # streams (largest bins first) so that one bin's last wave overlaps the next's
-        fork = torch.cuda.Event()
-        fork.record(st)
-        used = []
-        for idx, b in enumerate(reversed(self.bins)):
-            bs = self.bin_streams[idx % len(self.bin_streams)]
-            if idx < len(self.bin_streams):
-                bs.wait_event(fork)
-                used.append(bs)
-            shb = _lib.stream_handle(bs)
-            v = self._bin_views(b)
-            k, nb, w, tld = b["k"], b["nb"], b["w"], b["tld"]
-            _lib.check(lib.mhm_dense_systems(k, nb, tld, nb, w, 1, P(v["n_of"]), P(v["t_of"]), P(v["stiffness"]),
-                                             P(v["mass"]), P(v["load"]), P(v["coupling"]), P(v["aug"]), P(v["rhs"]),
-                                             P(v["action"]), P(v["corrected"]), P(v["cell_status"]), shb),
-                       "mhm_dense_systems")
+        # streams (largest bins first) so that one bin's last wave overlaps the next's.
+        # With ``ragged`` the factorizations and the checked solves of all bins run as
+        # one launch each (ragged descriptors) between a forked system stage and a
+        # forked contribution stage.
+        def forked(stage):
+            fork = torch.cuda.Event()
+            fork.record(st)
+            used = []
+            for idx, b in enumerate(reversed(self.bins)):
+                bs = self.bin_streams[idx % len(self.bin_streams)]
+                if idx < len(self.bin_streams):
+                    bs.wait_event(fork)
+                    used.append(bs)
+                stage(b, self._bin_views(b), bs, _lib.stream_handle(bs))
+            for bs in used:
+                join = torch.cuda.Event()
+                join.record(bs)
+                st.wait_event(join)
+
+        def systems(b, v, bs, shb):
+            _lib.check(lib.mhm_dense_systems(b["k"], b["nb"], b["tld"], b["nb"], b["w"], 1, P(v["n_of"]), P(v["t_of"]),
+                                             P(v["stiffness"]), P(v["mass"]), P(v["load"]), P(v["coupling"]),
+                                             P(v["aug"]), P(v["rhs"]), P(v["action"]), P(v["corrected"]),
+                                             P(v["cell_status"]), shb), "mhm_dense_systems")
+
+        def factor_solve(b, v, bs, shb):
+            k, nb, w = b["k"], b["nb"], b["w"]
             _lib.check(lib.mhm_batched_factor(k, nb, P(v["aug"]), P(v["factors"]), P(v["pivots"]), P(v["rs"]),
                                               P(v["cs"]), P(v["factor_status"]), shb), "mhm_batched_factor")
             with torch.cuda.stream(bs):
@@ -382,14 +411,34 @@ class PolygonP2Plan:
             _lib.check(lib.mhm_batched_solve(k, nb, w, P(v["aug"]), P(v["factors"]), P(v["pivots"]), P(v["rs"]),
                                              P(v["cs"]), P(v["rhs"]), P(v["solution"]), P(v["work"]), 1e-10, 0.0,
                                              2, P(v["solve_status"]), shb), "mhm_batched_solve")
-            _lib.check(lib.mhm_dense_contributions(k, nb, tld, nb, w, tld, P(v["n_of"]), P(v["t_of"]),
-                                                   P(v["solution"]), P(v["coupling"]), P(v["action"]),
-                                                   P(v["load"]), P(v["block_off"]), P(v["lofs"]), P(self.blocks),
-                                                   P(self.loads), shb), "mhm_dense_contributions")
-        for bs in used:
-            join = torch.cuda.Event()
-            join.record(bs)
-            st.wait_event(join)
+
+        def contributions(b, v, bs, shb):
+            _lib.check(lib.mhm_dense_contributions(b["k"], b["nb"], b["tld"], b["nb"], b["w"], b["tld"],
+                                                   P(v["n_of"]), P(v["t_of"]), P(v["solution"]), P(v["coupling"]),
+                                                   P(v["action"]), P(v["load"]), P(v["block_off"]), P(v["lofs"]),
+                                                   P(self.blocks), P(self.loads), shb), "mhm_dense_contributions")
+
+        if self.ragged:
+            forked(systems)
+            cnt = len(self.order)
+            _lib.check(lib.mhm_batched_factor_ragged(cnt, P(self.d_ragged), self.ragged_max_n, P(self.aug),
+                                                     P(self.factors), P(self.pivots), P(self.row_scale),
+                                                     P(self.col_scale), P(self.factor_status), sh),
+                       "mhm_batched_factor_ragged")
+            with torch.cuda.stream(st):
+                self.solve_status.copy_(self.factor_status)
+            _lib.check(lib.mhm_batched_solve_ragged(cnt, P(self.d_ragged), self.ragged_max_n, self.ragged_max_nrhs,
+                                                    P(self.aug), P(self.factors), P(self.pivots), P(self.row_scale),
+                                                    P(self.col_scale), P(self.rhs), P(self.solution), 1e-10, 0.0, 2,
+                                                    P(self.solve_status), sh), "mhm_batched_solve_ragged")
+            forked(contributions)
+        else:
+            def chain(b, v, bs, shb):
+                systems(b, v, bs, shb)
+                factor_solve(b, v, bs, shb)
+                contributions(b, v, bs, shb)
+
+            forked(chain)
         mark(1)
         p = self.pattern
         _lib.check(lib.mhm_skeleton_scatter(len(p.indices), P(d["slot_ptr"]), P(d["contrib"]), P(self.blocks),

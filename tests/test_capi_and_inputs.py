@@ -38,13 +38,14 @@ def test_struct_layout_matches_header(tmp_path):
     src = tmp_path / "layout.c"
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "mhm_b200.h"\n'
-        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n\", sizeof(mhm_q1_problem),"
+        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n\", sizeof(mhm_q1_problem),"
         " offsetof(mhm_q1_problem, kappa_const), offsetof(mhm_q1_problem, quad_order),"
         " sizeof(mhm_skeleton_system), offsetof(mhm_skeleton_system, nx),"
         " offsetof(mhm_skeleton_system, coarse_ay), offsetof(mhm_q1_problem, pixel_origin),"
         " offsetof(mhm_q1_problem, pixel_ny), sizeof(mhm_general_system), offsetof(mhm_general_system, cells),"
         " offsetof(mhm_general_system, coarse_inverse), offsetof(mhm_general_system, block_off),"
-        " offsetof(mhm_general_system, max_trace_row)); return 0;}\n")
+        " offsetof(mhm_general_system, max_trace_row), sizeof(mhm_ragged_matrix),"
+        " offsetof(mhm_ragged_matrix, slot)); return 0;}\n")
     exe = tmp_path / "layout"
     subprocess.run(["gcc", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
@@ -52,7 +53,8 @@ def test_struct_layout_matches_header(tmp_path):
             ctypes.sizeof(_lib.SkeletonSystem), _lib.SkeletonSystem.nx.offset, _lib.SkeletonSystem.coarse_ay.offset,
             _lib.Q1Problem.pixel_origin.offset, _lib.Q1Problem.pixel_ny.offset, ctypes.sizeof(_lib.GeneralSystem),
             _lib.GeneralSystem.cells.offset, _lib.GeneralSystem.coarse_inverse.offset,
-            _lib.GeneralSystem.block_off.offset, _lib.GeneralSystem.max_trace_row.offset]
+            _lib.GeneralSystem.block_off.offset, _lib.GeneralSystem.max_trace_row.offset,
+            ctypes.sizeof(_lib.RaggedMatrix), _lib.RaggedMatrix.slot.offset]
     assert got == want
 
 

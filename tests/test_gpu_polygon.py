@@ -130,9 +130,29 @@ def test_polygon_autotune_keeps_the_solution(tmp_path):
     cache = tmp_path / "tune.json"
     out = plan.autotune(field, 1.0, widths=(16, 64), streams=(1, 2), cache=cache)
     assert (out["bin_width"], out["streams"]) in {(16, 1), (16, 2), (64, 1), (64, 2)}
-    assert len(out["timings_ms"]) == 4 and not out["cached"]
+    assert len(out["timings_ms"]) == 8 and not out["cached"]
     sol = plan.solve(field, 1.0)
     assert rel(sol.trace, ref.trace) <= 1e-11
     assert rel(np.concatenate(sol.fields), np.concatenate(ref.fields)) <= 1e-11
     again = PolygonP2Plan(mesh, sk, rs).autotune(field, 1.0, widths=(16, 64), streams=(1, 2), cache=cache)
-    assert again["cached"] and (again["bin_width"], again["streams"]) == (out["bin_width"], out["streams"])
+    assert again["cached"]
+    assert (again["bin_width"], again["streams"], again["ragged"]) == (out["bin_width"], out["streams"], out["ragged"])
+
+
+def test_polygon_ragged_launch_equals_per_bin_launches():
+    """The single ragged factor / solve launch agrees with the per-bin launches to
+    rounding (bins of order <= 160 factor in shared memory on the per-bin path and with
+    the blocked kernel in the ragged launch)."""
+    from pymhm_b200.polygon import EdgeSkeleton, voronoi_mesh
+    from pymhm_b200.polygon_darcy import PolygonP2Plan
+    from pymhm_b200.workloads import DiscInclusions, disc_inclusions
+
+    mesh = voronoi_mesh(60, 29)
+    sk = EdgeSkeleton(mesh)
+    rs = np.random.default_rng(29).integers(2, 5, size=60)
+    field = DiscInclusions(*disc_inclusions(30, rmin=0.01, rmax=0.03, seed=30), inside=30.0)
+    a = PolygonP2Plan(mesh, sk, rs, ragged=True).solve(field, 1.0)
+    b = PolygonP2Plan(mesh, sk, rs, ragged=False).solve(field, 1.0)
+    assert rel(a.trace, b.trace) <= 1e-11
+    assert rel(np.concatenate(a.fields), np.concatenate(b.fields)) <= 1e-11
+    assert a.residual <= 1e-12 and b.residual <= 1e-12
