@@ -788,7 +788,9 @@ __global__ void __launch_bounds__(kGThreads, 1) general_pcg_kernel(const GParams
       ++outer;
       ++steps;
       {
-        const double need = 0.1 * fmin(P.rtol * bnorm / est, P.rtol / omega);
+        // the componentwise error is taken to shrink with the cycle's residual estimate
+        // (omega was measured at the cycle's start, where the estimate is beta0)
+        const double need = 0.1 * fmin(P.rtol * bnorm / est, P.rtol / (omega * (est / beta0)));
         status = inner_solve(P, ib, isc, zj, need, epoch, total_inner);
         if (status != MHM_SOLVE_OK) goto done;
       }

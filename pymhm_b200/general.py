@@ -145,7 +145,7 @@ class GeneralSkeleton:
         self.info = torch.zeros(4, dtype=torch.int32, device=self.device)
         self.stats = torch.zeros(3, dtype=torch.float64, device=self.device)
 
-    def launch(self, values, rhs, x, *, blocks=None, rtol=1e-13, inner_rtol=1e-10, max_inner=20000, max_outer=8,
+    def launch(self, values, rhs, x, *, blocks=None, rtol=1e-13, inner_rtol=1e-10, max_inner=20000, max_outer=16,
                stream=None):
         """Enqueue x = K^-1 rhs for the CSR ``values`` (device tensors, no host sync).
 

@@ -101,7 +101,7 @@ class PolygonP2Plan:
 
     def __init__(self, mesh: PolygonMesh, skeleton: EdgeSkeleton | None = None, refinements=2, *, order=4,
                  bin_width=32, streams=4, ragged=True, device=None, global_rtol=1e-13, inner_rtol=1e-10,
-                 max_inner=20000, max_outer=8, preconditioner="cell"):
+                 max_inner=20000, max_outer=16, preconditioner="cell"):
         import torch
 
         self.torch = torch

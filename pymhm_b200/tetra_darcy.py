@@ -54,7 +54,7 @@ class TetraP1Plan:
     refinement): topology, tables, sparsity and every buffer of the launch sequence."""
 
     def __init__(self, mesh: TetraMesh, skeleton: TriangularSkeleton | None = None, local_refinement: int = 2, *,
-                 device=None, global_rtol=1e-13, inner_rtol=1e-10, max_inner=20000, max_outer=8,
+                 device=None, global_rtol=1e-13, inner_rtol=1e-10, max_inner=20000, max_outer=16,
                  preconditioner="cell"):
         import torch
 
