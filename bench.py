@@ -311,16 +311,37 @@ def tetra_campaign(torch, steps=5, warmup=2, cube=8, local=8, cpu_cells=16, prec
     return out
 
 
+def passing_contrast(plan, discs, inside, fallbacks=(10.0, 3.0, 1.0)):
+    """The largest disc permeability of ``inside`` and ``fallbacks`` at which every cell's
+    local solve meets the reference's contract (its columnwise 1e-10 residual after two
+    corrections), with the failing cells counted at each one tried.  Voronoi cells
+    with short edges give sliver triangles, and some of those cells' systems are too
+    ill-conditioned for binary64 to reach 1e-10 once the discs add contrast; the
+    oracle (the reference's local solve) fails the same cells."""
+    from pymhm_b200.workloads import DiscInclusions
+
+    tried = []
+    for value in (inside, *[v for v in fallbacks if v < inside]):
+        plan.set_coefficients(DiscInclusions(*discs, inside=value), 1.0)
+        plan.launch()
+        bad = plan.failed_cells()
+        tried.append({"disc_permeability": value, "failing_cells": len(bad), "first": [int(c) for c in bad[:5]]})
+        if not len(bad):
+            return value, tried
+    raise RuntimeError(f"local contract fails at every contrast tried: {tried}")
+
+
 def polygon_campaign(torch, steps=3, warmup=1, count=2000, cpu_cells=8, preconditioner="cell", inside=30.0,
-                     contract_inside=1e4):
-    """Polygonal P2 Darcy (config 3 at local sizes up to 639): the Voronoi cells of
-    2000 seeded points in the unit square, each refined with the largest subdivision
-    count whose P2 space stays within a size drawn uniformly in [200, 639] (the batched
-    LU's blocked range; the configuration's 640-3000 sizes are not built), one Legendre P1
-    face space per edge (4-10 edges, 8-20 trace DOFs per cell), 300 seeded discs of
-    radius 0.01-0.03 with permeability ``inside`` in a background of 1, f = 1,
-    homogeneous Dirichlet data, FP64.  One solve at a time with CUDA events per stage;
-    the oracle's local stage on a sample of cells in this process beside it.
+                     contract_inside=1e4, lo=200, hi=3000):
+    """Polygonal P2 Darcy (config 3): the Voronoi cells of 2000 seeded points in the unit
+    square, each refined with the largest subdivision count whose P2 space stays within
+    a size drawn uniformly in [lo, hi] = [200, 3000], one Legendre P1 face space per edge
+    (4-10 edges, 8-20 trace DOFs per cell), 300 seeded discs of radius 0.01-0.03 with
+    permeability ``inside`` in a background of 1, f = 1, homogeneous Dirichlet data,
+    FP64.  Augmented orders up to 640 run in the small tier (ragged launches of the
+    shared-memory-panel LU), larger ones in the large tier (chunks of the windowed-pivot
+    LU in HBM).  One solve at a time with CUDA events per stage; the oracle's local
+    stage on a sample of cells in this process beside it.
 
     At the configuration's contrast of 1e4 the reference's own local solves fail its
     columnwise 1e-10 residual test on some of these cells (the same contract here), so
@@ -334,16 +355,18 @@ def polygon_campaign(torch, steps=3, warmup=1, count=2000, cpu_cells=8, precondi
     t0 = time.perf_counter()
     mesh = voronoi_mesh(count, SEED)
     sk = EdgeSkeleton(mesh)
-    rs = refinement_for_sizes(mesh, seed=SEED + 1)
+    rs = refinement_for_sizes(mesh, lo, hi, seed=SEED + 1)
     discs = disc_inclusions(300, rmin=0.01, rmax=0.03, seed=SEED + 2)
     field = DiscInclusions(*discs, inside=inside)
-    plan = PolygonP2Plan(mesh, sk, rs, preconditioner=preconditioner)
+    plan = PolygonP2Plan(mesh, sk, rs, preconditioner=preconditioner, workers=min(16, os.cpu_count() or 1))
     plan_s = time.perf_counter() - t0
     failed = []
     if contract_inside:
         plan.set_coefficients(DiscInclusions(*discs, inside=contract_inside), 1.0)
         plan.launch()
         failed = plan.failed_cells()
+    inside, tried = passing_contrast(plan, discs, inside)
+    field = DiscInclusions(*discs, inside=inside)
     plan.set_coefficients(field, 1.0)
     st = torch.cuda.current_stream()
     for _ in range(warmup):
@@ -363,10 +386,12 @@ def polygon_campaign(torch, steps=3, warmup=1, count=2000, cpu_cells=8, precondi
            "stages_ms": {"local_stage": float(per[:, 0].mean()), "skeleton_scatter": float(per[:, 1].mean()),
                          "general_pcg": float(per[:, 2].mean()), "reconstruct": float(per[:, 3].mean())},
            "macrocells": plan.M, "local_sizes": [int(plan.n_cells.min()), int(plan.n_cells.max())],
+           "large_tier": {"cells": int(sum(b["k"] for b in plan.bins if b["large"])), "chunks": len(plan.chunks),
+                          "workspace_gb": 2 * (0 if plan.ws_aug is None else plan.ws_aug.numel()) * 8 / 1e9},
            "trace_per_cell": [int(plan.t_cells.min()), int(plan.t_cells.max())], "bins": len(plan.bins),
            "skeleton_unknowns": plan.N, "global_iterations": sol.global_iterations,
            "outer_corrections": sol.outer_corrections, "residual": sol.residual, "preconditioner": preconditioner,
-           "disc_permeability": inside, "plan_build_s": plan_s}
+           "disc_permeability": inside, "contrasts_tried": tried, "plan_build_s": plan_s}
     if contract_inside:
         out["contract_failures"] = {"disc_permeability": contract_inside, "cells": len(failed),
                                     "first": [int(c) for c in failed[:10]]}
@@ -406,9 +431,11 @@ def profile_case(torch, cube=0, count=0):
         from pymhm_b200.polygon_darcy import PolygonP2Plan, refinement_for_sizes
 
         mesh = voronoi_mesh(count, SEED)
-        plan = PolygonP2Plan(mesh, EdgeSkeleton(mesh), refinement_for_sizes(mesh, seed=SEED + 1))
-        plan.set_coefficients(DiscInclusions(*disc_inclusions(300, rmin=0.01, rmax=0.03, seed=SEED + 2),
-                                             inside=30.0), 1.0)
+        plan = PolygonP2Plan(mesh, EdgeSkeleton(mesh), refinement_for_sizes(mesh, 200, 3000, seed=SEED + 1),
+                             workers=min(16, os.cpu_count() or 1))
+        discs = disc_inclusions(300, rmin=0.01, rmax=0.03, seed=SEED + 2)
+        inside, _ = passing_contrast(plan, discs, 30.0)
+        plan.set_coefficients(DiscInclusions(*discs, inside=inside), 1.0)
         launches = 1
     for _ in range(launches):
         plan.launch()
@@ -493,8 +520,8 @@ def parse():
                     help="only two solves of the 3D workload on the unit cube split into C^3 x 6 macro tetrahedra "
                          "(local refinement 8, the 40-layer field), for ncu")
     ap.add_argument("--polygon-case", type=int, default=0, metavar="M",
-                    help="only one solve of the polygon workload with M Voronoi cells (P2 sizes 200-639, "
-                         "disc permeability 30), for ncu")
+                    help="only the polygon workload with M Voronoi cells (P2 sizes 200-3000): the contrast "
+                         "search (disc permeability 30, else 10, 3, 1) and one solve, for ncu")
     ap.add_argument("--serving-full", action="store_true",
                     help="only the streamed-serving workload at its full size: 2000 requests at each of "
                          "50, 100, 200, 500, 1000 and 2000 arrivals/s, mixed and FP64")

@@ -552,6 +552,26 @@ int mhm_p2_assemble(int64_t elements, const double* points, const int64_t* trian
                     const int64_t* load_off, double* stiffness, double* mass, double* load,
                     void* stream);
 
+/*
+ * The two passes of mhm_p2_assemble as separate calls (the same arithmetic), for
+ * local matrices too large to hold at once: mhm_p2_elements fills element_scratch
+ * for every fine triangle; mhm_p2_assemble_rows then builds the dense rows of any
+ * contiguous range of nodes (node_cell, node_row and inc_ptr offset to its first
+ * node; dense_off may address a workspace that holds only those cells).
+ * Replaces, with mhm_p2_assemble, scalar_operators (fem/scalar/triangle.py:208-257)
+ * for the cells of a polygon batch whose P2 spaces exceed 639 unknowns.
+ */
+int mhm_p2_elements(int64_t elements, const double* points, const int64_t* triangles, int32_t nquad,
+                    const double* quad_bary, const double* quad_weights, int32_t grid,
+                    const int32_t* grid_ptr, const int32_t* grid_discs, const double* centres,
+                    const double* radii2, double inside, double outside, double source,
+                    double* element_scratch, void* stream);
+int mhm_p2_assemble_rows(int64_t nodes, const int32_t* node_cell, const int32_t* node_row,
+                         const int64_t* inc_ptr, const int64_t* inc, const int32_t* elem_dofs,
+                         const double* element_scratch, const int64_t* dense_off, const int32_t* ld_of,
+                         const int64_t* load_off, double* stiffness, double* mass, double* load,
+                         void* stream);
+
 /* u_K = R f - (R B) lambda_K + (1 - R A 1) c_K for dense cells (core/reconstruction.py:
  * 130-141): cell k's n_of[k] values go to fields + field_off[k]; its trace DOFs
  * are cell_dofs[dof_off[k] ...], its coarse unknown x[trace_size + cell_id[k]]. */
@@ -626,6 +646,30 @@ int mhm_batched_solve_ragged(int64_t count, const mhm_ragged_matrix* desc, int32
                              const int32_t* pivots, const double* row_scale, const double* col_scale,
                              const double* rhs, double* x, double rtol, double atol, int32_t max_refine,
                              int32_t* status, void* stream);
+
+/*
+ * Large orders (n <= 4096; larger get MHM_CELL_SIZE): ragged batches of the bordered
+ * local systems [[A, c], [c^T, 0]] (A positive semi-definite with the constants as
+ * its kernel, identity padding allowed).  The factorization is the blocked LU in
+ * HBM with the row search of each column restricted to its 32-column panel's
+ * diagonal window and the one row below it (the bordering row needs no more: the
+ * node rows' leading blocks are positive definite); the factors, pivots (LAPACK
+ * sequence), scales, rank test and status words are those of
+ * mhm_batched_factor_ragged, so the solve contract is the same.  The solve keeps
+ * its solution and correction blocks in `work`: 34 doubles per row of every system,
+ * system k's at work + 34 vec_off.  Replaces the reference's large-block route,
+ * `_condense_device` (execution/cuda.py:314-343: sparse cuDSS through the checked
+ * factorization for augmented sizes above dense_size_limit = 512, cuda.py:352), for
+ * the polygon batch's local P2 systems of order 640 to 4096.
+ */
+int mhm_batched_factor_large(int64_t count, const mhm_ragged_matrix* desc, int32_t max_n,
+                             const double* matrices, double* factors, int32_t* pivots,
+                             double* row_scale, double* col_scale, int32_t* status, void* stream);
+int mhm_batched_solve_large(int64_t count, const mhm_ragged_matrix* desc, int32_t max_n,
+                            int32_t max_nrhs, const double* matrices, const double* factors,
+                            const int32_t* pivots, const double* row_scale, const double* col_scale,
+                            const double* rhs, double* x, double* work, double rtol, double atol,
+                            int32_t max_refine, int32_t* status, void* stream);
 
 /* Library version string (host). */
 const char* mhm_version(void);

@@ -528,6 +528,242 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
   if (tid == 0) status[sidx] = st;
 }
 
+// ---------------------------------------------------------------------------------
+// Large orders (640 < n <= kLargeMaxN): blocked right-looking LU of one matrix per CTA
+// held in `factors` (HBM), with the row search of each column restricted to the
+// panel's diagonal window: rows kb .. kb + w of the panel kb .. kb + w - 1 (w <= 32
+// columns, one row past the block).  The local systems this serves are bordered
+// positive semi-definite matrices [[A, c], [c^T, 0]] (A with the constants as its
+// kernel, c^T 1 != 0) padded with identity rows.  For such a matrix every leading
+// block of node rows is positive definite, and the Schur complement left after any
+// panel does not depend on the row order inside the panel's window, so the trailing
+// matrix stays positive definite up to the last node row; the one pivot that needs a
+// row exchange is the last node's (zero in exact arithmetic), which the window's extra
+// row (the bordering row, directly below it) supplies.  Rows below the window are
+// never searched: their multipliers are the independent substitutions
+// L21 = A21 U11^-1, and no column has to be read whole before its pivot is known.
+// Per panel:
+//   (a) the window ((w + 1) x w) is factored in shared memory with partial pivoting
+//       over its rows (first maximum, as the other kernels);
+//   (b) the window's row exchanges are applied to the other columns of its rows;
+//   (c) U12 = L11^-1 A12, a thread per column;
+//   (d) L21 = A21 U11^-1 for the rows below the window, a thread per row;
+//   (e) A22 -= L21 U12 on the FP64 tensor cores: U12 is staged in shared memory 64
+//       columns at a time and each warp walks its 8-row blocks of the trailing matrix
+//       against that tile (A = -L21 and C from global memory, B from shared memory).
+// The pivot sequence is LAPACK's (piv[k] = row exchanged with k at step k), so the
+// solves of the blocked kernel apply unchanged.  The rank test is the same.
+// ---------------------------------------------------------------------------------
+constexpr int kLargeMaxN = 4096;
+constexpr int kUTile = 64;
+constexpr int kUStride = kUTile + 4;  // row stride of the staged U12 tile
+
+__global__ void __launch_bounds__(kLuThreads, 2) large_factor_kernel(
+    const mhm_ragged_matrix* __restrict__ desc, int max_n, const double* __restrict__ mats,
+    double* __restrict__ factors, int32_t* __restrict__ piv, double* __restrict__ rs, double* __restrict__ cs,
+    int32_t* __restrict__ status) {
+  __shared__ double Pn[(kPanel + 1) * kPanelStride];  // the window: (w + 1) x w
+  __shared__ double Us[kPanel * kUStride];             // U12 tile: 32 x 64
+  __shared__ double red[32];
+  __shared__ int sperm[kPanel];
+  __shared__ int apos[2 * kPanel + 2], asrc[2 * kPanel + 2];
+  __shared__ int srcrow[kPanel + 1];
+  __shared__ int naff;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  const mhm_ragged_matrix d = desc[blockIdx.x];
+  const int n = d.n, sidx = d.slot;
+  if (n < 1 || n > max_n) {
+    if (tid == 0) status[sidx] = MHM_CELL_SIZE;
+    return;
+  }
+  const size_t voff = (size_t)d.vec_off;
+  double* F = factors + d.mat_off;
+  int st = equilibrate(n, mats + d.mat_off, F, rs + voff, cs + voff);
+  for (int kb = 0; kb < n && st == MHM_CELL_OK; kb += kPanel) {
+    const int w = min(kPanel, n - kb), h = min(w + 1, n - kb);
+    for (int idx = tid; idx < h * kPanel; idx += blockDim.x) {
+      const int r = idx >> 5, c = idx & 31;
+      if (c < w) Pn[r * kPanelStride + c] = F[(size_t)(kb + r) * n + kb + c];
+    }
+    __syncthreads();
+    for (int c = 0; c < w; ++c) {
+      // the previous column's multipliers are scaled in the pivot-search phase (its
+      // elimination ended at the last barrier; the columns differ)
+      if (c > 0) {
+        const double pinv = 1.0 / Pn[(c - 1) * kPanelStride + (c - 1)];
+        for (int r = c + tid; r < h; r += blockDim.x) Pn[r * kPanelStride + c - 1] *= pinv;
+      }
+      if (wid == nw - 1) {
+        double best = -1.0;
+        int bi = c;
+        for (int r = c + lane; r < h; r += 32) {
+          const double v = fabs(Pn[r * kPanelStride + c]);
+          if (v > best) { best = v; bi = r; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+          const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+          if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+        }
+        if (lane == 0) sperm[c] = bi;
+      }
+      __syncthreads();
+      const int p = sperm[c];
+      if (p != c && tid < w) {
+        const double t = Pn[c * kPanelStride + tid];
+        Pn[c * kPanelStride + tid] = Pn[p * kPanelStride + tid];
+        Pn[p * kPanelStride + tid] = t;
+      }
+      __syncthreads();
+      const double dg = Pn[c * kPanelStride + c];
+      if (dg == 0.0) { st = MHM_CELL_SINGULAR_PIVOT; break; }
+      const double inv = 1.0 / dg;
+      // (row below the pivot, column right of it): at most 32 x 31 independent pairs
+      const int cols = w - c - 1, rows = h - c - 1;
+      for (int idx = tid; idx < rows * 32; idx += blockDim.x) {
+        const int r = c + 1 + (idx >> 5), j = c + 1 + (idx & 31);
+        if (j - c - 1 < cols)
+          Pn[r * kPanelStride + j] = fma(-Pn[r * kPanelStride + c] * inv, Pn[c * kPanelStride + j],
+                                         Pn[r * kPanelStride + j]);
+      }
+      __syncthreads();
+    }
+    if (st != MHM_CELL_OK) break;
+    {
+      const double pinv = 1.0 / Pn[(w - 1) * kPanelStride + (w - 1)];
+      for (int r = w + tid; r < h; r += blockDim.x) Pn[r * kPanelStride + w - 1] *= pinv;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < h * kPanel; idx += blockDim.x) {
+      const int r = idx >> 5, c = idx & 31;
+      if (c < w) F[(size_t)(kb + r) * n + kb + c] = Pn[r * kPanelStride + c];
+    }
+    for (int c = tid; c < w; c += blockDim.x) piv[voff + kb + c] = kb + sperm[c];
+    // (b) compose the window's exchanges: srcrow[r] = the window row that ends at r
+    if (tid == 0) {
+      for (int r = 0; r < h; ++r) srcrow[r] = r;
+      for (int c = 0; c < w; ++c) {
+        const int p = sperm[c];
+        if (p != c) {
+          const int t = srcrow[c];
+          srcrow[c] = srcrow[p];
+          srcrow[p] = t;
+        }
+      }
+      int cnt = 0;
+      for (int r = 0; r < h; ++r)
+        if (srcrow[r] != r) {
+          apos[cnt] = r;
+          asrc[cnt] = srcrow[r];
+          ++cnt;
+        }
+      naff = cnt;
+    }
+    __syncthreads();
+    const int moved = naff;
+    if (moved > 0)
+      for (int j = tid; j < n - w; j += blockDim.x) {
+        const int col = j < kb ? j : j + w;
+        double v[kPanel + 1];
+#pragma unroll
+        for (int k = 0; k < kPanel + 1; ++k) v[k] = k < moved ? F[(size_t)(kb + asrc[k]) * n + col] : 0.0;
+#pragma unroll
+        for (int k = 0; k < kPanel + 1; ++k)
+          if (k < moved) F[(size_t)(kb + apos[k]) * n + col] = v[k];
+      }
+    __syncthreads();
+    // (c) U12 = L11^-1 A12
+    for (int j = kb + w + tid; j < n; j += blockDim.x) {
+      double x[kPanel];
+#pragma unroll
+      for (int r = 0; r < kPanel; ++r) x[r] = r < w ? F[(size_t)(kb + r) * n + j] : 0.0;
+#pragma unroll
+      for (int r = 1; r < kPanel; ++r)
+#pragma unroll
+        for (int q = 0; q < r; ++q) x[r] = fma(-Pn[r * kPanelStride + q], x[q], x[r]);
+#pragma unroll
+      for (int r = 0; r < kPanel; ++r)
+        if (r < w) F[(size_t)(kb + r) * n + j] = x[r];
+    }
+    // (d) L21 = A21 U11^-1 for the rows below the window
+    for (int r = kb + h + tid; r < n; r += blockDim.x) {
+      double x[kPanel];
+#pragma unroll
+      for (int j = 0; j < kPanel; ++j) x[j] = j < w ? F[(size_t)r * n + kb + j] : 0.0;
+#pragma unroll
+      for (int j = 0; j < kPanel; ++j) {
+        double v = x[j];
+#pragma unroll
+        for (int q = 0; q < j; ++q) v = fma(-x[q], Pn[q * kPanelStride + j], v);
+        x[j] = j < w ? v * (1.0 / Pn[j * kPanelStride + j]) : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < kPanel; ++j)
+        if (j < w) F[(size_t)r * n + kb + j] = x[j];
+    }
+    __syncthreads();
+    // (e) A22 -= L21 U12.  Fragments: A[lane/4][lane%4], B[lane%4][lane/4],
+    // C[lane/4][2 (lane%4) + {0, 1}]; panel columns past w are masked to 0.
+    const int m2 = n - kb - w, base = kb + w;
+    const int fr = lane >> 2, fc = lane & 3;
+    const int ksteps = (w + 3) >> 2;
+    for (int tj = 0; tj < m2; tj += kUTile) {
+      for (int idx = tid; idx < kPanel * kUTile; idx += blockDim.x) {
+        const int r = idx >> 6, c = idx & (kUTile - 1);
+        Us[r * kUStride + c] = (r < w && tj + c < m2) ? F[(size_t)(kb + r) * n + base + tj + c] : 0.0;
+      }
+      __syncthreads();
+      for (int rb = 8 * wid; rb < m2; rb += 8 * nw) {
+        const int i = rb + fr;
+        const size_t row = (size_t)(base + (i < m2 ? i : m2 - 1)) * n;
+        double av[kPanel / 4];
+#pragma unroll
+        for (int s = 0; s < kPanel / 4; ++s) {
+          const int q = 4 * s + fc;
+          av[s] = q < w ? -F[row + kb + q] : 0.0;
+        }
+        double acc[8][2];
+#pragma unroll
+        for (int b = 0; b < 8; ++b)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int j = tj + 8 * b + 2 * fc + e;
+            acc[b][e] = (i < m2 && j < m2) ? F[row + base + j] : 0.0;
+          }
+#pragma unroll
+        for (int s = 0; s < kPanel / 4; ++s) {
+          if (s >= ksteps) break;
+          double bv[8];
+#pragma unroll
+          for (int b = 0; b < 8; ++b) bv[b] = Us[(4 * s + fc) * kUStride + 8 * b + fr];
+#pragma unroll
+          for (int b = 0; b < 8; ++b) dmma_8x8x4(acc[b][0], acc[b][1], av[s], bv[b]);
+        }
+        if (i < m2) {
+#pragma unroll
+          for (int b = 0; b < 8; ++b)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int j = tj + 8 * b + 2 * fc + e;
+              if (j < m2) F[row + base + j] = acc[b][e];
+            }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (st == MHM_CELL_OK) {
+    double dmin = 1e300, amax = 0.0;
+    for (int i = tid; i < n; i += blockDim.x) dmin = fmin(dmin, fabs(F[(size_t)i * n + i]));
+    for (int i = wid; i < n; i += nw)
+      for (int j = lane; j < n; j += 32) amax = fmax(amax, fabs(F[(size_t)i * n + j]));
+    dmin = block_min(dmin, red);
+    amax = block_max(amax, red);
+    if (dmin <= 2.220446049250313e-16 * n * amax) st = MHM_CELL_RANK_DEFICIENT;
+  }
+  if (tid == 0) status[sidx] = st;
+}
+
 // W <- U^-1 L^-1 W for the shared-memory block W (n, nrhs), in place, by chunks of
 // 32 rows (right-looking): the chunk's diagonal block (in Dg) is solved with one
 // warp per column, a lane per row; then every row beyond the chunk subtracts its
@@ -631,15 +867,19 @@ __device__ void chunked_lu_solve(int n, int nrhs, int ws, const double* LU, doub
 // permutation is composed once, every application reads the factors in chunks, the
 // residual B - A X is one warp per row in double-double arithmetic, then the
 // reference's columnwise max-scaled acceptance (cuda.py:230-255).
-template <int NR>
 // With desc (ragged batches), CTA m solves columns c0 .. c0 + NR - 1 of the system
 // desc[m] describes (order n, nrhs columns, offsets, status word); a system with no
-// column in that range is skipped.
+// column in that range is skipped.  With GW (large orders), the solution and the
+// correction blocks X and W live in gwork (2 x 17 doubles per row of the system, at
+// 34 vec_off) instead of shared memory, and the accurate residual reads its rows
+// without the register prefetch.
+template <int NR, bool GW = false>
 __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
     int n_uniform, int nrhs_uniform, int ldr_uniform, int c0, const double* __restrict__ mats,
     const double* __restrict__ factors, const int32_t* __restrict__ piv, const double* __restrict__ rs,
     const double* __restrict__ cs, const double* __restrict__ rhs, double* __restrict__ x, double rtol, double atol,
-    int max_refine, int32_t* __restrict__ status, const mhm_ragged_matrix* __restrict__ desc, int max_n) {
+    int max_refine, int32_t* __restrict__ status, const mhm_ragged_matrix* __restrict__ desc, int max_n,
+    double* __restrict__ gwork) {
   extern __shared__ __align__(16) double sm[];
   int n = n_uniform, nrhs = nrhs_uniform, ldr = ldr_uniform, sidx = blockIdx.x;
   size_t moff = (size_t)n_uniform * n_uniform * blockIdx.x, voff = (size_t)n_uniform * blockIdx.x,
@@ -662,9 +902,9 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
   // X and W are (n, nrhs) with an odd row stride ws = nrhs | 1, so that lanes reading
   // consecutive rows of one column hit distinct shared-memory banks
   const int ws = nrhs | 1;
-  double* X = sm;                          // (n, ws)
-  double* W = X + (size_t)n * ws;          // (n, ws)
-  double* Dg = W + (size_t)n * ws;         // 2 x 32 x 33
+  double* X = GW ? gwork + 34 * voff : sm;                        // (n, ws)
+  double* W = GW ? X + (size_t)n * 17 : X + (size_t)n * ws;       // (n, ws)
+  double* Dg = GW ? sm : W + (size_t)n * ws;                      // 2 x 32 x 33
   double* part = Dg + 2 * 32 * 33;         // 32 x 16
   double* colr = part + 32 * 16;           // (3, 16): bmax, b2, r2 per column
   int* perm = reinterpret_cast<int*>(colr + 3 * 16);
@@ -813,15 +1053,15 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
     for (int c = 0; c < NR; ++c) wr2[c] = 0.0;
     // each lane's (at most 20) entries of the warp's next row are loaded while the
     // current row is summed
-    constexpr int kPer = kBlockedMaxN / 32;
+    constexpr int kPer = GW ? 1 : kBlockedMaxN / 32;
     double av[kPer], an[kPer];
-    if (wid < n) {
+    if (!GW && wid < n) {
       const double* row = A + (size_t)wid * n;
 #pragma unroll
       for (int u = 0; u < kPer; ++u) av[u] = lane + 32 * u < n ? row[lane + 32 * u] : 0.0;
     }
     for (int i = wid; i < n; i += nw) {
-      if (i + nw < n) {
+      if (!GW && i + nw < n) {
         const double* nrow = A + (size_t)(i + nw) * n;
 #pragma unroll
         for (int u = 0; u < kPer; ++u) an[u] = lane + 32 * u < n ? nrow[lane + 32 * u] : 0.0;
@@ -829,13 +1069,23 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
       double hi[NR], lo[NR];
 #pragma unroll
       for (int c = 0; c < NR; ++c) hi[c] = lo[c] = 0.0;
-#pragma unroll
-      for (int u = 0; u < kPer; ++u) {
-        const int j = lane + 32 * u;
-        if (j < n) {
+      if constexpr (GW) {
+        const double* row = A + (size_t)i * n;
+        for (int j = lane; j < n; j += 32) {
+          const double a = row[j];
 #pragma unroll
           for (int c = 0; c < NR; ++c)
-            if (c < nrhs) dd_fma(hi[c], lo[c], -av[u], X[(size_t)j * ws + c]);
+            if (c < nrhs) dd_fma(hi[c], lo[c], -a, X[(size_t)j * ws + c]);
+        }
+      } else {
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+          const int j = lane + 32 * u;
+          if (j < n) {
+#pragma unroll
+            for (int c = 0; c < NR; ++c)
+              if (c < nrhs) dd_fma(hi[c], lo[c], -av[u], X[(size_t)j * ws + c]);
+          }
         }
       }
 #pragma unroll
@@ -860,8 +1110,10 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
           wr2[c] = fma(rv, rv, wr2[c]);
         }
       }
+      if constexpr (!GW) {
 #pragma unroll
-      for (int u = 0; u < kPer; ++u) av[u] = an[u];
+        for (int u = 0; u < kPer; ++u) av[u] = an[u];
+      }
     }
     if (lane == 0)
 #pragma unroll
@@ -897,6 +1149,10 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
   }
   if (tid == 0 && result != MHM_CELL_OK) status[sidx] = result;
 }
+
+// Shared memory of the GW solve: the diagonal blocks, partial sums and the row
+// permutation (X and W are in global memory).
+size_t large_solve_smem(int n) { return ((size_t)2 * 32 * 33 + 32 * 16 + 3 * 16) * 8 + (size_t)2 * n * 4; }
 
 size_t chunked_solve_smem(int n, int nrhs) {
   return ((size_t)2 * n * (nrhs | 1) + 2 * 32 * 33 + 32 * 16 + 3 * 16) * 8 + (size_t)2 * n * 4;
@@ -957,7 +1213,7 @@ extern "C" int mhm_batched_solve(int64_t count, int32_t n, int32_t nrhs, const d
         return MHM_ERR_LAUNCH;
       kernel<<<(unsigned)count, kLuThreads, sm, st>>>(n, cols, nrhs, c0, matrices, factors, pivots, row_scale,
                                                       col_scale, rhs, x, rtol, atol, max_refine, status, nullptr,
-                                                      n);
+                                                      n, nullptr);
       return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
     };
     for (int c0 = 0; c0 < nrhs; c0 += group) {
@@ -1011,7 +1267,44 @@ extern "C" int mhm_batched_solve_ragged(int64_t count, const mhm_ragged_matrix* 
   for (int c0 = 0; c0 < max_nrhs; c0 += 16) {
     batched_solve_chunked_kernel<16><<<(unsigned)count, kLuThreads, sm, st>>>(
         max_n, group, group, c0, matrices, factors, pivots, row_scale, col_scale, rhs, x, rtol, atol, max_refine,
-        status, desc, max_n);
+        status, desc, max_n, nullptr);
+    if (cudaGetLastError() != cudaSuccess) return MHM_ERR_LAUNCH;
+  }
+  return MHM_OK;
+}
+
+extern "C" int mhm_batched_factor_large(int64_t count, const mhm_ragged_matrix* desc, int32_t max_n,
+                                        const double* matrices, double* factors, int32_t* pivots,
+                                        double* row_scale, double* col_scale, int32_t* status, void* stream) {
+  if (count < 1 || !desc || max_n < 1 || max_n > kLargeMaxN || !matrices || !factors || !pivots || !row_scale ||
+      !col_scale || !status)
+    return MHM_ERR_ARGUMENT;
+  if (count > 0x7fffffff) return MHM_ERR_UNSUPPORTED;
+  large_factor_kernel<<<(unsigned)count, kLuThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+      desc, max_n, matrices, factors, pivots, row_scale, col_scale, status);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+extern "C" int mhm_batched_solve_large(int64_t count, const mhm_ragged_matrix* desc, int32_t max_n,
+                                       int32_t max_nrhs, const double* matrices, const double* factors,
+                                       const int32_t* pivots, const double* row_scale, const double* col_scale,
+                                       const double* rhs, double* x, double* work, double rtol, double atol,
+                                       int32_t max_refine, int32_t* status, void* stream) {
+  if (count < 1 || !desc || max_n < 1 || max_n > kLargeMaxN || max_nrhs < 1 || !matrices || !factors ||
+      !pivots || !row_scale || !col_scale || !rhs || !x || !work || !status || max_refine < 0 || !(rtol >= 0) ||
+      !(atol >= 0))
+    return MHM_ERR_ARGUMENT;
+  if (count > 0x7fffffff) return MHM_ERR_UNSUPPORTED;
+  const int group = max_nrhs < 16 ? max_nrhs : 16;
+  const size_t sm = large_solve_smem(max_n);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaFuncSetAttribute(batched_solve_chunked_kernel<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sm) != cudaSuccess)
+    return MHM_ERR_LAUNCH;
+  for (int c0 = 0; c0 < max_nrhs; c0 += 16) {
+    batched_solve_chunked_kernel<16, true><<<(unsigned)count, kLuThreads, sm, st>>>(
+        max_n, group, group, c0, matrices, factors, pivots, row_scale, col_scale, rhs, x, rtol, atol, max_refine,
+        status, desc, max_n, work);
     if (cudaGetLastError() != cudaSuccess) return MHM_ERR_LAUNCH;
   }
   return MHM_OK;

@@ -204,3 +204,40 @@ extern "C" int mhm_p2_assemble(int64_t elements, const double* points, const int
                                                                      load_off, stiffness, mass, load);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
+
+// The two passes of mhm_p2_assemble as separate calls, for callers that assemble the
+// node rows in several parts (local matrices too large to hold at once): the element
+// pass over every fine triangle once, then the row pass over any contiguous range of
+// nodes (pointer offsets into node_cell, node_row and inc_ptr).
+extern "C" int mhm_p2_elements(int64_t elements, const double* points, const int64_t* triangles, int32_t nquad,
+                               const double* quad_bary, const double* quad_weights, int32_t grid,
+                               const int32_t* grid_ptr, const int32_t* grid_discs, const double* centres,
+                               const double* radii2, double inside, double outside, double source,
+                               double* element_scratch, void* stream) {
+  if (elements < 1 || nquad < 1 || grid < 0 || !points || !triangles || !quad_bary || !quad_weights ||
+      (grid > 0 && (!grid_ptr || !grid_discs || !centres || !radii2)) || !element_scratch)
+    return MHM_ERR_ARGUMENT;
+  p2_element_kernel<<<blocks_for(elements), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      elements, points, triangles, nquad, quad_bary, quad_weights, grid, grid_ptr, grid_discs, centres, radii2,
+      inside, outside, source, element_scratch);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+extern "C" int mhm_p2_assemble_rows(int64_t nodes, const int32_t* node_cell, const int32_t* node_row,
+                                    const int64_t* inc_ptr, const int64_t* inc, const int32_t* elem_dofs,
+                                    const double* element_scratch, const int64_t* dense_off, const int32_t* ld_of,
+                                    const int64_t* load_off, double* stiffness, double* mass, double* load,
+                                    void* stream) {
+  if (nodes < 1 || !node_cell || !node_row || !inc_ptr || !inc || !elem_dofs || !element_scratch || !dense_off ||
+      !ld_of || !load_off || !stiffness || !mass || !load)
+    return MHM_ERR_ARGUMENT;
+  const size_t smem = (size_t)kDenseWarps * 2 * kMaxRow * sizeof(double);
+  if (cudaFuncSetAttribute(p2_dense_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return MHM_ERR_LAUNCH;
+  int64_t dblocks = (nodes + kDenseWarps - 1) / kDenseWarps;
+  if (dblocks > 148 * 16) dblocks = 148 * 16;
+  p2_dense_kernel<<<(unsigned)dblocks, kDenseWarps * 32, smem, static_cast<cudaStream_t>(stream)>>>(
+      nodes, node_cell, node_row, inc_ptr, inc, elem_dofs, element_scratch, dense_off, ld_of, load_off, stiffness,
+      mass, load);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}

@@ -313,3 +313,33 @@ def p2_trace_coupling(coarse: PolygonMesh, cell: int, fine: TriangleMesh, skelet
                 matrix[ids, side * skeleton.modes:(side + 1) * skeleton.modes] += basis.T @ (
                     w[:, None] * space.evaluate(param))
     return matrix
+
+
+def _cell_local_data(args):
+    """Worker of ``local_data``: (fine mesh, P2 nodal space, trace coupling) per cell."""
+    coarse, skeleton, cells, refinements = args
+    out = []
+    for c, r in zip(cells, refinements):
+        fine = coarse.submesh(int(c), int(r))
+        out.append((fine, p2_nodal_space(fine), p2_trace_coupling(coarse, int(c), fine, skeleton)))
+    return out
+
+
+def local_data(coarse: PolygonMesh, skeleton: EdgeSkeleton, refinements, workers: int = 1):
+    """Every cell's refined local mesh, P2 nodal space and trace coupling (host work of a
+    polygon plan, independent per cell).  With ``workers`` > 1, batches of a few hundred
+    cells and more are split over that many spawned processes (the same functions, so
+    the same results); spawned children import the calling program's main module, so a
+    script that asks for workers keeps its top-level work under
+    ``if __name__ == "__main__":``."""
+    M = len(coarse.cells)
+    rs = np.broadcast_to(np.asarray(refinements, dtype=np.int64), (M,))
+    if M < 256 or workers < 2:
+        return _cell_local_data((coarse, skeleton, range(M), rs))
+    import multiprocessing
+    from concurrent.futures import ProcessPoolExecutor
+
+    parts = [p for p in np.array_split(np.arange(M), 4 * workers) if len(p)]
+    with ProcessPoolExecutor(workers, mp_context=multiprocessing.get_context("spawn")) as pool:
+        done = pool.map(_cell_local_data, [(coarse, skeleton, p, rs[p]) for p in parts])
+        return [item for part in done for item in part]

@@ -27,11 +27,12 @@ import numpy as np
 from . import _lib
 from .errors import LinearSolveError
 from .general import GeneralSkeleton
-from .polygon import EdgeSkeleton, PolygonMesh, p2_nodal_space, p2_trace_coupling
+from .polygon import EdgeSkeleton, PolygonMesh, local_data, p2_nodal_space
 from .topology import block_offsets, skeleton_pattern_ragged, transpose_slots
 from .workloads import DiscInclusions
 
-MAX_AUGMENTED = 640  # the batched LU's blocked shared-memory panel
+MAX_AUGMENTED = 640  # the batched LU's blocked shared-memory panel (small tier)
+LARGE_MAX = 4096  # the large-order LU in HBM (large tier)
 
 
 def triangle_rule(order: int):
@@ -101,7 +102,7 @@ class PolygonP2Plan:
 
     def __init__(self, mesh: PolygonMesh, skeleton: EdgeSkeleton | None = None, refinements=2, *, order=4,
                  bin_width=32, streams=4, ragged=True, device=None, global_rtol=1e-13, inner_rtol=1e-10,
-                 max_inner=20000, max_outer=16, preconditioner="cell"):
+                 max_inner=20000, max_outer=16, preconditioner="cell", workspace_bytes=None, workers=1):
         import torch
 
         self.torch = torch
@@ -119,16 +120,22 @@ class PolygonP2Plan:
         rs = np.broadcast_to(np.asarray(refinements, dtype=np.int64), (M,))
         sk = self.skeleton
         self.T, self.N = sk.size, sk.size + M
-        fines = [mesh.submesh(c, int(rs[c])) for c in range(M)]
-        spaces = [p2_nodal_space(f) for f in fines]
+        data = local_data(mesh, sk, rs, workers=int(workers))
+        fines = [f for f, _, _ in data]
+        spaces = [sp for _, sp, _ in data]
         self.n_cells = np.array([len(nodes) for _, nodes in spaces], dtype=np.int64)
         cell_dofs = [sk.cell_dofs(c) for c in range(M)]
         self.t_cells = np.array([len(d) for d in cell_dofs], dtype=np.int64)
-        if self.n_cells.max() + 1 > MAX_AUGMENTED:
-            raise NotImplementedError(f"local P2 spaces up to {MAX_AUGMENTED - 1} unknowns on this path")
+        if self.n_cells.max() + 1 > LARGE_MAX:
+            raise NotImplementedError(f"local P2 spaces up to {LARGE_MAX - 1} unknowns on this path")
+        # Cells whose augmented systems exceed the small tier's order are condensed in
+        # chunks: their dense matrices share one workspace (two halves: the augmented
+        # matrix, assembled in place over the stiffness, and the factors, which first
+        # hold the mass matrix), so only their responses stay resident.
+        self.workspace_bytes = None if workspace_bytes is None else int(workspace_bytes)
         if self.t_cells.max() > 28:
             raise NotImplementedError("at most 28 trace DOFs per cell")
-        couplings = [p2_trace_coupling(mesh, c, fines[c], sk) for c in range(M)]
+        couplings = [cp for _, _, cp in data]
         self.nodes = int(sum(self.n_cells))
         # ---- skeleton reduction and global solve -------------------------------------
         self.cell_dofs_list = cell_dofs
@@ -166,7 +173,8 @@ class PolygonP2Plan:
         self.bin_width = bin_width
         # ---- bins by padded augmented size -------------------------------------------
         nb_c = ((self.n_cells + 1 + bin_width - 1) // bin_width) * bin_width
-        nb_c = np.minimum(nb_c, MAX_AUGMENTED)
+        small_c = self.n_cells + 1 <= MAX_AUGMENTED
+        nb_c = np.where(small_c, np.minimum(nb_c, MAX_AUGMENTED), np.minimum(nb_c, LARGE_MAX))
         order_cells = np.argsort(nb_c, kind="stable")
         self.order = order_cells
         self.bins = []
@@ -177,9 +185,12 @@ class PolygonP2Plan:
             k = len(members)
             tld = int(self.t_cells[members].max())
             w = tld + 2
+            large = bool(nb > MAX_AUGMENTED or not small_c[members].all())
             self.bins.append(dict(nb=int(nb), tld=tld, w=w, k=k, cells=members, pos=pos, dense=dense_base,
-                                  rhs=rhs_base, cpl=cpl_base, load=load_base, act=act_base, vec=vec_base))
-            dense_base += k * nb * nb
+                                  rhs=rhs_base, cpl=cpl_base, load=load_base, act=act_base, vec=vec_base,
+                                  large=large))
+            if not large:
+                dense_base += k * nb * nb
             rhs_base += k * nb * w
             cpl_base += k * nb * tld
             load_base += k * nb
@@ -197,7 +208,7 @@ class PolygonP2Plan:
                 fine = fines[c]
                 dofs, _ = spaces[c]
                 slot = b["pos"] + j
-                dense_off[slot] = b["dense"] + j * b["nb"] * b["nb"]
+                dense_off[slot] = b["dense"] + j * b["nb"] * b["nb"]  # large tier: set per chunk below
                 load_off[slot] = b["load"] + j * b["nb"]
                 ld_of[slot] = b["nb"]
                 pts.append(fine.points)
@@ -215,6 +226,58 @@ class PolygonP2Plan:
                 p_base += len(fine.points)
                 e_base += len(dofs)
         self.elements = e_base
+        node_ptr = np.r_[0, np.cumsum(self.n_cells[self.order])]
+        # ---- large tier: chunks of consecutive slots (largest first) whose dense
+        # matrices fit one half of the workspace; their dense offsets are chunk-relative
+        large_bins = [b for b in self.bins if b["large"]]
+        self.chunks = []
+        ws_half = 0
+        if large_bins:
+            need = sum(b["k"] * b["nb"] * b["nb"] for b in large_bins)
+            budget = self.workspace_bytes
+            if budget is None:
+                free, _ = torch.cuda.mem_get_info(dev)
+                budget = min(48 << 30, int(0.4 * free))
+            half = max(budget // 16, max(b["nb"] for b in large_bins) ** 2)  # doubles per half
+            cur = None
+            for b in reversed(large_bins):
+                for j in reversed(range(b["k"])):
+                    size = b["nb"] * b["nb"]
+                    if cur is None or cur["used"] + size > half:
+                        cur = dict(used=0, slots=[])
+                        self.chunks.append(cur)
+                    cur["slots"].append((b, j))
+                    cur["used"] += size
+            for ch in self.chunks:
+                ws_half = max(ws_half, ch["used"])
+                # ascending slots at ascending offsets, so that a bin's cells in a chunk
+                # sit at the bin's stride from one another
+                off, placed = 0, []
+                for b, j in reversed(ch["slots"]):
+                    dense_off[b["pos"] + j] = off
+                    placed.append((b, j, off))
+                    off += b["nb"] * b["nb"]
+                ch["slots"] = placed
+                s0 = ch["slots"][0][0]["pos"] + ch["slots"][0][1]
+                s1 = ch["slots"][-1][0]["pos"] + ch["slots"][-1][1] + 1
+                ch["s0"], ch["s1"] = s0, s1
+                ch["nodes"] = (int(node_ptr[s0]), int(node_ptr[s1]))
+                parts = []
+                for b, j, off in ch["slots"]:
+                    if parts and parts[-1]["bin"] is b:
+                        parts[-1]["j1"] = j + 1
+                    else:
+                        parts.append(dict(bin=b, j0=j, j1=j + 1, ws=off))
+                ch["parts"] = parts
+                rec = np.array([(off, b["vec"] + j * b["nb"], b["rhs"] + j * b["nb"] * b["w"], b["nb"], b["w"],
+                                 b["pos"] + j, 0) for b, j, off in reversed(ch["slots"])],
+                               dtype=[("mat_off", "<i8"), ("vec_off", "<i8"), ("rhs_off", "<i8"), ("n", "<i4"),
+                                      ("nrhs", "<i4"), ("slot", "<i4"), ("reserved", "<i4")])
+                ch["desc"] = torch.as_tensor(rec.view(np.uint8).copy()).to(dev)
+                ch["count"] = len(rec)
+                ch["max_n"] = int(rec["n"].max())
+                ch["max_w"] = int(rec["nrhs"].max())
+        self.small_nodes = int(node_ptr[sum(b["k"] for b in self.bins if not b["large"])])
         # per bin-order slot: sizes and output offsets
         o = self.order
         self.d = dict(
@@ -245,6 +308,9 @@ class PolygonP2Plan:
         self.load = torch.empty(load_base, **f64)
         self.aug = torch.empty(dense_base, **f64)
         self.factors = torch.empty(dense_base, **f64)
+        self.ws_aug = torch.empty(ws_half, **f64) if ws_half else None
+        self.ws_factors = torch.empty(ws_half, **f64) if ws_half else None
+        self.large_work = torch.empty(34 * vec_base, **f64) if ws_half else None
         self.rhs = torch.empty(rhs_base, **f64)
         self.solution = torch.empty(rhs_base, **f64)
         self.work = torch.empty(rhs_base, **f64)
@@ -258,15 +324,16 @@ class PolygonP2Plan:
         # one ragged descriptor per cell for the single-launch factor and solve, the
         # largest systems first (CTAs start in this order)
         desc = []
-        for b in reversed(self.bins):
+        for b in reversed([b for b in self.bins if not b["large"]]):
             nb, w = b["nb"], b["w"]
             for j in range(b["k"]):
                 desc.append((b["dense"] + j * nb * nb, b["vec"] + j * nb, b["rhs"] + j * nb * w, nb, w, b["pos"] + j, 0))
         rec = np.array(desc, dtype=[("mat_off", "<i8"), ("vec_off", "<i8"), ("rhs_off", "<i8"), ("n", "<i4"),
                                     ("nrhs", "<i4"), ("slot", "<i4"), ("reserved", "<i4")])
-        self.d_ragged = torch.as_tensor(rec.view(np.uint8).copy()).to(dev)
-        self.ragged_max_n = int(max(b["nb"] for b in self.bins))
-        self.ragged_max_nrhs = int(max(b["w"] for b in self.bins))
+        self.d_ragged = torch.as_tensor(rec.view(np.uint8).copy()).to(dev) if desc else None
+        self.ragged_count = len(desc)
+        self.ragged_max_n = int(max([b["nb"] for b in self.bins if not b["large"]], default=0))
+        self.ragged_max_nrhs = int(max([b["w"] for b in self.bins if not b["large"]], default=0))
         self.factor_status = torch.empty(M, dtype=torch.int32, device=dev)
         self.solve_status = torch.empty(M, dtype=torch.int32, device=dev)
         self.blocks = torch.empty(int(bofs[-1]), **f64)
@@ -342,11 +409,12 @@ class PolygonP2Plan:
         k, nb, w, tld = b["k"], b["nb"], b["w"], b["tld"]
         s = slice(b["pos"], b["pos"] + k)
         d = self.d
+        dense = None if b["large"] else slice(b["dense"], b["dense"] + k * nb * nb)  # large tier: chunk workspace
         return dict(
-            stiffness=self.stiffness[b["dense"]: b["dense"] + k * nb * nb],
-            mass=self.mass[b["dense"]: b["dense"] + k * nb * nb],
-            aug=self.aug[b["dense"]: b["dense"] + k * nb * nb],
-            factors=self.factors[b["dense"]: b["dense"] + k * nb * nb],
+            stiffness=None if dense is None else self.stiffness[dense],
+            mass=None if dense is None else self.mass[dense],
+            aug=None if dense is None else self.aug[dense],
+            factors=None if dense is None else self.factors[dense],
             load=self.load[b["load"]: b["load"] + k * nb],
             coupling=d["coupling"][b["cpl"]: b["cpl"] + k * nb * tld],
             rhs=self.rhs[b["rhs"]: b["rhs"] + k * nb * w], solution=self.solution[b["rhs"]: b["rhs"] + k * nb * w],
@@ -370,22 +438,34 @@ class PolygonP2Plan:
                 events[k].record(st)
 
         mark(0)
-        _lib.check(lib.mhm_p2_assemble(self.elements, P(d["points"]), P(d["tris"]), len(d["qw"]), P(d["qbary"]),
-                                       P(d["qw"]), fld["grid"], P(fld["ptr"]), P(fld["flat"]), P(fld["centres"]),
-                                       P(fld["r2"]), fld["inside"], fld["outside"], self.source, P(self.elem),
-                                       self.nodes, P(d["node_cell"]), P(d["node_row"]), P(d["inc_ptr"]), P(d["inc"]),
-                                       P(d["edofs"]), P(d["dense_off"]), P(d["ld_of"]), P(d["load_off"]),
-                                       P(self.stiffness), P(self.mass), P(self.load), sh), "mhm_p2_assemble")
+        if not self.chunks:
+            _lib.check(lib.mhm_p2_assemble(self.elements, P(d["points"]), P(d["tris"]), len(d["qw"]), P(d["qbary"]),
+                                           P(d["qw"]), fld["grid"], P(fld["ptr"]), P(fld["flat"]), P(fld["centres"]),
+                                           P(fld["r2"]), fld["inside"], fld["outside"], self.source, P(self.elem),
+                                           self.nodes, P(d["node_cell"]), P(d["node_row"]), P(d["inc_ptr"]),
+                                           P(d["inc"]), P(d["edofs"]), P(d["dense_off"]), P(d["ld_of"]),
+                                           P(d["load_off"]), P(self.stiffness), P(self.mass), P(self.load), sh),
+                       "mhm_p2_assemble")
+        else:
+            _lib.check(lib.mhm_p2_elements(self.elements, P(d["points"]), P(d["tris"]), len(d["qw"]), P(d["qbary"]),
+                                           P(d["qw"]), fld["grid"], P(fld["ptr"]), P(fld["flat"]), P(fld["centres"]),
+                                           P(fld["r2"]), fld["inside"], fld["outside"], self.source, P(self.elem),
+                                           sh), "mhm_p2_elements")
+            if self.small_nodes:
+                self._assemble_rows(0, self.small_nodes, self.stiffness, self.mass, sh)
+        small = [b for b in self.bins if not b["large"]]
         # the bins' chains are independent until the scatter: fork them over side
         # streams (largest bins first) so that one bin's last wave overlaps the next's.
         # With ``ragged`` the factorizations and the checked solves of all bins run as
         # one launch each (ragged descriptors) between a forked system stage and a
         # forked contribution stage.
-        def forked(stage):
+        def forked(stage, bins):
+            if not bins:
+                return
             fork = torch.cuda.Event()
             fork.record(st)
             used = []
-            for idx, b in enumerate(reversed(self.bins)):
+            for idx, b in enumerate(reversed(bins)):
                 bs = self.bin_streams[idx % len(self.bin_streams)]
                 if idx < len(self.bin_streams):
                     bs.wait_event(fork)
@@ -419,26 +499,31 @@ class PolygonP2Plan:
                                                    P(self.blocks), P(self.loads), shb), "mhm_dense_contributions")
 
         if self.ragged:
-            forked(systems)
-            cnt = len(self.order)
-            _lib.check(lib.mhm_batched_factor_ragged(cnt, P(self.d_ragged), self.ragged_max_n, P(self.aug),
-                                                     P(self.factors), P(self.pivots), P(self.row_scale),
-                                                     P(self.col_scale), P(self.factor_status), sh),
-                       "mhm_batched_factor_ragged")
-            with torch.cuda.stream(st):
-                self.solve_status.copy_(self.factor_status)
-            _lib.check(lib.mhm_batched_solve_ragged(cnt, P(self.d_ragged), self.ragged_max_n, self.ragged_max_nrhs,
-                                                    P(self.aug), P(self.factors), P(self.pivots), P(self.row_scale),
-                                                    P(self.col_scale), P(self.rhs), P(self.solution), 1e-10, 0.0, 2,
-                                                    P(self.solve_status), sh), "mhm_batched_solve_ragged")
-            forked(contributions)
+            forked(systems, small)
+            cnt = self.ragged_count
+            if cnt:
+                _lib.check(lib.mhm_batched_factor_ragged(cnt, P(self.d_ragged), self.ragged_max_n, P(self.aug),
+                                                         P(self.factors), P(self.pivots), P(self.row_scale),
+                                                         P(self.col_scale), P(self.factor_status), sh),
+                           "mhm_batched_factor_ragged")
+                with torch.cuda.stream(st):
+                    self.solve_status[:cnt].copy_(self.factor_status[:cnt])
+                _lib.check(lib.mhm_batched_solve_ragged(cnt, P(self.d_ragged), self.ragged_max_n,
+                                                        self.ragged_max_nrhs, P(self.aug), P(self.factors),
+                                                        P(self.pivots), P(self.row_scale), P(self.col_scale),
+                                                        P(self.rhs), P(self.solution), 1e-10, 0.0, 2,
+                                                        P(self.solve_status), sh), "mhm_batched_solve_ragged")
+            self._large_chunks(st, sh)
+            forked(contributions, self.bins)
         else:
             def chain(b, v, bs, shb):
                 systems(b, v, bs, shb)
                 factor_solve(b, v, bs, shb)
                 contributions(b, v, bs, shb)
 
-            forked(chain)
+            forked(chain, small)
+            self._large_chunks(st, sh)
+            forked(contributions, [b for b in self.bins if b["large"]])
         mark(1)
         p = self.pattern
         _lib.check(lib.mhm_skeleton_scatter(len(p.indices), P(d["slot_ptr"]), P(d["contrib"]), P(self.blocks),
@@ -457,6 +542,47 @@ class PolygonP2Plan:
                                                  P(v["cell_id"]), self.T, P(self.x), P(v["field_off"]),
                                                  P(self.fields), sh), "mhm_dense_reconstruct")
         mark(4)
+
+    def _assemble_rows(self, n0, n1, stiffness, mass, sh):
+        """Dense rows of the nodes n0 .. n1 - 1 (bin order) into ``stiffness`` / ``mass``
+        at the slots' dense offsets (chunk-relative for the large tier)."""
+        P, d = _lib.ptr, self.d
+        _lib.check(self.lib.mhm_p2_assemble_rows(n1 - n0, P(d["node_cell"][n0:]), P(d["node_row"][n0:]),
+                                                 P(d["inc_ptr"][n0:]), P(d["inc"]), P(d["edofs"]), P(self.elem),
+                                                 P(d["dense_off"]), P(d["ld_of"]), P(d["load_off"]), P(stiffness),
+                                                 P(mass), P(self.load), sh), "mhm_p2_assemble_rows")
+
+    def _large_chunks(self, st, sh):
+        """The large tier, one chunk after another on ``st``: node rows into the workspace,
+        the augmented systems in place over the stiffness (per bin part), then one
+        large-order factorization and one checked solve launch over the chunk's cells
+        (largest first).  The responses land in the resident right-hand-side layout."""
+        torch, P, lib, d = self.torch, _lib.ptr, self.lib, self.d
+        for ch in self.chunks:
+            n0, n1 = ch["nodes"]
+            self._assemble_rows(n0, n1, self.ws_aug, self.ws_factors, sh)
+            for part in ch["parts"]:
+                b, j0, j1, ws = part["bin"], part["j0"], part["j1"], part["ws"]
+                nb, w, tld = b["nb"], b["w"], b["tld"]
+                sl = slice(b["pos"] + j0, b["pos"] + j1)
+                _lib.check(lib.mhm_dense_systems(j1 - j0, nb, tld, nb, w, 1, P(d["n_of"][sl]), P(d["t_of"][sl]),
+                                                 P(self.ws_aug[ws:]), P(self.ws_factors[ws:]),
+                                                 P(self.load[b["load"] + j0 * nb:]),
+                                                 P(d["coupling"][b["cpl"] + j0 * nb * tld:]), P(self.ws_aug[ws:]),
+                                                 P(self.rhs[b["rhs"] + j0 * nb * w:]),
+                                                 P(self.action[b["act"] + j0 * 3 * nb:]), P(self.corrected[sl]),
+                                                 P(self.cell_status[sl]), sh), "mhm_dense_systems")
+            _lib.check(lib.mhm_batched_factor_large(ch["count"], P(ch["desc"]), ch["max_n"], P(self.ws_aug),
+                                                    P(self.ws_factors), P(self.pivots), P(self.row_scale),
+                                                    P(self.col_scale), P(self.factor_status), sh),
+                       "mhm_batched_factor_large")
+            with torch.cuda.stream(st):
+                self.solve_status[ch["s0"]: ch["s1"]].copy_(self.factor_status[ch["s0"]: ch["s1"]])
+            _lib.check(lib.mhm_batched_solve_large(ch["count"], P(ch["desc"]), ch["max_n"], ch["max_w"],
+                                                   P(self.ws_aug), P(self.ws_factors), P(self.pivots),
+                                                   P(self.row_scale), P(self.col_scale), P(self.rhs),
+                                                   P(self.solution), P(self.large_work), 1e-10, 0.0, 2,
+                                                   P(self.solve_status), sh), "mhm_batched_solve_large")
 
     def failed_cells(self) -> np.ndarray:
         """Macrocells (global ids) whose local stage failed the reference's contract
