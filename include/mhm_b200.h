@@ -71,6 +71,7 @@ extern "C" {
 #define MHM_CELL_ZERO_ROW 6        /* equilibration met a zero row                  */
 #define MHM_CELL_ZERO_COLUMN 7     /* equilibration met a zero column               */
 #define MHM_CELL_SIZE 8            /* a ragged batch's matrix exceeds the launch maximum */
+#define MHM_CELL_TIMEOUT 9         /* an on-chip copy did not complete within its wait limit */
 
 /* Global solve status (mhm_skeleton_solve `info` array, entry 0). */
 #define MHM_SOLVE_OK 0
@@ -655,9 +656,9 @@ int mhm_batched_solve_ragged(int64_t count, const mhm_ragged_matrix* desc, int32
  * diagonal window and the one row below it (the bordering row needs no more: the
  * node rows' leading blocks are positive definite); the factors, pivots (LAPACK
  * sequence), scales, rank test and status words are those of
- * mhm_batched_factor_ragged, so the solve contract is the same.  The solve keeps
- * its solution and correction blocks in `work`: 34 doubles per row of every system,
- * system k's at work + 34 vec_off.  Replaces the reference's large-block route,
+ * mhm_batched_factor_ragged, so the solve contract is the same.  The solve handles
+ * up to 32 right-hand sides per pass and keeps its solution and correction blocks in
+ * `work`: 66 doubles per row of every system, system k's at work + 66 vec_off.  Replaces the reference's large-block route,
  * `_condense_device` (execution/cuda.py:314-343: sparse cuDSS through the checked
  * factorization for augmented sizes above dense_size_limit = 512, cuda.py:352), for
  * the polygon batch's local P2 systems of order 640 to 4096.

@@ -16,6 +16,7 @@ MHM_OK, MHM_ERR_ARGUMENT, MHM_ERR_LAUNCH, MHM_ERR_UNSUPPORTED = 0, 1, 2, 3
 CELL_OK, CELL_KERNEL, CELL_SINGULAR_PIVOT, CELL_RANK_DEFICIENT = 0, 1, 2, 3
 CELL_RESIDUAL, CELL_NONFINITE, CELL_ZERO_ROW, CELL_ZERO_COLUMN = 4, 5, 6, 7
 CELL_SIZE = 8
+CELL_TIMEOUT = 9
 SOLVE_OK, SOLVE_NOT_CONVERGED, SOLVE_BREAKDOWN, SOLVE_BARRIER_TIMEOUT, SOLVE_NONFINITE = 0, 1, 2, 3, 4
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 
@@ -36,6 +37,7 @@ CELL_MESSAGES = {
     CELL_ZERO_ROW: "batched matrix contains a zero row",
     CELL_ZERO_COLUMN: "batched matrix contains a zero column",
     CELL_SIZE: "a ragged batch's matrix exceeds the launch's largest order",
+    CELL_TIMEOUT: "a local factorization's on-chip copy did not complete within its wait limit",
 }
 
 SOLVE_MESSAGES = {

@@ -557,18 +557,60 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
 constexpr int kLargeMaxN = 4096;
 constexpr int kUTile = 64;
 constexpr int kUStride = kUTile + 4;  // row stride of the staged U12 tile
+// Per-warp stages of the trailing update: 16 C rows of 64 columns, the row stride
+// chosen so that the fragment loads (two doubles a lane) hit distinct banks.
+constexpr int kCStride = kUTile + 8;
+constexpr int kStageDoubles = 16 * kCStride;
+constexpr size_t kLargeStageBytes = (size_t)(kLuThreads / 32) * 2 * kStageDoubles * sizeof(double);
+constexpr long long kSpinLimit = 1ll << 24;  // polls of an mbarrier before a copy is given up
 
-__global__ void __launch_bounds__(kLuThreads, 2) large_factor_kernel(
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+// Polls the barrier's phase with a limit; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (long long k = 0; k < kSpinLimit; ++k) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+// Bulk copy (TMA engine, no multicast) of `bytes` (a multiple of 16; both addresses
+// 16-byte aligned) from global to this CTA's shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+// Orders this thread's earlier shared-memory accesses before later async-proxy writes.
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__global__ void __launch_bounds__(kLuThreads, 1) large_factor_kernel(
     const mhm_ragged_matrix* __restrict__ desc, int max_n, const double* __restrict__ mats,
     double* __restrict__ factors, int32_t* __restrict__ piv, double* __restrict__ rs, double* __restrict__ cs,
     int32_t* __restrict__ status) {
+  extern __shared__ __align__(16) double stages[];    // per warp: two trailing-update stages
   __shared__ double Pn[(kPanel + 1) * kPanelStride];  // the window: (w + 1) x w
-  __shared__ double Us[kPanel * kUStride];             // U12 tile: 32 x 64
+  __shared__ __align__(16) double Us[kPanel * kUStride];  // U12 tile: 32 x 64
   __shared__ double red[32];
+  __shared__ __align__(8) uint64_t bars[2 * (kLuThreads / 32)];
   __shared__ int sperm[kPanel];
   __shared__ int apos[2 * kPanel + 2], asrc[2 * kPanel + 2];
   __shared__ int srcrow[kPanel + 1];
-  __shared__ int naff;
+  __shared__ int naff, abort_all;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
   const mhm_ragged_matrix d = desc[blockIdx.x];
   const int n = d.n, sidx = d.slot;
@@ -578,6 +620,16 @@ __global__ void __launch_bounds__(kLuThreads, 2) large_factor_kernel(
   }
   const size_t voff = (size_t)d.vec_off;
   double* F = factors + d.mat_off;
+  // bulk copies need 16-byte aligned rows: an even order and an aligned matrix
+  const bool bulk = (n % 2 == 0) && ((reinterpret_cast<uintptr_t>(F) & 15) == 0);
+  uint32_t qcount = 0;  // this warp's bulk-copy stages used so far (stage q & 1, phase q >> 1)
+  if (lane == 0) {
+    mbar_init(&bars[2 * wid], 1);
+    mbar_init(&bars[2 * wid + 1], 1);
+  }
+  if (tid == 0) abort_all = 0;
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  __syncthreads();
   int st = equilibrate(n, mats + d.mat_off, F, rs + voff, cs + voff);
   for (int kb = 0; kb < n && st == MHM_CELL_OK; kb += kPanel) {
     const int w = min(kPanel, n - kb), h = min(w + 1, n - kb);
@@ -707,50 +759,154 @@ __global__ void __launch_bounds__(kLuThreads, 2) large_factor_kernel(
     const int m2 = n - kb - w, base = kb + w;
     const int fr = lane >> 2, fc = lane & 3;
     const int ksteps = (w + 3) >> 2;
-    for (int tj = 0; tj < m2; tj += kUTile) {
+    for (int tj = 0; tj < m2 && !abort_all; tj += kUTile) {
       for (int idx = tid; idx < kPanel * kUTile; idx += blockDim.x) {
         const int r = idx >> 6, c = idx & (kUTile - 1);
         Us[r * kUStride + c] = (r < w && tj + c < m2) ? F[(size_t)(kb + r) * n + base + tj + c] : 0.0;
       }
+      // this thread's earlier global writes (factors, swaps, trailing stores) before the
+      // bulk copies that read them
+      if (bulk) asm volatile("fence.proxy.async;" ::: "memory");
       __syncthreads();
-      for (int rb = 8 * wid; rb < m2; rb += 8 * nw) {
-        const int i = rb + fr;
-        const size_t row = (size_t)(base + (i < m2 ? i : m2 - 1)) * n;
-        double av[kPanel / 4];
+      if (bulk) {
+        // Each warp's 16-row blocks of C arrive by bulk copies (the TMA engine, one copy
+        // per row) into the warp's two shared-memory stages: block t + 1 is in flight,
+        // and its L21 rows are loaded into registers, while block t is on the tensor
+        // cores (16 independent accumulator tiles per k-step).  Here w = 32 (a trailing
+        // matrix exists only below a full panel).
+        const int cols = min(kUTile, m2 - tj);
+        const uint32_t cbytes = (uint32_t)cols * 8u;
+        const int nblk = 16 * wid < m2 ? (m2 - 16 * wid + 16 * nw - 1) / (16 * nw) : 0;
+        double* stg = stages + (size_t)wid * 2 * kStageDoubles;
+        auto issue = [&](int t, uint32_t q) {
+          const int rb = 16 * wid + 16 * nw * t;
+          const int rows = min(16, m2 - rb);
+          uint64_t* bar = &bars[2 * wid + (q & 1u)];
+          fence_proxy_async_smem();
+          if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)rows * cbytes);
+          __syncwarp();
+          if (lane < rows)
+            bulk_copy_g2s(stg + (q & 1u) * kStageDoubles + lane * kCStride,
+                          F + (size_t)(base + rb + lane) * n + base + tj, cbytes, bar);
+        };
+        auto load_l21 = [&](int t, double (&a)[2][kPanel / 4]) {
+          const int rb = 16 * wid + 16 * nw * t;
 #pragma unroll
-        for (int s = 0; s < kPanel / 4; ++s) {
-          const int q = 4 * s + fc;
-          av[s] = q < w ? -F[row + kb + q] : 0.0;
+          for (int h = 0; h < 2; ++h) {
+            const int i = min(rb + 8 * h + fr, m2 - 1);
+#pragma unroll
+            for (int s = 0; s < kPanel / 4; ++s) a[h][s] = -F[(size_t)(base + i) * n + kb + 4 * s + fc];
+          }
+        };
+        double av[2][kPanel / 4];
+        if (nblk > 0) {
+          issue(0, qcount);
+          load_l21(0, av);
         }
-        double acc[8][2];
+        for (int t = 0; t < nblk; ++t) {
+          const uint32_t q = qcount + (uint32_t)t;
+          double an[2][kPanel / 4];
+          if (t + 1 < nblk) {
+            issue(t + 1, q + 1);
+            load_l21(t + 1, an);
+          }
+          if (!mbar_wait_bounded(&bars[2 * wid + (q & 1u)], (q >> 1) & 1u)) {
+            // a copy that never lands: wait once more (bounded) for it and the next one,
+            // then give up on this matrix without issuing more copies
+            mbar_wait_bounded(&bars[2 * wid + (q & 1u)], (q >> 1) & 1u);
+            if (t + 1 < nblk) mbar_wait_bounded(&bars[2 * wid + ((q + 1) & 1u)], ((q + 1) >> 1) & 1u);
+            if (lane == 0) abort_all = 1;
+            break;
+          }
+          const double* sC = stg + (q & 1u) * kStageDoubles;
+          const int rb = 16 * wid + 16 * nw * t;
+          double acc[2][8][2];
 #pragma unroll
-        for (int b = 0; b < 8; ++b)
+          for (int h = 0; h < 2; ++h) {
+            const int i = rb + 8 * h + fr;
 #pragma unroll
-          for (int e = 0; e < 2; ++e) {
-            const int j = tj + 8 * b + 2 * fc + e;
-            acc[b][e] = (i < m2 && j < m2) ? F[row + base + j] : 0.0;
+            for (int b = 0; b < 8; ++b) {
+              const int jj = 8 * b + 2 * fc;
+              const bool ok = i < m2 && jj < cols;  // cols is even: a pair is in or out
+              const double2 v =
+                  ok ? *reinterpret_cast<const double2*>(sC + (8 * h + fr) * kCStride + jj) : make_double2(0.0, 0.0);
+              acc[h][b][0] = v.x;
+              acc[h][b][1] = v.y;
+            }
           }
 #pragma unroll
-        for (int s = 0; s < kPanel / 4; ++s) {
-          if (s >= ksteps) break;
-          double bv[8];
+          for (int s = 0; s < kPanel / 4; ++s) {
+            double bv[8];
 #pragma unroll
-          for (int b = 0; b < 8; ++b) bv[b] = Us[(4 * s + fc) * kUStride + 8 * b + fr];
+            for (int b = 0; b < 8; ++b) bv[b] = Us[(4 * s + fc) * kUStride + 8 * b + fr];
 #pragma unroll
-          for (int b = 0; b < 8; ++b) dmma_8x8x4(acc[b][0], acc[b][1], av[s], bv[b]);
+            for (int b = 0; b < 8; ++b) {
+              dmma_8x8x4(acc[0][b][0], acc[0][b][1], av[0][s], bv[b]);
+              dmma_8x8x4(acc[1][b][0], acc[1][b][1], av[1][s], bv[b]);
+            }
+          }
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int i = rb + 8 * h + fr;
+            if (i < m2) {
+              double* crow = F + (size_t)(base + i) * n + base + tj;
+#pragma unroll
+              for (int b = 0; b < 8; ++b) {
+                const int jj = 8 * b + 2 * fc;
+                if (jj < cols) *reinterpret_cast<double2*>(crow + jj) = make_double2(acc[h][b][0], acc[h][b][1]);
+              }
+            }
+          }
+          __syncwarp();  // every lane has read the stage before block t + 2 is copied into it
+          if (t + 1 < nblk) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+              for (int s = 0; s < kPanel / 4; ++s) av[h][s] = an[h][s];
+          }
+          if (t + 1 == nblk) qcount += (uint32_t)nblk;
         }
-        if (i < m2) {
+      } else {
+        for (int rb = 8 * wid; rb < m2; rb += 8 * nw) {
+          const int i = rb + fr;
+          const size_t row = (size_t)(base + (i < m2 ? i : m2 - 1)) * n;
+          double av[kPanel / 4];
+#pragma unroll
+          for (int s = 0; s < kPanel / 4; ++s) {
+            const int q = 4 * s + fc;
+            av[s] = q < w ? -F[row + kb + q] : 0.0;
+          }
+          double acc[8][2];
 #pragma unroll
           for (int b = 0; b < 8; ++b)
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
               const int j = tj + 8 * b + 2 * fc + e;
-              if (j < m2) F[row + base + j] = acc[b][e];
+              acc[b][e] = (i < m2 && j < m2) ? F[row + base + j] : 0.0;
             }
+#pragma unroll
+          for (int s = 0; s < kPanel / 4; ++s) {
+            if (s >= ksteps) break;
+            double bv[8];
+#pragma unroll
+            for (int b = 0; b < 8; ++b) bv[b] = Us[(4 * s + fc) * kUStride + 8 * b + fr];
+#pragma unroll
+            for (int b = 0; b < 8; ++b) dmma_8x8x4(acc[b][0], acc[b][1], av[s], bv[b]);
+          }
+          if (i < m2) {
+#pragma unroll
+            for (int b = 0; b < 8; ++b)
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                const int j = tj + 8 * b + 2 * fc + e;
+                if (j < m2) F[row + base + j] = acc[b][e];
+              }
+          }
         }
       }
       __syncthreads();
     }
+    if (abort_all) st = MHM_CELL_TIMEOUT;
   }
   if (st == MHM_CELL_OK) {
     double dmin = 1e300, amax = 0.0;
@@ -771,6 +927,7 @@ __global__ void __launch_bounds__(kLuThreads, 2) large_factor_kernel(
 // loads issued together.  The threads whose rows form the next chunk also load
 // that chunk's diagonal block (into the other half of Dg) in the same pass.
 // W (n, nrhs) with row stride ws.
+template <int NCB = 2>
 __device__ void chunked_lu_solve(int n, int nrhs, int ws, const double* LU, double* W, double* Dg) {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
   const int nchunk = (n + 31) / 32;
@@ -821,9 +978,9 @@ __device__ void chunked_lu_solve(int n, int nrhs, int ws, const double* LU, doub
       for (int rb = r0 + 8 * wid; rb < r1; rb += 8 * nw) {
         const int i = rb + fr;
         const bool iv = i < r1;
-        double acc[2][2];
+        double acc[NCB][2];
 #pragma unroll
-        for (int cb = 0; cb < 2; ++cb)
+        for (int cb = 0; cb < NCB; ++cb)
 #pragma unroll
           for (int e = 0; e < 2; ++e) {
             const int col = 8 * cb + 2 * fc + e;
@@ -835,7 +992,7 @@ __device__ void chunked_lu_solve(int n, int nrhs, int ws, const double* LU, doub
           const int k = k0 + fc;
           const double av = (iv && k < h) ? -row[k] : 0.0;
 #pragma unroll
-          for (int cb = 0; cb < 2; ++cb) {
+          for (int cb = 0; cb < NCB; ++cb) {
             if (cb >= ncb) break;
             const int col = 8 * cb + fr;
             const double bv = (k < h && col < nrhs) ? W[(size_t)(i0 + k) * ws + col] : 0.0;
@@ -844,7 +1001,7 @@ __device__ void chunked_lu_solve(int n, int nrhs, int ws, const double* LU, doub
         }
         if (iv) {
 #pragma unroll
-          for (int cb = 0; cb < 2; ++cb)
+          for (int cb = 0; cb < NCB; ++cb)
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
               const int col = 8 * cb + 2 * fc + e;
@@ -863,6 +1020,94 @@ __device__ void chunked_lu_solve(int n, int nrhs, int ws, const double* LU, doub
   }
 }
 
+// W <- U^-1 L^-1 W for a block W (n, nrhs <= 32, row stride ws) in global memory
+// (large orders), left-looking by chunks of 32 rows: each chunk's rows first subtract
+// the already solved rows' contributions, LU[chunk, solved] W[solved] (one GEMM on the
+// FP64 tensor cores streaming the factor rows and the solved rows from global memory;
+// the warps split the inner dimension, each forming all 16 output tiles of 8 x 8 over
+// its share, and the 8 partials are summed in warp order through `part` (8 x 32 x 32)),
+// then the chunk is solved against its diagonal block in shared memory (a warp per
+// column, a lane per row).  Every factor entry is read once per direction.  Dg holds
+// the diagonal block and Wc the chunk's right-hand sides (32 x 33 each).
+__device__ void gw_lu_solve(int n, int nrhs, int ws, const double* LU, double* W, double* Dg, double* Wc,
+                            double* part) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  const int fr = lane >> 2, fc = lane & 3;
+  const int nchunk = (n + 31) / 32;
+  const int ncb = (nrhs + 7) >> 3;
+  for (int dir = 0; dir < 2; ++dir) {
+    const bool lower = dir == 0;
+    for (int q = 0; q < nchunk; ++q) {
+      const int i0 = lower ? q * 32 : (nchunk - 1 - q) * 32;
+      const int h = min(32, n - i0);
+      const int k0 = lower ? 0 : i0 + h, k1 = lower ? i0 : n;
+      for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
+        const int r = idx >> 5, c = idx & 31;
+        Dg[r * 33 + c] = (r < h && c < h) ? LU[(size_t)(i0 + r) * n + i0 + c] : 0.0;
+        Wc[r * 33 + c] = (r < h && c < nrhs) ? W[(size_t)(i0 + r) * ws + c] : 0.0;
+      }
+      // warp wid takes the k-steps wid, wid + nw, ... of [k0, k1) and forms the whole
+      // 32 x 32 partial product (16 tiles of 8 x 8) over them
+      double acc[4][4][2] = {};
+      const double* arow[4];
+#pragma unroll
+      for (int rb = 0; rb < 4; ++rb) {
+        const int row = min(i0 + 8 * rb + fr, i0 + h - 1);
+        arow[rb] = LU + (size_t)row * n;
+      }
+#pragma unroll 2
+      for (int k = k0 + 4 * wid; k < k1; k += 4 * nw) {
+        const int kk = k + fc;
+        const bool kv = kk < k1;
+        double a[4], b[4];
+#pragma unroll
+        for (int rb = 0; rb < 4; ++rb) a[rb] = kv ? arow[rb][kk] : 0.0;
+#pragma unroll
+        for (int cb = 0; cb < 4; ++cb) {
+          const int col = 8 * cb + fr;
+          b[cb] = (kv && cb < ncb && col < nrhs) ? W[(size_t)kk * ws + col] : 0.0;
+        }
+#pragma unroll
+        for (int rb = 0; rb < 4; ++rb)
+#pragma unroll
+          for (int cb = 0; cb < 4; ++cb) dmma_8x8x4(acc[rb][cb][0], acc[rb][cb][1], a[rb], b[cb]);
+      }
+      // the warps' partials, summed in warp order (deterministic)
+#pragma unroll
+      for (int rb = 0; rb < 4; ++rb)
+#pragma unroll
+        for (int cb = 0; cb < 4; ++cb)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) part[wid * 1024 + (8 * rb + fr) * 32 + 8 * cb + 2 * fc + e] = acc[rb][cb][e];
+      __syncthreads();
+      for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
+        double t = 0.0;
+        for (int w = 0; w < nw; ++w) t += part[w * 1024 + idx];
+        const int r = idx >> 5, c = idx & 31;
+        Wc[r * 33 + c] -= t;
+      }
+      __syncthreads();
+      for (int c = wid; c < nrhs; c += nw) {
+        double v = lane < h ? Wc[lane * 33 + c] : 0.0;
+        if (lower) {
+          for (int sidx = 0; sidx < h; ++sidx) {
+            const double xs = __shfl_sync(0xffffffffu, v, sidx);
+            if (lane > sidx && lane < h) v = fma(-Dg[lane * 33 + sidx], xs, v);
+          }
+        } else {
+          for (int sidx = h - 1; sidx >= 0; --sidx) {
+            if (lane == sidx) v = v / Dg[sidx * 33 + sidx];
+            const double xs = __shfl_sync(0xffffffffu, v, sidx);
+            if (lane < sidx) v = fma(-Dg[lane * 33 + sidx], xs, v);
+          }
+        }
+        if (lane < h) W[(size_t)(i0 + lane) * ws + c] = v;
+      }
+      __syncthreads();
+    }
+  }
+}
+
 // Solve with the right-hand sides in shared memory (n nrhs small enough): the
 // permutation is composed once, every application reads the factors in chunks, the
 // residual B - A X is one warp per row in double-double arithmetic, then the
@@ -870,9 +1115,9 @@ __device__ void chunked_lu_solve(int n, int nrhs, int ws, const double* LU, doub
 // With desc (ragged batches), CTA m solves columns c0 .. c0 + NR - 1 of the system
 // desc[m] describes (order n, nrhs columns, offsets, status word); a system with no
 // column in that range is skipped.  With GW (large orders), the solution and the
-// correction blocks X and W live in gwork (2 x 17 doubles per row of the system, at
-// 34 vec_off) instead of shared memory, and the accurate residual reads its rows
-// without the register prefetch.
+// correction blocks X and W live in gwork (2 x (KC + 1) doubles per row of the
+// system, at 2 (KC + 1) vec_off) instead of shared memory, and the accurate residual
+// reads its rows without the register prefetch.
 template <int NR, bool GW = false>
 __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
     int n_uniform, int nrhs_uniform, int ldr_uniform, int c0, const double* __restrict__ mats,
@@ -880,6 +1125,8 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
     const double* __restrict__ cs, const double* __restrict__ rhs, double* __restrict__ x, double rtol, double atol,
     int max_refine, int32_t* __restrict__ status, const mhm_ragged_matrix* __restrict__ desc, int max_n,
     double* __restrict__ gwork) {
+  constexpr int KC = NR > 16 ? NR : 16;  // column capacity of the partial sums
+  constexpr int NCB = KC / 8;            // 8-column blocks of the tensor-core steps
   extern __shared__ __align__(16) double sm[];
   int n = n_uniform, nrhs = nrhs_uniform, ldr = ldr_uniform, sidx = blockIdx.x;
   size_t moff = (size_t)n_uniform * n_uniform * blockIdx.x, voff = (size_t)n_uniform * blockIdx.x,
@@ -902,12 +1149,13 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
   // X and W are (n, nrhs) with an odd row stride ws = nrhs | 1, so that lanes reading
   // consecutive rows of one column hit distinct shared-memory banks
   const int ws = nrhs | 1;
-  double* X = GW ? gwork + 34 * voff : sm;                        // (n, ws)
-  double* W = GW ? X + (size_t)n * 17 : X + (size_t)n * ws;       // (n, ws)
+  double* X = GW ? gwork + 2 * (KC + 1) * voff : sm;              // (n, ws)
+  double* W = GW ? X + (size_t)n * (KC + 1) : X + (size_t)n * ws; // (n, ws)
   double* Dg = GW ? sm : W + (size_t)n * ws;                      // 2 x 32 x 33
-  double* part = Dg + 2 * 32 * 33;         // 32 x 16
-  double* colr = part + 32 * 16;           // (3, 16): bmax, b2, r2 per column
-  int* perm = reinterpret_cast<int*>(colr + 3 * 16);
+  double* part = Dg + 2 * 32 * 33;         // 32 x KC
+  double* colr = part + 32 * KC;           // (3, KC): bmax, b2, r2 per column
+  // GW: the triangular solves' partial products (8 x 32 x 32) follow colr
+  int* perm = reinterpret_cast<int*>(colr + 3 * KC + (GW ? 8 * 1024 : 0));
   int* iperm = perm + n;
   __shared__ int flag;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
@@ -929,7 +1177,7 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
     for (int i = 0; i < n; ++i) iperm[perm[i]] = i;
     flag = 0;
   }
-  if (tid < 16) colr[tid] = colr[16 + tid] = 0.0;
+  if (tid < KC) colr[tid] = colr[KC + tid] = 0.0;
   __syncthreads();
   int nonfinite = 0;
   // (row, column) loops run over n x NR slots (NR a power of two: shift and mask, no
@@ -958,7 +1206,7 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
       b2 += bv * bv;
     }
     b2 = warp_sum(b2);
-    if (lane == 0) { colr[c] = scale; colr[16 + c] = b2; }
+    if (lane == 0) { colr[c] = scale; colr[KC + c] = b2; }
   }
   // X = csc .* U^-1 L^-1 P (rsc .* B)
   for (int idx = tid; idx < n * NR; idx += blockDim.x) {
@@ -968,7 +1216,10 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
     W[i * ws + c] = B[(size_t)src * ldr + c] * rsc[src];
   }
   __syncthreads();
-  chunked_lu_solve(n, nrhs, ws, LU, W, Dg);
+  if constexpr (GW)
+    gw_lu_solve(n, nrhs, ws, LU, W, Dg, Dg + 32 * 33, colr + 3 * KC);
+  else
+    chunked_lu_solve<NCB>(n, nrhs, ws, LU, W, Dg);
   for (int idx = tid; idx < n * NR; idx += blockDim.x) {
     const int i = idx / NR, c = idx % NR;
     if (c < nrhs) X[i * ws + c] = W[i * ws + c] * csc[i];
@@ -989,18 +1240,18 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
     {
       const int fr = lane >> 2, fc = lane & 3;
       const int ncb = (nrhs + 7) >> 3;
-      double s2[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+      double s2[NCB][2] = {};
       for (int rb = 8 * wid; rb < n; rb += 8 * nw) {
         const int i = rb + fr;
         const bool iv = i < n;
         const double* arow = A + (size_t)(iv ? i : rb) * n;
-        double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+        double acc[NCB][2] = {};
 #pragma unroll 8
         for (int k0 = 0; k0 < n; k0 += 4) {
           const int kk = k0 + fc;
           const double a = (iv && kk < n) ? arow[kk] : 0.0;
 #pragma unroll
-          for (int cb = 0; cb < 2; ++cb) {
+          for (int cb = 0; cb < NCB; ++cb) {
             if (cb >= ncb) break;
             const int col = 8 * cb + fr;
             const double bx = (kk < n && col < nrhs) ? X[(size_t)kk * ws + col] : 0.0;
@@ -1009,7 +1260,7 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
         }
         if (iv) {
 #pragma unroll
-          for (int cb = 0; cb < 2; ++cb)
+          for (int cb = 0; cb < NCB; ++cb)
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
               const int col = 8 * cb + 2 * fc + e;
@@ -1021,7 +1272,7 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
         }
       }
 #pragma unroll
-      for (int cb = 0; cb < 2; ++cb)
+      for (int cb = 0; cb < NCB; ++cb)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           double v = s2[cb][e];
@@ -1029,15 +1280,15 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
           v += __shfl_xor_sync(0xffffffffu, v, 8);
           v += __shfl_xor_sync(0xffffffffu, v, 16);
           const int col = 8 * cb + 2 * fc + e;
-          if (fr == 0 && cb < ncb && col < nrhs) part[wid * 16 + col] = v;
+          if (fr == 0 && cb < ncb && col < nrhs) part[wid * KC + col] = v;
         }
       __syncthreads();
       if (tid == 0) {
         int ok = 1;
         for (int c = 0; c < nrhs; ++c) {
           double t = 0.0;
-          for (int q = 0; q < nw; ++q) t += part[q * 16 + c];
-          const double limit = fmax(atol / colr[c], rtol * sqrt(colr[16 + c]));
+          for (int q = 0; q < nw; ++q) t += part[q * KC + c];
+          const double limit = fmax(atol / colr[c], rtol * sqrt(colr[KC + c]));
           if (!(sqrt(t) <= limit)) ok = 0;
         }
         flag = ok;
@@ -1117,26 +1368,29 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
     }
     if (lane == 0)
 #pragma unroll
-      for (int c = 0; c < NR; ++c) part[wid * 16 + c] = wr2[c];
+      for (int c = 0; c < NR; ++c) part[wid * KC + c] = wr2[c];
     __syncthreads();
     if (tid == 0) {
       for (int c = 0; c < nrhs; ++c) {
         double t = 0.0;
-        for (int q = 0; q < nw; ++q) t += part[q * 16 + c];
-        colr[32 + c] = t;
+        for (int q = 0; q < nw; ++q) t += part[q * KC + c];
+        colr[2 * KC + c] = t;
       }
       int ok = 1;
       for (int c = 0; c < nrhs; ++c) {
         const double scale = colr[c];
-        const double limit = fmax(atol / scale, rtol * sqrt(colr[16 + c]));
-        if (!(sqrt(colr[32 + c]) <= limit)) ok = 0;
+        const double limit = fmax(atol / scale, rtol * sqrt(colr[KC + c]));
+        if (!(sqrt(colr[2 * KC + c]) <= limit)) ok = 0;
       }
       flag = ok;
     }
     __syncthreads();
     if (flag) { result = MHM_CELL_OK; break; }
     if (pass == max_refine) break;
-    chunked_lu_solve(n, nrhs, ws, LU, W, Dg);
+    if constexpr (GW)
+    gw_lu_solve(n, nrhs, ws, LU, W, Dg, Dg + 32 * 33, colr + 3 * KC);
+  else
+    chunked_lu_solve<NCB>(n, nrhs, ws, LU, W, Dg);
     for (int idx = tid; idx < n * NR; idx += blockDim.x) {
       const int i = idx / NR, c = idx % NR;
       if (c < nrhs) X[i * ws + c] += W[i * ws + c] * csc[i];
@@ -1152,7 +1406,7 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
 
 // Shared memory of the GW solve: the diagonal blocks, partial sums and the row
 // permutation (X and W are in global memory).
-size_t large_solve_smem(int n) { return ((size_t)2 * 32 * 33 + 32 * 16 + 3 * 16) * 8 + (size_t)2 * n * 4; }
+size_t large_solve_smem(int n) { return ((size_t)2 * 32 * 33 + 32 * 32 + 3 * 32 + 8 * 1024) * 8 + (size_t)2 * n * 4; }
 
 size_t chunked_solve_smem(int n, int nrhs) {
   return ((size_t)2 * n * (nrhs | 1) + 2 * 32 * 33 + 32 * 16 + 3 * 16) * 8 + (size_t)2 * n * 4;
@@ -1280,7 +1534,10 @@ extern "C" int mhm_batched_factor_large(int64_t count, const mhm_ragged_matrix* 
       !col_scale || !status)
     return MHM_ERR_ARGUMENT;
   if (count > 0x7fffffff) return MHM_ERR_UNSUPPORTED;
-  large_factor_kernel<<<(unsigned)count, kLuThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+  if (cudaFuncSetAttribute(large_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kLargeStageBytes) != cudaSuccess)
+    return MHM_ERR_LAUNCH;
+  large_factor_kernel<<<(unsigned)count, kLuThreads, kLargeStageBytes, static_cast<cudaStream_t>(stream)>>>(
       desc, max_n, matrices, factors, pivots, row_scale, col_scale, status);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
@@ -1295,14 +1552,14 @@ extern "C" int mhm_batched_solve_large(int64_t count, const mhm_ragged_matrix* d
       !(atol >= 0))
     return MHM_ERR_ARGUMENT;
   if (count > 0x7fffffff) return MHM_ERR_UNSUPPORTED;
-  const int group = max_nrhs < 16 ? max_nrhs : 16;
+  const int group = max_nrhs < 32 ? max_nrhs : 32;
   const size_t sm = large_solve_smem(max_n);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (cudaFuncSetAttribute(batched_solve_chunked_kernel<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(batched_solve_chunked_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)sm) != cudaSuccess)
     return MHM_ERR_LAUNCH;
-  for (int c0 = 0; c0 < max_nrhs; c0 += 16) {
-    batched_solve_chunked_kernel<16, true><<<(unsigned)count, kLuThreads, sm, st>>>(
+  for (int c0 = 0; c0 < max_nrhs; c0 += 32) {
+    batched_solve_chunked_kernel<32, true><<<(unsigned)count, kLuThreads, sm, st>>>(
         max_n, group, group, c0, matrices, factors, pivots, row_scale, col_scale, rhs, x, rtol, atol, max_refine,
         status, desc, max_n, work);
     if (cudaGetLastError() != cudaSuccess) return MHM_ERR_LAUNCH;

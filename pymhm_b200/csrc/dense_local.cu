@@ -74,13 +74,16 @@ __global__ void tet_kappa_kernel(int64_t cells, const double* __restrict__ point
 // n + 1 are an identity block with zero right-hand sides (solution zero there).
 // ---------------------------------------------------------------------------------
 constexpr int kDThreads = 256;
+constexpr int kTileStride = 33;  // odd: a thread's row of a staged tile spans distinct banks
+constexpr size_t kSystemSmem = (size_t)kDThreads * kTileStride * sizeof(double);  // a 32 x 33 tile per warp
 
-__global__ void __launch_bounds__(kDThreads) dense_system_kernel(
+__global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
     int lds, int tld, int nb, int w, int normalize, const int32_t* __restrict__ n_of,
     const int32_t* __restrict__ t_of,
     const double* __restrict__ stiffness, const double* __restrict__ mass, const double* __restrict__ load,
     const double* __restrict__ coupling, double* __restrict__ aug, double* __restrict__ rhs,
     double* __restrict__ action, uint8_t* __restrict__ corrected, int32_t* __restrict__ status) {
+  extern __shared__ __align__(16) double tiles[];
   __shared__ double red[32];
   __shared__ int nonzero;
   const int64_t cell = blockIdx.x;
@@ -97,28 +100,59 @@ __global__ void __launch_bounds__(kDThreads) dense_system_kernel(
   // that the kernel check reads, and the constraint C = M 1
   double amax = 0.0, fro = 0.0, r2 = 0.0, l2 = 0.0, cmax = 0.0, csum = 0.0;
   __syncthreads();
-  for (int i = tid; i < n; i += blockDim.x) {
-    double hi = 0.0, lo = 0.0, plain = 0.0, chi = 0.0, clo = 0.0, cplain = 0.0;
-    for (int j = 0; j < n; ++j) {
-      const double a = A[(int64_t)i * lds + j];
-      amax = fmax(amax, fabs(a));
-      fro = fma(a, a, fro);
-      dd_add(hi, lo, a);
-      plain += a;
-      const double b = A[(int64_t)j * lds + i];
-      dd_add(chi, clo, b);
-      cplain += b;
+  // Thread t owns rows t, t + blockDim, ... and walks each row's columns in ascending
+  // order (every sum below keeps that order).  Each warp works alone on 32 of those
+  // rows at a time (lane l on row r0 + l): per chunk of 32 columns its lanes load the
+  // rows' entries into the warp's shared-memory tile (a row per step, coalesced) and
+  // the column entries A[j][r0 + l] into registers, all 64 loads in flight at once;
+  // then each lane sums its row from the tile and its column from the registers.
+  double* tile = tiles + (size_t)(tid >> 5) * 32 * kTileStride;  // this warp's (32, 33)
+  const int lane0 = tid & 31;
+  for (int r0 = tid - lane0; r0 < n; r0 += blockDim.x) {
+    const int i = r0 + lane0;
+    double hi = 0.0, lo = 0.0, plain = 0.0, chi = 0.0, clo = 0.0, cplain = 0.0, c = 0.0;
+    for (int c0 = 0; c0 < n; c0 += 32) {
+      const int jn = min(32, n - c0);
+      double colv[32];
+#pragma unroll
+      for (int q = 0; q < 32; ++q) {
+        tile[q * kTileStride + lane0] = (r0 + q < n && c0 + lane0 < n) ? A[(int64_t)(r0 + q) * lds + c0 + lane0] : 0.0;
+        colv[q] = (q < jn && i < n) ? A[(int64_t)(c0 + q) * lds + i] : 0.0;
+      }
+      __syncwarp();
+      if (i < n) {
+#pragma unroll
+        for (int q = 0; q < 32; ++q) {
+          if (q < jn) {
+            const double a = tile[lane0 * kTileStride + q];
+            amax = fmax(amax, fabs(a));
+            fro = fma(a, a, fro);
+            dd_add(hi, lo, a);
+            plain += a;
+            dd_add(chi, clo, colv[q]);
+            cplain += colv[q];
+          }
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < 32; ++q)
+        tile[q * kTileStride + lane0] = (r0 + q < n && c0 + lane0 < n) ? Mm[(int64_t)(r0 + q) * lds + c0 + lane0] : 0.0;
+      __syncwarp();
+      if (i < n)
+        for (int q = 0; q < jn; ++q) c += tile[lane0 * kTileStride + q];
+      __syncwarp();
     }
-    const double ai = hi + lo, ti = chi + clo;
-    act[i] = ai;
-    act[nb + i] = ti;
-    if (ai != 0.0 || ti != 0.0) nonzero = 1;
-    r2 = fma(plain, plain, r2);
-    l2 = fma(cplain, cplain, l2);
-    double c = 0.0;
-    for (int j = 0; j < n; ++j) c += Mm[(int64_t)i * lds + j];
-    act[2 * nb + i] = c;
-    csum += c;
+    if (i < n) {
+      const double ai = hi + lo, ti = chi + clo;
+      act[i] = ai;
+      act[nb + i] = ti;
+      if (ai != 0.0 || ti != 0.0) nonzero = 1;
+      r2 = fma(plain, plain, r2);
+      l2 = fma(cplain, cplain, l2);
+      act[2 * nb + i] = c;
+      csum += c;
+    }
   }
   amax = block_max(amax, red);
   fro = block_sum(fro, red);
@@ -315,7 +349,10 @@ extern "C" int mhm_dense_systems(int64_t count, int32_t lds, int32_t tld, int32_
   if (count < 1 || count > INT32_MAX || lds < 1 || tld < 1 || nb < 2 || nb > lds + 64 || w < 3 || !n_of ||
       !t_of || !stiffness || !mass || !load || !coupling || !aug || !rhs || !action || !corrected || !status)
     return MHM_ERR_ARGUMENT;
-  dense_system_kernel<<<(unsigned)count, kDThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+  if (cudaFuncSetAttribute(dense_system_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSystemSmem) !=
+      cudaSuccess)
+    return MHM_ERR_LAUNCH;
+  dense_system_kernel<<<(unsigned)count, kDThreads, kSystemSmem, static_cast<cudaStream_t>(stream)>>>(
       lds, tld, nb, w, normalize, n_of, t_of, stiffness, mass, load, coupling, aug, rhs, action, corrected,
       status);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;

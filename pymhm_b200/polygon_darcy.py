@@ -310,7 +310,7 @@ class PolygonP2Plan:
         self.factors = torch.empty(dense_base, **f64)
         self.ws_aug = torch.empty(ws_half, **f64) if ws_half else None
         self.ws_factors = torch.empty(ws_half, **f64) if ws_half else None
-        self.large_work = torch.empty(34 * vec_base, **f64) if ws_half else None
+        self.large_work = torch.empty(66 * vec_base, **f64) if ws_half else None
         self.rhs = torch.empty(rhs_base, **f64)
         self.solution = torch.empty(rhs_base, **f64)
         self.work = torch.empty(rhs_base, **f64)
@@ -425,9 +425,11 @@ class PolygonP2Plan:
             field_off=d["field_off"][s], corrected=self.corrected[s], cell_status=self.cell_status[s],
             factor_status=self.factor_status[s], solve_status=self.solve_status[s])
 
-    def launch(self, stream=None, *, events=None):
+    def launch(self, stream=None, *, events=None, factor_events=None):
         """Enqueue one complete solve on ``stream`` (no host synchronisation).  ``events``:
-        five CUDA events around the local stage, reduction, global solve and reconstruction."""
+        five CUDA events around the local stage, reduction, global solve and reconstruction;
+        ``factor_events``: a list that receives a (start, end) pair of CUDA events around
+        each large-tier factorization launch."""
         torch = self.torch
         P, lib, sh = _lib.ptr, self.lib, _lib.stream_handle(stream)
         st = torch.cuda.current_stream() if stream is None else stream
@@ -513,7 +515,7 @@ class PolygonP2Plan:
                                                         P(self.pivots), P(self.row_scale), P(self.col_scale),
                                                         P(self.rhs), P(self.solution), 1e-10, 0.0, 2,
                                                         P(self.solve_status), sh), "mhm_batched_solve_ragged")
-            self._large_chunks(st, sh)
+            self._large_chunks(st, sh, factor_events)
             forked(contributions, self.bins)
         else:
             def chain(b, v, bs, shb):
@@ -522,7 +524,7 @@ class PolygonP2Plan:
                 contributions(b, v, bs, shb)
 
             forked(chain, small)
-            self._large_chunks(st, sh)
+            self._large_chunks(st, sh, factor_events)
             forked(contributions, [b for b in self.bins if b["large"]])
         mark(1)
         p = self.pattern
@@ -552,30 +554,50 @@ class PolygonP2Plan:
                                                  P(d["dense_off"]), P(d["ld_of"]), P(d["load_off"]), P(stiffness),
                                                  P(mass), P(self.load), sh), "mhm_p2_assemble_rows")
 
-    def _large_chunks(self, st, sh):
+    def _large_chunks(self, st, sh, factor_events=None):
         """The large tier, one chunk after another on ``st``: node rows into the workspace,
         the augmented systems in place over the stiffness (per bin part), then one
         large-order factorization and one checked solve launch over the chunk's cells
         (largest first).  The responses land in the resident right-hand-side layout."""
         torch, P, lib, d = self.torch, _lib.ptr, self.lib, self.d
+        if not hasattr(self, "chunk_streams"):
+            self.chunk_streams = [torch.cuda.Stream(device=self.device) for _ in range(8)]
         for ch in self.chunks:
             n0, n1 = ch["nodes"]
             self._assemble_rows(n0, n1, self.ws_aug, self.ws_factors, sh)
-            for part in ch["parts"]:
+            # a bin part is a few dozen cells: the parts' system launches run side by
+            # side on the chunk streams, so that together they fill the SMs
+            fork = torch.cuda.Event()
+            fork.record(st)
+            used = self.chunk_streams[: len(ch["parts"])]
+            for cs in used:
+                cs.wait_event(fork)
+            for idx, part in enumerate(ch["parts"]):
                 b, j0, j1, ws = part["bin"], part["j0"], part["j1"], part["ws"]
                 nb, w, tld = b["nb"], b["w"], b["tld"]
                 sl = slice(b["pos"] + j0, b["pos"] + j1)
+                csh = _lib.stream_handle(used[idx % len(used)])
                 _lib.check(lib.mhm_dense_systems(j1 - j0, nb, tld, nb, w, 1, P(d["n_of"][sl]), P(d["t_of"][sl]),
                                                  P(self.ws_aug[ws:]), P(self.ws_factors[ws:]),
                                                  P(self.load[b["load"] + j0 * nb:]),
                                                  P(d["coupling"][b["cpl"] + j0 * nb * tld:]), P(self.ws_aug[ws:]),
                                                  P(self.rhs[b["rhs"] + j0 * nb * w:]),
                                                  P(self.action[b["act"] + j0 * 3 * nb:]), P(self.corrected[sl]),
-                                                 P(self.cell_status[sl]), sh), "mhm_dense_systems")
+                                                 P(self.cell_status[sl]), csh), "mhm_dense_systems")
+            for cs in used:
+                join = torch.cuda.Event()
+                join.record(cs)
+                st.wait_event(join)
+            if factor_events is not None:
+                factor_events.append(torch.cuda.Event(enable_timing=True))
+                factor_events[-1].record(st)
             _lib.check(lib.mhm_batched_factor_large(ch["count"], P(ch["desc"]), ch["max_n"], P(self.ws_aug),
                                                     P(self.ws_factors), P(self.pivots), P(self.row_scale),
                                                     P(self.col_scale), P(self.factor_status), sh),
                        "mhm_batched_factor_large")
+            if factor_events is not None:
+                factor_events.append(torch.cuda.Event(enable_timing=True))
+                factor_events[-1].record(st)
             with torch.cuda.stream(st):
                 self.solve_status[ch["s0"]: ch["s1"]].copy_(self.factor_status[ch["s0"]: ch["s1"]])
             _lib.check(lib.mhm_batched_solve_large(ch["count"], P(ch["desc"]), ch["max_n"], ch["max_w"],

@@ -60,7 +60,7 @@ def run_large(mats, rhss, max_n=None):
     nv = int(voff[-1])
     piv = torch.empty(nv, dtype=torch.int32, device=dev)
     rs, cs = torch.empty(nv, dtype=torch.float64, device=dev), torch.empty(nv, dtype=torch.float64, device=dev)
-    work = torch.empty(34 * nv, dtype=torch.float64, device=dev)
+    work = torch.empty(66 * nv, dtype=torch.float64, device=dev)
     status = torch.full((len(mats),), -1, dtype=torch.int32, device=dev)
     mx = max(m.shape[0] for m in mats) if max_n is None else max_n
     mw = max(r.shape[1] for r in rhss)
