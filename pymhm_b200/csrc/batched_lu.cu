@@ -622,7 +622,8 @@ __global__ void __launch_bounds__(kLuThreads, 1) large_factor_kernel(
   double* F = factors + d.mat_off;
   // bulk copies need 16-byte aligned rows: an even order and an aligned matrix
   const bool bulk = (n % 2 == 0) && ((reinterpret_cast<uintptr_t>(F) & 15) == 0);
-  uint32_t qcount = 0;  // this warp's bulk-copy stages used so far (stage q & 1, phase q >> 1)
+  uint32_t qcount = 0;     // this warp's bulk-copy stages used so far (stage q & 1, phase q >> 1)
+  bool prefetched = false;  // the next tile's first block is already in flight
   if (lane == 0) {
     mbar_init(&bars[2 * wid], 1);
     mbar_init(&bars[2 * wid + 1], 1);
@@ -774,21 +775,26 @@ __global__ void __launch_bounds__(kLuThreads, 1) large_factor_kernel(
         // and its L21 rows are loaded into registers, while block t is on the tensor
         // cores (16 independent accumulator tiles per k-step).  Here w = 32 (a trailing
         // matrix exists only below a full panel).
+        // The first block of the next tile is issued during this tile's last block, so
+        // the pipeline does not drain at the tile boundary (C blocks do not depend on
+        // the U12 tile).
         const int cols = min(kUTile, m2 - tj);
         const uint32_t cbytes = (uint32_t)cols * 8u;
         const int nblk = 16 * wid < m2 ? (m2 - 16 * wid + 16 * nw - 1) / (16 * nw) : 0;
         double* stg = stages + (size_t)wid * 2 * kStageDoubles;
-        auto issue = [&](int t, uint32_t q) {
+        auto issue_at = [&](int t, uint32_t q, int tjx) {
           const int rb = 16 * wid + 16 * nw * t;
           const int rows = min(16, m2 - rb);
+          const uint32_t cb = (uint32_t)min(kUTile, m2 - tjx) * 8u;
           uint64_t* bar = &bars[2 * wid + (q & 1u)];
           fence_proxy_async_smem();
-          if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)rows * cbytes);
+          if (lane == 0) mbar_arrive_expect_tx(bar, (uint32_t)rows * cb);
           __syncwarp();
           if (lane < rows)
             bulk_copy_g2s(stg + (q & 1u) * kStageDoubles + lane * kCStride,
-                          F + (size_t)(base + rb + lane) * n + base + tj, cbytes, bar);
+                          F + (size_t)(base + rb + lane) * n + base + tjx, cb, bar);
         };
+        auto issue = [&](int t, uint32_t q) { issue_at(t, q, tj); };
         auto load_l21 = [&](int t, double (&a)[2][kPanel / 4]) {
           const int rb = 16 * wid + 16 * nw * t;
 #pragma unroll
@@ -800,21 +806,26 @@ __global__ void __launch_bounds__(kLuThreads, 1) large_factor_kernel(
         };
         double av[2][kPanel / 4];
         if (nblk > 0) {
-          issue(0, qcount);
+          if (!prefetched) issue(0, qcount);
           load_l21(0, av);
         }
+        prefetched = false;
         for (int t = 0; t < nblk; ++t) {
           const uint32_t q = qcount + (uint32_t)t;
           double an[2][kPanel / 4];
           if (t + 1 < nblk) {
             issue(t + 1, q + 1);
             load_l21(t + 1, an);
+          } else if (tj + kUTile < m2) {
+            issue_at(0, q + 1, tj + kUTile);
+            prefetched = true;
           }
           if (!mbar_wait_bounded(&bars[2 * wid + (q & 1u)], (q >> 1) & 1u)) {
             // a copy that never lands: wait once more (bounded) for it and the next one,
             // then give up on this matrix without issuing more copies
             mbar_wait_bounded(&bars[2 * wid + (q & 1u)], (q >> 1) & 1u);
-            if (t + 1 < nblk) mbar_wait_bounded(&bars[2 * wid + ((q + 1) & 1u)], ((q + 1) >> 1) & 1u);
+            if (t + 1 < nblk || prefetched)
+              mbar_wait_bounded(&bars[2 * wid + ((q + 1) & 1u)], ((q + 1) >> 1) & 1u);
             if (lane == 0) abort_all = 1;
             break;
           }
