@@ -1066,7 +1066,7 @@ __device__ void gw_lu_solve(int n, int nrhs, int ws, const double* LU, double* W
         const int row = min(i0 + 8 * rb + fr, i0 + h - 1);
         arow[rb] = LU + (size_t)row * n;
       }
-#pragma unroll 2
+#pragma unroll 4
       for (int k = k0 + 4 * wid; k < k1; k += 4 * nw) {
         const int kk = k + fc;
         const bool kv = kk < k1;
