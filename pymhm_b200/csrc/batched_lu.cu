@@ -598,6 +598,42 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32
 // Orders this thread's earlier shared-memory accesses before later async-proxy writes.
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// (c) U12 = L11^-1 A12, a thread per column, and (d) L21 = A21 U11^-1 for the rows
+// below the window, a thread per row (kept out of line: their 32-entry rows need
+// registers that the trailing update uses for its accumulators).
+__device__ __noinline__ void panel_solves(double* F, int n, int kb, int w, int h, const double* Pn) {
+  const int tid = threadIdx.x;
+    // (c) U12 = L11^-1 A12
+    for (int j = kb + w + tid; j < n; j += blockDim.x) {
+      double x[kPanel];
+#pragma unroll
+      for (int r = 0; r < kPanel; ++r) x[r] = r < w ? F[(size_t)(kb + r) * n + j] : 0.0;
+#pragma unroll
+      for (int r = 1; r < kPanel; ++r)
+#pragma unroll
+        for (int q = 0; q < r; ++q) x[r] = fma(-Pn[r * kPanelStride + q], x[q], x[r]);
+#pragma unroll
+      for (int r = 0; r < kPanel; ++r)
+        if (r < w) F[(size_t)(kb + r) * n + j] = x[r];
+    }
+    // (d) L21 = A21 U11^-1 for the rows below the window
+    for (int r = kb + h + tid; r < n; r += blockDim.x) {
+      double x[kPanel];
+#pragma unroll
+      for (int j = 0; j < kPanel; ++j) x[j] = j < w ? F[(size_t)r * n + kb + j] : 0.0;
+#pragma unroll
+      for (int j = 0; j < kPanel; ++j) {
+        double v = x[j];
+#pragma unroll
+        for (int q = 0; q < j; ++q) v = fma(-x[q], Pn[q * kPanelStride + j], v);
+        x[j] = j < w ? v * (1.0 / Pn[j * kPanelStride + j]) : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < kPanel; ++j)
+        if (j < w) F[(size_t)r * n + kb + j] = x[j];
+    }
+}
+
 __global__ void __launch_bounds__(kLuThreads, 1) large_factor_kernel(
     const mhm_ragged_matrix* __restrict__ desc, int max_n, const double* __restrict__ mats,
     double* __restrict__ factors, int32_t* __restrict__ piv, double* __restrict__ rs, double* __restrict__ cs,
@@ -725,35 +761,7 @@ __global__ void __launch_bounds__(kLuThreads, 1) large_factor_kernel(
           if (k < moved) F[(size_t)(kb + apos[k]) * n + col] = v[k];
       }
     __syncthreads();
-    // (c) U12 = L11^-1 A12
-    for (int j = kb + w + tid; j < n; j += blockDim.x) {
-      double x[kPanel];
-#pragma unroll
-      for (int r = 0; r < kPanel; ++r) x[r] = r < w ? F[(size_t)(kb + r) * n + j] : 0.0;
-#pragma unroll
-      for (int r = 1; r < kPanel; ++r)
-#pragma unroll
-        for (int q = 0; q < r; ++q) x[r] = fma(-Pn[r * kPanelStride + q], x[q], x[r]);
-#pragma unroll
-      for (int r = 0; r < kPanel; ++r)
-        if (r < w) F[(size_t)(kb + r) * n + j] = x[r];
-    }
-    // (d) L21 = A21 U11^-1 for the rows below the window
-    for (int r = kb + h + tid; r < n; r += blockDim.x) {
-      double x[kPanel];
-#pragma unroll
-      for (int j = 0; j < kPanel; ++j) x[j] = j < w ? F[(size_t)r * n + kb + j] : 0.0;
-#pragma unroll
-      for (int j = 0; j < kPanel; ++j) {
-        double v = x[j];
-#pragma unroll
-        for (int q = 0; q < j; ++q) v = fma(-x[q], Pn[q * kPanelStride + j], v);
-        x[j] = j < w ? v * (1.0 / Pn[j * kPanelStride + j]) : 0.0;
-      }
-#pragma unroll
-      for (int j = 0; j < kPanel; ++j)
-        if (j < w) F[(size_t)r * n + kb + j] = x[j];
-    }
+    panel_solves(F, n, kb, w, h, Pn);
     __syncthreads();
     // (e) A22 -= L21 U12.  Fragments: A[lane/4][lane%4], B[lane%4][lane/4],
     // C[lane/4][2 (lane%4) + {0, 1}]; panel columns past w are masked to 0.
