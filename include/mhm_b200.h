@@ -176,6 +176,24 @@ int mhm_q1_condense_offline(const mhm_q1_problem* p /* host */, int32_t precisio
                             int32_t* cell_iters, void* factors, void* stream);
 
 /*
+ * The local stage of up to 16 independent problems of one shape (macro grid, local
+ * refinement, trace spaces, precision) in one launch: problem k's macrocells are the
+ * CTAs (x, k), each reading problems[k] (host array) and writing problem k's own
+ * outputs (host arrays of device pointers, as for mhm_q1_condense).  factors may be
+ * NULL (a fresh condensation for every problem, mhm_q1_condense) or hold, per problem,
+ * NULL or a factor store to keep that problem's cell factors in
+ * (mhm_q1_condense_offline).  Permeability modes 0-2 only (no pre-pass); problems of
+ * different shapes give MHM_ERR_ARGUMENT, modes 3-6 MHM_ERR_UNSUPPORTED.  Every
+ * cell's arithmetic is that of the single-problem launch, so the outputs are
+ * identical.  Serving requests that arrive together batch their local stages this way
+ * (the per-request launches of a serving loop, core/offline.py:148-229, in one).
+ */
+int mhm_q1_condense_batch(int32_t count, const mhm_q1_problem* problems, int32_t precision,
+                          int32_t max_refine, double tol, double* const* solution, double* const* blocks,
+                          double* const* loads, uint8_t* const* corrected, int32_t* const* cell_status,
+                          int32_t* const* cell_iters, void* const* factors, void* stream);
+
+/*
  * Source response only (OfflineLocalProblem.response, core/offline.py:121-127):
  * re-assembles every cell with p's source and the offline permeability, reuses
  * `factors` instead of factoring, refines the source column and writes solution

@@ -100,6 +100,8 @@ _SIGNATURES = {
     "mhm_q1_rhs_width": (C.c_int32, [C.POINTER(Q1Problem)]),
     "mhm_q1_condense_smem_bytes": (C.c_int64, [C.POINTER(Q1Problem), C.c_int32]),
     "mhm_q1_condense": (C.c_int, [C.POINTER(Q1Problem), C.c_int32, C.c_int32, C.c_double, P, P, P, P, P, P, P]),
+    "mhm_q1_condense_batch": (C.c_int, [C.c_int32, C.POINTER(Q1Problem), C.c_int32, C.c_int32, C.c_double, P, P, P,
+                                        P, P, P, P, P]),
     "mhm_q1_factor_bytes": (C.c_int64, [C.POINTER(Q1Problem), C.c_int32]),
     "mhm_q1_condense_offline": (C.c_int, [C.POINTER(Q1Problem), C.c_int32, C.c_int32, C.c_double, P, P, P, P, P,
                                           P, P, P]),

@@ -670,10 +670,11 @@ __device__ __forceinline__ void assemble_cell(const Q1Args& a, int cell, double*
   __syncthreads();
 }
 
+// One macrocell's local stage (the body of q1_condense_kernel and of its batched
+// form): `a` describes the cell's problem, `cell` its index within that problem.
 template <typename T, int NNX, bool CUT>
-__global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_kernel(const Q1Args a) {
+__device__ __forceinline__ void condense_cell(const Q1Args& a, const int cell) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const int cell = blockIdx.x;
   const int tid = threadIdx.x;
   const int n = a.n, nnx = NNX > 0 ? NNX : a.nnx, nny = a.nny, w = a.w, t = a.t;
   const int nb = nnx * nnx, np1 = n + 1;
@@ -1025,6 +1026,24 @@ __global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_ker
     a.iters[cell] = it;
     a.corrected[cell] = any_nonzero ? 1 : 0;
   }
+}
+
+template <typename T, int NNX, bool CUT>
+__global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_kernel(const __grid_constant__ Q1Args a) {
+  condense_cell<T, NNX, CUT>(a, blockIdx.x);
+}
+
+// Several problems of one shape in one launch: blockIdx.y selects the problem (its
+// own permeability, source and output buffers), blockIdx.x the macrocell.
+constexpr int kMaxBatch = 16;
+struct Q1Batch {
+  Q1Args a[kMaxBatch];
+};
+
+template <typename T, int NNX>
+__global__ void __launch_bounds__(kThreads, Occupancy<T>::value) q1_condense_batch_kernel(
+    const __grid_constant__ Q1Batch b) {
+  condense_cell<T, NNX, false>(b.a[blockIdx.y], blockIdx.x);
 }
 
 // Pixel that holds the centre of global fine cell (gx, gy): points on a pixel line
@@ -1407,6 +1426,25 @@ int launch_condense(const Q1Args& a, int cells, cudaStream_t s) {
   }
 }
 
+template <typename T, int NNX>
+int launch_batch_variant(const Q1Batch& b, int count, int cells, size_t smem, cudaStream_t s) {
+  if (cudaFuncSetAttribute(q1_condense_batch_kernel<T, NNX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return MHM_ERR_LAUNCH;
+  q1_condense_batch_kernel<T, NNX><<<dim3(cells, count), kThreads, smem, s>>>(b);
+  return MHM_OK;
+}
+
+template <typename T>
+int launch_batch(const Q1Batch& b, int count, int cells, int nnx, size_t smem, cudaStream_t s) {
+  switch (nnx) {
+    case 5: return launch_batch_variant<T, 5>(b, count, cells, smem, s);
+    case 9: return launch_batch_variant<T, 9>(b, count, cells, smem, s);
+    case 17: return launch_batch_variant<T, 17>(b, count, cells, smem, s);
+    default: return launch_batch_variant<T, 0>(b, count, cells, smem, s);
+  }
+}
+
 }  // namespace
 }  // namespace mhm
 
@@ -1484,6 +1522,48 @@ extern "C" int mhm_q1_condense_offline(const mhm_q1_problem* p, int32_t precisio
                                        void* factors, void* stream) {
   return run_condense(p, precision, max_refine, tol, solution, blocks, loads, corrected, cell_status,
                       cell_iters, 1, factors, stream);
+}
+
+extern "C" int mhm_q1_condense_batch(int32_t count, const mhm_q1_problem* problems, int32_t precision,
+                                     int32_t max_refine, double tol, double* const* solution, double* const* blocks,
+                                     double* const* loads, uint8_t* const* corrected, int32_t* const* cell_status,
+                                     int32_t* const* cell_iters, void* const* factors, void* stream) {
+  if (count < 1 || count > kMaxBatch || !problems || !solution || !blocks || !loads || !corrected ||
+      !cell_status || !cell_iters || max_refine < 1 || !(tol > 0))
+    return MHM_ERR_ARGUMENT;
+  if (precision != MHM_PRECISION_FP64 && precision != MHM_PRECISION_MIXED) return MHM_ERR_ARGUMENT;
+  Q1Batch b;
+  for (int k = 0; k < count; ++k) {
+    Q1Args& a = b.a[k];
+    const int rc = fill_args(&problems[k], precision, a);
+    if (rc != MHM_OK) return rc;
+    if (!solution[k] || !blocks[k] || !loads[k] || !corrected[k] || !cell_status[k] || !cell_iters[k])
+      return MHM_ERR_ARGUMENT;
+    // one shape per launch (shared-memory layout and kernel variant), and no
+    // permeability pre-pass (pixel fields that cut the fine cells, Gauss-point fields)
+    if (a.cut_mode || a.kmode >= 3) return MHM_ERR_UNSUPPORTED;
+    const Q1Args& a0 = b.a[0];
+    if (a.nx != a0.nx || a.ny != a0.ny || a.rx != a0.rx || a.ry != a0.ry || a.t != a0.t || a.w != a0.w ||
+        a.smem != a0.smem)
+      return MHM_ERR_ARGUMENT;
+    if (a.smem > 227 * 1024) return MHM_ERR_UNSUPPORTED;
+    a.max_refine = max_refine;
+    a.tol = tol;
+    a.sol = solution[k];
+    a.blocks = blocks[k];
+    a.loads = loads[k];
+    a.corrected = corrected[k];
+    a.status = cell_status[k];
+    a.iters = cell_iters[k];
+    a.mode = (factors && factors[k]) ? 1 : 0;
+    a.factors = (factors && factors[k]) ? factors[k] : nullptr;
+  }
+  const int cells = b.a[0].nx * b.a[0].ny;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int rc = precision == MHM_PRECISION_FP64 ? launch_batch<double>(b, count, cells, b.a[0].nnx, b.a[0].smem, s)
+                                                 : launch_batch<float>(b, count, cells, b.a[0].nnx, b.a[0].smem, s);
+  if (rc != MHM_OK) return rc;
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
 
 extern "C" int mhm_q1_source_response(const mhm_q1_problem* p, int32_t precision, int32_t max_refine,

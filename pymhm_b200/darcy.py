@@ -491,7 +491,9 @@ class CartesianQ1Plan:
         ``local`` selects the local stage: ``"condense"``; ``"offline"`` (condense and
         keep each cell's factor, see ``prepare_offline``); ``"online"`` (source
         response only with the kept factors; Schur blocks and the skeleton matrix
-        are reused, only the right-hand side is reduced).
+        are reused, only the right-hand side is reduced); ``"batched"`` (the local
+        stage was enqueued on ``stream`` by ``condense_batch`` together with other
+        plans': the launch starts at the reduction).
         """
         L, s = self.lib, _lib.stream_handle(stream)
         P = _lib.ptr
@@ -532,8 +534,8 @@ class CartesianQ1Plan:
                                                 P(self.solution), P(self.loads), P(self.corrected),
                                                 P(self.cell_status), P(self.cell_iters), s),
                        "mhm_q1_source_response")
-        else:
-            raise ValueError("local must be 'condense', 'offline' or 'online'")
+        elif local != "batched":
+            raise ValueError("local must be 'condense', 'offline', 'online' or 'batched'")
         mark(1, cur)
         pat = self.pattern
         # online: the skeleton matrix is unchanged, only the right-hand side is reduced
@@ -932,6 +934,53 @@ class CartesianQ1Plan:
         indptr, indices, data = self.export_csc()
         return sparse.csc_matrix((data.cpu().numpy(), indices.cpu().numpy(), indptr.cpu().numpy()),
                                  shape=(self.N, self.N))
+
+
+def condense_batch(plans, *, offline=False, stream=None):
+    """One launch of the local stage of several plans of one shape (macro grid, local
+    refinement, trace spaces, precision), each with its own permeability and source
+    already set: the cells of plan k are the CTAs (x, k) of ``mhm_q1_condense_batch``,
+    which writes every plan's own responses, Schur blocks and status words exactly as
+    its own ``mhm_q1_condense`` launch would.  With ``offline``, each plan keeps its
+    cells' factors for later sources (``prepare_offline``).  Follow with
+    ``plan.launch(stream, local="batched")`` per plan.  This is the cross-request
+    batching of a serving loop's local stages; at most 16 plans per launch and
+    permeabilities without a pre-pass (constant, per fine cell, or pixels aligned with
+    the fine grid)."""
+    import ctypes as C
+
+    plans = list(plans)
+    if not 1 <= len(plans) <= 16:
+        raise ValueError("condense_batch takes 1 to 16 plans")
+    first = plans[0]
+    for p in plans:
+        if p.precision != first.precision or (p.mesh.nx, p.mesh.ny, p.rx, p.ry) != (first.mesh.nx, first.mesh.ny,
+                                                                                   first.rx, first.ry):
+            raise ValueError("condense_batch needs plans of one shape and precision")
+    torch = first.torch
+    lib = first.lib
+    prec = PRECISIONS[first.precision]
+    if offline:
+        for p in plans:
+            if getattr(p, "factors", None) is None:
+                nbytes = int(lib.mhm_q1_factor_bytes(p.q1, prec))
+                if nbytes <= 0:
+                    raise RuntimeError("could not size the factor store")
+                p.factors = torch.empty(nbytes, dtype=torch.uint8, device=p.device)
+    k = len(plans)
+    P = _lib.ptr
+
+    def arr(name):
+        return (C.c_void_p * k)(*[P(getattr(p, name)) for p in plans])
+
+    problems = (_lib.Q1Problem * k)(*[p.q1 for p in plans])
+    factors = arr("factors") if offline else None
+    _lib.check(lib.mhm_q1_condense_batch(k, problems, prec, first.max_refine, first.local_tol, arr("solution"),
+                                         arr("blocks"), arr("loads"), arr("corrected"), arr("cell_status"),
+                                         arr("cell_iters"), factors, _lib.stream_handle(stream)),
+               "mhm_q1_condense_batch")
+    for p in plans:
+        p._factors_current = bool(offline)
 
 
 def solve_darcy_quadrilateral(mesh, *, permeability=1.0, source=0.0, dirichlet=0.0, neumann=None,
