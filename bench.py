@@ -482,7 +482,7 @@ def profile_case(torch, cube=0, count=0):
             "global_iterations": int(info[1]), "inner_solves": int(info[2]), "residual": float(stats[0])}
 
 
-def serving_campaign(torch, lambdas=(100, 500, 2000), requests=150, precisions=("mixed", "fp64")):
+def serving_campaign(torch, lambdas=(100, 500, 2000), requests=150, precisions=("mixed", "fp64"), batch_local=False):
     """Streamed serving (continuous batching with admission by HBM footprint): Poisson
     arrivals at each rate in ``lambdas``; per request a macro grid from {16, 32, 64}^2,
     a local refinement from {4, 8, 16}^2, a seeded log-normal permeability (sigma in
@@ -491,8 +491,9 @@ def serving_campaign(torch, lambdas=(100, 500, 2000), requests=150, precisions=(
     factors kept, the others through the kept factors.  Before timing, as many slots per
     shape as requests may be in flight (8) are reserved (plans built, both steps
     captured as CUDA graphs), so that no slot is built inside a timed stream, and one
-    untimed stream warms them.  Returns p50/p99 latency (arrival to results in pinned host
-    memory) and solves/s per rate and precision."""
+    untimed stream warms them.  With ``batch_local``, requests of one shape admitted
+    together share one local-stage launch.  Returns p50/p99 latency (arrival to results
+    in pinned host memory) and solves/s per rate and precision."""
     from pymhm_b200.serving import DarcyRequest, ServingEngine, summarize
     from pymhm_b200.workloads import lognormal_permeability
 
@@ -518,7 +519,7 @@ def serving_campaign(torch, lambdas=(100, 500, 2000), requests=150, precisions=(
 
     result = {}
     for prec in precisions:
-        engine = ServingEngine(precision=prec, max_in_flight=8)
+        engine = ServingEngine(precision=prec, max_in_flight=8, batch_local=batch_local)
         for m in SERVING_MACRO:
             for r in SERVING_LOCAL:
                 engine.reserve((m, r, FACE_DEGREE), engine.max_in_flight)
@@ -526,7 +527,10 @@ def serving_campaign(torch, lambdas=(100, 500, 2000), requests=150, precisions=(
         engine.run(warm, realtime=False)
         per = {}
         for lam in lambdas:
+            before = dict(engine.stats)
             per[f"lambda_{lam}"] = summarize(engine.run(stream(lam, requests, lam)))
+            per[f"lambda_{lam}"]["batched_requests"] = (engine.stats.get("batched_requests", 0)
+                                                        - before.get("batched_requests", 0))
         per["slots"] = len(engine.slots)
         per["peak_device_bytes"] = int(engine.stats.get("peak_bytes", 0))
         result[prec] = per
@@ -534,7 +538,8 @@ def serving_campaign(torch, lambdas=(100, 500, 2000), requests=150, precisions=(
         torch.cuda.empty_cache()
     result["workload"] = (f"{requests} requests per rate, Poisson arrivals; macro in {SERVING_MACRO}^2, local in "
                           f"{SERVING_LOCAL}^2, P2 faces, 1..8 constant sources per request (kept factors); "
-                          "HBM budget 150 GB, 8 requests in flight")
+                          "HBM budget 150 GB, 8 requests in flight; same-shape requests admitted together "
+                          f"share one local-stage launch: {bool(batch_local)}")
     return result
 
 

@@ -801,12 +801,16 @@ class CartesianQ1Plan:
         ``source_mode`` 0).  ``"condense"`` captures a complete fresh solve with the
         coefficients exactly as set (pointwise sources included); its replays take no
         source and refuse to run once ``set_coefficients`` has moved the coefficient
-        buffers.  The graph's launches run once eagerly before the capture."""
+        buffers.  ``"batched"`` captures the reduction, global solve and reconstruction
+        that follow a ``condense_batch`` local stage (its replays take no source).  The
+        graph's launches run once eagerly before the capture."""
         torch = self.torch
-        if local not in ("offline", "online", "condense"):
-            raise ValueError("local must be 'offline', 'online' or 'condense'")
+        if local not in ("offline", "online", "condense", "batched"):
+            raise ValueError("local must be 'offline', 'online', 'condense' or 'batched'")
         if local == "condense":
             return self._capture_graph(local, stream, keep=self._keep)
+        if local == "batched":  # the rest of a solve whose local stage ran in condense_batch
+            return self._capture_graph(local, stream)
         if local == "online" and not getattr(self, "_factors_current", False):
             raise RuntimeError("prepare_offline() must run before capturing online queries")
         if local == "offline" and getattr(self, "factors", None) is None:
@@ -851,6 +855,15 @@ class CartesianQ1Plan:
         graph = (getattr(self, "_graphs", None) or {}).get(local)
         if graph is None:
             raise RuntimeError(f"capture({local!r}) must run first")
+        if local == "batched":
+            if source is not None:
+                raise ValueError("the batched remainder takes no source: the local stage consumed it")
+            st = self._graph_stream if stream is None else stream
+            if after is not st:
+                st.wait_stream(torch.cuda.current_stream() if after is None else after)
+            with torch.cuda.stream(st):
+                graph.replay()
+            return st
         if local == "condense":
             if source is not None:
                 raise ValueError("the captured fresh solve reads the coefficients set before capture; "

@@ -54,6 +54,35 @@ def test_results_are_the_same_alone_and_in_the_mix(precision):
             assert rel(res.x[k][: plan.T], sol.trace) <= tol
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_batched_local_stages_give_the_same_results(precision):
+    """Requests of one shape admitted together share one local-stage launch
+    (``condense_batch``); every source of every request equals the unbatched loop's
+    result bit for bit."""
+    from pymhm_b200.serving import DarcyRequest, ServingEngine
+    from pymhm_b200.workloads import lognormal_permeability
+
+    rng = np.random.default_rng(23)
+    reqs = []
+    for i in range(8):
+        macro, ref = [(8, 8), (4, 16)][i % 2]
+        n = macro * ref
+        kappa = lognormal_permeability(n, n, sigma=2.0, ell=0.1, seed=int(rng.integers(1 << 30)))
+        sources = tuple(float(v) for v in rng.uniform(0.5, 2.0, int(rng.integers(1, 4))))
+        reqs.append(DarcyRequest(macro, ref, kappa, sources))
+    batched = ServingEngine(precision=precision, max_in_flight=8, keep_fields=True, batch_local=True)
+    got = batched.run(reqs, realtime=False)
+    assert batched.stats["batched_requests"] == 8 and batched.stats["batched_local_launches"] == 2
+    plain = ServingEngine(precision=precision, max_in_flight=8, keep_fields=True)
+    ref = plain.run(reqs, realtime=False)
+    assert "batched_requests" not in plain.stats
+    for req, a, b in zip(reqs, got, ref):
+        for k in range(len(req.sources)):
+            assert np.array_equal(a.x[k], b.x[k])
+            assert np.array_equal(a.fields[k], b.fields[k])
+            assert np.array_equal(a.flux[k], b.flux[k])
+
+
 def test_admission_respects_the_hbm_budget():
     from pymhm_b200.serving import ServingEngine
 
