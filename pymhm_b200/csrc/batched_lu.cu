@@ -1256,7 +1256,71 @@ __global__ void __launch_bounds__(kLuThreads) batched_solve_chunked_kernel(
     // B[lane%4][lane/4], C[lane/4][2 (lane%4) + {0, 1}]), with per lane the sums of
     // (r / scale)^2 of its columns; only when it fails the acceptance, the accurate
     // residual below, which also feeds the correction.
-    {
+    if constexpr (GW) {
+      // large orders: 32 rows at a time, the eight warps splitting the inner dimension
+      // (each forms the 32-row block's partial product for all columns over its share
+      // of k, the partials summed in warp order through the shared buffer after colr),
+      // so X is read once per 32 rows and every warp streams a short k-range.  Thread
+      // t keeps the sum of (r / scale)^2 of column t % 32 over its rows.
+      const int fr = lane >> 2, fc = lane & 3;
+      const int ncb = (nrhs + 7) >> 3;
+      double* pp = colr + 3 * KC;  // (8, 32, 32) partials
+      double s2c = 0.0;
+      for (int i0 = 0; i0 < n; i0 += 32) {
+        double acc[4][NCB][2] = {};
+        const double* arow[4];
+#pragma unroll
+        for (int rb = 0; rb < 4; ++rb) arow[rb] = A + (size_t)min(i0 + 8 * rb + fr, n - 1) * n;
+#pragma unroll 4
+        for (int k = 4 * wid; k < n; k += 4 * nw) {
+          const int kk = k + fc;
+          const bool kv = kk < n;
+          double a[4], b[NCB];
+#pragma unroll
+          for (int rb = 0; rb < 4; ++rb) a[rb] = kv ? arow[rb][kk] : 0.0;
+#pragma unroll
+          for (int cb = 0; cb < NCB; ++cb) {
+            const int col = 8 * cb + fr;
+            b[cb] = (kv && cb < ncb && col < nrhs) ? X[(size_t)kk * ws + col] : 0.0;
+          }
+#pragma unroll
+          for (int rb = 0; rb < 4; ++rb)
+#pragma unroll
+            for (int cb = 0; cb < NCB; ++cb) dmma_8x8x4(acc[rb][cb][0], acc[rb][cb][1], a[rb], b[cb]);
+        }
+#pragma unroll
+        for (int rb = 0; rb < 4; ++rb)
+#pragma unroll
+          for (int cb = 0; cb < NCB; ++cb)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) pp[wid * 1024 + (8 * rb + fr) * 32 + 8 * cb + 2 * fc + e] = acc[rb][cb][e];
+        __syncthreads();
+        for (int idx = tid; idx < 32 * 32; idx += blockDim.x) {
+          const int r = idx >> 5, c = idx & 31;
+          if (i0 + r < n && c < nrhs) {
+            double t = 0.0;
+            for (int q = 0; q < nw; ++q) t += pp[q * 1024 + idx];
+            const double rv = (B[(size_t)(i0 + r) * ldr + c] - t) / colr[c];
+            s2c = fma(rv, rv, s2c);
+          }
+        }
+        __syncthreads();
+      }
+      part[wid * KC + lane] = s2c;  // column lane of this warp's rows
+      __syncthreads();
+      if (tid == 0) {
+        int ok = 1;
+        for (int c = 0; c < nrhs; ++c) {
+          double t = 0.0;
+          for (int q = 0; q < nw; ++q) t += part[q * KC + c];
+          const double limit = fmax(atol / colr[c], rtol * sqrt(colr[KC + c]));
+          if (!(sqrt(t) <= limit)) ok = 0;
+        }
+        flag = ok;
+      }
+      __syncthreads();
+      if (flag) { result = MHM_CELL_OK; break; }
+    } else {
       const int fr = lane >> 2, fc = lane & 3;
       const int ncb = (nrhs + 7) >> 3;
       double s2[NCB][2] = {};

@@ -237,7 +237,7 @@ class PolygonP2Plan:
             budget = self.workspace_bytes
             if budget is None:
                 free, _ = torch.cuda.mem_get_info(dev)
-                budget = min(48 << 30, int(0.4 * free))
+                budget = min(112 << 30, int(0.6 * free))
             half = max(budget // 16, max(b["nb"] for b in large_bins) ** 2)  # doubles per half
             cur = None
             for b in reversed(large_bins):
