@@ -557,11 +557,16 @@ __global__ void __launch_bounds__(kLuThreads) batched_factor_blocked_kernel(
 constexpr int kLargeMaxN = 4096;
 constexpr int kUTile = 64;
 constexpr int kUStride = kUTile + 4;  // row stride of the staged U12 tile
-// Per-warp stages of the trailing update: 16 C rows of 64 columns, the row stride
-// chosen so that the fragment loads (two doubles a lane) hit distinct banks.
+// The factorization runs kLargeThreads threads a CTA; in the trailing update each warp
+// takes blocks of kBlockRows rows (kHalves 8-row halves).  Per-warp stages: kBlockRows
+// C rows of 64 columns, the row stride chosen so that the fragment loads (two doubles
+// a lane) hit distinct banks.
+constexpr int kLargeThreads = 512;
+constexpr int kBlockRows = 8;
+constexpr int kHalves = kBlockRows / 8;
 constexpr int kCStride = kUTile + 8;
-constexpr int kStageDoubles = 16 * kCStride;
-constexpr size_t kLargeStageBytes = (size_t)(kLuThreads / 32) * 2 * kStageDoubles * sizeof(double);
+constexpr int kStageDoubles = kBlockRows * kCStride;
+constexpr size_t kLargeStageBytes = (size_t)(kLargeThreads / 32) * 2 * kStageDoubles * sizeof(double);
 constexpr long long kSpinLimit = 1ll << 24;  // polls of an mbarrier before a copy is given up
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -634,7 +639,7 @@ __device__ __noinline__ void panel_solves(double* F, int n, int kb, int w, int h
     }
 }
 
-__global__ void __launch_bounds__(kLuThreads, 1) large_factor_kernel(
+__global__ void __launch_bounds__(kLargeThreads, 1) large_factor_kernel(
     const mhm_ragged_matrix* __restrict__ desc, int max_n, const double* __restrict__ mats,
     double* __restrict__ factors, int32_t* __restrict__ piv, double* __restrict__ rs, double* __restrict__ cs,
     int32_t* __restrict__ status) {
@@ -642,7 +647,7 @@ __global__ void __launch_bounds__(kLuThreads, 1) large_factor_kernel(
   __shared__ double Pn[(kPanel + 1) * kPanelStride];  // the window: (w + 1) x w
   __shared__ __align__(16) double Us[kPanel * kUStride];  // U12 tile: 32 x 64
   __shared__ double red[32];
-  __shared__ __align__(8) uint64_t bars[2 * (kLuThreads / 32)];
+  __shared__ __align__(8) uint64_t bars[2 * (kLargeThreads / 32)];
   __shared__ int sperm[kPanel];
   __shared__ int apos[2 * kPanel + 2], asrc[2 * kPanel + 2];
   __shared__ int srcrow[kPanel + 1];
@@ -788,11 +793,11 @@ __global__ void __launch_bounds__(kLuThreads, 1) large_factor_kernel(
         // the U12 tile).
         const int cols = min(kUTile, m2 - tj);
         const uint32_t cbytes = (uint32_t)cols * 8u;
-        const int nblk = 16 * wid < m2 ? (m2 - 16 * wid + 16 * nw - 1) / (16 * nw) : 0;
+        const int nblk = kBlockRows * wid < m2 ? (m2 - kBlockRows * wid + kBlockRows * nw - 1) / (kBlockRows * nw) : 0;
         double* stg = stages + (size_t)wid * 2 * kStageDoubles;
         auto issue_at = [&](int t, uint32_t q, int tjx) {
-          const int rb = 16 * wid + 16 * nw * t;
-          const int rows = min(16, m2 - rb);
+          const int rb = kBlockRows * wid + kBlockRows * nw * t;
+          const int rows = min(kBlockRows, m2 - rb);
           const uint32_t cb = (uint32_t)min(kUTile, m2 - tjx) * 8u;
           uint64_t* bar = &bars[2 * wid + (q & 1u)];
           fence_proxy_async_smem();
@@ -803,16 +808,16 @@ __global__ void __launch_bounds__(kLuThreads, 1) large_factor_kernel(
                           F + (size_t)(base + rb + lane) * n + base + tjx, cb, bar);
         };
         auto issue = [&](int t, uint32_t q) { issue_at(t, q, tj); };
-        auto load_l21 = [&](int t, double (&a)[2][kPanel / 4]) {
-          const int rb = 16 * wid + 16 * nw * t;
+        auto load_l21 = [&](int t, double (&a)[kHalves][kPanel / 4]) {
+          const int rb = kBlockRows * wid + kBlockRows * nw * t;
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
+          for (int h = 0; h < kHalves; ++h) {
             const int i = min(rb + 8 * h + fr, m2 - 1);
 #pragma unroll
             for (int s = 0; s < kPanel / 4; ++s) a[h][s] = -F[(size_t)(base + i) * n + kb + 4 * s + fc];
           }
         };
-        double av[2][kPanel / 4];
+        double av[kHalves][kPanel / 4];
         if (nblk > 0) {
           if (!prefetched) issue(0, qcount);
           load_l21(0, av);
@@ -820,7 +825,7 @@ __global__ void __launch_bounds__(kLuThreads, 1) large_factor_kernel(
         prefetched = false;
         for (int t = 0; t < nblk; ++t) {
           const uint32_t q = qcount + (uint32_t)t;
-          double an[2][kPanel / 4];
+          double an[kHalves][kPanel / 4];
           if (t + 1 < nblk) {
             issue(t + 1, q + 1);
             load_l21(t + 1, an);
@@ -838,10 +843,10 @@ __global__ void __launch_bounds__(kLuThreads, 1) large_factor_kernel(
             break;
           }
           const double* sC = stg + (q & 1u) * kStageDoubles;
-          const int rb = 16 * wid + 16 * nw * t;
-          double acc[2][8][2];
+          const int rb = kBlockRows * wid + kBlockRows * nw * t;
+          double acc[kHalves][8][2];
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
+          for (int h = 0; h < kHalves; ++h) {
             const int i = rb + 8 * h + fr;
 #pragma unroll
             for (int b = 0; b < 8; ++b) {
@@ -859,13 +864,12 @@ __global__ void __launch_bounds__(kLuThreads, 1) large_factor_kernel(
 #pragma unroll
             for (int b = 0; b < 8; ++b) bv[b] = Us[(4 * s + fc) * kUStride + 8 * b + fr];
 #pragma unroll
-            for (int b = 0; b < 8; ++b) {
-              dmma_8x8x4(acc[0][b][0], acc[0][b][1], av[0][s], bv[b]);
-              dmma_8x8x4(acc[1][b][0], acc[1][b][1], av[1][s], bv[b]);
-            }
+            for (int b = 0; b < 8; ++b)
+#pragma unroll
+              for (int h = 0; h < kHalves; ++h) dmma_8x8x4(acc[h][b][0], acc[h][b][1], av[h][s], bv[b]);
           }
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
+          for (int h = 0; h < kHalves; ++h) {
             const int i = rb + 8 * h + fr;
             if (i < m2) {
               double* crow = F + (size_t)(base + i) * n + base + tj;
@@ -879,7 +883,7 @@ __global__ void __launch_bounds__(kLuThreads, 1) large_factor_kernel(
           __syncwarp();  // every lane has read the stage before block t + 2 is copied into it
           if (t + 1 < nblk) {
 #pragma unroll
-            for (int h = 0; h < 2; ++h)
+            for (int h = 0; h < kHalves; ++h)
 #pragma unroll
               for (int s = 0; s < kPanel / 4; ++s) av[h][s] = an[h][s];
           }
@@ -1620,7 +1624,7 @@ extern "C" int mhm_batched_factor_large(int64_t count, const mhm_ragged_matrix* 
   if (cudaFuncSetAttribute(large_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)kLargeStageBytes) != cudaSuccess)
     return MHM_ERR_LAUNCH;
-  large_factor_kernel<<<(unsigned)count, kLuThreads, kLargeStageBytes, static_cast<cudaStream_t>(stream)>>>(
+  large_factor_kernel<<<(unsigned)count, kLargeThreads, kLargeStageBytes, static_cast<cudaStream_t>(stream)>>>(
       desc, max_n, matrices, factors, pivots, row_scale, col_scale, status);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
