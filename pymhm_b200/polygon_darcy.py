@@ -561,7 +561,7 @@ class PolygonP2Plan:
         (largest first).  The responses land in the resident right-hand-side layout."""
         torch, P, lib, d = self.torch, _lib.ptr, self.lib, self.d
         if not hasattr(self, "chunk_streams"):
-            self.chunk_streams = [torch.cuda.Stream(device=self.device) for _ in range(8)]
+            self.chunk_streams = [torch.cuda.Stream(device=self.device) for _ in range(16)]
         for ch in self.chunks:
             n0, n1 = ch["nodes"]
             self._assemble_rows(n0, n1, self.ws_aug, self.ws_factors, sh)
