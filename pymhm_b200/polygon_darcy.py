@@ -98,7 +98,15 @@ class PolygonSolution:
 
 class PolygonP2Plan:
     """Device-resident plan of one polygonal problem shape (mesh, skeleton, per-cell
-    refinement): local meshes, couplings, bins, sparsity and every buffer."""
+    refinement): local meshes, couplings, bins, sparsity and every buffer.
+
+    Local P2 spaces up to 639 unknowns form the small tier (every dense matrix
+    resident, ragged launches of the shared-memory-panel LU); larger ones, up to 4095,
+    the large tier: their dense matrices pass through a workspace of
+    ``workspace_bytes`` (default: the smaller of 112 GiB and 60 % of free device
+    memory) in chunks, largest first, factored by the windowed-pivot LU in HBM.
+    ``workers`` spawned processes build the cells' local meshes and couplings on the
+    host (1: in this process)."""
 
     def __init__(self, mesh: PolygonMesh, skeleton: EdgeSkeleton | None = None, refinements=2, *, order=4,
                  bin_width=32, streams=4, ragged=True, device=None, global_rtol=1e-13, inner_rtol=1e-10,
