@@ -667,6 +667,20 @@ int mhm_batched_solve_ragged(int64_t count, const mhm_ragged_matrix* desc, int32
                              int32_t* status, void* stream);
 
 /*
+ * mhm_dense_systems over ragged cells in one launch: cell k of the launch is described
+ * by desc[k] (order nb = n with lds = nb, nrhs = w columns, its stiffness, mass and
+ * augmented matrix at mat_off (the augmented matrix may overwrite the stiffness), its
+ * load at vec_off, actions at 3 vec_off, right-hand sides at rhs_off, sizes, flag
+ * and status at slot) and by cpl_off[k] / tld_of[k] (its coupling block and width).
+ * Same arithmetic per cell as mhm_dense_systems.
+ */
+int mhm_dense_systems_ragged(int64_t count, const mhm_ragged_matrix* desc, const int64_t* cpl_off,
+                             const int32_t* tld_of, int32_t normalize, const int32_t* n_of,
+                             const int32_t* t_of, const double* stiffness, const double* mass,
+                             const double* load, const double* coupling, double* aug, double* rhs,
+                             double* action, uint8_t* corrected, int32_t* status, void* stream);
+
+/*
  * Large orders (n <= 4096; larger get MHM_CELL_SIZE): ragged batches of the bordered
  * local systems [[A, c], [c^T, 0]] (A positive semi-definite with the constants as
  * its kernel, identity padding allowed).  The factorization is the blocked LU in

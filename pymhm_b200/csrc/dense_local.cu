@@ -77,23 +77,46 @@ constexpr int kDThreads = 256;
 constexpr int kTileStride = 33;  // odd: a thread's row of a staged tile spans distinct banks
 constexpr size_t kSystemSmem = (size_t)kDThreads * kTileStride * sizeof(double);  // a 32 x 33 tile per warp
 
+// With desc (ragged launches), CTA k builds the system desc[k] describes: order nb =
+// desc.n (= lds), w = desc.nrhs columns, its matrices at mat_off (stiffness, mass and
+// augmented matrix alike), load at vec_off, actions at 3 vec_off, right-hand sides at
+// rhs_off, coupling at cpl_off[k] with tld_of[k] columns, and the cell's sizes, flag
+// and status at slot.
 __global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
     int lds, int tld, int nb, int w, int normalize, const int32_t* __restrict__ n_of,
     const int32_t* __restrict__ t_of,
     const double* __restrict__ stiffness, const double* __restrict__ mass, const double* __restrict__ load,
     const double* __restrict__ coupling, double* __restrict__ aug, double* __restrict__ rhs,
-    double* __restrict__ action, uint8_t* __restrict__ corrected, int32_t* __restrict__ status) {
+    double* __restrict__ action, uint8_t* __restrict__ corrected, int32_t* __restrict__ status,
+    const mhm_ragged_matrix* __restrict__ desc, const int64_t* __restrict__ cpl_off,
+    const int32_t* __restrict__ tld_of) {
   extern __shared__ __align__(16) double tiles[];
   __shared__ double red[32];
   __shared__ int nonzero;
-  const int64_t cell = blockIdx.x;
+  int64_t cell = blockIdx.x;
   const int tid = threadIdx.x;
+  int64_t moff = cell * (int64_t)lds * lds, koff = cell * (int64_t)nb * nb, roff = cell * (int64_t)nb * w,
+          aoff = cell * 3 * (int64_t)nb, loff = cell * (int64_t)lds, coff = cell * (int64_t)lds * tld;
+  if (desc) {
+    const mhm_ragged_matrix d = desc[blockIdx.x];
+    cell = d.slot;
+    nb = lds = d.n;
+    w = d.nrhs;
+    tld = tld_of[blockIdx.x];
+    moff = koff = d.mat_off;
+    roff = d.rhs_off;
+    aoff = 3 * d.vec_off;
+    loff = d.vec_off;
+    coff = cpl_off[blockIdx.x];
+  }
   const int n = n_of[cell], t = t_of[cell];
-  const double* A = stiffness + cell * (int64_t)lds * lds;
-  const double* Mm = mass + cell * (int64_t)lds * lds;
-  double* K = aug + cell * (int64_t)nb * nb;
-  double* R = rhs + cell * (int64_t)nb * w;
-  double* act = action + cell * 3 * (int64_t)nb;  // rows: A 1, A^T 1, the constraint
+  const double* A = stiffness + moff;
+  const double* Mm = mass + moff;
+  double* K = aug + koff;
+  double* R = rhs + roff;
+  double* act = action + aoff;  // rows: A 1, A^T 1, the constraint
+  const double* ldv = load + loff;
+  const double* cpl = coupling + coff;
   if (tid == 0) nonzero = 0;
   // max |A| and ||A||_F^2, the retained action A 1 and the test action A^T 1 (double-double
   // sums, the reference's extended-precision _matrix_action), the plain products A 1
@@ -189,8 +212,8 @@ __global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
     for (int col = lane; col < w; col += 32) {
       double v = 0.0;
       if (i < n) {
-        if (col == 0) v = load[cell * lds + i];
-        else if (col <= t) v = coupling[(cell * lds + i) * tld + (col - 1)];
+        if (col == 0) v = ldv[i];
+        else if (col <= t) v = cpl[(int64_t)i * tld + (col - 1)];
         else if (col == t + 1) v = corr ? act[i] : 0.0;
       }
       Ri[col] = v;
@@ -354,7 +377,24 @@ extern "C" int mhm_dense_systems(int64_t count, int32_t lds, int32_t tld, int32_
     return MHM_ERR_LAUNCH;
   dense_system_kernel<<<(unsigned)count, kDThreads, kSystemSmem, static_cast<cudaStream_t>(stream)>>>(
       lds, tld, nb, w, normalize, n_of, t_of, stiffness, mass, load, coupling, aug, rhs, action, corrected,
-      status);
+      status, nullptr, nullptr, nullptr);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+extern "C" int mhm_dense_systems_ragged(int64_t count, const mhm_ragged_matrix* desc, const int64_t* cpl_off,
+                                        const int32_t* tld_of, int32_t normalize, const int32_t* n_of,
+                                        const int32_t* t_of, const double* stiffness, const double* mass,
+                                        const double* load, const double* coupling, double* aug, double* rhs,
+                                        double* action, uint8_t* corrected, int32_t* status, void* stream) {
+  if (count < 1 || count > INT32_MAX || !desc || !cpl_off || !tld_of || !n_of || !t_of || !stiffness || !mass ||
+      !load || !coupling || !aug || !rhs || !action || !corrected || !status)
+    return MHM_ERR_ARGUMENT;
+  if (cudaFuncSetAttribute(dense_system_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSystemSmem) !=
+      cudaSuccess)
+    return MHM_ERR_LAUNCH;
+  dense_system_kernel<<<(unsigned)count, kDThreads, kSystemSmem, static_cast<cudaStream_t>(stream)>>>(
+      0, 0, 0, 0, normalize, n_of, t_of, stiffness, mass, load, coupling, aug, rhs, action, corrected, status, desc,
+      cpl_off, tld_of);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
 

@@ -15,6 +15,10 @@ cells padded with an identity block (their solution is zero there).  One solve:
    equilibrated LU), ``mhm_dense_contributions`` (tensor-core products);
 3. ``mhm_skeleton_scatter`` (ordered, ragged blocks) and ``mhm_general_solve``;
 4. per bin: ``mhm_dense_reconstruct``.
+
+Cells above augmented order 640 (the large tier) take, per workspace chunk,
+``mhm_p2_assemble_rows``, ``mhm_dense_systems_ragged``, ``mhm_batched_factor_large``
+and ``mhm_batched_solve_large`` in step 2.
 """
 
 from __future__ import annotations
@@ -282,6 +286,11 @@ class PolygonP2Plan:
                                dtype=[("mat_off", "<i8"), ("vec_off", "<i8"), ("rhs_off", "<i8"), ("n", "<i4"),
                                       ("nrhs", "<i4"), ("slot", "<i4"), ("reserved", "<i4")])
                 ch["desc"] = torch.as_tensor(rec.view(np.uint8).copy()).to(dev)
+                # the coupling blocks and widths, in the descriptors' order
+                ch["cpl_off"] = torch.as_tensor(np.array([b["cpl"] + j * b["nb"] * b["tld"]
+                                                          for b, j, _ in reversed(ch["slots"])], dtype=np.int64)).to(dev)
+                ch["tld_of"] = torch.as_tensor(np.array([b["tld"] for b, _, _ in reversed(ch["slots"])],
+                                                        dtype=np.int32)).to(dev)
                 ch["count"] = len(rec)
                 ch["max_n"] = int(rec["n"].max())
                 ch["max_w"] = int(rec["nrhs"].max())
@@ -564,38 +573,21 @@ class PolygonP2Plan:
 
     def _large_chunks(self, st, sh, factor_events=None):
         """The large tier, one chunk after another on ``st``: node rows into the workspace,
-        the augmented systems in place over the stiffness (per bin part), then one
-        large-order factorization and one checked solve launch over the chunk's cells
-        (largest first).  The responses land in the resident right-hand-side layout."""
+        then one ragged launch each of the augmented systems (in place over the
+        stiffness), the large-order factorization and the checked solve over the chunk's
+        cells (largest first).  The responses land in the resident right-hand-side
+        layout."""
         torch, P, lib, d = self.torch, _lib.ptr, self.lib, self.d
-        if not hasattr(self, "chunk_streams"):
-            self.chunk_streams = [torch.cuda.Stream(device=self.device) for _ in range(16)]
         for ch in self.chunks:
             n0, n1 = ch["nodes"]
             self._assemble_rows(n0, n1, self.ws_aug, self.ws_factors, sh)
-            # a bin part is a few dozen cells: the parts' system launches run side by
-            # side on the chunk streams, so that together they fill the SMs
-            fork = torch.cuda.Event()
-            fork.record(st)
-            used = self.chunk_streams[: len(ch["parts"])]
-            for cs in used:
-                cs.wait_event(fork)
-            for idx, part in enumerate(ch["parts"]):
-                b, j0, j1, ws = part["bin"], part["j0"], part["j1"], part["ws"]
-                nb, w, tld = b["nb"], b["w"], b["tld"]
-                sl = slice(b["pos"] + j0, b["pos"] + j1)
-                csh = _lib.stream_handle(used[idx % len(used)])
-                _lib.check(lib.mhm_dense_systems(j1 - j0, nb, tld, nb, w, 1, P(d["n_of"][sl]), P(d["t_of"][sl]),
-                                                 P(self.ws_aug[ws:]), P(self.ws_factors[ws:]),
-                                                 P(self.load[b["load"] + j0 * nb:]),
-                                                 P(d["coupling"][b["cpl"] + j0 * nb * tld:]), P(self.ws_aug[ws:]),
-                                                 P(self.rhs[b["rhs"] + j0 * nb * w:]),
-                                                 P(self.action[b["act"] + j0 * 3 * nb:]), P(self.corrected[sl]),
-                                                 P(self.cell_status[sl]), csh), "mhm_dense_systems")
-            for cs in used:
-                join = torch.cuda.Event()
-                join.record(cs)
-                st.wait_event(join)
+            # the augmented systems of every cell of the chunk, in place over the
+            # stiffness, in one ragged launch (largest first)
+            _lib.check(lib.mhm_dense_systems_ragged(ch["count"], P(ch["desc"]), P(ch["cpl_off"]), P(ch["tld_of"]), 1,
+                                                    P(d["n_of"]), P(d["t_of"]), P(self.ws_aug), P(self.ws_factors),
+                                                    P(self.load), P(d["coupling"]), P(self.ws_aug), P(self.rhs),
+                                                    P(self.action), P(self.corrected), P(self.cell_status), sh),
+                       "mhm_dense_systems_ragged")
             if factor_events is not None:
                 factor_events.append(torch.cuda.Event(enable_timing=True))
                 factor_events[-1].record(st)
