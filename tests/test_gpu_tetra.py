@@ -118,3 +118,19 @@ def test_tetra_preconditioners_agree():
     assert rel(sols["cell"].trace, sols["face"].trace) <= 1e-11
     assert rel(sols["cell"].fields, sols["face"].fields) <= 1e-11
     assert sols["cell"].global_iterations < sols["face"].global_iterations
+
+
+def test_tetra_pivoting_variants_agree():
+    """The windowed-pivot LU (default) and full partial pivoting give the same 3D
+    solution to rounding."""
+    from pymhm_b200.tetra import TetraMesh, TriangularSkeleton
+    from pymhm_b200.tetra_darcy import TetraP1Plan
+    from pymhm_b200.workloads import LayeredField, layered_lognormal_permeability
+
+    mesh = TetraMesh.unit_cube(3)
+    sk = TriangularSkeleton(mesh, 1)
+    field = LayeredField(layered_lognormal_permeability(12, 16, sigma=3.0, ell=0.1, contrast=1e6, seed=31))
+    a = TetraP1Plan(mesh, sk, 4).solve(field, 1.0)
+    b = TetraP1Plan(mesh, sk, 4, lu="partial").solve(field, 1.0)
+    assert rel(a.trace, b.trace) <= 1e-11
+    assert rel(a.fields, b.fields) <= 1e-11
