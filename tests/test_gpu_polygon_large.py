@@ -115,6 +115,32 @@ def test_large_orders_report_contract_failures():
     assert rel(xs[0], np.linalg.solve(good, rhss[0])) <= 1e-10
 
 
+def test_large_orders_odd_and_contract_codes():
+    """Odd orders (701, 999: rows not 16-byte aligned, so the trailing update loads C
+    and L21 directly instead of by bulk copies) match LAPACK; a bordering row orthogonal
+    to the constants makes the system singular (rank test or zero pivot), and a
+    non-finite entry gives the non-finite code."""
+    from pymhm_b200 import _lib
+
+    rng = np.random.default_rng(4103)
+    odd = [bordered_system(rng, 700, 701), bordered_system(rng, 990, 999, contrast=30.0)]
+    sing = bordered_system(rng, 800, 801)
+    c = rng.standard_normal(800)
+    c -= c.mean()  # orthogonal to the constants: [[A, c], [c^T, 0]] is singular
+    sing[:800, 800] = c
+    sing[800, :800] = c
+    nanm = bordered_system(rng, 700, 704)
+    nanm[3, 5] = np.nan
+    mats = odd + [sing, nanm]
+    rhss = [rng.standard_normal((m.shape[0], 6)) for m in mats]
+    xs, status = run_large(mats, rhss)
+    assert status[0] == _lib.CELL_OK and status[1] == _lib.CELL_OK
+    for K, b, x in zip(odd, rhss, xs):
+        assert rel(x, np.linalg.solve(K, b)) <= 1e-10
+    assert status[2] in (_lib.CELL_RANK_DEFICIENT, _lib.CELL_SINGULAR_PIVOT, _lib.CELL_RESIDUAL)
+    assert status[3] == _lib.CELL_NONFINITE
+
+
 def large_polygon_case():
     from pymhm_b200.polygon import EdgeSkeleton, voronoi_mesh
     from pymhm_b200.workloads import DiscInclusions, disc_inclusions
