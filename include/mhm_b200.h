@@ -599,6 +599,51 @@ int mhm_dense_reconstruct(int64_t count, int32_t nb, int32_t w, const int32_t* n
                           const int32_t* cell_id, int64_t trace_size, const double* x,
                           const int64_t* field_off, double* fields, void* stream);
 
+/*
+ * Mixed RT0 / P0 local problems of polygonal macrocells (the "mixed" branch of
+ * _DarcyLocalFactory, _legacy/models/darcy/primal.py:80-103: rt0_operators,
+ * fem/scalar/operators.py:324-364, and normal_flux_blocks, fem/hdiv/mixed.py:77-112).
+ * Local unknowns: the fine faces' fluxes, the fine cells' pressures, the boundary
+ * faces' multipliers.  mhm_rt0_elements writes every fine triangle's saddle block
+ * [[M, -s, S], [-s^T, 0, 0], [S^T, 0, 0]] over the slots (face 0, face 1, face 2,
+ * pressure, multiplier a, multiplier b) in the mhm_p2_elements layout (so that
+ * mhm_p2_assemble_rows builds the dense rows): M_ab = sum_q w_q area
+ * kappa(x_q)^-1 phi_a . phi_b with phi_s = sign_s (x - v_(s+2)%3) / (2 area) (the
+ * triangle's vertices counter-clockwise), the pressure mass (the area) and the load
+ * (-area sum_q w_q source) on the pressure slot.  info (elements, 5): the faces'
+ * signs (+1 / -1) and the local faces (0..2, or -1) selected by the two multiplier
+ * slots.  Permeability as mhm_p2_elements.
+ */
+int mhm_rt0_elements(int64_t elements, const double* points, const int64_t* triangles, const int32_t* info,
+                     int32_t nquad, const double* quad_bary, const double* quad_weights, int32_t grid,
+                     const int32_t* grid_ptr, const int32_t* grid_discs, const double* centres,
+                     const double* radii2, double inside, double outside, double source,
+                     double* element_scratch, void* stream);
+
+/*
+ * mhm_dense_systems, mhm_dense_contributions and mhm_dense_reconstruct for a
+ * declared kernel Z other than the ones vector: kernel (0 / 1 per unknown, in the
+ * load's layout; kernel_fields in the fields' layout).  The systems test A Z and
+ * A^T Z at 1e-10 ||A||_F ||Z||, border with C = M Z / (Z^T M Z) (primal.py:99-100)
+ * and put A Z in the corrected column; the contributions use E = Z - R A Z and
+ * write the blocks and loads negated (the mixed blocks are negative semi-definite;
+ * the negated system has the same solution); reconstruction adds E c_K.
+ */
+int mhm_mixed_systems(int64_t count, int32_t lds, int32_t tld, int32_t nb, int32_t w, const int32_t* n_of,
+                      const int32_t* t_of, const double* matrix, const double* mass, const double* load,
+                      const double* coupling, const double* kernel, double* aug, double* rhs, double* action,
+                      uint8_t* corrected, int32_t* status, void* stream);
+int mhm_mixed_contributions(int64_t count, int32_t lds, int32_t tld, int32_t nb, int32_t w, int32_t max_t,
+                            const int32_t* n_of, const int32_t* t_of, const double* solution,
+                            const double* coupling, const double* action, const double* load,
+                            const double* kernel, const int64_t* block_off, const int64_t* load_off,
+                            double* blocks, double* loads, void* stream);
+int mhm_mixed_reconstruct(int64_t count, int32_t nb, int32_t w, const int32_t* n_of, const int32_t* t_of,
+                          const double* solution, const int64_t* cell_dofs, const int64_t* dof_off,
+                          const int32_t* cell_id, int64_t trace_size, const double* x,
+                          const int64_t* field_off, const double* kernel_fields, double* fields,
+                          void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Reconstruction u_K = R f - (R B) lambda_K + E c_K and flux -K grad u       */
 /* ------------------------------------------------------------------------ */

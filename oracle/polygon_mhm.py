@@ -10,6 +10,12 @@ Test infrastructure only: imported by ``tests/`` and ``bench.py``'s CPU arm, nev
 * driver            ``_legacy/models/darcy/primal.py:28-106, 173-344``
                     (``_DarcyLocalFactory``: kernel 1, constraint M 1 / (1^T M 1),
                     quadrature count max(4, degree + 2), homogeneous Dirichlet data)
+* mixed RT0 / P0  ``fem/scalar/operators.py:324-364`` (``rt0_operators``: the face
+                    basis sign (x - opposite vertex) / (2 area), the inverse
+                    permeability at the Duffy points), ``fem/hdiv/mixed.py:77-112``
+                    (``normal_flux_blocks``), ``primal.py:80-103`` (kernel zero on the
+                    fluxes and one on the pressures and multipliers, constraint the
+                    cell areas over their total, coupling minus the flux map)
 * condensation, contributions, assembly and the global SuperLU solve: the generic
   functions of ``oracle/q1_mhm.py``.
 
@@ -25,7 +31,8 @@ from scipy import sparse
 
 from oracle import q1_mhm as q
 from oracle.tetra_mhm import diffusion_blocks, triangle_quadrature
-from pymhm_b200.polygon import EdgeSkeleton, PolygonMesh, TriangleMesh, p2_nodal_space, p2_trace_coupling
+from pymhm_b200.polygon import (EdgeSkeleton, PolygonMesh, TriangleMesh, p2_nodal_space, p2_trace_coupling,
+                                rt0_coupling)
 
 
 def p1_geometry(mesh: TriangleMesh):
@@ -86,13 +93,62 @@ def local_problem(coarse: PolygonMesh, skeleton: EdgeSkeleton, cell: int, fine: 
     return q.LocalProblem(A, B, f, skeleton.cell_dofs(cell), constraints)
 
 
+def _samples(field, flat, shape):
+    raw = field(flat) if callable(field) else field
+    return np.broadcast_to(np.asarray(raw, dtype=float), (len(flat),)).reshape(shape)
+
+
+def rt0_operators(fine: TriangleMesh, permeability=1.0, source=0.0, order=4):
+    """``rt0_operators`` for a scalar permeability and source: the flux mass (faces x
+    faces, K^-1 weighted), the signed divergence (cells x faces) and the P0 source
+    moments."""
+    bary, weights = triangle_quadrature(order)
+    v = fine.points[fine.cells]
+    physical = np.einsum("qi,tij->tqj", bary, v)
+    flat = physical.reshape(-1, 2)
+    kap = _samples(permeability, flat, physical.shape[:2])
+    areas = fine.areas
+    opposite = v[:, [2, 0, 1]]  # face s runs from vertex s to s + 1
+    basis = (fine.signs[:, None, :, None] * (physical[:, :, None, :] - opposite[:, None, :, :])
+             / (2 * areas)[:, None, None, None])
+    blocks = np.einsum("q,tqia,tq,tqja,t->tij", weights, basis, 1.0 / kap, basis, areas)
+    nf, nt = len(fine.faces), len(fine.cells)
+    mass = sparse.coo_matrix((blocks.ravel(), (np.repeat(fine.cell_faces, 3, axis=1).ravel(),
+                                               np.tile(fine.cell_faces, (1, 3)).ravel())), shape=(nf, nf)).tocsc()
+    divergence = sparse.coo_matrix((fine.signs.ravel().astype(float),
+                                    (np.repeat(np.arange(nt), 3), fine.cell_faces.ravel())), shape=(nt, nf)).tocsc()
+    load = np.sum(_samples(source, flat, physical.shape[:2]) * weights, axis=1) * areas
+    return mass, divergence, load
+
+
+def mixed_local_problem(coarse: PolygonMesh, skeleton: EdgeSkeleton, cell: int, fine: TriangleMesh, permeability,
+                        source):
+    """``_DarcyLocalFactory.__call__``, mixed (``primal.py:80-103``) with
+    ``normal_flux_blocks``: unknowns (fluxes, pressures, boundary multipliers)."""
+    mass, div, force = rt0_operators(fine, permeability, source)
+    nq, npres = len(fine.faces), len(fine.cells)
+    bfaces = fine.boundary_faces
+    nb = len(bfaces)
+    sel = sparse.coo_matrix((np.ones(nb), (bfaces, np.arange(nb))), shape=(nq, nb)).tocsc()
+    zero = sparse.csc_matrix((npres, nb))
+    matrix = sparse.bmat([[mass, -div.T, sel], [-div, None, zero], [sel.T, zero.T, None]], format="csc")
+    load = np.r_[np.zeros(nq), -force, np.zeros(nb)]
+    kernel = np.r_[np.zeros(nq), np.ones(npres + nb)]
+    mean = np.r_[np.zeros(nq), fine.areas, np.zeros(nb)]
+    constraints = (mean / (kernel @ mean))[:, None]
+    return q.LocalProblem(matrix, rt0_coupling(coarse, cell, fine, skeleton), load, skeleton.cell_dofs(cell),
+                          constraints, kernel)
+
+
 def solve_darcy_p2(coarse: PolygonMesh, skeleton: EdgeSkeleton, fines, permeability=1.0, source=0.0,
-                   keep_responses=False):
-    """``solve_darcy`` (``primal.py:173-344``) for degree two, the given local meshes and
+                   keep_responses=False, formulation="primal"):
+    """``solve_darcy`` (``primal.py:173-344``) for degree two (or, ``formulation="mixed"``,
+    RT0 / P0 with its negated boundary load, zero here), the given local meshes and
     homogeneous Dirichlet data.  Returns trace, coarse unknowns and fields per cell."""
+    build = mixed_local_problem if formulation == "mixed" else local_problem
     responses, contribs = [], []
     for cell, fine in enumerate(fines):
-        resp = q.condense(local_problem(coarse, skeleton, cell, fine, permeability, source))
+        resp = q.condense(build(coarse, skeleton, cell, fine, permeability, source))
         contribs.append(q.contribution(resp, skeleton.size + cell))
         responses.append(resp)
     matrix, rhs, scale = q.assemble_global(contribs, skeleton.size, np.zeros(skeleton.size))

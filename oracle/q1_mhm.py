@@ -593,31 +593,36 @@ class EquilibratedLU:
 
 @dataclass
 class LocalProblem:
-    """Cartesian Q1 instance of ``LocalProblem`` (``core/contracts.py:92-211``) with Z=1, C=M 1."""
+    """``LocalProblem`` (``core/contracts.py:92-211``) with one declared kernel vector Z
+    (``kernel``; default the ones vector, the primal problems; the mixed RT0 problems
+    declare zero fluxes and unit pressures) and C = M Z scaled as the driver gives it."""
 
     matrix: sparse.csc_matrix
     coupling: np.ndarray
     load: np.ndarray
     trace_dofs: np.ndarray
     constraints: np.ndarray
+    kernel: np.ndarray | None = None
     action: np.ndarray = field(init=False)
     test_action: np.ndarray = field(init=False)
     corrected: bool = field(init=False)
 
     def __post_init__(self):
         n = self.matrix.shape[0]
-        kernel = np.ones((n, 1))
+        self.kernel = np.ones((n, 1)) if self.kernel is None else np.asarray(self.kernel, dtype=float).reshape(n, 1)
+        kernel = self.kernel
         scale = float(np.max(np.abs(self.matrix.data), initial=0.0))
         if scale:
             normalized = self.matrix.copy()
             normalized.data /= scale
             norm = float(splinalg.norm(normalized))
+            kernel = kernel / np.max(np.abs(kernel), axis=0)
             ref = norm * np.linalg.norm(kernel, axis=0)
             for op in (normalized, normalized.T):
                 if np.any(np.linalg.norm(op @ kernel, axis=0) > 1e-10 * ref):
                     raise ValueError("declared kernel is not a left and right nullspace")
-        self.action = matrix_action(self.matrix, kernel)
-        self.test_action = matrix_action(self.matrix.T, kernel)
+        self.action = matrix_action(self.matrix, self.kernel)
+        self.test_action = matrix_action(self.matrix.T, self.kernel)
         self.corrected = bool(np.any(self.action) or np.any(self.test_action))
 
     def condensation_system(self):
@@ -645,8 +650,7 @@ class LocalResponse:
 
     @property
     def retained(self):
-        n = len(self.source)
-        return np.ones((n, 1)) if self.coarse_vectors is None else self.coarse_vectors
+        return self.problem.kernel if self.coarse_vectors is None else self.coarse_vectors
 
 
 def condense(problem: LocalProblem):
@@ -656,15 +660,14 @@ def condense(problem: LocalProblem):
     n = problem.matrix.shape[0]
     width = problem.coupling.shape[1] + 1
     x = sol[:n]
-    coarse = np.ones((n, 1)) - x[:, width:] if problem.corrected else None
+    coarse = problem.kernel - x[:, width:] if problem.corrected else None
     return LocalResponse(problem, x[:, 0], x[:, 1:width], coarse)
 
 
 def contribution(resp: LocalResponse, coarse_dof: int):
     """``local_global_contribution`` + ``local_condensed_load`` (``contributions.py:14-74``, ``reconstruction.py:91-127``)."""
     p = resp.problem
-    n = len(resp.source)
-    z = np.ones((n, 1))
+    z = p.kernel
     e = resp.retained
     g = p.coupling.T @ e
     if resp.coarse_vectors is None:

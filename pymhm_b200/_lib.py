@@ -145,6 +145,14 @@ _SIGNATURES = {
     "mhm_batched_solve_ragged": (C.c_int, [C.c_int64, P, C.c_int32, C.c_int32, P, P, P, P, P, P, P, C.c_double,
                                            C.c_double, C.c_int32, P, P]),
     "mhm_batched_factor_large": (C.c_int, [C.c_int64, P, C.c_int32, P, P, P, P, P, P, P]),
+    "mhm_rt0_elements": (C.c_int, [C.c_int64, P, P, P, C.c_int32, P, P, C.c_int32, P, P, P, P, C.c_double,
+                                   C.c_double, C.c_double, P, P]),
+    "mhm_mixed_systems": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, P, P, P, P, P, P,
+                                    P, P, P, P, P]),
+    "mhm_mixed_contributions": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P,
+                                          P, P, P, P, P, P, P, P, P, P]),
+    "mhm_mixed_reconstruct": (C.c_int, [C.c_int64, C.c_int32, C.c_int32, P, P, P, P, P, P, C.c_int64, P, P, P, P,
+                                        P]),
     "mhm_dense_systems_ragged": (C.c_int, [C.c_int64, P, P, P, C.c_int32, P, P, P, P, P, P, P, P, P, P, P, P]),
     "mhm_batched_solve_large": (C.c_int, [C.c_int64, P, C.c_int32, C.c_int32, P, P, P, P, P, P, P, P, C.c_double,
                                           C.c_double, C.c_int32, P, P]),

@@ -71,7 +71,10 @@ __global__ void tet_kappa_kernel(int64_t cells, const double* __restrict__ point
 // t = t_of[k] trace columns; its stiffness, mass (rows of lds), load (lds) and
 // coupling (lds x tld) sit at k times their strides; its augmented matrix is nb x nb
 // (nb >= n + 1) and its right-hand sides nb x w (w >= t + 2).  Rows and columns past
-// n + 1 are an identity block with zero right-hand sides (solution zero there).
+// n + 1 are an identity block with zero right-hand sides (solution zero there).  The
+// declared kernel Z is the ones vector, or with kvec a 0/1 vector per cell in the
+// load's layout (the mixed RT0 problems: zero on the fluxes, one on the cell and
+// boundary pressures); the constraint is M Z.
 // ---------------------------------------------------------------------------------
 constexpr int kDThreads = 256;
 constexpr int kTileStride = 33;  // odd: a thread's row of a staged tile spans distinct banks
@@ -89,7 +92,7 @@ __global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
     const double* __restrict__ coupling, double* __restrict__ aug, double* __restrict__ rhs,
     double* __restrict__ action, uint8_t* __restrict__ corrected, int32_t* __restrict__ status,
     const mhm_ragged_matrix* __restrict__ desc, const int64_t* __restrict__ cpl_off,
-    const int32_t* __restrict__ tld_of) {
+    const int32_t* __restrict__ tld_of, const double* __restrict__ kvec) {
   extern __shared__ __align__(16) double tiles[];
   __shared__ double red[32];
   __shared__ int nonzero;
@@ -117,11 +120,12 @@ __global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
   double* act = action + aoff;  // rows: A 1, A^T 1, the constraint
   const double* ldv = load + loff;
   const double* cpl = coupling + coff;
+  const double* zk = kvec ? kvec + loff : nullptr;  // the declared kernel Z (null: ones)
   if (tid == 0) nonzero = 0;
   // max |A| and ||A||_F^2, the retained action A 1 and the test action A^T 1 (double-double
   // sums, the reference's extended-precision _matrix_action), the plain products A 1
   // that the kernel check reads, and the constraint C = M 1
-  double amax = 0.0, fro = 0.0, r2 = 0.0, l2 = 0.0, cmax = 0.0, csum = 0.0;
+  double amax = 0.0, fro = 0.0, r2 = 0.0, l2 = 0.0, cmax = 0.0, csum = 0.0, zsum = 0.0;
   __syncthreads();
   // Thread t owns rows t, t + blockDim, ... and walks each row's columns in ascending
   // order (every sum below keeps that order).  Each warp works alone on 32 of those
@@ -148,12 +152,13 @@ __global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
         for (int q = 0; q < 32; ++q) {
           if (q < jn) {
             const double a = tile[lane0 * kTileStride + q];
+            const double zq = zk ? zk[c0 + q] : 1.0;  // 0 or 1: the products are exact
             amax = fmax(amax, fabs(a));
             fro = fma(a, a, fro);
-            dd_add(hi, lo, a);
-            plain += a;
-            dd_add(chi, clo, colv[q]);
-            cplain += colv[q];
+            dd_add(hi, lo, a * zq);
+            plain += a * zq;
+            dd_add(chi, clo, colv[q] * zq);
+            cplain += colv[q] * zq;
           }
         }
       }
@@ -163,7 +168,7 @@ __global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
         tile[q * kTileStride + lane0] = (r0 + q < n && c0 + lane0 < n) ? Mm[(int64_t)(r0 + q) * lds + c0 + lane0] : 0.0;
       __syncwarp();
       if (i < n)
-        for (int q = 0; q < jn; ++q) c += tile[lane0 * kTileStride + q];
+        for (int q = 0; q < jn; ++q) c += tile[lane0 * kTileStride + q] * (zk ? zk[c0 + q] : 1.0);
       __syncwarp();
     }
     if (i < n) {
@@ -174,7 +179,9 @@ __global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
       r2 = fma(plain, plain, r2);
       l2 = fma(cplain, cplain, l2);
       act[2 * nb + i] = c;
-      csum += c;
+      const double zi = zk ? zk[i] : 1.0;
+      csum += zi * c;
+      zsum += zi * zi;
     }
   }
   amax = block_max(amax, red);
@@ -182,17 +189,17 @@ __global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
   r2 = block_sum(r2, red);
   l2 = block_sum(l2, red);
   csum = block_sum(csum, red);
-  // the 2D primal driver divides the constraint by its total, the cell's area
-  // (primal.py:69-71); the 3D driver keeps M 1 (primal_3d.py:58-65)
+  zsum = block_sum(zsum, red);
+  // the 2D drivers divide the constraint M Z by Z^T M Z, the cell's area (primal.py:
+  // 69-71, 99-100); the 3D driver keeps M 1 (primal_3d.py:58-65)
   const double cdiv = normalize ? csum : 1.0;
   for (int i = tid; i < n; i += blockDim.x) cmax = fmax(cmax, fabs(act[2 * nb + i] / cdiv));
   cmax = block_max(cmax, red);
   __syncthreads();
   const int corr = nonzero;
-  // declared kernel: ||A 1|| and ||A^T 1|| <= 1e-10 ||A||_F sqrt(n) (both scaled by max|A|)
+  // declared kernel: ||A Z|| and ||A^T Z|| <= 1e-10 ||A||_F ||Z|| (both scaled by max|A|)
   int st = MHM_CELL_OK;
-  if (amax > 0.0 && (sqrt(r2) > 1e-10 * sqrt(fro) * sqrt((double)n) ||
-                     sqrt(l2) > 1e-10 * sqrt(fro) * sqrt((double)n)))
+  if (amax > 0.0 && (sqrt(r2) > 1e-10 * sqrt(fro) * sqrt(zsum) || sqrt(l2) > 1e-10 * sqrt(fro) * sqrt(zsum)))
     st = MHM_CELL_KERNEL;
   const double scale = (cmax > 0.0) ? fmin(1.0, (amax > 0.0 ? amax : 1.0) / cmax) : 1.0;
   // the augmented matrix and the right-hand sides, a warp per row (no index division)
@@ -227,16 +234,18 @@ __global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
 
 // ---------------------------------------------------------------------------------
 // Condensation products on the tensor cores.  Per cell one GEMM P = L^T X with
-//   L = [B | A^T 1 | 1]          (n x (t+2): the t trace columns, the test action, ones)
-//   X = [R f | R B | E | 1 | f]  (n x (t+4), E = 1 - R (A 1))
+//   L = [B | A^T Z | Z]          (n x (t+2): the t trace columns, the test action, Z)
+//   X = [R f | R B | E | Z | f]  (n x (t+4), E = Z - R (A Z))
+// (Z the ones vector, or kvec in the load's layout as for the systems)
 // in FP64 mma.sync m8n8k4 tiles over a TILE x TILE output (t + 4 <= TILE), one warp
 // per 8 x 8 output tile over k-steps of 4 rows, operands staged in shared memory.  Then
 //   block[a][b] = P[a][1+b],  block[a][t] = -P[a][t+1]              (B^T lifts, -B^T E)
 //   block[t][b] = -(P[b][t+2] - P[t][1+b]),  block[t][t] = -P[t][t+1]
 //   load[a] = P[a][0],  load[t] = P[t][0] - P[t+1][t+3]
-// (contributions.py:40-47, reconstruction.py:91-127, corrected branch; with A 1 = 0
-// the test action is zero, E = 1 and these are the uncorrected formulas).  The block
-// and load of cell k go to blocks + block_off[k] and loads + load_off[k].
+// (contributions.py:40-47, reconstruction.py:91-127, corrected branch; with A Z = 0
+// the test action is zero, E = Z and these are the uncorrected formulas).  The block
+// and load of cell k, times sgn (1, or -1 for the mixed problems, whose blocks are
+// negative semi-definite), go to blocks + block_off[k] and loads + load_off[k].
 // ---------------------------------------------------------------------------------
 constexpr int kKChunk = 32;
 
@@ -251,7 +260,7 @@ __global__ void __launch_bounds__(TILE * TILE / 2) dense_contrib_kernel(
     int lds, int tld, int nb, int w, const int32_t* __restrict__ n_of, const int32_t* __restrict__ t_of,
     const double* __restrict__ solution, const double* __restrict__ coupling, const double* __restrict__ action,
     const double* __restrict__ load, const int64_t* __restrict__ block_off, const int64_t* __restrict__ load_off,
-    double* __restrict__ blocks, double* __restrict__ loads) {
+    double* __restrict__ blocks, double* __restrict__ loads, const double* __restrict__ kvec, double sgn) {
   constexpr int kTilesPerSide = TILE / 8;
   __shared__ double Ls[kKChunk][TILE + 1];  // L rows (k) x columns (m)
   __shared__ double Xs[kKChunk][TILE + 1];  // X rows (k) x columns (n)
@@ -263,6 +272,7 @@ __global__ void __launch_bounds__(TILE * TILE / 2) dense_contrib_kernel(
   const double* Bm = coupling + cell * (int64_t)lds * tld;
   const double* tact = action + cell * 3 * (int64_t)nb + nb;
   const double* f = load + cell * (int64_t)lds;
+  const double* zk = kvec ? kvec + cell * (int64_t)lds : nullptr;
   const int tm = warp / kTilesPerSide, tn = warp % kTilesPerSide;  // this warp's 8 x 8 output tile
   double d0 = 0.0, d1 = 0.0;
   for (int k0 = 0; k0 < n; k0 += kKChunk) {
@@ -272,14 +282,15 @@ __global__ void __launch_bounds__(TILE * TILE / 2) dense_contrib_kernel(
       const int i = k0 + k;
       double lv = 0.0, xv = 0.0;
       if (i < n) {
+        const double zi = zk ? zk[i] : 1.0;
         if (c < t) lv = Bm[(int64_t)i * tld + c];
         else if (c == t) lv = tact[i];
-        else if (c == t + 1) lv = 1.0;
+        else if (c == t + 1) lv = zi;
         const double* xr = X + (int64_t)i * w;
         if (c == 0) xv = xr[0];
         else if (c <= t) xv = xr[c];
-        else if (c == t + 1) xv = 1.0 - xr[t + 1];
-        else if (c == t + 2) xv = 1.0;
+        else if (c == t + 1) xv = zi - xr[t + 1];
+        else if (c == t + 2) xv = zi;
         else if (c == t + 3) xv = f[i];
       }
       Ls[k][c] = lv;
@@ -312,20 +323,21 @@ __global__ void __launch_bounds__(TILE * TILE / 2) dense_contrib_kernel(
     else if (a < t) v = -Ps[a][t + 1];
     else if (b < t) v = -(Ps[b][t + 2] - Ps[t][1 + b]);
     else v = -Ps[t][t + 1];
-    blk[e] = v;
+    blk[e] = sgn * v;
   }
-  for (int a = tid; a < t1; a += blockDim.x) ld[a] = (a < t) ? Ps[a][0] : Ps[t][0] - Ps[t + 1][t + 3];
+  for (int a = tid; a < t1; a += blockDim.x) ld[a] = sgn * ((a < t) ? Ps[a][0] : Ps[t][0] - Ps[t + 1][t + 3]);
 }
 
 // u = R f - (R B) lambda_K + E c_K, thread per (cell, node i < tile of rows); fields of
 // cell k at fields + field_off[k], its trace DOFs at cell_dofs + dof_off[k], its coarse
-// unknown x[trace_size + cell_id[k]].
+// unknown x[trace_size + cell_id[k]]; E = Z - R (A Z), Z the ones vector or kfield in
+// the fields' layout.
 __global__ void dense_reconstruct_kernel(int64_t cells, int nb, int w, const int32_t* __restrict__ n_of,
                                          const int32_t* __restrict__ t_of, const double* __restrict__ solution,
                                          const int64_t* __restrict__ cell_dofs, const int64_t* __restrict__ dof_off,
                                          const int32_t* __restrict__ cell_id, int64_t trace_size,
                                          const double* __restrict__ x, const int64_t* __restrict__ field_off,
-                                         double* __restrict__ fields) {
+                                         double* __restrict__ fields, const double* __restrict__ kfield) {
   const int64_t total = cells * (int64_t)nb;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < total; id += stride) {
@@ -337,7 +349,8 @@ __global__ void dense_reconstruct_kernel(int64_t cells, int nb, int w, const int
     const int64_t* dofs = cell_dofs + dof_off[cell];
     double u = xr[0];
     for (int b = 0; b < t; ++b) u = fma(-xr[1 + b], x[dofs[b]], u);
-    u = fma(1.0 - xr[t + 1], x[trace_size + cell_id[cell]], u);
+    const double zi = kfield ? kfield[field_off[cell] + i] : 1.0;
+    u = fma(zi - xr[t + 1], x[trace_size + cell_id[cell]], u);
     fields[field_off[cell] + i] = u;
   }
 }
@@ -365,10 +378,11 @@ extern "C" int mhm_tet_kappa(int64_t cells, const double* points, int32_t npoint
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
 
-extern "C" int mhm_dense_systems(int64_t count, int32_t lds, int32_t tld, int32_t nb, int32_t w,
-                                 int32_t normalize, const int32_t* n_of, const int32_t* t_of, const double* stiffness,
-                                 const double* mass, const double* load, const double* coupling, double* aug,
-                                 double* rhs, double* action, uint8_t* corrected, int32_t* status, void* stream) {
+namespace {
+int launch_systems(int64_t count, int32_t lds, int32_t tld, int32_t nb, int32_t w, int32_t normalize,
+                   const int32_t* n_of, const int32_t* t_of, const double* stiffness, const double* mass,
+                   const double* load, const double* coupling, const double* kvec, double* aug, double* rhs,
+                   double* action, uint8_t* corrected, int32_t* status, void* stream) {
   if (count < 1 || count > INT32_MAX || lds < 1 || tld < 1 || nb < 2 || nb > lds + 64 || w < 3 || !n_of ||
       !t_of || !stiffness || !mass || !load || !coupling || !aug || !rhs || !action || !corrected || !status)
     return MHM_ERR_ARGUMENT;
@@ -377,8 +391,59 @@ extern "C" int mhm_dense_systems(int64_t count, int32_t lds, int32_t tld, int32_
     return MHM_ERR_LAUNCH;
   dense_system_kernel<<<(unsigned)count, kDThreads, kSystemSmem, static_cast<cudaStream_t>(stream)>>>(
       lds, tld, nb, w, normalize, n_of, t_of, stiffness, mass, load, coupling, aug, rhs, action, corrected,
-      status, nullptr, nullptr, nullptr);
+      status, nullptr, nullptr, nullptr, kvec);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+int launch_contributions(int64_t count, int32_t lds, int32_t tld, int32_t nb, int32_t w, int32_t max_t,
+                         const int32_t* n_of, const int32_t* t_of, const double* solution, const double* coupling,
+                         const double* action, const double* load, const double* kvec, double sgn,
+                         const int64_t* block_off, const int64_t* load_off, double* blocks, double* loads,
+                         void* stream) {
+  if (count < 1 || count > INT32_MAX || lds < 1 || tld < 1 || nb < 2 || w < 3 || max_t < 1 || max_t > 28 ||
+      !n_of || !t_of || !solution || !coupling || !action || !load || !block_off || !load_off || !blocks ||
+      !loads)
+    return MHM_ERR_ARGUMENT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (max_t + 4 <= 16)
+    dense_contrib_kernel<16><<<(unsigned)count, 128, 0, st>>>(lds, tld, nb, w, n_of, t_of, solution, coupling,
+                                                               action, load, block_off, load_off, blocks, loads,
+                                                               kvec, sgn);
+  else
+    dense_contrib_kernel<32><<<(unsigned)count, 512, 0, st>>>(lds, tld, nb, w, n_of, t_of, solution, coupling,
+                                                               action, load, block_off, load_off, blocks, loads,
+                                                               kvec, sgn);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+int launch_reconstruct(int64_t count, int32_t nb, int32_t w, const int32_t* n_of, const int32_t* t_of,
+                       const double* solution, const int64_t* cell_dofs, const int64_t* dof_off,
+                       const int32_t* cell_id, int64_t trace_size, const double* x, const int64_t* field_off,
+                       const double* kfield, double* fields, void* stream) {
+  if (count < 1 || nb < 2 || w < 3 || trace_size < 1 || !n_of || !t_of || !solution || !cell_dofs || !dof_off ||
+      !cell_id || !x || !field_off || !fields)
+    return MHM_ERR_ARGUMENT;
+  dense_reconstruct_kernel<<<grid_for(count * nb), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      count, nb, w, n_of, t_of, solution, cell_dofs, dof_off, cell_id, trace_size, x, field_off, fields, kfield);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+}  // namespace
+
+extern "C" int mhm_dense_systems(int64_t count, int32_t lds, int32_t tld, int32_t nb, int32_t w,
+                                 int32_t normalize, const int32_t* n_of, const int32_t* t_of, const double* stiffness,
+                                 const double* mass, const double* load, const double* coupling, double* aug,
+                                 double* rhs, double* action, uint8_t* corrected, int32_t* status, void* stream) {
+  return launch_systems(count, lds, tld, nb, w, normalize, n_of, t_of, stiffness, mass, load, coupling, nullptr,
+                        aug, rhs, action, corrected, status, stream);
+}
+
+extern "C" int mhm_mixed_systems(int64_t count, int32_t lds, int32_t tld, int32_t nb, int32_t w,
+                                 const int32_t* n_of, const int32_t* t_of, const double* matrix, const double* mass,
+                                 const double* load, const double* coupling, const double* kernel, double* aug,
+                                 double* rhs, double* action, uint8_t* corrected, int32_t* status, void* stream) {
+  if (!kernel) return MHM_ERR_ARGUMENT;
+  return launch_systems(count, lds, tld, nb, w, 1, n_of, t_of, matrix, mass, load, coupling, kernel, aug, rhs,
+                        action, corrected, status, stream);
 }
 
 extern "C" int mhm_dense_systems_ragged(int64_t count, const mhm_ragged_matrix* desc, const int64_t* cpl_off,
@@ -394,7 +459,7 @@ extern "C" int mhm_dense_systems_ragged(int64_t count, const mhm_ragged_matrix* 
     return MHM_ERR_LAUNCH;
   dense_system_kernel<<<(unsigned)count, kDThreads, kSystemSmem, static_cast<cudaStream_t>(stream)>>>(
       0, 0, 0, 0, normalize, n_of, t_of, stiffness, mass, load, coupling, aug, rhs, action, corrected, status, desc,
-      cpl_off, tld_of);
+      cpl_off, tld_of, nullptr);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }
 
@@ -403,28 +468,34 @@ extern "C" int mhm_dense_contributions(int64_t count, int32_t lds, int32_t tld, 
                                        const double* solution, const double* coupling, const double* action,
                                        const double* load, const int64_t* block_off, const int64_t* load_off,
                                        double* blocks, double* loads, void* stream) {
-  if (count < 1 || count > INT32_MAX || lds < 1 || tld < 1 || nb < 2 || w < 3 || max_t < 1 || max_t > 28 ||
-      !n_of || !t_of || !solution || !coupling || !action || !load || !block_off || !load_off || !blocks ||
-      !loads)
-    return MHM_ERR_ARGUMENT;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (max_t + 4 <= 16)
-    dense_contrib_kernel<16><<<(unsigned)count, 128, 0, st>>>(lds, tld, nb, w, n_of, t_of, solution, coupling,
-                                                               action, load, block_off, load_off, blocks, loads);
-  else
-    dense_contrib_kernel<32><<<(unsigned)count, 512, 0, st>>>(lds, tld, nb, w, n_of, t_of, solution, coupling,
-                                                               action, load, block_off, load_off, blocks, loads);
-  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+  return launch_contributions(count, lds, tld, nb, w, max_t, n_of, t_of, solution, coupling, action, load, nullptr,
+                              1.0, block_off, load_off, blocks, loads, stream);
+}
+
+extern "C" int mhm_mixed_contributions(int64_t count, int32_t lds, int32_t tld, int32_t nb, int32_t w,
+                                       int32_t max_t, const int32_t* n_of, const int32_t* t_of,
+                                       const double* solution, const double* coupling, const double* action,
+                                       const double* load, const double* kernel, const int64_t* block_off,
+                                       const int64_t* load_off, double* blocks, double* loads, void* stream) {
+  if (!kernel) return MHM_ERR_ARGUMENT;
+  return launch_contributions(count, lds, tld, nb, w, max_t, n_of, t_of, solution, coupling, action, load, kernel,
+                              -1.0, block_off, load_off, blocks, loads, stream);
 }
 
 extern "C" int mhm_dense_reconstruct(int64_t count, int32_t nb, int32_t w, const int32_t* n_of,
                                      const int32_t* t_of, const double* solution, const int64_t* cell_dofs,
                                      const int64_t* dof_off, const int32_t* cell_id, int64_t trace_size,
                                      const double* x, const int64_t* field_off, double* fields, void* stream) {
-  if (count < 1 || nb < 2 || w < 3 || trace_size < 1 || !n_of || !t_of || !solution || !cell_dofs || !dof_off ||
-      !cell_id || !x || !field_off || !fields)
-    return MHM_ERR_ARGUMENT;
-  dense_reconstruct_kernel<<<grid_for(count * nb), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      count, nb, w, n_of, t_of, solution, cell_dofs, dof_off, cell_id, trace_size, x, field_off, fields);
-  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+  return launch_reconstruct(count, nb, w, n_of, t_of, solution, cell_dofs, dof_off, cell_id, trace_size, x,
+                            field_off, nullptr, fields, stream);
+}
+
+extern "C" int mhm_mixed_reconstruct(int64_t count, int32_t nb, int32_t w, const int32_t* n_of,
+                                     const int32_t* t_of, const double* solution, const int64_t* cell_dofs,
+                                     const int64_t* dof_off, const int32_t* cell_id, int64_t trace_size,
+                                     const double* x, const int64_t* field_off, const double* kernel_fields,
+                                     double* fields, void* stream) {
+  if (!kernel_fields) return MHM_ERR_ARGUMENT;
+  return launch_reconstruct(count, nb, w, n_of, t_of, solution, cell_dofs, dof_off, cell_id, trace_size, x,
+                            field_off, kernel_fields, fields, stream);
 }

@@ -1,4 +1,5 @@
-// P2 triangle local operators of polygonal macrocells (config 3), dense per cell.
+// P2 triangle local operators of polygonal macrocells (config 3), dense per cell, and
+// the mixed RT0 / P0 local saddles of the same cells (rt0_element_kernel).
 //
 // Reference (PyMHM 1.3.2, src/pymhm/): scalar_operators (fem/scalar/triangle.py:
 // 208-257) with the Duffy rule triangle_quadrature (fem/scalar/operators.py:63-69),
@@ -102,6 +103,73 @@ __global__ void p2_element_kernel(int64_t elements, const double* __restrict__ p
         out[36 + i * 6 + j] = out[36 + j * 6 + i] = Mm[k];
       }
     for (int i = 0; i < 6; ++i) out[72 + i] = F[i];
+  }
+}
+
+// Mixed RT0 / P0 elements (rt0_operators, fem/scalar/operators.py:324-364, and the
+// saddle of normal_flux_blocks, fem/hdiv/mixed.py:77-112), one thread per fine
+// triangle, written in the P2 element layout so that p2_dense_kernel builds the dense
+// rows: local slots (face 0, face 1, face 2, cell pressure, boundary multiplier a,
+// boundary multiplier b).  The face basis is sign_s (x - v_(s+2)%3) / (2 area) (the
+// triangle's vertices counter-clockwise, face s from vertex s to s + 1); the first 36
+// entries hold [[M, -s, S], [-s^T, 0, 0], [S^T, 0, 0]] with
+// M_ab = sum_q w_q area kappa(x_q)^-1 phi_a(x_q).phi_b(x_q) and S the 0/1 selector of
+// the faces that info[3], info[4] name (-1: a padding slot, all zero); the next 36 the
+// pressure mass (the area on the pressure slot) and the last 6 the load, -area sum_q
+// w_q f on the pressure slot.  info (elements, 5): the three signs, the two selected
+// local faces.
+__global__ void rt0_element_kernel(int64_t elements, const double* __restrict__ points,
+                                   const int64_t* __restrict__ tri, const int32_t* __restrict__ info, int nquad,
+                                   const double* __restrict__ qbary, const double* __restrict__ qw, int grid,
+                                   const int32_t* __restrict__ gptr, const int32_t* __restrict__ glist,
+                                   const double* __restrict__ centres, const double* __restrict__ r2, double inside,
+                                   double outside, double source, double* __restrict__ elem) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < elements; e += stride) {
+    double p[3][2];
+    for (int v = 0; v < 3; ++v) {
+      const int64_t id = tri[3 * e + v];
+      p[v][0] = points[2 * id];
+      p[v][1] = points[2 * id + 1];
+    }
+    const double a0 = p[1][0] - p[0][0], a1 = p[1][1] - p[0][1];
+    const double b0 = p[2][0] - p[0][0], b1 = p[2][1] - p[0][1];
+    const double area = __dmul_rn(__dadd_rn(__dmul_rn(a0, b1), -__dmul_rn(a1, b0)), 0.5);
+    const int32_t* in = info + 5 * e;
+    const double sg[3] = {(double)in[0], (double)in[1], (double)in[2]};
+    const double inv2a = 1.0 / (2.0 * area);
+    double Mf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // (0,0) (1,0) (1,1) (2,0) (2,1) (2,2)
+    double fsum = 0.0;
+    for (int q = 0; q < nquad; ++q) {
+      const double l0 = qbary[3 * q], l1 = qbary[3 * q + 1], l2 = qbary[3 * q + 2];
+      double xq[2];
+      for (int j = 0; j < 2; ++j)
+        xq[j] = __dadd_rn(__dadd_rn(__dmul_rn(l0, p[0][j]), __dmul_rn(l1, p[1][j])), __dmul_rn(l2, p[2][j]));
+      const double kap = disc_value(xq[0], xq[1], grid, gptr, glist, centres, r2, inside, outside);
+      double phi[3][2];
+      for (int f = 0; f < 3; ++f) {
+        const int opp = (f + 2) % 3;
+        phi[f][0] = sg[f] * (xq[0] - p[opp][0]) * inv2a;
+        phi[f][1] = sg[f] * (xq[1] - p[opp][1]) * inv2a;
+      }
+      const double wk = qw[q] * area / kap;
+      int k = 0;
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j <= i; ++j, ++k) Mf[k] = fma(wk, phi[i][0] * phi[j][0] + phi[i][1] * phi[j][1], Mf[k]);
+      fsum = fma(source, qw[q], fsum);
+    }
+    double* out = elem + e * kElemStride;
+    for (int k = 0; k < kElemStride; ++k) out[k] = 0.0;
+    int k = 0;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j <= i; ++j, ++k) out[i * 6 + j] = out[j * 6 + i] = Mf[k];
+    for (int f = 0; f < 3; ++f) {
+      out[f * 6 + 3] = out[3 * 6 + f] = -sg[f];
+      for (int m = 0; m < 2; ++m)
+        if (in[3 + m] == f) out[f * 6 + 4 + m] = out[(4 + m) * 6 + f] = 1.0;
+    }
+    out[36 + 3 * 6 + 3] = area;
+    out[72 + 3] = -(fsum * area);
   }
 }
 
@@ -239,5 +307,20 @@ extern "C" int mhm_p2_assemble_rows(int64_t nodes, const int32_t* node_cell, con
   p2_dense_kernel<<<(unsigned)dblocks, kDenseWarps * 32, smem, static_cast<cudaStream_t>(stream)>>>(
       nodes, node_cell, node_row, inc_ptr, inc, elem_dofs, element_scratch, dense_off, ld_of, load_off, stiffness,
       mass, load);
+  return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
+}
+
+extern "C" int mhm_rt0_elements(int64_t elements, const double* points, const int64_t* triangles,
+                                const int32_t* info, int32_t nquad, const double* quad_bary,
+                                const double* quad_weights, int32_t grid, const int32_t* grid_ptr,
+                                const int32_t* grid_discs, const double* centres, const double* radii2, double inside,
+                                double outside, double source, double* element_scratch, void* stream) {
+  if (elements < 1 || nquad < 1 || grid < 0 || !points || !triangles || !info || !quad_bary || !quad_weights ||
+      (grid > 0 && (!grid_ptr || !grid_discs || !centres || !radii2)) || !element_scratch || !(inside > 0) ||
+      !(outside > 0))
+    return MHM_ERR_ARGUMENT;
+  rt0_element_kernel<<<blocks_for(elements), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      elements, points, triangles, info, nquad, quad_bary, quad_weights, grid, grid_ptr, grid_discs, centres, radii2,
+      inside, outside, source, element_scratch);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
 }

@@ -315,18 +315,116 @@ def p2_trace_coupling(coarse: PolygonMesh, cell: int, fine: TriangleMesh, skelet
     return matrix
 
 
-def _cell_local_data(args):
-    """Worker of ``local_data``: (fine mesh, P2 nodal space, trace coupling) per cell."""
-    coarse, skeleton, cells, refinements = args
-    out = []
-    for c, r in zip(cells, refinements):
-        fine = coarse.submesh(int(c), int(r))
-        out.append((fine, p2_nodal_space(fine), p2_trace_coupling(coarse, int(c), fine, skeleton)))
+def rt0_space(fine: TriangleMesh):
+    """Unknowns of the mixed RT0 / P0 local problem (``normal_flux_blocks``,
+    ``fem/hdiv/mixed.py:77-112``: the fine faces' fluxes, the fine cells' pressures, the
+    boundary faces' multipliers in ``fine.boundary_faces`` order) and every fine
+    triangle's six element slots (its three faces, its pressure, two multipliers).
+
+    Returns ``(slots, valid, info, kernel)``: slots (triangles, 6) local unknowns;
+    valid marks the slots that hold the triangle's own unknowns (a triangle's boundary
+    faces select their multipliers; the other multiplier slots name distinct
+    multipliers with zero entries); info (triangles, 5) the faces' signs and the local
+    faces the two multiplier slots select (-1 for none); kernel the declared kernel Z
+    (zero fluxes, unit pressures and multipliers)."""
+    nq, npres = len(fine.faces), len(fine.cells)
+    bfaces = fine.boundary_faces
+    nb = len(bfaces)
+    where = np.full(nq, -1, dtype=np.int64)
+    where[bfaces] = np.arange(nb)
+    slots = np.empty((npres, 6), dtype=np.int64)
+    valid = np.ones((npres, 6), dtype=bool)
+    info = np.full((npres, 5), -1, dtype=np.int32)
+    slots[:, :3] = fine.cell_faces
+    slots[:, 3] = nq + np.arange(npres)
+    info[:, :3] = fine.signs
+    for t in range(npres):
+        own = [(s, int(where[f])) for s, f in enumerate(fine.cell_faces[t]) if where[f] >= 0]
+        if len(own) > 2:
+            raise NotImplementedError("a fine triangle with three boundary faces (a one-triangle local mesh)")
+        taken = {k for _, k in own}
+        spare = (k for k in range(nb) if k not in taken)
+        for m in range(2):
+            if m < len(own):
+                info[t, 3 + m] = own[m][0]
+                slots[t, 4 + m] = nq + npres + own[m][1]
+            else:
+                valid[t, 4 + m] = False
+                slots[t, 4 + m] = nq + npres + next(spare)
+    kernel = np.r_[np.zeros(nq), np.ones(npres + nb)]
+    return slots, valid, info, kernel
+
+
+def rt0_flux_map(coarse: PolygonMesh, cell: int, fine: TriangleMesh, skeleton: EdgeSkeleton) -> np.ndarray:
+    """The RT0 half of ``face_integration`` (``fem/scalar/operators.py:200-244``): per fine
+    boundary face (rows in ``fine.boundary_faces`` order) lying on a macro edge, the
+    integrated outward flux of each trace mode, sign * length * Gauss sum of the modes
+    on the face's parameter interval split at the space's breaks."""
+    from numpy.polynomial.legendre import leggauss
+
+    space = skeleton.space
+    bfaces = fine.boundary_faces
+    rt = np.zeros((len(bfaces), skeleton.modes * len(coarse.cell_faces[cell])))
+    gauss, gw = leggauss(max(space.degrees) + 2)
+    for side, face in enumerate(coarse.cell_faces[cell]):
+        start, end = coarse.points[coarse.faces[face]]
+        tangent = end - start
+        length2 = tangent @ tangent
+        sign = coarse.signs[cell][side]
+        cols = slice(side * skeleton.modes, (side + 1) * skeleton.modes)
+        for row, ff in enumerate(bfaces):
+            coords = fine.points[fine.faces[ff]]
+            t = (coords - start) @ tangent / length2
+            if (not np.allclose(coords, start + t[:, None] * tangent, atol=1e-12, rtol=1e-12)
+                    or min(t) < -1e-12 or max(t) > 1 + 1e-12):
+                continue
+            lo, hi = np.clip(np.sort(t), 0, 1)
+            cuts = sorted({lo, hi, *(b for b in space.breaks if lo < b < hi)})
+            for left, right in zip(cuts[:-1], cuts[1:]):
+                param = left + (gauss + 1) * (right - left) / 2
+                w = gw * (right - left) / 2 * np.sqrt(length2) * sign
+                rt[row, cols] += w @ space.evaluate(param)
+    return rt
+
+
+def rt0_coupling(coarse: PolygonMesh, cell: int, fine: TriangleMesh, skeleton: EdgeSkeleton) -> np.ndarray:
+    """The mixed coupling of ``normal_flux_blocks``: minus the flux map on the boundary
+    multipliers' rows, zero on the fluxes and pressures."""
+    rt = rt0_flux_map(coarse, cell, fine, skeleton)
+    out = np.zeros((len(fine.faces) + len(fine.cells) + rt.shape[0], rt.shape[1]))
+    out[len(fine.faces) + len(fine.cells):] = -rt
     return out
 
 
-def local_data(coarse: PolygonMesh, skeleton: EdgeSkeleton, refinements, workers: int = 1):
-    """Every cell's refined local mesh, P2 nodal space and trace coupling (host work of a
+def check_rt0_skeleton(skeleton: EdgeSkeleton, refinements) -> None:
+    """``_DarcyLocalFactory``'s RT0 condition (``primal.py:81-90``): degree-zero trace
+    segments whose breaks fall on the fine edges of every cell's refinement."""
+    space = skeleton.space
+    if any(space.degrees):
+        raise ValueError("RT0 needs degree-zero trace segments aligned with fine edges")
+    for r in np.unique(np.asarray(refinements, dtype=np.int64)):
+        b = np.array(space.breaks) * r
+        if not np.allclose(b, np.round(b), atol=1e-12, rtol=0):
+            raise ValueError("RT0 needs degree-zero trace segments aligned with fine edges")
+
+
+def _cell_local_data(args):
+    """Worker of ``local_data``: (fine mesh, local space, trace coupling) per cell."""
+    coarse, skeleton, cells, refinements, formulation = args
+    out = []
+    for c, r in zip(cells, refinements):
+        fine = coarse.submesh(int(c), int(r))
+        if formulation == "mixed":
+            out.append((fine, rt0_space(fine), rt0_coupling(coarse, int(c), fine, skeleton)))
+        else:
+            out.append((fine, p2_nodal_space(fine), p2_trace_coupling(coarse, int(c), fine, skeleton)))
+    return out
+
+
+def local_data(coarse: PolygonMesh, skeleton: EdgeSkeleton, refinements, workers: int = 1,
+               formulation: str = "primal"):
+    """Every cell's refined local mesh, local space (P2 nodes, or the RT0 / P0 slots of
+    ``rt0_space`` for ``formulation="mixed"``) and trace coupling (host work of a
     polygon plan, independent per cell).  With ``workers`` > 1, batches of a few hundred
     cells and more are split over that many spawned processes (the same functions, so
     the same results); spawned children import the calling program's main module, so a
@@ -335,11 +433,11 @@ def local_data(coarse: PolygonMesh, skeleton: EdgeSkeleton, refinements, workers
     M = len(coarse.cells)
     rs = np.broadcast_to(np.asarray(refinements, dtype=np.int64), (M,))
     if M < 256 or workers < 2:
-        return _cell_local_data((coarse, skeleton, range(M), rs))
+        return _cell_local_data((coarse, skeleton, range(M), rs, formulation))
     import multiprocessing
     from concurrent.futures import ProcessPoolExecutor
 
     parts = [p for p in np.array_split(np.arange(M), 4 * workers) if len(p)]
     with ProcessPoolExecutor(workers, mp_context=multiprocessing.get_context("spawn")) as pool:
-        done = pool.map(_cell_local_data, [(coarse, skeleton, p, rs[p]) for p in parts])
+        done = pool.map(_cell_local_data, [(coarse, skeleton, p, rs[p], formulation) for p in parts])
         return [item for part in done for item in part]

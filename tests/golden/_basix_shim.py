@@ -20,6 +20,14 @@ Lagrange basis on triangles and tetrahedra (barycentric coordinates).
 The tetrahedral fixtures (``make_tetra_golden.py``) need the Bernstein basis of the
 triangular skeleton faces too.
 
+The mixed RT0 fixtures (``make_polygon_rt0_golden.py``) need a basis of the lowest
+Raviart-Thomas space on the reference triangle (``vector_tabulation("RT", "triangle",
+1, ...)``, ``src/pymhm/fem/hdiv/reference.py:18-37``).  The reference turns whatever
+candidate basis it gets into its canonical face-moment basis by exact moments
+(``rt_moment_coefficients``, ``src/pymhm/fem/hdiv/rt.py:64-88``), so any basis of
+RT0 = {a + b x} gives the same result up to rounding: here (x, y), (x - 1, y),
+(x, y - 1), each of divergence 2.
+
 All are restated here from their published mathematics: the nodal Lagrange
 basis on the declared node order (unique polynomial interpolant, obtained by a
 Legendre-Vandermonde solve) with exact Kronecker rows at literal nodes, as the
@@ -164,6 +172,19 @@ def bernstein_tabulation(points, exponents):
     return vals, grads
 
 
+def vector_tabulation(family, cell, degree, points):
+    """Values (points, 3, 2) and divergence (points, 3) of a basis of RT0 on the
+    reference triangle (see the module docstring); other spaces are not covered."""
+    if (family, cell, int(degree)) != ("RT", "triangle", 1):
+        raise NotImplementedError("the fixture shim covers the lowest Raviart-Thomas space on triangles")
+    x = np.asarray(points, dtype=float)
+    vals = np.empty((len(x), 3, 2))
+    for k, shift in enumerate(((0.0, 0.0), (1.0, 0.0), (0.0, 1.0))):
+        vals[:, k, 0] = x[:, 0] - shift[0]
+        vals[:, k, 1] = x[:, 1] - shift[1]
+    return vals, np.full((len(x), 3), 2.0)
+
+
 def install():
     """Patch the reference modules in place (idempotent)."""
     import pymhm.fem.reference as ref
@@ -174,3 +195,8 @@ def install():
     ref.legendre_values = legendre_values
     ref.bernstein_tabulation = bernstein_tabulation
     quad.simplex_lagrange_tabulation = simplex_lagrange_tabulation
+    import pymhm.fem.hdiv.rt as rt
+
+    rt.vector_tabulation = vector_tabulation
+    rt.legendre_values = legendre_values
+    rt.rt_moment_coefficients.cache_clear()
