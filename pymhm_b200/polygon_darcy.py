@@ -1,4 +1,4 @@
-"""Primal P2 Darcy on polygonal macro meshes (config 3), on the GPU.
+"""Primal P2 (and mixed RT0 / P0) Darcy on polygonal macro meshes (config 3), on the GPU.
 
 GPU counterpart of ``solve_darcy`` (PyMHM 1.3.2, ``src/pymhm/_legacy/models/darcy/
 primal.py:173-344``) for degree-two local spaces on every macrocell's own refinement
@@ -19,6 +19,12 @@ cells padded with an identity block (their solution is zero there).  One solve:
 Cells above augmented order 640 (the large tier) take, per workspace chunk,
 ``mhm_p2_assemble_rows``, ``mhm_dense_systems_ragged``, ``mhm_batched_factor_large``
 and ``mhm_batched_solve_large`` in step 2.
+
+The mixed formulation (``formulation="mixed"``) replaces step 1 by ``mhm_rt0_elements``
+and ``mhm_p2_assemble_rows`` and the dense calls by ``mhm_mixed_systems``,
+``mhm_mixed_contributions`` and ``mhm_mixed_reconstruct`` (declared kernel zero on the
+fluxes; blocks and loads negated, which leaves the solution unchanged and the trace
+block positive semi-definite for the global PCG).
 """
 
 from __future__ import annotations
@@ -31,7 +37,7 @@ import numpy as np
 from . import _lib
 from .errors import LinearSolveError
 from .general import GeneralSkeleton
-from .polygon import EdgeSkeleton, PolygonMesh, local_data, p2_nodal_space
+from .polygon import EdgeSkeleton, PolygonMesh, check_rt0_skeleton, local_data, p2_nodal_space
 from .topology import block_offsets, skeleton_pattern_ragged, transpose_slots
 from .workloads import DiscInclusions
 
@@ -110,11 +116,19 @@ class PolygonP2Plan:
     ``workspace_bytes`` (default: the smaller of 112 GiB and 60 % of free device
     memory) in chunks, largest first, factored by the windowed-pivot LU in HBM.
     ``workers`` spawned processes build the cells' local meshes and couplings on the
-    host (1: in this process)."""
+    host (1: in this process).
+
+    ``formulation="mixed"`` condenses the mixed RT0 / P0 local problems of the same
+    cells instead (``_DarcyLocalFactory``'s mixed branch, ``primal.py:80-103``: fine-face
+    fluxes, fine-cell pressures and boundary multipliers, the declared kernel zero on
+    the fluxes and one on the rest, the skeleton a degree-zero ``FaceSpace`` aligned
+    with every cell's fine edges); its saddle systems take the small tier only (order
+    up to 639, full partial pivoting)."""
 
     def __init__(self, mesh: PolygonMesh, skeleton: EdgeSkeleton | None = None, refinements=2, *, order=4,
                  bin_width=32, streams=4, ragged=True, device=None, global_rtol=1e-13, inner_rtol=1e-10,
-                 max_inner=20000, max_outer=16, preconditioner="cell", workspace_bytes=None, workers=1):
+                 max_inner=20000, max_outer=16, preconditioner="cell", workspace_bytes=None, workers=1,
+                 formulation="primal"):
         import torch
 
         self.torch = torch
@@ -127,19 +141,26 @@ class PolygonP2Plan:
         if preconditioner not in ("cell", "face"):
             raise ValueError("preconditioner must be 'cell' (the cells' D S^-1 D) or 'face' (face blocks)")
         self.preconditioner = preconditioner
+        if formulation not in ("primal", "mixed"):
+            raise ValueError("formulation must be 'primal' or 'mixed'")
+        self.mixed = formulation == "mixed"
         M = len(mesh.cells)
         self.M = M
         rs = np.broadcast_to(np.asarray(refinements, dtype=np.int64), (M,))
         sk = self.skeleton
+        if self.mixed:
+            check_rt0_skeleton(sk, rs)
         self.T, self.N = sk.size, sk.size + M
-        data = local_data(mesh, sk, rs, workers=int(workers))
+        data = local_data(mesh, sk, rs, workers=int(workers), formulation=formulation)
         fines = [f for f, _, _ in data]
         spaces = [sp for _, sp, _ in data]
-        self.n_cells = np.array([len(nodes) for _, nodes in spaces], dtype=np.int64)
+        self.n_cells = np.array([len(sp[-1]) for sp in spaces], dtype=np.int64)
         cell_dofs = [sk.cell_dofs(c) for c in range(M)]
         self.t_cells = np.array([len(d) for d in cell_dofs], dtype=np.int64)
         if self.n_cells.max() + 1 > LARGE_MAX:
             raise NotImplementedError(f"local P2 spaces up to {LARGE_MAX - 1} unknowns on this path")
+        if self.mixed and self.n_cells.max() + 1 > MAX_AUGMENTED:
+            raise NotImplementedError(f"mixed local problems up to {MAX_AUGMENTED - 1} unknowns on this path")
         # Cells whose augmented systems exceed the small tier's order are condensed in
         # chunks: their dense matrices share one workspace (two halves: the augmented
         # matrix, assembled in place over the stiffness, and the factors, which first
@@ -211,6 +232,7 @@ class PolygonP2Plan:
             pos += k
         # ---- flattened elements and node incidences (cells in bin order) -------------
         pts, tris, edofs, node_cell, node_row, inc_ptr, incs = [], [], [], [], [], [0], []
+        rt_info, kvec_parts, kfield_parts = [], [], []
         dense_off = np.empty(M, dtype=np.int64)
         load_off = np.empty(M, dtype=np.int64)
         ld_of = np.empty(M, dtype=np.int32)
@@ -218,7 +240,8 @@ class PolygonP2Plan:
         for b in self.bins:
             for j, c in enumerate(b["cells"]):
                 fine = fines[c]
-                dofs, _ = spaces[c]
+                dofs = spaces[c][0]
+                valid = spaces[c][1] if self.mixed else np.ones(dofs.shape, dtype=bool)
                 slot = b["pos"] + j
                 dense_off[slot] = b["dense"] + j * b["nb"] * b["nb"]  # large tier: set per chunk below
                 load_off[slot] = b["load"] + j * b["nb"]
@@ -227,11 +250,16 @@ class PolygonP2Plan:
                 tris.append(fine.cells + p_base)
                 edofs.append(dofs.astype(np.int32))
                 n = int(self.n_cells[c])
-                flat = dofs.ravel()
-                code = (e_base + np.arange(len(dofs)))[:, None] * 6 + np.arange(6)[None, :]
-                srt = np.lexsort((code.ravel(), flat))
+                flat = dofs[valid]
+                code = ((e_base + np.arange(len(dofs)))[:, None] * 6 + np.arange(6)[None, :])[valid]
+                srt = np.lexsort((code, flat))
                 counts = np.bincount(flat, minlength=n)
-                incs.append(code.ravel()[srt])
+                incs.append(code[srt])
+                if self.mixed:
+                    rt_info.append(spaces[c][2])
+                    z = spaces[c][3]
+                    kvec_parts.append(np.r_[z, np.zeros(b["nb"] - n)])
+                    kfield_parts.append((c, z))
                 inc_ptr.extend((inc_ptr[-1] + np.cumsum(counts)).tolist())
                 node_cell.append(np.full(n, slot, dtype=np.int32))
                 node_row.append(np.arange(n, dtype=np.int32))
@@ -311,6 +339,15 @@ class PolygonP2Plan:
             slot_ptr=up(self.pattern.slot_ptr, torch.int64), contrib=up(self.pattern.contrib, torch.int64),
             load_ptr=up(self.pattern.load_ptr, torch.int64), load_contrib=up(self.pattern.load_contrib, torch.int64),
             indptr=up(self.pattern.indptr, torch.int64), indices=up(self.pattern.indices, torch.int32))
+        if self.mixed:
+            # the declared kernels: in the load's layout (bin order, padded to each
+            # bin's order) and in the fields' layout (cell order)
+            self.d["rt_info"] = up(np.concatenate(rt_info), torch.int32)
+            self.d["kvec"] = up(np.concatenate(kvec_parts), torch.float64)
+            kf = np.empty(self.nodes)
+            for c, z in kfield_parts:
+                kf[self.field_off_h[c]: self.field_off_h[c + 1]] = z
+            self.d["kfield"] = up(kf, torch.float64)
         cpl = np.zeros(cpl_base)
         for b in self.bins:
             for j, c in enumerate(b["cells"]):
@@ -433,6 +470,7 @@ class PolygonP2Plan:
             aug=None if dense is None else self.aug[dense],
             factors=None if dense is None else self.factors[dense],
             load=self.load[b["load"]: b["load"] + k * nb],
+            kvec=self.d["kvec"][b["load"]: b["load"] + k * nb] if self.mixed else None,
             coupling=d["coupling"][b["cpl"]: b["cpl"] + k * nb * tld],
             rhs=self.rhs[b["rhs"]: b["rhs"] + k * nb * w], solution=self.solution[b["rhs"]: b["rhs"] + k * nb * w],
             work=self.work[b["rhs"]: b["rhs"] + k * nb * w], action=self.action[b["act"]: b["act"] + k * 3 * nb],
@@ -457,7 +495,13 @@ class PolygonP2Plan:
                 events[k].record(st)
 
         mark(0)
-        if not self.chunks:
+        if self.mixed:
+            _lib.check(lib.mhm_rt0_elements(self.elements, P(d["points"]), P(d["tris"]), P(d["rt_info"]), len(d["qw"]),
+                                            P(d["qbary"]), P(d["qw"]), fld["grid"], P(fld["ptr"]), P(fld["flat"]),
+                                            P(fld["centres"]), P(fld["r2"]), fld["inside"], fld["outside"],
+                                            self.source, P(self.elem), sh), "mhm_rt0_elements")
+            self._assemble_rows(0, self.nodes, self.stiffness, self.mass, sh)
+        elif not self.chunks:
             _lib.check(lib.mhm_p2_assemble(self.elements, P(d["points"]), P(d["tris"]), len(d["qw"]), P(d["qbary"]),
                                            P(d["qw"]), fld["grid"], P(fld["ptr"]), P(fld["flat"]), P(fld["centres"]),
                                            P(fld["r2"]), fld["inside"], fld["outside"], self.source, P(self.elem),
@@ -496,6 +540,13 @@ class PolygonP2Plan:
                 st.wait_event(join)
 
         def systems(b, v, bs, shb):
+            if self.mixed:
+                _lib.check(lib.mhm_mixed_systems(b["k"], b["nb"], b["tld"], b["nb"], b["w"], P(v["n_of"]),
+                                                 P(v["t_of"]), P(v["stiffness"]), P(v["mass"]), P(v["load"]),
+                                                 P(v["coupling"]), P(v["kvec"]), P(v["aug"]), P(v["rhs"]),
+                                                 P(v["action"]), P(v["corrected"]), P(v["cell_status"]), shb),
+                           "mhm_mixed_systems")
+                return
             _lib.check(lib.mhm_dense_systems(b["k"], b["nb"], b["tld"], b["nb"], b["w"], 1, P(v["n_of"]), P(v["t_of"]),
                                              P(v["stiffness"]), P(v["mass"]), P(v["load"]), P(v["coupling"]),
                                              P(v["aug"]), P(v["rhs"]), P(v["action"]), P(v["corrected"]),
@@ -512,6 +563,13 @@ class PolygonP2Plan:
                                              2, P(v["solve_status"]), shb), "mhm_batched_solve")
 
         def contributions(b, v, bs, shb):
+            if self.mixed:
+                _lib.check(lib.mhm_mixed_contributions(b["k"], b["nb"], b["tld"], b["nb"], b["w"], b["tld"],
+                                                       P(v["n_of"]), P(v["t_of"]), P(v["solution"]),
+                                                       P(v["coupling"]), P(v["action"]), P(v["load"]), P(v["kvec"]),
+                                                       P(v["block_off"]), P(v["lofs"]), P(self.blocks),
+                                                       P(self.loads), shb), "mhm_mixed_contributions")
+                return
             _lib.check(lib.mhm_dense_contributions(b["k"], b["nb"], b["tld"], b["nb"], b["w"], b["tld"],
                                                    P(v["n_of"]), P(v["t_of"]), P(v["solution"]), P(v["coupling"]),
                                                    P(v["action"]), P(v["load"]), P(v["block_off"]), P(v["lofs"]),
@@ -556,6 +614,12 @@ class PolygonP2Plan:
         mark(3)
         for b in self.bins:
             v = self._bin_views(b)
+            if self.mixed:
+                _lib.check(lib.mhm_mixed_reconstruct(b["k"], b["nb"], b["w"], P(v["n_of"]), P(v["t_of"]),
+                                                     P(v["solution"]), P(d["flat_dofs"]), P(v["dof_off"]),
+                                                     P(v["cell_id"]), self.T, P(self.x), P(v["field_off"]),
+                                                     P(d["kfield"]), P(self.fields), sh), "mhm_mixed_reconstruct")
+                continue
             _lib.check(lib.mhm_dense_reconstruct(b["k"], b["nb"], b["w"], P(v["n_of"]), P(v["t_of"]),
                                                  P(v["solution"]), P(d["flat_dofs"]), P(v["dof_off"]),
                                                  P(v["cell_id"]), self.T, P(self.x), P(v["field_off"]),
@@ -674,14 +738,25 @@ def solve_darcy(mesh: PolygonMesh, *, permeability=1.0, source=0.0, dirichlet=0.
                 skeleton: EdgeSkeleton | None = None, local_refinement=4, local_meshes=None, quadrature_order=4,
                 formulation="primal", degree=1, **_ignored) -> PolygonSolution:
     """GPU counterpart of ``solve_darcy`` (``primal.py:173-344``) on a ``PolygonMesh`` for
-    ``degree=2``, homogeneous Dirichlet data, a constant source and a constant or
-    ``DiscInclusions`` permeability.  ``local_refinement`` may be one count or one per
-    cell (the uneven local sizes of a polygon batch)."""
-    if int(degree) != 2 or formulation != "primal":
+    the primal ``degree=2`` or the mixed RT0 / P0 (``formulation="mixed"``,
+    ``degree=1``) formulation, homogeneous Dirichlet data, a constant source and a
+    constant or ``DiscInclusions`` permeability.  ``local_refinement`` may be one count
+    or one per cell (the uneven local sizes of a polygon batch).  Mixed solutions hold
+    each cell's fluxes, pressures and boundary multipliers, in that order."""
+    if formulation not in ("primal", "mixed"):
+        raise ValueError("formulation must be 'primal' or 'mixed'")
+    if formulation == "mixed" and int(degree) != 1:
+        raise ValueError("RT0 uses degree=1; higher-order primal locals use formulation=primal")
+    if formulation == "primal" and int(degree) != 2:
         raise NotImplementedError("the GPU polygon path implements the primal degree-two formulation")
     if local_meshes is not None or neumann:
         raise NotImplementedError("explicit local meshes and Neumann data are not on the GPU polygon path")
     if np.ndim(dirichlet) != 0 or float(dirichlet) != 0.0:
         raise NotImplementedError("the GPU polygon path takes homogeneous Dirichlet data")
-    plan = PolygonP2Plan(mesh, skeleton, local_refinement, order=max(int(quadrature_order), 4))
+    if formulation == "mixed" and skeleton is None:
+        from .topology import FaceSpace
+
+        skeleton = EdgeSkeleton(mesh, FaceSpace.uniform(0))
+    plan = PolygonP2Plan(mesh, skeleton, local_refinement, order=max(int(quadrature_order), 4),
+                         formulation=formulation)
     return plan.solve(permeability, source)
