@@ -85,6 +85,7 @@ constexpr size_t kSystemSmem = (size_t)kDThreads * kTileStride * sizeof(double);
 // augmented matrix alike), load at vec_off, actions at 3 vec_off, right-hand sides at
 // rhs_off, coupling at cpl_off[k] with tld_of[k] columns, and the cell's sizes, flag
 // and status at slot.
+template <bool kKernel>
 __global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
     int lds, int tld, int nb, int w, int normalize, const int32_t* __restrict__ n_of,
     const int32_t* __restrict__ t_of,
@@ -120,7 +121,7 @@ __global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
   double* act = action + aoff;  // rows: A 1, A^T 1, the constraint
   const double* ldv = load + loff;
   const double* cpl = coupling + coff;
-  const double* zk = kvec ? kvec + loff : nullptr;  // the declared kernel Z (null: ones)
+  const double* zk = kKernel ? kvec + loff : nullptr;  // the declared kernel Z (kKernel false: ones)
   if (tid == 0) nonzero = 0;
   // max |A| and ||A||_F^2, the retained action A 1 and the test action A^T 1 (double-double
   // sums, the reference's extended-precision _matrix_action), the plain products A 1
@@ -152,13 +153,20 @@ __global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
         for (int q = 0; q < 32; ++q) {
           if (q < jn) {
             const double a = tile[lane0 * kTileStride + q];
-            const double zq = zk ? zk[c0 + q] : 1.0;  // 0 or 1: the products are exact
             amax = fmax(amax, fabs(a));
             fro = fma(a, a, fro);
-            dd_add(hi, lo, a * zq);
-            plain += a * zq;
-            dd_add(chi, clo, colv[q] * zq);
-            cplain += colv[q] * zq;
+            if (kKernel) {
+              const double zq = zk[c0 + q];  // 0 or 1: the products are exact
+              dd_add(hi, lo, a * zq);
+              plain += a * zq;
+              dd_add(chi, clo, colv[q] * zq);
+              cplain += colv[q] * zq;
+            } else {
+              dd_add(hi, lo, a);
+              plain += a;
+              dd_add(chi, clo, colv[q]);
+              cplain += colv[q];
+            }
           }
         }
       }
@@ -168,7 +176,10 @@ __global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
         tile[q * kTileStride + lane0] = (r0 + q < n && c0 + lane0 < n) ? Mm[(int64_t)(r0 + q) * lds + c0 + lane0] : 0.0;
       __syncwarp();
       if (i < n)
-        for (int q = 0; q < jn; ++q) c += tile[lane0 * kTileStride + q] * (zk ? zk[c0 + q] : 1.0);
+        for (int q = 0; q < jn; ++q) {
+          const double m = tile[lane0 * kTileStride + q];
+          c += kKernel ? m * zk[c0 + q] : m;
+        }
       __syncwarp();
     }
     if (i < n) {
@@ -179,9 +190,12 @@ __global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
       r2 = fma(plain, plain, r2);
       l2 = fma(cplain, cplain, l2);
       act[2 * nb + i] = c;
-      const double zi = zk ? zk[i] : 1.0;
-      csum += zi * c;
-      zsum += zi * zi;
+      if (kKernel) {
+        csum += zk[i] * c;
+        zsum += zk[i] * zk[i];
+      } else {
+        csum += c;
+      }
     }
   }
   amax = block_max(amax, red);
@@ -189,7 +203,7 @@ __global__ void __launch_bounds__(kDThreads, 2) dense_system_kernel(
   r2 = block_sum(r2, red);
   l2 = block_sum(l2, red);
   csum = block_sum(csum, red);
-  zsum = block_sum(zsum, red);
+  zsum = kKernel ? block_sum(zsum, red) : (double)n;
   // the 2D drivers divide the constraint M Z by Z^T M Z, the cell's area (primal.py:
   // 69-71, 99-100); the 3D driver keeps M 1 (primal_3d.py:58-65)
   const double cdiv = normalize ? csum : 1.0;
@@ -386,10 +400,10 @@ int launch_systems(int64_t count, int32_t lds, int32_t tld, int32_t nb, int32_t 
   if (count < 1 || count > INT32_MAX || lds < 1 || tld < 1 || nb < 2 || nb > lds + 64 || w < 3 || !n_of ||
       !t_of || !stiffness || !mass || !load || !coupling || !aug || !rhs || !action || !corrected || !status)
     return MHM_ERR_ARGUMENT;
-  if (cudaFuncSetAttribute(dense_system_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSystemSmem) !=
-      cudaSuccess)
+  auto kernel = kvec ? dense_system_kernel<true> : dense_system_kernel<false>;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSystemSmem) != cudaSuccess)
     return MHM_ERR_LAUNCH;
-  dense_system_kernel<<<(unsigned)count, kDThreads, kSystemSmem, static_cast<cudaStream_t>(stream)>>>(
+  kernel<<<(unsigned)count, kDThreads, kSystemSmem, static_cast<cudaStream_t>(stream)>>>(
       lds, tld, nb, w, normalize, n_of, t_of, stiffness, mass, load, coupling, aug, rhs, action, corrected,
       status, nullptr, nullptr, nullptr, kvec);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
@@ -454,10 +468,10 @@ extern "C" int mhm_dense_systems_ragged(int64_t count, const mhm_ragged_matrix* 
   if (count < 1 || count > INT32_MAX || !desc || !cpl_off || !tld_of || !n_of || !t_of || !stiffness || !mass ||
       !load || !coupling || !aug || !rhs || !action || !corrected || !status)
     return MHM_ERR_ARGUMENT;
-  if (cudaFuncSetAttribute(dense_system_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSystemSmem) !=
-      cudaSuccess)
+  if (cudaFuncSetAttribute(dense_system_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kSystemSmem) != cudaSuccess)
     return MHM_ERR_LAUNCH;
-  dense_system_kernel<<<(unsigned)count, kDThreads, kSystemSmem, static_cast<cudaStream_t>(stream)>>>(
+  dense_system_kernel<false><<<(unsigned)count, kDThreads, kSystemSmem, static_cast<cudaStream_t>(stream)>>>(
       0, 0, 0, 0, normalize, n_of, t_of, stiffness, mass, load, coupling, aug, rhs, action, corrected, status, desc,
       cpl_off, tld_of, nullptr);
   return cudaGetLastError() == cudaSuccess ? MHM_OK : MHM_ERR_LAUNCH;
