@@ -81,3 +81,15 @@ def test_rt0_skeleton_alignment():
         check_rt0_skeleton(EdgeSkeleton(mesh, FaceSpace.uniform(0, 2)), [2, 3])
     with pytest.raises(ValueError, match="aligned"):
         check_rt0_skeleton(EdgeSkeleton(mesh, FaceSpace.uniform(1)), [2])
+
+
+def test_rt0_solve_darcy_arguments():
+    """The reference's argument errors (``primal.py:149-152, 245-249``), raised before
+    any device work."""
+    from pymhm_b200.polygon_darcy import solve_darcy
+
+    mesh = voronoi_mesh(12, 3)
+    with pytest.raises(ValueError, match="degree=1"):
+        solve_darcy(mesh, formulation="mixed", degree=2)
+    with pytest.raises(ValueError, match="formulation"):
+        solve_darcy(mesh, formulation="dual")
